@@ -1,0 +1,472 @@
+"""Benchmark of the B200 join + runtime-filter + aggregate path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload star|join|agg] [--scale S]
+
+Default workload (`star`): the star join with runtime Bloom filters --
+fact 300M rows {fk_a in [0, 20M), fk_b in [0, 1M), price, discount}, dim_a
+20M and dim_b 1M rows with a 5%-selective int32 predicate and a 25-value int32
+attribute; a blocked Bloom filter per filtered dimension applied to the fact
+scan, a two-join probe and GROUP BY dim_a.attr SUM(price * (1 - discount)).
+One step = one whole query (both dimension builds with their filters, the
+fact probe, the grouped result). The metric is fact rows per second
+(Mrows/s, higher is better).
+
+With --gpus N > 1 (torchrun, one process per GPU) every rank runs the query
+on its own shard of the fact stream (different fact rows, the same
+dimensions): weak scaling, no collective on the data path; the step time is
+the max over ranks.
+
+Inputs are generated on the device by the library's counter-based generators
+(synthetic, seeded). `value` is measured with inputs resident in HBM; `e2e`
+runs the same query through the C ABI with host Arrow buffers (pinned), the
+host-to-device copies inside the timed region. The fact columns (9.6 GB)
+exceed the 126 MB L2, so no L2 flush is needed between steps.
+
+--impl reference times the reference algorithm restated in C (the CPU oracle,
+multi-threaded over all host cores) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---- clocks during the timed region ------------------------------------------------------
+class Clocks:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        exe = shutil.which("nvidia-smi")
+        if exe:
+            self.proc = subprocess.Popen([exe, "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---- distributed plumbing ----------------------------------------------------------------
+def dist_init(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, value, device):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---- the CPU baseline (the oracle's multi-threaded restatement) ---------------------------
+def cpu_star(scale, sample_rows, threads, seed=None):
+    """Times the star query on the host cores with the CPU oracle on the first
+    `sample_rows` fact rows (dimensions at full size); returns the whole-query
+    rate extrapolated to the full fact table (build time + full probe)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+    W = importlib.import_module("krishiv-engine_b200.workloads")
+    seed = W.STAR_SEED if seed is None else seed
+    nf, na, nb = int(300_000_000 * scale), int(20_000_000 * scale), int(1_000_000 * scale)
+    s = min(sample_rows, nf)
+    L = O.lib()
+    fk_a, _ = O.gen_column(0, seed, 1, s, lo=0, hi=na - 1)
+    fk_b, _ = O.gen_column(0, seed, 2, s, lo=0, hi=nb - 1)
+    price, _ = O.gen_column(0, seed, 3, s, lo=1000, hi=10_000_000)
+    disc, _ = O.gen_column(2, seed, 4, s, x0=0.0, x1=0.1)
+    dims = []
+    for base, n in ((10, na), (20, nb)):
+        key, _ = O.gen_column(3, seed + base, base + 1, n, lo=0, hi=n)
+        pred, _ = O.gen_column(1, seed, base + 2, n, lo=0, hi=19)
+        attr, _ = O.gen_column(1, seed, base + 3, n, lo=0, hi=24)
+        dims.append((key, pred, attr))
+    vp, i64, i32, dbl = C.c_void_p, C.c_int64, C.c_int32, C.c_double
+    L.orc_star_query.restype = i64
+    L.orc_star_query.argtypes = [vp, vp, vp, i64, i32, vp, vp, vp, i64, i32, vp, vp, vp, vp, i64, i32, i32, i32,
+                                 vp, vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(dbl), C.POINTER(dbl)]
+    out_sum = np.zeros(4096)
+    out_cnt = np.zeros(4096, dtype=np.int64)
+    passed, joined, tb, tp = i64(), i64(), dbl(), dbl()
+    (ka, pa_, aa), (kb_, pb, ab) = dims
+    L.orc_star_query(ka.ctypes.data, pa_.ctypes.data, aa.ctypes.data, na, 7, kb_.ctypes.data, pb.ctypes.data,
+                     ab.ctypes.data, nb, 7, fk_a.ctypes.data, fk_b.ctypes.data, price.ctypes.data,
+                     disc.ctypes.data, s, 0, threads, 1, out_sum.ctypes.data, out_cnt.ctypes.data, C.byref(passed),
+                     C.byref(joined), C.byref(tb), C.byref(tp))
+    probe_rate = s / tp.value
+    whole = tb.value + nf / probe_rate
+    return {"value": nf / whole / 1e6, "build_s": tb.value, "probe_rows_per_s": probe_rate, "sample_rows": s,
+            "threads": threads, "groups": int((out_cnt > 0).sum()), "joined": joined.value}
+
+
+# ---- workloads on the GPU ----------------------------------------------------------------
+def run_star(args, kb, W, rt, rank, world, pg, device):
+    import torch
+    stream = torch.cuda.current_stream()
+    data = W.star(rt, scale=args.scale, fact_row0=rank * int(300_000_000 * args.scale))
+    torch.cuda.synchronize()
+    dim_a, dim_b, fact = kb.DeviceBatch(data.dim_a), kb.DeviceBatch(data.dim_b), kb.DeviceBatch(data.fact)
+
+    def make(mode):
+        return kb.StarPipeline(rt, kb.star_spec(W.PRED_VALUE, W.PRED_VALUE, group_by=0, mode=mode))
+
+    def timed(pipe, steps, warmup, kernel_events=None):
+        for _ in range(warmup):
+            pipe.reset()
+            pipe.build_device(dim_a, dim_b)
+            pipe.probe_device(fact)
+            pipe.result()
+        torch.cuda.synchronize()
+        barrier(pg)
+        launches0 = rt.launches
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        kev = []
+        start.record(stream)
+        for _ in range(steps):
+            pipe.reset()
+            pipe.build_device(dim_a, dim_b)
+            if kernel_events is not None:
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                pipe.probe_device(fact)
+                b.record(stream)
+                kev.append((a, b))
+            else:
+                pipe.probe_device(fact)
+            pipe.result()
+        end.record(stream)
+        torch.cuda.synchronize()
+        barrier(pg)
+        ms = start.elapsed_time(end) / steps
+        if kernel_events is not None:
+            kernel_events.extend(a.elapsed_time(b) for a, b in kev)
+        return ms, rt.launches - launches0
+
+    fused = make(kb.STAR_FUSED)
+    kernel_ms = []
+    with Clocks(device) as clk:
+        ms, launches = timed(fused, args.steps, args.warmup, kernel_ms)
+    ms_max = max_over_ranks(pg, ms, device)
+    counters = fused.counters()
+    result = fused.result()
+    plain = make(kb.STAR_PLAIN)
+    plain_ms, _ = timed(plain, max(2, args.steps // 2), 1)
+    plain_ms = max_over_ranks(pg, plain_ms, device)
+    plain_res = plain.result()
+    # fused and plain agree (same groups; sums within the float tolerance)
+    fr = dict(zip(result.column(0).to_pylist(), result.column(1).to_pylist()))
+    pr = dict(zip(plain_res.column(0).to_pylist(), plain_res.column(1).to_pylist()))
+    agree = sorted(fr) == sorted(pr) and all(abs(fr[k] - pr[k]) <= 1e-12 * abs(pr[k]) for k in fr)
+    nf = data.fact_rows
+    # The dominant kernel: the fused fact probe. Algorithmic bytes per launch:
+    # both key columns of every fact row, price and discount of the joined rows.
+    kern_ms = statistics.median(kernel_ms)
+    alg_bytes = 16 * nf + 16 * counters["joined_rows"]
+    peak, peak_kind = hbm_peak()
+    achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
+    out = {
+        "metric": "star join+agg probe Mrows/s (fact rows per second, whole query)",
+        "value": world * nf / (ms_max * 1e-3) / 1e6,
+        "unit": "Mrows/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int64 keys, float64 sums",
+        "data": "synthetic (seeded counter-based generators on the device)",
+        "config": {"workload": "star join + runtime Bloom filters + GROUP BY attr SUM(price*(1-discount))",
+                   "fact_rows_per_gpu": nf, "dim_a_rows": data.dim_a_rows, "dim_b_rows": data.dim_b_rows,
+                   "selectivity": "5% per dimension", "groups": 25, "mode": "fused (batched) pipeline",
+                   "l2": "inputs (9.6 GB per GPU) larger than L2; no flush"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "star_fused_kernel", "achieved": achieved, "peak": peak,
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": profile_traffic("star_fused_kernel", nf),
+                     "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms},
+        "plain": {"ms_per_step": plain_ms, "value": world * nf / (plain_ms * 1e-3) / 1e6,
+                  "fused_speedup": plain_ms / ms_max, "results_agree": agree},
+        "counters": {k: counters[k] for k in ("passed_filters", "joined_rows", "dim_a_keys", "dim_b_keys",
+                                              "filter_a_bytes", "filter_b_bytes")},
+        "clocks": clk.summary(),
+    }
+    del plain
+    if not args.no_e2e:
+        out["e2e"] = run_star_e2e(args, kb, rt, data, pg, device)
+    return out
+
+
+def run_star_e2e(args, kb, rt, data, pg, device):
+    """The same query through the C ABI with host (pinned) Arrow buffers; the
+    host-to-device copies and the result's device-to-host read are timed."""
+    import pyarrow as pa
+    import torch
+
+    def host_batch(cols):
+        arrays, names, keep = [], [], []
+        for name, t, _ in cols:
+            h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            h.copy_(t)
+            keep.append(h)
+            arrays.append(pa.array(h.numpy()))
+            names.append(name)
+        return pa.RecordBatch.from_arrays(arrays, names=names), keep
+
+    fact, k1 = host_batch(data.fact)
+    dim_a, k2 = host_batch(data.dim_a)
+    dim_b, k3 = host_batch(data.dim_b)
+    pipe = kb.StarPipeline(rt, kb.star_spec(7, 7, group_by=0, mode=kb.STAR_FUSED))
+    steps = max(2, args.steps // 2)
+    for _ in range(1):
+        pipe.reset()
+        pipe.build(dim_a, dim_b)
+        pipe.probe(fact)
+        pipe.result()
+    torch.cuda.synchronize()
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        pipe.reset()
+        pipe.build(dim_a, dim_b)
+        pipe.probe(fact)
+        res = pipe.result()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    dt = max_over_ranks(pg, dt, device)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    h2d = sum(t.numel() * t.element_size() for _, t, _ in data.fact + data.dim_a + data.dim_b)
+    return {"value": world * data.fact_rows / dt / 1e6, "unit": "Mrows/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": res.num_rows * 12, "ms_per_step": dt * 1e3, "steps": steps,
+            "timing": "host wall clock around synchronous C-ABI calls"}
+
+
+def profile_traffic(kernel, rows):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/<kernel>.md: 'dram_bytes_per_row: X'), scaled to `rows`."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_row:"):
+                return float(line.split(":")[1]) * rows
+    except OSError:
+        pass
+    return None
+
+
+def run_join(args, kb, W, rt, rank, world, pg, device):
+    import torch
+    stream = torch.cuda.current_stream()
+    build, probe = W.join(rt, scale=args.scale)
+    torch.cuda.synchronize()
+    bb, pb = kb.DeviceBatch(build), kb.DeviceBatch(probe)
+    nb, np_ = int(build[0][1].shape[0]), int(probe[0][1].shape[0])
+
+    def step():
+        j = kb.HashJoin(rt, kb.join_spec("inner", probe_out=[0, 1], build_out=[1], build_rows_hint=nb))
+        j.build_push_device(bb)
+        j.build_finish()
+        r = j.probe_device(pb)
+        return j, r
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(pg)
+    launches0 = rt.launches
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(args.steps):
+        j, r = step()
+    e.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(pg, s.elapsed_time(e) / args.steps, device)
+    out_rows = r.rows
+    alg = 16 * nb + 12 * np_ + 20 * out_rows
+    peak, kind = hbm_peak()
+    return {"metric": "plain inner hash join (build+probe rows per second)",
+            "value": world * (nb + np_) / (ms * 1e-3) / 1e6, "unit": "Mrows/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64 keys", "data": "synthetic",
+            "config": {"workload": "inner join 1M build x 10M probe (50% match), output (k, v, w)",
+                       "build_rows": nb, "probe_rows": np_, "output_rows": out_rows},
+            "gpu_launches": rt.launches - launches0,
+            "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "peak_source": kind,
+                         "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None}}
+
+
+def run_agg(args, kb, W, rt, rank, world, pg, device):
+    import torch
+    stream = torch.cuda.current_stream()
+    cols = W.agg(rt, scale=args.scale)
+    torch.cuda.synchronize()
+    db = kb.DeviceBatch(cols)
+    n = int(cols[0][1].shape[0])
+    aggs = [(f, c) for c in (1, 2, 3) for f in ("sum", "count", "min", "max", "avg")]
+
+    def step(mode):
+        a = kb.HashAggregate(rt, kb.agg_spec(0, aggs, mode=mode, expected_groups=1_000_000))
+        a.push_device(db)
+        a.finish()
+        return a.result_device()
+
+    res = {}
+    for mode, name in ((kb.MODE_SHARED, "shared"), (kb.MODE_GLOBAL, "global")):
+        for _ in range(args.warmup):
+            step(mode)
+        torch.cuda.synchronize()
+        barrier(pg)
+        launches0 = rt.launches
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(args.steps):
+            r = step(mode)
+        e.record(stream)
+        torch.cuda.synchronize()
+        res[name] = (max_over_ranks(pg, s.elapsed_time(e) / args.steps, device), rt.launches - launches0, r.rows)
+    ms, launches, groups = res["shared"]
+    alg = n * (8 + 8 + 8 + 4 + 3 / 8) + groups * 136
+    peak, kind = hbm_peak()
+    return {"metric": "grouped aggregate rows per second", "value": world * n / (ms * 1e-3) / 1e6, "unit": "Mrows/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int128/double-double",
+            "data": "synthetic", "config": {"workload": "100M rows Zipf(1.1) over 1M keys, 15 aggregates",
+                                            "rows": n, "groups": groups},
+            "gpu_launches": launches,
+            "plain_global_table": {"ms_per_step": res["global"][0], "value": world * n / (res["global"][0] * 1e-3) / 1e6},
+            "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "peak_source": kind,
+                         "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["star", "join", "agg"], default="star")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=20_000_000)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local, pg = dist_init(args.gpus)
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        steps = []
+        info = None
+        for _ in range(args.warmup + args.steps):
+            info = cpu_star(args.scale, min(args.cpu_sample, 5_000_000), threads)
+            steps.append(info["value"])
+        v = statistics.median(steps[args.warmup:])
+        line = {"impl": "reference", "metric": "star join+agg probe Mrows/s (fact rows per second, whole query)",
+                "value": v, "unit": "Mrows/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "config": {"workload": "star join + runtime Bloom filters + GROUP BY attr SUM(price*(1-discount))",
+                           "fact_rows": int(300_000_000 * args.scale)},
+                "cpu_baseline": {"value": v, "unit": "Mrows/s", "cores": threads, "kind": "port",
+                                 "sample": f"full dimensions, first {info['sample_rows']} fact rows per step, "
+                                           "whole-query rate extrapolated (build + full probe)"},
+                "e2e": {"value": v, "unit": "Mrows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    device = local
+    kb = importlib.import_module("krishiv-engine_b200")
+    W = importlib.import_module("krishiv-engine_b200.workloads")
+    rt = kb.Runtime(local, 0, torch.cuda.current_stream().cuda_stream)
+    runner = {"star": run_star, "join": run_join, "agg": run_agg}[args.workload]
+    out = runner(args, kb, W, rt, rank, world, pg, device)
+    if rank == 0 and args.workload == "star" and not args.no_cpu:
+        c = cpu_star(args.scale, args.cpu_sample, threads)
+        out["cpu_baseline"] = {"value": c["value"], "unit": "Mrows/s", "cores": threads, "kind": "port",
+                               "sample": f"full dimensions + first {c['sample_rows']} fact rows, whole-query "
+                                         f"rate extrapolated to {int(300_000_000 * args.scale)} rows "
+                                         f"(build {c['build_s']:.2f} s, probe {c['probe_rows_per_s'] / 1e6:.1f} Mrows/s)"}
+    if rank == 0:
+        print(json.dumps(out))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,359 @@
+/*
+ * krv_gpu.h -- C ABI of the B200 (sm_100a) hash join, grouped hash aggregate
+ * and runtime key filter (split-block Bloom) operators.
+ *
+ * The operators are drop-ins for the Krishiv engine's physical operators on
+ * this path. Each entry point names the reference interface it replaces
+ * (file:line in the Krishiv engine repository). Data crosses as Arrow
+ * RecordBatches through the Arrow C Data Interface (host buffers) or the
+ * Arrow C Device Data Interface (CUDA device buffers), see krv_arrow.h.
+ *
+ * Conventions
+ *  - Every call returns a krv_status. Negative values are errors; the text
+ *    of the last error on the calling thread is krv_last_error().
+ *  - Inputs are borrowed: the caller owns an input ArrowArray until the call
+ *    returns and the library never calls its release callback. Outputs are
+ *    moved to the caller, who releases them (the C Data Interface's release
+ *    callback frees the library-owned buffers).
+ *  - A handle is thread-compatible: one thread at a time. Every handle runs
+ *    on its runtime's CUDA stream. A built join table is read-only after
+ *    krv_join_build_finish.
+ *  - Device memory is charged to the runtime's HBM budget; a call that would
+ *    exceed it returns KRV_NEED_MEMORY and krv_last_need_bytes() tells how
+ *    many bytes it asked for (the reference's SinkStatus::NeedMemory /
+ *    OperatorOutput::NeedMemory, crates/krishiv-exec/src/operator.rs:188-477).
+ *  - Kernels never trap. They report errors through a device status word.
+ */
+#ifndef KRV_GPU_H
+#define KRV_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "krv_arrow.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Every declaration below is an exported symbol of libkrv_gpu.so (the
+ * library builds with hidden visibility by default). */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef int32_t krv_status;
+
+/* Operator protocol (OperatorOutput / SinkStatus, operator.rs:188-311, 346-477) */
+#define KRV_OK 0
+#define KRV_NEED_MORE_INPUT 1   /* output (if any) written; feed the next batch */
+#define KRV_HAVE_MORE_OUTPUT 2  /* output written; call again with no input */
+#define KRV_FINISHED 3          /* no more output */
+/* Errors (KrishivError classes the path raises) */
+#define KRV_INVALID_ARGUMENT (-1)
+#define KRV_UNSUPPORTED (-2)          /* KRISHIV_UNSUPPORTED_FEATURE, join/mod.rs:745-752 */
+#define KRV_NEED_MEMORY (-3)          /* over the HBM budget */
+#define KRV_ARITHMETIC_OVERFLOW (-4)  /* ARITHMETIC_OVERFLOW, aggregate/mod.rs:1177 (ANSI) */
+#define KRV_CUDA_ERROR (-5)
+#define KRV_TIMEOUT (-6)              /* a device wait gave up (bounded spin) */
+#define KRV_TOO_MANY_ROWS (-7)        /* SCALAR_SUBQUERY_TOO_MANY_ROWS (single-match join) */
+#define KRV_INTERNAL (-8)
+
+/* Text of the last failing call on this thread ("" if none). */
+const char *krv_last_error(void);
+/* Bytes the last KRV_NEED_MEMORY on this thread asked for. */
+int64_t krv_last_need_bytes(void);
+/* Library version string. */
+const char *krv_version(void);
+
+/* ---- runtime: device, stream and HBM budget ------------------------------ */
+typedef struct krv_runtime krv_runtime;
+/* `cuda_stream` (a cudaStream_t) or NULL for a stream the runtime creates.
+ * `hbm_budget_bytes` <= 0: no budget beyond the device's free memory.
+ * Replaces the per-query memory pool (crates/krishiv-memory/src/lib.rs:1-30)
+ * for device memory. */
+krv_status krv_runtime_create(int32_t device, int64_t hbm_budget_bytes, void *cuda_stream,
+                              krv_runtime **out);
+void krv_runtime_destroy(krv_runtime *rt);
+krv_status krv_runtime_synchronize(krv_runtime *rt);
+int64_t krv_runtime_used_bytes(const krv_runtime *rt);
+int64_t krv_runtime_budget_bytes(const krv_runtime *rt);
+void *krv_runtime_stream(const krv_runtime *rt);
+/* Kernels this library launched on the runtime since it was created. */
+int64_t krv_runtime_launches(const krv_runtime *rt);
+
+/* ---- hash join ------------------------------------------------------------ */
+/* JoinType, crates/krishiv-exec/src/join/mod.rs:216-293 */
+#define KRV_JOIN_INNER 0
+#define KRV_JOIN_LEFT_OUTER 1
+#define KRV_JOIN_LEFT_SEMI 2
+#define KRV_JOIN_LEFT_ANTI 3
+#define KRV_JOIN_NULL_AWARE_ANTI 4
+#define KRV_JOIN_EXISTENCE 5
+#define KRV_JOIN_RIGHT_SEMI 6
+#define KRV_JOIN_RIGHT_ANTI 7
+#define KRV_JOIN_RIGHT_OUTER 8
+#define KRV_JOIN_FULL_OUTER 9
+
+#define KRV_MAX_KEYS 4
+#define KRV_MAX_OUT_COLUMNS 32
+
+/* JoinSpec, join/mod.rs:327-350, plus the join's config keys
+ * (krishiv.exec.join.radixBits, crates/krishiv-common/src/config/
+ * registry_join.rs:11-160) and the runtime filter options. */
+typedef struct {
+    int32_t join_type;                     /* KRV_JOIN_* */
+    int32_t n_keys;                        /* 1..KRV_MAX_KEYS */
+    int32_t probe_keys[KRV_MAX_KEYS];      /* probe (left) key columns */
+    int32_t build_keys[KRV_MAX_KEYS];      /* build (right) key columns */
+    int32_t null_safe[KRV_MAX_KEYS];       /* `<=>` instead of `=` */
+    int32_t single_match;                  /* LeftOuter only: > 1 match fails */
+    int32_t has_residual_filter;           /* must be 0: residual filters are unsupported */
+    /* Output projection: probe columns then build columns. -1 = every column. */
+    int32_t n_probe_out;
+    int32_t probe_out[KRV_MAX_OUT_COLUMNS];
+    int32_t n_build_out;
+    int32_t build_out[KRV_MAX_OUT_COLUMNS];
+    /* Tuning; 0 selects the autotuned value. */
+    int32_t radix_bits;        /* level-0 partitions of a partitioned build */
+    float max_load;            /* hash-table load factor */
+    uint64_t seed;             /* table hash seed g = fin(h ^ seed) (0: fixed default) */
+    int32_t runtime_filter;    /* build a key filter at build_finish (one key only) */
+    int32_t pad0;
+    int64_t build_rows_hint;   /* presize the build arena */
+    int64_t max_output_rows;   /* output batch bound; 0 = one batch per input */
+} krv_join_spec;
+void krv_join_spec_init(krv_join_spec *spec);
+
+/* Counters (join/mod.rs:353-607) */
+typedef struct {
+    int64_t build_rows;
+    int64_t build_keys;        /* distinct keys indexed */
+    int64_t table_slots;
+    int64_t probe_rows;
+    int64_t output_rows;
+    int64_t max_chain;         /* longest duplicate chain */
+    int64_t partitions;        /* level-0 partitions of a partitioned build */
+} krv_join_counters;
+
+typedef struct krv_join krv_join;
+typedef struct krv_key_filter krv_key_filter;
+
+/* HashJoin::try_new (join/mod.rs:1014) */
+krv_status krv_join_create(krv_runtime *rt, const krv_join_spec *spec, krv_join **out);
+/* BuildSink::sink (join/build.rs:1225-1335) */
+krv_status krv_join_build_push(krv_join *j, const struct ArrowArray *batch,
+                               const struct ArrowSchema *schema);
+krv_status krv_join_build_push_device(krv_join *j, const struct ArrowDeviceArray *batch,
+                                      const struct ArrowSchema *schema);
+/* BuildSink::finalize (join/build.rs:1366-1695) */
+krv_status krv_join_build_finish(krv_join *j);
+/* ProbeOp::execute (join/probe.rs:1103): joins `in` (NULL to drain pending
+ * output) into `out`. KRV_NEED_MORE_INPUT when this input is done,
+ * KRV_HAVE_MORE_OUTPUT when more output waits. */
+krv_status krv_join_probe(krv_join *j, const struct ArrowArray *in,
+                          const struct ArrowSchema *in_schema, struct ArrowArray *out,
+                          struct ArrowSchema *out_schema);
+krv_status krv_join_probe_device(krv_join *j, const struct ArrowDeviceArray *in,
+                                 const struct ArrowSchema *in_schema,
+                                 struct ArrowDeviceArray *out, struct ArrowSchema *out_schema);
+/* ProbeOp::finish / end_input (join/probe.rs:1149-1228) and emit_build
+ * (:610-): rows emitted once every probe row is known (right semi/anti,
+ * right/full outer build rows). KRV_HAVE_MORE_OUTPUT or KRV_FINISHED. */
+krv_status krv_join_finish(krv_join *j, struct ArrowArray *out, struct ArrowSchema *out_schema);
+krv_status krv_join_finish_device(krv_join *j, struct ArrowDeviceArray *out,
+                                  struct ArrowSchema *out_schema);
+/* The runtime filter published at build_finish (BuildSink::publish,
+ * join/build.rs:482). A new reference: destroy it with krv_key_filter_destroy. */
+krv_status krv_join_key_filter(krv_join *j, krv_key_filter **out);
+krv_status krv_join_counters_get(const krv_join *j, krv_join_counters *out);
+void krv_join_destroy(krv_join *j);
+
+/* ---- grouped hash aggregate ---------------------------------------------- */
+/* AggregateFunction (aggregate/mod.rs:134), the core five */
+#define KRV_AGG_COUNT_STAR 0
+#define KRV_AGG_COUNT 1
+#define KRV_AGG_SUM 2
+#define KRV_AGG_MIN 3
+#define KRV_AGG_MAX 4
+#define KRV_AGG_AVG 5
+
+#define KRV_AGG_MODE_AUTO 0
+#define KRV_AGG_MODE_GLOBAL 1   /* one global hash table */
+#define KRV_AGG_MODE_SHARED 2   /* shared-memory pre-aggregation + global table */
+
+#define KRV_MAX_AGGREGATES 32
+
+typedef struct {
+    int32_t function;  /* KRV_AGG_* */
+    int32_t column;    /* input column (ignored by COUNT(*)) */
+} krv_agg_expr;
+
+/* AggregateSpec, aggregate/mod.rs:1083-1108 (final output, one group key) */
+typedef struct {
+    int32_t n_group_by;             /* 1 (one int32/int64 key column) */
+    int32_t group_by[KRV_MAX_KEYS];
+    int32_t n_aggregates;
+    krv_agg_expr aggregates[KRV_MAX_AGGREGATES];
+    int32_t ansi;                   /* spark.sql.ansi.enabled: overflow raises */
+    int32_t mode;                   /* KRV_AGG_MODE_* */
+    int64_t expected_groups;        /* planner estimate (0: unknown) */
+    int64_t max_output_rows;        /* output batch bound; 0 = one batch */
+} krv_agg_spec;
+void krv_agg_spec_init(krv_agg_spec *spec);
+
+typedef struct krv_agg krv_agg;
+/* HashAggregate::new (aggregate/sink.rs:222) */
+krv_status krv_agg_create(krv_runtime *rt, const krv_agg_spec *spec, krv_agg **out);
+/* HashAggregate::sink (aggregate/sink.rs:1459) */
+krv_status krv_agg_push(krv_agg *a, const struct ArrowArray *batch,
+                        const struct ArrowSchema *schema);
+krv_status krv_agg_push_device(krv_agg *a, const struct ArrowDeviceArray *batch,
+                               const struct ArrowSchema *schema);
+/* HashAggregate::finalize (aggregate/sink.rs:1585) */
+krv_status krv_agg_finish(krv_agg *a);
+/* impl Source for HashAggregate (aggregate/sink.rs:1854): the next result
+ * batch (group key, then one column per aggregate). KRV_HAVE_MORE_OUTPUT
+ * while more batches wait, KRV_FINISHED with the last one. */
+krv_status krv_agg_next_output(krv_agg *a, struct ArrowArray *out,
+                               struct ArrowSchema *out_schema);
+krv_status krv_agg_next_output_device(krv_agg *a, struct ArrowDeviceArray *out,
+                                      struct ArrowSchema *out_schema);
+/* Groups currently in the table. */
+int64_t krv_agg_groups(const krv_agg *a);
+void krv_agg_destroy(krv_agg *a);
+
+/* ---- runtime key filter (split-block Bloom) ------------------------------- */
+/* KeyFilterOptions, crates/krishiv-io/src/runtime_filter/filter.rs:29-73 */
+typedef struct {
+    int64_t max_values;        /* 50 */
+    int64_t exact_max_values;  /* 4096 (member.rs:38) */
+    int32_t bloom;             /* 1 */
+    int32_t pad0;
+    int64_t bloom_max_items;   /* 4,000,000 */
+    int64_t bloom_max_bytes;   /* 8 MiB */
+    double bloom_fpp;          /* 0.01 */
+    double bloom_max_fpp;      /* 0.05 */
+    int64_t bloom_bytes;       /* planned size, 0 = sized for the keys */
+} krv_key_filter_options;
+/* KeyFilterOptions::default (filter.rs:89-104) */
+void krv_key_filter_options_default(krv_key_filter_options *o);
+
+#define KRV_FILTER_RANGE 0   /* min/max only (or a dense range: exact) */
+#define KRV_FILTER_EXACT 1   /* exact set of <= exact_max_values keys */
+#define KRV_FILTER_BLOOM 2   /* range + split-block Bloom filter */
+#define KRV_FILTER_EMPTY 3   /* no key: nothing passes */
+
+typedef struct {
+    int32_t form;
+    int32_t nulls_pass;
+    int32_t has_range;
+    int32_t pad0;
+    int64_t lo, hi;
+    int64_t keys;         /* non-NULL keys added, duplicates counted */
+    int64_t distinct;     /* distinct keys (exact) */
+    int64_t bloom_bytes;
+} krv_key_filter_info;
+
+/* KeyFilterBuilder::add + finish (filter.rs:157-593) over column `column` of
+ * `batch` (int64 keys; NULL keys are not kept, as for an `=` join key). */
+krv_status krv_key_filter_build(krv_runtime *rt, const krv_key_filter_options *opt,
+                                const struct ArrowArray *batch, const struct ArrowSchema *schema,
+                                int32_t column, krv_key_filter **out);
+krv_status krv_key_filter_build_device(krv_runtime *rt, const krv_key_filter_options *opt,
+                                       const struct ArrowDeviceArray *batch,
+                                       const struct ArrowSchema *schema, int32_t column,
+                                       krv_key_filter **out);
+/* KeyFilter::evaluate (filter.rs:768-798): a boolean column, TRUE where the
+ * row of `column` may match. */
+krv_status krv_key_filter_evaluate(krv_key_filter *f, const struct ArrowArray *batch,
+                                   const struct ArrowSchema *schema, int32_t column,
+                                   struct ArrowArray *out, struct ArrowSchema *out_schema);
+krv_status krv_key_filter_evaluate_device(krv_key_filter *f, const struct ArrowDeviceArray *batch,
+                                          const struct ArrowSchema *schema, int32_t column,
+                                          struct ArrowDeviceArray *out,
+                                          struct ArrowSchema *out_schema);
+krv_status krv_key_filter_info_get(const krv_key_filter *f, krv_key_filter_info *out);
+/* The Bloom bits in the Parquet SBBF layout (RuntimeBloom::to_bytes). */
+krv_status krv_key_filter_bloom_bytes(const krv_key_filter *f, void *host_out, int64_t nbytes);
+void krv_key_filter_destroy(krv_key_filter *f);
+
+/* ---- star join pipeline (runtime filter + two joins + grouped sum) --------
+ * The fused plan shape
+ *   SELECT d.attr, SUM(f.price * (1 - f.discount))
+ *   FROM fact f JOIN dim_a a ON f.fk_a = a.key JOIN dim_b b ON f.fk_b = b.key
+ *   WHERE a.pred = :pa AND b.pred = :pb GROUP BY <a or b>.attr
+ * built from the operators above: HashJoinNode (join/mod.rs:1188-1211) twice,
+ * the runtime filters they publish applied to the fact scan's row stage
+ * (crates/krishiv-exec/src/operators/runtime_filter.rs:1-45) and a
+ * HashAggregate. KRV_STAR_FUSED runs the fact side as one persistent kernel;
+ * KRV_STAR_PLAIN runs one operator per launch through the operator API. */
+#define KRV_STAR_FUSED 0
+#define KRV_STAR_PLAIN 1
+typedef struct {
+    int32_t dim_key, dim_pred, dim_attr;             /* columns of both dimension batches */
+    int32_t pred_a, pred_b;                          /* the equality constants */
+    int32_t fact_fk_a, fact_fk_b, fact_price, fact_discount;
+    int32_t group_by;                                /* 0: dim_a.attr, 1: dim_b.attr */
+    int32_t use_filters;                             /* apply the runtime filters */
+    int32_t mode;                                    /* KRV_STAR_* */
+} krv_star_spec;
+void krv_star_spec_init(krv_star_spec *spec);
+typedef struct krv_star krv_star;
+typedef struct {
+    int64_t fact_rows;
+    int64_t passed_filters;    /* fact rows that passed both runtime filters */
+    int64_t joined_rows;       /* fact rows that joined both dimensions */
+    int64_t dim_a_keys, dim_b_keys;
+    int32_t filter_a_form, filter_b_form;
+    int64_t filter_a_bytes, filter_b_bytes;
+} krv_star_counters;
+krv_status krv_star_create(krv_runtime *rt, const krv_star_spec *spec, krv_star **out);
+krv_status krv_star_build(krv_star *s, const struct ArrowArray *dim_a,
+                          const struct ArrowSchema *schema_a, const struct ArrowArray *dim_b,
+                          const struct ArrowSchema *schema_b);
+krv_status krv_star_build_device(krv_star *s, const struct ArrowDeviceArray *dim_a,
+                                 const struct ArrowSchema *schema_a,
+                                 const struct ArrowDeviceArray *dim_b,
+                                 const struct ArrowSchema *schema_b);
+/* Adds one fact batch to the running aggregate. */
+krv_status krv_star_probe(krv_star *s, const struct ArrowArray *fact,
+                          const struct ArrowSchema *schema);
+krv_status krv_star_probe_device(krv_star *s, const struct ArrowDeviceArray *fact,
+                                 const struct ArrowSchema *schema);
+/* The result so far: (attr int32, sum float64), one row per group with rows. */
+krv_status krv_star_result(krv_star *s, struct ArrowArray *out, struct ArrowSchema *out_schema);
+krv_status krv_star_reset(krv_star *s);
+krv_status krv_star_counters_get(const krv_star *s, krv_star_counters *out);
+void krv_star_destroy(krv_star *s);
+
+/* ---- synthetic data on the device (benchmarks) ----------------------------
+ * Counter-based SplitMix64 generators: value(seed, column, row) is the same
+ * function on every device and in the CPU test oracle. */
+#define KRV_GEN_UNIFORM_I64 0   /* int64 uniform in [lo, hi] */
+#define KRV_GEN_UNIFORM_I32 1   /* int32 uniform in [lo, hi] */
+#define KRV_GEN_UNIT_F64 2      /* float64 lo + (hi - lo) * u, u uniform in [0, 1) */
+#define KRV_GEN_PERMUTATION 3   /* int64 permutation of [0, n) (lo + perm) */
+#define KRV_GEN_ZIPF 4          /* int64: a Zipf(s = x0) rank over [0, hi) through a permutation */
+typedef struct {
+    int32_t kind;
+    uint32_t column;       /* stream id of this column */
+    uint64_t seed;
+    int64_t lo, hi;        /* integer bounds / scale */
+    double x0, x1;         /* float bounds / Zipf exponent */
+    double null_fraction;  /* share of NULL rows (validity stream column + 0x10000) */
+    int64_t row0;          /* first row number (generate rows [row0, row0 + n)) */
+} krv_gen_spec;
+/* Fills `n` values at device pointer `out` (and the validity bitmap at
+ * `out_valid`, bit offset 0, when null_fraction > 0 and out_valid != NULL). */
+krv_status krv_gen_fill(krv_runtime *rt, const krv_gen_spec *spec, int64_t n, void *out,
+                        void *out_valid);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif

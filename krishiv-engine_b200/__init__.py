@@ -1,0 +1,713 @@
+"""Python binding of libkrv_gpu.so, the B200 hash join, grouped aggregate and
+runtime key filter operators (C ABI: include/krv_gpu.h).
+
+The package directory name has a hyphen, so import it with importlib:
+
+    kb = importlib.import_module("krishiv-engine_b200")
+
+Data crosses as Arrow record batches: pyarrow batches through the Arrow C Data
+Interface (host buffers), or device columns (torch CUDA tensors) through the
+Arrow C Device Data Interface. There is no CPU fallback: if the CUDA library
+is missing every call fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, List, Optional, Sequence
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkrv_gpu.so")
+
+# ---- status codes (krv_gpu.h) --------------------------------------------------------
+OK, NEED_MORE_INPUT, HAVE_MORE_OUTPUT, FINISHED = 0, 1, 2, 3
+INVALID_ARGUMENT, UNSUPPORTED, NEED_MEMORY, ARITHMETIC_OVERFLOW = -1, -2, -3, -4
+CUDA_ERROR, TIMEOUT, TOO_MANY_ROWS, INTERNAL = -5, -6, -7, -8
+
+INNER, LEFT_OUTER, LEFT_SEMI, LEFT_ANTI, NULL_AWARE_ANTI, EXISTENCE = 0, 1, 2, 3, 4, 5
+RIGHT_SEMI, RIGHT_ANTI, RIGHT_OUTER, FULL_OUTER = 6, 7, 8, 9
+JOIN_TYPES = {"inner": INNER, "left_outer": LEFT_OUTER, "left_semi": LEFT_SEMI, "left_anti": LEFT_ANTI,
+              "null_aware_anti": NULL_AWARE_ANTI, "existence": EXISTENCE, "right_semi": RIGHT_SEMI,
+              "right_anti": RIGHT_ANTI, "right_outer": RIGHT_OUTER, "full_outer": FULL_OUTER}
+
+COUNT_STAR, COUNT, SUM, MIN, MAX, AVG = 0, 1, 2, 3, 4, 5
+AGG_FUNCS = {"count_star": COUNT_STAR, "count": COUNT, "sum": SUM, "min": MIN, "max": MAX, "avg": AVG}
+MODE_AUTO, MODE_GLOBAL, MODE_SHARED = 0, 1, 2
+
+FILTER_RANGE, FILTER_EXACT, FILTER_BLOOM, FILTER_EMPTY = 0, 1, 2, 3
+STAR_FUSED, STAR_PLAIN = 0, 1
+
+GEN_UNIFORM_I64, GEN_UNIFORM_I32, GEN_UNIT_F64, GEN_PERMUTATION, GEN_ZIPF = 0, 1, 2, 3, 4
+
+MAX_KEYS = 4
+MAX_OUT = 32
+MAX_AGGS = 32
+
+
+class KrvError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+# ---- Arrow C (Device) Data Interface --------------------------------------------------
+class ArrowSchema(C.Structure):
+    pass
+
+
+ArrowSchema._fields_ = [("format", C.c_char_p), ("name", C.c_char_p), ("metadata", C.c_char_p),
+                        ("flags", C.c_int64), ("n_children", C.c_int64),
+                        ("children", C.POINTER(C.POINTER(ArrowSchema))),
+                        ("dictionary", C.POINTER(ArrowSchema)),
+                        ("release", C.CFUNCTYPE(None, C.POINTER(ArrowSchema))),
+                        ("private_data", C.c_void_p)]
+
+
+class ArrowArray(C.Structure):
+    pass
+
+
+ArrowArray._fields_ = [("length", C.c_int64), ("null_count", C.c_int64), ("offset", C.c_int64),
+                       ("n_buffers", C.c_int64), ("n_children", C.c_int64),
+                       ("buffers", C.POINTER(C.c_void_p)),
+                       ("children", C.POINTER(C.POINTER(ArrowArray))),
+                       ("dictionary", C.POINTER(ArrowArray)),
+                       ("release", C.CFUNCTYPE(None, C.POINTER(ArrowArray))),
+                       ("private_data", C.c_void_p)]
+
+
+class ArrowDeviceArray(C.Structure):
+    _fields_ = [("array", ArrowArray), ("device_id", C.c_int64), ("device_type", C.c_int32),
+                ("sync_event", C.c_void_p), ("reserved", C.c_int64 * 3)]
+
+
+ARROW_DEVICE_CUDA = 2
+
+# ---- specs (krv_gpu.h) ------------------------------------------------------------------
+class JoinSpec(C.Structure):
+    _fields_ = [("join_type", C.c_int32), ("n_keys", C.c_int32), ("probe_keys", C.c_int32 * MAX_KEYS),
+                ("build_keys", C.c_int32 * MAX_KEYS), ("null_safe", C.c_int32 * MAX_KEYS),
+                ("single_match", C.c_int32), ("has_residual_filter", C.c_int32),
+                ("n_probe_out", C.c_int32), ("probe_out", C.c_int32 * MAX_OUT),
+                ("n_build_out", C.c_int32), ("build_out", C.c_int32 * MAX_OUT),
+                ("radix_bits", C.c_int32), ("max_load", C.c_float), ("seed", C.c_uint64),
+                ("runtime_filter", C.c_int32), ("pad0", C.c_int32), ("build_rows_hint", C.c_int64),
+                ("max_output_rows", C.c_int64)]
+
+
+class JoinCounters(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("build_rows", "build_keys", "table_slots", "probe_rows",
+                                         "output_rows", "max_chain", "partitions")]
+
+
+class AggExpr(C.Structure):
+    _fields_ = [("function", C.c_int32), ("column", C.c_int32)]
+
+
+class AggSpec(C.Structure):
+    _fields_ = [("n_group_by", C.c_int32), ("group_by", C.c_int32 * MAX_KEYS), ("n_aggregates", C.c_int32),
+                ("aggregates", AggExpr * MAX_AGGS), ("ansi", C.c_int32), ("mode", C.c_int32),
+                ("expected_groups", C.c_int64), ("max_output_rows", C.c_int64)]
+
+
+class KeyFilterOptions(C.Structure):
+    _fields_ = [("max_values", C.c_int64), ("exact_max_values", C.c_int64), ("bloom", C.c_int32),
+                ("pad0", C.c_int32), ("bloom_max_items", C.c_int64), ("bloom_max_bytes", C.c_int64),
+                ("bloom_fpp", C.c_double), ("bloom_max_fpp", C.c_double), ("bloom_bytes", C.c_int64)]
+
+
+class KeyFilterInfo(C.Structure):
+    _fields_ = [("form", C.c_int32), ("nulls_pass", C.c_int32), ("has_range", C.c_int32), ("pad0", C.c_int32),
+                ("lo", C.c_int64), ("hi", C.c_int64), ("keys", C.c_int64), ("distinct", C.c_int64),
+                ("bloom_bytes", C.c_int64)]
+
+
+class StarSpec(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("dim_key", "dim_pred", "dim_attr", "pred_a", "pred_b", "fact_fk_a",
+                                         "fact_fk_b", "fact_price", "fact_discount", "group_by", "use_filters",
+                                         "mode")]
+
+
+class StarCounters(C.Structure):
+    _fields_ = [("fact_rows", C.c_int64), ("passed_filters", C.c_int64), ("joined_rows", C.c_int64),
+                ("dim_a_keys", C.c_int64), ("dim_b_keys", C.c_int64), ("filter_a_form", C.c_int32),
+                ("filter_b_form", C.c_int32), ("filter_a_bytes", C.c_int64), ("filter_b_bytes", C.c_int64)]
+
+
+class GenSpec(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("column", C.c_uint32), ("seed", C.c_uint64), ("lo", C.c_int64),
+                ("hi", C.c_int64), ("x0", C.c_double), ("x1", C.c_double), ("null_fraction", C.c_double),
+                ("row0", C.c_int64)]
+
+
+# ---- library ------------------------------------------------------------------------------
+_lib = None
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "krv_last_error": (C.c_char_p, []),
+    "krv_last_need_bytes": (C.c_int64, []),
+    "krv_version": (C.c_char_p, []),
+    "krv_runtime_create": (C.c_int32, [C.c_int32, C.c_int64, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "krv_runtime_destroy": (None, [C.c_void_p]),
+    "krv_runtime_synchronize": (C.c_int32, [C.c_void_p]),
+    "krv_runtime_used_bytes": (C.c_int64, [C.c_void_p]),
+    "krv_runtime_budget_bytes": (C.c_int64, [C.c_void_p]),
+    "krv_runtime_stream": (C.c_void_p, [C.c_void_p]),
+    "krv_runtime_launches": (C.c_int64, [C.c_void_p]),
+    "krv_join_spec_init": (None, [C.POINTER(JoinSpec)]),
+    "krv_join_create": (C.c_int32, [C.c_void_p, C.POINTER(JoinSpec), C.POINTER(C.c_void_p)]),
+    "krv_join_build_push": (C.c_int32, [C.c_void_p, C.POINTER(ArrowArray), C.POINTER(ArrowSchema)]),
+    "krv_join_build_push_device": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema)]),
+    "krv_join_build_finish": (C.c_int32, [C.c_void_p]),
+    "krv_join_probe": (C.c_int32, [C.c_void_p, C.POINTER(ArrowArray), C.POINTER(ArrowSchema),
+                                   C.POINTER(ArrowArray), C.POINTER(ArrowSchema)]),
+    "krv_join_probe_device": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema),
+                                          C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema)]),
+    "krv_join_finish": (C.c_int32, [C.c_void_p, C.POINTER(ArrowArray), C.POINTER(ArrowSchema)]),
+    "krv_join_finish_device": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema)]),
+    "krv_join_key_filter": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "krv_join_counters_get": (C.c_int32, [C.c_void_p, C.POINTER(JoinCounters)]),
+    "krv_join_destroy": (None, [C.c_void_p]),
+    "krv_agg_spec_init": (None, [C.POINTER(AggSpec)]),
+    "krv_agg_create": (C.c_int32, [C.c_void_p, C.POINTER(AggSpec), C.POINTER(C.c_void_p)]),
+    "krv_agg_push": (C.c_int32, [C.c_void_p, C.POINTER(ArrowArray), C.POINTER(ArrowSchema)]),
+    "krv_agg_push_device": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema)]),
+    "krv_agg_finish": (C.c_int32, [C.c_void_p]),
+    "krv_agg_next_output": (C.c_int32, [C.c_void_p, C.POINTER(ArrowArray), C.POINTER(ArrowSchema)]),
+    "krv_agg_next_output_device": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema)]),
+    "krv_agg_groups": (C.c_int64, [C.c_void_p]),
+    "krv_agg_destroy": (None, [C.c_void_p]),
+    "krv_key_filter_options_default": (None, [C.POINTER(KeyFilterOptions)]),
+    "krv_key_filter_build": (C.c_int32, [C.c_void_p, C.POINTER(KeyFilterOptions), C.POINTER(ArrowArray),
+                                         C.POINTER(ArrowSchema), C.c_int32, C.POINTER(C.c_void_p)]),
+    "krv_key_filter_build_device": (C.c_int32, [C.c_void_p, C.POINTER(KeyFilterOptions),
+                                                C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema), C.c_int32,
+                                                C.POINTER(C.c_void_p)]),
+    "krv_key_filter_evaluate": (C.c_int32, [C.c_void_p, C.POINTER(ArrowArray), C.POINTER(ArrowSchema), C.c_int32,
+                                            C.POINTER(ArrowArray), C.POINTER(ArrowSchema)]),
+    "krv_key_filter_evaluate_device": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema),
+                                                   C.c_int32, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema)]),
+    "krv_key_filter_info_get": (C.c_int32, [C.c_void_p, C.POINTER(KeyFilterInfo)]),
+    "krv_key_filter_bloom_bytes": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64]),
+    "krv_key_filter_destroy": (None, [C.c_void_p]),
+    "krv_star_spec_init": (None, [C.POINTER(StarSpec)]),
+    "krv_star_create": (C.c_int32, [C.c_void_p, C.POINTER(StarSpec), C.POINTER(C.c_void_p)]),
+    "krv_star_build": (C.c_int32, [C.c_void_p, C.POINTER(ArrowArray), C.POINTER(ArrowSchema),
+                                   C.POINTER(ArrowArray), C.POINTER(ArrowSchema)]),
+    "krv_star_build_device": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema),
+                                          C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema)]),
+    "krv_star_probe": (C.c_int32, [C.c_void_p, C.POINTER(ArrowArray), C.POINTER(ArrowSchema)]),
+    "krv_star_probe_device": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema)]),
+    "krv_star_result": (C.c_int32, [C.c_void_p, C.POINTER(ArrowArray), C.POINTER(ArrowSchema)]),
+    "krv_star_reset": (C.c_int32, [C.c_void_p]),
+    "krv_star_counters_get": (C.c_int32, [C.c_void_p, C.POINTER(StarCounters)]),
+    "krv_star_destroy": (None, [C.c_void_p]),
+    "krv_gen_fill": (C.c_int32, [C.c_void_p, C.POINTER(GenSpec), C.c_int64, C.c_void_p, C.c_void_p]),
+}
+
+
+def exported_names() -> List[str]:
+    return sorted(_SIGS)
+
+
+def lib():
+    """Loads libkrv_gpu.so (built by build.py). Fails loudly when missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run python krishiv-engine_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def build(jobs: int = 8) -> str:
+    """Compiles the CUDA library in-tree (nvcc, sm_100a)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_krv_build", os.path.join(HERE, "build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.build(jobs)
+
+
+def check(status: int) -> int:
+    """Raises KrvError for a negative status (with the library's error text)."""
+    if status >= 0:
+        return status
+    msg = lib().krv_last_error().decode("utf-8", "replace")
+    raise KrvError(status, msg)
+
+
+# ---- Arrow helpers ----------------------------------------------------------------------
+def _release_array(arr: ArrowArray):
+    if arr.release:
+        arr.release(C.byref(arr))
+
+
+def _release_schema(s: ArrowSchema):
+    if s.release:
+        s.release(C.byref(s))
+
+
+class HostBatch:
+    """A pyarrow RecordBatch exported through the C Data Interface for one
+    borrowed call; released when the call is done (a context manager)."""
+
+    def __init__(self, batch):
+        self.array = ArrowArray()
+        self.schema = ArrowSchema()
+        batch._export_to_c(C.addressof(self.array), C.addressof(self.schema))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        _release_array(self.array)
+        _release_schema(self.schema)
+
+
+def import_host(arr: ArrowArray, schema: ArrowSchema):
+    import pyarrow as pa
+    return pa.RecordBatch._import_from_c(C.addressof(arr), C.addressof(schema))
+
+
+_NOOP_ARRAY_RELEASE = C.CFUNCTYPE(None, C.POINTER(ArrowArray))(lambda p: None)
+
+_TORCH_FORMAT = {}
+
+
+def _format_of(t) -> str:
+    import torch
+    return {torch.int64: "l", torch.int32: "i", torch.float64: "g", torch.uint8: "C"}[t.dtype]
+
+
+class DeviceBatch:
+    """Device columns (torch CUDA tensors) as an ArrowDeviceArray, borrowed
+    by the library for the duration of one call.
+
+    `columns`: list of (name, tensor, valid_tensor_or_None, arrow_type_or_None).
+    A validity tensor is a uint8 bitmap (bit i = row i). The Arrow type
+    defaults from the tensor dtype; pass e.g. pa.decimal64(15, 2) for an
+    int64 tensor of unscaled decimals."""
+
+    def __init__(self, columns: Sequence, device: int = 0):
+        import pyarrow as pa
+        self._keep = []
+        n = int(columns[0][1].shape[0]) if columns else 0
+        fields = []
+        self.children = (C.POINTER(ArrowArray) * max(1, len(columns)))()
+        self._child_structs = []
+        for i, col in enumerate(columns):
+            name, t, valid = col[0], col[1], col[2] if len(col) > 2 else None
+            atype = col[3] if len(col) > 3 and col[3] is not None else None
+            if atype is None:
+                atype = {"l": pa.int64(), "i": pa.int32(), "g": pa.float64(), "C": pa.uint8()}[_format_of(t)]
+            fields.append(pa.field(name, atype, nullable=valid is not None))
+            bufs = (C.c_void_p * 2)(valid.data_ptr() if valid is not None else None, t.data_ptr())
+            a = ArrowArray(length=n, null_count=-1 if valid is not None else 0, offset=0, n_buffers=2,
+                           n_children=0, buffers=bufs, children=None, dictionary=None,
+                           release=_NOOP_ARRAY_RELEASE, private_data=None)
+            self._keep += [t, valid, bufs, a]
+            self._child_structs.append(a)
+            self.children[i] = C.pointer(a)
+        top_bufs = (C.c_void_p * 1)(None)
+        self._keep.append(top_bufs)
+        self.dev = ArrowDeviceArray()
+        self.dev.array = ArrowArray(length=n, null_count=0, offset=0, n_buffers=1, n_children=len(columns),
+                                    buffers=top_bufs, children=self.children, dictionary=None,
+                                    release=_NOOP_ARRAY_RELEASE, private_data=None)
+        self.dev.device_id = device
+        self.dev.device_type = ARROW_DEVICE_CUDA
+        self.dev.sync_event = None
+        self.pa_schema = pa.schema(fields)
+        self.schema = ArrowSchema()
+        self.pa_schema._export_to_c(C.addressof(self.schema))
+
+    def __del__(self):
+        try:
+            _release_schema(self.schema)
+        except Exception:
+            pass
+
+
+class _CudaArray:
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 3,
+                                         "strides": None}
+
+
+class DeviceResult:
+    """A library-owned ArrowDeviceArray moved to Python. Columns are exposed as
+    torch tensors that share its device memory; the memory is released when
+    this object goes away."""
+
+    _TYPESTR = {"l": "<i8", "i": "<i4", "g": "<f8", "C": "|u1", "tdD": "<i4"}
+
+    def __init__(self, dev: ArrowDeviceArray, schema: ArrowSchema):
+        import torch
+        self.dev = dev
+        self.schema = schema
+        self.rows = dev.array.length
+        self.names, self.formats, self.columns, self.valid = [], [], [], []
+        for i in range(dev.array.n_children):
+            cs = schema.children[i].contents
+            fmt = cs.format.decode()
+            self.names.append(cs.name.decode() if cs.name else "")
+            self.formats.append(fmt)
+            ch = dev.array.children[i].contents
+            data = ch.buffers[1]
+            vptr = ch.buffers[0]
+            if fmt.startswith("d:"):
+                width = 8 if fmt.endswith(",64") else 16
+                ts, n = "<i8", self.rows * (width // 8)
+            elif fmt == "b":
+                ts, n = "|u1", (self.rows + 7) // 8
+            else:
+                ts, n = self._TYPESTR[fmt], self.rows
+            self.columns.append(torch.as_tensor(_CudaArray(data, n, ts), device="cuda") if n and data else None)
+            self.valid.append(torch.as_tensor(_CudaArray(vptr, (self.rows + 7) // 8, "|u1"), device="cuda")
+                              if vptr and self.rows else None)
+
+    def __del__(self):
+        try:
+            _release_array(self.dev.array)
+            _release_schema(self.schema)
+        except Exception:
+            pass
+
+
+# ---- operators ------------------------------------------------------------------------------
+class Runtime:
+    """A device, a CUDA stream and an HBM budget (krv_runtime_create)."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0, stream: Optional[int] = None):
+        h = C.c_void_p()
+        check(lib().krv_runtime_create(device, budget_bytes, stream, C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def synchronize(self):
+        check(lib().krv_runtime_synchronize(self.h))
+
+    @property
+    def used_bytes(self) -> int:
+        return lib().krv_runtime_used_bytes(self.h)
+
+    @property
+    def launches(self) -> int:
+        return lib().krv_runtime_launches(self.h)
+
+    @property
+    def stream(self) -> int:
+        return lib().krv_runtime_stream(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().krv_runtime_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def join_spec(join_type="inner", probe_keys=(0,), build_keys=(0,), null_safe=None, single_match=False,
+              probe_out=None, build_out=None, runtime_filter=False, max_load=0.0, max_output_rows=0,
+              build_rows_hint=0) -> JoinSpec:
+    s = JoinSpec()
+    lib().krv_join_spec_init(C.byref(s))
+    s.join_type = JOIN_TYPES[join_type] if isinstance(join_type, str) else int(join_type)
+    s.n_keys = len(probe_keys)
+    for i, (p, b) in enumerate(zip(probe_keys, build_keys)):
+        s.probe_keys[i] = p
+        s.build_keys[i] = b
+        s.null_safe[i] = int(bool(null_safe[i])) if null_safe else 0
+    s.single_match = int(single_match)
+    if probe_out is not None:
+        s.n_probe_out = len(probe_out)
+        for i, c in enumerate(probe_out):
+            s.probe_out[i] = c
+    if build_out is not None:
+        s.n_build_out = len(build_out)
+        for i, c in enumerate(build_out):
+            s.build_out[i] = c
+    s.runtime_filter = int(runtime_filter)
+    s.max_load = max_load
+    s.max_output_rows = max_output_rows
+    s.build_rows_hint = build_rows_hint
+    return s
+
+
+class HashJoin:
+    """The hash join operator (HashJoin, crates/krishiv-exec/src/join/mod.rs:1014)."""
+
+    def __init__(self, rt: Runtime, spec: JoinSpec):
+        self.rt = rt
+        h = C.c_void_p()
+        check(lib().krv_join_create(rt.h, C.byref(spec), C.byref(h)))
+        self.h = h
+
+    def build_push(self, batch):
+        with HostBatch(batch) as hb:
+            check(lib().krv_join_build_push(self.h, C.byref(hb.array), C.byref(hb.schema)))
+
+    def build_push_device(self, db: DeviceBatch):
+        check(lib().krv_join_build_push_device(self.h, C.byref(db.dev), C.byref(db.schema)))
+
+    def build_finish(self):
+        check(lib().krv_join_build_finish(self.h))
+
+    def probe(self, batch) -> list:
+        """All output batches (pyarrow) of one probe batch."""
+        out = []
+        with HostBatch(batch) as hb:
+            arr, sch = ArrowArray(), ArrowSchema()
+            st = check(lib().krv_join_probe(self.h, C.byref(hb.array), C.byref(hb.schema), C.byref(arr),
+                                            C.byref(sch)))
+            out.append(import_host(arr, sch))
+        while st == HAVE_MORE_OUTPUT:
+            arr, sch = ArrowArray(), ArrowSchema()
+            st = check(lib().krv_join_probe(self.h, None, None, C.byref(arr), C.byref(sch)))
+            out.append(import_host(arr, sch))
+        return out
+
+    def probe_device(self, db: DeviceBatch) -> DeviceResult:
+        dev, sch = ArrowDeviceArray(), ArrowSchema()
+        check(lib().krv_join_probe_device(self.h, C.byref(db.dev), C.byref(db.schema), C.byref(dev), C.byref(sch)))
+        return DeviceResult(dev, sch)
+
+    def finish(self) -> list:
+        out = []
+        st = HAVE_MORE_OUTPUT
+        while st == HAVE_MORE_OUTPUT:
+            arr, sch = ArrowArray(), ArrowSchema()
+            st = check(lib().krv_join_finish(self.h, C.byref(arr), C.byref(sch)))
+            out.append(import_host(arr, sch))
+        return out
+
+    def key_filter(self) -> "KeyFilter":
+        h = C.c_void_p()
+        check(lib().krv_join_key_filter(self.h, C.byref(h)))
+        return KeyFilter(self.rt, h)
+
+    def counters(self) -> Dict[str, int]:
+        c = JoinCounters()
+        check(lib().krv_join_counters_get(self.h, C.byref(c)))
+        return {n: getattr(c, n) for n, _ in JoinCounters._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().krv_join_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def agg_spec(group_by: int, aggregates: Sequence, ansi=True, mode=MODE_AUTO, expected_groups=0,
+             max_output_rows=0) -> AggSpec:
+    s = AggSpec()
+    lib().krv_agg_spec_init(C.byref(s))
+    s.n_group_by = 1
+    s.group_by[0] = group_by
+    s.n_aggregates = len(aggregates)
+    for i, (f, c) in enumerate(aggregates):
+        s.aggregates[i].function = AGG_FUNCS[f] if isinstance(f, str) else int(f)
+        s.aggregates[i].column = c
+    s.ansi = int(ansi)
+    s.mode = mode
+    s.expected_groups = expected_groups
+    s.max_output_rows = max_output_rows
+    return s
+
+
+class HashAggregate:
+    """The grouped hash aggregate (HashAggregate, crates/krishiv-exec/src/aggregate/sink.rs:181)."""
+
+    def __init__(self, rt: Runtime, spec: AggSpec):
+        self.rt = rt
+        h = C.c_void_p()
+        check(lib().krv_agg_create(rt.h, C.byref(spec), C.byref(h)))
+        self.h = h
+
+    def push(self, batch):
+        with HostBatch(batch) as hb:
+            check(lib().krv_agg_push(self.h, C.byref(hb.array), C.byref(hb.schema)))
+
+    def push_device(self, db: DeviceBatch):
+        check(lib().krv_agg_push_device(self.h, C.byref(db.dev), C.byref(db.schema)))
+
+    def finish(self):
+        check(lib().krv_agg_finish(self.h))
+
+    def result(self) -> list:
+        out = []
+        st = HAVE_MORE_OUTPUT
+        while st == HAVE_MORE_OUTPUT:
+            arr, sch = ArrowArray(), ArrowSchema()
+            st = check(lib().krv_agg_next_output(self.h, C.byref(arr), C.byref(sch)))
+            out.append(import_host(arr, sch))
+        return out
+
+    def result_device(self) -> DeviceResult:
+        dev, sch = ArrowDeviceArray(), ArrowSchema()
+        check(lib().krv_agg_next_output_device(self.h, C.byref(dev), C.byref(sch)))
+        return DeviceResult(dev, sch)
+
+    @property
+    def groups(self) -> int:
+        return lib().krv_agg_groups(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().krv_agg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def key_filter_options(**kw) -> KeyFilterOptions:
+    o = KeyFilterOptions()
+    lib().krv_key_filter_options_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class KeyFilter:
+    """A runtime key filter (KeyFilter, crates/krishiv-io/src/runtime_filter/filter.rs:627)."""
+
+    def __init__(self, rt: Runtime, h):
+        self.rt = rt
+        self.h = h
+
+    @classmethod
+    def build(cls, rt: Runtime, batch, column: int, options: Optional[KeyFilterOptions] = None):
+        h = C.c_void_p()
+        with HostBatch(batch) as hb:
+            check(lib().krv_key_filter_build(rt.h, C.byref(options) if options else None, C.byref(hb.array),
+                                             C.byref(hb.schema), column, C.byref(h)))
+        return cls(rt, h)
+
+    @classmethod
+    def build_device(cls, rt: Runtime, db: DeviceBatch, column: int, options: Optional[KeyFilterOptions] = None):
+        h = C.c_void_p()
+        check(lib().krv_key_filter_build_device(rt.h, C.byref(options) if options else None, C.byref(db.dev),
+                                                C.byref(db.schema), column, C.byref(h)))
+        return cls(rt, h)
+
+    def evaluate(self, batch, column: int):
+        with HostBatch(batch) as hb:
+            arr, sch = ArrowArray(), ArrowSchema()
+            check(lib().krv_key_filter_evaluate(self.h, C.byref(hb.array), C.byref(hb.schema), column,
+                                                C.byref(arr), C.byref(sch)))
+            return import_host(arr, sch).column(0)
+
+    def evaluate_device(self, db: DeviceBatch, column: int) -> DeviceResult:
+        dev, sch = ArrowDeviceArray(), ArrowSchema()
+        check(lib().krv_key_filter_evaluate_device(self.h, C.byref(db.dev), C.byref(db.schema), column,
+                                                   C.byref(dev), C.byref(sch)))
+        return DeviceResult(dev, sch)
+
+    def info(self) -> Dict[str, int]:
+        i = KeyFilterInfo()
+        check(lib().krv_key_filter_info_get(self.h, C.byref(i)))
+        return {n: getattr(i, n) for n, _ in KeyFilterInfo._fields_ if n != "pad0"}
+
+    def bloom_bytes(self) -> bytes:
+        n = self.info()["bloom_bytes"]
+        buf = C.create_string_buffer(n)
+        check(lib().krv_key_filter_bloom_bytes(self.h, buf, n))
+        return buf.raw
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().krv_key_filter_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def star_spec(pred_a: int, pred_b: int, group_by: int = 0, use_filters: bool = True, mode: int = STAR_FUSED):
+    s = StarSpec()
+    lib().krv_star_spec_init(C.byref(s))
+    s.pred_a, s.pred_b, s.group_by, s.use_filters, s.mode = pred_a, pred_b, group_by, int(use_filters), mode
+    return s
+
+
+class StarPipeline:
+    """Star join with runtime filters and a grouped sum (krv_star_*)."""
+
+    def __init__(self, rt: Runtime, spec: StarSpec):
+        self.rt = rt
+        h = C.c_void_p()
+        check(lib().krv_star_create(rt.h, C.byref(spec), C.byref(h)))
+        self.h = h
+
+    def build(self, dim_a, dim_b):
+        with HostBatch(dim_a) as a, HostBatch(dim_b) as b:
+            check(lib().krv_star_build(self.h, C.byref(a.array), C.byref(a.schema), C.byref(b.array),
+                                       C.byref(b.schema)))
+
+    def build_device(self, a: DeviceBatch, b: DeviceBatch):
+        check(lib().krv_star_build_device(self.h, C.byref(a.dev), C.byref(a.schema), C.byref(b.dev),
+                                          C.byref(b.schema)))
+
+    def probe(self, fact):
+        with HostBatch(fact) as f:
+            check(lib().krv_star_probe(self.h, C.byref(f.array), C.byref(f.schema)))
+
+    def probe_device(self, f: DeviceBatch):
+        check(lib().krv_star_probe_device(self.h, C.byref(f.dev), C.byref(f.schema)))
+
+    def result(self):
+        arr, sch = ArrowArray(), ArrowSchema()
+        check(lib().krv_star_result(self.h, C.byref(arr), C.byref(sch)))
+        return import_host(arr, sch)
+
+    def reset(self):
+        check(lib().krv_star_reset(self.h))
+
+    def counters(self) -> Dict[str, int]:
+        c = StarCounters()
+        check(lib().krv_star_counters_get(self.h, C.byref(c)))
+        return {n: getattr(c, n) for n, _ in StarCounters._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().krv_star_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gen_fill(rt: Runtime, out, kind: int, seed: int, column: int, lo: int = 0, hi: int = 0, x0: float = 0.0,
+             x1: float = 0.0, null_fraction: float = 0.0, row0: int = 0, valid=None):
+    """Fills the CUDA tensor `out` (and bitmap `valid`) with a counter-based
+    synthetic column (krv_gen_fill)."""
+    s = GenSpec(kind=kind, column=column, seed=seed, lo=lo, hi=hi, x0=x0, x1=x1, null_fraction=null_fraction,
+                row0=row0)
+    check(lib().krv_gen_fill(rt.h, C.byref(s), int(out.shape[0]), out.data_ptr(),
+                             valid.data_ptr() if valid is not None else None))

@@ -1,0 +1,913 @@
+// aggregate.cu -- the grouped hash aggregate: COUNT(*), COUNT, SUM, MIN, MAX,
+// AVG over int32/int64/decimal/float64 columns, grouped by one int32 or int64
+// key, with Spark's result types, exact integer and decimal arithmetic and
+// ANSI overflow errors.
+//
+// Reference: crates/krishiv-exec/src/aggregate/ (HashAggregate, sink.rs:181;
+// result types, mod.rs:588-740; accumulators, accumulator.rs:212-590 and
+// accumulator/fold.rs; decimal AVG, accumulator/helpers.rs:539-610).
+//
+// Device layout. A global table maps each key to a dense group id: `keys`
+// (int64, empty = 0x8080...80) and `gids` (u32) of S = 2^k slots, probed
+// linearly from the key's hash; group g's accumulators are one record of
+// `rec` bytes at states + g * rec (rows, then per value column its non-NULL
+// count, sum, min and max as needed). Group 0 is the NULL key and group 1 the
+// key equal to the empty marker. In the shared-memory mode every CTA keeps a
+// small table of (key, group id, record) for the keys it sees first (under
+// Zipf keys, the heavy ones) and merges it into the global records at the end.
+//
+// Accumulation is exact and order-independent: counts and integer sums are
+// integer atomics, decimal and int64 sums are 128-bit (two 64-bit atomics
+// with carry), float64 sums are double-double (TwoSum-compensated atomics),
+// MIN/MAX of floats use an order-preserving integer map with NaN largest.
+#include <algorithm>
+#include <cmath>
+#include <string>
+
+#include "krv_device.cuh"
+#include "ops.h"
+
+namespace krv {
+
+namespace {
+
+constexpr long long kEmptyKey = (long long)0x8080808080808080ULL;
+constexpr uint32_t kPending = 0xFFFFFFFFu;
+constexpr uint32_t kOverflowGid = 0xFFFFFFFEu;
+constexpr uint32_t kNullGid = 0, kMarkerGid = 1, kFirstGid = 2;
+constexpr int kMaxValueCols = 8;
+
+enum : int32_t { F_SUM = 1, F_MIN = 2, F_MAX = 4 };
+
+struct AggColDev {
+    const void *data;
+    const uint8_t *valid;
+    int64_t voff;
+    int32_t type;  // Type
+    int32_t flags;
+    int32_t off_count, off_sum, off_min, off_max;
+};
+struct AggPlanDev {
+    AggColDev c[kMaxValueCols];
+    int32_t ncols;
+    int32_t rec;  // record bytes, a multiple of 16
+    int32_t off_rows;
+    int32_t pad;
+};
+struct KeyIn {
+    const void *data;
+    const uint8_t *valid;
+    int64_t voff;
+    int32_t width;  // 4 or 8
+    int32_t pad;
+};
+struct TableDev {
+    long long *keys;
+    uint32_t *gids;
+    uint64_t mask;
+    uint8_t *states;
+    long long *gkeys;
+    unsigned long long *ngroups;
+    unsigned long long limit;
+    uint32_t *status;
+};
+
+__device__ __forceinline__ long long key_at(const KeyIn &k, int64_t i) {
+    return k.width == 4 ? (long long)static_cast<const int32_t *>(k.data)[i]
+                        : static_cast<const long long *>(k.data)[i];
+}
+
+__device__ __forceinline__ void init_record(const AggPlanDev &P, uint8_t *r) {
+    for (int b = 0; b < P.rec; b += 8) *reinterpret_cast<unsigned long long *>(r + b) = 0ull;
+    for (int c = 0; c < P.ncols; c++) {
+        const AggColDev &C = P.c[c];
+        if (C.flags & F_MIN) {
+            if (C.type == (int)Type::I32 || C.type == (int)Type::Date32) *reinterpret_cast<int *>(r + C.off_min) = INT_MAX;
+            else if (C.type == (int)Type::F64) *reinterpret_cast<unsigned long long *>(r + C.off_min) = ~0ull;
+            else *reinterpret_cast<long long *>(r + C.off_min) = LLONG_MAX;
+        }
+        if (C.flags & F_MAX) {
+            if (C.type == (int)Type::I32 || C.type == (int)Type::Date32) *reinterpret_cast<int *>(r + C.off_max) = INT_MIN;
+            else if (C.type == (int)Type::F64) *reinterpret_cast<unsigned long long *>(r + C.off_max) = 0ull;
+            else *reinterpret_cast<long long *>(r + C.off_max) = LLONG_MIN;
+        }
+    }
+}
+
+// Accumulator::update for one row (accumulator/fold.rs): NULL inputs are
+// skipped; the row counts toward COUNT(*) regardless.
+__device__ __forceinline__ void update_record(const AggPlanDev &P, uint8_t *r, int64_t i) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(r + P.off_rows), 1ull);
+    for (int c = 0; c < P.ncols; c++) {
+        const AggColDev &C = P.c[c];
+        if (!bit_get(C.valid, C.voff, i)) continue;
+        atomicAdd(reinterpret_cast<unsigned long long *>(r + C.off_count), 1ull);
+        if (C.type == (int)Type::I32 || C.type == (int)Type::Date32) {
+            const int v = static_cast<const int *>(C.data)[i];
+            if (C.flags & F_SUM) atomicAdd(reinterpret_cast<unsigned long long *>(r + C.off_sum), (unsigned long long)(long long)v);
+            if (C.flags & F_MIN) atomicMin(reinterpret_cast<int *>(r + C.off_min), v);
+            if (C.flags & F_MAX) atomicMax(reinterpret_cast<int *>(r + C.off_max), v);
+        } else if (C.type == (int)Type::F64) {
+            const double v = static_cast<const double *>(C.data)[i];
+            if (C.flags & F_SUM)
+                atomic_add_dd(reinterpret_cast<double *>(r + C.off_sum), reinterpret_cast<double *>(r + C.off_sum + 8), v);
+            if (C.flags & (F_MIN | F_MAX)) {
+                const unsigned long long key = f64_order_key(v);
+                if (C.flags & F_MIN) atomicMin(reinterpret_cast<unsigned long long *>(r + C.off_min), key);
+                if (C.flags & F_MAX) atomicMax(reinterpret_cast<unsigned long long *>(r + C.off_max), key);
+            }
+        } else if (C.type == (int)Type::Dec128) {
+            const long long *p = static_cast<const long long *>(C.data) + 2 * i;
+            if (C.flags & F_SUM)
+                atomic_add_i128(reinterpret_cast<unsigned long long *>(r + C.off_sum),
+                                reinterpret_cast<long long *>(r + C.off_sum + 8), p[0], p[1]);
+        } else {  // I64, Dec64
+            const long long v = static_cast<const long long *>(C.data)[i];
+            if (C.flags & F_SUM)
+                atomic_add_i128_from_i64(reinterpret_cast<unsigned long long *>(r + C.off_sum),
+                                         reinterpret_cast<long long *>(r + C.off_sum + 8), v);
+            if (C.flags & F_MIN) atomicMin(reinterpret_cast<long long *>(r + C.off_min), v);
+            if (C.flags & F_MAX) atomicMax(reinterpret_cast<long long *>(r + C.off_max), v);
+        }
+    }
+}
+
+// Accumulator::merge (accumulator.rs:1159): folds the partial record `src`
+// into `dst`.
+__device__ __forceinline__ void merge_record(const AggPlanDev &P, uint8_t *dst, const uint8_t *src) {
+    const unsigned long long rows = *reinterpret_cast<const unsigned long long *>(src + P.off_rows);
+    if (!rows) return;
+    atomicAdd(reinterpret_cast<unsigned long long *>(dst + P.off_rows), rows);
+    for (int c = 0; c < P.ncols; c++) {
+        const AggColDev &C = P.c[c];
+        const unsigned long long cnt = *reinterpret_cast<const unsigned long long *>(src + C.off_count);
+        if (!cnt) continue;
+        atomicAdd(reinterpret_cast<unsigned long long *>(dst + C.off_count), cnt);
+        if (C.type == (int)Type::I32 || C.type == (int)Type::Date32) {
+            if (C.flags & F_SUM)
+                atomicAdd(reinterpret_cast<unsigned long long *>(dst + C.off_sum),
+                          *reinterpret_cast<const unsigned long long *>(src + C.off_sum));
+            if (C.flags & F_MIN) atomicMin(reinterpret_cast<int *>(dst + C.off_min), *reinterpret_cast<const int *>(src + C.off_min));
+            if (C.flags & F_MAX) atomicMax(reinterpret_cast<int *>(dst + C.off_max), *reinterpret_cast<const int *>(src + C.off_max));
+        } else if (C.type == (int)Type::F64) {
+            if (C.flags & F_SUM)
+                atomic_add_dd2(reinterpret_cast<double *>(dst + C.off_sum), reinterpret_cast<double *>(dst + C.off_sum + 8),
+                               *reinterpret_cast<const double *>(src + C.off_sum),
+                               *reinterpret_cast<const double *>(src + C.off_sum + 8));
+            if (C.flags & F_MIN)
+                atomicMin(reinterpret_cast<unsigned long long *>(dst + C.off_min),
+                          *reinterpret_cast<const unsigned long long *>(src + C.off_min));
+            if (C.flags & F_MAX)
+                atomicMax(reinterpret_cast<unsigned long long *>(dst + C.off_max),
+                          *reinterpret_cast<const unsigned long long *>(src + C.off_max));
+        } else {
+            if (C.flags & F_SUM)
+                atomic_add_i128(reinterpret_cast<unsigned long long *>(dst + C.off_sum),
+                                reinterpret_cast<long long *>(dst + C.off_sum + 8),
+                                *reinterpret_cast<const long long *>(src + C.off_sum),
+                                *reinterpret_cast<const long long *>(src + C.off_sum + 8));
+            if (C.type != (int)Type::Dec128) {
+                if (C.flags & F_MIN)
+                    atomicMin(reinterpret_cast<long long *>(dst + C.off_min), *reinterpret_cast<const long long *>(src + C.off_min));
+                if (C.flags & F_MAX)
+                    atomicMax(reinterpret_cast<long long *>(dst + C.off_max), *reinterpret_cast<const long long *>(src + C.off_max));
+            }
+        }
+    }
+}
+
+// A claimed slot's group id, published by its claimer right after the claim.
+// The wait is bounded: past the limit the kernel reports ST_TIMEOUT.
+__device__ __forceinline__ uint32_t wait_gid(const TableDev &T, uint64_t pos) {
+    for (int it = 0; it < (1 << 22); it++) {
+        const uint32_t g = *reinterpret_cast<volatile uint32_t *>(T.gids + pos);
+        if (g != kPending) {
+            __threadfence();
+            return g;
+        }
+        __nanosleep(20);
+    }
+    atomicOr(T.status, ST_TIMEOUT);
+    return kOverflowGid;
+}
+
+// The group of key k: found, or inserted with a fresh dense id. kOverflowGid
+// when the table is past its load limit (the row is deferred to a bigger
+// table).
+__device__ uint32_t find_or_insert(const TableDev &T, const AggPlanDev &P, long long k) {
+    uint64_t pos = hash_word((uint64_t)k) & T.mask;
+    for (uint64_t p = 0; p <= T.mask; p++) {
+        const long long cur = __ldcg(T.keys + pos);
+        if (cur == k) return wait_gid(T, pos);
+        if (cur == kEmptyKey) {
+            if (__ldcg(T.ngroups) >= T.limit) return kOverflowGid;
+            const long long old = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(T.keys + pos),
+                                                       (unsigned long long)kEmptyKey, (unsigned long long)k);
+            if (old == kEmptyKey) {
+                const uint32_t g = (uint32_t)atomicAdd(T.ngroups, 1ull);
+                init_record(P, T.states + (size_t)g * P.rec);
+                T.gkeys[g] = k;
+                __threadfence();
+                atomicExch(T.gids + pos, g);
+                return g;
+            }
+            if (old == k) return wait_gid(T, pos);
+        }
+        pos = (pos + 1) & T.mask;
+    }
+    return kOverflowGid;
+}
+
+__device__ __forceinline__ uint32_t group_of(const TableDev &T, const AggPlanDev &P, const KeyIn &key, int64_t r,
+                                             long long &k) {
+    if (!bit_get(key.valid, key.voff, r)) return kNullGid;
+    k = key_at(key, r);
+    if (k == kEmptyKey) return kMarkerGid;
+    return find_or_insert(T, P, k);
+}
+
+__device__ __forceinline__ void defer(uint32_t *ovf_rows, unsigned long long *ovf_count, int64_t r) {
+    const unsigned long long at = atomicAdd(ovf_count, 1ull);
+    ovf_rows[at] = (uint32_t)r;
+}
+
+// Global mode: every row goes to the global table.
+__global__ void __launch_bounds__(256) agg_global_kernel(AggPlanDev P, TableDev T, KeyIn key, int64_t n,
+                                                         const uint32_t *rows_idx, uint32_t *ovf_rows,
+                                                         unsigned long long *ovf_count) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int64_t r = rows_idx ? (int64_t)rows_idx[i] : i;
+        long long k = 0;
+        const uint32_t g = group_of(T, P, key, r, k);
+        if (g == kOverflowGid) {
+            defer(ovf_rows, ovf_count, r);
+            continue;
+        }
+        update_record(P, T.states + (size_t)g * P.rec, r);
+    }
+}
+
+// Shared-memory pre-aggregation: a CTA-private table of `E` (power of two)
+// entries filled up to `fill` keys; rows of other keys go to the global table.
+__global__ void __launch_bounds__(1024) agg_shared_kernel(AggPlanDev P, TableDev T, KeyIn key, int64_t n,
+                                                          const uint32_t *rows_idx, uint32_t *ovf_rows,
+                                                          unsigned long long *ovf_count, int E, int fill) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint8_t *srec = smem;                                              // E * rec
+    long long *skeys = reinterpret_cast<long long *>(smem + (size_t)E * P.rec);  // E
+    uint32_t *sgid = reinterpret_cast<uint32_t *>(skeys + E);         // E
+    int *sfill = reinterpret_cast<int *>(sgid + E);
+    for (int e = threadIdx.x; e < E; e += blockDim.x) {
+        skeys[e] = kEmptyKey;
+        init_record(P, srec + (size_t)e * P.rec);
+    }
+    if (threadIdx.x == 0) *sfill = 0;
+    __syncthreads();
+    const int emask = E - 1;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int64_t r = rows_idx ? (int64_t)rows_idx[i] : i;
+        if (!bit_get(key.valid, key.voff, r)) {
+            update_record(P, T.states + (size_t)kNullGid * P.rec, r);
+            continue;
+        }
+        const long long k = key_at(key, r);
+        if (k == kEmptyKey) {
+            update_record(P, T.states + (size_t)kMarkerGid * P.rec, r);
+            continue;
+        }
+        int slot = -1;
+        uint32_t g = kPending;
+        int pos = (int)(hash_word((uint64_t)k) & (uint64_t)emask);
+        for (int p = 0; p < 16; p++) {
+            const long long cur = *reinterpret_cast<volatile long long *>(skeys + pos);
+            if (cur == k) {
+                slot = pos;
+                break;
+            }
+            if (cur == kEmptyKey) {
+                if (*reinterpret_cast<volatile int *>(sfill) >= fill) break;
+                if (g == kPending) {
+                    g = find_or_insert(T, P, k);
+                    if (g == kOverflowGid) break;
+                }
+                const long long old = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(skeys + pos),
+                                                           (unsigned long long)kEmptyKey, (unsigned long long)k);
+                if (old == kEmptyKey) {
+                    sgid[pos] = g;
+                    atomicAdd(sfill, 1);
+                    slot = pos;
+                    break;
+                }
+                if (old == k) {
+                    slot = pos;
+                    break;
+                }
+            }
+            pos = (pos + 1) & emask;
+        }
+        if (slot >= 0) {
+            update_record(P, srec + (size_t)slot * P.rec, r);
+            continue;
+        }
+        if (g == kPending) g = find_or_insert(T, P, k);
+        if (g == kOverflowGid) {
+            defer(ovf_rows, ovf_count, r);
+            continue;
+        }
+        update_record(P, T.states + (size_t)g * P.rec, r);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < E; e += blockDim.x)
+        if (skeys[e] != kEmptyKey) merge_record(P, T.states + (size_t)sgid[e] * P.rec, srec + (size_t)e * P.rec);
+}
+
+__global__ void init_special_kernel(AggPlanDev P, uint8_t *states) {
+    if (threadIdx.x < 2) init_record(P, states + (size_t)threadIdx.x * P.rec);
+}
+
+// Re-inserts the (key, group id) pairs of an old table into a bigger one.
+__global__ void rehash_kernel(const long long *okeys, const uint32_t *ogids, uint64_t on, long long *nkeys,
+                              uint32_t *ngids, uint64_t nmask) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < on; i += (uint64_t)gridDim.x * blockDim.x) {
+        const long long k = okeys[i];
+        if (k == kEmptyKey) continue;
+        uint64_t pos = hash_word((uint64_t)k) & nmask;
+        for (uint64_t p = 0; p <= nmask; p++) {
+            const unsigned long long old =
+                atomicCAS(reinterpret_cast<unsigned long long *>(nkeys + pos), (unsigned long long)kEmptyKey,
+                          (unsigned long long)k);
+            if (old == (unsigned long long)kEmptyKey) {
+                ngids[pos] = ogids[i];
+                break;
+            }
+            pos = (pos + 1) & nmask;
+        }
+    }
+}
+
+// ---- results -------------------------------------------------------------------
+struct OutExprDev {
+    int32_t func;
+    int32_t col;      // value column index in the plan (-1: COUNT(*))
+    int32_t otype;    // result Type
+    int32_t rp, rs;   // result precision/scale (decimals)
+    int32_t in_type;
+    int32_t in_scale;
+    int32_t ansi;
+    void *dst;
+    uint32_t *dst_valid;
+};
+constexpr int kMaxExprs = KRV_MAX_AGGREGATES;
+struct OutPlanDev {
+    OutExprDev e[kMaxExprs];
+    int32_t n;
+    int32_t nspecial;
+    uint32_t special[2];
+};
+
+__device__ __forceinline__ unsigned __int128 pow10_u128(int p) {
+    unsigned __int128 v = 1;
+    for (int i = 0; i < p && i < 38; i++) v *= 10;
+    return v;
+}
+
+// avg_decimal (helpers.rs:539-590): HALF_UP to scale 39, then HALF_UP to s.
+__device__ bool avg_decimal_slow(__int128 sum, int ss, long long count, int p, int s, __int128 &out) {
+    const bool negative = (sum < 0) != (count < 0);
+    const unsigned __int128 a = sum < 0 ? (unsigned __int128)(-sum) : (unsigned __int128)sum;
+    const unsigned __int128 b = (unsigned __int128)(count < 0 ? -(__int128)count : (__int128)count);
+    unsigned __int128 in = a / b, rem = a % b;
+    const int nfrac = 39 - ss;
+    uint8_t frac[40];
+    for (int i = 0; i < nfrac; i++) {
+        rem *= 10;
+        frac[i] = (uint8_t)(rem / b);
+        rem %= b;
+    }
+    rem *= 10;
+    if ((uint8_t)(rem / b) >= 5) {
+        int i = nfrac - 1;
+        bool carry = true;
+        while (i >= 0 && carry) {
+            if (frac[i] == 9) frac[i] = 0;
+            else {
+                frac[i]++;
+                carry = false;
+            }
+            i--;
+        }
+        if (carry) in += 1;
+    }
+    int keep = s - ss;
+    if (keep < 0) keep = 0;
+    const bool up = keep < nfrac && frac[keep] >= 5;
+    unsigned __int128 v = in;
+    const unsigned __int128 lim = ((unsigned __int128)1) << 126;
+    for (int i = 0; i < keep; i++) {
+        if (v > lim / 10) return false;
+        v = v * 10 + frac[i];
+    }
+    v += up ? 1 : 0;
+    if (v >= pow10_u128(p)) return false;
+    out = negative ? -(__int128)v : (__int128)v;
+    return true;
+}
+
+// avg_fast (helpers.rs:595-610): one HALF_UP division when the result scale is
+// at most 19 and not below the sum's; else the digit loop.
+__device__ bool avg_decimal(__int128 sum, int ss, long long count, int p, int s, __int128 &out) {
+    if (count == 0) return false;
+    if (s <= 19 && s >= ss) {
+        const unsigned __int128 mag = sum < 0 ? (unsigned __int128)(-sum) : (unsigned __int128)sum;
+        const unsigned __int128 mul = pow10_u128(s - ss);
+        if (mag <= (~(unsigned __int128)0) / mul) {
+            const unsigned __int128 nn = mag * mul;
+            const unsigned __int128 d = (unsigned __int128)(count < 0 ? -(__int128)count : (__int128)count);
+            unsigned __int128 q = nn / d;
+            const unsigned __int128 r = nn % d;
+            q += (r >= d - r) ? 1 : 0;
+            if (q >= pow10_u128(p)) return false;
+            out = ((sum < 0) != (count < 0)) ? -(__int128)q : (__int128)q;
+            return true;
+        }
+    }
+    return avg_decimal_slow(sum, ss, count, p, s, out);
+}
+
+__global__ void __launch_bounds__(256) finalize_kernel(AggPlanDev P, OutPlanDev O, const uint8_t *states,
+                                                       const long long *gkeys, int64_t nout, int key_width,
+                                                       void *key_out, uint32_t *key_valid, uint32_t *status) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nout; base += stride) {
+        const int64_t r = base + threadIdx.x;
+        const bool live = r < nout;
+        uint32_t g = 0;
+        if (live) g = r < O.nspecial ? O.special[r] : (uint32_t)(r - O.nspecial + kFirstGid);
+        const uint8_t *rec = states + (size_t)g * P.rec;
+        // Group key.
+        bool kv = live && g != kNullGid;
+        if (live) {
+            const long long k = g == kNullGid ? 0 : g == kMarkerGid ? kEmptyKey : gkeys[g];
+            if (key_width == 4) static_cast<int *>(key_out)[r] = (int)k;
+            else static_cast<long long *>(key_out)[r] = k;
+        }
+        if (key_valid) {
+            const unsigned w = __ballot_sync(0xFFFFFFFFu, kv);
+            if ((threadIdx.x & 31) == 0 && live) key_valid[r >> 5] = w;
+        }
+        for (int e = 0; e < O.n; e++) {
+            const OutExprDev &X = O.e[e];
+            bool valid = false;
+            if (live) {
+                const unsigned long long rows = *reinterpret_cast<const unsigned long long *>(rec + P.off_rows);
+                if (X.func == KRV_AGG_COUNT_STAR) {
+                    static_cast<long long *>(X.dst)[r] = (long long)rows;
+                    valid = true;
+                } else {
+                    const AggColDev &C = P.c[X.col];
+                    const unsigned long long cnt = *reinterpret_cast<const unsigned long long *>(rec + C.off_count);
+                    if (X.func == KRV_AGG_COUNT) {
+                        static_cast<long long *>(X.dst)[r] = (long long)cnt;
+                        valid = true;
+                    } else if (cnt > 0) {
+                        const bool i32 = C.type == (int)Type::I32 || C.type == (int)Type::Date32;
+                        if (X.func == KRV_AGG_MIN || X.func == KRV_AGG_MAX) {
+                            const int off = X.func == KRV_AGG_MIN ? C.off_min : C.off_max;
+                            if (i32) static_cast<int *>(X.dst)[r] = *reinterpret_cast<const int *>(rec + off);
+                            else if (C.type == (int)Type::F64)
+                                static_cast<double *>(X.dst)[r] =
+                                    f64_from_order_key(*reinterpret_cast<const unsigned long long *>(rec + off));
+                            else static_cast<long long *>(X.dst)[r] = *reinterpret_cast<const long long *>(rec + off);
+                            valid = true;
+                        } else if (C.type == (int)Type::F64) {
+                            const double hi = *reinterpret_cast<const double *>(rec + C.off_sum);
+                            const double lo = *reinterpret_cast<const double *>(rec + C.off_sum + 8);
+                            double s = isfinite(hi) ? __dadd_rn(hi, lo) : hi;
+                            if (X.func == KRV_AGG_AVG) s = __ddiv_rn(s, (double)cnt);
+                            static_cast<double *>(X.dst)[r] = s;
+                            valid = true;
+                        } else if (i32) {
+                            const long long s = *reinterpret_cast<const long long *>(rec + C.off_sum);
+                            if (X.func == KRV_AGG_SUM) static_cast<long long *>(X.dst)[r] = s;
+                            else static_cast<double *>(X.dst)[r] = __ddiv_rn((double)s, (double)cnt);
+                            valid = true;
+                        } else {
+                            const unsigned long long lo = *reinterpret_cast<const unsigned long long *>(rec + C.off_sum);
+                            const long long hi = *reinterpret_cast<const long long *>(rec + C.off_sum + 8);
+                            const __int128 sum = (__int128)(((unsigned __int128)(unsigned long long)hi << 64) | lo);
+                            const bool fits64 = (hi == 0 && !(lo >> 63)) || (hi == -1 && (lo >> 63));
+                            if (C.type == (int)Type::I64) {
+                                if (X.func == KRV_AGG_SUM) {
+                                    // SumInt: ANSI raises on overflow, else wraps (two's complement).
+                                    if (!fits64 && X.ansi) atomicOr(status, ST_OVERFLOW);
+                                    static_cast<long long *>(X.dst)[r] = (long long)lo;
+                                    valid = true;
+                                } else {
+                                    const double s = fits64 ? (double)(long long)lo
+                                                            : (double)hi * 18446744073709551616.0 + (double)lo;
+                                    static_cast<double *>(X.dst)[r] = __ddiv_rn(s, (double)cnt);
+                                    valid = true;
+                                }
+                            } else {
+                                __int128 v = sum;
+                                bool ok = true;
+                                if (X.func == KRV_AGG_SUM) {
+                                    const unsigned __int128 mag = sum < 0 ? (unsigned __int128)(-sum) : (unsigned __int128)sum;
+                                    ok = mag < pow10_u128(X.rp);
+                                } else {
+                                    ok = avg_decimal(sum, X.in_scale, (long long)cnt, X.rp, X.rs, v);
+                                }
+                                if (!ok) {
+                                    if (X.ansi) atomicOr(status, ST_OVERFLOW);
+                                } else {
+                                    if (X.otype == (int)Type::Dec64) static_cast<long long *>(X.dst)[r] = (long long)v;
+                                    else {
+                                        long long *d = static_cast<long long *>(X.dst) + 2 * r;
+                                        d[0] = (long long)(unsigned long long)v;
+                                        d[1] = (long long)(v >> 64);
+                                    }
+                                    valid = true;
+                                }
+                                if (!ok) {
+                                    if (X.otype == (int)Type::Dec64) static_cast<long long *>(X.dst)[r] = 0;
+                                    else {
+                                        long long *d = static_cast<long long *>(X.dst) + 2 * r;
+                                        d[0] = 0;
+                                        d[1] = 0;
+                                    }
+                                }
+                            }
+                        }
+                    } else {
+                        // No non-NULL input: NULL result with a zeroed value.
+                        const int w = X.otype == (int)Type::Dec128 ? 16
+                                      : (X.otype == (int)Type::I32 || X.otype == (int)Type::Date32) ? 4
+                                                                                                     : 8;
+                        if (w == 4) static_cast<int *>(X.dst)[r] = 0;
+                        else if (w == 8) static_cast<long long *>(X.dst)[r] = 0;
+                        else {
+                            static_cast<long long *>(X.dst)[2 * r] = 0;
+                            static_cast<long long *>(X.dst)[2 * r + 1] = 0;
+                        }
+                    }
+                }
+            }
+            if (X.dst_valid) {
+                const unsigned w = __ballot_sync(0xFFFFFFFFu, valid);
+                if ((threadIdx.x & 31) == 0 && live) X.dst_valid[r >> 5] = w;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+class HashAggregate {
+  public:
+    HashAggregate(Runtime *rt, const krv_agg_spec &spec);
+    void push(const DevBatch &b);
+    void finish() { finished_ = true; }
+    DevBatch result();
+    int64_t groups() const { return known_groups_; }
+
+  private:
+    void plan(const DevBatch &b);
+    void alloc_table(uint64_t slots);
+    void grow(uint64_t need_groups);
+    void launch(const DevBatch &b, const KeyIn &key, int64_t n, const uint32_t *rows_idx, uint32_t *ovf,
+                unsigned long long *ovf_count);
+
+    Runtime *rt_;
+    krv_agg_spec spec_;
+    bool planned_ = false, finished_ = false;
+    AggPlanDev P_{};
+    std::vector<int> value_cols_;  // input column of each plan column
+    std::vector<DType> input_types_;
+    std::vector<std::string> input_names_;
+    DType key_type_;
+    std::string key_name_;
+    DBuf keys_, gids_, states_, gkeys_, ngroups_;
+    uint64_t slots_ = 0;
+    unsigned long long limit_ = 0;
+    int64_t known_groups_ = 2;     // exact after a sync
+    int64_t pending_rows_ = 0;     // rows pushed since known_groups_ was read
+    int mode_ = KRV_AGG_MODE_SHARED;
+    int smem_entries_ = 0;
+};
+
+HashAggregate::HashAggregate(Runtime *rt, const krv_agg_spec &spec) : rt_(rt), spec_(spec) {
+    if (spec.n_group_by != 1) fail(KRV_UNSUPPORTED, "the GPU aggregate groups by exactly one key column");
+    if (spec.n_aggregates < 0 || spec.n_aggregates > KRV_MAX_AGGREGATES)
+        fail(KRV_INVALID_ARGUMENT, "aggregate count out of range");
+    for (int e = 0; e < spec.n_aggregates; e++)
+        if (spec.aggregates[e].function < KRV_AGG_COUNT_STAR || spec.aggregates[e].function > KRV_AGG_AVG)
+            fail(KRV_UNSUPPORTED, "aggregate function " + std::to_string(spec.aggregates[e].function));
+    mode_ = spec.mode == KRV_AGG_MODE_GLOBAL ? KRV_AGG_MODE_GLOBAL : KRV_AGG_MODE_SHARED;
+}
+
+void HashAggregate::plan(const DevBatch &b) {
+    const int kc = spec_.group_by[0];
+    if (kc < 0 || kc >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "group-by column out of range");
+    key_type_ = b.cols[kc].type;
+    key_name_ = b.cols[kc].name;
+    if (key_type_.id != Type::I32 && key_type_.id != Type::I64 && key_type_.id != Type::Date32 &&
+        key_type_.id != Type::Dec64)
+        fail(KRV_UNSUPPORTED, "group key of type " + key_type_.format());
+    for (const DevCol &c : b.cols) {
+        input_types_.push_back(c.type);
+        input_names_.push_back(c.name);
+    }
+    // One plan column per distinct input column; flags from its aggregates.
+    P_.ncols = 0;
+    std::vector<int32_t> flags;
+    for (int e = 0; e < spec_.n_aggregates; e++) {
+        const krv_agg_expr &x = spec_.aggregates[e];
+        if (x.function == KRV_AGG_COUNT_STAR) continue;
+        if (x.column < 0 || x.column >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "aggregate column out of range");
+        const DType t = b.cols[x.column].type;
+        if (t.id == Type::Bool || t.id == Type::U8) fail(KRV_UNSUPPORTED, "aggregate over " + t.format());
+        if (t.id == Type::Dec128 && (x.function == KRV_AGG_MIN || x.function == KRV_AGG_MAX))
+            fail(KRV_UNSUPPORTED, "MIN/MAX of decimal128 on the GPU aggregate");
+        int at = -1;
+        for (size_t i = 0; i < value_cols_.size(); i++)
+            if (value_cols_[i] == x.column) at = (int)i;
+        if (at < 0) {
+            if ((int)value_cols_.size() == kMaxValueCols) fail(KRV_UNSUPPORTED, "more than 8 aggregated columns");
+            value_cols_.push_back(x.column);
+            flags.push_back(0);
+            at = (int)value_cols_.size() - 1;
+        }
+        if (x.function == KRV_AGG_SUM || x.function == KRV_AGG_AVG) flags[at] |= F_SUM;
+        if (x.function == KRV_AGG_MIN) flags[at] |= F_MIN;
+        if (x.function == KRV_AGG_MAX) flags[at] |= F_MAX;
+    }
+    // Record layout: 16-byte sums first, then 8-byte fields, then 4-byte ones.
+    int off = 0;
+    P_.ncols = (int)value_cols_.size();
+    for (int c = 0; c < P_.ncols; c++) {
+        const DType t = b.cols[value_cols_[c]].type;
+        AggColDev &C = P_.c[c];
+        C.type = (int)t.id;
+        C.flags = flags[c];
+        C.off_count = C.off_sum = C.off_min = C.off_max = -1;
+        const bool wide = t.id == Type::I64 || t.id == Type::Dec64 || t.id == Type::Dec128 || t.id == Type::F64;
+        if ((C.flags & F_SUM) && wide) {
+            C.off_sum = off;
+            off += 16;
+        }
+    }
+    P_.off_rows = off;
+    off += 8;
+    for (int c = 0; c < P_.ncols; c++) {
+        AggColDev &C = P_.c[c];
+        const bool i32 = C.type == (int)Type::I32 || C.type == (int)Type::Date32;
+        C.off_count = off;
+        off += 8;
+        if ((C.flags & F_SUM) && i32) {
+            C.off_sum = off;
+            off += 8;
+        }
+        if (!i32) {
+            if (C.flags & F_MIN) {
+                C.off_min = off;
+                off += 8;
+            }
+            if (C.flags & F_MAX) {
+                C.off_max = off;
+                off += 8;
+            }
+        }
+    }
+    for (int c = 0; c < P_.ncols; c++) {
+        AggColDev &C = P_.c[c];
+        const bool i32 = C.type == (int)Type::I32 || C.type == (int)Type::Date32;
+        if (i32) {
+            if (C.flags & F_MIN) {
+                C.off_min = off;
+                off += 4;
+            }
+            if (C.flags & F_MAX) {
+                C.off_max = off;
+                off += 4;
+            }
+        }
+    }
+    P_.rec = (off + 15) & ~15;
+    // Shared-memory entries: the largest power of two whose records, keys
+    // and ids fit the opt-in shared memory of one CTA.
+    const int per = P_.rec + 12;
+    int e = 1;
+    while ((e * 2) * per + 64 <= std::min(rt_->max_smem_optin, 200 * 1024)) e *= 2;
+    smem_entries_ = e >= 64 ? e : 0;
+    if (smem_entries_ == 0) mode_ = KRV_AGG_MODE_GLOBAL;
+    const uint64_t hint = spec_.expected_groups > 0 ? (uint64_t)spec_.expected_groups : 65536;
+    alloc_table(std::max<uint64_t>(1024, next_pow2((uint64_t)(hint * 2))));
+    planned_ = true;
+}
+
+void HashAggregate::alloc_table(uint64_t slots) {
+    slots_ = slots;
+    limit_ = (unsigned long long)(slots * 3 / 4);
+    keys_ = DBuf(rt_, slots * 8);
+    gids_ = DBuf(rt_, slots * 4);
+    KRV_CUDA(cudaMemsetAsync(keys_.get(), 0x80, slots * 8, rt_->stream));
+    KRV_CUDA(cudaMemsetAsync(gids_.get(), 0xFF, slots * 4, rt_->stream));
+    const size_t gcap = slots + kFirstGid;
+    DBuf states(rt_, gcap * (size_t)P_.rec);
+    DBuf gkeys(rt_, gcap * 8);
+    if (states_.get()) {
+        KRV_CUDA(cudaMemcpyAsync(states.get(), states_.get(), (size_t)known_groups_ * P_.rec, cudaMemcpyDeviceToDevice,
+                                 rt_->stream));
+        KRV_CUDA(cudaMemcpyAsync(gkeys.get(), gkeys_.get(), (size_t)known_groups_ * 8, cudaMemcpyDeviceToDevice,
+                                 rt_->stream));
+    } else {
+        init_special_kernel<<<1, 32, 0, rt_->stream>>>(P_, states.as<uint8_t>());
+        rt_->launches++;
+        check_launch("init_special_kernel");
+        ngroups_ = DBuf(rt_, 8);
+        const unsigned long long first = kFirstGid;
+        KRV_CUDA(cudaMemcpyAsync(ngroups_.get(), &first, 8, cudaMemcpyHostToDevice, rt_->stream));
+        KRV_CUDA(cudaStreamSynchronize(rt_->stream));
+    }
+    states_ = std::move(states);
+    gkeys_ = std::move(gkeys);
+}
+
+void HashAggregate::grow(uint64_t need_groups) {
+    DBuf okeys = std::move(keys_), ogids = std::move(gids_);
+    const uint64_t oslots = slots_;
+    uint64_t ns = next_pow2(std::max<uint64_t>(oslots * 2, need_groups * 2));
+    alloc_table(ns);
+    rehash_kernel<<<grid_for(rt_, (int64_t)oslots, 256, 8), 256, 0, rt_->stream>>>(
+        okeys.as<long long>(), ogids.as<uint32_t>(), oslots, keys_.as<long long>(), gids_.as<uint32_t>(), slots_ - 1);
+    rt_->launches++;
+    check_launch("rehash_kernel");
+}
+
+void HashAggregate::launch(const DevBatch &b, const KeyIn &key, int64_t n, const uint32_t *rows_idx, uint32_t *ovf,
+                           unsigned long long *ovf_count) {
+    AggPlanDev P = P_;
+    for (int c = 0; c < P.ncols; c++) {
+        const DevCol &col = b.cols[value_cols_[c]];
+        P.c[c].data = col.data;
+        P.c[c].valid = col.valid;
+        P.c[c].voff = col.valid_off;
+    }
+    TableDev T{keys_.as<long long>(), gids_.as<uint32_t>(), slots_ - 1, states_.as<uint8_t>(), gkeys_.as<long long>(),
+               ngroups_.as<unsigned long long>(), limit_, status_word(rt_)};
+    if (mode_ == KRV_AGG_MODE_SHARED) {
+        const int E = smem_entries_;
+        const size_t smem = (size_t)E * (P.rec + 12) + 16;
+        KRV_CUDA(cudaFuncSetAttribute(agg_shared_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int grid = (int)std::min<int64_t>(rt_->sm_count, ceil_div(std::max<int64_t>(n, 1), 1024));
+        agg_shared_kernel<<<grid, 1024, smem, rt_->stream>>>(P, T, key, n, rows_idx, ovf, ovf_count, E, E * 5 / 8);
+    } else {
+        agg_global_kernel<<<grid_for(rt_, n, 256, 8), 256, 0, rt_->stream>>>(P, T, key, n, rows_idx, ovf, ovf_count);
+    }
+    rt_->launches++;
+    check_launch("aggregate kernel");
+}
+
+void HashAggregate::push(const DevBatch &b) {
+    if (finished_) fail(KRV_INVALID_ARGUMENT, "push after finish");
+    DeviceGuard g(rt_);
+    if (!planned_) plan(b);
+    if (b.cols.size() != input_types_.size()) fail(KRV_INVALID_ARGUMENT, "batches differ in columns");
+    for (size_t i = 0; i < b.cols.size(); i++)
+        if (b.cols[i].type != input_types_[i]) fail(KRV_INVALID_ARGUMENT, "batches differ in types");
+    const int64_t n = b.rows;
+    if (n == 0) return;
+    if (n >= (int64_t)0xFFFFFFF0ll) fail(KRV_UNSUPPORTED, "aggregate batches of 2^32 rows or more");
+    const DevCol &kc = b.cols[spec_.group_by[0]];
+    KeyIn key{kc.data, kc.valid, kc.valid_off, kc.type.width(), 0};
+    clear_status(rt_);
+    DBuf ovf_count(rt_, 8);
+    KRV_CUDA(cudaMemsetAsync(ovf_count.get(), 0, 8, rt_->stream));
+    DBuf ovf(rt_, (size_t)n * 4);
+    launch(b, key, n, nullptr, ovf.as<uint32_t>(), ovf_count.as<unsigned long long>());
+    pending_rows_ += n;
+    // No row can have been deferred while the table had room for every row
+    // pushed since the last count: skip the synchronization then.
+    const bool may_defer = known_groups_ + pending_rows_ > (int64_t)limit_;
+    if (!may_defer) {
+        const uint32_t st = take_status(rt_);
+        if (st & ST_TIMEOUT) fail(KRV_TIMEOUT, "aggregate: a wait for a group id gave up");
+        return;
+    }
+    DBuf idx;
+    for (int round = 0; round < 16; round++) {
+        const unsigned long long deferred = read_scalar<unsigned long long>(rt_, ovf_count.get());
+        known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());
+        pending_rows_ = 0;
+        const uint32_t st = take_status(rt_);
+        if (st & ST_TIMEOUT) fail(KRV_TIMEOUT, "aggregate: a wait for a group id gave up");
+        if (deferred == 0) return;
+        grow((uint64_t)known_groups_ + deferred);
+        idx = DBuf(rt_, (size_t)deferred * 4);
+        KRV_CUDA(cudaMemcpyAsync(idx.get(), ovf.get(), (size_t)deferred * 4, cudaMemcpyDeviceToDevice, rt_->stream));
+        KRV_CUDA(cudaMemsetAsync(ovf_count.get(), 0, 8, rt_->stream));
+        launch(b, key, (int64_t)deferred, idx.as<uint32_t>(), ovf.as<uint32_t>(), ovf_count.as<unsigned long long>());
+        pending_rows_ = (int64_t)deferred;
+    }
+    fail(KRV_INTERNAL, "aggregate: table growth did not converge");
+}
+
+DevBatch HashAggregate::result() {
+    DeviceGuard g(rt_);
+    DevBatch out;
+    if (!planned_) return out;
+    known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());
+    pending_rows_ = 0;
+    // Which of the two special groups (NULL key, marker key) have rows.
+    unsigned long long special_rows[2];
+    for (int s = 0; s < 2; s++)
+        special_rows[s] = read_scalar<unsigned long long>(rt_, states_.as<uint8_t>() + (size_t)s * P_.rec + P_.off_rows);
+    OutPlanDev O{};
+    O.nspecial = 0;
+    for (uint32_t s = 0; s < 2; s++)
+        if (special_rows[s]) O.special[O.nspecial++] = s;
+    const int64_t nout = O.nspecial + (known_groups_ - kFirstGid);
+    const bool key_nullable = special_rows[0] != 0;
+    DevCol kcol = make_col(rt_, key_type_, nout, key_nullable, key_name_);
+    out.cols.push_back(kcol);
+    O.n = spec_.n_aggregates;
+    for (int e = 0; e < spec_.n_aggregates; e++) {
+        const krv_agg_expr &x = spec_.aggregates[e];
+        OutExprDev &X = O.e[e];
+        X.func = x.function;
+        X.ansi = spec_.ansi;
+        X.col = -1;
+        DType ot{Type::I64, 0, 0};
+        std::string name;
+        static const char *fname[] = {"count(1)", "count", "sum", "min", "max", "avg"};
+        if (x.function == KRV_AGG_COUNT_STAR) {
+            name = "count(1)";
+        } else {
+            for (size_t i = 0; i < value_cols_.size(); i++)
+                if (value_cols_[i] == x.column) X.col = (int)i;
+            const DType it = input_types_[x.column];
+            X.in_type = (int)it.id;
+            X.in_scale = it.scale;
+            name = std::string(fname[x.function]) + "(" + input_names_[x.column] + ")";
+            const bool dec = it.id == Type::Dec64 || it.id == Type::Dec128;
+            switch (x.function) {
+            case KRV_AGG_COUNT: ot = DType{Type::I64, 0, 0}; break;
+            case KRV_AGG_MIN:
+            case KRV_AGG_MAX: ot = it; break;
+            case KRV_AGG_SUM:
+                if (dec) {
+                    // sum_decimal (aggregate/mod.rs:929-931) on decimal_on's carrier (:1018-1024)
+                    const int p = std::min(38, it.precision + 10);
+                    ot = DType{(it.id == Type::Dec64 && p <= 18) ? Type::Dec64 : Type::Dec128, p, it.scale};
+                } else if (it.id == Type::F64) {
+                    ot = DType{Type::F64, 0, 0};
+                } else {
+                    ot = DType{Type::I64, 0, 0};
+                }
+                break;
+            case KRV_AGG_AVG:
+                if (dec) {
+                    const int p = std::min(38, it.precision + 4), s = std::min(38, it.scale + 4);
+                    ot = DType{(it.id == Type::Dec64 && p <= 18) ? Type::Dec64 : Type::Dec128, p, s};
+                } else {
+                    ot = DType{Type::F64, 0, 0};
+                }
+                break;
+            }
+        }
+        X.otype = (int)ot.id;
+        X.rp = ot.precision;
+        X.rs = ot.scale;
+        const bool nullable = !(x.function == KRV_AGG_COUNT_STAR || x.function == KRV_AGG_COUNT);
+        DevCol c = make_col(rt_, ot, nout, nullable, name);
+        X.dst = const_cast<void *>(c.data);
+        X.dst_valid = nullable ? (uint32_t *)c.valid : nullptr;
+        out.cols.push_back(c);
+    }
+    out.rows = nout;
+    clear_status(rt_);
+    if (nout > 0) {
+        finalize_kernel<<<grid_for(rt_, nout, 256, 8), 256, 0, rt_->stream>>>(
+            P_, O, states_.as<uint8_t>(), gkeys_.as<long long>(), nout, key_type_.width(), const_cast<void *>(kcol.data),
+            key_nullable ? (uint32_t *)kcol.valid : nullptr, status_word(rt_));
+        rt_->launches++;
+        check_launch("finalize_kernel");
+    }
+    const uint32_t st = take_status(rt_);
+    if (st & ST_OVERFLOW)
+        fail(KRV_ARITHMETIC_OVERFLOW, "ARITHMETIC_OVERFLOW: an aggregate overflowed its result type (ANSI mode)");
+    return out;
+}
+
+HashAggregate *make_aggregate(Runtime *rt, const krv_agg_spec &spec) {
+    return new HashAggregate(rt, spec);
+}
+void agg_push(HashAggregate *a, const DevBatch &b) { a->push(b); }
+void agg_finish(HashAggregate *a) { a->finish(); }
+DevBatch agg_result(HashAggregate *a) { return a->result(); }
+int64_t agg_groups(const HashAggregate *a) { return a->groups(); }
+void agg_destroy(HashAggregate *a) { delete a; }
+
+}  // namespace krv

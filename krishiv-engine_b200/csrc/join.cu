@@ -1,0 +1,734 @@
+// join.cu -- the hash join operator: build arena, open-addressing table over
+// the engine's key hash, warp-cooperative probe with warp-aggregated output
+// compaction fused with the payload gather, and the right/full join tails.
+//
+// Reference: crates/krishiv-exec/src/join/ (HashJoin, join/mod.rs:1014;
+// BuildSink, join/build.rs; ProbeOp, join/probe.rs; JoinIndex,
+// crates/krishiv-exec/src/rows/index.rs).
+//
+// Table layout (one per join): `slots` is a power-of-two array of u64,
+// each (tag << 32) | (row + 1) with tag the top 32 bits of g = fin(h ^ seed)
+// and 0 = empty, probed linearly from g & mask; `next` chains the build rows
+// of one key newest-first (the reference's salted directory keeps a 16-bit
+// salt and row + 1 the same way, rows/index.rs:1-32, 211-283). A probe reads
+// a build row's key only when the 32-bit tag matches.
+#include <algorithm>
+#include <string>
+
+#include "krv_device.cuh"
+#include "ops.h"
+
+namespace krv {
+
+namespace {
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+__device__ __forceinline__ bool key_valid(const KeyColDev &c, int64_t i) {
+    return bit_get(c.valid, c.voff, i);
+}
+
+__device__ __forceinline__ void key_words(const KeyColDev &c, int64_t i, uint64_t &w0, uint64_t &w1) {
+    if (c.width == 4) {
+        w0 = static_cast<const uint32_t *>(c.data)[i];
+        w1 = 0;
+    } else if (c.width == 8) {
+        w0 = static_cast<const uint64_t *>(c.data)[i];
+        if (c.is_float) w0 = normalize_f64_bits(w0);
+        w1 = 0;
+    } else {
+        const uint64_t *p = static_cast<const uint64_t *>(c.data) + 2 * i;
+        w0 = p[0];
+        w1 = p[1];
+    }
+}
+
+// Every `=` key valid (join/keys.rs:17-19: a NULL `=` key never matches).
+__device__ __forceinline__ bool matchable(const KeysDev &k, int64_t i) {
+    for (int c = 0; c < k.n; c++)
+        if (!((k.null_safe >> c) & 1u) && !key_valid(k.c[c], i)) return false;
+    return true;
+}
+
+// The seedless row hash h (rows/layout.rs:487-555): NULL under a validity bit
+// (null-safe key) mixes NULL_HASH, a value mixes its 8-byte words.
+__device__ __forceinline__ uint64_t row_hash(const KeysDev &k, int64_t i) {
+    uint64_t h = 0;  // fold(SEEDLESS = 0, MIX)
+    for (int c = 0; c < k.n; c++) {
+        if (!key_valid(k.c[c], i)) {
+            if ((k.null_safe >> c) & 1u) h = mix(h, kNullHash);
+            continue;
+        }
+        uint64_t w0, w1;
+        key_words(k.c[c], i, w0, w1);
+        h = mix(h, w0);
+        if (k.c[c].width == 16) h = mix(h, w1);
+    }
+    return fold(h, kFinish);
+}
+
+__device__ __forceinline__ bool keys_eq(const KeysDev &a, int64_t i, const KeysDev &b, int64_t j) {
+    for (int c = 0; c < a.n; c++) {
+        const bool va = key_valid(a.c[c], i), vb = key_valid(b.c[c], j);
+        if (va != vb) return false;
+        if (!va) continue;
+        uint64_t a0, a1, b0, b1;
+        key_words(a.c[c], i, a0, a1);
+        key_words(b.c[c], j, b0, b1);
+        if (a0 != b0 || a1 != b1) return false;
+    }
+    return true;
+}
+
+// FAST: one non-float int64 key column.
+template <bool FAST>
+__device__ __forceinline__ uint64_t hash_of(const KeysDev &k, int64_t i) {
+    if (FAST) return hash_word(static_cast<const uint64_t *>(k.c[0].data)[i]);
+    return row_hash(k, i);
+}
+template <bool FAST>
+__device__ __forceinline__ bool eq_of(const KeysDev &a, int64_t i, const KeysDev &b, int64_t j) {
+    if (FAST)
+        return static_cast<const int64_t *>(a.c[0].data)[i] == static_cast<const int64_t *>(b.c[0].data)[j];
+    return keys_eq(a, i, b, j);
+}
+
+template <bool FAST>
+__global__ void __launch_bounds__(256) build_kernel(KeysDev keys, int64_t n, unsigned long long *slots,
+                                                    uint64_t mask, uint32_t *next, uint64_t seed,
+                                                    unsigned long long *ctr, uint32_t *status) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+        uint32_t nx = kNone;
+        if (!matchable(keys, i)) {
+            next[i] = nx;
+            ctr[1] = 1;  // a NULL `=` key in the build (null-aware anti join)
+            continue;
+        }
+        const uint64_t g = finalize(hash_of<FAST>(keys, i), seed);
+        const unsigned long long entry = ((g >> 32) << 32) | (unsigned long long)(i + 1);
+        uint64_t pos = g & mask;
+        for (uint64_t probes = 0;; probes++) {
+            if (probes > mask) {
+                atomicOr(status, ST_CAPACITY);
+                break;
+            }
+            unsigned long long s = __ldcg(slots + pos);
+            if (s == 0) {
+                const unsigned long long old = atomicCAS(slots + pos, 0ull, entry);
+                if (old == 0) {
+                    atomicAdd(ctr, 1ull);
+                    break;
+                }
+                s = old;
+            }
+            if ((s >> 32) == (entry >> 32) && eq_of<FAST>(keys, i, keys, (int64_t)(s & 0xFFFFFFFFull) - 1)) {
+                // Same key: this row becomes the head, the old head its next.
+                const unsigned long long old = atomicExch(slots + pos, entry);
+                nx = (uint32_t)(old & 0xFFFFFFFFull) - 1u;
+                break;
+            }
+            pos = (pos + 1) & mask;
+        }
+        next[i] = nx;
+    }
+}
+
+template <bool FAST>
+__device__ __forceinline__ uint32_t lookup(const KeysDev &pk, int64_t i, const KeysDev &bk,
+                                           const unsigned long long *slots, uint64_t mask, uint64_t seed) {
+    const uint64_t g = finalize(hash_of<FAST>(pk, i), seed);
+    const unsigned long long tag = g >> 32;
+    uint64_t pos = g & mask;
+    for (uint64_t probes = 0; probes <= mask; probes++) {
+        const unsigned long long s = __ldg(slots + pos);
+        if (s == 0) return kNone;
+        if ((s >> 32) == tag) {
+            const int64_t o = (int64_t)(s & 0xFFFFFFFFull) - 1;
+            if (eq_of<FAST>(pk, i, bk, o)) return (uint32_t)o;
+        }
+        pos = (pos + 1) & mask;
+    }
+    return kNone;
+}
+
+struct OutColDev {
+    const void *src;
+    const uint8_t *src_valid;
+    int64_t src_voff;
+    void *dst;
+    uint32_t *dst_valid;  // zeroed bitmap words, or null (non-nullable output)
+    int32_t width;
+    int32_t side;         // 0 probe row, 1 build row, 2 constant NULL
+};
+struct OutDev {
+    OutColDev c[2 * KRV_MAX_OUT_COLUMNS];
+    int32_t n;
+};
+
+__device__ __forceinline__ void copy_value(void *dst, const void *src, int64_t di, int64_t si, int w) {
+    switch (w) {
+    case 1: static_cast<uint8_t *>(dst)[di] = static_cast<const uint8_t *>(src)[si]; break;
+    case 4: static_cast<uint32_t *>(dst)[di] = static_cast<const uint32_t *>(src)[si]; break;
+    case 8: static_cast<uint64_t *>(dst)[di] = static_cast<const uint64_t *>(src)[si]; break;
+    default:
+        static_cast<uint4 *>(dst)[di] = static_cast<const uint4 *>(src)[si];
+        break;
+    }
+}
+__device__ __forceinline__ void zero_value(void *dst, int64_t di, int w) {
+    switch (w) {
+    case 1: static_cast<uint8_t *>(dst)[di] = 0; break;
+    case 4: static_cast<uint32_t *>(dst)[di] = 0; break;
+    case 8: static_cast<uint64_t *>(dst)[di] = 0; break;
+    default: static_cast<uint4 *>(dst)[di] = make_uint4(0, 0, 0, 0); break;
+    }
+}
+
+// Writes one round of a warp's output rows: lane `want` writes row `pos`
+// from probe row `prow` and build row `brow` (kNone: NULL build side; a
+// negative prow: NULL probe side). Validity bits of the round are combined in
+// rank order and OR-ed in with at most two atomics per column.
+__device__ __forceinline__ void emit_round(const OutDev &out, bool want, unsigned long long pos,
+                                           unsigned long long first, int64_t prow, uint32_t brow,
+                                           unsigned long long cap) {
+    const unsigned ballot = __ballot_sync(kFull, want);
+    const unsigned rank = __popc(ballot & lanemask_lt());
+    for (int k = 0; k < out.n; k++) {
+        const OutColDev &c = out.c[k];
+        bool v = false;
+        if (want && pos < cap) {
+            if (c.side == 0 && prow >= 0) {
+                copy_value(c.dst, c.src, (int64_t)pos, prow, c.width);
+                v = bit_get(c.src_valid, c.src_voff, prow);
+            } else if (c.side == 1 && brow != kNone) {
+                copy_value(c.dst, c.src, (int64_t)pos, brow, c.width);
+                v = bit_get(c.src_valid, c.src_voff, brow);
+            } else {
+                zero_value(c.dst, (int64_t)pos, c.width);
+            }
+        }
+        if (c.dst_valid) {
+            const unsigned m = __reduce_or_sync(kFull, (want && v) ? (1u << rank) : 0u);
+            if (lane_id() == 0 && m) {
+                const unsigned long long w = first >> 5;
+                const unsigned sh = (unsigned)(first & 31);
+                const unsigned long long capw = (cap + 31) >> 5;
+                if (w < capw) atomicOr(c.dst_valid + w, m << sh);
+                if (sh && w + 1 < capw && (m >> (32 - sh))) atomicOr(c.dst_valid + w + 1, m >> (32 - sh));
+            }
+        }
+    }
+}
+
+// Allocates this round's output rows for the warp: returns the first row of
+// the round (same on every lane) and this lane's row.
+__device__ __forceinline__ unsigned long long round_alloc(unsigned long long *count, bool want,
+                                                          unsigned long long &pos) {
+    const unsigned ballot = __ballot_sync(kFull, want);
+    unsigned long long first = 0;
+    if (lane_id() == 0 && ballot) first = atomicAdd(count, (unsigned long long)__popc(ballot));
+    first = __shfl_sync(kFull, first, 0);
+    pos = first + __popc(ballot & lanemask_lt());
+    return first;
+}
+
+// Pairs: inner, left outer, right outer, full outer (join/probe.rs:266-502).
+template <bool FAST>
+__global__ void __launch_bounds__(256) probe_pairs_kernel(KeysDev pk, KeysDev bk, int64_t n,
+                                                          const unsigned long long *slots, uint64_t mask,
+                                                          const uint32_t *next, uint64_t seed, OutDev out,
+                                                          unsigned long long cap, unsigned long long *count,
+                                                          uint8_t *marks, int pads_probe, int single_match,
+                                                          uint32_t *status, unsigned long long *max_chain) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += stride) {
+        const int64_t i = base + threadIdx.x;
+        const bool live = i < n;
+        uint32_t cur = kNone;
+        if (live && matchable(pk, i)) cur = lookup<FAST>(pk, i, bk, slots, mask, seed);
+        bool pad = live && cur == kNone && pads_probe;
+        unsigned chain = 0;
+        while (__any_sync(kFull, cur != kNone || pad)) {
+            const bool want = cur != kNone || pad;
+            unsigned long long pos;
+            const unsigned long long first = round_alloc(count, want, pos);
+            emit_round(out, want, pos, first, i, cur, cap);
+            if (cur != kNone) {
+                if (marks) marks[cur] = 1;
+                chain++;
+                cur = next[cur];
+            } else {
+                pad = false;
+            }
+        }
+        if (single_match && chain > 1) atomicOr(status, ST_TOO_MANY);
+        if (chain > 1) atomicMax(max_chain, (unsigned long long)chain);
+    }
+}
+
+// Probe rows once: semi, anti, null-aware anti (join/mod.rs:27-34).
+// kind 0 semi, 1 anti, 2 null-aware anti.
+template <bool FAST>
+__global__ void __launch_bounds__(256) probe_rows_kernel(KeysDev pk, KeysDev bk, int64_t n,
+                                                         const unsigned long long *slots, uint64_t mask,
+                                                         uint64_t seed, OutDev out, unsigned long long cap,
+                                                         unsigned long long *count, int kind, int build_empty,
+                                                         int build_has_null) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += stride) {
+        const int64_t i = base + threadIdx.x;
+        const bool live = i < n;
+        bool ok = false;
+        if (live) {
+            const bool m = matchable(pk, i);
+            const bool hit = m && !build_empty && lookup<FAST>(pk, i, bk, slots, mask, seed) != kNone;
+            if (kind == 0) ok = hit;
+            else if (kind == 1) ok = !hit;
+            else ok = build_empty || (!build_has_null && m && !hit);
+        }
+        unsigned long long pos;
+        const unsigned long long first = round_alloc(count, ok, pos);
+        emit_round(out, ok, pos, first, i, kNone, cap);
+    }
+}
+
+// Existence: every probe row once plus `exists` (join/mod.rs:35-45). Rows
+// keep their positions; the flag of rows [base, base + 32) is one word.
+template <bool FAST>
+__global__ void __launch_bounds__(256) probe_exists_kernel(KeysDev pk, KeysDev bk, int64_t n,
+                                                           const unsigned long long *slots, uint64_t mask,
+                                                           uint64_t seed, uint32_t *exists, int build_empty) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += stride) {
+        const int64_t i = base + threadIdx.x;
+        bool hit = false;
+        if (i < n && !build_empty && matchable(pk, i)) hit = lookup<FAST>(pk, i, bk, slots, mask, seed) != kNone;
+        const unsigned word = __ballot_sync(kFull, hit);
+        if (lane_id() == 0 && (i < n)) exists[i >> 5] = word;
+    }
+}
+
+// Build rows by their marks once the probe side is done (emit_build,
+// join/probe.rs:610-): kind 0 right semi (marked rows with a matchable key),
+// kind 1 unmatched rows (right anti, right outer, full outer).
+__global__ void __launch_bounds__(256) tail_kernel(int64_t nb, const uint8_t *marks, KeysDev bk, int kind,
+                                                   OutDev out, unsigned long long cap,
+                                                   unsigned long long *count) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nb; base += stride) {
+        const int64_t r = base + threadIdx.x;
+        bool ok = false;
+        if (r < nb) ok = kind == 0 ? (marks[r] != 0 && matchable(bk, r)) : marks[r] == 0;
+        unsigned long long pos;
+        const unsigned long long first = round_alloc(count, ok, pos);
+        emit_round(out, ok, pos, first, -1, ok ? (uint32_t)r : kNone, cap);
+    }
+}
+
+void zero(Runtime *rt, void *p, size_t bytes) {
+    if (bytes) KRV_CUDA(cudaMemsetAsync(p, 0, bytes, rt->stream));
+}
+
+}  // namespace
+
+KeysDev keys_of(const DevBatch &b, const int32_t *cols, int n, const int32_t *null_safe) {
+    KeysDev k{};
+    k.n = n;
+    for (int i = 0; i < n; i++) {
+        if (cols[i] < 0 || cols[i] >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "key column out of range");
+        const DevCol &c = b.cols[cols[i]];
+        const int w = c.type.width();
+        if (w != 4 && w != 8 && w != 16) fail(KRV_UNSUPPORTED, "key column of type " + c.type.format());
+        k.c[i] = KeyColDev{c.data, c.valid, c.valid_off, w, c.type.id == Type::F64 ? 1 : 0};
+        if (null_safe && null_safe[i]) k.null_safe |= 1u << i;
+    }
+    return k;
+}
+
+static bool fast_keys(const KeysDev &k) { return k.n == 1 && k.c[0].width == 8 && !k.c[0].is_float; }
+
+HashJoin::HashJoin(Runtime *rt, const krv_join_spec &spec) : rt_(rt), spec_(spec) {
+    if (spec.n_keys < 1 || spec.n_keys > KRV_MAX_KEYS) fail(KRV_INVALID_ARGUMENT, "join needs 1..4 keys");
+    if (spec.join_type < KRV_JOIN_INNER || spec.join_type > KRV_JOIN_FULL_OUTER)
+        fail(KRV_INVALID_ARGUMENT, "unknown join type");
+    if (spec.has_residual_filter)
+        fail(KRV_UNSUPPORTED, "KRISHIV_UNSUPPORTED_FEATURE: residual join filters on the GPU join");
+    if (spec.single_match && spec.join_type != KRV_JOIN_LEFT_OUTER)
+        fail(KRV_INVALID_ARGUMENT, "single_match is for left outer joins only");
+    if (spec.join_type == KRV_JOIN_NULL_AWARE_ANTI && (spec.n_keys != 1 || spec.null_safe[0]))
+        fail(KRV_INVALID_ARGUMENT, "a null-aware anti join has one `=` key");
+    if (spec.n_probe_out > KRV_MAX_OUT_COLUMNS || spec.n_build_out > KRV_MAX_OUT_COLUMNS)
+        fail(KRV_INVALID_ARGUMENT, "too many output columns");
+    if (spec_.max_load <= 0.f || spec_.max_load > 0.9f) spec_.max_load = 0.5f;
+    if (spec_.seed == 0) spec_.seed = 0x4B52565F4A4F494EULL;  // fixed: results never depend on it
+    counters_.partitions = 1;
+}
+
+void HashJoin::append_arena(const DevBatch &b) {
+    if (!have_schema_) {
+        for (const DevCol &c : b.cols) {
+            DevCol a;
+            a.type = c.type;
+            a.name = c.name;
+            a.nullable = c.nullable;
+            arena_cols_.push_back(a);
+        }
+        arena_data_.resize(b.cols.size());
+        arena_valid_.resize(b.cols.size());
+        have_schema_ = true;
+    } else {
+        if (b.cols.size() != arena_cols_.size()) fail(KRV_INVALID_ARGUMENT, "build batches differ in columns");
+        for (size_t i = 0; i < b.cols.size(); i++)
+            if (b.cols[i].type != arena_cols_[i].type) fail(KRV_INVALID_ARGUMENT, "build batches differ in types");
+    }
+    const int64_t need = build_rows_ + b.rows;
+    if (need > (int64_t)0xFFFFFFFEll) fail(KRV_UNSUPPORTED, "more than 2^32-2 build rows in one table");
+    if (need > arena_cap_) {
+        int64_t cap = std::max<int64_t>({need, arena_cap_ * 2, spec_.build_rows_hint, 1024});
+        for (size_t i = 0; i < arena_cols_.size(); i++) {
+            const DType t = arena_cols_[i].type;
+            const size_t bytes = t.id == Type::Bool ? (size_t)ceil_div(cap, 8) : (size_t)cap * t.width();
+            auto nd = std::make_shared<DBuf>(rt_, bytes);
+            auto nv = std::make_shared<DBuf>(rt_, (size_t)ceil_div(cap, 32) * 4 + 8);
+            zero(rt_, nv->get(), nv->bytes());
+            if (build_rows_) {
+                const size_t old = t.id == Type::Bool ? (size_t)ceil_div(build_rows_, 8) : (size_t)build_rows_ * t.width();
+                KRV_CUDA(cudaMemcpyAsync(nd->get(), arena_data_[i]->get(), old, cudaMemcpyDeviceToDevice, rt_->stream));
+                KRV_CUDA(cudaMemcpyAsync(nv->get(), arena_valid_[i]->get(), (size_t)ceil_div(build_rows_, 8),
+                                         cudaMemcpyDeviceToDevice, rt_->stream));
+            }
+            arena_data_[i] = nd;
+            arena_valid_[i] = nv;
+        }
+        arena_cap_ = cap;
+    }
+    for (size_t i = 0; i < arena_cols_.size(); i++) {
+        const DevCol &c = b.cols[i];
+        const DType t = c.type;
+        if (t.id == Type::Bool) fail(KRV_UNSUPPORTED, "boolean build columns");
+        const size_t w = (size_t)t.width();
+        if (b.rows)
+            KRV_CUDA(cudaMemcpyAsync(arena_data_[i]->as<uint8_t>() + build_rows_ * w, c.data, (size_t)b.rows * w,
+                                     cudaMemcpyDeviceToDevice, rt_->stream));
+        append_bits(rt_, c.valid, c.valid_off, b.rows, arena_valid_[i]->as<uint8_t>(), build_rows_);
+        if (c.valid) arena_cols_[i].nullable = true;
+    }
+    build_rows_ = need;
+}
+
+void HashJoin::build_push(DevBatch b) {
+    if (built_) fail(KRV_INVALID_ARGUMENT, "build_push after build_finish");
+    DeviceGuard g(rt_);
+    append_arena(b);
+}
+
+HashJoin::TableDev HashJoin::table_dev() const {
+    return TableDev{slots_.as<unsigned long long>(), mask_, next_.as<uint32_t>(), spec_.seed};
+}
+
+void HashJoin::build_finish() {
+    if (built_) fail(KRV_INVALID_ARGUMENT, "build_finish called twice");
+    DeviceGuard g(rt_);
+    built_ = true;
+    arena_.rows = build_rows_;
+    arena_.cols.clear();
+    for (size_t i = 0; i < arena_cols_.size(); i++) {
+        DevCol c = arena_cols_[i];
+        c.length = build_rows_;
+        c.hold_data = arena_data_[i];
+        c.hold_valid = arena_valid_[i];
+        c.data = c.hold_data ? c.hold_data->get() : nullptr;
+        c.valid = c.hold_valid ? c.hold_valid->as<uint8_t>() : nullptr;
+        c.valid_off = 0;
+        arena_.cols.push_back(c);
+    }
+    const uint64_t want = (uint64_t)std::ceil((double)std::max<int64_t>(build_rows_, 1) / spec_.max_load);
+    const uint64_t slots = std::max<uint64_t>(1024, next_pow2(want));
+    mask_ = slots - 1;
+    slots_ = DBuf(rt_, slots * 8);
+    zero(rt_, slots_.get(), slots * 8);
+    next_ = DBuf(rt_, (size_t)std::max<int64_t>(build_rows_, 1) * 4);
+    counters_dev_ = DBuf(rt_, 64);
+    zero(rt_, counters_dev_.get(), 64);
+    const int jt = spec_.join_type;
+    const bool preserved = jt == KRV_JOIN_RIGHT_SEMI || jt == KRV_JOIN_RIGHT_ANTI || jt == KRV_JOIN_RIGHT_OUTER ||
+                           jt == KRV_JOIN_FULL_OUTER;
+    if (preserved) {
+        marks_ = DBuf(rt_, (size_t)std::max<int64_t>(build_rows_, 1));
+        zero(rt_, marks_.get(), marks_.bytes());
+    }
+    clear_status(rt_);
+    if (build_rows_ > 0) {
+        if (arena_.cols.empty()) fail(KRV_INVALID_ARGUMENT, "build batches without columns");
+        KeysDev k = keys_of(arena_, spec_.build_keys, spec_.n_keys, spec_.null_safe);
+        const int threads = 256;
+        const int grid = grid_for(rt_, build_rows_, threads, 8);
+        auto *ctr = counters_dev_.as<unsigned long long>();
+        if (fast_keys(k))
+            build_kernel<true><<<grid, threads, 0, rt_->stream>>>(k, build_rows_, slots_.as<unsigned long long>(), mask_,
+                                                                 next_.as<uint32_t>(), spec_.seed, ctr, status_word(rt_));
+        else
+            build_kernel<false><<<grid, threads, 0, rt_->stream>>>(k, build_rows_, slots_.as<unsigned long long>(), mask_,
+                                                                  next_.as<uint32_t>(), spec_.seed, ctr, status_word(rt_));
+        rt_->launches++;
+        check_launch("build_kernel");
+    }
+    unsigned long long host_ctr[2];
+    KRV_CUDA(cudaMemcpyAsync(host_ctr, counters_dev_.get(), 16, cudaMemcpyDeviceToHost, rt_->stream));
+    const uint32_t st = take_status(rt_);
+    if (st & ST_CAPACITY) fail(KRV_INTERNAL, "join table full");
+    counters_.build_rows = build_rows_;
+    counters_.build_keys = (int64_t)host_ctr[0];
+    counters_.table_slots = (int64_t)slots;
+    any_null_build_ = host_ctr[1] != 0;
+    // The runtime filter of a one-key join (BuildSink::publish, join/build.rs:482).
+    if (spec_.runtime_filter && spec_.n_keys == 1) {
+        const DevCol &key = arena_.cols[spec_.build_keys[0]];
+        if (key.type.id == Type::I64) {
+            krv_key_filter_options o;
+            krv_key_filter_options_default(&o);
+            filter_ = build_key_filter(rt_, o, key);
+        }
+    }
+}
+
+static std::vector<int> projection(int n, const int32_t *cols, int ncols) {
+    std::vector<int> v;
+    if (n < 0) {
+        for (int i = 0; i < ncols; i++) v.push_back(i);
+    } else {
+        for (int i = 0; i < n; i++) {
+            if (cols[i] < 0 || cols[i] >= ncols) fail(KRV_INVALID_ARGUMENT, "projection column out of range");
+            v.push_back(cols[i]);
+        }
+    }
+    return v;
+}
+
+DevBatch HashJoin::probe(const DevBatch &in) {
+    if (!built_) fail(KRV_INVALID_ARGUMENT, "probe before build_finish");
+    DeviceGuard g(rt_);
+    const int jt = spec_.join_type;
+    const int64_t n = in.rows;
+    counters_.probe_rows += n;
+    if (probe_types_.empty()) {
+        for (const DevCol &c : in.cols) {
+            probe_types_.push_back(c.type);
+            probe_names_.push_back(c.name);
+            probe_nullable_.push_back(c.nullable);
+        }
+    }
+    KeysDev pk = keys_of(in, spec_.probe_keys, spec_.n_keys, spec_.null_safe);
+    KeysDev bk{};
+    if (build_rows_ > 0) bk = keys_of(arena_, spec_.build_keys, spec_.n_keys, spec_.null_safe);
+    else bk = pk;  // never dereferenced: the table is empty
+    for (int c = 0; c < spec_.n_keys; c++) {
+        const DevCol &pc = in.cols[spec_.probe_keys[c]];
+        if (build_rows_ > 0 && pc.type != arena_.cols[spec_.build_keys[c]].type)
+            fail(KRV_INVALID_ARGUMENT, "probe and build key types differ");
+    }
+    const bool fast = fast_keys(pk);
+    const auto pcols = projection(spec_.n_probe_out, spec_.probe_out, (int)in.cols.size());
+    const auto bcols = projection(spec_.n_build_out, spec_.build_out, (int)arena_cols_.size());
+    const int threads = 256;
+    const int grid = grid_for(rt_, n, threads, 8);
+    const auto *slots = slots_.as<unsigned long long>();
+    DevBatch out;
+
+    if (jt == KRV_JOIN_EXISTENCE) {
+        out.rows = n;
+        for (int pc : pcols) {
+            const DevCol &s = in.cols[pc];
+            DevCol d = make_col(rt_, s.type, n, s.nullable || s.valid, s.name);
+            const size_t bytes = s.type.id == Type::Bool ? (size_t)ceil_div(n, 8) : (size_t)n * s.type.width();
+            if (bytes) KRV_CUDA(cudaMemcpyAsync(const_cast<void *>(d.data), s.data, bytes, cudaMemcpyDeviceToDevice, rt_->stream));
+            if (d.valid) {
+                zero(rt_, const_cast<uint8_t *>(d.valid), d.hold_valid->bytes());
+                append_bits(rt_, s.valid, s.valid_off, n, const_cast<uint8_t *>(d.valid), 0);
+            }
+            out.cols.push_back(d);
+        }
+        DevCol ex = make_col(rt_, DType{Type::Bool, 0, 0}, n, false, "exists");
+        zero(rt_, const_cast<void *>(ex.data), ex.hold_data->bytes());
+        if (n > 0) {
+            if (fast)
+                probe_exists_kernel<true><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, spec_.seed,
+                                                                             (uint32_t *)ex.data, build_rows_ == 0);
+            else
+                probe_exists_kernel<false><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, spec_.seed,
+                                                                              (uint32_t *)ex.data, build_rows_ == 0);
+            rt_->launches++;
+            check_launch("probe_exists_kernel");
+        }
+        out.cols.push_back(ex);
+        counters_.output_rows += n;
+        return out;
+    }
+
+    const bool pairs = jt == KRV_JOIN_INNER || jt == KRV_JOIN_LEFT_OUTER || jt == KRV_JOIN_RIGHT_OUTER ||
+                       jt == KRV_JOIN_FULL_OUTER;
+    if (!pairs && (jt == KRV_JOIN_RIGHT_SEMI || jt == KRV_JOIN_RIGHT_ANTI)) {
+        // Probe only marks build rows; output comes at finish.
+        if (n > 0 && build_rows_ > 0) {
+            OutDev od{};
+            od.n = 0;
+            DBuf cnt(rt_, 8);
+            zero(rt_, cnt.get(), 8);
+            auto *mc = counters_dev_.as<unsigned long long>() + 2;
+            if (fast)
+                probe_pairs_kernel<true><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, next_.as<uint32_t>(),
+                                                                            spec_.seed, od, 0, cnt.as<unsigned long long>(),
+                                                                            marks_.as<uint8_t>(), 0, 0, status_word(rt_), mc);
+            else
+                probe_pairs_kernel<false><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, next_.as<uint32_t>(),
+                                                                             spec_.seed, od, 0, cnt.as<unsigned long long>(),
+                                                                             marks_.as<uint8_t>(), 0, 0, status_word(rt_), mc);
+            rt_->launches++;
+            check_launch("probe_pairs_kernel");
+        }
+        // Nothing is emitted by this batch: an empty batch of the output shape.
+        DevBatch empty;
+        for (int bc : bcols) {
+            const DevCol &meta = arena_cols_[bc];
+            empty.cols.push_back(make_col(rt_, meta.type, 0, meta.nullable, meta.name));
+        }
+        return empty;
+    }
+
+    const bool build_nullable = jt == KRV_JOIN_LEFT_OUTER || jt == KRV_JOIN_FULL_OUTER;
+    const bool probe_nullable = jt == KRV_JOIN_RIGHT_OUTER || jt == KRV_JOIN_FULL_OUTER;
+    unsigned long long cap = (unsigned long long)std::max<int64_t>(n, 1);
+    DBuf cnt(rt_, 8);
+    for (int attempt = 0; attempt < 4; attempt++) {
+        out = DevBatch{};
+        OutDev od{};
+        for (int pc : pcols) {
+            const DevCol &s = in.cols[pc];
+            if (s.type.id == Type::Bool) fail(KRV_UNSUPPORTED, "boolean probe payload columns");
+            const bool nullable = s.nullable || s.valid || probe_nullable;
+            DevCol d = make_col(rt_, s.type, (int64_t)cap, nullable, s.name);
+            if (d.valid) zero(rt_, const_cast<uint8_t *>(d.valid), d.hold_valid->bytes());
+            od.c[od.n++] = OutColDev{s.data, s.valid, s.valid_off, const_cast<void *>(d.data),
+                                     (uint32_t *)d.valid, s.type.width(), 0};
+            out.cols.push_back(d);
+        }
+        if (pairs) {
+            for (int bc : bcols) {
+                const DevCol &s = arena_.cols.empty() ? DevCol{} : arena_.cols[bc];
+                const DevCol &meta = arena_cols_[bc];
+                const bool nullable = meta.nullable || build_nullable;
+                DevCol d = make_col(rt_, meta.type, (int64_t)cap, nullable, meta.name);
+                if (d.valid) zero(rt_, const_cast<uint8_t *>(d.valid), d.hold_valid->bytes());
+                od.c[od.n++] = OutColDev{s.data, meta.nullable ? s.valid : nullptr, 0, const_cast<void *>(d.data),
+                                         (uint32_t *)d.valid, meta.type.width(), 1};
+                out.cols.push_back(d);
+            }
+        }
+        zero(rt_, cnt.get(), 8);
+        clear_status(rt_);
+        if (n > 0) {
+            auto *count = cnt.as<unsigned long long>();
+            if (pairs) {
+                if (build_rows_ > 0 || jt == KRV_JOIN_LEFT_OUTER || jt == KRV_JOIN_FULL_OUTER) {
+                    // An empty build still has an all-empty table: every lookup misses.
+                    auto *mc = counters_dev_.as<unsigned long long>() + 2;
+                    uint8_t *marks = marks_.get() ? marks_.as<uint8_t>() : nullptr;
+                    const int pad = jt == KRV_JOIN_LEFT_OUTER || jt == KRV_JOIN_FULL_OUTER;
+                    if (fast)
+                        probe_pairs_kernel<true><<<grid, threads, 0, rt_->stream>>>(
+                            pk, bk, n, slots, mask_, next_.as<uint32_t>(), spec_.seed, od, cap, count, marks, pad,
+                            spec_.single_match, status_word(rt_), mc);
+                    else
+                        probe_pairs_kernel<false><<<grid, threads, 0, rt_->stream>>>(
+                            pk, bk, n, slots, mask_, next_.as<uint32_t>(), spec_.seed, od, cap, count, marks, pad,
+                            spec_.single_match, status_word(rt_), mc);
+                    rt_->launches++;
+                    check_launch("probe_pairs_kernel");
+                }
+            } else {
+                const int kind = jt == KRV_JOIN_LEFT_SEMI ? 0 : jt == KRV_JOIN_LEFT_ANTI ? 1 : 2;
+                const unsigned long long *sl = slots;
+                const uint64_t mask = mask_;
+                if (fast)
+                    probe_rows_kernel<true><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, sl, mask, spec_.seed, od, cap,
+                                                                               count, kind, build_rows_ == 0,
+                                                                               any_null_build_);
+                else
+                    probe_rows_kernel<false><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, sl, mask, spec_.seed, od, cap,
+                                                                                count, kind, build_rows_ == 0,
+                                                                                any_null_build_);
+                rt_->launches++;
+                check_launch("probe_rows_kernel");
+            }
+        }
+        const unsigned long long got = read_scalar<unsigned long long>(rt_, cnt.get());
+        const uint32_t st = take_status(rt_);
+        if (st & ST_TOO_MANY) fail(KRV_TOO_MANY_ROWS, "SCALAR_SUBQUERY_TOO_MANY_ROWS: a probe row matched more than one build row");
+        if (got <= cap) {
+            out.rows = (int64_t)got;
+            for (DevCol &c : out.cols) c.length = out.rows;
+            counters_.output_rows += out.rows;
+            return out;
+        }
+        cap = got;  // output larger than guessed: run again with room for all of it
+    }
+    fail(KRV_INTERNAL, "join output did not converge");
+}
+
+DevBatch HashJoin::finish() {
+    if (!built_) fail(KRV_INVALID_ARGUMENT, "finish before build_finish");
+    DeviceGuard g(rt_);
+    const int jt = spec_.join_type;
+    const bool tail = jt == KRV_JOIN_RIGHT_SEMI || jt == KRV_JOIN_RIGHT_ANTI || jt == KRV_JOIN_RIGHT_OUTER ||
+                      jt == KRV_JOIN_FULL_OUTER;
+    if (!tail || finished_) {
+        finished_ = true;
+        return DevBatch{};
+    }
+    finished_ = true;
+    const bool with_probe = jt == KRV_JOIN_RIGHT_OUTER || jt == KRV_JOIN_FULL_OUTER;
+    if (with_probe && probe_types_.empty())
+        fail(KRV_INVALID_ARGUMENT, "an outer join's tail needs the probe schema: probe at least one batch");
+    const auto bcols = projection(spec_.n_build_out, spec_.build_out, (int)arena_cols_.size());
+    std::vector<int> pcols;
+    if (with_probe) pcols = projection(spec_.n_probe_out, spec_.probe_out, (int)probe_types_.size());
+    const unsigned long long cap = (unsigned long long)std::max<int64_t>(build_rows_, 1);
+    DevBatch out;
+    OutDev od{};
+    for (int pc : pcols) {
+        DevCol d = make_col(rt_, probe_types_[pc], (int64_t)cap, true, probe_names_[pc]);
+        zero(rt_, const_cast<uint8_t *>(d.valid), d.hold_valid->bytes());
+        od.c[od.n++] = OutColDev{nullptr, nullptr, 0, const_cast<void *>(d.data), (uint32_t *)d.valid,
+                                 probe_types_[pc].width(), 2};
+        out.cols.push_back(d);
+    }
+    for (int bc : bcols) {
+        const DevCol &meta = arena_cols_[bc];
+        const DevCol &s = arena_.cols[bc];
+        const bool nullable = meta.nullable || jt == KRV_JOIN_FULL_OUTER;
+        DevCol d = make_col(rt_, meta.type, (int64_t)cap, nullable, meta.name);
+        if (d.valid) zero(rt_, const_cast<uint8_t *>(d.valid), d.hold_valid->bytes());
+        od.c[od.n++] = OutColDev{s.data, meta.nullable ? s.valid : nullptr, 0, const_cast<void *>(d.data),
+                                 (uint32_t *)d.valid, meta.type.width(), 1};
+        out.cols.push_back(d);
+    }
+    DBuf cnt(rt_, 8);
+    zero(rt_, cnt.get(), 8);
+    if (build_rows_ > 0) {
+        KeysDev bk = keys_of(arena_, spec_.build_keys, spec_.n_keys, spec_.null_safe);
+        const int threads = 256;
+        tail_kernel<<<grid_for(rt_, build_rows_, threads, 8), threads, 0, rt_->stream>>>(
+            build_rows_, marks_.as<uint8_t>(), bk, jt == KRV_JOIN_RIGHT_SEMI ? 0 : 1, od, cap,
+            cnt.as<unsigned long long>());
+        rt_->launches++;
+        check_launch("tail_kernel");
+    }
+    out.rows = (int64_t)read_scalar<unsigned long long>(rt_, cnt.get());
+    for (DevCol &c : out.cols) c.length = out.rows;
+    counters_.output_rows += out.rows;
+    return out;
+}
+
+}  // namespace krv

@@ -1,0 +1,149 @@
+// ops.h -- the operator classes behind the C ABI (krv_gpu.h). Each mirrors
+// the Krishiv engine operator it replaces; the file:line of that operator is
+// on the class.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "krv_internal.h"
+
+namespace krv {
+
+// ---- device key views ----------------------------------------------------------
+struct KeyColDev {
+    const void *data;
+    const uint8_t *valid;
+    int64_t voff;
+    int32_t width;      // 4, 8 or 16
+    int32_t is_float;   // float64 key: normalized before hashing/comparing
+};
+struct KeysDev {
+    KeyColDev c[KRV_MAX_KEYS];
+    int32_t n;
+    uint32_t null_safe;  // bit k: key k is compared with <=>
+};
+KeysDev keys_of(const DevBatch &b, const int32_t *cols, int n, const int32_t *null_safe);
+
+// ---- runtime key filter (crates/krishiv-io/src/runtime_filter/filter.rs:627) ----
+struct KeyFilterImpl {
+    Runtime *rt = nullptr;
+    krv_key_filter_info info{};
+    krv_key_filter_options opt{};
+    DBuf bloom;          // Parquet SBBF words (info.bloom_bytes)
+    DBuf exact_slots;    // exact set: open-addressing int64 set (EMPTY = INT64_MIN)
+    uint64_t exact_mask = 0;
+    int32_t exact_has_min = 0;  // INT64_MIN is in the exact set
+};
+// KeyFilterBuilder add + finish over the valid rows of an int64 column.
+std::shared_ptr<KeyFilterImpl> build_key_filter(Runtime *rt, const krv_key_filter_options &opt,
+                                                const DevCol &keys);
+// KeyFilter::evaluate: a boolean column (bit-packed, no NULLs).
+DevCol evaluate_key_filter(const KeyFilterImpl &f, const DevCol &keys);
+// Device view for fused kernels.
+struct KeyFilterDev {
+    int32_t form;
+    int32_t has_range;
+    int64_t lo, hi;
+    const uint32_t *bloom;
+    uint64_t nblocks;
+    const unsigned long long *exact;
+    uint64_t exact_mask;
+    int32_t exact_has_min;
+    int32_t nulls_pass;
+};
+KeyFilterDev key_filter_dev(const KeyFilterImpl &f);
+
+// ---- hash join (crates/krishiv-exec/src/join/mod.rs:1014 HashJoin) -------------
+class HashJoin {
+  public:
+    HashJoin(Runtime *rt, const krv_join_spec &spec);
+    void build_push(DevBatch b);
+    void build_finish();
+    // Joins one probe batch; returns the output batch (all rows of it).
+    DevBatch probe(const DevBatch &in);
+    // Rows emitted after the last probe batch (right/full joins).
+    DevBatch finish();
+    std::shared_ptr<KeyFilterImpl> key_filter() const { return filter_; }
+    krv_join_counters counters() const { return counters_; }
+    const krv_join_spec &spec() const { return spec_; }
+    // Takes the probe key columns and the output projection of `s` (a plan
+    // that probes one built table with batches of another shape).
+    void set_probe_shape(const krv_join_spec &s) {
+        for (int i = 0; i < KRV_MAX_KEYS; i++) spec_.probe_keys[i] = s.probe_keys[i];
+        spec_.n_probe_out = s.n_probe_out;
+        spec_.n_build_out = s.n_build_out;
+        for (int i = 0; i < KRV_MAX_OUT_COLUMNS; i++) {
+            spec_.probe_out[i] = s.probe_out[i];
+            spec_.build_out[i] = s.build_out[i];
+        }
+        probe_types_.clear();
+        probe_names_.clear();
+        probe_nullable_.clear();
+    }
+
+    // Pending output batches for the bounded-output protocol.
+    std::vector<DevBatch> pending;
+
+    // Device view of the built table (for fused pipelines).
+    struct TableDev {
+        unsigned long long *slots;
+        uint64_t mask;
+        const uint32_t *next;
+        uint64_t seed;
+    };
+    TableDev table_dev() const;
+    const DevBatch &arena() const { return arena_; }
+
+  private:
+    void append_arena(const DevBatch &b);
+    Runtime *rt_;
+    krv_join_spec spec_;
+    std::vector<DevCol> arena_cols_;    // growable build arena
+    std::vector<std::shared_ptr<DBuf>> arena_data_, arena_valid_;
+    int64_t arena_cap_ = 0;
+    DevBatch arena_;                    // view of the arena
+    bool have_schema_ = false;
+    DBuf slots_, next_, marks_, counters_dev_;
+    uint64_t mask_ = 0;
+    int64_t build_rows_ = 0;
+    bool built_ = false;
+    bool any_null_build_ = false;
+    bool finished_ = false;
+    std::vector<DType> probe_types_;
+    std::vector<std::string> probe_names_;
+    std::vector<bool> probe_nullable_;
+    std::shared_ptr<KeyFilterImpl> filter_;
+    krv_join_counters counters_{};
+};
+
+// ---- grouped hash aggregate (crates/krishiv-exec/src/aggregate/sink.rs:181) ----
+class HashAggregate;
+HashAggregate *make_aggregate(Runtime *rt, const krv_agg_spec &spec);
+void agg_push(HashAggregate *a, const DevBatch &b);
+void agg_finish(HashAggregate *a);
+DevBatch agg_result(HashAggregate *a);
+int64_t agg_groups(const HashAggregate *a);
+void agg_destroy(HashAggregate *a);
+
+// ---- star pipeline -------------------------------------------------------------
+class StarPipeline;
+StarPipeline *make_star(Runtime *rt, const krv_star_spec &spec);
+void star_build(StarPipeline *s, const DevBatch &a, const DevBatch &b);
+void star_probe(StarPipeline *s, const DevBatch &fact);
+DevBatch star_result(StarPipeline *s);
+void star_reset(StarPipeline *s);
+krv_star_counters star_counters(const StarPipeline *s);
+void star_destroy(StarPipeline *s);
+
+// ---- generators ------------------------------------------------------------------
+void gen_fill(Runtime *rt, const krv_gen_spec &spec, int64_t n, void *out, void *out_valid);
+
+// ---- small device utilities (util.cu) --------------------------------------------
+// Copies n bits from (src, src_off) into (dst, dst_off); dst bits must be zero.
+void append_bits(Runtime *rt, const uint8_t *src, int64_t src_off, int64_t n, uint8_t *dst,
+                 int64_t dst_off);
+// Sets n bits starting at dst_off to 1 (dst bits must be zero).
+void set_bits(Runtime *rt, uint8_t *dst, int64_t dst_off, int64_t n);
+
+}  // namespace krv

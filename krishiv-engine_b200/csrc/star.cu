@@ -1,0 +1,630 @@
+// star.cu -- the star-join pipeline: two dimension builds that publish
+// runtime key filters, the fact side filtered by both and probed against both
+// tables, and a grouped float64 sum of price * (1 - discount).
+//
+// Two forms of the same plan:
+//  - fused: the fact side is one kernel; each fact row is read once, tested
+//    against dimension B's Bloom filter (staged in shared memory) and A's
+//    (L2-resident), probed against both tables only when both filters pass,
+//    and its value added to a per-CTA shared-memory accumulator of its group;
+//    CTAs merge their accumulators at the end with compensated atomics;
+//  - plain: one operator per launch through the operator classes (runtime
+//    filter evaluate, compaction, join probe, join probe, projection,
+//    aggregate), each materializing its output in HBM.
+//
+// Reference plan pieces: HashJoinNode (crates/krishiv-exec/src/join/
+// mod.rs:1188-1211), runtime filters published by the build
+// (join/build.rs:482) and applied in the scan's row stage
+// (crates/krishiv-exec/src/operators/runtime_filter.rs:1-45), HashAggregate
+// (crates/krishiv-exec/src/aggregate/sink.rs:181).
+//
+// The per-row value is computed as the CPU does it: (double)price, then
+// 1.0 - discount and one product, each rounded (no fused multiply-add).
+#include <algorithm>
+#include <memory>
+
+#include "krv_device.cuh"
+#include "krv_filter.cuh"
+#include "ops.h"
+
+namespace krv {
+
+namespace {
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr long long kAttrEmpty = (long long)0x8080808080808080ULL;
+constexpr int kMaxSmemGroups = 1024;
+
+struct TableView {
+    const unsigned long long *slots;
+    uint64_t mask;
+    const uint32_t *next;
+    uint64_t seed;
+    const long long *keys;  // build key column
+    const int32_t *gid;     // dense group id of each build row's attribute
+};
+
+__device__ __forceinline__ uint32_t table_lookup(const TableView &t, long long k) {
+    const uint64_t g = finalize(hash_word((uint64_t)k), t.seed);
+    const unsigned long long tag = g >> 32;
+    uint64_t pos = g & t.mask;
+    for (uint64_t p = 0; p <= t.mask; p++) {
+        const unsigned long long s = __ldg(t.slots + pos);
+        if (s == 0) return kNone;
+        if ((s >> 32) == tag) {
+            const uint32_t o = (uint32_t)(s & 0xFFFFFFFFull) - 1u;
+            if (__ldg(t.keys + o) == k) return o;
+        }
+        pos = (pos + 1) & t.mask;
+    }
+    return kNone;
+}
+
+struct StarArgs {
+    const long long *fk_a, *fk_b, *price;
+    const double *disc;
+    int64_t n;
+    KeyFilterDev fa, fb;
+    int use_filters;
+    int group_by;  // 0: dim A's attribute, 1: dim B's
+    TableView ta, tb;
+    int ngroups;
+    int bloom_b_smem_words;  // > 0: stage B's Bloom words in shared memory
+    double *sum_hi, *sum_lo;
+    unsigned long long *cnt;
+    unsigned long long *stats;  // [0] rows passing both filters, [1] joined rows
+};
+
+__device__ __forceinline__ void star_row(const StarArgs &A, const KeyFilterDev &fb, int64_t i, long long a, long long b,
+                                         double *s_hi, double *s_lo, unsigned long long *s_cnt, unsigned &passed,
+                                         unsigned &joined) {
+    if (A.use_filters) {
+        if (!filter_pass(fb, b)) return;
+        if (!filter_pass(A.fa, a)) return;
+    }
+    passed++;
+    uint32_t ra = table_lookup(A.ta, a);
+    if (ra == kNone) return;
+    const uint32_t rb0 = table_lookup(A.tb, b);
+    if (rb0 == kNone) return;
+    const double price = (double)__ldcs(A.price + i);
+    const double disc = __ldcs(A.disc + i);
+    const double v = __dmul_rn(price, __dsub_rn(1.0, disc));
+    // Every (a, b) match pair contributes (chains are one long for unique keys).
+    for (int ca = 0; ra != kNone && ca < (1 << 20); ca++, ra = A.ta.next[ra]) {
+        for (uint32_t rb = rb0; rb != kNone; rb = A.tb.next[rb]) {
+            joined++;
+            const int g = A.group_by == 0 ? A.ta.gid[ra] : A.tb.gid[rb];
+            if (g < kMaxSmemGroups && s_hi) {
+                atomic_add_dd(s_hi + g, s_lo + g, v);
+                atomicAdd(s_cnt + g, 1ull);
+            } else {
+                atomic_add_dd(A.sum_hi + g, A.sum_lo + g, v);
+                atomicAdd(A.cnt + g, 1ull);
+            }
+        }
+    }
+}
+
+// The fused fact-side kernel: persistent CTAs stream the two key columns with
+// evict-first loads, 4 rows per thread per step.
+__global__ void __launch_bounds__(512) star_fused_kernel(StarArgs A) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int G = A.ngroups < kMaxSmemGroups ? A.ngroups : kMaxSmemGroups;
+    // The Bloom words first (16-byte aligned for the vector loads), then the
+    // group accumulators.
+    uint32_t *s_bloom = reinterpret_cast<uint32_t *>(smem);
+    double *s_hi = reinterpret_cast<double *>(smem + (size_t)A.bloom_b_smem_words * 4);
+    double *s_lo = s_hi + G;
+    unsigned long long *s_cnt = reinterpret_cast<unsigned long long *>(s_lo + G);
+    __shared__ unsigned s_passed, s_joined;
+    for (int g = threadIdx.x; g < G; g += blockDim.x) {
+        s_hi[g] = 0.0;
+        s_lo[g] = 0.0;
+        s_cnt[g] = 0;
+    }
+    KeyFilterDev fb = A.fb;
+    if (A.bloom_b_smem_words > 0) {
+        const uint4 *src = reinterpret_cast<const uint4 *>(A.fb.bloom);
+        uint4 *dst = reinterpret_cast<uint4 *>(s_bloom);
+        for (int w = threadIdx.x; w < A.bloom_b_smem_words / 4; w += blockDim.x) dst[w] = src[w];
+        fb.bloom = s_bloom;
+    }
+    if (threadIdx.x == 0) {
+        s_passed = 0;
+        s_joined = 0;
+    }
+    __syncthreads();
+    unsigned passed = 0, joined = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x * 4;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x * 4 + threadIdx.x; base < A.n; base += stride) {
+        long long a[4], b[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int64_t i = base + (int64_t)u * blockDim.x;
+            if (i < A.n) {
+                a[u] = __ldcs(A.fk_a + i);
+                b[u] = __ldcs(A.fk_b + i);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int64_t i = base + (int64_t)u * blockDim.x;
+            if (i < A.n) star_row(A, fb, i, a[u], b[u], s_hi, s_lo, s_cnt, passed, joined);
+        }
+    }
+    atomicAdd(&s_passed, passed);
+    atomicAdd(&s_joined, joined);
+    __syncthreads();
+    for (int g = threadIdx.x; g < G; g += blockDim.x)
+        if (s_cnt[g]) {
+            atomic_add_dd2(A.sum_hi + g, A.sum_lo + g, s_hi[g], s_lo[g]);
+            atomicAdd(A.cnt + g, s_cnt[g]);
+        }
+    if (threadIdx.x == 0) {
+        atomicAdd(A.stats, (unsigned long long)s_passed);
+        atomicAdd(A.stats + 1, (unsigned long long)s_joined);
+    }
+}
+
+// Rows of a dimension with pred == value: their key and attribute, compacted
+// (the filter below the join build).
+__global__ void __launch_bounds__(256) dim_select_kernel(const long long *key, const int32_t *pred, const int32_t *attr,
+                                                         int64_t n, int32_t value, long long *okey, int32_t *oattr,
+                                                         unsigned long long *count) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += stride) {
+        const int64_t i = base + threadIdx.x;
+        const bool ok = i < n && pred[i] == value;
+        unsigned long long pos;
+        const unsigned ballot = __ballot_sync(0xFFFFFFFFu, ok);
+        unsigned long long first = 0;
+        if (lane_id() == 0 && ballot) first = atomicAdd(count, (unsigned long long)__popc(ballot));
+        first = __shfl_sync(0xFFFFFFFFu, first, 0);
+        pos = first + __popc(ballot & lanemask_lt());
+        if (ok) {
+            okey[pos] = key[i];
+            oattr[pos] = attr[i];
+        }
+    }
+}
+
+// Dense group ids of the attribute values: one small open-addressing table.
+__global__ void attr_gid_kernel(const int32_t *attr, int64_t n, long long *tkeys, int32_t *tgid, uint64_t mask,
+                                int32_t *gid_out, int32_t *gattr, unsigned int *ngroups, uint32_t *status) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const long long k = attr[i];
+        uint64_t pos = hash_word((uint64_t)k) & mask;
+        int32_t g = -1;
+        for (uint64_t p = 0; p <= mask; p++) {
+            const long long cur = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(tkeys + pos),
+                                                       (unsigned long long)kAttrEmpty, (unsigned long long)k);
+            if (cur == kAttrEmpty) {
+                g = (int32_t)atomicAdd(ngroups, 1u);
+                gattr[g] = (int32_t)k;
+                __threadfence();
+                atomicExch(tgid + pos, g);
+                break;
+            }
+            if (cur == k) {
+                for (int it = 0; it < (1 << 22); it++) {
+                    g = *reinterpret_cast<volatile int32_t *>(tgid + pos);
+                    if (g >= 0) break;
+                    __nanosleep(20);
+                }
+                if (g < 0) atomicOr(status, ST_TIMEOUT);
+                break;
+            }
+            pos = (pos + 1) & mask;
+        }
+        gid_out[i] = g < 0 ? 0 : g;
+    }
+}
+
+// Plain form helpers: the scan's row stage keeps rows passing both filters.
+__global__ void __launch_bounds__(256) compact4_kernel(const uint32_t *pass_a, const uint32_t *pass_b, int64_t n,
+                                                       const long long *c0, const long long *c1, const long long *c2,
+                                                       const double *c3, long long *o0, long long *o1, long long *o2,
+                                                       double *o3, unsigned long long *count) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += stride) {
+        const int64_t i = base + threadIdx.x;
+        bool ok = false;
+        if (i < n) ok = ((pass_a[i >> 5] & pass_b[i >> 5]) >> (i & 31)) & 1u;
+        const unsigned ballot = __ballot_sync(0xFFFFFFFFu, ok);
+        unsigned long long first = 0;
+        if (lane_id() == 0 && ballot) first = atomicAdd(count, (unsigned long long)__popc(ballot));
+        first = __shfl_sync(0xFFFFFFFFu, first, 0);
+        const unsigned long long pos = first + __popc(ballot & lanemask_lt());
+        if (ok) {
+            o0[pos] = c0[i];
+            o1[pos] = c1[i];
+            o2[pos] = c2[i];
+            o3[pos] = c3[i];
+        }
+    }
+}
+
+// Plain form: the projection price * (1 - discount).
+__global__ void project_kernel(const long long *price, const double *disc, int64_t n, double *out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = __dmul_rn((double)price[i], __dsub_rn(1.0, disc[i]));
+}
+
+}  // namespace
+
+class StarPipeline {
+  public:
+    StarPipeline(Runtime *rt, const krv_star_spec &s) : rt_(rt), spec_(s) {
+        if (s.group_by != 0 && s.group_by != 1) fail(KRV_INVALID_ARGUMENT, "group_by is 0 (dim a) or 1 (dim b)");
+        if (s.mode != KRV_STAR_FUSED && s.mode != KRV_STAR_PLAIN) fail(KRV_INVALID_ARGUMENT, "unknown star mode");
+    }
+
+    struct Dim {
+        std::unique_ptr<HashJoin> join;  // inner join on key, build columns (key, attr, gid)
+        DBuf key, attr, gid;
+        int64_t rows = 0;
+    };
+
+    void build_dim(const DevBatch &d, int32_t value, Dim &out) {
+        const int c_key = spec_.dim_key, c_pred = spec_.dim_pred, c_attr = spec_.dim_attr;
+        const int nc = (int)d.cols.size();
+        if (c_key < 0 || c_key >= nc || c_pred < 0 || c_pred >= nc || c_attr < 0 || c_attr >= nc)
+            fail(KRV_INVALID_ARGUMENT, "dimension column out of range");
+        if (d.cols[c_key].type.id != Type::I64 || d.cols[c_pred].type.id != Type::I32 ||
+            d.cols[c_attr].type.id != Type::I32)
+            fail(KRV_UNSUPPORTED, "star dimension columns are (int64 key, int32 pred, int32 attr)");
+        if (d.cols[c_key].valid || d.cols[c_pred].valid || d.cols[c_attr].valid)
+            fail(KRV_UNSUPPORTED, "star dimension columns without NULLs");
+        const int64_t n = d.rows;
+        out.key = DBuf(rt_, (size_t)std::max<int64_t>(n, 1) * 8);
+        out.attr = DBuf(rt_, (size_t)std::max<int64_t>(n, 1) * 4);
+        DBuf cnt(rt_, 8);
+        KRV_CUDA(cudaMemsetAsync(cnt.get(), 0, 8, rt_->stream));
+        if (n > 0) {
+            dim_select_kernel<<<grid_for(rt_, n, 256, 8), 256, 0, rt_->stream>>>(
+                static_cast<const long long *>(d.cols[c_key].data), static_cast<const int32_t *>(d.cols[c_pred].data),
+                static_cast<const int32_t *>(d.cols[c_attr].data), n, value, out.key.as<long long>(),
+                out.attr.as<int32_t>(), cnt.as<unsigned long long>());
+            rt_->launches++;
+            check_launch("dim_select_kernel");
+        }
+        out.rows = (int64_t)read_scalar<unsigned long long>(rt_, cnt.get());
+        // Dense group ids of the attribute (shared by both dimensions).
+        out.gid = DBuf(rt_, (size_t)std::max<int64_t>(out.rows, 1) * 4);
+        if (out.rows > 0) {
+            attr_gid_kernel<<<grid_for(rt_, out.rows, 256, 8), 256, 0, rt_->stream>>>(
+                out.attr.as<int32_t>(), out.rows, gkeys_.as<long long>(), gtab_.as<int32_t>(), gmask_, out.gid.as<int32_t>(),
+                gattr_.as<int32_t>(), ngroups_.as<unsigned int>(), status_word(rt_));
+            rt_->launches++;
+            check_launch("attr_gid_kernel");
+        }
+        DevBatch b;
+        b.rows = out.rows;
+        DevCol k;
+        k.type = DType{Type::I64, 0, 0};
+        k.length = out.rows;
+        k.data = out.key.get();
+        k.name = "key";
+        k.nullable = false;
+        DevCol a = k;
+        a.type = DType{Type::I32, 0, 0};
+        a.data = out.attr.get();
+        a.name = "attr";
+        DevCol g = a;
+        g.data = out.gid.get();
+        g.name = "gid";
+        b.cols = {k, a, g};
+        krv_join_spec js;
+        krv_join_spec_init(&js);
+        js.join_type = KRV_JOIN_INNER;
+        js.n_keys = 1;
+        js.probe_keys[0] = 0;
+        js.build_keys[0] = 0;
+        js.runtime_filter = spec_.use_filters;
+        out.join.reset(new HashJoin(rt_, js));
+        out.join->build_push(b);
+        out.join->build_finish();
+    }
+
+    void build(const DevBatch &a, const DevBatch &b) {
+        DeviceGuard g(rt_);
+        // Attribute -> dense group id table (at most 2^16 distinct values).
+        gmask_ = (1u << 16) - 1;
+        gkeys_ = DBuf(rt_, (gmask_ + 1) * 8);
+        gtab_ = DBuf(rt_, (gmask_ + 1) * 4);
+        gattr_ = DBuf(rt_, (gmask_ + 1) * 4);
+        ngroups_ = DBuf(rt_, 8);
+        KRV_CUDA(cudaMemsetAsync(gkeys_.get(), 0x80, (gmask_ + 1) * 8, rt_->stream));
+        KRV_CUDA(cudaMemsetAsync(gtab_.get(), 0xFF, (gmask_ + 1) * 4, rt_->stream));
+        KRV_CUDA(cudaMemsetAsync(ngroups_.get(), 0, 8, rt_->stream));
+        clear_status(rt_);
+        dims_[0] = Dim{};
+        dims_[1] = Dim{};
+        // Only the grouping dimension's attribute names groups; the other's
+        // ids are never read.
+        build_dim(a, spec_.pred_a, dims_[0]);
+        build_dim(b, spec_.pred_b, dims_[1]);
+        if (take_status(rt_) & ST_TIMEOUT) fail(KRV_TIMEOUT, "star build: a wait for a group id gave up");
+        ngroups_host_ = (int)read_scalar<unsigned int>(rt_, ngroups_.get());
+        if (ngroups_host_ > (int)gmask_ / 2) fail(KRV_UNSUPPORTED, "more than 32768 distinct attribute values");
+        const size_t G = (size_t)std::max(ngroups_host_, 1);
+        sum_hi_ = DBuf(rt_, G * 8);
+        sum_lo_ = DBuf(rt_, G * 8);
+        cnt_ = DBuf(rt_, G * 8);
+        stats_ = DBuf(rt_, 16);
+        reset();
+        counters_.dim_a_keys = dims_[0].join->counters().build_keys;
+        counters_.dim_b_keys = dims_[1].join->counters().build_keys;
+        auto fa = dims_[0].join->key_filter(), fb = dims_[1].join->key_filter();
+        counters_.filter_a_form = fa ? fa->info.form : -1;
+        counters_.filter_b_form = fb ? fb->info.form : -1;
+        counters_.filter_a_bytes = fa ? fa->info.bloom_bytes : 0;
+        counters_.filter_b_bytes = fb ? fb->info.bloom_bytes : 0;
+        built_ = true;
+    }
+
+    void reset() {
+        const size_t G = (size_t)std::max(ngroups_host_, 1);
+        KRV_CUDA(cudaMemsetAsync(sum_hi_.get(), 0, G * 8, rt_->stream));
+        KRV_CUDA(cudaMemsetAsync(sum_lo_.get(), 0, G * 8, rt_->stream));
+        KRV_CUDA(cudaMemsetAsync(cnt_.get(), 0, G * 8, rt_->stream));
+        KRV_CUDA(cudaMemsetAsync(stats_.get(), 0, 16, rt_->stream));
+        counters_.fact_rows = 0;
+        if (plain_agg_) {
+            agg_destroy(plain_agg_);
+            plain_agg_ = nullptr;
+        }
+    }
+
+    void check_fact(const DevBatch &f) const {
+        const int nc = (int)f.cols.size();
+        const int c[4] = {spec_.fact_fk_a, spec_.fact_fk_b, spec_.fact_price, spec_.fact_discount};
+        const Type t[4] = {Type::I64, Type::I64, Type::I64, Type::F64};
+        for (int i = 0; i < 4; i++) {
+            if (c[i] < 0 || c[i] >= nc) fail(KRV_INVALID_ARGUMENT, "fact column out of range");
+            if (f.cols[c[i]].type.id != t[i])
+                fail(KRV_UNSUPPORTED, "star fact columns are (int64 fk_a, int64 fk_b, int64 price, float64 discount)");
+            if (f.cols[c[i]].valid) fail(KRV_UNSUPPORTED, "star fact columns without NULLs");
+        }
+    }
+
+    TableView view(const Dim &d) const {
+        auto t = d.join->table_dev();
+        return TableView{t.slots, t.mask, t.next, t.seed, static_cast<const long long *>(d.join->arena().cols[0].data),
+                         static_cast<const int32_t *>(d.join->arena().cols[2].data)};
+    }
+
+    void probe_fused(const DevBatch &f) {
+        StarArgs A{};
+        A.fk_a = static_cast<const long long *>(f.cols[spec_.fact_fk_a].data);
+        A.fk_b = static_cast<const long long *>(f.cols[spec_.fact_fk_b].data);
+        A.price = static_cast<const long long *>(f.cols[spec_.fact_price].data);
+        A.disc = static_cast<const double *>(f.cols[spec_.fact_discount].data);
+        A.n = f.rows;
+        auto fa = dims_[0].join->key_filter(), fb = dims_[1].join->key_filter();
+        A.use_filters = spec_.use_filters && fa && fb;
+        if (A.use_filters) {
+            A.fa = key_filter_dev(*fa);
+            A.fb = key_filter_dev(*fb);
+        }
+        A.group_by = spec_.group_by;
+        A.ta = view(dims_[0]);
+        A.tb = view(dims_[1]);
+        A.ngroups = ngroups_host_;
+        A.sum_hi = sum_hi_.as<double>();
+        A.sum_lo = sum_lo_.as<double>();
+        A.cnt = cnt_.as<unsigned long long>();
+        A.stats = stats_.as<unsigned long long>();
+        const int G = std::min(ngroups_host_, kMaxSmemGroups);
+        size_t smem = (size_t)G * 24;
+        smem = (smem + 15) & ~size_t(15);
+        A.bloom_b_smem_words = 0;
+        if (A.use_filters && A.fb.form == KRV_FILTER_BLOOM && fb->info.bloom_bytes <= 96 * 1024) {
+            A.bloom_b_smem_words = (int)(fb->info.bloom_bytes / 4);
+            smem += (size_t)fb->info.bloom_bytes;
+        }
+        KRV_CUDA(cudaFuncSetAttribute(star_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, star_fused_kernel, 512, smem));
+        per_sm = std::max(1, std::min(per_sm, 4));
+        const int grid = (int)std::min<int64_t>((int64_t)rt_->sm_count * per_sm, ceil_div(std::max<int64_t>(f.rows, 1), 512 * 4));
+        if (f.rows > 0) {
+            star_fused_kernel<<<grid, 512, smem, rt_->stream>>>(A);
+            rt_->launches++;
+            check_launch("star_fused_kernel");
+        }
+    }
+
+    void probe_plain(const DevBatch &f) {
+        auto fa = dims_[0].join->key_filter(), fb = dims_[1].join->key_filter();
+        const int64_t n = f.rows;
+        const DevCol &ca = f.cols[spec_.fact_fk_a], &cb = f.cols[spec_.fact_fk_b];
+        const DevCol &cp = f.cols[spec_.fact_price], &cd = f.cols[spec_.fact_discount];
+        // 1-2. the row stage: both runtime filters, then compaction
+        DevBatch kept;
+        if (spec_.use_filters && fa && fb) {
+            DevCol pb = evaluate_key_filter(*fb, cb);
+            DevCol pa = evaluate_key_filter(*fa, ca);
+            DevCol o0 = make_col(rt_, ca.type, n, false, "fk_a"), o1 = make_col(rt_, cb.type, n, false, "fk_b");
+            DevCol o2 = make_col(rt_, cp.type, n, false, "price"), o3 = make_col(rt_, cd.type, n, false, "discount");
+            DBuf cnt(rt_, 8);
+            KRV_CUDA(cudaMemsetAsync(cnt.get(), 0, 8, rt_->stream));
+            if (n > 0) {
+                compact4_kernel<<<grid_for(rt_, n, 256, 8), 256, 0, rt_->stream>>>(
+                    (const uint32_t *)pa.data, (const uint32_t *)pb.data, n, (const long long *)ca.data,
+                    (const long long *)cb.data, (const long long *)cp.data, (const double *)cd.data, (long long *)o0.data,
+                    (long long *)o1.data, (long long *)o2.data, (double *)o3.data, cnt.as<unsigned long long>());
+                rt_->launches++;
+                check_launch("compact4_kernel");
+            }
+            kept.rows = (int64_t)read_scalar<unsigned long long>(rt_, cnt.get());
+            kept.cols = {o0, o1, o2, o3};
+            for (auto &c : kept.cols) c.length = kept.rows;
+            counters_.passed_filters += kept.rows;
+        } else {
+            kept.rows = n;
+            kept.cols = {ca, cb, cp, cd};
+        }
+        // 3. fact' JOIN dim_a -> (fk_b, price, discount, a.gid)
+        krv_join_spec js;
+        krv_join_spec_init(&js);
+        js.join_type = KRV_JOIN_INNER;
+        js.n_keys = 1;
+        js.probe_keys[0] = 0;
+        js.n_probe_out = 3;
+        js.probe_out[0] = 1;
+        js.probe_out[1] = 2;
+        js.probe_out[2] = 3;
+        js.n_build_out = 1;
+        js.build_out[0] = 2;
+        DevBatch j1 = probe_with(*dims_[0].join, kept, js);
+        // 4. JOIN dim_b -> (price, discount, a.gid, b.gid)
+        js.probe_keys[0] = 0;
+        js.probe_out[0] = 1;
+        js.probe_out[1] = 2;
+        js.probe_out[2] = 3;
+        DevBatch j2 = probe_with(*dims_[1].join, j1, js);
+        counters_.joined_rows += j2.rows;
+        // 5. projection: (gid, price * (1 - discount))
+        DevCol val = make_col(rt_, DType{Type::F64, 0, 0}, j2.rows, false, "value");
+        if (j2.rows > 0) {
+            project_kernel<<<grid_for(rt_, j2.rows, 256, 8), 256, 0, rt_->stream>>>(
+                (const long long *)j2.cols[0].data, (const double *)j2.cols[1].data, j2.rows, (double *)val.data);
+            rt_->launches++;
+            check_launch("project_kernel");
+        }
+        DevBatch proj;
+        proj.rows = j2.rows;
+        proj.cols = {j2.cols[spec_.group_by == 0 ? 2 : 3], val};
+        // 6. GROUP BY gid: SUM(value), COUNT(*)
+        if (!plain_agg_) {
+            krv_agg_spec as;
+            krv_agg_spec_init(&as);
+            as.n_group_by = 1;
+            as.group_by[0] = 0;
+            as.n_aggregates = 2;
+            as.aggregates[0] = krv_agg_expr{KRV_AGG_SUM, 1};
+            as.aggregates[1] = krv_agg_expr{KRV_AGG_COUNT_STAR, 0};
+            as.expected_groups = std::max(ngroups_host_, 1);
+            as.mode = KRV_AGG_MODE_GLOBAL;
+            plain_agg_ = make_aggregate(rt_, as);
+        }
+        if (proj.rows > 0) agg_push(plain_agg_, proj);
+    }
+
+    // A probe of `in` against the built join `j` with another projection.
+    DevBatch probe_with(HashJoin &j, const DevBatch &in, const krv_join_spec &proj) {
+        const krv_join_spec saved = j.spec();
+        j.set_probe_shape(proj);
+        DevBatch out = j.probe(in);
+        j.set_probe_shape(saved);
+        return out;
+    }
+
+    void probe(const DevBatch &f) {
+        if (!built_) fail(KRV_INVALID_ARGUMENT, "star probe before build");
+        DeviceGuard g(rt_);
+        check_fact(f);
+        counters_.fact_rows += f.rows;
+        if (spec_.mode == KRV_STAR_FUSED) probe_fused(f);
+        else probe_plain(f);
+    }
+
+    DevBatch result() {
+        DeviceGuard g(rt_);
+        DevBatch out;
+        const int G = std::max(ngroups_host_, 0);
+        std::vector<double> hi(G), lo(G);
+        std::vector<unsigned long long> cnt(G);
+        std::vector<int32_t> gattr(G);
+        if (G > 0) {
+            KRV_CUDA(cudaMemcpyAsync(gattr.data(), gattr_.get(), (size_t)G * 4, cudaMemcpyDeviceToHost, rt_->stream));
+        }
+        if (spec_.mode == KRV_STAR_FUSED) {
+            if (G > 0) {
+                KRV_CUDA(cudaMemcpyAsync(hi.data(), sum_hi_.get(), (size_t)G * 8, cudaMemcpyDeviceToHost, rt_->stream));
+                KRV_CUDA(cudaMemcpyAsync(lo.data(), sum_lo_.get(), (size_t)G * 8, cudaMemcpyDeviceToHost, rt_->stream));
+                KRV_CUDA(cudaMemcpyAsync(cnt.data(), cnt_.get(), (size_t)G * 8, cudaMemcpyDeviceToHost, rt_->stream));
+            }
+            unsigned long long st[2];
+            KRV_CUDA(cudaMemcpyAsync(st, stats_.get(), 16, cudaMemcpyDeviceToHost, rt_->stream));
+            KRV_CUDA(cudaStreamSynchronize(rt_->stream));
+            counters_.passed_filters = (int64_t)st[0];
+            counters_.joined_rows = (int64_t)st[1];
+            // The groups with rows, in group-id order: (attr, hi + lo), the
+            // double-double sum rounded once.
+            std::vector<int32_t> oa;
+            std::vector<double> os;
+            for (int g = 0; g < G; g++)
+                if (cnt[g]) {
+                    oa.push_back(gattr[g]);
+                    os.push_back(std::isfinite(hi[g]) ? hi[g] + lo[g] : hi[g]);
+                }
+            return host_result(oa, os);
+        }
+        KRV_CUDA(cudaStreamSynchronize(rt_->stream));
+        std::vector<int32_t> oa;
+        std::vector<double> os;
+        if (plain_agg_) {
+            DevBatch r = agg_result(plain_agg_);
+            const int64_t m = r.rows;
+            std::vector<int32_t> gid(m);
+            std::vector<double> sum(m);
+            if (m > 0) {
+                KRV_CUDA(cudaMemcpyAsync(gid.data(), r.cols[0].data, (size_t)m * 4, cudaMemcpyDeviceToHost, rt_->stream));
+                KRV_CUDA(cudaMemcpyAsync(sum.data(), r.cols[1].data, (size_t)m * 8, cudaMemcpyDeviceToHost, rt_->stream));
+                KRV_CUDA(cudaStreamSynchronize(rt_->stream));
+            }
+            for (int64_t i = 0; i < m; i++) {
+                oa.push_back(gattr[gid[i]]);
+                os.push_back(sum[i]);
+            }
+        }
+        return host_result(oa, os);
+    }
+
+    DevBatch host_result(const std::vector<int32_t> &attr, const std::vector<double> &sum) {
+        DevBatch out;
+        const int64_t m = (int64_t)attr.size();
+        DevCol a = make_col(rt_, DType{Type::I32, 0, 0}, m, false, "attr");
+        DevCol s = make_col(rt_, DType{Type::F64, 0, 0}, m, false, "sum");
+        if (m > 0) {
+            KRV_CUDA(cudaMemcpyAsync(const_cast<void *>(a.data), attr.data(), (size_t)m * 4, cudaMemcpyHostToDevice, rt_->stream));
+            KRV_CUDA(cudaMemcpyAsync(const_cast<void *>(s.data), sum.data(), (size_t)m * 8, cudaMemcpyHostToDevice, rt_->stream));
+            KRV_CUDA(cudaStreamSynchronize(rt_->stream));
+        }
+        out.rows = m;
+        out.cols = {a, s};
+        return out;
+    }
+
+    krv_star_counters counters() const { return counters_; }
+
+  private:
+    Runtime *rt_;
+    krv_star_spec spec_;
+    Dim dims_[2];
+    DBuf gkeys_, gtab_, gattr_, ngroups_;
+    uint32_t gmask_ = 0;
+    int ngroups_host_ = 0;
+    DBuf sum_hi_, sum_lo_, cnt_, stats_;
+    HashAggregate *plain_agg_ = nullptr;
+    bool built_ = false;
+    krv_star_counters counters_{};
+
+  public:
+    ~StarPipeline() {
+        if (plain_agg_) agg_destroy(plain_agg_);
+    }
+};
+
+StarPipeline *make_star(Runtime *rt, const krv_star_spec &spec) { return new StarPipeline(rt, spec); }
+void star_build(StarPipeline *s, const DevBatch &a, const DevBatch &b) { s->build(a, b); }
+void star_probe(StarPipeline *s, const DevBatch &fact) { s->probe(fact); }
+DevBatch star_result(StarPipeline *s) { return s->result(); }
+void star_reset(StarPipeline *s) { s->reset(); }
+krv_star_counters star_counters(const StarPipeline *s) { return s->counters(); }
+void star_destroy(StarPipeline *s) { delete s; }
+
+}  // namespace krv

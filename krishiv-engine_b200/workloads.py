@@ -1,0 +1,93 @@
+"""Synthetic workloads of the benchmarks, generated on the device with the
+library's counter-based generators (krv_gen_fill), so every run and every
+row range is reproducible and the CPU oracle can regenerate any sample.
+
+Shapes (rows at scale 1.0):
+  star:   fact 300,000,000 {fk_a uniform [0, 20M), fk_b uniform [0, 1M),
+          price int64 uniform [1,000, 10,000,000], discount float64 uniform
+          [0, 0.1)}; dim_a 20,000,000 and dim_b 1,000,000 rows {key: a
+          permutation of [0, rows), pred int32 uniform [0, 20) (pred = 7
+          selects 5%), attr int32 uniform [0, 25)}.
+  join:   build 1,000,000 {k: a permutation of [0, 1M), v int64 uniform};
+          probe 10,000,000 {k uniform [0, 2M) (about half match), w int32}.
+  agg:    100,000,000 rows {k: Zipf(1.1) over 1,000,000 values, dec
+          decimal(15,2) unscaled uniform [100, 1e7], f float64 uniform [0, 1),
+          q int32 uniform [1, 50]; 2% NULLs per value column}.
+"""
+from __future__ import annotations
+
+import importlib
+from dataclasses import dataclass
+
+STAR_SEED = 0x4B52560003
+JOIN_SEED = 0x4B52560001
+AGG_SEED = 0x4B52560002
+PRED_VALUE = 7
+
+
+def _kb():
+    return importlib.import_module("krishiv-engine_b200")
+
+
+def _col(rt, n, dtype, kind, seed, column, **kw):
+    import torch
+    t = torch.empty(n, dtype=dtype, device=f"cuda:{rt.device}")
+    valid = None
+    if kw.get("null_fraction", 0.0) > 0:
+        valid = torch.empty((n + 31) // 32 * 4, dtype=torch.uint8, device=t.device)
+    _kb().gen_fill(rt, t, kind, seed, column, valid=valid, **kw)
+    return t, valid
+
+
+@dataclass
+class StarData:
+    fact: list      # [(name, tensor, valid)]
+    dim_a: list
+    dim_b: list
+    fact_rows: int
+    dim_a_rows: int
+    dim_b_rows: int
+
+
+def star(rt, scale: float = 1.0, seed: int = STAR_SEED, fact_row0: int = 0) -> StarData:
+    """The star-join inputs; `fact_row0` selects which fact rows (a shard of
+    the fact stream for one of several devices)."""
+    import torch
+    kb = _kb()
+    nf, na, nb = int(300_000_000 * scale), int(20_000_000 * scale), int(1_000_000 * scale)
+    r0 = dict(row0=fact_row0)
+    fk_a, _ = _col(rt, nf, torch.int64, kb.GEN_UNIFORM_I64, seed, 1, lo=0, hi=na - 1, **r0)
+    fk_b, _ = _col(rt, nf, torch.int64, kb.GEN_UNIFORM_I64, seed, 2, lo=0, hi=nb - 1, **r0)
+    price, _ = _col(rt, nf, torch.int64, kb.GEN_UNIFORM_I64, seed, 3, lo=1000, hi=10_000_000, **r0)
+    disc, _ = _col(rt, nf, torch.float64, kb.GEN_UNIT_F64, seed, 4, x0=0.0, x1=0.1, **r0)
+    dims = []
+    for base, n in ((10, na), (20, nb)):
+        key, _ = _col(rt, n, torch.int64, kb.GEN_PERMUTATION, seed + base, base + 1, lo=0, hi=n)
+        pred, _ = _col(rt, n, torch.int32, kb.GEN_UNIFORM_I32, seed, base + 2, lo=0, hi=19)
+        attr, _ = _col(rt, n, torch.int32, kb.GEN_UNIFORM_I32, seed, base + 3, lo=0, hi=24)
+        dims.append([("key", key, None), ("pred", pred, None), ("attr", attr, None)])
+    fact = [("fk_a", fk_a, None), ("fk_b", fk_b, None), ("price", price, None), ("discount", disc, None)]
+    return StarData(fact, dims[0], dims[1], nf, na, nb)
+
+
+def join(rt, scale: float = 1.0, seed: int = JOIN_SEED):
+    import torch
+    kb = _kb()
+    nb, np_ = int(1_000_000 * scale), int(10_000_000 * scale)
+    bk, _ = _col(rt, nb, torch.int64, kb.GEN_PERMUTATION, seed, 1, lo=0, hi=nb)
+    bv, _ = _col(rt, nb, torch.int64, kb.GEN_UNIFORM_I64, seed, 2, lo=-(2**62), hi=2**62)
+    pk, _ = _col(rt, np_, torch.int64, kb.GEN_UNIFORM_I64, seed, 3, lo=0, hi=2 * nb - 1)
+    pw, _ = _col(rt, np_, torch.int32, kb.GEN_UNIFORM_I32, seed, 4, lo=-(2**31), hi=2**31 - 1)
+    return [("k", bk, None), ("v", bv, None)], [("k", pk, None), ("w", pw, None)]
+
+
+def agg(rt, scale: float = 1.0, seed: int = AGG_SEED, domain: int = 1_000_000):
+    import pyarrow as pa
+    import torch
+    kb = _kb()
+    n = int(100_000_000 * scale)
+    k, _ = _col(rt, n, torch.int64, kb.GEN_ZIPF, seed, 1, lo=0, hi=domain, x0=1.1)
+    dec, dv = _col(rt, n, torch.int64, kb.GEN_UNIFORM_I64, seed, 2, lo=100, hi=10_000_000, null_fraction=0.02)
+    f, fv = _col(rt, n, torch.float64, kb.GEN_UNIT_F64, seed, 3, x0=0.0, x1=1.0, null_fraction=0.02)
+    q, qv = _col(rt, n, torch.int32, kb.GEN_UNIFORM_I32, seed, 4, lo=1, hi=50, null_fraction=0.02)
+    return [("k", k, None), ("dec", dec, dv, pa.decimal64(15, 2)), ("f", f, fv), ("q", q, qv)]

@@ -1,0 +1,60 @@
+"""The C-ABI library without a GPU: it loads, exports every function that
+include/krv_gpu.h declares, the Python binding covers each, and calls that
+need a device fail with a status (never a crash) when none is present."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    text = open(os.path.join(ROOT, "include", "krv_gpu.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(krv_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    names = declared()
+    for must in ("krv_join_create", "krv_join_build_push", "krv_join_build_finish", "krv_join_probe",
+                 "krv_join_finish", "krv_agg_create", "krv_agg_push", "krv_agg_finish", "krv_agg_next_output",
+                 "krv_key_filter_build", "krv_key_filter_evaluate", "krv_star_probe", "krv_last_error"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(kb):
+    lib = C.CDLL(kb.LIB_PATH)
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_every_symbol(kb):
+    assert sorted(kb.exported_names()) == declared()
+    kb.lib()  # every signature binds
+
+
+def test_spec_initializers(kb):
+    s = kb.join_spec("left_outer", probe_keys=(0, 1), build_keys=(2, 3), null_safe=[0, 1])
+    assert s.join_type == kb.LEFT_OUTER and s.n_keys == 2 and s.build_keys[1] == 3 and s.null_safe[1] == 1
+    assert s.n_probe_out == -1 and s.n_build_out == -1
+    a = kb.agg_spec(0, [("sum", 1), ("count_star", 0)])
+    assert a.n_aggregates == 2 and a.aggregates[0].function == kb.SUM
+    o = kb.key_filter_options()
+    assert (o.max_values, o.exact_max_values, o.bloom_max_items, o.bloom_max_bytes) == (50, 4096, 4000000, 8 << 20)
+    assert (o.bloom_fpp, o.bloom_max_fpp) == (0.01, 0.05)
+
+
+def test_no_device_is_an_error_status(kb):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    with pytest.raises(kb.KrvError) as e:
+        kb.Runtime(0)
+    assert e.value.status in (kb.CUDA_ERROR, kb.INVALID_ARGUMENT)
+    assert kb.lib().krv_last_error()
+
+
+def test_version(kb):
+    assert b"sm_100a" in kb.lib().krv_version()
