@@ -307,6 +307,7 @@ typedef struct {
     int64_t dim_a_keys, dim_b_keys;
     int32_t filter_a_form, filter_b_form;
     int64_t filter_a_bytes, filter_b_bytes;
+    int64_t fk_a_sectors;      /* 32-byte sectors of fk_a the fused kernel read */
 } krv_star_counters;
 krv_status krv_star_create(krv_runtime *rt, const krv_star_spec *spec, krv_star **out);
 krv_status krv_star_build(krv_star *s, const struct ArrowArray *dim_a,

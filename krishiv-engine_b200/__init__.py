@@ -131,7 +131,8 @@ class StarSpec(C.Structure):
 class StarCounters(C.Structure):
     _fields_ = [("fact_rows", C.c_int64), ("passed_filters", C.c_int64), ("joined_rows", C.c_int64),
                 ("dim_a_keys", C.c_int64), ("dim_b_keys", C.c_int64), ("filter_a_form", C.c_int32),
-                ("filter_b_form", C.c_int32), ("filter_a_bytes", C.c_int64), ("filter_b_bytes", C.c_int64)]
+                ("filter_b_form", C.c_int32), ("filter_a_bytes", C.c_int64), ("filter_b_bytes", C.c_int64),
+                ("fk_a_sectors", C.c_int64)]
 
 
 class GenSpec(C.Structure):
@@ -390,6 +391,20 @@ class Runtime:
         check(lib().krv_runtime_create(device, budget_bytes, stream, C.byref(h)))
         self.h = h
         self.device = device
+
+    @classmethod
+    def on_torch_stream(cls, device: int = 0, budget_bytes: int = 0, stream=None) -> "Runtime":
+        """A runtime on a torch CUDA stream that is made current, so torch
+        tensors, events and the library's kernels are ordered on one stream.
+        (The legacy default stream has the handle 0, which the C ABI reads as
+        "create a stream", hence a dedicated stream.)"""
+        import torch
+        torch.cuda.set_device(device)
+        s = stream if stream is not None else torch.cuda.Stream(device=device)
+        torch.cuda.set_stream(s)
+        r = cls(device, budget_bytes, s.cuda_stream)
+        r.torch_stream = s
+        return r
 
     def synchronize(self):
         check(lib().krv_runtime_synchronize(self.h))

@@ -107,6 +107,9 @@ __global__ void __launch_bounds__(256) stats_kernel(const int64_t *keys, const u
         }
         uint64_t pos = hash_word((uint64_t)k) & mask;
         for (uint64_t p = 0; p <= mask; p++) {
+            // Past the exact forms' capacity the set is abandoned: stop at once
+            // (thousands of concurrent inserts may have filled it).
+            if (*(volatile unsigned int *)&st->overflow) break;
             const unsigned long long s = __ldcg(set + pos);
             if (s == (unsigned long long)k) break;
             if (s == (unsigned long long)kEmptyKey) {
@@ -172,6 +175,8 @@ __global__ void __launch_bounds__(256) evaluate_kernel(KeyFilterDev f, const int
 }
 }  // namespace
 
+void finish_bloom(Runtime *rt, const krv_key_filter_options &opt, const DevCol &keys, KeyFilterImpl &f);
+
 KeyFilterDev key_filter_dev(const KeyFilterImpl &f) {
     KeyFilterDev d{};
     d.form = f.info.form;
@@ -188,13 +193,30 @@ KeyFilterDev key_filter_dev(const KeyFilterImpl &f) {
 }
 
 std::shared_ptr<KeyFilterImpl> build_key_filter(Runtime *rt, const krv_key_filter_options &opt,
-                                                const DevCol &keys) {
+                                                const DevCol &keys, const KeyStats *known) {
     if (keys.type.id != Type::I64) fail(KRV_UNSUPPORTED, "key filters over int64 keys only");
     DeviceGuard g(rt);
     auto f = std::make_shared<KeyFilterImpl>();
     f->rt = rt;
     f->opt = opt;
     const uint64_t distinct_max = (uint64_t)std::max<int64_t>(opt.max_values, opt.exact_max_values);
+    if (known && (known->rows == 0 || (uint64_t)known->distinct > distinct_max)) {
+        // A join build counted the rows, distinct keys and range: no exact form
+        // can apply, so no pass over the keys is needed before the Bloom.
+        krv_key_filter_info &info = f->info;
+        info.keys = known->rows;
+        info.nulls_pass = 0;
+        if (known->rows == 0) {
+            info.form = KRV_FILTER_EMPTY;
+            return f;
+        }
+        info.has_range = 1;
+        info.lo = known->lo;
+        info.hi = known->hi;
+        info.distinct = -1;
+        finish_bloom(rt, opt, keys, *f);
+        return f;
+    }
     const uint64_t set_slots = std::max<uint64_t>(64, next_pow2(2 * (distinct_max + 1)));
     f->exact_slots = DBuf(rt, set_slots * 8);
     f->exact_mask = set_slots - 1;
@@ -240,28 +262,39 @@ std::shared_ptr<KeyFilterImpl> build_key_filter(Runtime *rt, const krv_key_filte
     }
     f->exact_slots.reset();
     info.distinct = -1;  // more than the exact forms hold
-    // bloom() (filter.rs:606-621): sized for every kept row, capped.
-    if (!opt.bloom || (uint64_t)st.rows > (uint64_t)opt.bloom_max_items) {
+    finish_bloom(rt, opt, keys, *f);
+    return f;
+}
+
+// bloom() (filter.rs:606-621): a Bloom filter sized for every kept row
+// (info.keys), capped, unless expected to pass too many false positives;
+// else the range alone.
+void finish_bloom(Runtime *rt, const krv_key_filter_options &opt, const DevCol &keys, KeyFilterImpl &f) {
+    krv_key_filter_info &info = f.info;
+    const uint64_t rows = (uint64_t)info.keys;
+    if (!opt.bloom || rows > (uint64_t)opt.bloom_max_items) {
         info.form = KRV_FILTER_RANGE;
-        return f;
+        return;
     }
-    int64_t bytes = opt.bloom_bytes > 0 ? opt.bloom_bytes : bloom_bytes_for(st.rows, opt.bloom_fpp);
+    int64_t bytes = opt.bloom_bytes > 0 ? opt.bloom_bytes : bloom_bytes_for(rows, opt.bloom_fpp);
     bytes = std::min<int64_t>(bytes, opt.bloom_max_bytes);
     bytes = std::max<int64_t>(1, ceil_div(bytes, kBlockBytes)) * kBlockBytes;  // with_bytes (bloom.rs:115-121)
-    if (bloom_expected_fpp(bytes, st.rows) > opt.bloom_max_fpp) {
+    if (bloom_expected_fpp(bytes, rows) > opt.bloom_max_fpp) {
         info.form = KRV_FILTER_RANGE;
-        return f;
+        return;
     }
-    f->bloom = DBuf(rt, (size_t)bytes);
-    KRV_CUDA(cudaMemsetAsync(f->bloom.get(), 0, (size_t)bytes, rt->stream));
-    bloom_insert_kernel<<<grid_for(rt, n, 256, 8), 256, 0, rt->stream>>>(
-        static_cast<const int64_t *>(keys.data), keys.valid, keys.valid_off, n, f->bloom.as<uint32_t>(),
-        (uint64_t)(bytes / kBlockBytes));
-    rt->launches++;
-    check_launch("bloom_insert_kernel");
+    f.bloom = DBuf(rt, (size_t)bytes);
+    KRV_CUDA(cudaMemsetAsync(f.bloom.get(), 0, (size_t)bytes, rt->stream));
+    const int64_t n = keys.length;
+    if (n > 0) {
+        bloom_insert_kernel<<<grid_for(rt, n, 256, 8), 256, 0, rt->stream>>>(
+            static_cast<const int64_t *>(keys.data), keys.valid, keys.valid_off, n, f.bloom.as<uint32_t>(),
+            (uint64_t)(bytes / kBlockBytes));
+        rt->launches++;
+        check_launch("bloom_insert_kernel");
+    }
     info.form = KRV_FILTER_BLOOM;
     info.bloom_bytes = bytes;
-    return f;
 }
 
 DevCol evaluate_key_filter(const KeyFilterImpl &f, const DevCol &keys) {

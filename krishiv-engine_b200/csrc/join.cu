@@ -98,13 +98,23 @@ template <bool FAST>
 __global__ void __launch_bounds__(256) build_kernel(KeysDev keys, int64_t n, unsigned long long *slots,
                                                     uint64_t mask, uint32_t *next, uint64_t seed,
                                                     unsigned long long *ctr, uint32_t *status) {
+    // ctr: [0] distinct keys, [1] a NULL `=` key seen, [2] min / [3] max of an
+    // int64 key (FAST), [4] indexed rows.
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    unsigned long long heads = 0, rows = 0;
+    long long lo = LLONG_MAX, hi = LLONG_MIN;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
         uint32_t nx = kNone;
         if (!matchable(keys, i)) {
             next[i] = nx;
             ctr[1] = 1;  // a NULL `=` key in the build (null-aware anti join)
             continue;
+        }
+        rows++;
+        if (FAST) {
+            const long long k = static_cast<const long long *>(keys.c[0].data)[i];
+            lo = k < lo ? k : lo;
+            hi = k > hi ? k : hi;
         }
         const uint64_t g = finalize(hash_of<FAST>(keys, i), seed);
         const unsigned long long entry = ((g >> 32) << 32) | (unsigned long long)(i + 1);
@@ -118,7 +128,7 @@ __global__ void __launch_bounds__(256) build_kernel(KeysDev keys, int64_t n, uns
             if (s == 0) {
                 const unsigned long long old = atomicCAS(slots + pos, 0ull, entry);
                 if (old == 0) {
-                    atomicAdd(ctr, 1ull);
+                    heads++;
                     break;
                 }
                 s = old;
@@ -132,6 +142,22 @@ __global__ void __launch_bounds__(256) build_kernel(KeysDev keys, int64_t n, uns
             pos = (pos + 1) & mask;
         }
         next[i] = nx;
+    }
+    // One atomic per warp and counter.
+    for (int d = 16; d > 0; d >>= 1) {
+        heads += __shfl_xor_sync(0xFFFFFFFFu, heads, d);
+        rows += __shfl_xor_sync(0xFFFFFFFFu, rows, d);
+        const long long ol = __shfl_xor_sync(0xFFFFFFFFu, lo, d), oh = __shfl_xor_sync(0xFFFFFFFFu, hi, d);
+        lo = ol < lo ? ol : lo;
+        hi = oh > hi ? oh : hi;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (heads) atomicAdd(ctr, heads);
+        if (rows) atomicAdd(ctr + 4, rows);
+        if (FAST && rows) {
+            atomicMin(reinterpret_cast<long long *>(ctr + 2), lo);
+            atomicMax(reinterpret_cast<long long *>(ctr + 3), hi);
+        }
     }
 }
 
@@ -409,13 +435,33 @@ void HashJoin::append_arena(const DevBatch &b) {
         const DType t = c.type;
         if (t.id == Type::Bool) fail(KRV_UNSUPPORTED, "boolean build columns");
         const size_t w = (size_t)t.width();
-        if (b.rows)
-            KRV_CUDA(cudaMemcpyAsync(arena_data_[i]->as<uint8_t>() + build_rows_ * w, c.data, (size_t)b.rows * w,
-                                     cudaMemcpyDeviceToDevice, rt_->stream));
-        append_bits(rt_, c.valid, c.valid_off, b.rows, arena_valid_[i]->as<uint8_t>(), build_rows_);
         if (c.valid) arena_cols_[i].nullable = true;
+        if (b.rows == 0) continue;  // an empty batch only fixes the schema
+        KRV_CUDA(cudaMemcpyAsync(arena_data_[i]->as<uint8_t>() + build_rows_ * w, c.data, (size_t)b.rows * w,
+                                 cudaMemcpyDeviceToDevice, rt_->stream));
+        append_bits(rt_, c.valid, c.valid_off, b.rows, arena_valid_[i]->as<uint8_t>(), build_rows_);
     }
     build_rows_ = need;
+}
+
+void HashJoin::build_adopt(DevBatch b) {
+    if (built_ || have_schema_) fail(KRV_INVALID_ARGUMENT, "build_adopt takes the whole build side, before any push");
+    if (b.rows > (int64_t)0xFFFFFFFEll) fail(KRV_UNSUPPORTED, "more than 2^32-2 build rows in one table");
+    for (const DevCol &c : b.cols) {
+        if (!c.hold_data || c.hold_data->get() != c.data) fail(KRV_INVALID_ARGUMENT, "build_adopt needs owned columns");
+        if (c.type.id == Type::Bool) fail(KRV_UNSUPPORTED, "boolean build columns");
+        DevCol m;
+        m.type = c.type;
+        m.name = c.name;
+        m.nullable = c.nullable || c.valid;
+        arena_cols_.push_back(m);
+        arena_data_.push_back(c.hold_data);
+        arena_valid_.push_back(c.valid && c.valid_off == 0 ? c.hold_valid : nullptr);
+        if (c.valid && (c.valid_off != 0 || !c.hold_valid)) fail(KRV_INVALID_ARGUMENT, "build_adopt needs owned bitmaps");
+    }
+    have_schema_ = true;
+    build_rows_ = b.rows;
+    arena_cap_ = b.rows;
 }
 
 void HashJoin::build_push(DevBatch b) {
@@ -451,7 +497,11 @@ void HashJoin::build_finish() {
     zero(rt_, slots_.get(), slots * 8);
     next_ = DBuf(rt_, (size_t)std::max<int64_t>(build_rows_, 1) * 4);
     counters_dev_ = DBuf(rt_, 64);
-    zero(rt_, counters_dev_.get(), 64);
+    {
+        // [0] keys, [1] NULL seen, [2] min, [3] max, [4] indexed rows, [6] longest chain
+        const unsigned long long init[8] = {0, 0, (unsigned long long)LLONG_MAX, (unsigned long long)LLONG_MIN, 0, 0, 0, 0};
+        KRV_CUDA(cudaMemcpyAsync(counters_dev_.get(), init, 64, cudaMemcpyHostToDevice, rt_->stream));
+    }
     const int jt = spec_.join_type;
     const bool preserved = jt == KRV_JOIN_RIGHT_SEMI || jt == KRV_JOIN_RIGHT_ANTI || jt == KRV_JOIN_RIGHT_OUTER ||
                            jt == KRV_JOIN_FULL_OUTER;
@@ -475,9 +525,9 @@ void HashJoin::build_finish() {
         rt_->launches++;
         check_launch("build_kernel");
     }
-    unsigned long long host_ctr[2];
-    KRV_CUDA(cudaMemcpyAsync(host_ctr, counters_dev_.get(), 16, cudaMemcpyDeviceToHost, rt_->stream));
-    const uint32_t st = take_status(rt_);
+    unsigned long long host_ctr[8];
+    KRV_CUDA(cudaMemcpyAsync(host_ctr, counters_dev_.get(), 64, cudaMemcpyDeviceToHost, rt_->stream));
+    const uint32_t st = take_status(rt_);  // synchronizes: host_ctr is ready too
     if (st & ST_CAPACITY) fail(KRV_INTERNAL, "join table full");
     counters_.build_rows = build_rows_;
     counters_.build_keys = (int64_t)host_ctr[0];
@@ -489,7 +539,11 @@ void HashJoin::build_finish() {
         if (key.type.id == Type::I64) {
             krv_key_filter_options o;
             krv_key_filter_options_default(&o);
-            filter_ = build_key_filter(rt_, o, key);
+            // The build already counted the kept rows, the distinct keys and
+            // their range: the filter builder needs no pass of its own unless
+            // an exact form may apply.
+            KeyStats ks{(int64_t)host_ctr[4], (int64_t)host_ctr[0], (long long)host_ctr[2], (long long)host_ctr[3]};
+            filter_ = build_key_filter(rt_, o, key, &ks);
         }
     }
 }
@@ -564,6 +618,7 @@ DevBatch HashJoin::probe(const DevBatch &in) {
         }
         out.cols.push_back(ex);
         counters_.output_rows += n;
+        remember_shape(out);
         return out;
     }
 
@@ -576,7 +631,7 @@ DevBatch HashJoin::probe(const DevBatch &in) {
             od.n = 0;
             DBuf cnt(rt_, 8);
             zero(rt_, cnt.get(), 8);
-            auto *mc = counters_dev_.as<unsigned long long>() + 2;
+            auto *mc = counters_dev_.as<unsigned long long>() + 6;
             if (fast)
                 probe_pairs_kernel<true><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, next_.as<uint32_t>(),
                                                                             spec_.seed, od, 0, cnt.as<unsigned long long>(),
@@ -633,7 +688,7 @@ DevBatch HashJoin::probe(const DevBatch &in) {
             if (pairs) {
                 if (build_rows_ > 0 || jt == KRV_JOIN_LEFT_OUTER || jt == KRV_JOIN_FULL_OUTER) {
                     // An empty build still has an all-empty table: every lookup misses.
-                    auto *mc = counters_dev_.as<unsigned long long>() + 2;
+                    auto *mc = counters_dev_.as<unsigned long long>() + 6;
                     uint8_t *marks = marks_.get() ? marks_.as<uint8_t>() : nullptr;
                     const int pad = jt == KRV_JOIN_LEFT_OUTER || jt == KRV_JOIN_FULL_OUTER;
                     if (fast)
@@ -670,6 +725,7 @@ DevBatch HashJoin::probe(const DevBatch &in) {
             out.rows = (int64_t)got;
             for (DevCol &c : out.cols) c.length = out.rows;
             counters_.output_rows += out.rows;
+            remember_shape(out);
             return out;
         }
         cap = got;  // output larger than guessed: run again with room for all of it
@@ -684,8 +740,11 @@ DevBatch HashJoin::finish() {
     const bool tail = jt == KRV_JOIN_RIGHT_SEMI || jt == KRV_JOIN_RIGHT_ANTI || jt == KRV_JOIN_RIGHT_OUTER ||
                       jt == KRV_JOIN_FULL_OUTER;
     if (!tail || finished_) {
+        // Nothing waits for the end: an empty batch of the probe output's shape.
         finished_ = true;
-        return DevBatch{};
+        DevBatch empty;
+        for (const DevCol &m : out_meta_) empty.cols.push_back(make_col(rt_, m.type, 0, m.nullable, m.name));
+        return empty;
     }
     finished_ = true;
     const bool with_probe = jt == KRV_JOIN_RIGHT_OUTER || jt == KRV_JOIN_FULL_OUTER;

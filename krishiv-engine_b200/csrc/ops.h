@@ -36,8 +36,15 @@ struct KeyFilterImpl {
     int32_t exact_has_min = 0;  // INT64_MIN is in the exact set
 };
 // KeyFilterBuilder add + finish over the valid rows of an int64 column.
+// What a join build already knows about its keys: the kept rows, the
+// distinct keys and their range.
+struct KeyStats {
+    int64_t rows;
+    int64_t distinct;
+    long long lo, hi;
+};
 std::shared_ptr<KeyFilterImpl> build_key_filter(Runtime *rt, const krv_key_filter_options &opt,
-                                                const DevCol &keys);
+                                                const DevCol &keys, const KeyStats *known = nullptr);
 // KeyFilter::evaluate: a boolean column (bit-packed, no NULLs).
 DevCol evaluate_key_filter(const KeyFilterImpl &f, const DevCol &keys);
 // Device view for fused kernels.
@@ -59,6 +66,9 @@ class HashJoin {
   public:
     HashJoin(Runtime *rt, const krv_join_spec &spec);
     void build_push(DevBatch b);
+    // Takes a batch whose columns own their device memory as the whole build
+    // side, without copying (one batch, before any push).
+    void build_adopt(DevBatch b);
     void build_finish();
     // Joins one probe batch; returns the output batch (all rows of it).
     DevBatch probe(const DevBatch &in);
@@ -97,6 +107,18 @@ class HashJoin {
 
   private:
     void append_arena(const DevBatch &b);
+    // The column shape (types, names, nullability) of the probe output.
+    void remember_shape(const DevBatch &out) {
+        out_meta_.clear();
+        for (const DevCol &c : out.cols) {
+            DevCol m;
+            m.type = c.type;
+            m.name = c.name;
+            m.nullable = c.nullable;
+            out_meta_.push_back(m);
+        }
+    }
+    std::vector<DevCol> out_meta_;
     Runtime *rt_;
     krv_join_spec spec_;
     std::vector<DevCol> arena_cols_;    // growable build arena

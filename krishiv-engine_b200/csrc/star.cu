@@ -26,146 +26,13 @@
 #include "krv_device.cuh"
 #include "krv_filter.cuh"
 #include "ops.h"
+#include "star_fused.cuh"
 
 namespace krv {
 
 namespace {
 
-constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr long long kAttrEmpty = (long long)0x8080808080808080ULL;
-constexpr int kMaxSmemGroups = 1024;
-
-struct TableView {
-    const unsigned long long *slots;
-    uint64_t mask;
-    const uint32_t *next;
-    uint64_t seed;
-    const long long *keys;  // build key column
-    const int32_t *gid;     // dense group id of each build row's attribute
-};
-
-__device__ __forceinline__ uint32_t table_lookup(const TableView &t, long long k) {
-    const uint64_t g = finalize(hash_word((uint64_t)k), t.seed);
-    const unsigned long long tag = g >> 32;
-    uint64_t pos = g & t.mask;
-    for (uint64_t p = 0; p <= t.mask; p++) {
-        const unsigned long long s = __ldg(t.slots + pos);
-        if (s == 0) return kNone;
-        if ((s >> 32) == tag) {
-            const uint32_t o = (uint32_t)(s & 0xFFFFFFFFull) - 1u;
-            if (__ldg(t.keys + o) == k) return o;
-        }
-        pos = (pos + 1) & t.mask;
-    }
-    return kNone;
-}
-
-struct StarArgs {
-    const long long *fk_a, *fk_b, *price;
-    const double *disc;
-    int64_t n;
-    KeyFilterDev fa, fb;
-    int use_filters;
-    int group_by;  // 0: dim A's attribute, 1: dim B's
-    TableView ta, tb;
-    int ngroups;
-    int bloom_b_smem_words;  // > 0: stage B's Bloom words in shared memory
-    double *sum_hi, *sum_lo;
-    unsigned long long *cnt;
-    unsigned long long *stats;  // [0] rows passing both filters, [1] joined rows
-};
-
-__device__ __forceinline__ void star_row(const StarArgs &A, const KeyFilterDev &fb, int64_t i, long long a, long long b,
-                                         double *s_hi, double *s_lo, unsigned long long *s_cnt, unsigned &passed,
-                                         unsigned &joined) {
-    if (A.use_filters) {
-        if (!filter_pass(fb, b)) return;
-        if (!filter_pass(A.fa, a)) return;
-    }
-    passed++;
-    uint32_t ra = table_lookup(A.ta, a);
-    if (ra == kNone) return;
-    const uint32_t rb0 = table_lookup(A.tb, b);
-    if (rb0 == kNone) return;
-    const double price = (double)__ldcs(A.price + i);
-    const double disc = __ldcs(A.disc + i);
-    const double v = __dmul_rn(price, __dsub_rn(1.0, disc));
-    // Every (a, b) match pair contributes (chains are one long for unique keys).
-    for (int ca = 0; ra != kNone && ca < (1 << 20); ca++, ra = A.ta.next[ra]) {
-        for (uint32_t rb = rb0; rb != kNone; rb = A.tb.next[rb]) {
-            joined++;
-            const int g = A.group_by == 0 ? A.ta.gid[ra] : A.tb.gid[rb];
-            if (g < kMaxSmemGroups && s_hi) {
-                atomic_add_dd(s_hi + g, s_lo + g, v);
-                atomicAdd(s_cnt + g, 1ull);
-            } else {
-                atomic_add_dd(A.sum_hi + g, A.sum_lo + g, v);
-                atomicAdd(A.cnt + g, 1ull);
-            }
-        }
-    }
-}
-
-// The fused fact-side kernel: persistent CTAs stream the two key columns with
-// evict-first loads, 4 rows per thread per step.
-__global__ void __launch_bounds__(512) star_fused_kernel(StarArgs A) {
-    extern __shared__ __align__(16) uint8_t smem[];
-    const int G = A.ngroups < kMaxSmemGroups ? A.ngroups : kMaxSmemGroups;
-    // The Bloom words first (16-byte aligned for the vector loads), then the
-    // group accumulators.
-    uint32_t *s_bloom = reinterpret_cast<uint32_t *>(smem);
-    double *s_hi = reinterpret_cast<double *>(smem + (size_t)A.bloom_b_smem_words * 4);
-    double *s_lo = s_hi + G;
-    unsigned long long *s_cnt = reinterpret_cast<unsigned long long *>(s_lo + G);
-    __shared__ unsigned s_passed, s_joined;
-    for (int g = threadIdx.x; g < G; g += blockDim.x) {
-        s_hi[g] = 0.0;
-        s_lo[g] = 0.0;
-        s_cnt[g] = 0;
-    }
-    KeyFilterDev fb = A.fb;
-    if (A.bloom_b_smem_words > 0) {
-        const uint4 *src = reinterpret_cast<const uint4 *>(A.fb.bloom);
-        uint4 *dst = reinterpret_cast<uint4 *>(s_bloom);
-        for (int w = threadIdx.x; w < A.bloom_b_smem_words / 4; w += blockDim.x) dst[w] = src[w];
-        fb.bloom = s_bloom;
-    }
-    if (threadIdx.x == 0) {
-        s_passed = 0;
-        s_joined = 0;
-    }
-    __syncthreads();
-    unsigned passed = 0, joined = 0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x * 4;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x * 4 + threadIdx.x; base < A.n; base += stride) {
-        long long a[4], b[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int64_t i = base + (int64_t)u * blockDim.x;
-            if (i < A.n) {
-                a[u] = __ldcs(A.fk_a + i);
-                b[u] = __ldcs(A.fk_b + i);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int64_t i = base + (int64_t)u * blockDim.x;
-            if (i < A.n) star_row(A, fb, i, a[u], b[u], s_hi, s_lo, s_cnt, passed, joined);
-        }
-    }
-    atomicAdd(&s_passed, passed);
-    atomicAdd(&s_joined, joined);
-    __syncthreads();
-    for (int g = threadIdx.x; g < G; g += blockDim.x)
-        if (s_cnt[g]) {
-            atomic_add_dd2(A.sum_hi + g, A.sum_lo + g, s_hi[g], s_lo[g]);
-            atomicAdd(A.cnt + g, s_cnt[g]);
-        }
-    if (threadIdx.x == 0) {
-        atomicAdd(A.stats, (unsigned long long)s_passed);
-        atomicAdd(A.stats + 1, (unsigned long long)s_joined);
-    }
-}
 
 // Rows of a dimension with pred == value: their key and attribute, compacted
 // (the filter below the join build).
@@ -299,22 +166,21 @@ class StarPipeline {
             rt_->launches++;
             check_launch("attr_gid_kernel");
         }
+        // The compacted (key, attr, gid) columns become the join's build arena
+        // as they are: no copy.
         DevBatch b;
         b.rows = out.rows;
-        DevCol k;
-        k.type = DType{Type::I64, 0, 0};
-        k.length = out.rows;
-        k.data = out.key.get();
-        k.name = "key";
-        k.nullable = false;
-        DevCol a = k;
-        a.type = DType{Type::I32, 0, 0};
-        a.data = out.attr.get();
-        a.name = "attr";
-        DevCol g = a;
-        g.data = out.gid.get();
-        g.name = "gid";
-        b.cols = {k, a, g};
+        auto own = [&](DBuf &buf, Type t, const char *name) {
+            DevCol c;
+            c.type = DType{t, 0, 0};
+            c.length = out.rows;
+            c.name = name;
+            c.nullable = false;
+            c.hold_data = std::make_shared<DBuf>(std::move(buf));
+            c.data = c.hold_data->get();
+            return c;
+        };
+        b.cols = {own(out.key, Type::I64, "key"), own(out.attr, Type::I32, "attr"), own(out.gid, Type::I32, "gid")};
         krv_join_spec js;
         krv_join_spec_init(&js);
         js.join_type = KRV_JOIN_INNER;
@@ -323,7 +189,7 @@ class StarPipeline {
         js.build_keys[0] = 0;
         js.runtime_filter = spec_.use_filters;
         out.join.reset(new HashJoin(rt_, js));
-        out.join->build_push(b);
+        out.join->build_adopt(std::move(b));
         out.join->build_finish();
     }
 
@@ -352,7 +218,7 @@ class StarPipeline {
         sum_hi_ = DBuf(rt_, G * 8);
         sum_lo_ = DBuf(rt_, G * 8);
         cnt_ = DBuf(rt_, G * 8);
-        stats_ = DBuf(rt_, 16);
+        stats_ = DBuf(rt_, 32);
         reset();
         counters_.dim_a_keys = dims_[0].join->counters().build_keys;
         counters_.dim_b_keys = dims_[1].join->counters().build_keys;
@@ -361,15 +227,23 @@ class StarPipeline {
         counters_.filter_b_form = fb ? fb->info.form : -1;
         counters_.filter_a_bytes = fa ? fa->info.bloom_bytes : 0;
         counters_.filter_b_bytes = fb ? fb->info.bloom_bytes : 0;
+        if (spec_.mode == KRV_STAR_FUSED && spec_.use_filters) {
+            if (fa) build_bits(0, *fa);
+            if (fb) build_bits(1, *fb);
+        }
         built_ = true;
     }
 
     void reset() {
+        counters_.fact_rows = 0;
+        counters_.passed_filters = 0;
+        counters_.joined_rows = 0;
+        if (!sum_hi_.get()) return;  // nothing built yet
         const size_t G = (size_t)std::max(ngroups_host_, 1);
         KRV_CUDA(cudaMemsetAsync(sum_hi_.get(), 0, G * 8, rt_->stream));
         KRV_CUDA(cudaMemsetAsync(sum_lo_.get(), 0, G * 8, rt_->stream));
         KRV_CUDA(cudaMemsetAsync(cnt_.get(), 0, G * 8, rt_->stream));
-        KRV_CUDA(cudaMemsetAsync(stats_.get(), 0, 16, rt_->stream));
+        KRV_CUDA(cudaMemsetAsync(stats_.get(), 0, 32, rt_->stream));
         counters_.fact_rows = 0;
         if (plain_agg_) {
             agg_destroy(plain_agg_);
@@ -389,10 +263,23 @@ class StarPipeline {
         }
     }
 
-    TableView view(const Dim &d) const {
+    StarTable view(const Dim &d) const {
         auto t = d.join->table_dev();
-        return TableView{t.slots, t.mask, t.next, t.seed, static_cast<const long long *>(d.join->arena().cols[0].data),
+        return StarTable{t.slots, t.mask, t.next, t.seed, static_cast<const long long *>(d.join->arena().cols[0].data),
                          static_cast<const int32_t *>(d.join->arena().cols[2].data)};
+    }
+
+    template <int BMODE, bool VEC>
+    void launch_fused(const StarArgs &A, size_t smem) {
+        auto kern = star_fused_kernel<BMODE, VEC>;
+        KRV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStarThreads, smem));
+        per_sm = std::max(1, std::min(per_sm, 2));
+        const int grid = (int)std::min<int64_t>((int64_t)rt_->sm_count * per_sm, ceil_div(A.n, kStarTile));
+        kern<<<grid, kStarThreads, smem, rt_->stream>>>(A);
+        rt_->launches++;
+        check_launch("star_fused_kernel");
     }
 
     void probe_fused(const DevBatch &f) {
@@ -402,6 +289,8 @@ class StarPipeline {
         A.price = static_cast<const long long *>(f.cols[spec_.fact_price].data);
         A.disc = static_cast<const double *>(f.cols[spec_.fact_discount].data);
         A.n = f.rows;
+        if (A.n <= 0) return;
+        if (A.n >= (int64_t)0xFFFFFFFFll) fail(KRV_UNSUPPORTED, "fact batches of 2^32 rows or more");
         auto fa = dims_[0].join->key_filter(), fb = dims_[1].join->key_filter();
         A.use_filters = spec_.use_filters && fa && fb;
         if (A.use_filters) {
@@ -416,24 +305,44 @@ class StarPipeline {
         A.sum_lo = sum_lo_.as<double>();
         A.cnt = cnt_.as<unsigned long long>();
         A.stats = stats_.as<unsigned long long>();
-        const int G = std::min(ngroups_host_, kMaxSmemGroups);
-        size_t smem = (size_t)G * 24;
-        smem = (smem + 15) & ~size_t(15);
-        A.bloom_b_smem_words = 0;
-        if (A.use_filters && A.fb.form == KRV_FILTER_BLOOM && fb->info.bloom_bytes <= 96 * 1024) {
-            A.bloom_b_smem_words = (int)(fb->info.bloom_bytes / 4);
-            smem += (size_t)fb->info.bloom_bytes;
-        }
-        KRV_CUDA(cudaFuncSetAttribute(star_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int per_sm = 0;
-        KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, star_fused_kernel, 512, smem));
-        per_sm = std::max(1, std::min(per_sm, 4));
-        const int grid = (int)std::min<int64_t>((int64_t)rt_->sm_count * per_sm, ceil_div(std::max<int64_t>(f.rows, 1), 512 * 4));
-        if (f.rows > 0) {
-            star_fused_kernel<<<grid, 512, smem, rt_->stream>>>(A);
-            rt_->launches++;
-            check_launch("star_fused_kernel");
-        }
+        // The filters' answer bitmaps (built with the dimensions): B's goes to
+        // shared memory when it fits beside the queues.
+        A.bits_a = A.use_filters && bits_[0].get() ? bits_[0].as<uint32_t>() : nullptr;
+        A.bits_b = A.use_filters && bits_[1].get() ? bits_[1].as<uint32_t>() : nullptr;
+        A.bits_b_smem_words = 0;
+        if (A.bits_b && star_smem_bytes((int)bits_words_[1], ngroups_host_) <= (size_t)rt_->max_smem_optin - 1024)
+            A.bits_b_smem_words = (int)bits_words_[1];
+        const size_t smem = star_smem_bytes(A.bits_b_smem_words, ngroups_host_);
+        if (smem > (size_t)rt_->max_smem_optin) fail(KRV_UNSUPPORTED, "star pipeline: shared memory over the limit");
+        // 16-byte vector loads of fk_b need a 16-byte aligned column.
+        const bool vec = (reinterpret_cast<uintptr_t>(A.fk_b) & 15) == 0;
+        const bool staged = A.bits_b_smem_words > 0;
+        if (staged && vec) launch_fused<1, true>(A, smem);
+        else if (staged) launch_fused<1, false>(A, smem);
+        else if (vec) launch_fused<0, true>(A, smem);
+        else launch_fused<0, false>(A, smem);
+    }
+
+    // The answer bitmap of dimension d's filter over its key range, when the
+    // range has at most 2^28 values (32 MiB).
+    void build_bits(int d, const KeyFilterImpl &f) {
+        bits_[d].reset();
+        bits_words_[d] = 0;
+        if (f.info.form == KRV_FILTER_EMPTY || !f.info.has_range) return;
+        const __int128 range = (__int128)f.info.hi - (__int128)f.info.lo + 1;
+        if (range <= 0 || range > ((__int128)1 << 28)) return;
+        const uint64_t values = (uint64_t)range;
+        const uint64_t words = (values + 127) / 128 * 4;  // whole 16-byte groups
+        // Only a bitmap that fits in shared memory pays for its evaluation: one
+        // evaluated in L2 costs about what the per-row probes it replaces do.
+        if (star_smem_bytes((int)std::min<uint64_t>(words, 1u << 30), ngroups_host_) > (size_t)rt_->max_smem_optin - 1024)
+            return;
+        bits_[d] = DBuf(rt_, words * 4);
+        filter_bitmap_kernel<<<grid_for(rt_, (int64_t)words, 256, 8), 256, 0, rt_->stream>>>(
+            key_filter_dev(f), f.info.lo, words, values, bits_[d].as<uint32_t>());
+        rt_->launches++;
+        check_launch("filter_bitmap_kernel");
+        bits_words_[d] = (int64_t)words;
     }
 
     void probe_plain(const DevBatch &f) {
@@ -547,11 +456,12 @@ class StarPipeline {
                 KRV_CUDA(cudaMemcpyAsync(lo.data(), sum_lo_.get(), (size_t)G * 8, cudaMemcpyDeviceToHost, rt_->stream));
                 KRV_CUDA(cudaMemcpyAsync(cnt.data(), cnt_.get(), (size_t)G * 8, cudaMemcpyDeviceToHost, rt_->stream));
             }
-            unsigned long long st[2];
-            KRV_CUDA(cudaMemcpyAsync(st, stats_.get(), 16, cudaMemcpyDeviceToHost, rt_->stream));
+            unsigned long long st[3];
+            KRV_CUDA(cudaMemcpyAsync(st, stats_.get(), 24, cudaMemcpyDeviceToHost, rt_->stream));
             KRV_CUDA(cudaStreamSynchronize(rt_->stream));
             counters_.passed_filters = (int64_t)st[0];
             counters_.joined_rows = (int64_t)st[1];
+            counters_.fk_a_sectors = (int64_t)st[2];
             // The groups with rows, in group-id order: (attr, hi + lo), the
             // double-double sum rounded once.
             std::vector<int32_t> oa;
@@ -609,6 +519,8 @@ class StarPipeline {
     uint32_t gmask_ = 0;
     int ngroups_host_ = 0;
     DBuf sum_hi_, sum_lo_, cnt_, stats_;
+    DBuf bits_[2];               // filter answer bitmaps of dimensions a and b
+    int64_t bits_words_[2] = {0, 0};
     HashAggregate *plain_agg_ = nullptr;
     bool built_ = false;
     krv_star_counters counters_{};

@@ -49,12 +49,14 @@ class StarData:
     dim_b_rows: int
 
 
-def star(rt, scale: float = 1.0, seed: int = STAR_SEED, fact_row0: int = 0) -> StarData:
+def star(rt, scale: float = 1.0, seed: int = STAR_SEED, fact_row0: int = 0, fact_scale=None) -> StarData:
     """The star-join inputs; `fact_row0` selects which fact rows (a shard of
-    the fact stream for one of several devices)."""
+    the fact stream for one of several devices); `fact_scale` (default
+    `scale`) sizes the fact table alone, the dimensions keep `scale`."""
     import torch
     kb = _kb()
-    nf, na, nb = int(300_000_000 * scale), int(20_000_000 * scale), int(1_000_000 * scale)
+    fs = scale if fact_scale is None else fact_scale
+    nf, na, nb = int(300_000_000 * fs), int(20_000_000 * scale), int(1_000_000 * scale)
     r0 = dict(row0=fact_row0)
     fk_a, _ = _col(rt, nf, torch.int64, kb.GEN_UNIFORM_I64, seed, 1, lo=0, hi=na - 1, **r0)
     fk_b, _ = _col(rt, nf, torch.int64, kb.GEN_UNIFORM_I64, seed, 2, lo=0, hi=nb - 1, **r0)

@@ -39,6 +39,6 @@ def rt(kb):
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     torch.cuda.init()
-    r = kb.Runtime(0, 0, torch.cuda.current_stream().cuda_stream)
+    r = kb.Runtime.on_torch_stream(0)
     yield r
     r.synchronize()

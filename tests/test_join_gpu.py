@@ -82,7 +82,7 @@ def test_join_types_random_duplicates(kb, rt, oracle, jt):
                                                                    rng.integers(0, 3, 20000))]
     build = [(int(x) if x >= 0 else None, int(y)) for x, y in zip(rng.integers(-20, 3000, 9000),
                                                                    rng.integers(0, 3, 9000))]
-    for nkeys in (1, 2):
+    for nkeys in ((1,) if jt == "null_aware_anti" else (1, 2)):
         want = oracle_pairs(oracle, jt, probe, build, nkeys, False)
         got = gpu_pairs(kb, rt, jt, probe, build, nkeys, False, build_batches=3)
         assert got == want, (jt, nkeys)
@@ -183,7 +183,7 @@ def test_device_path_matches_host_path(kb, rt, oracle):
 
 def test_budget_need_memory(kb):
     import torch
-    small = kb.Runtime(0, 1 << 20, torch.cuda.current_stream().cuda_stream)
+    small = kb.Runtime(0, 1 << 20, torch.cuda.current_stream().cuda_stream or None)
     j = kb.HashJoin(small, kb.join_spec("inner"))
     with pytest.raises(kb.KrvError) as e:
         j.build_push(batch(k=pa.array(np.arange(1 << 20, dtype=np.int64))))
