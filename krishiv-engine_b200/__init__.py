@@ -17,7 +17,8 @@ import os
 from typing import Dict, List, Optional, Sequence
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libkrv_gpu.so")
+# KRV_LIB_PATH selects another build of the library (e.g. an installed copy).
+LIB_PATH = os.environ.get("KRV_LIB_PATH") or os.path.join(HERE, "libkrv_gpu.so")
 
 # ---- status codes (krv_gpu.h) --------------------------------------------------------
 OK, NEED_MORE_INPUT, HAVE_MORE_OUTPUT, FINISHED = 0, 1, 2, 3

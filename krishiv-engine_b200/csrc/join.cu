@@ -533,6 +533,9 @@ void HashJoin::build_finish() {
     counters_.build_keys = (int64_t)host_ctr[0];
     counters_.table_slots = (int64_t)slots;
     any_null_build_ = host_ctr[1] != 0;
+    indexed_rows_ = (int64_t)host_ctr[4];
+    key_lo_ = (long long)host_ctr[2];
+    key_hi_ = (long long)host_ctr[3];
     // The runtime filter of a one-key join (BuildSink::publish, join/build.rs:482).
     if (spec_.runtime_filter && spec_.n_keys == 1) {
         const DevCol &key = arena_.cols[spec_.build_keys[0]];

@@ -104,6 +104,10 @@ class HashJoin {
     };
     TableDev table_dev() const;
     const DevBatch &arena() const { return arena_; }
+    // What the build saw of a one-int64-key table: indexed rows and key range.
+    int64_t indexed_rows() const { return indexed_rows_; }
+    long long key_lo() const { return key_lo_; }
+    long long key_hi() const { return key_hi_; }
 
   private:
     void append_arena(const DevBatch &b);
@@ -119,6 +123,8 @@ class HashJoin {
         }
     }
     std::vector<DevCol> out_meta_;
+    int64_t indexed_rows_ = 0;
+    long long key_lo_ = 0, key_hi_ = -1;
     Runtime *rt_;
     krv_join_spec spec_;
     std::vector<DevCol> arena_cols_;    // growable build arena

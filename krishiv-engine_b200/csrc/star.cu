@@ -36,22 +36,38 @@ constexpr long long kAttrEmpty = (long long)0x8080808080808080ULL;
 
 // Rows of a dimension with pred == value: their key and attribute, compacted
 // (the filter below the join build).
+// Each warp takes chunks of 16 x 32 rows: it reads pred for the chunk (one
+// ballot per 32 rows), reserves the chunk's output with one atomic, then
+// writes the survivors in row order.
+constexpr int kSelectSteps = 16;
 __global__ void __launch_bounds__(256) dim_select_kernel(const long long *key, const int32_t *pred, const int32_t *attr,
                                                          int64_t n, int32_t value, long long *okey, int32_t *oattr,
                                                          unsigned long long *count) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += stride) {
-        const int64_t i = base + threadIdx.x;
-        const bool ok = i < n && pred[i] == value;
-        unsigned long long pos;
-        const unsigned ballot = __ballot_sync(0xFFFFFFFFu, ok);
-        unsigned long long first = 0;
-        if (lane_id() == 0 && ballot) first = atomicAdd(count, (unsigned long long)__popc(ballot));
-        first = __shfl_sync(0xFFFFFFFFu, first, 0);
-        pos = first + __popc(ballot & lanemask_lt());
-        if (ok) {
-            okey[pos] = key[i];
-            oattr[pos] = attr[i];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
+    const int64_t chunk = 32 * kSelectSteps;
+    for (int64_t c0 = ((int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5)) * chunk; c0 < n;
+         c0 += warps * chunk) {
+        unsigned ballots[kSelectSteps];
+        int total = 0;
+#pragma unroll
+        for (int s = 0; s < kSelectSteps; s++) {
+            const int64_t i = c0 + s * 32 + lane;
+            ballots[s] = __ballot_sync(0xFFFFFFFFu, i < n && pred[i] == value);
+            total += __popc(ballots[s]);
+        }
+        unsigned long long base = 0;
+        if (lane == 0 && total) base = atomicAdd(count, (unsigned long long)total);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+#pragma unroll
+        for (int s = 0; s < kSelectSteps; s++) {
+            if ((ballots[s] >> lane) & 1u) {
+                const int64_t i = c0 + s * 32 + lane;
+                const unsigned long long pos = base + __popc(ballots[s] & lanemask_lt());
+                okey[pos] = key[i];
+                oattr[pos] = attr[i];
+            }
+            base += __popc(ballots[s]);
         }
     }
 }
@@ -64,8 +80,12 @@ __global__ void attr_gid_kernel(const int32_t *attr, int64_t n, long long *tkeys
         uint64_t pos = hash_word((uint64_t)k) & mask;
         int32_t g = -1;
         for (uint64_t p = 0; p <= mask; p++) {
-            const long long cur = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(tkeys + pos),
-                                                       (unsigned long long)kAttrEmpty, (unsigned long long)k);
+            // A plain read first: few distinct values, so nearly every row finds
+            // its value already there and needs no atomic.
+            long long cur = __ldcg(tkeys + pos);
+            if (cur == kAttrEmpty)
+                cur = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(tkeys + pos),
+                                           (unsigned long long)kAttrEmpty, (unsigned long long)k);
             if (cur == kAttrEmpty) {
                 g = (int32_t)atomicAdd(ngroups, 1u);
                 gattr[g] = (int32_t)k;
@@ -231,6 +251,10 @@ class StarPipeline {
             if (fa) build_bits(0, *fa);
             if (fb) build_bits(1, *fb);
         }
+        if (spec_.mode == KRV_STAR_FUSED) {
+            build_direct(0);
+            build_direct(1);
+        }
         built_ = true;
     }
 
@@ -269,17 +293,23 @@ class StarPipeline {
                          static_cast<const int32_t *>(d.join->arena().cols[2].data)};
     }
 
-    template <int BMODE, bool VEC>
-    void launch_fused(const StarArgs &A, size_t smem) {
-        auto kern = star_fused_kernel<BMODE, VEC>;
+    template <int BMODE, bool VEC, bool KB32>
+    void launch_scan(const StarArgs &A, int grid, size_t smem) {
+        auto kern = star_scan_kernel<BMODE, VEC, KB32>;
         KRV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int per_sm = 0;
-        KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStarThreads, smem));
-        per_sm = std::max(1, std::min(per_sm, 2));
-        const int grid = (int)std::min<int64_t>((int64_t)rt_->sm_count * per_sm, ceil_div(A.n, kStarTile));
-        kern<<<grid, kStarThreads, smem, rt_->stream>>>(A);
+        kern<<<grid, kScanThreads, smem, rt_->stream>>>(A);
         rt_->launches++;
-        check_launch("star_fused_kernel");
+        check_launch("star_scan_kernel");
+    }
+
+    template <bool DIRECT, bool KB32>
+    void launch_join(const StarArgs &A, int regions, int slices, int G) {
+        auto kern = star_join_kernel<DIRECT, KB32>;
+        const size_t smem = star_join_smem(G);
+        KRV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<regions * slices, kJoinThreads, smem, rt_->stream>>>(A, regions, slices, G);
+        rt_->launches++;
+        check_launch("star_join_kernel");
     }
 
     void probe_fused(const DevBatch &f) {
@@ -300,27 +330,89 @@ class StarPipeline {
         A.group_by = spec_.group_by;
         A.ta = view(dims_[0]);
         A.tb = view(dims_[1]);
+        A.da = direct_[0];
+        A.db = direct_[1];
         A.ngroups = ngroups_host_;
         A.sum_hi = sum_hi_.as<double>();
         A.sum_lo = sum_lo_.as<double>();
         A.cnt = cnt_.as<unsigned long long>();
         A.stats = stats_.as<unsigned long long>();
-        // The filters' answer bitmaps (built with the dimensions): B's goes to
-        // shared memory when it fits beside the queues.
-        A.bits_a = A.use_filters && bits_[0].get() ? bits_[0].as<uint32_t>() : nullptr;
+        // B's filter answer bitmap (built with the dimensions) is staged in
+        // shared memory when it fits.
         A.bits_b = A.use_filters && bits_[1].get() ? bits_[1].as<uint32_t>() : nullptr;
-        A.bits_b_smem_words = 0;
-        if (A.bits_b && star_smem_bytes((int)bits_words_[1], ngroups_host_) <= (size_t)rt_->max_smem_optin - 1024)
-            A.bits_b_smem_words = (int)bits_words_[1];
-        const size_t smem = star_smem_bytes(A.bits_b_smem_words, ngroups_host_);
-        if (smem > (size_t)rt_->max_smem_optin) fail(KRV_UNSUPPORTED, "star pipeline: shared memory over the limit");
+        const size_t limit = (size_t)rt_->max_smem_optin - 1024;
+        const bool staged = A.bits_b && star_scan_smem((int)bits_words_[1]) <= limit;
+        A.bits_b_smem_words = staged ? (int)bits_words_[1] : 0;
+        // The survivor list: one region per scan CTA, as large as the rows it scans.
+        const int64_t tiles = ceil_div(A.n, kScanTile);
+        const int grid = (int)std::min<int64_t>(rt_->sm_count, tiles);
+        A.region = (uint64_t)ceil_div(tiles, grid) * kScanTile;
+        const uint64_t entries = A.region * (uint64_t)grid;
+        // B's key range below 2^32: a survivor keeps fk_b - lo in 32 bits.
+        const bool kb32 = A.use_filters && A.fb.has_range &&
+                          (unsigned long long)(A.fb.hi - A.fb.lo) < 0xFFFFFFFFull;
+        if (surv_cap_ < entries || surv_kb64_ != !kb32) {
+            surv_row_ = DBuf(rt_, entries * 4);
+            surv_kb_ = DBuf(rt_, entries * (kb32 ? 4 : 8));
+            surv_cap_ = entries;
+            surv_kb64_ = !kb32;
+        }
+        if (region_count_.bytes() < (size_t)grid * 8) region_count_ = DBuf(rt_, (size_t)rt_->sm_count * 8);
+        A.surv_row = surv_row_.as<uint32_t>();
+        A.surv_kb32 = kb32 ? surv_kb_.as<uint32_t>() : nullptr;
+        A.surv_kb64 = kb32 ? nullptr : surv_kb_.as<long long>();
+        A.region_count = region_count_.as<unsigned long long>();
         // 16-byte vector loads of fk_b need a 16-byte aligned column.
         const bool vec = (reinterpret_cast<uintptr_t>(A.fk_b) & 15) == 0;
-        const bool staged = A.bits_b_smem_words > 0;
-        if (staged && vec) launch_fused<1, true>(A, smem);
-        else if (staged) launch_fused<1, false>(A, smem);
-        else if (vec) launch_fused<0, true>(A, smem);
-        else launch_fused<0, false>(A, smem);
+        const size_t smem = star_scan_smem(A.bits_b_smem_words);
+        if (staged) {
+            if (vec && kb32) launch_scan<1, true, true>(A, grid, smem);
+            else if (vec) launch_scan<1, true, false>(A, grid, smem);
+            else if (kb32) launch_scan<1, false, true>(A, grid, smem);
+            else launch_scan<1, false, false>(A, grid, smem);
+        } else {
+            if (vec && kb32) launch_scan<0, true, true>(A, grid, smem);
+            else if (vec) launch_scan<0, true, false>(A, grid, smem);
+            else if (kb32) launch_scan<0, false, true>(A, grid, smem);
+            else launch_scan<0, false, false>(A, grid, smem);
+        }
+        // Join over the survivors: several CTAs per region, so hundreds of
+        // thousands of independent probes hide the memory latency.
+        const int G = std::max(1, std::min(ngroups_host_, 256));
+        const int slices = 4;
+        const bool direct = A.da.width && A.db.width;
+        if (direct && kb32) launch_join<true, true>(A, grid, slices, G);
+        else if (direct) launch_join<true, false>(A, grid, slices, G);
+        else if (kb32) launch_join<false, true>(A, grid, slices, G);
+        else launch_join<false, false>(A, grid, slices, G);
+    }
+
+    // A direct index (key -> group id) of dimension d when its keys are
+    // unique and span at most 2^26 values and the ids fit 1 or 2 bytes.
+    void build_direct(int d) {
+        direct_[d] = StarDirect{nullptr, 0, 0, 0};
+        direct_buf_[d].reset();
+        const HashJoin &j = *dims_[d].join;
+        const int64_t rows = j.indexed_rows();
+        if (rows <= 0 || j.counters().build_keys != rows || j.counters().build_rows != rows) return;
+        const __int128 span = (__int128)j.key_hi() - (__int128)j.key_lo();
+        if (span < 0 || span >= ((__int128)1 << 26)) return;
+        const int width = ngroups_host_ < 127 ? 1 : ngroups_host_ < 32767 ? 2 : 0;
+        if (!width) return;
+        const size_t bytes = ((size_t)span + 1) * width;
+        direct_buf_[d] = DBuf(rt_, bytes);
+        KRV_CUDA(cudaMemsetAsync(direct_buf_[d].get(), 0xFF, bytes, rt_->stream));
+        const long long *keys = static_cast<const long long *>(j.arena().cols[0].data);
+        const int32_t *gid = static_cast<const int32_t *>(j.arena().cols[2].data);
+        if (width == 1)
+            direct_index_kernel<int8_t><<<grid_for(rt_, rows, 256, 8), 256, 0, rt_->stream>>>(
+                keys, gid, rows, j.key_lo(), direct_buf_[d].as<int8_t>());
+        else
+            direct_index_kernel<int16_t><<<grid_for(rt_, rows, 256, 8), 256, 0, rt_->stream>>>(
+                keys, gid, rows, j.key_lo(), direct_buf_[d].as<int16_t>());
+        rt_->launches++;
+        check_launch("direct_index_kernel");
+        direct_[d] = StarDirect{direct_buf_[d].get(), j.key_lo(), (unsigned long long)span, width};
     }
 
     // The answer bitmap of dimension d's filter over its key range, when the
@@ -335,10 +427,10 @@ class StarPipeline {
         const uint64_t words = (values + 127) / 128 * 4;  // whole 16-byte groups
         // Only a bitmap that fits in shared memory pays for its evaluation: one
         // evaluated in L2 costs about what the per-row probes it replaces do.
-        if (star_smem_bytes((int)std::min<uint64_t>(words, 1u << 30), ngroups_host_) > (size_t)rt_->max_smem_optin - 1024)
+        if (star_scan_smem((int)std::min<uint64_t>(words, 1u << 30)) > (size_t)rt_->max_smem_optin - 1024)
             return;
         bits_[d] = DBuf(rt_, words * 4);
-        filter_bitmap_kernel<<<grid_for(rt_, (int64_t)words, 256, 8), 256, 0, rt_->stream>>>(
+        filter_bitmap_kernel<<<grid_for(rt_, (int64_t)(words * 32), 256, 8), 256, 0, rt_->stream>>>(
             key_filter_dev(f), f.info.lo, words, values, bits_[d].as<uint32_t>());
         rt_->launches++;
         check_launch("filter_bitmap_kernel");
@@ -520,6 +612,11 @@ class StarPipeline {
     int ngroups_host_ = 0;
     DBuf sum_hi_, sum_lo_, cnt_, stats_;
     DBuf bits_[2];               // filter answer bitmaps of dimensions a and b
+    DBuf direct_buf_[2];         // direct key -> group id indexes
+    DBuf surv_row_, surv_kb_, region_count_;  // fact rows that passed B's filter
+    uint64_t surv_cap_ = 0;
+    bool surv_kb64_ = false;
+    StarDirect direct_[2] = {};
     int64_t bits_words_[2] = {0, 0};
     HashAggregate *plain_agg_ = nullptr;
     bool built_ = false;
