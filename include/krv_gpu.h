@@ -350,6 +350,33 @@ typedef struct {
 krv_status krv_gen_fill(krv_runtime *rt, const krv_gen_spec *spec, int64_t n, void *out,
                         void *out_valid);
 
+/* ---- grouped SUM/COUNT with no allocation ----------------------------------
+ * No counterpart in the reference. For a caller that may not allocate device
+ * memory where it calls (all of HBM is in its own accounted pool, or a
+ * cudaMalloc / cudaFree would stall its device): GROUP BY keys with SUM(values)
+ * and COUNT(*), both int64 columns without NULLs, the results of
+ * krv_agg_create/push/finish for that spec with ansi = 0. The hash table is a
+ * fixed device array of this library (4 MiB per device); the call allocates
+ * nothing and only launches kernels on `stream` (NULL: the default stream) of
+ * the current device. All pointers are device memory of that device.
+ *  - max_groups may be at most KRV_SCRATCH_MAX_GROUPS (larger: an
+ *    KRV_INVALID_ARGUMENT error before any device work); out_keys, out_sums
+ *    and out_counts hold max_groups values each;
+ *  - out_info[0] = the number of groups written (in no particular order), or
+ *    -1 when the input had more distinct keys than max_groups (the outputs are
+ *    then void; so are they when a key found no free slot in 8192 probes, which
+ *    takes more distinct keys than the table holds); out_info[1] = 1 when some
+ *    sum left int64 and wrapped;
+ *  - nothing has to start at zero: each call clears its table first;
+ *  - the first call on a device looks up the table's address there: make it
+ *    before any stream capture;
+ *  - the table is shared by all calls on a device: calls that overlap in time
+ *    (other streams or host threads) race. Calls in order on one stream do not. */
+#define KRV_SCRATCH_MAX_GROUPS 65536
+krv_status krv_agg_sum_i64_scratch(const int64_t *keys, const int64_t *values, int64_t n,
+                                   int64_t max_groups, int64_t *out_keys, int64_t *out_sums,
+                                   int64_t *out_counts, int64_t *out_info, void *stream);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

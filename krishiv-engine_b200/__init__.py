@@ -43,6 +43,7 @@ GEN_UNIFORM_I64, GEN_UNIFORM_I32, GEN_UNIT_F64, GEN_PERMUTATION, GEN_ZIPF = 0, 1
 MAX_KEYS = 4
 MAX_OUT = 32
 MAX_AGGS = 32
+SCRATCH_MAX_GROUPS = 65536  # KRV_SCRATCH_MAX_GROUPS
 
 
 class KrvError(RuntimeError):
@@ -206,6 +207,8 @@ _SIGS = {
     "krv_star_counters_get": (C.c_int32, [C.c_void_p, C.POINTER(StarCounters)]),
     "krv_star_destroy": (None, [C.c_void_p]),
     "krv_gen_fill": (C.c_int32, [C.c_void_p, C.POINTER(GenSpec), C.c_int64, C.c_void_p, C.c_void_p]),
+    "krv_agg_sum_i64_scratch": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 
@@ -727,3 +730,19 @@ def gen_fill(rt: Runtime, out, kind: int, seed: int, column: int, lo: int = 0, h
                 row0=row0)
     check(lib().krv_gen_fill(rt.h, C.byref(s), int(out.shape[0]), out.data_ptr(),
                              valid.data_ptr() if valid is not None else None))
+
+
+def agg_sum_i64_scratch(keys, values, out_keys, out_sums, out_counts, out_info, stream=None):
+    """GROUP BY `keys` SUM(`values`), COUNT(*) without allocating device memory
+    (krv_agg_sum_i64_scratch). All arguments are int64 CUDA tensors of the
+    current device; the three outputs hold max_groups = len(out_keys) values
+    (at most SCRATCH_MAX_GROUPS) and out_info two: the group count (-1 when the
+    keys had more distinct values than max_groups) and a wrap flag. `stream`
+    is a raw cudaStream_t handle (None: the default stream). Asynchronous."""
+    n = int(keys.shape[0])
+    if int(values.shape[0]) != n:
+        raise ValueError("keys and values differ in length")
+    g = int(out_keys.shape[0])
+    check(lib().krv_agg_sum_i64_scratch(keys.data_ptr() if n else None, values.data_ptr() if n else None, n, g,
+                                        out_keys.data_ptr() if g else None, out_sums.data_ptr() if g else None,
+                                        out_counts.data_ptr() if g else None, out_info.data_ptr(), stream))
