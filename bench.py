@@ -231,13 +231,15 @@ def run_star(args, kb, W, rt, rank, world, pg, device):
     pr = dict(zip(plain_res.column(0).to_pylist(), plain_res.column(1).to_pylist()))
     agree = sorted(fr) == sorted(pr) and all(abs(fr[k] - pr[k]) <= 1e-12 * abs(pr[k]) for k in fr)
     nf = data.fact_rows
-    # The dominant kernel: the fused fact probe. Algorithmic bytes per launch:
-    # fk_b of every fact row, the 32-byte sectors of fk_a holding a row that
-    # passed dimension B's filter (counted by the kernel), and the price and
-    # discount sectors of every joined row (2 x 32 bytes).
+    # The dominant launch pair: the fact probe (star_scan_kernel streams fk_b
+    # and appends the rows passing B's filter; star_join_kernel probes them).
+    # Algorithmic bytes per unit: 16 B per fact row (both key columns) and
+    # 16 B per joined row (price and discount). The design reads fk_a only in
+    # the 32-byte sectors of rows that pass B's filter, counted by the scan;
+    # that figure is reported beside it.
     kern_ms = statistics.median(kernel_ms)
-    alg_bytes = 8 * nf + 32 * counters["fk_a_sectors"] + 64 * counters["joined_rows"]
-    touch_model = 16 * nf + 16 * counters["joined_rows"]
+    alg_bytes = 16 * nf + 16 * counters["joined_rows"]
+    sector_bytes = 8 * nf + 32 * counters["fk_a_sectors"] + 64 * counters["joined_rows"]
     peak, peak_kind = hbm_peak()
     achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
     out = {
@@ -258,11 +260,12 @@ def run_star(args, kb, W, rt, rank, world, pg, device):
                    "selectivity": "5% per dimension", "groups": 25, "mode": "fused (batched) pipeline",
                    "l2": "inputs (9.6 GB per GPU) larger than L2; no flush"},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": "star_fused_kernel", "achieved": achieved, "peak": peak,
-                     "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": profile_traffic("star_fused_kernel", nf),
+        "roofline": {"bound": "hbm", "kernel": "star_scan_kernel + star_join_kernel (fact probe)",
+                     "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": profile_traffic("star_probe", nf),
                      "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms,
-                     "both_key_columns_model_GBps": touch_model / (kern_ms * 1e-3) / 1e9},
+                     "sectors_read_bytes": sector_bytes,
+                     "sectors_read_GBps": sector_bytes / (kern_ms * 1e-3) / 1e9},
         "plain": {"ms_per_step": plain_ms, "value": world * nf / (plain_ms * 1e-3) / 1e6,
                   "fused_speedup": plain_ms / ms_max, "results_agree": agree},
         "counters": {k: counters[k] for k in ("passed_filters", "joined_rows", "dim_a_keys", "dim_b_keys",
@@ -271,11 +274,11 @@ def run_star(args, kb, W, rt, rank, world, pg, device):
     }
     del plain
     if not args.no_e2e:
-        out["e2e"] = run_star_e2e(args, kb, rt, data, pg, device)
+        out["e2e"] = run_star_e2e(args, kb, W, rt, data, pg, device)
     return out
 
 
-def run_star_e2e(args, kb, rt, data, pg, device):
+def run_star_e2e(args, kb, W, rt, data, pg, device):
     """The same query through the C ABI with host (pinned) Arrow buffers; the
     host-to-device copies and the result's device-to-host read are timed."""
     import pyarrow as pa
@@ -294,9 +297,9 @@ def run_star_e2e(args, kb, rt, data, pg, device):
     fact, k1 = host_batch(data.fact)
     dim_a, k2 = host_batch(data.dim_a)
     dim_b, k3 = host_batch(data.dim_b)
-    pipe = kb.StarPipeline(rt, kb.star_spec(7, 7, group_by=0, mode=kb.STAR_FUSED))
+    pipe = kb.StarPipeline(rt, kb.star_spec(W.PRED_VALUE, W.PRED_VALUE, group_by=0, mode=kb.STAR_FUSED))
     steps = max(2, args.steps // 2)
-    for _ in range(1):
+    for _ in range(args.warmup):
         pipe.reset()
         pipe.build(dim_a, dim_b)
         pipe.probe(fact)
@@ -313,19 +316,30 @@ def run_star_e2e(args, kb, rt, data, pg, device):
     dt = (time.perf_counter() - t0) / steps
     dt = max_over_ranks(pg, dt, device)
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    h2d = sum(t.numel() * t.element_size() for _, t, _ in data.fact + data.dim_a + data.dim_b)
+    c = pipe.counters()
+    # The host columns are page-locked, so the kernels read them in place:
+    # every dimension row (key, pred, attr), fk_b of every fact row, the fk_a
+    # sectors of rows that passed B's filter and the price and discount
+    # sectors of joined rows cross the host link; nothing else does.
+    dims = sum(t.numel() * t.element_size() for _, t, _ in data.dim_a + data.dim_b)
+    h2d = dims + 8 * data.fact_rows + 32 * c["fk_a_sectors"] + 64 * c["joined_rows"]
+    resident = sum(t.numel() * t.element_size() for _, t, _ in data.fact + data.dim_a + data.dim_b)
     return {"value": world * data.fact_rows / dt / 1e6, "unit": "Mrows/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": res.num_rows * 12, "ms_per_step": dt * 1e3, "steps": steps,
+            "host_input_bytes": resident,
+            "transfer": "page-locked host Arrow buffers read in place by the kernels; h2d = the 32-byte "
+                        "sectors they read",
             "timing": "host wall clock around synchronous C-ABI calls"}
 
 
-def profile_traffic(kernel, rows):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary
-    (profiles/<kernel>.md: 'dram_bytes_per_row: X'), scaled to `rows`."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}.md")
+def profile_traffic(name, rows):
+    """DRAM bytes (read + write) of one launch of `name` over `rows` fact
+    rows, from the committed ncu summary (profiles/<name>_dram.md, line
+    'dram_bytes_per_fact_row: X'), scaled to `rows`."""
+    path = os.path.join(ROOT, "profiles", f"{name}_dram.md")
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_row:"):
+            if line.startswith("dram_bytes_per_fact_row:"):
                 return float(line.split(":")[1]) * rows
     except OSError:
         pass

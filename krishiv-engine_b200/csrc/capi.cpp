@@ -186,6 +186,7 @@ krv_status krv_join_build_push(krv_join *j, const ArrowArray *batch, const Arrow
     return guard([&] {
         need(j, "join");
         krv::DeviceGuard g(&j->owner->rt);
+        krv::HostBorrow hb(&j->owner->rt);
         j->j->build_push(krv::import_host(&j->owner->rt, batch, schema));
         return KRV_OK;
     });
@@ -218,8 +219,13 @@ static krv_status join_probe_impl(krv_join *j, const In *in, const ArrowSchema *
         if (in) {
             if (!j->pending.empty()) krv::fail(KRV_INVALID_ARGUMENT, "drain pending output (input NULL) first");
             DevBatch inb;
-            if constexpr (Device) inb = krv::import_device(rt, in, in_schema);
-            else inb = krv::import_host(rt, in, in_schema);
+            std::unique_ptr<krv::HostBorrow> hb;
+            if constexpr (Device) {
+                inb = krv::import_device(rt, in, in_schema);
+            } else {
+                hb.reset(new krv::HostBorrow(rt));
+                inb = krv::import_host(rt, in, in_schema);
+            }
             b = take_first(j->j->probe(inb), j->j->spec().max_output_rows, j->pending);
         } else {
             if (j->pending.empty()) krv::fail(KRV_INVALID_ARGUMENT, "no pending output and no input");
@@ -312,6 +318,7 @@ krv_status krv_agg_push(krv_agg *a, const ArrowArray *batch, const ArrowSchema *
     return guard([&] {
         need(a, "aggregate");
         krv::DeviceGuard g(&a->owner->rt);
+        krv::HostBorrow hb(&a->owner->rt);
         krv::agg_push(a->a, krv::import_host(&a->owner->rt, batch, schema));
         return KRV_OK;
     });
@@ -382,6 +389,7 @@ static krv_status filter_build_impl(krv_runtime *rt, const krv_key_filter_option
         krv_key_filter_options o;
         if (opt) o = *opt;
         else krv_key_filter_options_default(&o);
+        krv::HostBorrow hb(&rt->rt);
         DevBatch b;
         if constexpr (Device) b = krv::import_device(&rt->rt, batch, schema);
         else b = krv::import_host(&rt->rt, batch, schema);
@@ -408,6 +416,7 @@ static krv_status filter_eval_impl(krv_key_filter *f, const In *batch, const Arr
         need(out, "out");
         krv::Runtime *rt = f->f->rt;
         krv::DeviceGuard g(rt);
+        krv::HostBorrow hb(rt);
         DevBatch b;
         if constexpr (Device) b = krv::import_device(rt, batch, schema);
         else b = krv::import_host(rt, batch, schema);
@@ -485,7 +494,11 @@ krv_status krv_star_build(krv_star *s, const ArrowArray *a, const ArrowSchema *s
         need(s, "star");
         krv::Runtime *rt = &s->owner->rt;
         krv::DeviceGuard g(rt);
-        krv::star_build(s->s, krv::import_host(rt, a, sa), krv::import_host(rt, b, sb));
+        krv::HostBorrow hb(rt);
+        // The build reads each dimension column once: page-locked columns are
+        // read in place.
+        krv::star_build(s->s, krv::import_host(rt, a, sa, krv::HostRead::InPlace),
+                        krv::import_host(rt, b, sb, krv::HostRead::InPlace));
         return KRV_OK;
     });
 }
@@ -504,7 +517,12 @@ krv_status krv_star_probe(krv_star *s, const ArrowArray *fact, const ArrowSchema
         need(s, "star");
         krv::Runtime *rt = &s->owner->rt;
         krv::DeviceGuard g(rt);
-        krv::star_probe(s->s, krv::import_host(rt, fact, schema));
+        krv::HostBorrow hb(rt);
+        // The fused probe streams fk_b once and reads fk_a, price and discount
+        // only for the rows that pass the filters: page-locked columns are
+        // read in place, so only those bytes cross the host link.
+        const krv::HostRead mode = krv::star_fused(s->s) ? krv::HostRead::InPlace : krv::HostRead::Copy;
+        krv::star_probe(s->s, krv::import_host(rt, fact, schema, mode));
         return KRV_OK;
     });
 }

@@ -59,6 +59,22 @@ struct Runtime {
     int max_smem_optin = 227 * 1024;
     void *status_dev = nullptr;   // device status words (errors from kernels)
     void *status_host = nullptr;  // pinned mirror
+    // Work queued on the stream still reads the caller's host buffers
+    // (copies from page-locked memory, or columns read in place).
+    bool host_borrowed = false;
+};
+
+// Scope of a call that takes host batches: the caller owns its buffers again
+// when the call returns, so the call waits for the work that reads them.
+struct HostBorrow {
+    Runtime *rt;
+    explicit HostBorrow(Runtime *r) : rt(r) { rt->host_borrowed = false; }
+    ~HostBorrow() {
+        if (rt->host_borrowed) cudaStreamSynchronize(rt->stream);
+        rt->host_borrowed = false;
+    }
+    HostBorrow(const HostBorrow &) = delete;
+    HostBorrow &operator=(const HostBorrow &) = delete;
 };
 
 // Makes `rt`'s device current for the scope.
@@ -143,7 +159,13 @@ struct DevBatch {
 };
 
 // Import: host batch -> device (copies), device batch -> views (no copy).
-DevBatch import_host(Runtime *rt, const ArrowArray *arr, const ArrowSchema *schema);
+// With HostRead::InPlace, columns in page-locked host memory (cudaHostAlloc,
+// cudaHostRegister) become views that kernels read where they lie, over the
+// host link, and only the bytes a kernel touches cross it; other columns are
+// copied. Either way the calling entry point holds a HostBorrow.
+enum class HostRead { Copy, InPlace };
+DevBatch import_host(Runtime *rt, const ArrowArray *arr, const ArrowSchema *schema,
+                     HostRead mode = HostRead::Copy);
 DevBatch import_device(Runtime *rt, const ArrowDeviceArray *arr, const ArrowSchema *schema);
 // Export: moves the batch's buffers to the caller.
 void export_host(Runtime *rt, const DevBatch &b, ArrowArray *out, ArrowSchema *out_schema);

@@ -162,6 +162,7 @@ void star_probe(StarPipeline *s, const DevBatch &fact);
 DevBatch star_result(StarPipeline *s);
 void star_reset(StarPipeline *s);
 krv_star_counters star_counters(const StarPipeline *s);
+bool star_fused(const StarPipeline *s);  // KRV_STAR_FUSED plan
 void star_destroy(StarPipeline *s);
 
 // ---- generators ------------------------------------------------------------------

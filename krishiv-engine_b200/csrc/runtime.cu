@@ -201,8 +201,40 @@ static void check_struct(const ArrowArray *arr, const ArrowSchema *schema) {
     if (arr->release == nullptr) fail(KRV_INVALID_ARGUMENT, "released ArrowArray");
 }
 
+// The device address of host range [p, p + bytes) when all of it is
+// page-locked host memory mapped for the device, else nullptr.
+static const uint8_t *mapped_host(const uint8_t *p, size_t bytes) {
+    if (!p || bytes == 0) return nullptr;
+    cudaPointerAttributes a0{}, a1{};
+    if (cudaPointerGetAttributes(&a0, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a0.type != cudaMemoryTypeHost || !a0.devicePointer) return nullptr;
+    const uint8_t *last = p + bytes - 1;
+    if (cudaPointerGetAttributes(&a1, last) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a1.type != cudaMemoryTypeHost || !a1.devicePointer) return nullptr;
+    const uint8_t *d0 = static_cast<const uint8_t *>(a0.devicePointer);
+    if (static_cast<const uint8_t *>(a1.devicePointer) != d0 + (bytes - 1)) return nullptr;
+    return d0;
+}
+
+// Whether host pointer p is page-locked (a copy from it runs asynchronously).
+static bool page_locked(const void *p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 template <bool Device>
-static DevBatch import_impl(Runtime *rt, const ArrowArray *arr, const ArrowSchema *schema) {
+static DevBatch import_impl(Runtime *rt, const ArrowArray *arr, const ArrowSchema *schema,
+                            HostRead mode = HostRead::Copy) {
     check_struct(arr, schema);
     DevBatch b;
     b.rows = arr->length;
@@ -241,17 +273,27 @@ static DevBatch import_impl(Runtime *rt, const ArrowArray *arr, const ArrowSchem
                 bytes = (size_t)b.rows * (size_t)w;
                 src = data + off * w;
             }
-            col.hold_data = std::make_shared<DBuf>(rt, bytes > 0 ? bytes : 8);
-            if (bytes)
-                KRV_CUDA(cudaMemcpyAsync(col.hold_data->get(), src, bytes, cudaMemcpyHostToDevice, rt->stream));
-            col.data = col.hold_data->get();
+            const uint8_t *in_place = mode == HostRead::InPlace ? mapped_host(src, bytes) : nullptr;
+            if (in_place) {
+                col.data = in_place;
+                rt->host_borrowed = true;
+            } else {
+                col.hold_data = std::make_shared<DBuf>(rt, bytes > 0 ? bytes : 8);
+                if (bytes) {
+                    KRV_CUDA(cudaMemcpyAsync(col.hold_data->get(), src, bytes, cudaMemcpyHostToDevice, rt->stream));
+                    if (page_locked(src)) rt->host_borrowed = true;
+                }
+                col.data = col.hold_data->get();
+            }
             if (valid) {
                 const int64_t first = off / 8, last = (off + b.rows + 7) / 8;
                 const size_t vb = (size_t)(last - first);
                 col.hold_valid = std::make_shared<DBuf>(rt, vb > 0 ? vb : 8);
-                if (vb)
+                if (vb) {
                     KRV_CUDA(cudaMemcpyAsync(col.hold_valid->get(), valid + first, vb, cudaMemcpyHostToDevice,
                                              rt->stream));
+                    if (page_locked(valid + first)) rt->host_borrowed = true;
+                }
                 col.valid = static_cast<const uint8_t *>(col.hold_valid->get());
                 col.valid_off = off % 8;
             }
@@ -261,8 +303,8 @@ static DevBatch import_impl(Runtime *rt, const ArrowArray *arr, const ArrowSchem
     return b;
 }
 
-DevBatch import_host(Runtime *rt, const ArrowArray *arr, const ArrowSchema *schema) {
-    return import_impl<false>(rt, arr, schema);
+DevBatch import_host(Runtime *rt, const ArrowArray *arr, const ArrowSchema *schema, HostRead mode) {
+    return import_impl<false>(rt, arr, schema, mode);
 }
 
 DevBatch import_device(Runtime *rt, const ArrowDeviceArray *arr, const ArrowSchema *schema) {

@@ -602,6 +602,7 @@ class StarPipeline {
     }
 
     krv_star_counters counters() const { return counters_; }
+    bool fused() const { return spec_.mode == KRV_STAR_FUSED; }
 
   private:
     Runtime *rt_;
@@ -634,6 +635,7 @@ void star_probe(StarPipeline *s, const DevBatch &fact) { s->probe(fact); }
 DevBatch star_result(StarPipeline *s) { return s->result(); }
 void star_reset(StarPipeline *s) { s->reset(); }
 krv_star_counters star_counters(const StarPipeline *s) { return s->counters(); }
+bool star_fused(const StarPipeline *s) { return s->fused(); }
 void star_destroy(StarPipeline *s) { delete s; }
 
 }  // namespace krv

@@ -78,3 +78,43 @@ def test_star_same_alone_and_after_reset(kb, rt):
     b = dict(zip(second["attr"], second["sum"]))
     for k in a:
         assert rel_err(a[k], b[k]) <= FLOAT_TOL
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_star_host_batches(kb, rt, oracle, pinned):
+    """Host Arrow batches through krv_star_build / krv_star_probe: page-locked
+    columns are read in place by the kernels, pageable ones are copied; both
+    give the oracle's answer, and the caller may overwrite its buffers as soon
+    as the calls return."""
+    import pyarrow as pa
+    import torch
+    W = importlib.import_module("krishiv-engine_b200.workloads")
+    data = W.star(rt, scale=0.01)
+    torch.cuda.synchronize()
+    passed, joined, want, _ = oracle_star(oracle, data, 0)
+    keep = []
+
+    def host(cols):
+        arrays = []
+        for name, t, _ in cols:
+            h = torch.empty(t.shape, dtype=t.dtype, pin_memory=pinned)
+            h.copy_(t)
+            keep.append(h)
+            arrays.append(pa.array(h.numpy()))
+        return pa.RecordBatch.from_arrays(arrays, names=[n for n, _, _ in cols])
+
+    fact, dim_a, dim_b = host(data.fact), host(data.dim_a), host(data.dim_b)
+    s = kb.StarPipeline(rt, kb.star_spec(7, 7, group_by=0, mode=kb.STAR_FUSED))
+    s.build(dim_a, dim_b)
+    half = data.fact_rows // 2
+    for lo, hi in ((0, half), (half, data.fact_rows)):
+        s.probe(fact.slice(lo, hi - lo))
+    for h in keep:  # the library no longer reads the caller's buffers
+        h.fill_(-1)
+    out = s.result()
+    c = s.counters()
+    assert c["passed_filters"] == passed and c["joined_rows"] == joined
+    got = dict(zip(out.column(0).to_pylist(), out.column(1).to_pylist()))
+    assert sorted(got) == sorted(want)
+    for k, (ws, _) in want.items():
+        assert rel_err(got[k], ws) <= FLOAT_TOL, (k, got[k], ws)
