@@ -29,7 +29,6 @@ multi-threaded over all host cores) on a bounded sample of the same workload.
 from __future__ import annotations
 
 import argparse
-import ctypes as C
 import importlib
 import json
 import os
@@ -116,18 +115,26 @@ def dist_init(n_gpus):
     return rank, world, local, pg
 
 
+def star_config(scale, fact_scale):
+    """The star workload's description, the same for both arms."""
+    nf = int(300_000_000 * fact_scale)
+    return {"workload": "star join + runtime Bloom filters + GROUP BY attr SUM(price*(1-discount))",
+            "fact_rows_per_gpu": nf, "dim_a_rows": int(20_000_000 * scale), "dim_b_rows": int(1_000_000 * scale),
+            "selectivity": "5% per dimension", "groups": 25,
+            "l2": f"inputs ({nf * 32 / 1e9:.1f} GB per GPU) larger than L2; no flush"}
+
+
 def barrier(pg):
     if pg is not None:
         pg.barrier()
 
 
 def max_over_ranks(pg, value, device):
-    if pg is None:
-        return value
-    import torch
-    t = torch.tensor([value], dtype=torch.float64, device=device)
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
+    return _shard().max_over_ranks(pg, value, device)
+
+
+def _shard():
+    return importlib.import_module("krishiv-engine_b200.shard")
 
 
 # ---- the CPU baseline (the oracle's multi-threaded restatement) ---------------------------
@@ -136,39 +143,17 @@ def cpu_star(scale, sample_rows, threads, seed=None):
     `sample_rows` fact rows (dimensions at full size); returns the whole-query
     rate extrapolated to the full fact table (build time + full probe)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
     import oracle as O
     W = importlib.import_module("krishiv-engine_b200.workloads")
     seed = W.STAR_SEED if seed is None else seed
-    nf, na, nb = int(300_000_000 * scale), int(20_000_000 * scale), int(1_000_000 * scale)
+    nf = int(300_000_000 * scale)
     s = min(sample_rows, nf)
-    L = O.lib()
-    fk_a, _ = O.gen_column(0, seed, 1, s, lo=0, hi=na - 1)
-    fk_b, _ = O.gen_column(0, seed, 2, s, lo=0, hi=nb - 1)
-    price, _ = O.gen_column(0, seed, 3, s, lo=1000, hi=10_000_000)
-    disc, _ = O.gen_column(2, seed, 4, s, x0=0.0, x1=0.1)
-    dims = []
-    for base, n in ((10, na), (20, nb)):
-        key, _ = O.gen_column(3, seed + base, base + 1, n, lo=0, hi=n)
-        pred, _ = O.gen_column(1, seed, base + 2, n, lo=0, hi=19)
-        attr, _ = O.gen_column(1, seed, base + 3, n, lo=0, hi=24)
-        dims.append((key, pred, attr))
-    vp, i64, i32, dbl = C.c_void_p, C.c_int64, C.c_int32, C.c_double
-    L.orc_star_query.restype = i64
-    L.orc_star_query.argtypes = [vp, vp, vp, i64, i32, vp, vp, vp, i64, i32, vp, vp, vp, vp, i64, i32, i32, i32,
-                                 vp, vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(dbl), C.POINTER(dbl)]
-    out_sum = np.zeros(4096)
-    out_cnt = np.zeros(4096, dtype=np.int64)
-    passed, joined, tb, tp = i64(), i64(), dbl(), dbl()
-    (ka, pa_, aa), (kb_, pb, ab) = dims
-    L.orc_star_query(ka.ctypes.data, pa_.ctypes.data, aa.ctypes.data, na, 7, kb_.ctypes.data, pb.ctypes.data,
-                     ab.ctypes.data, nb, 7, fk_a.ctypes.data, fk_b.ctypes.data, price.ctypes.data,
-                     disc.ctypes.data, s, 0, threads, 1, out_sum.ctypes.data, out_cnt.ctypes.data, C.byref(passed),
-                     C.byref(joined), C.byref(tb), C.byref(tp))
-    probe_rate = s / tp.value
-    whole = tb.value + nf / probe_rate
-    return {"value": nf / whole / 1e6, "build_s": tb.value, "probe_rows_per_s": probe_rate, "sample_rows": s,
-            "threads": threads, "groups": int((out_cnt > 0).sum()), "joined": joined.value}
+    fact, dims = O.star_inputs(scale, seed, fact_rows=s, pred=W.PRED_VALUE)
+    groups, passed, joined, tb, tp = O.star_query(fact, dims, pred=W.PRED_VALUE, threads=threads)
+    probe_rate = s / tp
+    whole = tb + nf / probe_rate
+    return {"value": nf / whole / 1e6, "build_s": tb, "probe_rows_per_s": probe_rate, "sample_rows": s,
+            "threads": threads, "groups": len(groups), "joined": joined}
 
 
 # ---- workloads on the GPU ----------------------------------------------------------------
@@ -176,7 +161,8 @@ def run_star(args, kb, W, rt, rank, world, pg, device):
     import torch
     stream = torch.cuda.current_stream()
     fs = args.fact_scale if args.fact_scale is not None else args.scale
-    data = W.star(rt, scale=args.scale, fact_row0=rank * int(300_000_000 * fs), fact_scale=fs)
+    row0, _ = _shard().weak_shard(int(300_000_000 * fs), rank)
+    data = W.star(rt, scale=args.scale, fact_row0=row0, fact_scale=fs)
     torch.cuda.synchronize()
     dim_a, dim_b, fact = kb.DeviceBatch(data.dim_a), kb.DeviceBatch(data.dim_b), kb.DeviceBatch(data.fact)
 
@@ -222,6 +208,10 @@ def run_star(args, kb, W, rt, rank, world, pg, device):
     ms_max = max_over_ranks(pg, ms, device)
     counters = fused.counters()
     result = fused.result()
+    # Each rank holds the groups of its own fact rows; the job's answer is
+    # their merge (a gather of a few groups per rank).
+    partial = {int(g): (float(v), 0) for g, v in zip(result.column(0).to_pylist(), result.column(1).to_pylist())}
+    merged = _shard().all_merge_groups(pg, partial) if pg is not None else partial
     plain = make(kb.STAR_PLAIN)
     plain_ms, _ = timed(plain, max(2, args.steps // 2), 1)
     plain_ms = max_over_ranks(pg, plain_ms, device)
@@ -255,10 +245,9 @@ def run_star(args, kb, W, rt, rank, world, pg, device):
         "vs_baseline": None,
         "dtype": "int64 keys, float64 sums",
         "data": "synthetic (seeded counter-based generators on the device)",
-        "config": {"workload": "star join + runtime Bloom filters + GROUP BY attr SUM(price*(1-discount))",
-                   "fact_rows_per_gpu": nf, "dim_a_rows": data.dim_a_rows, "dim_b_rows": data.dim_b_rows,
-                   "selectivity": "5% per dimension", "groups": 25, "mode": "fused (batched) pipeline",
-                   "l2": "inputs (9.6 GB per GPU) larger than L2; no flush"},
+        "config": star_config(args.scale, fs),
+        "mode": "fused (batched) pipeline",
+        "groups": len(merged),
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": "star_scan_kernel + star_join_kernel (fact probe)",
                      "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
@@ -445,11 +434,12 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=20_000_000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    rank, world, local, pg = dist_init(args.gpus)
     threads = os.cpu_count() or 1
 
     if args.impl == "reference":
-        if rank != 0:
+        # The reference's CPU operators on the host cores: rank 0 alone works
+        # (no process group; the other ranks exit at once).
+        if int(os.environ.get("RANK", "0")) != 0:
             return
         steps = []
         info = None
@@ -458,10 +448,9 @@ def main():
             steps.append(info["value"])
         v = statistics.median(steps[args.warmup:])
         line = {"impl": "reference", "metric": "star join+agg probe Mrows/s (fact rows per second, whole query)",
-                "value": v, "unit": "Mrows/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+                "value": v, "unit": "Mrows/s", "n_gpus": args.gpus, "device": "host CPU cores", "steps": args.steps, "warmup": args.warmup,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "config": {"workload": "star join + runtime Bloom filters + GROUP BY attr SUM(price*(1-discount))",
-                           "fact_rows": int(300_000_000 * args.scale)},
+                "config": star_config(args.scale, args.fact_scale if args.fact_scale is not None else args.scale),
                 "cpu_baseline": {"value": v, "unit": "Mrows/s", "cores": threads, "kind": "port",
                                  "sample": f"full dimensions, first {info['sample_rows']} fact rows per step, "
                                            "whole-query rate extrapolated (build + full probe)"},
@@ -469,6 +458,7 @@ def main():
         print(json.dumps(line))
         return
 
+    rank, world, local, pg = dist_init(args.gpus)
     import torch
     torch.cuda.set_device(local)
     device = local

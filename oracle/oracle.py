@@ -308,3 +308,39 @@ def zipf_cdf(s, n):
     cdf = np.empty(n, dtype=np.float64)
     lib().orc_zipf_cdf(s, n, cdf.ctypes.data)
     return cdf
+
+
+def star_inputs(scale, seed, fact_row0=0, fact_rows=None, pred=7):
+    """The star query's columns (the device generators' functions): fact rows
+    [fact_row0, fact_row0 + fact_rows) and both dimensions in full."""
+    nf, na, nb = int(300_000_000 * scale), int(20_000_000 * scale), int(1_000_000 * scale)
+    n = nf if fact_rows is None else fact_rows
+    r0 = dict(row0=fact_row0)
+    fact = (gen_column(0, seed, 1, n, lo=0, hi=na - 1, **r0)[0], gen_column(0, seed, 2, n, lo=0, hi=nb - 1, **r0)[0],
+            gen_column(0, seed, 3, n, lo=1000, hi=10_000_000, **r0)[0], gen_column(2, seed, 4, n, x0=0.0, x1=0.1, **r0)[0])
+    dims = []
+    for base, m in ((10, na), (20, nb)):
+        dims.append((gen_column(3, seed + base, base + 1, m, lo=0, hi=m)[0], gen_column(1, seed, base + 2, m, lo=0, hi=19)[0],
+                     gen_column(1, seed, base + 3, m, lo=0, hi=24)[0]))
+    return fact, dims
+
+
+def star_query(fact, dims, pred=7, group_by=0, threads=1, use_filters=True):
+    """orc_star_query: {group: (sum, count)}, rows passing the filters, joined
+    rows, build seconds, probe seconds."""
+    L = lib()
+    vp, i64, i32, dbl = C.c_void_p, C.c_int64, C.c_int32, C.c_double
+    L.orc_star_query.restype = i64
+    L.orc_star_query.argtypes = [vp, vp, vp, i64, i32, vp, vp, vp, i64, i32, vp, vp, vp, vp, i64, i32, i32, i32,
+                                 vp, vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(dbl), C.POINTER(dbl)]
+    fk_a, fk_b, price, disc = fact
+    (ka, pa, aa), (kb, pb, ab) = dims
+    out_sum = np.zeros(4096)
+    out_cnt = np.zeros(4096, dtype=np.int64)
+    passed, joined, tb, tp = i64(), i64(), dbl(), dbl()
+    L.orc_star_query(ka.ctypes.data, pa.ctypes.data, aa.ctypes.data, len(ka), pred, kb.ctypes.data, pb.ctypes.data,
+                     ab.ctypes.data, len(kb), pred, fk_a.ctypes.data, fk_b.ctypes.data, price.ctypes.data,
+                     disc.ctypes.data, len(fk_a), group_by, threads, 1 if use_filters else 0, out_sum.ctypes.data,
+                     out_cnt.ctypes.data, C.byref(passed), C.byref(joined), C.byref(tb), C.byref(tp))
+    groups = {int(g): (float(out_sum[g]), int(out_cnt[g])) for g in np.nonzero(out_cnt)[0]}
+    return groups, passed.value, joined.value, tb.value, tp.value
