@@ -321,6 +321,121 @@ def run_star_e2e(args, kb, W, rt, data, pg, device):
             "timing": "host wall clock around synchronous C-ABI calls"}
 
 
+def run_serve(args, kb, W, rt, rank, world, pg, device):
+    """The served request stream: join + grouped aggregate requests against
+    resident tables, batched (ticks over a device work queue) against plain
+    (one request at a time through the operators). Closed loop (every request
+    queued at once) gives each mode's capacity; open loop (Poisson arrivals)
+    at equal offered loads gives p50 / p99 latency."""
+    import numpy as np
+    import torch
+    temps = W.serve_templates(rt, args.templates, scale=args.scale)
+    torch.cuda.synchronize()
+    tables_b = [kb.DeviceBatch(t.build) for t in temps]
+    probes = [kb.DeviceBatch(t.probe) for t in temps]
+    rows_of = np.array([t.probe_rows for t in temps], dtype=np.float64)
+
+    def server(mode):
+        s = kb.Server(rt, kb.server_options(mode=mode, tick_rows=args.tick_rows,
+                                            hbm_budget_bytes=args.serve_budget))
+        tids = [s.add_table(tb) for tb in tables_b]
+        torch.cuda.synchronize()
+        return s, tids
+
+    def stream(mode, arrivals, which, warm=0):
+        s, tids = server(mode)
+        for j in range(min(warm, len(temps))):  # warm the tables and the tuner
+            s.submit(tids[j], probes[j])
+        while s.step(wait=True) > 0 or s.poll() is not None:
+            while s.poll() is not None:
+                pass
+        n = len(arrivals)
+        done = np.full(n, np.nan)
+        ids = {}
+        i = 0
+        t0 = time.perf_counter()
+        finished = 0
+        while finished < n:
+            now = time.perf_counter() - t0
+            while i < n and arrivals[i] <= now:
+                ids[s.submit(tids[which[i]], probes[which[i]])] = i
+                i += 1
+            left = s.step(wait=False)
+            while True:
+                p = s.poll()
+                if p is None:
+                    break
+                rid, st, _ = p
+                if st != kb.OK:
+                    raise RuntimeError(f"request failed with status {st}")
+                done[ids.pop(rid)] = time.perf_counter() - t0
+                finished += 1
+            if left == 0 and i < n:
+                time.sleep(max(0.0, min(arrivals[i] - (time.perf_counter() - t0), 0.001)))
+        elapsed = np.nanmax(done) - arrivals[0]
+        lat = (done - arrivals) * 1e3
+        stats = s.stats()
+        s.close()
+        return {"requests": n, "elapsed_s": float(elapsed), "requests_per_s": n / elapsed,
+                "Mrows_per_s": float(rows_of[which].sum() / elapsed / 1e6),
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)), "stats": stats}
+
+    n = args.requests
+    zero, which = W.serve_arrivals(n, 0.0, len(temps))
+    zero = np.zeros(n)
+    with Clocks(device) as clk:
+        cap_b = stream(kb.SERVE_BATCHED, zero, which, warm=len(temps))
+        cap_p = stream(kb.SERVE_PLAIN, zero[: args.plain_requests], which[: args.plain_requests], warm=2)
+        load = args.serve_load
+        rate = load * cap_p["requests_per_s"]
+        arr, wh = W.serve_arrivals(args.plain_requests, rate, len(temps))
+        at_plain_p = stream(kb.SERVE_PLAIN, arr, wh, warm=2)
+        at_plain_b = stream(kb.SERVE_BATCHED, arr, wh, warm=len(temps))
+        rate_b = load * cap_b["requests_per_s"]
+        arr_b, wh_b = W.serve_arrivals(n, rate_b, len(temps))
+        at_batched = stream(kb.SERVE_BATCHED, arr_b, wh_b, warm=len(temps))
+    # the same request alone and in the mix
+    s, tids = server(kb.SERVE_BATCHED)
+    j = int(which[0])
+    rid = s.submit(tids[j], probes[j])
+    while s.step(wait=True) > 0:
+        pass
+    alone = None
+    while (p := s.poll()) is not None:
+        alone = {int(a): (int(b), int(c)) for a, b, c in zip(*(t.cpu().tolist() for t in p[2].columns))} if p[2].rows else {}
+    mix_ids = [s.submit(tids[int(w)], probes[int(w)]) for w in which[:64]]
+    first = mix_ids[0]
+    in_mix = None
+    while s.step(wait=True) > 0 or in_mix is None:
+        while (p := s.poll()) is not None:
+            if p[0] == first:
+                in_mix = {int(a): (int(b), int(c)) for a, b, c in zip(*(t.cpu().tolist() for t in p[2].columns))} \
+                    if p[2].rows else {}
+    s.close()
+    peak, kind = hbm_peak()
+    alg = 16.0 * cap_b["Mrows_per_s"] * 1e6 / 1e9
+    return {
+        "metric": "served join+agg requests: probe rows/s (closed loop) and p50/p99 latency (open loop)",
+        "value": cap_b["Mrows_per_s"], "unit": "Mrows/s", "n_gpus": world, "steps": n, "warmup": len(temps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded counter-based generators on the device)",
+        "config": {"workload": "SELECT t.g, SUM(p.x), COUNT(*) FROM p JOIN t USING (k) GROUP BY t.g, request stream",
+                   "templates": len(temps), "requests": n, "build_rows": f"log-uniform [1e3, {5e7 * args.scale:.0f}]",
+                   "probe_rows": "10 x build", "groups": "log-uniform [10, 1e6]", "match": "uniform [0.1, 1.0]",
+                   "tick_rows": args.tick_rows, "offered_load": load,
+                   "l2": "templates (probe inputs several GB) larger than L2; no flush"},
+        "batched_capacity": cap_b, "plain_capacity": cap_p,
+        "capacity_ratio": cap_b["requests_per_s"] / cap_p["requests_per_s"],
+        "open_loop_at_plain_load": {"requests_per_s_offered": rate, "plain": at_plain_p, "batched": at_plain_b},
+        "open_loop_at_batched_load": {"requests_per_s_offered": rate_b, "batched": at_batched},
+        "same_alone_and_in_mix": alone == in_mix,
+        "roofline": {"bound": "hbm", "achieved": alg, "peak": peak, "peak_source": kind, "unit": "GB/s",
+                     "frac": alg / peak, "traffic": None,
+                     "note": "16 B (k, x) per probe row over the closed-loop batched run"},
+        "clocks": clk.summary(),
+    }
+
+
 def profile_traffic(name, rows):
     """DRAM bytes (read + write) of one launch of `name` over `rows` fact
     rows, from the committed ncu summary (profiles/<name>_dram.md, line
@@ -425,13 +540,19 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["star", "join", "agg"], default="star")
+    ap.add_argument("--workload", choices=["star", "join", "agg", "serve"], default="star")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--fact-scale", type=float, default=None,
                     help="size the fact table alone (profiling small cases with full dimensions)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=20_000_000)
+    ap.add_argument("--requests", type=int, default=2000, help="serve: requests per batched run")
+    ap.add_argument("--plain-requests", type=int, default=400, help="serve: requests per plain run")
+    ap.add_argument("--templates", type=int, default=32, help="serve: request templates")
+    ap.add_argument("--tick-rows", type=int, default=16 << 20, help="serve: probe rows per tick")
+    ap.add_argument("--serve-budget", type=int, default=8 << 30, help="serve: HBM budget of running requests")
+    ap.add_argument("--serve-load", type=float, default=0.7, help="serve: offered load / capacity")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     threads = os.cpu_count() or 1
@@ -465,7 +586,7 @@ def main():
     kb = importlib.import_module("krishiv-engine_b200")
     W = importlib.import_module("krishiv-engine_b200.workloads")
     rt = kb.Runtime.on_torch_stream(local)
-    runner = {"star": run_star, "join": run_join, "agg": run_agg}[args.workload]
+    runner = {"star": run_star, "join": run_join, "agg": run_agg, "serve": run_serve}[args.workload]
     out = runner(args, kb, W, rt, rank, world, pg, device)
     if rank == 0 and args.workload == "star" and not args.no_cpu:
         c = cpu_star(args.scale, args.cpu_sample, threads)

@@ -350,6 +350,70 @@ typedef struct {
 krv_status krv_gen_fill(krv_runtime *rt, const krv_gen_spec *spec, int64_t n, void *out,
                         void *out_valid);
 
+/* ---- request server: batched and served join + aggregate -----------------
+ * SELECT t.g, SUM(p.x), COUNT(*) FROM p JOIN t ON p.k = t.k GROUP BY t.g for a
+ * stream of probe requests p against build tables t kept resident on the
+ * device. The reference runs each such query as a pipeline of its operators
+ * (HashJoinNode, join/mod.rs:1188-1211; HashAggregate, aggregate/sink.rs:181);
+ * the server is the batching/serving loop around them. Requests are admitted
+ * while the state of the running ones (48 bytes per group of their table)
+ * fits hbm_budget_bytes, the NeedMemory rule of operator.rs:314-330.
+ *  - KRV_SERVE_BATCHED: ticks of at most tick_rows probe rows from every
+ *    running request, one probe + aggregate launch per tick fed from a device
+ *    work queue, captured as a CUDA graph; large requests span ticks.
+ *  - KRV_SERVE_PLAIN: one request at a time through the join and aggregate
+ *    operators, one launch per operator step.
+ * Tables are (int64 key, int64 group) without NULL groups; requests are
+ * (int64 key, int64 value) device batches, NULL keys never match, values
+ * without NULLs. The caller keeps a request's buffers alive and unchanged until
+ * it is polled. Results are device batches (group int64, SUM int64, COUNT
+ * int64), one row per group with a match, in no particular order. */
+#define KRV_SERVE_BATCHED 0
+#define KRV_SERVE_PLAIN 1
+typedef struct {
+    int32_t mode;               /* KRV_SERVE_* */
+    int32_t autotune;           /* try the candidate kernel shapes on the first ticks */
+    int32_t ansi;               /* a SUM that leaves int64 fails its request */
+    int32_t max_tick_requests;  /* requests running at once (1..512; 0: 512) */
+    int64_t tick_rows;          /* probe rows per tick (0: 64 Mi) */
+    int64_t hbm_budget_bytes;   /* device bytes for running requests (0: no limit) */
+} krv_server_options;
+void krv_server_options_init(krv_server_options *o);
+typedef struct {
+    int64_t ticks;
+    int64_t requests_done;
+    int64_t rows_probed;
+    int64_t pending;        /* submitted, not admitted */
+    int64_t running;        /* admitted, rows left */
+    int64_t budget_in_use;  /* bytes of admitted requests' state */
+    int32_t tuned;          /* the autotuner has chosen */
+    int32_t threads;        /* chosen shape: threads per CTA */
+    int64_t item_rows;      /* rows per work item */
+    int32_t smem_groups;    /* shared-memory aggregation up to this many groups */
+    int32_t pad0;
+} krv_server_stats;
+typedef struct krv_server krv_server;
+krv_status krv_server_create(krv_runtime *rt, const krv_server_options *o, krv_server **out);
+/* Builds a resident table from columns key_column and group_column. */
+krv_status krv_server_add_table(krv_server *s, const struct ArrowDeviceArray *batch,
+                                const struct ArrowSchema *schema, int32_t key_column,
+                                int32_t group_column, int64_t *table_id);
+krv_status krv_server_drop_table(krv_server *s, int64_t table_id);
+krv_status krv_server_submit(krv_server *s, int64_t table_id, const struct ArrowDeviceArray *probe,
+                             const struct ArrowSchema *schema, int32_t key_column,
+                             int32_t value_column, int64_t *request_id);
+/* Retires finished work and starts the next (a tick, or one plain request);
+ * with wait != 0 also waits for the oldest tick. *outstanding = requests not
+ * yet finished. */
+krv_status krv_server_step(krv_server *s, int32_t wait, int64_t *outstanding);
+/* KRV_OK with the next finished request (its status in *request_status; the
+ * result in out when that is KRV_OK, else out is left released), or
+ * KRV_FINISHED when no request has finished. */
+krv_status krv_server_poll(krv_server *s, int64_t *request_id, krv_status *request_status,
+                           struct ArrowDeviceArray *out, struct ArrowSchema *out_schema);
+krv_status krv_server_stats_get(const krv_server *s, krv_server_stats *out);
+void krv_server_destroy(krv_server *s);
+
 /* ---- grouped SUM/COUNT with no allocation ----------------------------------
  * No counterpart in the reference. For a caller that may not allocate device
  * memory where it calls (all of HBM is in its own accounted pool, or a

@@ -44,6 +44,7 @@ MAX_KEYS = 4
 MAX_OUT = 32
 MAX_AGGS = 32
 SCRATCH_MAX_GROUPS = 65536  # KRV_SCRATCH_MAX_GROUPS
+SERVE_BATCHED, SERVE_PLAIN = 0, 1
 
 
 class KrvError(RuntimeError):
@@ -137,6 +138,17 @@ class StarCounters(C.Structure):
                 ("fk_a_sectors", C.c_int64)]
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("autotune", C.c_int32), ("ansi", C.c_int32), ("max_tick_requests", C.c_int32),
+                ("tick_rows", C.c_int64), ("hbm_budget_bytes", C.c_int64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("ticks", C.c_int64), ("requests_done", C.c_int64), ("rows_probed", C.c_int64),
+                ("pending", C.c_int64), ("running", C.c_int64), ("budget_in_use", C.c_int64), ("tuned", C.c_int32),
+                ("threads", C.c_int32), ("item_rows", C.c_int64), ("smem_groups", C.c_int32), ("pad0", C.c_int32)]
+
+
 class GenSpec(C.Structure):
     _fields_ = [("kind", C.c_int32), ("column", C.c_uint32), ("seed", C.c_uint64), ("lo", C.c_int64),
                 ("hi", C.c_int64), ("x0", C.c_double), ("x1", C.c_double), ("null_fraction", C.c_double),
@@ -207,6 +219,18 @@ _SIGS = {
     "krv_star_counters_get": (C.c_int32, [C.c_void_p, C.POINTER(StarCounters)]),
     "krv_star_destroy": (None, [C.c_void_p]),
     "krv_gen_fill": (C.c_int32, [C.c_void_p, C.POINTER(GenSpec), C.c_int64, C.c_void_p, C.c_void_p]),
+    "krv_server_options_init": (None, [C.POINTER(ServerOptions)]),
+    "krv_server_create": (C.c_int32, [C.c_void_p, C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
+    "krv_server_add_table": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema), C.c_int32,
+                                         C.c_int32, C.POINTER(C.c_int64)]),
+    "krv_server_drop_table": (C.c_int32, [C.c_void_p, C.c_int64]),
+    "krv_server_submit": (C.c_int32, [C.c_void_p, C.c_int64, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema),
+                                      C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
+    "krv_server_step": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
+    "krv_server_poll": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                                    C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema)]),
+    "krv_server_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(ServerStats)]),
+    "krv_server_destroy": (None, [C.c_void_p]),
     "krv_agg_sum_i64_scratch": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_void_p]),
 }
@@ -746,3 +770,74 @@ def agg_sum_i64_scratch(keys, values, out_keys, out_sums, out_counts, out_info, 
     check(lib().krv_agg_sum_i64_scratch(keys.data_ptr() if n else None, values.data_ptr() if n else None, n, g,
                                         out_keys.data_ptr() if g else None, out_sums.data_ptr() if g else None,
                                         out_counts.data_ptr() if g else None, out_info.data_ptr(), stream))
+
+
+def server_options(**kw) -> ServerOptions:
+    o = ServerOptions()
+    lib().krv_server_options_init(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Server:
+    """Join + grouped aggregate requests against resident build tables
+    (krv_server_*): SELECT t.g, SUM(p.x), COUNT(*) FROM p JOIN t USING (k)
+    GROUP BY t.g. Requests are DeviceBatch probes; the server keeps them (and
+    so their tensors) until they are polled."""
+
+    def __init__(self, rt: Runtime, opts: ServerOptions = None):
+        self.rt = rt
+        h = C.c_void_p()
+        check(lib().krv_server_create(rt.h, C.byref(opts) if opts is not None else None, C.byref(h)))
+        self.h = h
+        self._inflight = {}
+
+    def add_table(self, db: DeviceBatch, key_column: int = 0, group_column: int = 1) -> int:
+        tid = C.c_int64()
+        check(lib().krv_server_add_table(self.h, C.byref(db.dev), C.byref(db.schema), key_column, group_column,
+                                         C.byref(tid)))
+        return tid.value
+
+    def drop_table(self, table_id: int):
+        check(lib().krv_server_drop_table(self.h, table_id))
+
+    def submit(self, table_id: int, db: DeviceBatch, key_column: int = 0, value_column: int = 1) -> int:
+        rid = C.c_int64()
+        check(lib().krv_server_submit(self.h, table_id, C.byref(db.dev), C.byref(db.schema), key_column, value_column,
+                                      C.byref(rid)))
+        self._inflight[rid.value] = db
+        return rid.value
+
+    def step(self, wait: bool = False) -> int:
+        n = C.c_int64()
+        check(lib().krv_server_step(self.h, 1 if wait else 0, C.byref(n)))
+        return n.value
+
+    def poll(self):
+        """(request id, status, DeviceResult or None) of the next finished
+        request, or None when none has finished."""
+        rid, st = C.c_int64(), C.c_int32()
+        dev, sch = ArrowDeviceArray(), ArrowSchema()
+        s = check(lib().krv_server_poll(self.h, C.byref(rid), C.byref(st), C.byref(dev), C.byref(sch)))
+        if s == FINISHED:
+            return None
+        self._inflight.pop(rid.value, None)
+        return rid.value, st.value, (DeviceResult(dev, sch) if st.value == OK else None)
+
+    def stats(self) -> Dict[str, int]:
+        c = ServerStats()
+        check(lib().krv_server_stats_get(self.h, C.byref(c)))
+        return {n: getattr(c, n) for n, _ in ServerStats._fields_ if n != "pad0"}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().krv_server_destroy(self.h)
+            self.h = None
+        self._inflight = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -37,6 +37,10 @@ struct krv_star {
     krv_runtime *owner;
     krv::StarPipeline *s = nullptr;
 };
+struct krv_server {
+    krv_runtime *owner;
+    krv::Server *s = nullptr;
+};
 
 namespace {
 
@@ -565,6 +569,110 @@ void krv_star_destroy(krv_star *s) {
     if (!s) return;
     krv::DeviceGuard g(&s->owner->rt);
     krv::star_destroy(s->s);
+    delete s;
+}
+
+// ---- request server -----------------------------------------------------------------
+void krv_server_options_init(krv_server_options *o) {
+    if (!o) return;
+    *o = krv_server_options{};
+    o->mode = KRV_SERVE_BATCHED;
+    o->autotune = 1;
+    o->ansi = 1;
+    o->max_tick_requests = 512;
+    o->tick_rows = 64ll << 20;
+    o->hbm_budget_bytes = 0;
+}
+krv_status krv_server_create(krv_runtime *rt, const krv_server_options *o, krv_server **out) {
+    return guard([&] {
+        need(rt, "runtime");
+        need(out, "out");
+        *out = nullptr;
+        krv_server_options opt;
+        if (o) opt = *o;
+        else krv_server_options_init(&opt);
+        krv::DeviceGuard g(&rt->rt);
+        auto h = std::make_unique<krv_server>();
+        h->owner = rt;
+        h->s = krv::make_server(&rt->rt, opt);
+        *out = h.release();
+        return KRV_OK;
+    });
+}
+krv_status krv_server_add_table(krv_server *s, const ArrowDeviceArray *batch, const ArrowSchema *schema,
+                                int32_t key_column, int32_t group_column, int64_t *table_id) {
+    return guard([&] {
+        need(s, "server");
+        need(table_id, "table_id");
+        krv::Runtime *rt = &s->owner->rt;
+        krv::DeviceGuard g(rt);
+        *table_id = krv::server_add_table(s->s, krv::import_device(rt, batch, schema), key_column, group_column);
+        return KRV_OK;
+    });
+}
+krv_status krv_server_drop_table(krv_server *s, int64_t table_id) {
+    return guard([&] {
+        need(s, "server");
+        krv::DeviceGuard g(&s->owner->rt);
+        krv::server_drop_table(s->s, table_id);
+        return KRV_OK;
+    });
+}
+krv_status krv_server_submit(krv_server *s, int64_t table_id, const ArrowDeviceArray *probe,
+                             const ArrowSchema *schema, int32_t key_column, int32_t value_column,
+                             int64_t *request_id) {
+    return guard([&] {
+        need(s, "server");
+        need(request_id, "request_id");
+        krv::Runtime *rt = &s->owner->rt;
+        krv::DeviceGuard g(rt);
+        *request_id = krv::server_submit(s->s, table_id, krv::import_device(rt, probe, schema), key_column,
+                                         value_column);
+        return KRV_OK;
+    });
+}
+krv_status krv_server_step(krv_server *s, int32_t wait, int64_t *outstanding) {
+    return guard([&] {
+        need(s, "server");
+        const int64_t n = krv::server_step(s->s, wait != 0);
+        if (outstanding) *outstanding = n;
+        return KRV_OK;
+    });
+}
+krv_status krv_server_poll(krv_server *s, int64_t *request_id, krv_status *request_status, ArrowDeviceArray *out,
+                           ArrowSchema *out_schema) {
+    return guard([&] {
+        need(s, "server");
+        need(request_id, "request_id");
+        need(request_status, "request_status");
+        need(out, "out");
+        need(out_schema, "out_schema");
+        out->array.release = nullptr;
+        out_schema->release = nullptr;
+        krv::Runtime *rt = &s->owner->rt;
+        krv::DeviceGuard g(rt);
+        DevBatch b;
+        int64_t id = 0;
+        krv_status st = KRV_OK;
+        if (!krv::server_poll(s->s, id, st, b)) return (krv_status)KRV_FINISHED;
+        *request_id = id;
+        *request_status = st;
+        if (st == KRV_OK) krv::export_device(rt, b, out, out_schema);
+        return (krv_status)KRV_OK;
+    });
+}
+krv_status krv_server_stats_get(const krv_server *s, krv_server_stats *out) {
+    return guard([&] {
+        need(s, "server");
+        need(out, "out");
+        *out = krv::server_stats(s->s);
+        return KRV_OK;
+    });
+}
+void krv_server_destroy(krv_server *s) {
+    if (!s) return;
+    krv::DeviceGuard g(&s->owner->rt);
+    krv::server_destroy(s->s);
     delete s;
 }
 

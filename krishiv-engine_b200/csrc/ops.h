@@ -165,6 +165,17 @@ krv_star_counters star_counters(const StarPipeline *s);
 bool star_fused(const StarPipeline *s);  // KRV_STAR_FUSED plan
 void star_destroy(StarPipeline *s);
 
+// ---- request server (serve.cu) -------------------------------------------------------
+class Server;
+Server *make_server(Runtime *rt, const krv_server_options &o);
+int64_t server_add_table(Server *s, const DevBatch &b, int key_col, int group_col);
+void server_drop_table(Server *s, int64_t id);
+int64_t server_submit(Server *s, int64_t table, const DevBatch &b, int key_col, int value_col);
+int64_t server_step(Server *s, bool wait);
+bool server_poll(Server *s, int64_t &id, krv_status &status, DevBatch &out);
+krv_server_stats server_stats(const Server *s);
+void server_destroy(Server *s);
+
 // ---- generators ------------------------------------------------------------------
 void gen_fill(Runtime *rt, const krv_gen_spec &spec, int64_t n, void *out, void *out_valid);
 

@@ -13,6 +13,13 @@ Shapes (rows at scale 1.0):
   agg:    100,000,000 rows {k: Zipf(1.1) over 1,000,000 values, dec
           decimal(15,2) unscaled uniform [100, 1e7], f float64 uniform [0, 1),
           q int32 uniform [1, 50]; 2% NULLs per value column}.
+  serve:  request templates, each a resident build table {k: a permutation
+          of [0, nb) (unique), g int64 uniform [0, G)} and a probe of 10 * nb
+          rows {k: with probability r uniform over the build keys, else
+          uniform over the disjoint range [2^40, 2^41); x int64 uniform
+          [-1e9, 1e9]}; nb log-uniform over [1e3, 5e7 * scale], G log-uniform
+          over [10, 1e6] (at most nb), r uniform over [0.1, 1.0]; requests
+          pick templates uniformly and arrive as a Poisson process.
 """
 from __future__ import annotations
 
@@ -22,6 +29,7 @@ from dataclasses import dataclass
 STAR_SEED = 0x4B52560003
 JOIN_SEED = 0x4B52560001
 AGG_SEED = 0x4B52560002
+SERVE_SEED = 0x4B52560005
 PRED_VALUE = 7
 
 
@@ -93,3 +101,54 @@ def agg(rt, scale: float = 1.0, seed: int = AGG_SEED, domain: int = 1_000_000):
     f, fv = _col(rt, n, torch.float64, kb.GEN_UNIT_F64, seed, 3, x0=0.0, x1=1.0, null_fraction=0.02)
     q, qv = _col(rt, n, torch.int32, kb.GEN_UNIFORM_I32, seed, 4, lo=1, hi=50, null_fraction=0.02)
     return [("k", k, None), ("dec", dec, dv, pa.decimal64(15, 2)), ("f", f, fv), ("q", q, qv)]
+
+
+@dataclass
+class ServeTemplate:
+    build: list        # [(name, tensor, valid)]: k, g
+    probe: list        # [(name, tensor, valid)]: k, x
+    build_rows: int
+    probe_rows: int
+    groups: int        # G of the generator (distinct groups <= G)
+    match: float       # r
+
+
+def serve_templates(rt, count: int, scale: float = 1.0, seed: int = SERVE_SEED, max_build=None):
+    """`count` request templates of the served request stream (see the module
+    docstring); template j is generated from (seed, j) alone. `scale` scales
+    the largest build (5e7 rows); the smallest stays 1e3 rows."""
+    import math
+
+    import numpy as np
+    import torch
+    kb = _kb()
+    rng = np.random.default_rng(seed)
+    lo_b, hi_b = 1e3, max(1e3, 5e7 * scale)
+    if max_build is not None:
+        hi_b = min(hi_b, max_build)
+    out = []
+    for j in range(count):
+        nb = max(1, int(round(math.exp(rng.uniform(math.log(max(lo_b, 1.0)), math.log(max(hi_b, 2.0)))))))
+        G = max(1, min(nb, int(round(math.exp(rng.uniform(math.log(10), math.log(1e6)))))))
+        r = float(rng.uniform(0.1, 1.0))
+        npr = 10 * nb
+        sj = seed + 0x1000 * (j + 1)
+        k, _ = _col(rt, nb, torch.int64, kb.GEN_PERMUTATION, sj, 1, lo=0, hi=nb)
+        g, _ = _col(rt, nb, torch.int64, kb.GEN_UNIFORM_I64, sj, 2, lo=0, hi=G - 1)
+        kin, _ = _col(rt, npr, torch.int64, kb.GEN_UNIFORM_I64, sj, 3, lo=0, hi=nb - 1)
+        kout, _ = _col(rt, npr, torch.int64, kb.GEN_UNIFORM_I64, sj, 4, lo=1 << 40, hi=(1 << 41) - 1)
+        u, _ = _col(rt, npr, torch.int64, kb.GEN_UNIFORM_I64, sj, 5, lo=0, hi=999_999)
+        x, _ = _col(rt, npr, torch.int64, kb.GEN_UNIFORM_I64, sj, 6, lo=-1_000_000_000, hi=1_000_000_000)
+        pk = torch.where(u < int(r * 1_000_000), kin, kout)
+        del kin, kout, u
+        out.append(ServeTemplate([("k", k, None), ("g", g, None)], [("k", pk, None), ("x", x, None)], nb, npr, G, r))
+    return out
+
+
+def serve_arrivals(n: int, rate_per_s: float, templates: int, seed: int = SERVE_SEED):
+    """Poisson arrival times (seconds from 0) and the template of each of `n`
+    requests."""
+    import numpy as np
+    rng = np.random.default_rng(seed ^ 0x5EED)
+    gaps = rng.exponential(1.0 / rate_per_s, n) if rate_per_s > 0 else np.zeros(n)
+    return np.cumsum(gaps) - gaps[0], rng.integers(0, templates, n)
