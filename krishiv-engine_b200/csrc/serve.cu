@@ -46,6 +46,19 @@ constexpr int kMaxTickItems = 16384;
 constexpr int kSmemGroupsMax = 2048;  // shared-memory aggregation limit (48 KiB)
 constexpr unsigned long long kGroupEmpty = 0x8000000000000000ull;
 
+// How a resident table answers key -> group id:
+//  - kDirect: unique keys over a span of at most 4 x rows: gid at key - lo;
+//  - kRecords: unique keys: (key, gid) records at the join table's slot
+//    positions, probed in the same order, one 16-byte read per step;
+//  - kChains: duplicate keys: the join table's slots and newest-first chains.
+enum Layout : int32_t { kDirect = 0, kRecords = 1, kChains = 2 };
+
+struct Record {
+    long long key;
+    int32_t gid;   // -1: empty slot
+    int32_t pad;
+};
+
 struct TableView {
     const unsigned long long *slots;
     uint64_t mask;
@@ -53,6 +66,12 @@ struct TableView {
     uint64_t seed;
     const long long *keys;
     const int32_t *gid;
+    const Record *rec;       // kRecords
+    const int32_t *direct;   // kDirect
+    long long lo;            // kDirect: smallest key
+    unsigned long long span; // kDirect: largest key - lo
+    int32_t layout;
+    int32_t pad;
 };
 
 // One running request, as the tick kernels see it.
@@ -112,6 +131,44 @@ __device__ __forceinline__ uint32_t table_head(const TableView &t, long long k) 
     return kNoRow;
 }
 
+__device__ __forceinline__ int record_gid(const TableView &t, long long k) {
+    const uint64_t g = finalize(hash_word((uint64_t)k), t.seed);
+    uint64_t pos = g & t.mask;
+    for (uint64_t p = 0; p <= t.mask; p++) {
+        const longlong2 r = __ldg(reinterpret_cast<const longlong2 *>(t.rec + pos));
+        const int gid = (int)(int32_t)(r.y & 0xFFFFFFFFll);
+        if (gid < 0) return -1;
+        if (r.x == k) return gid;
+        pos = (pos + 1) & t.mask;
+    }
+    return -1;
+}
+
+__device__ __forceinline__ int direct_gid(const TableView &t, long long k) {
+    const unsigned long long off = (unsigned long long)(k - t.lo);
+    return off <= t.span ? __ldg(t.direct + off) : -1;
+}
+
+// Fills the records of a table with unique keys from its join slots.
+__global__ void records_kernel(const unsigned long long *slots, uint64_t n, const long long *keys,
+                               const int32_t *gid, Record *rec) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long s = slots[i];
+        Record r{0, -1, 0};
+        if (s) {
+            const uint32_t row = (uint32_t)(s & 0xFFFFFFFFull) - 1u;
+            r.key = keys[row];
+            r.gid = gid[row];
+        }
+        rec[i] = r;
+    }
+}
+
+__global__ void direct_kernel(const long long *keys, const int32_t *gid, int64_t n, long long lo, int32_t *direct) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        direct[(unsigned long long)(keys[i] - lo)] = gid[i];
+}
+
 __global__ void tick_init_kernel(TickDev d) {
     const TickHeader h = *d.hdr;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -164,6 +221,24 @@ __global__ void __launch_bounds__(THREADS) tick_probe_kernel(TickDev d) {
                 has[u] = r < end && (!R.kvalid || bit_get(R.kvalid, R.kvoff, r));
                 k[u] = has[u] ? __ldcs(R.k + r) : 0;
                 x[u] = has[u] ? __ldcs(R.x + r) : 0;
+            }
+            if (R.t.layout != kChains) {
+                int g[U];
+#pragma unroll
+                for (int u = 0; u < U; u++)
+                    g[u] = !has[u] ? -1 : R.t.layout == kDirect ? direct_gid(R.t, k[u]) : record_gid(R.t, k[u]);
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    if (g[u] < 0) continue;
+                    if (sm) {
+                        atomic_add_i128_from_i64(s_lo + g[u], s_hi + g[u], x[u]);
+                        atomicAdd(s_cnt + g[u], 1ull);
+                    } else {
+                        atomic_add_i128_from_i64(R.lo + g[u], R.hi + g[u], x[u]);
+                        atomicAdd(R.cnt + g[u], 1ull);
+                    }
+                }
+                continue;
             }
 #pragma unroll
             for (int u = 0; u < U; u++) row[u] = has[u] ? table_head(R.t, k[u]) : kNoRow;
@@ -286,6 +361,11 @@ struct ResidentTable {
     std::unique_ptr<HashJoin> join;  // inner join on key; arena (key, group)
     DBuf gid;                        // dense group id per build row
     DBuf gkeys;                      // group value per dense id
+    DBuf rec;                        // kRecords: (key, gid) per join slot
+    DBuf direct;                     // kDirect: gid per key - lo
+    int32_t layout = kChains;
+    long long lo = 0;
+    unsigned long long span = 0;
     int64_t rows = 0;
     int64_t ngroups = 0;
 };
@@ -379,9 +459,42 @@ class Server {
             check_launch("gdir_lookup_kernel");
         }
         t->ngroups = (int64_t)read_scalar<unsigned long long>(rt_, count.get());
+        choose_layout(*t);
         const int64_t id = next_table_++;
         tables_[id] = t;
         return id;
+    }
+
+    // Unique non-NULL keys get a one-read lookup: a direct array when the keys
+    // are dense (span at most 4 x rows), else records at the slot positions.
+    void choose_layout(ResidentTable &t) {
+        HashJoin &j = *t.join;
+        const int64_t rows = t.rows;
+        const auto c = j.counters();
+        t.layout = kChains;
+        if (rows <= 0 || j.indexed_rows() != rows || c.build_keys != rows) return;
+        const __int128 span = (__int128)j.key_hi() - (__int128)j.key_lo();
+        const long long *keys = static_cast<const long long *>(j.arena().cols[0].data);
+        if (span >= 0 && span < (__int128)4 * rows && span < ((__int128)1 << 31)) {
+            t.lo = j.key_lo();
+            t.span = (unsigned long long)span;
+            t.direct = DBuf(rt_, ((size_t)span + 1) * 4);
+            KRV_CUDA(cudaMemsetAsync(t.direct.get(), 0xFF, ((size_t)span + 1) * 4, rt_->stream));
+            direct_kernel<<<grid_for(rt_, rows, 256, 8), 256, 0, rt_->stream>>>(keys, t.gid.as<int32_t>(), rows, t.lo,
+                                                                               t.direct.as<int32_t>());
+            rt_->launches++;
+            check_launch("direct_kernel");
+            t.layout = kDirect;
+            return;
+        }
+        const auto tv = j.table_dev();
+        const uint64_t n = tv.mask + 1;
+        t.rec = DBuf(rt_, n * sizeof(Record));
+        records_kernel<<<grid_for(rt_, (int64_t)n, 256, 8), 256, 0, rt_->stream>>>(tv.slots, n, keys,
+                                                                                  t.gid.as<int32_t>(), t.rec.as<Record>());
+        rt_->launches++;
+        check_launch("records_kernel");
+        t.layout = kRecords;
     }
 
     void drop_table(int64_t id) {
@@ -582,7 +695,7 @@ class Server {
         d.kvoff = r.k.valid_off;
         d.x = static_cast<const long long *>(r.x.data);
         d.t = TableView{tv.slots, tv.mask, tv.next, tv.seed, static_cast<const long long *>(t.join->arena().cols[0].data),
-                        t.gid.as<int32_t>()};
+                        t.gid.as<int32_t>(), t.rec.as<Record>(), t.direct.as<int32_t>(), t.lo, t.span, t.layout, 0};
         d.lo = r.acc.as<unsigned long long>();
         d.hi = reinterpret_cast<long long *>(d.lo + ng);
         d.cnt = d.lo + 2 * ng;

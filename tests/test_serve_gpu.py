@@ -56,22 +56,26 @@ def run_all(kb, srv, submits):
 
 
 def make_case(kb, rt, seed=5):
-    """Three tables (few groups, many groups, duplicate keys) and 24 probes
-    of uneven sizes, some with NULL keys, one empty."""
-    import torch
+    """Five tables and 24 probes of uneven sizes, some with NULL keys, one
+    empty. The tables cover every lookup layout and both aggregations:
+    dense unique keys (direct array) with few and with many groups, sparse
+    unique keys (records) with many and with few groups, duplicate keys
+    (chains)."""
     rng = np.random.default_rng(seed)
     tables = []
-    specs = [(5000, 40), (20000, 6000), (3000, 300)]
+    specs = [(5000, 40), (20000, 6000), (3000, 300), (8000, 3000), (6000, 500)]
     for i, (nb, G) in enumerate(specs):
         if i == 2:  # duplicate keys: every key three times
             k = np.repeat(rng.permutation(nb // 3), 3).astype(np.int64)
+        elif i in (0, 3):  # dense keys
+            k = rng.permutation(nb).astype(np.int64) + 12345 - 4000 * i
         else:
             k = rng.permutation(nb).astype(np.int64) * 7 - 1000
         g = rng.integers(-(2**40), 2**40, G)[rng.integers(0, G, k.size)].astype(np.int64)
         tables.append((k, g))
     probes = []
     for j in range(24):
-        ti = j % 3
+        ti = j % 5
         bk = tables[ti][0]
         n = 0 if j == 5 else int(rng.integers(1, 60000))
         hit = rng.random(n) < rng.uniform(0.1, 1.0)
