@@ -156,6 +156,42 @@ def cpu_star(scale, sample_rows, threads, seed=None):
             "threads": threads, "groups": len(groups), "joined": joined}
 
 
+def cpu_join(scale, threads=1):
+    """The oracle's hash join (single thread) on the whole plain-join workload:
+    build + probe rows per second."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    W = importlib.import_module("krishiv-engine_b200.workloads")
+    nb, np_ = int(1_000_000 * scale), int(10_000_000 * scale)
+    bk, _ = O.gen_column(3, W.JOIN_SEED, 1, nb, lo=0, hi=nb)
+    pk, _ = O.gen_column(0, W.JOIN_SEED, 3, np_, lo=0, hi=2 * nb - 1)
+    t0 = time.perf_counter()
+    p, b = O.hash_join(0, [(bk, None)], [(pk, None)])
+    dt = time.perf_counter() - t0
+    return {"value": (nb + np_) / dt / 1e6, "rows_out": int(p.size), "seconds": dt}
+
+
+def cpu_agg(scale, sample):
+    """The oracle's grouped aggregate (single thread) over the first `sample`
+    rows of the aggregate workload, 15 aggregates: rows per second."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    W = importlib.import_module("krishiv-engine_b200.workloads")
+    n = min(sample, int(100_000_000 * scale))
+    seed = W.AGG_SEED
+    k, _ = O.gen_column(4, seed, 1, n, lo=0, hi=1_000_000, x0=1.1)
+    dec, dv = O.gen_column(0, seed, 2, n, lo=100, hi=10_000_000, null_fraction=0.02)
+    f, fv = O.gen_column(2, seed, 3, n, x0=0.0, x1=1.0, null_fraction=0.02)
+    q, qv = O.gen_column(1, seed, 4, n, lo=1, hi=50, null_fraction=0.02)
+    cols = [{"values": dec, "valid": dv, "type": O.T_DEC64, "precision": 15, "scale": 2},
+            {"values": f, "valid": fv, "type": O.T_F64}, {"values": q, "valid": qv, "type": O.T_I32}]
+    exprs = [(fn, c) for c in range(3) for fn in (O.SUM, O.COUNT, O.MIN, O.MAX, O.AVG)]
+    t0 = time.perf_counter()
+    O.hash_aggregate(k, None, cols, exprs)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt / 1e6, "rows": n, "seconds": dt}
+
+
 # ---- workloads on the GPU ----------------------------------------------------------------
 def run_star(args, kb, W, rt, rank, world, pg, device):
     import torch
@@ -471,11 +507,12 @@ def run_join(args, kb, W, rt, rank, world, pg, device):
     barrier(pg)
     launches0 = rt.launches
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record(stream)
-    for _ in range(args.steps):
-        j, r = step()
-    e.record(stream)
-    torch.cuda.synchronize()
+    with Clocks(device) as clk:
+        s.record(stream)
+        for _ in range(args.steps):
+            j, r = step()
+        e.record(stream)
+        torch.cuda.synchronize()
     ms = max_over_ranks(pg, s.elapsed_time(e) / args.steps, device)
     out_rows = r.rows
     alg = 16 * nb + 12 * np_ + 20 * out_rows
@@ -485,10 +522,16 @@ def run_join(args, kb, W, rt, rank, world, pg, device):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64 keys", "data": "synthetic",
             "config": {"workload": "inner join 1M build x 10M probe (50% match), output (k, v, w)",
-                       "build_rows": nb, "probe_rows": np_, "output_rows": out_rows},
+                       "build_rows": nb, "probe_rows": np_, "output_rows": out_rows,
+                       "l2": "inputs (136 MB) larger than L2; each step rebuilds the table"},
             "gpu_launches": rt.launches - launches0,
             "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "peak_source": kind,
-                         "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None}}
+                         "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None,
+                         "note": "whole step (build + probe); 16 B per build row, 12 B per probe row, 20 B per output row"},
+            "clocks": clk.summary(),
+            "cpu_baseline": None if args.no_cpu or rank != 0 else dict(
+                unit="Mrows/s", cores=1, kind="port", sample="the whole workload", **{
+                    k: v for k, v in cpu_join(args.scale).items() if k == "value"})}
 
 
 def run_agg(args, kb, W, rt, rank, world, pg, device):
@@ -506,7 +549,7 @@ def run_agg(args, kb, W, rt, rank, world, pg, device):
         a.finish()
         return a.result_device()
 
-    res = {}
+    res, clocks = {}, {}
     for mode, name in ((kb.MODE_SHARED, "shared"), (kb.MODE_GLOBAL, "global")):
         for _ in range(args.warmup):
             step(mode)
@@ -514,11 +557,13 @@ def run_agg(args, kb, W, rt, rank, world, pg, device):
         barrier(pg)
         launches0 = rt.launches
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record(stream)
-        for _ in range(args.steps):
-            r = step(mode)
-        e.record(stream)
-        torch.cuda.synchronize()
+        with Clocks(device) as clk:
+            s.record(stream)
+            for _ in range(args.steps):
+                r = step(mode)
+            e.record(stream)
+            torch.cuda.synchronize()
+        clocks[name] = clk.summary()
         res[name] = (max_over_ranks(pg, s.elapsed_time(e) / args.steps, device), rt.launches - launches0, r.rows)
     ms, launches, groups = res["shared"]
     alg = n * (8 + 8 + 8 + 4 + 3 / 8) + groups * 136
@@ -527,11 +572,17 @@ def run_agg(args, kb, W, rt, rank, world, pg, device):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int128/double-double",
             "data": "synthetic", "config": {"workload": "100M rows Zipf(1.1) over 1M keys, 15 aggregates",
-                                            "rows": n, "groups": groups},
+                                            "rows": n, "groups": groups,
+                                            "l2": "inputs (2.8 GB) larger than L2; no flush"},
             "gpu_launches": launches,
             "plain_global_table": {"ms_per_step": res["global"][0], "value": world * n / (res["global"][0] * 1e-3) / 1e6},
             "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "peak_source": kind,
-                         "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None}}
+                         "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None,
+                         "note": "whole step; 28.4 B per row (key, three value columns, three bitmaps) + 136 B per group"},
+            "clocks": clocks["shared"],
+            "cpu_baseline": None if args.no_cpu or rank != 0 else dict(
+                unit="Mrows/s", cores=1, kind="port", sample=f"first {min(args.cpu_sample, n)} rows", **{
+                    k: v for k, v in cpu_agg(args.scale, min(args.cpu_sample, n)).items() if k == "value"})}
 
 
 def main():
