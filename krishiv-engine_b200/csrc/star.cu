@@ -21,6 +21,7 @@
 // The per-row value is computed as the CPU does it: (double)price, then
 // 1.0 - discount and one product, each rounded (no fused multiply-add).
 #include <algorithm>
+#include <climits>
 #include <memory>
 
 #include "krv_device.cuh"
@@ -42,8 +43,9 @@ constexpr long long kAttrEmpty = (long long)0x8080808080808080ULL;
 constexpr int kSelectSteps = 16;
 __global__ void __launch_bounds__(256) dim_select_kernel(const long long *key, const int32_t *pred, const int32_t *attr,
                                                          int64_t n, int32_t value, long long *okey, int32_t *oattr,
-                                                         unsigned long long *count) {
+                                                         unsigned long long *count, long long *range) {
     const int lane = threadIdx.x & 31;
+    long long lo = LLONG_MAX, hi = LLONG_MIN;  // selected keys' range (when `range`)
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
     const int64_t chunk = 32 * kSelectSteps;
     for (int64_t c0 = ((int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5)) * chunk; c0 < n;
@@ -64,11 +66,37 @@ __global__ void __launch_bounds__(256) dim_select_kernel(const long long *key, c
             if ((ballots[s] >> lane) & 1u) {
                 const int64_t i = c0 + s * 32 + lane;
                 const unsigned long long pos = base + __popc(ballots[s] & lanemask_lt());
-                okey[pos] = key[i];
+                const long long k = key[i];
+                okey[pos] = k;
                 oattr[pos] = attr[i];
+                lo = k < lo ? k : lo;
+                hi = k > hi ? k : hi;
             }
             base += __popc(ballots[s]);
         }
+    }
+    if (range) {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            const long long a = __shfl_xor_sync(0xFFFFFFFFu, lo, d), b = __shfl_xor_sync(0xFFFFFFFFu, hi, d);
+            lo = a < lo ? a : lo;
+            hi = b > hi ? b : hi;
+        }
+        if (lane == 0 && lo <= hi) {
+            atomicMin(range, lo);
+            atomicMax(range + 1, hi);
+        }
+    }
+}
+
+// A dimension with unique keys: group id (int16, -1 = no key) at key - lo.
+// Two rows with one key leave the index incomplete and set *dup.
+__global__ void dim_index_kernel(const long long *key, const int32_t *gid, int64_t n, long long lo,
+                                 unsigned short *direct, unsigned int *dup) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned long long off = (unsigned long long)(key[i] - lo);
+        const unsigned short old = atomicCAS(direct + off, (unsigned short)0xFFFFu, (unsigned short)gid[i]);
+        if (old != (unsigned short)0xFFFFu) atomicOr(dup, 1u);
     }
 }
 
@@ -153,7 +181,7 @@ class StarPipeline {
         int64_t rows = 0;
     };
 
-    void build_dim(const DevBatch &d, int32_t value, Dim &out) {
+    void check_dim(const DevBatch &d) const {
         const int c_key = spec_.dim_key, c_pred = spec_.dim_pred, c_attr = spec_.dim_attr;
         const int nc = (int)d.cols.size();
         if (c_key < 0 || c_key >= nc || c_pred < 0 || c_pred >= nc || c_attr < 0 || c_attr >= nc)
@@ -163,6 +191,108 @@ class StarPipeline {
             fail(KRV_UNSUPPORTED, "star dimension columns are (int64 key, int32 pred, int32 attr)");
         if (d.cols[c_key].valid || d.cols[c_pred].valid || d.cols[c_attr].valid)
             fail(KRV_UNSUPPORTED, "star dimension columns without NULLs");
+    }
+
+    // The fused plan's build when both dimensions have unique keys over spans
+    // of at most 2^26 values (the common star schema): select both, then
+    // dense group ids, an int16 direct index and the key filter from the
+    // selection's count and range; two host reads in all. False (nothing
+    // kept) when a dimension does not qualify: the join-table build runs.
+    bool build_fast(const DevBatch *dims[2], const int32_t values[2]) {
+        struct Sel {
+            DBuf key, attr, gid;
+            int64_t rows = 0;
+            long long lo = 0, hi = -1;
+        } sel[2];
+        // [0..1] counts, [2..5] (lo, hi) per dimension
+        DBuf ctl(rt_, 6 * 8);
+        const unsigned long long init[6] = {0, 0, (unsigned long long)LLONG_MAX, (unsigned long long)LLONG_MIN,
+                                            (unsigned long long)LLONG_MAX, (unsigned long long)LLONG_MIN};
+        KRV_CUDA(cudaMemcpyAsync(ctl.get(), init, sizeof(init), cudaMemcpyHostToDevice, rt_->stream));
+        for (int d = 0; d < 2; d++) {
+            const DevBatch &b = *dims[d];
+            const int64_t n = b.rows;
+            sel[d].key = DBuf(rt_, (size_t)std::max<int64_t>(n, 1) * 8);
+            sel[d].attr = DBuf(rt_, (size_t)std::max<int64_t>(n, 1) * 4);
+            if (n > 0) {
+                dim_select_kernel<<<grid_for(rt_, n, 256, 8), 256, 0, rt_->stream>>>(
+                    static_cast<const long long *>(b.cols[spec_.dim_key].data),
+                    static_cast<const int32_t *>(b.cols[spec_.dim_pred].data),
+                    static_cast<const int32_t *>(b.cols[spec_.dim_attr].data), n, values[d], sel[d].key.as<long long>(),
+                    sel[d].attr.as<int32_t>(), ctl.as<unsigned long long>() + d, ctl.as<long long>() + 2 + 2 * d);
+                rt_->launches++;
+                check_launch("dim_select_kernel");
+            }
+        }
+        unsigned long long got[6];
+        KRV_CUDA(cudaMemcpyAsync(got, ctl.get(), sizeof(got), cudaMemcpyDeviceToHost, rt_->stream));
+        KRV_CUDA(cudaStreamSynchronize(rt_->stream));
+        for (int d = 0; d < 2; d++) {
+            sel[d].rows = (int64_t)got[d];
+            sel[d].lo = (long long)got[2 + 2 * d];
+            sel[d].hi = (long long)got[3 + 2 * d];
+            if (sel[d].rows <= 0) return false;
+            const __int128 span = (__int128)sel[d].hi - (__int128)sel[d].lo;
+            if (span < 0 || span >= ((__int128)1 << 26)) return false;
+        }
+        // dense group ids, then the direct indexes (duplicates flagged)
+        DBuf flags(rt_, 4 * 4);  // [0] ngroups, [1..2] duplicate keys, [3] status
+        KRV_CUDA(cudaMemsetAsync(flags.get(), 0, 16, rt_->stream));
+        DBuf direct[2];
+        for (int d = 0; d < 2; d++) {
+            const int64_t rows = sel[d].rows;
+            sel[d].gid = DBuf(rt_, (size_t)rows * 4);
+            attr_gid_kernel<<<grid_for(rt_, rows, 256, 8), 256, 0, rt_->stream>>>(
+                sel[d].attr.as<int32_t>(), rows, gkeys_.as<long long>(), gtab_.as<int32_t>(), gmask_, sel[d].gid.as<int32_t>(),
+                gattr_.as<int32_t>(), flags.as<unsigned int>(), flags.as<uint32_t>() + 3);
+            rt_->launches++;
+            check_launch("attr_gid_kernel");
+            const size_t span = (size_t)(sel[d].hi - sel[d].lo) + 1;
+            direct[d] = DBuf(rt_, span * 2);
+            KRV_CUDA(cudaMemsetAsync(direct[d].get(), 0xFF, span * 2, rt_->stream));
+            dim_index_kernel<<<grid_for(rt_, rows, 256, 8), 256, 0, rt_->stream>>>(
+                sel[d].key.as<long long>(), sel[d].gid.as<int32_t>(), rows, sel[d].lo, direct[d].as<unsigned short>(),
+                flags.as<unsigned int>() + 1 + d);
+            rt_->launches++;
+            check_launch("dim_index_kernel");
+        }
+        // key filters from the selection's stats (keys unique: distinct = rows)
+        std::shared_ptr<KeyFilterImpl> filt[2];
+        if (spec_.use_filters) {
+            krv_key_filter_options fo;
+            krv_key_filter_options_default(&fo);
+            for (int d = 0; d < 2; d++) {
+                DevCol kc;
+                kc.type = DType{Type::I64, 0, 0};
+                kc.length = sel[d].rows;
+                kc.nullable = false;
+                kc.data = sel[d].key.get();
+                const KeyStats ks{sel[d].rows, sel[d].rows, sel[d].lo, sel[d].hi};
+                filt[d] = build_key_filter(rt_, fo, kc, &ks);
+            }
+        }
+        uint32_t fl[4];
+        KRV_CUDA(cudaMemcpyAsync(fl, flags.get(), sizeof(fl), cudaMemcpyDeviceToHost, rt_->stream));
+        KRV_CUDA(cudaStreamSynchronize(rt_->stream));
+        if (fl[3] & ST_TIMEOUT) fail(KRV_TIMEOUT, "star build: a wait for a group id gave up");
+        if (fl[1] || fl[2]) return false;  // duplicate dimension keys: the join-table build
+        ngroups_host_ = (int)fl[0];
+        if (ngroups_host_ > (int)gmask_ / 2) fail(KRV_UNSUPPORTED, "more than 32768 distinct attribute values");
+        for (int d = 0; d < 2; d++) {
+            dims_[d] = Dim{};
+            dims_[d].rows = sel[d].rows;
+            filt_[d] = filt[d];
+            direct_buf_[d] = std::move(direct[d]);
+            direct_[d] = StarDirect{direct_buf_[d].get(), sel[d].lo, (unsigned long long)(sel[d].hi - sel[d].lo), 2};
+        }
+        counters_.dim_a_keys = sel[0].rows;
+        counters_.dim_b_keys = sel[1].rows;
+        return true;
+    }
+
+    void build_dim(const DevBatch &d, int32_t value, Dim &out) {
+        check_dim(d);
+        const int c_key = spec_.dim_key, c_pred = spec_.dim_pred, c_attr = spec_.dim_attr;
         const int64_t n = d.rows;
         out.key = DBuf(rt_, (size_t)std::max<int64_t>(n, 1) * 8);
         out.attr = DBuf(rt_, (size_t)std::max<int64_t>(n, 1) * 4);
@@ -172,7 +302,7 @@ class StarPipeline {
             dim_select_kernel<<<grid_for(rt_, n, 256, 8), 256, 0, rt_->stream>>>(
                 static_cast<const long long *>(d.cols[c_key].data), static_cast<const int32_t *>(d.cols[c_pred].data),
                 static_cast<const int32_t *>(d.cols[c_attr].data), n, value, out.key.as<long long>(),
-                out.attr.as<int32_t>(), cnt.as<unsigned long long>());
+                out.attr.as<int32_t>(), cnt.as<unsigned long long>(), nullptr);
             rt_->launches++;
             check_launch("dim_select_kernel");
         }
@@ -227,22 +357,44 @@ class StarPipeline {
         clear_status(rt_);
         dims_[0] = Dim{};
         dims_[1] = Dim{};
-        // Only the grouping dimension's attribute names groups; the other's
-        // ids are never read.
-        build_dim(a, spec_.pred_a, dims_[0]);
-        build_dim(b, spec_.pred_b, dims_[1]);
-        if (take_status(rt_) & ST_TIMEOUT) fail(KRV_TIMEOUT, "star build: a wait for a group id gave up");
-        ngroups_host_ = (int)read_scalar<unsigned int>(rt_, ngroups_.get());
-        if (ngroups_host_ > (int)gmask_ / 2) fail(KRV_UNSUPPORTED, "more than 32768 distinct attribute values");
+        filt_[0].reset();
+        filt_[1].reset();
+        for (int d = 0; d < 2; d++) {
+            direct_[d] = StarDirect{nullptr, 0, 0, 0};
+            direct_buf_[d].reset();
+        }
+        check_dim(a);
+        check_dim(b);
+        const DevBatch *dims[2] = {&a, &b};
+        const int32_t values[2] = {spec_.pred_a, spec_.pred_b};
+        const bool fast = spec_.mode == KRV_STAR_FUSED && build_fast(dims, values);
+        if (!fast) {
+            // The join-table build: reset the group ids the fast attempt made.
+            KRV_CUDA(cudaMemsetAsync(gkeys_.get(), 0x80, (gmask_ + 1) * 8, rt_->stream));
+            KRV_CUDA(cudaMemsetAsync(gtab_.get(), 0xFF, (gmask_ + 1) * 4, rt_->stream));
+            KRV_CUDA(cudaMemsetAsync(ngroups_.get(), 0, 8, rt_->stream));
+            clear_status(rt_);
+            // Only the grouping dimension's attribute names groups; the other's
+            // ids are never read.
+            build_dim(a, spec_.pred_a, dims_[0]);
+            build_dim(b, spec_.pred_b, dims_[1]);
+            if (take_status(rt_) & ST_TIMEOUT) fail(KRV_TIMEOUT, "star build: a wait for a group id gave up");
+            ngroups_host_ = (int)read_scalar<unsigned int>(rt_, ngroups_.get());
+            if (ngroups_host_ > (int)gmask_ / 2) fail(KRV_UNSUPPORTED, "more than 32768 distinct attribute values");
+            filt_[0] = dims_[0].join->key_filter();
+            filt_[1] = dims_[1].join->key_filter();
+        }
         const size_t G = (size_t)std::max(ngroups_host_, 1);
         sum_hi_ = DBuf(rt_, G * 8);
         sum_lo_ = DBuf(rt_, G * 8);
         cnt_ = DBuf(rt_, G * 8);
         stats_ = DBuf(rt_, 32);
         reset();
-        counters_.dim_a_keys = dims_[0].join->counters().build_keys;
-        counters_.dim_b_keys = dims_[1].join->counters().build_keys;
-        auto fa = dims_[0].join->key_filter(), fb = dims_[1].join->key_filter();
+        if (!fast) {
+            counters_.dim_a_keys = dims_[0].join->counters().build_keys;
+            counters_.dim_b_keys = dims_[1].join->counters().build_keys;
+        }
+        auto fa = filt_[0], fb = filt_[1];
         counters_.filter_a_form = fa ? fa->info.form : -1;
         counters_.filter_b_form = fb ? fb->info.form : -1;
         counters_.filter_a_bytes = fa ? fa->info.bloom_bytes : 0;
@@ -251,7 +403,7 @@ class StarPipeline {
             if (fa) build_bits(0, *fa);
             if (fb) build_bits(1, *fb);
         }
-        if (spec_.mode == KRV_STAR_FUSED) {
+        if (spec_.mode == KRV_STAR_FUSED && !fast) {
             build_direct(0);
             build_direct(1);
         }
@@ -288,6 +440,7 @@ class StarPipeline {
     }
 
     StarTable view(const Dim &d) const {
+        if (!d.join) return StarTable{};  // the fast build keeps direct indexes only
         auto t = d.join->table_dev();
         return StarTable{t.slots, t.mask, t.next, t.seed, static_cast<const long long *>(d.join->arena().cols[0].data),
                          static_cast<const int32_t *>(d.join->arena().cols[2].data)};
@@ -321,7 +474,7 @@ class StarPipeline {
         A.n = f.rows;
         if (A.n <= 0) return;
         if (A.n >= (int64_t)0xFFFFFFFFll) fail(KRV_UNSUPPORTED, "fact batches of 2^32 rows or more");
-        auto fa = dims_[0].join->key_filter(), fb = dims_[1].join->key_filter();
+        auto fa = filt_[0], fb = filt_[1];
         A.use_filters = spec_.use_filters && fa && fb;
         if (A.use_filters) {
             A.fa = key_filter_dev(*fa);
@@ -438,7 +591,7 @@ class StarPipeline {
     }
 
     void probe_plain(const DevBatch &f) {
-        auto fa = dims_[0].join->key_filter(), fb = dims_[1].join->key_filter();
+        auto fa = filt_[0], fb = filt_[1];
         const int64_t n = f.rows;
         const DevCol &ca = f.cols[spec_.fact_fk_a], &cb = f.cols[spec_.fact_fk_b];
         const DevCol &cp = f.cols[spec_.fact_price], &cd = f.cols[spec_.fact_discount];
@@ -608,6 +761,7 @@ class StarPipeline {
     Runtime *rt_;
     krv_star_spec spec_;
     Dim dims_[2];
+    std::shared_ptr<KeyFilterImpl> filt_[2];  // the dimensions' key filters
     DBuf gkeys_, gtab_, gattr_, ngroups_;
     uint32_t gmask_ = 0;
     int ngroups_host_ = 0;
