@@ -205,7 +205,7 @@ def run_star(args, kb, W, rt, rank, world, pg, device):
     def make(mode):
         return kb.StarPipeline(rt, kb.star_spec(W.PRED_VALUE, W.PRED_VALUE, group_by=0, mode=mode))
 
-    def timed(pipe, steps, warmup, kernel_events=None):
+    def timed(pipe, steps, warmup, kernel_events=None, phases=None):
         for _ in range(warmup):
             pipe.reset()
             pipe.build_device(dim_a, dim_b)
@@ -218,29 +218,39 @@ def run_star(args, kb, W, rt, rank, world, pg, device):
         kev = []
         start.record(stream)
         for _ in range(steps):
+            # events between the phases: reset | build | probe | result
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)] if kernel_events is not None else None
+            if ev:
+                ev[0].record(stream)
             pipe.reset()
+            if ev:
+                ev[1].record(stream)
             pipe.build_device(dim_a, dim_b)
-            if kernel_events is not None:
-                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a.record(stream)
-                pipe.probe_device(fact)
-                b.record(stream)
-                kev.append((a, b))
-            else:
-                pipe.probe_device(fact)
+            if ev:
+                ev[2].record(stream)
+            pipe.probe_device(fact)
+            if ev:
+                ev[3].record(stream)
             pipe.result()
+            if ev:
+                ev[4].record(stream)
+                kev.append(ev)
         end.record(stream)
         torch.cuda.synchronize()
         barrier(pg)
         ms = start.elapsed_time(end) / steps
         if kernel_events is not None:
-            kernel_events.extend(a.elapsed_time(b) for a, b in kev)
+            kernel_events.extend(ev[2].elapsed_time(ev[3]) for ev in kev)
+            if phases is not None:
+                for name, i in (("reset", 0), ("build", 1), ("probe", 2), ("result", 3)):
+                    phases[name] = statistics.median(ev[i].elapsed_time(ev[i + 1]) for ev in kev)
         return ms, rt.launches - launches0
 
     fused = make(kb.STAR_FUSED)
     kernel_ms = []
+    phases = {}
     with Clocks(device) as clk:
-        ms, launches = timed(fused, args.steps, args.warmup, kernel_ms)
+        ms, launches = timed(fused, args.steps, args.warmup, kernel_ms, phases)
     ms_max = max_over_ranks(pg, ms, device)
     counters = fused.counters()
     result = fused.result()
@@ -285,6 +295,7 @@ def run_star(args, kb, W, rt, rank, world, pg, device):
         "mode": "fused (batched) pipeline",
         "groups": len(merged),
         "gpu_launches": launches,
+        "phases_ms": phases,
         "roofline": {"bound": "hbm", "kernel": "star_scan_kernel + star_join_kernel (fact probe)",
                      "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": profile_traffic("star_probe", nf),

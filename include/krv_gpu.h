@@ -169,6 +169,28 @@ krv_status krv_join_key_filter(krv_join *j, krv_key_filter **out);
 krv_status krv_join_counters_get(const krv_join *j, krv_join_counters *out);
 void krv_join_destroy(krv_join *j);
 
+/* ---- partitioned (grace) hash join -----------------------------------------
+ * The engine's grace join (join/grace.rs:828-1481): both sides are radix
+ * partitioned by the key hash (level 0: top radix_bits of h, 3..6; a partition
+ * still too large is split 8 ways by bits [48-3d, 51-3d) of g); partitions are
+ * joined in HBM while their tables fit half of the device budget and spill to
+ * page-locked host memory otherwise. Inner and left outer joins on one int64
+ * key (NULL keys allowed); other columns 4 or 8 bytes wide, without NULLs.
+ * Same calls as krv_join_*: krv_join_probe returns the rows it can join now
+ * (KRV_HAVE_MORE_OUTPUT while more wait), and after the last probe batch
+ * krv_join_finish returns the spilled partitions' rows, one batch per call,
+ * KRV_HAVE_MORE_OUTPUT until the last (KRV_FINISHED). spec->build_rows_hint,
+ * when set, decides the partitions and which of them spill up front. */
+typedef struct {
+    int64_t device_budget_bytes;  /* device bytes for the join (0: the runtime's budget, else half the free memory) */
+    int64_t reserved[3];
+} krv_grace_options;
+void krv_grace_options_init(krv_grace_options *o);
+krv_status krv_join_create_partitioned(krv_runtime *rt, const krv_join_spec *spec, const krv_grace_options *opt,
+                                       krv_join **out);
+/* Partitions of a partitioned join that spilled to host memory. */
+int64_t krv_join_spilled_partitions(const krv_join *j);
+
 /* ---- grouped hash aggregate ---------------------------------------------- */
 /* AggregateFunction (aggregate/mod.rs:134), the core five */
 #define KRV_AGG_COUNT_STAR 0

@@ -138,6 +138,10 @@ class StarCounters(C.Structure):
                 ("fk_a_sectors", C.c_int64)]
 
 
+class GraceOptions(C.Structure):
+    _fields_ = [("device_budget_bytes", C.c_int64), ("reserved", C.c_int64 * 3)]
+
+
 class ServerOptions(C.Structure):
     _fields_ = [("mode", C.c_int32), ("autotune", C.c_int32), ("ansi", C.c_int32), ("max_tick_requests", C.c_int32),
                 ("tick_rows", C.c_int64), ("hbm_budget_bytes", C.c_int64)]
@@ -219,6 +223,10 @@ _SIGS = {
     "krv_star_counters_get": (C.c_int32, [C.c_void_p, C.POINTER(StarCounters)]),
     "krv_star_destroy": (None, [C.c_void_p]),
     "krv_gen_fill": (C.c_int32, [C.c_void_p, C.POINTER(GenSpec), C.c_int64, C.c_void_p, C.c_void_p]),
+    "krv_grace_options_init": (None, [C.POINTER(GraceOptions)]),
+    "krv_join_create_partitioned": (C.c_int32, [C.c_void_p, C.POINTER(JoinSpec), C.POINTER(GraceOptions),
+                                                C.POINTER(C.c_void_p)]),
+    "krv_join_spilled_partitions": (C.c_int64, [C.c_void_p]),
     "krv_server_options_init": (None, [C.POINTER(ServerOptions)]),
     "krv_server_create": (C.c_int32, [C.c_void_p, C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
     "krv_server_add_table": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema), C.c_int32,
@@ -463,7 +471,7 @@ class Runtime:
 
 def join_spec(join_type="inner", probe_keys=(0,), build_keys=(0,), null_safe=None, single_match=False,
               probe_out=None, build_out=None, runtime_filter=False, max_load=0.0, max_output_rows=0,
-              build_rows_hint=0) -> JoinSpec:
+              build_rows_hint=0, radix_bits=0) -> JoinSpec:
     s = JoinSpec()
     lib().krv_join_spec_init(C.byref(s))
     s.join_type = JOIN_TYPES[join_type] if isinstance(join_type, str) else int(join_type)
@@ -485,16 +493,27 @@ def join_spec(join_type="inner", probe_keys=(0,), build_keys=(0,), null_safe=Non
     s.max_load = max_load
     s.max_output_rows = max_output_rows
     s.build_rows_hint = build_rows_hint
+    s.radix_bits = radix_bits
     return s
 
 
 class HashJoin:
-    """The hash join operator (HashJoin, crates/krishiv-exec/src/join/mod.rs:1014)."""
+    """The hash join operator (HashJoin, crates/krishiv-exec/src/join/mod.rs:1014).
+    `partitioned=True` makes the partitioned (grace) join of
+    crates/krishiv-exec/src/join/grace.rs (krv_join_create_partitioned): inner
+    or left outer on one int64 key, within `device_budget` bytes (0: the
+    runtime's budget), spilling partitions to page-locked host memory."""
 
-    def __init__(self, rt: Runtime, spec: JoinSpec):
+    def __init__(self, rt: Runtime, spec: JoinSpec, partitioned: bool = False, device_budget: int = 0):
         self.rt = rt
         h = C.c_void_p()
-        check(lib().krv_join_create(rt.h, C.byref(spec), C.byref(h)))
+        if partitioned:
+            o = GraceOptions()
+            lib().krv_grace_options_init(C.byref(o))
+            o.device_budget_bytes = device_budget
+            check(lib().krv_join_create_partitioned(rt.h, C.byref(spec), C.byref(o), C.byref(h)))
+        else:
+            check(lib().krv_join_create(rt.h, C.byref(spec), C.byref(h)))
         self.h = h
 
     def build_push(self, batch):
@@ -525,6 +544,29 @@ class HashJoin:
         dev, sch = ArrowDeviceArray(), ArrowSchema()
         check(lib().krv_join_probe_device(self.h, C.byref(db.dev), C.byref(db.schema), C.byref(dev), C.byref(sch)))
         return DeviceResult(dev, sch)
+
+    def probe_device_all(self, db: DeviceBatch):
+        """Every output batch of one probe batch (device), one at a time."""
+        dev, sch = ArrowDeviceArray(), ArrowSchema()
+        st = check(lib().krv_join_probe_device(self.h, C.byref(db.dev), C.byref(db.schema), C.byref(dev),
+                                               C.byref(sch)))
+        yield DeviceResult(dev, sch)
+        while st == HAVE_MORE_OUTPUT:
+            dev, sch = ArrowDeviceArray(), ArrowSchema()
+            st = check(lib().krv_join_probe_device(self.h, None, None, C.byref(dev), C.byref(sch)))
+            yield DeviceResult(dev, sch)
+
+    def finish_device(self):
+        """The rows emitted after the last probe batch (device), one batch at a
+        time: a partitioned join's spilled partitions."""
+        st = HAVE_MORE_OUTPUT
+        while st == HAVE_MORE_OUTPUT:
+            dev, sch = ArrowDeviceArray(), ArrowSchema()
+            st = check(lib().krv_join_finish_device(self.h, C.byref(dev), C.byref(sch)))
+            yield DeviceResult(dev, sch)
+
+    def spilled_partitions(self) -> int:
+        return lib().krv_join_spilled_partitions(self.h)
 
     def finish(self) -> list:
         out = []

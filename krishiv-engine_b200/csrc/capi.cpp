@@ -22,7 +22,12 @@ struct krv_runtime {
 struct krv_join {
     krv_runtime *owner;
     std::unique_ptr<krv::HashJoin> j;
+    krv::GraceJoin *g = nullptr;  // a partitioned join instead of `j`
     std::vector<DevBatch> pending;
+    ~krv_join() {
+        if (g) krv::grace_destroy(g);
+    }
+    const krv_join_spec &spec() const { return g ? krv::grace_spec(g) : j->spec(); }
 };
 struct krv_agg {
     krv_runtime *owner;
@@ -88,6 +93,19 @@ DevBatch pop(std::vector<DevBatch> &pending) {
     DevBatch b = std::move(pending.back());
     pending.pop_back();
     return b;
+}
+
+// The first piece of several output batches; the rest wait in `pending`.
+DevBatch take_all(std::vector<DevBatch> bs, int64_t max_rows, std::vector<DevBatch> &pending) {
+    std::vector<DevBatch> pieces;
+    for (DevBatch &b : bs) {
+        std::vector<DevBatch> rest;
+        DevBatch first = take_first(std::move(b), max_rows, rest);
+        pieces.push_back(std::move(first));
+        for (size_t i = rest.size(); i-- > 0;) pieces.push_back(std::move(rest[i]));
+    }
+    for (size_t i = pieces.size(); i-- > 1;) pending.push_back(std::move(pieces[i]));
+    return std::move(pieces[0]);
 }
 
 }  // namespace
@@ -186,12 +204,39 @@ krv_status krv_join_create(krv_runtime *rt, const krv_join_spec *spec, krv_join 
     });
 }
 
+void krv_grace_options_init(krv_grace_options *o) {
+    if (o) *o = krv_grace_options{};
+}
+krv_status krv_join_create_partitioned(krv_runtime *rt, const krv_join_spec *spec, const krv_grace_options *opt,
+                                       krv_join **out) {
+    return guard([&] {
+        need(rt, "runtime");
+        need(spec, "spec");
+        need(out, "out");
+        *out = nullptr;
+        krv_grace_options o;
+        if (opt) o = *opt;
+        else krv_grace_options_init(&o);
+        krv::DeviceGuard g(&rt->rt);
+        auto h = std::make_unique<krv_join>();
+        h->owner = rt;
+        h->g = krv::make_grace(&rt->rt, *spec, o);
+        *out = h.release();
+        return KRV_OK;
+    });
+}
+int64_t krv_join_spilled_partitions(const krv_join *j) {
+    return j && j->g ? krv::grace_spilled_partitions(j->g) : 0;
+}
+
 krv_status krv_join_build_push(krv_join *j, const ArrowArray *batch, const ArrowSchema *schema) {
     return guard([&] {
         need(j, "join");
         krv::DeviceGuard g(&j->owner->rt);
         krv::HostBorrow hb(&j->owner->rt);
-        j->j->build_push(krv::import_host(&j->owner->rt, batch, schema));
+        DevBatch b = krv::import_host(&j->owner->rt, batch, schema);
+        if (j->g) krv::grace_build_push(j->g, b);
+        else j->j->build_push(b);
         return KRV_OK;
     });
 }
@@ -199,14 +244,18 @@ krv_status krv_join_build_push_device(krv_join *j, const ArrowDeviceArray *batch
     return guard([&] {
         need(j, "join");
         krv::DeviceGuard g(&j->owner->rt);
-        j->j->build_push(krv::import_device(&j->owner->rt, batch, schema));
+        DevBatch b = krv::import_device(&j->owner->rt, batch, schema);
+        if (j->g) krv::grace_build_push(j->g, b);
+        else j->j->build_push(b);
         return KRV_OK;
     });
 }
 krv_status krv_join_build_finish(krv_join *j) {
     return guard([&] {
         need(j, "join");
-        j->j->build_finish();
+        krv::DeviceGuard g(&j->owner->rt);
+        if (j->g) krv::grace_build_finish(j->g);
+        else j->j->build_finish();
         return KRV_OK;
     });
 }
@@ -230,7 +279,13 @@ static krv_status join_probe_impl(krv_join *j, const In *in, const ArrowSchema *
                 hb.reset(new krv::HostBorrow(rt));
                 inb = krv::import_host(rt, in, in_schema);
             }
-            b = take_first(j->j->probe(inb), j->j->spec().max_output_rows, j->pending);
+            if (j->g) {
+                std::vector<DevBatch> outs = krv::grace_probe(j->g, inb);
+                if (outs.empty()) outs.push_back(krv::grace_empty_output(j->g));
+                b = take_all(std::move(outs), j->spec().max_output_rows, j->pending);
+            } else {
+                b = take_first(j->j->probe(inb), j->j->spec().max_output_rows, j->pending);
+            }
         } else {
             if (j->pending.empty()) krv::fail(KRV_INVALID_ARGUMENT, "no pending output and no input");
             b = pop(j->pending);
@@ -258,11 +313,19 @@ static krv_status join_finish_impl(krv_join *j, Out *out, ArrowSchema *out_schem
         krv::Runtime *rt = &j->owner->rt;
         krv::DeviceGuard g(rt);
         DevBatch b;
-        if (j->pending.empty()) b = take_first(j->j->finish(), j->j->spec().max_output_rows, j->pending);
-        else b = pop(j->pending);
+        if (!j->pending.empty()) {
+            b = pop(j->pending);
+        } else if (j->g) {
+            DevBatch next;
+            if (krv::grace_finish_next(j->g, next)) b = take_first(std::move(next), j->spec().max_output_rows, j->pending);
+            else b = krv::grace_empty_output(j->g);
+        } else {
+            b = take_first(j->j->finish(), j->j->spec().max_output_rows, j->pending);
+        }
         if constexpr (Device) krv::export_device(rt, b, out, out_schema);
         else krv::export_host(rt, b, out, out_schema);
-        return j->pending.empty() ? KRV_FINISHED : KRV_HAVE_MORE_OUTPUT;
+        const bool more = !j->pending.empty() || (j->g && !krv::grace_done(j->g));
+        return more ? KRV_HAVE_MORE_OUTPUT : KRV_FINISHED;
     });
 }
 krv_status krv_join_finish(krv_join *j, ArrowArray *out, ArrowSchema *out_schema) {
@@ -277,6 +340,7 @@ krv_status krv_join_key_filter(krv_join *j, krv_key_filter **out) {
         need(j, "join");
         need(out, "out");
         *out = nullptr;
+        if (j->g) krv::fail(KRV_UNSUPPORTED, "partitioned joins publish no key filter");
         auto f = j->j->key_filter();
         if (!f) krv::fail(KRV_UNSUPPORTED, "this join published no key filter (runtime_filter off or not one int64 key)");
         *out = new krv_key_filter{f};
@@ -287,7 +351,7 @@ krv_status krv_join_counters_get(const krv_join *j, krv_join_counters *out) {
     return guard([&] {
         need(j, "join");
         need(out, "out");
-        *out = j->j->counters();
+        *out = j->g ? krv::grace_counters(j->g) : j->j->counters();
         return KRV_OK;
     });
 }

@@ -1,0 +1,608 @@
+// grace.cu -- the partitioned ("grace") hash join: inner and left outer joins
+// on one int64 key whose build side, with its hash tables, does not fit the
+// device memory budget.
+//
+// Reference: the engine's grace join (crates/krishiv-exec/src/join/grace.rs:
+// step :828, split :1397, scatter :1481) partitions both sides by the key
+// hash, spills partitions to disk and joins them one at a time, splitting a
+// partition that is still too large with the next level of hash bits. Here:
+//  - a radix partition pass (histogram, then a scatter staged in shared
+//    memory so that each partition's rows leave a tile as one contiguous,
+//    coalesced run) splits every batch into 2^radix partitions by the top
+//    `radix` bits of the row hash h (level 0, join/keys.rs:118-128); a split
+//    of a partition uses bits [48-3d, 51-3d) of g = fin(h ^ seed) (level d,
+//    hash.rs:139-148), 8 ways;
+//  - hybrid residency: partitions are joined in HBM while the build's
+//    estimated footprint (rows, table and chains) fits half of the runtime's
+//    HBM budget; the others spill to page-locked host memory;
+//  - every partition is joined by a HashJoin (the same table, probe and
+//    output code as the unpartitioned join), so the output rows are exactly
+//    those of the unpartitioned join, in another order;
+//  - NULL probe keys never match: their rows are padded at once (left outer)
+//    or dropped (inner); NULL build keys are dropped in the partition pass.
+// Spilled partitions are joined after the last probe batch, one output batch
+// per call, so the output never has to fit the budget.
+#include <algorithm>
+#include <deque>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "krv_device.cuh"
+#include "ops.h"
+
+namespace krv {
+
+namespace {
+
+constexpr int kPartThreads = 512;
+constexpr int kPartTile = 2048;  // rows staged per tile
+constexpr int kMaxParts = 64;    // 2^6: the reference clamps radix to 3..6
+constexpr int kMaxCols = 8;
+constexpr int kMaxLevel = 6;
+
+struct PartCol {
+    const void *src;
+    void *dst;
+    int width;  // 4 or 8
+};
+struct PartArgs {
+    const long long *key;
+    const uint8_t *kvalid;
+    int64_t kvoff;
+    int64_t n;
+    int level, bits;
+    uint64_t seed;
+    int nparts;      // partitions; bucket `nparts` holds NULL keys
+    int keep_nulls;  // write the NULL bucket (probe side) or drop it (build side)
+    PartCol c[kMaxCols];
+    int ncols;
+};
+
+__device__ __forceinline__ int part_of(const PartArgs &A, int64_t r) {
+    if (A.kvalid && !bit_get(A.kvalid, A.kvoff, r)) return A.nparts;
+    const uint64_t h = hash_word((uint64_t)A.key[r]);
+    if (A.level == 0) return (int)(h >> (64 - A.bits));
+    return (int)((finalize(h, A.seed) >> (48 - 3 * A.level)) & 7u);
+}
+
+__global__ void __launch_bounds__(256) part_hist_kernel(PartArgs A, unsigned long long *hist) {
+    __shared__ unsigned int s_hist[kMaxParts + 1];
+    for (int p = threadIdx.x; p <= A.nparts; p += blockDim.x) s_hist[p] = 0;
+    __syncthreads();
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&s_hist[part_of(A, r)], 1u);
+    __syncthreads();
+    for (int p = threadIdx.x; p <= A.nparts; p += blockDim.x)
+        if (s_hist[p]) atomicAdd(hist + p, (unsigned long long)s_hist[p]);
+}
+
+// Tiles of kPartTile rows: rank every row within its partition in shared
+// memory, claim each partition's run of the output with one atomic per tile,
+// then write the tile column by column in partition order (coalesced runs).
+__global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(PartArgs A, unsigned long long *cursor) {
+    __shared__ unsigned int s_cnt[kMaxParts + 1], s_off[kMaxParts + 2];
+    __shared__ unsigned long long s_base[kMaxParts + 1];
+    __shared__ uint8_t s_part[kPartTile];
+    __shared__ __align__(16) unsigned long long s_val[kPartTile];
+    constexpr int U = kPartTile / kPartThreads;
+    const int64_t ntiles = (A.n + kPartTile - 1) / kPartTile;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int64_t row0 = t * kPartTile;
+        for (int p = threadIdx.x; p <= A.nparts; p += kPartThreads) s_cnt[p] = 0;
+        __syncthreads();
+        int part[U];
+        unsigned rank[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int i = u * kPartThreads + threadIdx.x;
+            const int64_t r = row0 + i;
+            part[u] = r < A.n ? part_of(A, r) : -1;
+            if (part[u] == A.nparts && !A.keep_nulls) part[u] = -1;
+            rank[u] = part[u] >= 0 ? atomicAdd(&s_cnt[part[u]], 1u) : 0u;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned acc = 0;
+            for (int p = 0; p <= A.nparts; p++) {
+                s_off[p] = acc;
+                acc += s_cnt[p];
+            }
+            s_off[A.nparts + 1] = acc;
+        }
+        for (int p = threadIdx.x; p <= A.nparts; p += kPartThreads)
+            s_base[p] = s_cnt[p] ? atomicAdd(cursor + p, (unsigned long long)s_cnt[p]) : 0ull;
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (part[u] >= 0) s_part[s_off[part[u]] + rank[u]] = (uint8_t)part[u];
+        const unsigned total = s_off[A.nparts + 1];
+        for (int c = 0; c < A.ncols; c++) {
+            const PartCol C = A.c[c];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (part[u] < 0) continue;
+                const int64_t r = row0 + u * kPartThreads + threadIdx.x;
+                const unsigned slot = s_off[part[u]] + rank[u];
+                s_val[slot] = C.width == 8 ? static_cast<const unsigned long long *>(C.src)[r]
+                                           : (unsigned long long)static_cast<const uint32_t *>(C.src)[r];
+            }
+            __syncthreads();
+            for (unsigned j = threadIdx.x; j < total; j += kPartThreads) {
+                const int p = s_part[j];
+                const unsigned long long at = s_base[p] + (j - s_off[p]);
+                if (C.width == 8) static_cast<unsigned long long *>(C.dst)[at] = s_val[j];
+                else static_cast<uint32_t *>(C.dst)[at] = (uint32_t)s_val[j];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+int radix_for(int64_t build_rows, int64_t row_bytes, int64_t budget) {
+    // 2^radix partitions of at most a sixteenth of the budget each (3..6 bits).
+    if (budget <= 0 || build_rows <= 0) return 3;
+    const double total = (double)build_rows * (double)(row_bytes + 40);
+    int bits = 3;
+    while (bits < 6 && total / (double)(1 << bits) > (double)budget / 16.0) bits++;
+    return bits;
+}
+
+}  // namespace
+
+// ---- the operator ------------------------------------------------------------------
+class GraceJoin {
+  public:
+    GraceJoin(Runtime *rt, const krv_join_spec &spec, const krv_grace_options &opt) : rt_(rt), spec_(spec), opt_(opt) {
+        if (spec.join_type != KRV_JOIN_INNER && spec.join_type != KRV_JOIN_LEFT_OUTER)
+            fail(KRV_UNSUPPORTED, "partitioned joins are inner or left outer");
+        if (spec.n_keys != 1 || spec.null_safe[0])
+            fail(KRV_UNSUPPORTED, "partitioned joins have one `=` key");
+        if (spec.has_residual_filter)
+            fail(KRV_UNSUPPORTED, "KRISHIV_UNSUPPORTED_FEATURE: residual join filters on the GPU join");
+        spec_.runtime_filter = 0;
+        if (spec_.seed == 0) spec_.seed = 0x4B52565F4A4F494EULL;
+        budget_ = opt_.device_budget_bytes > 0 ? opt_.device_budget_bytes : rt_->budget;
+        if (budget_ <= 0) {
+            size_t free_b = 0, total_b = 0;
+            KRV_CUDA(cudaMemGetInfo(&free_b, &total_b));
+            budget_ = (int64_t)(free_b / 2);
+        }
+    }
+    ~GraceJoin() {
+        cudaStreamSynchronize(rt_->stream);  // copies into or out of the spill space
+        for (auto &b : host_blocks_) rt_->host_pool->give(b.first, b.second);
+    }
+
+    void build_push(const DevBatch &b) {
+        if (built_) fail(KRV_INVALID_ARGUMENT, "build_push after build_finish");
+        DeviceGuard g(rt_);
+        if (!schema_) init_schema(b);
+        check_shape(b, build_types_, spec_.build_keys[0], "build");
+        counters_.build_rows += b.rows;
+        if (b.rows == 0) return;
+        std::vector<Segment> segs = partition(b, spec_.build_keys[0], 0, parts_bits_, false);
+        for (int p = 0; p < nparts_; p++) {
+            Segment &s = segs[p];
+            if (s.rows == 0) continue;
+            Part &P = parts_[p];
+            if (P.spilled) {
+                P.build_host.push_back(spill(s));
+            } else {
+                P.join->build_push(s.batch);
+                P.build_rows += s.rows;
+                resident_rows_ += s.rows;
+            }
+        }
+        enforce_residency();
+    }
+
+    void build_finish() {
+        if (built_) fail(KRV_INVALID_ARGUMENT, "build_finish called twice");
+        DeviceGuard g(rt_);
+        if (!schema_) fail(KRV_INVALID_ARGUMENT, "a partitioned join needs the build side's schema: push a build batch");
+        for (auto &P : parts_)
+            if (!P.spilled) {
+                P.join->build_finish();
+                counters_.build_keys += P.join->counters().build_keys;
+                counters_.table_slots += P.join->counters().table_slots;
+            }
+        // A join over no build rows pads the NULL-key probe rows (left outer).
+        null_join_.reset(new HashJoin(rt_, spec_));
+        null_join_->build_push(empty_like(build_types_));
+        null_join_->build_finish();
+        built_ = true;
+    }
+
+    // The output of one probe batch that is ready now: its rows with NULL keys
+    // (left outer) and its rows of resident partitions. Rows of spilled
+    // partitions wait for finish.
+    std::vector<DevBatch> probe(const DevBatch &in) {
+        if (!built_) fail(KRV_INVALID_ARGUMENT, "probe before build_finish");
+        DeviceGuard g(rt_);
+        if (probe_types_.empty()) {
+            for (const DevCol &c : in.cols) probe_types_.push_back(c);
+            check_cols(in, spec_.probe_keys[0], "probe");
+        }
+        check_shape(in, probe_types_, spec_.probe_keys[0], "probe");
+        counters_.probe_rows += in.rows;
+        std::vector<DevBatch> out;
+        if (in.rows == 0) return out;
+        std::vector<Segment> segs = partition(in, spec_.probe_keys[0], 0, parts_bits_, true);
+        Segment &nulls = segs[nparts_];
+        if (nulls.rows > 0 && spec_.join_type == KRV_JOIN_LEFT_OUTER) keep(out, null_join_->probe(with_null_keys(nulls)));
+        for (int p = 0; p < nparts_; p++) {
+            Segment &s = segs[p];
+            if (s.rows == 0) continue;
+            Part &P = parts_[p];
+            if (P.spilled) P.probe_host.push_back(spill(s));
+            else keep(out, P.join->probe(s.batch));
+        }
+        return out;
+    }
+
+    // After the last probe batch: the next output batch of the spilled
+    // partitions; false when none is left.
+    bool finish_next(DevBatch &out) {
+        if (!built_) fail(KRV_INVALID_ARGUMENT, "finish before build_finish");
+        DeviceGuard g(rt_);
+        if (!finishing_) {
+            finishing_ = true;
+            for (auto &P : parts_) P.join.reset();  // resident tables are done
+            for (int p = 0; p < nparts_; p++)
+                if (parts_[p].spilled) tasks_.push_back(Task{0, std::move(parts_[p].build_host), std::move(parts_[p].probe_host)});
+        }
+        for (;;) {
+            if (cur_join_) {
+                if (cur_probe_ < cur_.probe_host.size()) {
+                    DevBatch pb = load(cur_.probe_host[cur_probe_++], probe_types_);
+                    DevBatch o = cur_join_->probe(pb);
+                    counters_.output_rows += o.rows;
+                    if (o.rows == 0) continue;
+                    out = o;
+                    return true;
+                }
+                cur_join_.reset();
+                cur_ = Task{};
+            }
+            if (tasks_.empty()) return false;
+            Task t = std::move(tasks_.front());
+            tasks_.pop_front();
+            int64_t rows = 0;
+            for (const HostChunk &c : t.build_host) rows += c.rows;
+            if (t.probe_host.empty()) continue;  // no probe rows: nothing to emit
+            if (rows * est_row_bytes() > budget_ / 2 && t.level < kMaxLevel) {
+                split(t);
+                continue;
+            }
+            if (rows * est_row_bytes() > budget_ / 2)
+                fail(KRV_NEED_MEMORY, "a partition of the build side stays above the memory budget after " +
+                                          std::to_string(kMaxLevel) + " levels of splits (one heavy key)");
+            krv_join_spec js = spec_;
+            js.build_rows_hint = rows;
+            cur_join_.reset(new HashJoin(rt_, js));
+            if (rows == 0) cur_join_->build_push(empty_like(build_types_));
+            else cur_join_->build_adopt(load_all(t.build_host, build_types_));
+            cur_join_->build_finish();
+            counters_.build_keys += cur_join_->counters().build_keys;
+            counters_.table_slots += cur_join_->counters().table_slots;
+            cur_ = std::move(t);
+            cur_probe_ = 0;
+        }
+    }
+
+    bool done() const { return finishing_ && !cur_join_ && tasks_.empty(); }
+    // A zero-row batch of the output's shape.
+    DevBatch empty_output() {
+        if (!built_ || probe_types_.empty()) return DevBatch{};
+        return null_join_->probe(empty_like(probe_types_));
+    }
+    const krv_join_spec &spec() const { return spec_; }
+    krv_join_counters counters() const {
+        krv_join_counters c = counters_;
+        c.partitions = nparts_ + splits_;
+        return c;
+    }
+    int64_t spilled_partitions() const {
+        int64_t n = 0;
+        for (const auto &P : parts_) n += P.spilled;
+        return n;
+    }
+
+  private:
+    struct Segment {
+        DevBatch batch;
+        int64_t rows = 0;
+    };
+    struct HostChunk {
+        std::vector<uint8_t *> cols;
+        int64_t rows = 0;
+    };
+    struct Part {
+        std::unique_ptr<HashJoin> join;  // resident: the partition's join
+        bool spilled = false;
+        int64_t build_rows = 0;
+        std::vector<HostChunk> build_host, probe_host;
+    };
+    struct Task {
+        int level = 0;
+        std::vector<HostChunk> build_host, probe_host;
+    };
+
+    void check_cols(const DevBatch &b, int key, const char *side) {
+        if (key < 0 || key >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, std::string(side) + " key column out of range");
+        if (b.cols[key].type.id != Type::I64) fail(KRV_UNSUPPORTED, "partitioned joins have an int64 key");
+        if ((int)b.cols.size() > kMaxCols) fail(KRV_UNSUPPORTED, "partitioned joins take at most 8 columns per side");
+        for (int i = 0; i < (int)b.cols.size(); i++) {
+            const int w = b.cols[i].type.width();
+            if (b.cols[i].type.id == Type::Bool || (w != 4 && w != 8))
+                fail(KRV_UNSUPPORTED, "partitioned joins take 4- and 8-byte columns");
+        }
+    }
+    void init_schema(const DevBatch &b) {
+        check_cols(b, spec_.build_keys[0], "build");
+        for (const DevCol &c : b.cols) build_types_.push_back(c);
+        int64_t row_bytes = 0;
+        for (const DevCol &c : b.cols) row_bytes += c.type.width();
+        row_bytes_ = row_bytes;
+        parts_bits_ = spec_.radix_bits >= 3 ? std::min(spec_.radix_bits, 6)
+                                            : radix_for(spec_.build_rows_hint, row_bytes_, budget_);
+        nparts_ = 1 << parts_bits_;
+        parts_.resize(nparts_);
+        // With a size hint the spilled partitions are known up front; without
+        // one, partitions spill as the resident footprint passes its share.
+        int resident = nparts_;
+        if (spec_.build_rows_hint > 0) {
+            const double per = (double)spec_.build_rows_hint / nparts_ * (double)est_row_bytes();
+            resident = (int)std::min<double>(nparts_, std::floor((double)budget_ / 2.0 / std::max(per, 1.0)));
+        }
+        for (int p = 0; p < nparts_; p++) {
+            parts_[p].spilled = p >= resident;
+            if (!parts_[p].spilled) {
+                krv_join_spec js = spec_;
+                js.build_rows_hint = spec_.build_rows_hint > 0 ? spec_.build_rows_hint / nparts_ * 9 / 8 + 1024 : 0;
+                parts_[p].join.reset(new HashJoin(rt_, js));
+                // the build schema, even for a partition that gets no rows
+                parts_[p].join->build_push(empty_like(build_types_));
+            }
+        }
+        schema_ = true;
+    }
+    void check_shape(const DevBatch &b, const std::vector<DevCol> &types, int key_col, const char *side) const {
+        if (b.cols.size() != types.size()) fail(KRV_INVALID_ARGUMENT, std::string(side) + " batches differ in columns");
+        for (size_t i = 0; i < types.size(); i++) {
+            if (b.cols[i].type != types[i].type) fail(KRV_INVALID_ARGUMENT, std::string(side) + " batches differ in types");
+            const bool key = (int)i == key_col;
+            if (!key && b.cols[i].valid)
+                fail(KRV_UNSUPPORTED, "partitioned joins take NULLs in the key column only");
+        }
+    }
+    // Device bytes per resident build row: the row, its table slots (up to 4
+    // per row at load 0.5 after the power-of-two rounding) and its chain link.
+    int64_t est_row_bytes() const { return row_bytes_ + 4 * 8 + 4; }
+
+    void enforce_residency() {
+        while (resident_rows_ * est_row_bytes() > budget_ / 2) {
+            int victim = -1;
+            for (int p = 0; p < nparts_; p++)
+                if (!parts_[p].spilled && (victim < 0 || parts_[p].build_rows > parts_[victim].build_rows)) victim = p;
+            if (victim < 0) break;
+            Part &P = parts_[victim];
+            if (P.build_rows > 0) {
+                Segment s;
+                s.batch = P.join->staged();
+                s.rows = P.build_rows;
+                P.build_host.push_back(spill(s));
+            }
+            resident_rows_ -= P.build_rows;
+            P.join.reset();
+            P.spilled = true;
+        }
+    }
+
+    // Partitions batch `b` by its key column at `level`: one segment (a
+    // device batch of the partition's rows) per partition, plus the NULL-key
+    // bucket at index nparts (kept when keep_nulls).
+    std::vector<Segment> partition(const DevBatch &b, int key, int level, int bits, bool keep_nulls) {
+        const int nparts = level == 0 ? (1 << bits) : 8;
+        PartArgs A{};
+        A.key = static_cast<const long long *>(b.cols[key].data);
+        A.kvalid = b.cols[key].valid;
+        A.kvoff = b.cols[key].valid_off;
+        A.n = b.rows;
+        A.level = level;
+        A.bits = bits;
+        A.seed = spec_.seed;
+        A.nparts = nparts;
+        A.keep_nulls = keep_nulls ? 1 : 0;
+        A.ncols = (int)b.cols.size();
+        DBuf ctr(rt_, (size_t)(nparts + 1) * 8 * 2);
+        unsigned long long *hist = ctr.as<unsigned long long>(), *cursor = hist + nparts + 1;
+        KRV_CUDA(cudaMemsetAsync(hist, 0, (size_t)(nparts + 1) * 8, rt_->stream));
+        part_hist_kernel<<<grid_for(rt_, b.rows, 256, 8), 256, 0, rt_->stream>>>(A, hist);
+        rt_->launches++;
+        check_launch("part_hist_kernel");
+        std::vector<unsigned long long> h(nparts + 1);
+        KRV_CUDA(cudaMemcpyAsync(h.data(), hist, (nparts + 1) * 8, cudaMemcpyDeviceToHost, rt_->stream));
+        KRV_CUDA(cudaStreamSynchronize(rt_->stream));
+        std::vector<unsigned long long> start(nparts + 1);
+        unsigned long long acc = 0;
+        for (int p = 0; p <= nparts; p++) {
+            start[p] = acc;
+            if (p < nparts || keep_nulls) acc += h[p];
+        }
+        KRV_CUDA(cudaMemcpyAsync(cursor, start.data(), (nparts + 1) * 8, cudaMemcpyHostToDevice, rt_->stream));
+        const int64_t kept = (int64_t)acc;
+        std::vector<std::shared_ptr<DBuf>> outs;
+        for (int c = 0; c < A.ncols; c++) {
+            const int w = b.cols[c].type.width();
+            outs.push_back(std::make_shared<DBuf>(rt_, (size_t)std::max<int64_t>(kept, 1) * w));
+            A.c[c] = PartCol{b.cols[c].data, outs.back()->get(), w};
+        }
+        if (kept > 0) {
+            part_scatter_kernel<<<grid_for(rt_, ceil_div(b.rows, kPartTile), 1, 4), kPartThreads, 0, rt_->stream>>>(
+                A, cursor);
+            rt_->launches++;
+            check_launch("part_scatter_kernel");
+        }
+        std::vector<Segment> segs(nparts + 1);
+        for (int p = 0; p <= nparts; p++) {
+            Segment &s = segs[p];
+            s.rows = (p < nparts || keep_nulls) ? (int64_t)h[p] : 0;
+            s.batch.rows = s.rows;
+            for (int c = 0; c < A.ncols; c++) {
+                DevCol col;
+                col.type = b.cols[c].type;
+                col.name = b.cols[c].name;
+                col.nullable = b.cols[c].nullable;
+                col.length = s.rows;
+                col.hold_data = outs[c];
+                col.data = outs[c]->as<uint8_t>() + start[p] * (size_t)b.cols[c].type.width();
+                s.batch.cols.push_back(col);
+            }
+        }
+        return segs;
+    }
+
+    // The NULL bucket's rows with their key column marked NULL.
+    DevBatch with_null_keys(const Segment &s) {
+        DevBatch b = s.batch;
+        const int key = spec_.probe_keys[0];
+        auto bits = std::make_shared<DBuf>(rt_, (size_t)ceil_div(s.rows, 8) + 8);
+        KRV_CUDA(cudaMemsetAsync(bits->get(), 0, bits->bytes(), rt_->stream));
+        b.cols[key].hold_valid = bits;
+        b.cols[key].valid = bits->as<uint8_t>();
+        b.cols[key].valid_off = 0;
+        b.cols[key].nullable = true;
+        return b;
+    }
+
+    DevBatch empty_like(const std::vector<DevCol> &types) {
+        DevBatch b;
+        for (const DevCol &t : types) b.cols.push_back(make_col(rt_, t.type, 0, t.nullable, t.name));
+        return b;
+    }
+
+    void keep(std::vector<DevBatch> &out, DevBatch b) {
+        counters_.output_rows += b.rows;
+        if (b.rows > 0) out.push_back(std::move(b));
+    }
+
+    uint8_t *host_alloc(size_t bytes) {
+        bytes = (bytes + 255) / 256 * 256;
+        if (bytes > HostPool::kBlock) {
+            uint8_t *p = rt_->host_pool->take(bytes);
+            host_blocks_.push_back({p, bytes});
+            return p;
+        }
+        if (host_blocks_.empty() || cur_block_used_ + bytes > HostPool::kBlock || cur_block_ == nullptr) {
+            cur_block_ = rt_->host_pool->take(HostPool::kBlock);
+            host_blocks_.push_back({cur_block_, HostPool::kBlock});
+            cur_block_used_ = 0;
+        }
+        uint8_t *p = cur_block_ + cur_block_used_;
+        cur_block_used_ += bytes;
+        return p;
+    }
+
+    // Copies a segment to the spill space (asynchronously, stream-ordered).
+    HostChunk spill(const Segment &s) {
+        HostChunk h;
+        h.rows = s.rows;
+        for (const DevCol &c : s.batch.cols) {
+            const size_t bytes = (size_t)s.rows * c.type.width();
+            uint8_t *p = host_alloc(bytes);
+            KRV_CUDA(cudaMemcpyAsync(p, c.data, bytes, cudaMemcpyDeviceToHost, rt_->stream));
+            h.cols.push_back(p);
+        }
+        spilled_bytes_ += (int64_t)s.rows * row_bytes_;
+        return h;
+    }
+
+    DevBatch load(const HostChunk &h, const std::vector<DevCol> &types) {
+        std::vector<HostChunk> one{h};
+        return load_all(one, types);
+    }
+    // The rows of chunks `hs`, back on the device as owned columns.
+    DevBatch load_all(const std::vector<HostChunk> &hs, const std::vector<DevCol> &types) {
+        int64_t rows = 0;
+        for (const HostChunk &h : hs) rows += h.rows;
+        DevBatch b;
+        b.rows = rows;
+        for (size_t c = 0; c < types.size(); c++) {
+            const int w = types[c].type.width();
+            DevCol col;
+            col.type = types[c].type;
+            col.name = types[c].name;
+            col.nullable = types[c].nullable;
+            col.length = rows;
+            col.hold_data = std::make_shared<DBuf>(rt_, (size_t)std::max<int64_t>(rows, 1) * w);
+            col.data = col.hold_data->get();
+            int64_t at = 0;
+            for (const HostChunk &h : hs) {
+                if (h.rows)
+                    KRV_CUDA(cudaMemcpyAsync(col.hold_data->as<uint8_t>() + at * w, h.cols[c], (size_t)h.rows * w,
+                                             cudaMemcpyHostToDevice, rt_->stream));
+                at += h.rows;
+            }
+            b.cols.push_back(col);
+        }
+        return b;
+    }
+
+    // Splits task `t` 8 ways with the next level of hash bits, chunk by chunk.
+    void split(Task &t) {
+        const int level = t.level + 1;
+        std::vector<Task> sub(8);
+        for (auto &s : sub) s.level = level;
+        for (const HostChunk &h : t.build_host) {
+            std::vector<Segment> segs = partition(load(h, build_types_), spec_.build_keys[0], level, 3, false);
+            for (int p = 0; p < 8; p++)
+                if (segs[p].rows) sub[p].build_host.push_back(spill(segs[p]));
+        }
+        for (const HostChunk &h : t.probe_host) {
+            std::vector<Segment> segs = partition(load(h, probe_types_), spec_.probe_keys[0], level, 3, false);
+            for (int p = 0; p < 8; p++)
+                if (segs[p].rows) sub[p].probe_host.push_back(spill(segs[p]));
+        }
+        splits_ += 8;
+        for (auto &s : sub) tasks_.push_front(std::move(s));
+    }
+
+    Runtime *rt_;
+    krv_join_spec spec_;
+    krv_grace_options opt_;
+    int64_t budget_ = 0;
+    bool schema_ = false, built_ = false, finishing_ = false;
+    std::vector<DevCol> build_types_, probe_types_;
+    int64_t row_bytes_ = 0;
+    int parts_bits_ = 3, nparts_ = 0;
+    int64_t splits_ = 0;
+    std::vector<Part> parts_;
+    int64_t resident_rows_ = 0, spilled_bytes_ = 0;
+    std::unique_ptr<HashJoin> null_join_;
+    std::deque<Task> tasks_;
+    Task cur_;
+    size_t cur_probe_ = 0;
+    std::unique_ptr<HashJoin> cur_join_;
+    std::vector<std::pair<uint8_t *, size_t>> host_blocks_;
+    uint8_t *cur_block_ = nullptr;
+    size_t cur_block_used_ = 0;
+    krv_join_counters counters_{};
+};
+
+GraceJoin *make_grace(Runtime *rt, const krv_join_spec &spec, const krv_grace_options &opt) {
+    return new GraceJoin(rt, spec, opt);
+}
+void grace_destroy(GraceJoin *g) { delete g; }
+void grace_build_push(GraceJoin *g, const DevBatch &b) { g->build_push(b); }
+void grace_build_finish(GraceJoin *g) { g->build_finish(); }
+std::vector<DevBatch> grace_probe(GraceJoin *g, const DevBatch &b) { return g->probe(b); }
+bool grace_finish_next(GraceJoin *g, DevBatch &out) { return g->finish_next(out); }
+bool grace_done(const GraceJoin *g) { return g->done(); }
+DevBatch grace_empty_output(GraceJoin *g) { return g->empty_output(); }
+const krv_join_spec &grace_spec(const GraceJoin *g) { return g->spec(); }
+krv_join_counters grace_counters(const GraceJoin *g) { return g->counters(); }
+int64_t grace_spilled_partitions(const GraceJoin *g) { return g->spilled_partitions(); }
+
+}  // namespace krv

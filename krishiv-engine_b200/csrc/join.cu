@@ -470,6 +470,21 @@ void HashJoin::build_push(DevBatch b) {
     append_arena(b);
 }
 
+DevBatch HashJoin::staged() const {
+    DevBatch b;
+    b.rows = build_rows_;
+    for (size_t i = 0; i < arena_cols_.size(); i++) {
+        DevCol c = arena_cols_[i];
+        c.length = build_rows_;
+        c.hold_data = arena_data_[i];
+        c.data = c.hold_data ? c.hold_data->get() : nullptr;
+        c.valid = nullptr;
+        c.valid_off = 0;
+        b.cols.push_back(c);
+    }
+    return b;
+}
+
 HashJoin::TableDev HashJoin::table_dev() const {
     return TableDev{slots_.as<unsigned long long>(), mask_, next_.as<uint32_t>(), spec_.seed};
 }

@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -48,6 +49,25 @@ struct Pool {
     std::atomic<bool> alive{true};
 };
 
+// Page-locked host blocks kept for reuse: the spill space of partitioned
+// joins (the engine spills grace partitions to disk; a GPU spills them over
+// the host link to host memory). Freed with the runtime.
+class HostPool {
+  public:
+    static constexpr size_t kBlock = size_t(256) << 20;
+    HostPool() = default;
+    HostPool(const HostPool &) = delete;
+    HostPool &operator=(const HostPool &) = delete;
+    ~HostPool();
+    // A block of at least `bytes` (kBlock, or exactly `bytes` when larger).
+    uint8_t *take(size_t bytes);
+    void give(uint8_t *p, size_t bytes);
+
+  private:
+    std::mutex mu_;
+    std::vector<std::pair<uint8_t *, size_t>> free_, all_;
+};
+
 struct Runtime {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -62,6 +82,7 @@ struct Runtime {
     // Work queued on the stream still reads the caller's host buffers
     // (copies from page-locked memory, or columns read in place).
     bool host_borrowed = false;
+    std::shared_ptr<HostPool> host_pool = std::make_shared<HostPool>();
 };
 
 // Scope of a call that takes host batches: the caller owns its buffers again

@@ -104,6 +104,8 @@ class HashJoin {
     };
     TableDev table_dev() const;
     const DevBatch &arena() const { return arena_; }
+    // The build rows pushed so far, before build_finish (data only).
+    DevBatch staged() const;
     // What the build saw of a one-int64-key table: indexed rows and key range.
     int64_t indexed_rows() const { return indexed_rows_; }
     long long key_lo() const { return key_lo_; }
@@ -144,6 +146,20 @@ class HashJoin {
     std::shared_ptr<KeyFilterImpl> filter_;
     krv_join_counters counters_{};
 };
+
+// ---- partitioned (grace) hash join (crates/krishiv-exec/src/join/grace.rs) ------
+class GraceJoin;
+GraceJoin *make_grace(Runtime *rt, const krv_join_spec &spec, const krv_grace_options &opt);
+void grace_destroy(GraceJoin *g);
+void grace_build_push(GraceJoin *g, const DevBatch &b);
+void grace_build_finish(GraceJoin *g);
+std::vector<DevBatch> grace_probe(GraceJoin *g, const DevBatch &b);
+bool grace_finish_next(GraceJoin *g, DevBatch &out);
+bool grace_done(const GraceJoin *g);
+DevBatch grace_empty_output(GraceJoin *g);
+const krv_join_spec &grace_spec(const GraceJoin *g);
+krv_join_counters grace_counters(const GraceJoin *g);
+int64_t grace_spilled_partitions(const GraceJoin *g);
 
 // ---- grouped hash aggregate (crates/krishiv-exec/src/aggregate/sink.rs:181) ----
 class HashAggregate;

@@ -142,6 +142,38 @@ DType parse_format(const char *fmt) {
     return t;
 }
 
+HostPool::~HostPool() {
+    for (auto &b : all_) cudaFreeHost(b.first);
+}
+
+uint8_t *HostPool::take(size_t bytes) {
+    const size_t want = bytes > kBlock ? bytes : kBlock;
+    {
+        std::lock_guard<std::mutex> lock(mu_);
+        for (size_t i = 0; i < free_.size(); i++)
+            if (free_[i].second == want) {
+                uint8_t *p = free_[i].first;
+                free_.erase(free_.begin() + (long)i);
+                return p;
+            }
+    }
+    void *p = nullptr;
+    const cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(KRV_NEED_MEMORY, std::string("page-locked host spill space: ") + cudaGetErrorString(e));
+    }
+    std::lock_guard<std::mutex> lock(mu_);
+    all_.push_back({static_cast<uint8_t *>(p), want});
+    return static_cast<uint8_t *>(p);
+}
+
+void HostPool::give(uint8_t *p, size_t bytes) {
+    const size_t want = bytes > kBlock ? bytes : kBlock;
+    std::lock_guard<std::mutex> lock(mu_);
+    free_.push_back({p, want});
+}
+
 int grid_for(const Runtime *rt, int64_t work_items, int threads, int per_sm) {
     const int64_t need = ceil_div(work_items > 0 ? work_items : 1, threads);
     const int64_t cap = (int64_t)rt->sm_count * per_sm;

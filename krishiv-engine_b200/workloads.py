@@ -20,6 +20,10 @@ Shapes (rows at scale 1.0):
           [-1e9, 1e9]}; nb log-uniform over [1e3, 5e7 * scale], G log-uniform
           over [10, 1e6] (at most nb), r uniform over [0.1, 1.0]; requests
           pick templates uniformly and arrive as a Poisson process.
+  grace:  build 500,000,000 {k int64 uniform [0, 1e9), p1, p2 int64}; probe
+          2,000,000,000 {k int64: 90% uniform [0, 1e9), 10% one of 100 heavy
+          keys; p int64}; 1% NULL keys on both sides (the key domain scales
+          with the rows).
 """
 from __future__ import annotations
 
@@ -30,6 +34,7 @@ STAR_SEED = 0x4B52560003
 JOIN_SEED = 0x4B52560001
 AGG_SEED = 0x4B52560002
 SERVE_SEED = 0x4B52560005
+GRACE_SEED = 0x4B52560004
 PRED_VALUE = 7
 
 
@@ -152,3 +157,35 @@ def serve_arrivals(n: int, rate_per_s: float, templates: int, seed: int = SERVE_
     rng = np.random.default_rng(seed ^ 0x5EED)
     gaps = rng.exponential(1.0 / rate_per_s, n) if rate_per_s > 0 else np.zeros(n)
     return np.cumsum(gaps) - gaps[0], rng.integers(0, templates, n)
+
+
+def grace_build(rt, scale: float = 1.0, seed: int = GRACE_SEED):
+    """The partitioned join's build side: (k, p1, p2), k NULL in 1% of rows."""
+    import torch
+    kb = _kb()
+    nb = int(500_000_000 * scale)
+    dom = int(1_000_000_000 * scale)
+    k, kv = _col(rt, nb, torch.int64, kb.GEN_UNIFORM_I64, seed, 1, lo=0, hi=dom - 1, null_fraction=0.01)
+    p1, _ = _col(rt, nb, torch.int64, kb.GEN_UNIFORM_I64, seed, 2, lo=-(2**62), hi=2**62)
+    p2, _ = _col(rt, nb, torch.int64, kb.GEN_UNIFORM_I64, seed, 3, lo=-(2**62), hi=2**62)
+    return [("k", k, kv), ("p1", p1, None), ("p2", p2, None)]
+
+
+def grace_probe(rt, scale: float = 1.0, seed: int = GRACE_SEED, chunk: int = 1 << 28):
+    """The partitioned join's probe side: (k, p); 10% of the rows take one of
+    100 heavy keys, 1% have a NULL key. Generated in chunks of `chunk` rows."""
+    import torch
+    kb = _kb()
+    n = int(2_000_000_000 * scale)
+    dom = int(1_000_000_000 * scale)
+    heavy, _ = _col(rt, 100, torch.int64, kb.GEN_UNIFORM_I64, seed, 20, lo=0, hi=dom - 1)
+    k, kv = _col(rt, n, torch.int64, kb.GEN_UNIFORM_I64, seed, 11, lo=0, hi=dom - 1, null_fraction=0.01)
+    p, _ = _col(rt, n, torch.int64, kb.GEN_UNIFORM_I64, seed, 12, lo=-(2**62), hi=2**62)
+    for r0 in range(0, n, chunk):
+        m = min(chunk, n - r0)
+        u, _ = _col(rt, m, torch.int64, kb.GEN_UNIFORM_I64, seed, 13, lo=0, hi=999, row0=r0)
+        h, _ = _col(rt, m, torch.int64, kb.GEN_UNIFORM_I64, seed, 14, lo=0, hi=99, row0=r0)
+        sl = k[r0:r0 + m]
+        torch.where(u < 100, heavy[h], sl, out=sl)
+        del u, h
+    return [("k", k, kv), ("p", p, None)]
