@@ -483,6 +483,141 @@ def run_serve(args, kb, W, rt, rank, world, pg, device):
     }
 
 
+def output_checksum(res):
+    """Order-independent checksum of one join output batch (k, p, b1, b2):
+    the wrapping sum over rows of a mix of the four values, NULLs mapped to
+    distinct constants; and the row count."""
+    import torch
+    if res.rows == 0:
+        return 0, 0
+    mult = (0x9E3779B97F4A7C15 - (1 << 64), 0x62A9D9ED799705F5, 0x165667B19E3779F9, 0x27D4EB2F165667C5)
+    null = (0x3C6EF372FE94F82B, 0x5851F42D4C957F2D, 0x14057B7EF767814F, 0x2545F4914F6CDD1D)
+    acc = None
+    for i, c in enumerate(res.columns):
+        v = c
+        if res.valid[i] is not None:
+            bits = res.valid[i][: (res.rows + 7) // 8]
+            m = ((bits.unsqueeze(1) >> torch.arange(8, device=c.device, dtype=torch.uint8)) & 1).reshape(-1)[: res.rows]
+            v = torch.where(m.bool(), c, torch.full_like(c, null[i]))
+        t = (v ^ (v >> 29)) * mult[i]
+        acc = t if acc is None else acc ^ t
+    return int(acc.sum()) & (2**64 - 1), res.rows
+
+
+def cpu_grace(scale):
+    """The oracle's left outer hash join (single thread) on the partitioned
+    join's workload at `scale`: build + probe rows per second."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    W = importlib.import_module("krishiv-engine_b200.workloads")
+    nb, np_ = int(500_000_000 * scale), int(2_000_000_000 * scale)
+    dom = int(1_000_000_000 * scale)
+    seed = W.GRACE_SEED
+    bk, bv = O.gen_column(0, seed, 1, nb, lo=0, hi=dom - 1, null_fraction=0.01)
+    pk, pv = O.gen_column(0, seed, 11, np_, lo=0, hi=dom - 1, null_fraction=0.01)
+    t0 = time.perf_counter()
+    O.hash_join(1, [(bk, bv)], [(pk, pv)])
+    dt = time.perf_counter() - t0
+    return {"value": (nb + np_) / dt / 1e6, "seconds": dt, "build_rows": nb, "probe_rows": np_}
+
+
+def run_grace(args, kb, W, rt, rank, world, pg, device):
+    """Survey config 4: left outer join, 500M build rows x 2B probe rows, under
+    a 24 GB device budget (a runtime whose allocations are capped), inputs
+    resident in HBM, every output batch consumed by a checksum."""
+    import torch
+    stream = torch.cuda.current_stream()
+    build = W.grace_build(rt, scale=args.scale)
+    probe = W.grace_probe(rt, scale=args.scale)
+    torch.cuda.synchronize()
+    nb, np_ = int(build[0][1].shape[0]), int(probe[0][1].shape[0])
+    budget = int(args.grace_budget * args.scale) if args.scale < 1 else int(args.grace_budget)
+    capped = kb.Runtime(device, budget, stream.cuda_stream)
+    bstep, pstep = 32 << 20, 32 << 20
+    phases = {}
+
+    def batches(cols, n, step):
+        for r0 in range(0, n, step):
+            m = min(step, n - r0)
+            yield kb.DeviceBatch([(nm, t[r0:r0 + m], None if v is None else v[r0 // 8:(r0 + m + 7) // 8 + 1])
+                                  for nm, t, v in cols])
+
+    def run_join(partitioned, r):
+        spec = kb.join_spec("left_outer", probe_out=[0, 1], build_out=[1, 2], build_rows_hint=nb,
+                            max_output_rows=64 << 20)
+        j = kb.HashJoin(r, spec, partitioned=partitioned, device_budget=budget if partitioned else 0)
+        t = [time.perf_counter()]
+        for db in batches(build, nb, bstep):
+            j.build_push_device(db)
+        j.build_finish()
+        torch.cuda.synchronize()
+        t.append(time.perf_counter())
+        total, rows, nbatches = 0, 0, 0
+        for db in batches(probe, np_, pstep):
+            for res in j.probe_device_all(db):
+                c, n = output_checksum(res)
+                total, rows, nbatches = (total + c) & (2**64 - 1), rows + n, nbatches + 1
+        torch.cuda.synchronize()
+        t.append(time.perf_counter())
+        for res in j.finish_device():
+            c, n = output_checksum(res)
+            total, rows, nbatches = (total + c) & (2**64 - 1), rows + n, nbatches + 1
+        torch.cuda.synchronize()
+        t.append(time.perf_counter())
+        phases.update(build_s=t[1] - t[0], probe_s=t[2] - t[1], finish_s=t[3] - t[2], output_batches=nbatches)
+        return j, total, rows
+
+    for _ in range(args.warmup):
+        run_join(True, capped)
+    torch.cuda.synchronize()
+    barrier(pg)
+    times = []
+    with Clocks(device) as clk:
+        j = None
+        for _ in range(args.steps):
+            j = None  # the previous join gives its device and spill memory back first
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            s.record(stream)
+            j, total, rows = run_join(True, capped)
+            e.record(stream)
+            torch.cuda.synchronize()
+            times.append((s.elapsed_time(e), (time.perf_counter() - t0) * 1e3))
+    ms = max_over_ranks(pg, statistics.median(t for t, _ in times), device)
+    counters = j.counters()
+    spilled = j.spilled_partitions()
+    last_phases = dict(phases)
+    del j
+    # The unpartitioned join, uncapped, on the same inputs: the same rows.
+    _, want_total, want_rows = run_join(False, rt)
+    torch.cuda.synchronize()
+    peak, kind = hbm_peak()
+    alg = 24 * nb + 16 * np_ + 40 * rows
+    out = {"metric": "partitioned left outer join under a device budget (build + probe rows per second)",
+           "value": world * (nb + np_) / (ms * 1e-3) / 1e6, "unit": "Mrows/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded counter-based generators on the device)",
+           "config": {"workload": "left outer join 500M build x 2B probe, 100 heavy probe keys, 1% NULL keys",
+                      "build_rows": nb, "probe_rows": np_, "output_rows": rows, "device_budget_bytes": budget,
+                      "partitions": counters["partitions"], "spilled_partitions": spilled,
+                      "consumer": "every output batch read once by an order-independent checksum (timed)",
+                      "l2": "inputs (44 GB) larger than L2; no flush"},
+           "wall_ms_per_step": statistics.median(w for _, w in times),
+           "phases": dict(last_phases),
+           "checksum_agrees": (total, rows) == (want_total, want_rows),
+           "gpu_launches": None,
+           "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "peak_source": kind,
+                        "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None,
+                        "note": "24 B per build row, 16 B per probe row, 40 B per output row; spilled partitions "
+                                "also cross the host link twice"},
+           "clocks": clk.summary()}
+    if rank == 0 and not args.no_cpu:
+        c = cpu_grace(0.001)
+        out["cpu_baseline"] = {"value": c["value"], "unit": "Mrows/s", "cores": 1, "kind": "port",
+                               "sample": f"the same workload at 1/1000 scale ({c['build_rows']} x {c['probe_rows']} rows)"}
+    return out
+
+
 def profile_traffic(name, rows):
     """DRAM bytes (read + write) of one launch of `name` over `rows` fact
     rows, from the committed ncu summary (profiles/<name>_dram.md, line
@@ -602,7 +737,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["star", "join", "agg", "serve"], default="star")
+    ap.add_argument("--workload", choices=["star", "join", "agg", "serve", "grace"], default="star")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--fact-scale", type=float, default=None,
                     help="size the fact table alone (profiling small cases with full dimensions)")
@@ -615,6 +750,7 @@ def main():
     ap.add_argument("--tick-rows", type=int, default=16 << 20, help="serve: probe rows per tick")
     ap.add_argument("--serve-budget", type=int, default=8 << 30, help="serve: HBM budget of running requests")
     ap.add_argument("--serve-load", type=float, default=0.7, help="serve: offered load / capacity")
+    ap.add_argument("--grace-budget", type=int, default=24 << 30, help="grace: device budget of the join")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     threads = os.cpu_count() or 1
@@ -648,7 +784,7 @@ def main():
     kb = importlib.import_module("krishiv-engine_b200")
     W = importlib.import_module("krishiv-engine_b200.workloads")
     rt = kb.Runtime.on_torch_stream(local)
-    runner = {"star": run_star, "join": run_join, "agg": run_agg, "serve": run_serve}[args.workload]
+    runner = {"star": run_star, "join": run_join, "agg": run_agg, "serve": run_serve, "grace": run_grace}[args.workload]
     out = runner(args, kb, W, rt, rank, world, pg, device)
     if rank == 0 and args.workload == "star" and not args.no_cpu:
         c = cpu_star(args.scale, args.cpu_sample, threads)

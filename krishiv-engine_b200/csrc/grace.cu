@@ -174,13 +174,16 @@ class GraceJoin {
         for (auto &b : host_blocks_) rt_->host_pool->give(b.first, b.second);
     }
 
-    void build_push(const DevBatch &b) {
+    void build_push(const DevBatch &in) {
         if (built_) fail(KRV_INVALID_ARGUMENT, "build_push after build_finish");
         DeviceGuard g(rt_);
-        if (!schema_) init_schema(b);
-        check_shape(b, build_types_, spec_.build_keys[0], "build");
-        counters_.build_rows += b.rows;
-        if (b.rows == 0) return;
+        if (!schema_) init_schema(in);
+        check_shape(in, build_types_, spec_.build_keys[0], "build");
+        counters_.build_rows += in.rows;
+        for (int64_t from = 0; from < in.rows; from += slice_rows()) build_slice(slice(in, from));
+    }
+
+    void build_slice(const DevBatch &b) {
         std::vector<Segment> segs = partition(b, spec_.build_keys[0], 0, parts_bits_, false);
         for (int p = 0; p < nparts_; p++) {
             Segment &s = segs[p];
@@ -191,7 +194,6 @@ class GraceJoin {
             } else {
                 P.join->build_push(s.batch);
                 P.build_rows += s.rows;
-                resident_rows_ += s.rows;
             }
         }
         enforce_residency();
@@ -227,18 +229,97 @@ class GraceJoin {
         check_shape(in, probe_types_, spec_.probe_keys[0], "probe");
         counters_.probe_rows += in.rows;
         std::vector<DevBatch> out;
-        if (in.rows == 0) return out;
+        int64_t out_rows = 0;
+        for (int64_t from = 0; from < in.rows; from += slice_rows()) probe_slice(slice(in, from), out, out_rows);
+        if (out.size() > 1) {
+            DevBatch one = concat(out);
+            out.clear();
+            out.push_back(std::move(one));
+        }
+        return out;
+    }
+
+    // The batches `bs` (one shape) as one batch: a device copy per column
+    // and batch, validity bits appended at their row offsets.
+    DevBatch concat(const std::vector<DevBatch> &bs) {
+        DevBatch o;
+        for (const DevBatch &b : bs) o.rows += b.rows;
+        const size_t ncols = bs[0].cols.size();
+        for (size_t c = 0; c < ncols; c++) {
+            const DevCol &m = bs[0].cols[c];
+            bool nullable = false;
+            for (const DevBatch &b : bs) nullable = nullable || b.cols[c].valid;
+            DevCol col = make_col(rt_, m.type, o.rows, nullable || m.nullable, m.name);
+            if (col.hold_valid) KRV_CUDA(cudaMemsetAsync(col.hold_valid->get(), 0, col.hold_valid->bytes(), rt_->stream));
+            const size_t w = (size_t)m.type.width();
+            int64_t at = 0;
+            for (const DevBatch &b : bs) {
+                const DevCol &x = b.cols[c];
+                if (b.rows)
+                    KRV_CUDA(cudaMemcpyAsync(static_cast<uint8_t *>(const_cast<void *>(col.data)) + at * w, x.data,
+                                             (size_t)b.rows * w, cudaMemcpyDeviceToDevice, rt_->stream));
+                if (col.hold_valid && b.rows) {
+                    uint8_t *dst = col.hold_valid->as<uint8_t>();
+                    if (x.valid) append_bits(rt_, x.valid, x.valid_off, b.rows, dst, at);
+                    else set_bits(rt_, dst, at, b.rows);
+                }
+                at += b.rows;
+            }
+            if (!col.hold_valid) col.valid = nullptr;
+            o.cols.push_back(col);
+        }
+        return o;
+    }
+
+    // One slice: NULL-key rows padded now (left outer); rows of resident
+    // partitions joined now while this call's output stays under a quarter
+    // of the budget, else deferred to host memory like those of spilled
+    // partitions (and joined at finish by the same resident tables).
+    void probe_slice(const DevBatch &in, std::vector<DevBatch> &out, int64_t &out_rows) {
         std::vector<Segment> segs = partition(in, spec_.probe_keys[0], 0, parts_bits_, true);
         Segment &nulls = segs[nparts_];
-        if (nulls.rows > 0 && spec_.join_type == KRV_JOIN_LEFT_OUTER) keep(out, null_join_->probe(with_null_keys(nulls)));
+        if (nulls.rows > 0 && spec_.join_type == KRV_JOIN_LEFT_OUTER) {
+            out_rows += nulls.rows;
+            keep(out, null_join_->probe(with_null_keys(nulls)));
+        }
+        const int64_t out_cap = budget_ / 8 / out_row_bytes();
         for (int p = 0; p < nparts_; p++) {
             Segment &s = segs[p];
             if (s.rows == 0) continue;
             Part &P = parts_[p];
-            if (P.spilled) P.probe_host.push_back(spill(s));
-            else keep(out, P.join->probe(s.batch));
+            if (P.spilled) {
+                P.probe_host.push_back(spill(s));
+            } else if (out_rows >= out_cap) {
+                P.deferred.push_back(spill(s));
+            } else {
+                DevBatch o = P.join->probe(s.batch);
+                out_rows += o.rows;
+                keep(out, std::move(o));
+            }
         }
-        return out;
+    }
+
+    // Bytes of one output row: every column of both sides.
+    int64_t out_row_bytes() const {
+        int64_t b = 0;
+        for (const DevCol &c : build_types_) b += c.type.width();
+        for (const DevCol &c : probe_types_) b += c.type.width();
+        return std::max<int64_t>(b, 8);
+    }
+
+    // Input batches are taken in slices whose partitioned copy and output
+    // stay within a sixteenth of the budget (a multiple of 64 rows, so that
+    // every slice starts on a byte of the validity bitmaps).
+    int64_t slice_rows() const {
+        const int64_t per = std::max<int64_t>(row_bytes_, 16) * 4;
+        return std::max<int64_t>(1 << 16, budget_ / 16 / per / 64 * 64);
+    }
+    DevBatch slice(const DevBatch &b, int64_t from) const {
+        if (from == 0 && b.rows <= slice_rows()) return b;
+        DevBatch s;
+        s.rows = std::min(slice_rows(), b.rows - from);
+        for (const DevCol &c : b.cols) s.cols.push_back(slice_col(c, from, s.rows));
+        return s;
     }
 
     // After the last probe batch: the next output batch of the spilled
@@ -248,15 +329,26 @@ class GraceJoin {
         DeviceGuard g(rt_);
         if (!finishing_) {
             finishing_ = true;
-            for (auto &P : parts_) P.join.reset();  // resident tables are done
             for (int p = 0; p < nparts_; p++)
                 if (parts_[p].spilled) tasks_.push_back(Task{0, std::move(parts_[p].build_host), std::move(parts_[p].probe_host)});
+        }
+        // Deferred rows of resident partitions, by their resident tables.
+        for (; deferred_part_ < nparts_; deferred_part_++, deferred_chunk_ = 0) {
+            Part &P = parts_[deferred_part_];
+            while (!P.spilled && deferred_chunk_ < P.deferred.size()) {
+                DevBatch o = P.join->probe(load_group(P.deferred, deferred_chunk_));
+                counters_.output_rows += o.rows;
+                if (o.rows > 0) {
+                    out = o;
+                    return true;
+                }
+            }
+            P.join.reset();  // this resident table is done
         }
         for (;;) {
             if (cur_join_) {
                 if (cur_probe_ < cur_.probe_host.size()) {
-                    DevBatch pb = load(cur_.probe_host[cur_probe_++], probe_types_);
-                    DevBatch o = cur_join_->probe(pb);
+                    DevBatch o = cur_join_->probe(load_group(cur_.probe_host, cur_probe_));
                     counters_.output_rows += o.rows;
                     if (o.rows == 0) continue;
                     out = o;
@@ -271,11 +363,11 @@ class GraceJoin {
             int64_t rows = 0;
             for (const HostChunk &c : t.build_host) rows += c.rows;
             if (t.probe_host.empty()) continue;  // no probe rows: nothing to emit
-            if (rows * est_row_bytes() > budget_ / 2 && t.level < kMaxLevel) {
+            if (est_part_bytes(rows) > resident_cap() && t.level < kMaxLevel) {
                 split(t);
                 continue;
             }
-            if (rows * est_row_bytes() > budget_ / 2)
+            if (est_part_bytes(rows) > resident_cap())
                 fail(KRV_NEED_MEMORY, "a partition of the build side stays above the memory budget after " +
                                           std::to_string(kMaxLevel) + " levels of splits (one heavy key)");
             krv_join_spec js = spec_;
@@ -291,7 +383,7 @@ class GraceJoin {
         }
     }
 
-    bool done() const { return finishing_ && !cur_join_ && tasks_.empty(); }
+    bool done() const { return finishing_ && deferred_part_ >= nparts_ && !cur_join_ && tasks_.empty(); }
     // A zero-row batch of the output's shape.
     DevBatch empty_output() {
         if (!built_ || probe_types_.empty()) return DevBatch{};
@@ -323,6 +415,7 @@ class GraceJoin {
         bool spilled = false;
         int64_t build_rows = 0;
         std::vector<HostChunk> build_host, probe_host;
+        std::vector<HostChunk> deferred;  // probe rows for the resident table, joined at finish
     };
     struct Task {
         int level = 0;
@@ -353,8 +446,8 @@ class GraceJoin {
         // one, partitions spill as the resident footprint passes its share.
         int resident = nparts_;
         if (spec_.build_rows_hint > 0) {
-            const double per = (double)spec_.build_rows_hint / nparts_ * (double)est_row_bytes();
-            resident = (int)std::min<double>(nparts_, std::floor((double)budget_ / 2.0 / std::max(per, 1.0)));
+            const int64_t per = std::max<int64_t>(est_part_bytes(spec_.build_rows_hint / nparts_ * 21 / 20), 1);
+            resident = (int)std::min<int64_t>(nparts_, resident_cap() / per);
         }
         for (int p = 0; p < nparts_; p++) {
             parts_[p].spilled = p >= resident;
@@ -377,12 +470,26 @@ class GraceJoin {
                 fail(KRV_UNSUPPORTED, "partitioned joins take NULLs in the key column only");
         }
     }
-    // Device bytes per resident build row: the row, its table slots (up to 4
-    // per row at load 0.5 after the power-of-two rounding) and its chain link.
-    int64_t est_row_bytes() const { return row_bytes_ + 4 * 8 + 4; }
+    // Device bytes of a partition's table over `rows` build rows: the rows
+    // (with their arena's headroom and validity bits), the chain links and the
+    // slots (a power of two of at least rows / 0.5).
+    int64_t est_part_bytes(int64_t rows) const {
+        uint64_t slots = 1;
+        while (slots < (uint64_t)(2 * rows)) slots <<= 1;
+        return rows * (row_bytes_ * 9 / 8 + 4 + 1) + (int64_t)slots * 8;
+    }
+    // The share of the budget that resident tables may take; the rest holds
+    // a slice's partitioned copy and a call's output.
+    int64_t resident_cap() const { return budget_ / 10 * 6; }
+    int64_t resident_bytes() const {
+        int64_t b = 0;
+        for (const auto &P : parts_)
+            if (!P.spilled) b += est_part_bytes(P.build_rows);
+        return b;
+    }
 
     void enforce_residency() {
-        while (resident_rows_ * est_row_bytes() > budget_ / 2) {
+        while (resident_bytes() > resident_cap()) {
             int victim = -1;
             for (int p = 0; p < nparts_; p++)
                 if (!parts_[p].spilled && (victim < 0 || parts_[p].build_rows > parts_[victim].build_rows)) victim = p;
@@ -394,7 +501,6 @@ class GraceJoin {
                 s.rows = P.build_rows;
                 P.build_host.push_back(spill(s));
             }
-            resident_rows_ -= P.build_rows;
             P.join.reset();
             P.spilled = true;
         }
@@ -519,6 +625,18 @@ class GraceJoin {
         return h;
     }
 
+    // Probe chunks from `at` on, as many as fit one slice, loaded as one
+    // device batch; `at` moves past them.
+    DevBatch load_group(const std::vector<HostChunk> &hs, size_t &at) {
+        std::vector<HostChunk> group;
+        int64_t rows = 0;
+        while (at < hs.size() && (group.empty() || rows + hs[at].rows <= slice_rows())) {
+            rows += hs[at].rows;
+            group.push_back(hs[at++]);
+        }
+        return load_all(group, probe_types_);
+    }
+
     DevBatch load(const HostChunk &h, const std::vector<DevCol> &types) {
         std::vector<HostChunk> one{h};
         return load_all(one, types);
@@ -579,11 +697,13 @@ class GraceJoin {
     int parts_bits_ = 3, nparts_ = 0;
     int64_t splits_ = 0;
     std::vector<Part> parts_;
-    int64_t resident_rows_ = 0, spilled_bytes_ = 0;
+    int64_t spilled_bytes_ = 0;
     std::unique_ptr<HashJoin> null_join_;
     std::deque<Task> tasks_;
     Task cur_;
     size_t cur_probe_ = 0;
+    int deferred_part_ = 0;
+    size_t deferred_chunk_ = 0;
     std::unique_ptr<HashJoin> cur_join_;
     std::vector<std::pair<uint8_t *, size_t>> host_blocks_;
     uint8_t *cur_block_ = nullptr;
