@@ -640,11 +640,21 @@ def run_join(args, kb, W, rt, rank, world, pg, device):
     bb, pb = kb.DeviceBatch(build), kb.DeviceBatch(probe)
     nb, np_ = int(build[0][1].shape[0]), int(probe[0][1].shape[0])
 
-    def step():
+    phase = {"build": [], "probe": []}
+
+    def step(ev=None):
         j = kb.HashJoin(rt, kb.join_spec("inner", probe_out=[0, 1], build_out=[1], build_rows_hint=nb))
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)] if ev is not None else None
+        if e:
+            e[0].record(stream)
         j.build_push_device(bb)
         j.build_finish()
+        if e:
+            e[1].record(stream)
         r = j.probe_device(pb)
+        if e:
+            e[2].record(stream)
+            ev.append(e)
         return j, r
 
     for _ in range(args.warmup):
@@ -653,13 +663,16 @@ def run_join(args, kb, W, rt, rank, world, pg, device):
     barrier(pg)
     launches0 = rt.launches
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    evs = []
     with Clocks(device) as clk:
         s.record(stream)
         for _ in range(args.steps):
-            j, r = step()
+            j, r = step(evs)
         e.record(stream)
         torch.cuda.synchronize()
     ms = max_over_ranks(pg, s.elapsed_time(e) / args.steps, device)
+    phase["build"] = statistics.median(x[0].elapsed_time(x[1]) for x in evs)
+    phase["probe"] = statistics.median(x[1].elapsed_time(x[2]) for x in evs)
     out_rows = r.rows
     alg = 16 * nb + 12 * np_ + 20 * out_rows
     peak, kind = hbm_peak()
@@ -671,6 +684,7 @@ def run_join(args, kb, W, rt, rank, world, pg, device):
                        "build_rows": nb, "probe_rows": np_, "output_rows": out_rows,
                        "l2": "inputs (136 MB) larger than L2; each step rebuilds the table"},
             "gpu_launches": rt.launches - launches0,
+            "phases_ms": phase,
             "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "peak_source": kind,
                          "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None,
                          "note": "whole step (build + probe); 16 B per build row, 12 B per probe row, 20 B per output row"},
