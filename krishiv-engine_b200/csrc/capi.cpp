@@ -147,7 +147,9 @@ krv_status krv_runtime_create(int32_t device, int64_t hbm_budget_bytes, void *cu
         KRV_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
         KRV_CUDA(cudaMalloc(&rt.status_dev, 64));
         KRV_CUDA(cudaMemset(rt.status_dev, 0, 64));
-        KRV_CUDA(cudaMallocHost(&rt.status_host, 64));
+        // page-locked, mapped: the status words and small results read back by a kernel
+        KRV_CUDA(cudaHostAlloc(&rt.status_host, 4096, cudaHostAllocMapped));
+        KRV_CUDA(cudaHostGetDevicePointer(&rt.status_host_dev, rt.status_host, 0));
         cudaSetDevice(prev);
         *out = h.release();
         return KRV_OK;

@@ -168,9 +168,15 @@ class GraceJoin {
             KRV_CUDA(cudaMemGetInfo(&free_b, &total_b));
             budget_ = (int64_t)(free_b / 2);
         }
+        KRV_CUDA(cudaStreamCreateWithFlags(&cs_, cudaStreamNonBlocking));
     }
     ~GraceJoin() {
-        cudaStreamSynchronize(rt_->stream);  // copies into or out of the spill space
+        cudaStreamSynchronize(cs_);  // copies into or out of the spill space
+        cudaStreamSynchronize(rt_->stream);
+        for (auto &f : inflight_) cudaEventDestroy(f.done);
+        inflight_.clear();
+        if (prefetch_.ready) cudaEventDestroy(prefetch_.ready);
+        cudaStreamDestroy(cs_);
         for (auto &b : host_blocks_) rt_->host_pool->give(b.first, b.second);
     }
 
@@ -329,6 +335,7 @@ class GraceJoin {
         DeviceGuard g(rt_);
         if (!finishing_) {
             finishing_ = true;
+            reap(true);  // every spill has landed in host memory
             for (int p = 0; p < nparts_; p++)
                 if (parts_[p].spilled) tasks_.push_back(Task{0, std::move(parts_[p].build_host), std::move(parts_[p].probe_host)});
         }
@@ -347,8 +354,11 @@ class GraceJoin {
         }
         for (;;) {
             if (cur_join_) {
-                if (cur_probe_ < cur_.probe_host.size()) {
-                    DevBatch o = cur_join_->probe(load_group(cur_.probe_host, cur_probe_));
+                if (prefetch_.pending || cur_probe_ < cur_.probe_host.size()) {
+                    DevBatch pb = prefetch_.pending ? take_prefetch() : load_group(cur_.probe_host, cur_probe_);
+                    // the next group crosses the host link while this one is probed
+                    if (cur_probe_ < cur_.probe_host.size()) start_prefetch(cur_.probe_host, cur_probe_);
+                    DevBatch o = cur_join_->probe(pb);
                     counters_.output_rows += o.rows;
                     if (o.rows == 0) continue;
                     out = o;
@@ -612,17 +622,112 @@ class GraceJoin {
     }
 
     // Copies a segment to the spill space (asynchronously, stream-ordered).
+    // Copies a segment to the spill space on the copy stream, so that the
+    // transfer overlaps the next slice's kernels; the segment's device
+    // buffers stay alive until the copy has landed.
     HostChunk spill(const Segment &s) {
         HostChunk h;
         h.rows = s.rows;
+        cudaEvent_t ready;
+        KRV_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        KRV_CUDA(cudaEventRecord(ready, rt_->stream));
+        KRV_CUDA(cudaStreamWaitEvent(cs_, ready, 0));
+        KRV_CUDA(cudaEventDestroy(ready));
+        InFlight f;
         for (const DevCol &c : s.batch.cols) {
             const size_t bytes = (size_t)s.rows * c.type.width();
             uint8_t *p = host_alloc(bytes);
-            KRV_CUDA(cudaMemcpyAsync(p, c.data, bytes, cudaMemcpyDeviceToHost, rt_->stream));
+            KRV_CUDA(cudaMemcpyAsync(p, c.data, bytes, cudaMemcpyDeviceToHost, cs_));
             h.cols.push_back(p);
+            f.hold.push_back(c.hold_data);
+            f.bytes += bytes;
         }
+        KRV_CUDA(cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming));
+        KRV_CUDA(cudaEventRecord(f.done, cs_));
+        inflight_bytes_ += f.bytes;
+        inflight_.push_back(std::move(f));
         spilled_bytes_ += (int64_t)s.rows * row_bytes_;
+        reap(false);
+        // A short queue of spills: other small transfers share the copy engines.
+        while (inflight_bytes_ > std::min<size_t>((size_t)(budget_ / 8), (size_t)1 << 30) && !inflight_.empty())
+            reap_one();
         return h;
+    }
+
+    // Releases the buffers of spills that have landed (all of them: wait).
+    void reap(bool all) {
+        while (!inflight_.empty()) {
+            if (all) {
+                reap_one();
+                continue;
+            }
+            const cudaError_t q = cudaEventQuery(inflight_.front().done);
+            if (q == cudaErrorNotReady) return;
+            if (q != cudaSuccess) fail(KRV_CUDA_ERROR, std::string("spill copy: ") + cudaGetErrorString(q));
+            reap_one();
+        }
+    }
+    void reap_one() {
+        InFlight &f = inflight_.front();
+        KRV_CUDA(cudaEventSynchronize(f.done));
+        KRV_CUDA(cudaEventDestroy(f.done));
+        inflight_bytes_ -= f.bytes;
+        inflight_.pop_front();
+    }
+
+    // The probe chunks from `at` on that fit one slice, copied to the device on
+    // the copy stream; take_prefetch orders the join's stream after them.
+    void start_prefetch(const std::vector<HostChunk> &hs, size_t &at) {
+        std::vector<HostChunk> group;
+        int64_t rows = 0;
+        while (at < hs.size() && (group.empty() || rows + hs[at].rows <= slice_rows())) {
+            rows += hs[at].rows;
+            group.push_back(hs[at++]);
+        }
+        prefetch_.batch = alloc_like(probe_types_, rows);  // allocated in the join's stream order
+        cudaEvent_t ready;
+        KRV_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        KRV_CUDA(cudaEventRecord(ready, rt_->stream));
+        KRV_CUDA(cudaStreamWaitEvent(cs_, ready, 0));
+        KRV_CUDA(cudaEventDestroy(ready));
+        copy_in(group, prefetch_.batch, cs_);
+        if (!prefetch_.ready) KRV_CUDA(cudaEventCreateWithFlags(&prefetch_.ready, cudaEventDisableTiming));
+        KRV_CUDA(cudaEventRecord(prefetch_.ready, cs_));
+        prefetch_.pending = true;
+    }
+    DevBatch take_prefetch() {
+        KRV_CUDA(cudaStreamWaitEvent(rt_->stream, prefetch_.ready, 0));
+        prefetch_.pending = false;
+        DevBatch b = std::move(prefetch_.batch);
+        prefetch_.batch = DevBatch{};
+        return b;
+    }
+    DevBatch alloc_like(const std::vector<DevCol> &types, int64_t rows) {
+        DevBatch b;
+        b.rows = rows;
+        for (const DevCol &t : types) {
+            DevCol col;
+            col.type = t.type;
+            col.name = t.name;
+            col.nullable = t.nullable;
+            col.length = rows;
+            col.hold_data = std::make_shared<DBuf>(rt_, (size_t)std::max<int64_t>(rows, 1) * t.type.width());
+            col.data = col.hold_data->get();
+            b.cols.push_back(col);
+        }
+        return b;
+    }
+    void copy_in(const std::vector<HostChunk> &hs, DevBatch &b, cudaStream_t st) {
+        for (size_t c = 0; c < b.cols.size(); c++) {
+            const int w = b.cols[c].type.width();
+            int64_t at = 0;
+            for (const HostChunk &h : hs) {
+                if (h.rows)
+                    KRV_CUDA(cudaMemcpyAsync(b.cols[c].hold_data->as<uint8_t>() + at * w, h.cols[c], (size_t)h.rows * w,
+                                             cudaMemcpyHostToDevice, st));
+                at += h.rows;
+            }
+        }
     }
 
     // Probe chunks from `at` on, as many as fit one slice, loaded as one
@@ -641,30 +746,14 @@ class GraceJoin {
         std::vector<HostChunk> one{h};
         return load_all(one, types);
     }
-    // The rows of chunks `hs`, back on the device as owned columns.
+    // The rows of chunks `hs`, back on the device as owned columns (after
+    // the spills still on their way to host memory, which they may be).
     DevBatch load_all(const std::vector<HostChunk> &hs, const std::vector<DevCol> &types) {
         int64_t rows = 0;
         for (const HostChunk &h : hs) rows += h.rows;
-        DevBatch b;
-        b.rows = rows;
-        for (size_t c = 0; c < types.size(); c++) {
-            const int w = types[c].type.width();
-            DevCol col;
-            col.type = types[c].type;
-            col.name = types[c].name;
-            col.nullable = types[c].nullable;
-            col.length = rows;
-            col.hold_data = std::make_shared<DBuf>(rt_, (size_t)std::max<int64_t>(rows, 1) * w);
-            col.data = col.hold_data->get();
-            int64_t at = 0;
-            for (const HostChunk &h : hs) {
-                if (h.rows)
-                    KRV_CUDA(cudaMemcpyAsync(col.hold_data->as<uint8_t>() + at * w, h.cols[c], (size_t)h.rows * w,
-                                             cudaMemcpyHostToDevice, rt_->stream));
-                at += h.rows;
-            }
-            b.cols.push_back(col);
-        }
+        if (!inflight_.empty()) KRV_CUDA(cudaStreamWaitEvent(rt_->stream, inflight_.back().done, 0));
+        DevBatch b = alloc_like(types, rows);
+        copy_in(hs, b, rt_->stream);
         return b;
     }
 
@@ -706,6 +795,19 @@ class GraceJoin {
     size_t deferred_chunk_ = 0;
     std::unique_ptr<HashJoin> cur_join_;
     std::vector<std::pair<uint8_t *, size_t>> host_blocks_;
+    cudaStream_t cs_ = nullptr;  // copies to and from the spill space
+    struct InFlight {
+        cudaEvent_t done = nullptr;
+        std::vector<std::shared_ptr<DBuf>> hold;
+        size_t bytes = 0;
+    };
+    std::deque<InFlight> inflight_;
+    size_t inflight_bytes_ = 0;
+    struct Prefetch {
+        DevBatch batch;
+        cudaEvent_t ready = nullptr;
+        bool pending = false;
+    } prefetch_;
     uint8_t *cur_block_ = nullptr;
     size_t cur_block_used_ = 0;
     krv_join_counters counters_{};

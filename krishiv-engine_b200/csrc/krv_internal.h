@@ -79,6 +79,7 @@ struct Runtime {
     int max_smem_optin = 227 * 1024;
     void *status_dev = nullptr;   // device status words (errors from kernels)
     void *status_host = nullptr;  // pinned mirror
+    void *status_host_dev = nullptr;  // its device address
     // Work queued on the stream still reads the caller's host buffers
     // (copies from page-locked memory, or columns read in place).
     bool host_borrowed = false;
@@ -201,10 +202,13 @@ DevCol make_col(Runtime *rt, DType t, int64_t n, bool nullable, const std::strin
 DevCol slice_col(const DevCol &c, int64_t from, int64_t n);
 
 // Copy a small device value to the host (synchronizes the stream).
+// Reads n (<= 4032) bytes of device memory after the work queued on the
+// runtime's stream: a one-block kernel stores them into mapped page-locked
+// memory, so the read does not queue behind bulk copies on the copy engines.
+void read_device(Runtime *rt, const void *dev, size_t n, void *host);
 template <class T> T read_scalar(Runtime *rt, const void *dev) {
     T v;
-    KRV_CUDA(cudaMemcpyAsync(&v, dev, sizeof(T), cudaMemcpyDeviceToHost, rt->stream));
-    KRV_CUDA(cudaStreamSynchronize(rt->stream));
+    read_device(rt, dev, sizeof(T), &v);
     return v;
 }
 

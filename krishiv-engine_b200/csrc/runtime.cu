@@ -184,11 +184,27 @@ uint32_t *status_word(Runtime *rt) { return static_cast<uint32_t *>(rt->status_d
 void clear_status(Runtime *rt) {
     KRV_CUDA(cudaMemsetAsync(rt->status_dev, 0, sizeof(uint32_t) * 4, rt->stream));
 }
-uint32_t take_status(Runtime *rt) {
-    KRV_CUDA(cudaMemcpyAsync(rt->status_host, rt->status_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                             rt->stream));
+namespace {
+__global__ void readback_kernel(const uint8_t *src, size_t n, volatile uint8_t *dst) {
+    for (size_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+}  // namespace
+
+void read_device(Runtime *rt, const void *dev, size_t n, void *host) {
+    if (n == 0) return;
+    if (n > 4032) fail(KRV_INTERNAL, "read_device: more than 4032 bytes");
+    volatile uint8_t *area = static_cast<volatile uint8_t *>(rt->status_host) + 64;
+    readback_kernel<<<1, 128, 0, rt->stream>>>(static_cast<const uint8_t *>(dev), n,
+                                               static_cast<volatile uint8_t *>(rt->status_host_dev) + 64);
+    check_launch("readback_kernel");
     KRV_CUDA(cudaStreamSynchronize(rt->stream));
-    return *static_cast<uint32_t *>(rt->status_host);
+    for (size_t i = 0; i < n; i++) static_cast<uint8_t *>(host)[i] = area[i];
+}
+
+uint32_t take_status(Runtime *rt) {
+    uint32_t v = 0;
+    read_device(rt, rt->status_dev, sizeof(uint32_t), &v);
+    return v;
 }
 
 DevCol make_col(Runtime *rt, DType t, int64_t n, bool nullable, const std::string &name) {
