@@ -132,6 +132,75 @@ __device__ __forceinline__ void update_record(const AggPlanDev &P, uint8_t *r, i
     }
 }
 
+// update_record for a record only one thread touches at a time: plain
+// arithmetic, the float64 sum compensated (TwoSum into hi, the error into lo).
+__device__ __forceinline__ void update_record_plain(const AggPlanDev &P, uint8_t *r, int64_t i) {
+    *reinterpret_cast<unsigned long long *>(r + P.off_rows) += 1ull;
+    for (int c = 0; c < P.ncols; c++) {
+        const AggColDev &C = P.c[c];
+        if (!bit_get(C.valid, C.voff, i)) continue;
+        *reinterpret_cast<unsigned long long *>(r + C.off_count) += 1ull;
+        if (C.type == (int)Type::I32 || C.type == (int)Type::Date32) {
+            const int v = static_cast<const int *>(C.data)[i];
+            if (C.flags & F_SUM) *reinterpret_cast<long long *>(r + C.off_sum) += (long long)v;
+            if (C.flags & F_MIN) {
+                int *m = reinterpret_cast<int *>(r + C.off_min);
+                *m = v < *m ? v : *m;
+            }
+            if (C.flags & F_MAX) {
+                int *m = reinterpret_cast<int *>(r + C.off_max);
+                *m = v > *m ? v : *m;
+            }
+        } else if (C.type == (int)Type::F64) {
+            const double v = static_cast<const double *>(C.data)[i];
+            if (C.flags & F_SUM) {
+                double *hi = reinterpret_cast<double *>(r + C.off_sum), *lo = hi + 1;
+                double sum, err;
+                two_sum(*hi, v, sum, err);
+                *hi = sum;
+                *lo = __dadd_rn(*lo, err);
+            }
+            if (C.flags & (F_MIN | F_MAX)) {
+                const unsigned long long key = f64_order_key(v);
+                if (C.flags & F_MIN) {
+                    unsigned long long *m = reinterpret_cast<unsigned long long *>(r + C.off_min);
+                    *m = key < *m ? key : *m;
+                }
+                if (C.flags & F_MAX) {
+                    unsigned long long *m = reinterpret_cast<unsigned long long *>(r + C.off_max);
+                    *m = key > *m ? key : *m;
+                }
+            }
+        } else if (C.type == (int)Type::Dec128) {
+            const long long *p = static_cast<const long long *>(C.data) + 2 * i;
+            if (C.flags & F_SUM) {
+                unsigned long long *lo = reinterpret_cast<unsigned long long *>(r + C.off_sum);
+                long long *hi = reinterpret_cast<long long *>(r + C.off_sum + 8);
+                const unsigned long long old = *lo;
+                *lo = old + (unsigned long long)p[0];
+                *hi += p[1] + (long long)(*lo < old);
+            }
+        } else {  // I64, Dec64
+            const long long v = static_cast<const long long *>(C.data)[i];
+            if (C.flags & F_SUM) {
+                unsigned long long *lo = reinterpret_cast<unsigned long long *>(r + C.off_sum);
+                long long *hi = reinterpret_cast<long long *>(r + C.off_sum + 8);
+                const unsigned long long old = *lo;
+                *lo = old + (unsigned long long)v;
+                *hi += (v < 0 ? -1ll : 0ll) + (long long)(*lo < old);
+            }
+            if (C.flags & F_MIN) {
+                long long *m = reinterpret_cast<long long *>(r + C.off_min);
+                *m = v < *m ? v : *m;
+            }
+            if (C.flags & F_MAX) {
+                long long *m = reinterpret_cast<long long *>(r + C.off_max);
+                *m = v > *m ? v : *m;
+            }
+        }
+    }
+}
+
 // Accumulator::merge (accumulator.rs:1159): folds the partial record `src`
 // into `dst`.
 __device__ __forceinline__ void merge_record(const AggPlanDev &P, uint8_t *dst, const uint8_t *src) {
@@ -250,29 +319,68 @@ __global__ void __launch_bounds__(256) agg_global_kernel(AggPlanDev P, TableDev 
 
 // Shared-memory pre-aggregation: a CTA-private table of `E` (power of two)
 // entries filled up to `fill` keys; rows of other keys go to the global table.
-__global__ void __launch_bounds__(1024) agg_shared_kernel(AggPlanDev P, TableDev T, KeyIn key, int64_t n,
-                                                          const uint32_t *rows_idx, uint32_t *ovf_rows,
-                                                          unsigned long long *ovf_count, int E, int fill) {
+// The `H` hottest keys (sampled on the host) also get one record per warp:
+// the lanes of a warp that hold rows of hot keys take turns updating their
+// warp's records with plain arithmetic (no atomics, no compare-and-swap float
+// adds), so a key that takes a large share of the rows is no longer updated
+// by every thread of the CTA through one record. The row loop runs the same
+// number of iterations on every lane, so the turns are taken by whole warps.
+constexpr int kHotKeys = 16;
+constexpr int kAggThreads = 1024;
+__global__ void __launch_bounds__(kAggThreads) agg_shared_kernel(AggPlanDev P, TableDev T, KeyIn key, int64_t n,
+                                                                 const uint32_t *rows_idx, uint32_t *ovf_rows,
+                                                                 unsigned long long *ovf_count, int E, int fill,
+                                                                 const long long *hot, int H) {
     extern __shared__ __align__(16) uint8_t smem[];
-    uint8_t *srec = smem;                                              // E * rec
-    long long *skeys = reinterpret_cast<long long *>(smem + (size_t)E * P.rec);  // E
-    uint32_t *sgid = reinterpret_cast<uint32_t *>(skeys + E);         // E
+    constexpr int kWarps = kAggThreads / 32;
+    uint8_t *wrec = smem;                                                          // kWarps * H * rec
+    uint8_t *srec = smem + (size_t)kWarps * H * P.rec;                             // E * rec
+    long long *skeys = reinterpret_cast<long long *>(srec + (size_t)E * P.rec);    // E
+    uint32_t *sgid = reinterpret_cast<uint32_t *>(skeys + E);                      // E
     int *sfill = reinterpret_cast<int *>(sgid + E);
+    __shared__ long long s_hot[kHotKeys];
+    __shared__ uint32_t s_hot_gid[kHotKeys];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int e = threadIdx.x; e < E; e += blockDim.x) {
         skeys[e] = kEmptyKey;
         init_record(P, srec + (size_t)e * P.rec);
+    }
+    for (int e = threadIdx.x; e < kWarps * H; e += blockDim.x) init_record(P, wrec + (size_t)e * P.rec);
+    if (threadIdx.x < H) {
+        // A hot key the global table has no room for is not hot in this CTA.
+        const long long k = hot[threadIdx.x];
+        const uint32_t g = find_or_insert(T, P, k);
+        s_hot[threadIdx.x] = k;
+        s_hot_gid[threadIdx.x] = g;
     }
     if (threadIdx.x == 0) *sfill = 0;
     __syncthreads();
     const int emask = E - 1;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
-        const int64_t r = rows_idx ? (int64_t)rows_idx[i] : i;
-        if (!bit_get(key.valid, key.voff, r)) {
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int64_t i = base + threadIdx.x;
+        const bool live = i < n;
+        const int64_t r = !live ? 0 : rows_idx ? (int64_t)rows_idx[i] : i;
+        const bool valid_key = live && bit_get(key.valid, key.voff, r);
+        const long long k = valid_key ? key_at(key, r) : 0;
+        int h = -1;
+        if (valid_key && k != kEmptyKey) {
+#pragma unroll
+            for (int j = 0; j < kHotKeys; j++)
+                if (j < H && h < 0 && s_hot[j] == k && s_hot_gid[j] < kOverflowGid) h = j;
+        }
+        unsigned turn = __ballot_sync(0xFFFFFFFFu, h >= 0);
+        while (turn) {
+            const int l = __ffs(turn) - 1;
+            turn &= turn - 1;
+            if (lane == l) update_record_plain(P, wrec + ((size_t)warp * H + h) * P.rec, r);
+            __syncwarp();
+        }
+        if (!live || h >= 0) continue;
+        if (!valid_key) {
             update_record(P, T.states + (size_t)kNullGid * P.rec, r);
             continue;
         }
-        const long long k = key_at(key, r);
         if (k == kEmptyKey) {
             update_record(P, T.states + (size_t)kMarkerGid * P.rec, r);
             continue;
@@ -321,6 +429,11 @@ __global__ void __launch_bounds__(1024) agg_shared_kernel(AggPlanDev P, TableDev
     __syncthreads();
     for (int e = threadIdx.x; e < E; e += blockDim.x)
         if (skeys[e] != kEmptyKey) merge_record(P, T.states + (size_t)sgid[e] * P.rec, srec + (size_t)e * P.rec);
+    for (int e = threadIdx.x; e < kWarps * H; e += blockDim.x) {
+        const int h = e % H;
+        if (s_hot_gid[h] < kOverflowGid)
+            merge_record(P, T.states + (size_t)s_hot_gid[h] * P.rec, wrec + (size_t)e * P.rec);
+    }
 }
 
 __global__ void init_special_kernel(AggPlanDev P, uint8_t *states) {
@@ -595,6 +708,12 @@ class HashAggregate {
     int64_t pending_rows_ = 0;     // rows pushed since known_groups_ was read
     int mode_ = KRV_AGG_MODE_SHARED;
     int smem_entries_ = 0;
+    // The hottest keys of the first batch (a strided sample), aggregated in
+    // warp-private records by the shared-memory kernel.
+    void sample_hot(const KeyIn &key, int64_t n);
+    bool sampled_ = false;
+    DBuf hot_;
+    int hot_count_ = 0;
 };
 
 HashAggregate::HashAggregate(Runtime *rt, const krv_agg_spec &spec) : rt_(rt), spec_(spec) {
@@ -759,15 +878,72 @@ void HashAggregate::launch(const DevBatch &b, const KeyIn &key, int64_t n, const
                ngroups_.as<unsigned long long>(), limit_, status_word(rt_)};
     if (mode_ == KRV_AGG_MODE_SHARED) {
         const int E = smem_entries_;
-        const size_t smem = (size_t)E * (P.rec + 12) + 16;
+        // as many hot keys as the shared memory left beside the table holds
+        const int64_t room = (int64_t)rt_->max_smem_optin - 1024 - (int64_t)E * (P.rec + 12) - 16;
+        const int H = (int)std::max<int64_t>(0, std::min<int64_t>(hot_count_, room / ((kAggThreads / 32) * P.rec)));
+        const size_t smem = (size_t)E * (P.rec + 12) + 16 + (size_t)(kAggThreads / 32) * H * P.rec;
         KRV_CUDA(cudaFuncSetAttribute(agg_shared_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        const int grid = (int)std::min<int64_t>(rt_->sm_count, ceil_div(std::max<int64_t>(n, 1), 1024));
-        agg_shared_kernel<<<grid, 1024, smem, rt_->stream>>>(P, T, key, n, rows_idx, ovf, ovf_count, E, E * 5 / 8);
+        const int grid = (int)std::min<int64_t>(rt_->sm_count, ceil_div(std::max<int64_t>(n, 1), kAggThreads));
+        agg_shared_kernel<<<grid, kAggThreads, smem, rt_->stream>>>(P, T, key, n, rows_idx, ovf, ovf_count, E, E * 5 / 8,
+                                                                    hot_.as<long long>(), H);
     } else {
         agg_global_kernel<<<grid_for(rt_, n, 256, 8), 256, 0, rt_->stream>>>(P, T, key, n, rows_idx, ovf, ovf_count);
     }
     rt_->launches++;
     check_launch("aggregate kernel");
+}
+
+namespace {
+__global__ void sample_keys_kernel(KeyIn key, int64_t n, int64_t step, int m, long long *out, uint8_t *ok) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+        const int64_t r = (int64_t)j * step;
+        const bool v = r < n && bit_get(key.valid, key.voff, r);
+        out[j] = v ? key_at(key, r) : 0;
+        ok[j] = v;
+    }
+}
+}  // namespace
+
+void HashAggregate::sample_hot(const KeyIn &key, int64_t n) {
+    sampled_ = true;
+    constexpr int kSample = 1 << 16;
+    const int m = (int)std::min<int64_t>(n, kSample);
+    if (m < 1024) return;  // too few rows for hot keys to matter
+    const int64_t step = n / m;
+    DBuf keys(rt_, (size_t)m * 8), ok(rt_, (size_t)m);
+    sample_keys_kernel<<<grid_for(rt_, m, 256, 4), 256, 0, rt_->stream>>>(key, n, step, m, keys.as<long long>(),
+                                                                          ok.as<uint8_t>());
+    rt_->launches++;
+    check_launch("sample_keys_kernel");
+    std::vector<long long> hk(m);
+    std::vector<uint8_t> hv(m);
+    KRV_CUDA(cudaMemcpyAsync(hk.data(), keys.get(), (size_t)m * 8, cudaMemcpyDeviceToHost, rt_->stream));
+    KRV_CUDA(cudaMemcpyAsync(hv.data(), ok.get(), (size_t)m, cudaMemcpyDeviceToHost, rt_->stream));
+    KRV_CUDA(cudaStreamSynchronize(rt_->stream));
+    std::vector<long long> v;
+    v.reserve(m);
+    for (int j = 0; j < m; j++)
+        if (hv[j] && hk[j] != kEmptyKey) v.push_back(hk[j]);
+    std::sort(v.begin(), v.end());
+    std::vector<std::pair<int, long long>> runs;  // (count, key)
+    for (size_t a = 0; a < v.size();) {
+        size_t b = a;
+        while (b < v.size() && v[b] == v[a]) b++;
+        runs.push_back({(int)(b - a), v[a]});
+        a = b;
+    }
+    std::sort(runs.begin(), runs.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    // hot: at least 0.2% of the sample each
+    std::vector<long long> hot;
+    for (const auto &rk : runs) {
+        if ((int)hot.size() == kHotKeys || rk.first * 500 < m) break;
+        hot.push_back(rk.second);
+    }
+    hot_count_ = (int)hot.size();
+    if (!hot_count_) return;
+    hot_ = DBuf(rt_, hot.size() * 8);
+    KRV_CUDA(cudaMemcpyAsync(hot_.get(), hot.data(), hot.size() * 8, cudaMemcpyHostToDevice, rt_->stream));
+    KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // `hot` is a stack vector
 }
 
 void HashAggregate::push(const DevBatch &b) {
@@ -782,6 +958,7 @@ void HashAggregate::push(const DevBatch &b) {
     if (n >= (int64_t)0xFFFFFFF0ll) fail(KRV_UNSUPPORTED, "aggregate batches of 2^32 rows or more");
     const DevCol &kc = b.cols[spec_.group_by[0]];
     KeyIn key{kc.data, kc.valid, kc.valid_off, kc.type.width(), 0};
+    if (mode_ == KRV_AGG_MODE_SHARED && !sampled_) sample_hot(key, n);
     clear_status(rt_);
     DBuf ovf_count(rt_, 8);
     KRV_CUDA(cudaMemsetAsync(ovf_count.get(), 0, 8, rt_->stream));
