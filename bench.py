@@ -572,6 +572,7 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
     torch.cuda.synchronize()
     barrier(pg)
     times = []
+    launches0 = capped.launches
     with Clocks(device) as clk:
         j = None
         for _ in range(args.steps):
@@ -587,6 +588,7 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
     counters = j.counters()
     spilled = j.spilled_partitions()
     last_phases = dict(phases)
+    launches1 = capped.launches
     del j
     # The unpartitioned join, uncapped, on the same inputs: the same rows.
     _, want_total, want_rows = run_join(False, rt)
@@ -605,7 +607,7 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
            "wall_ms_per_step": statistics.median(w for _, w in times),
            "phases": dict(last_phases),
            "checksum_agrees": (total, rows) == (want_total, want_rows),
-           "gpu_launches": None,
+           "gpu_launches": (launches1 - launches0) // max(1, args.steps),
            "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "peak_source": kind,
                         "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None,
                         "note": "24 B per build row, 16 B per probe row, 40 B per output row; spilled partitions "

@@ -53,6 +53,9 @@ template <class F>
 krv_status guard(F &&f) {
     try {
         krv::set_last_error(KRV_OK, "", 0);
+        // An error a runtime call left earlier on this thread (one this
+        // library already reported, or the caller's own) is not this call's.
+        cudaGetLastError();
         return f();
     } catch (const Error &e) {
         krv::set_last_error(e.code, e.msg, e.need_bytes);

@@ -294,6 +294,114 @@ __global__ void __launch_bounds__(256) probe_pairs_kernel(KeysDev pk, KeysDev bk
     }
 }
 
+// Pairs of an inner or left outer join on one int64 `=` key over a build
+// side with unique keys, with no build marks: every probe row has at most one
+// output row, so the kernel has no chain walks and no per-row loops, and its
+// warps stay converged. Every lane resolves kFastRows probe rows at once
+// (their slot loads in flight together); the CTA scans its warps' counts in
+// shared memory and reserves its run of the output with one atomic per
+// kFastRows x 256 probe rows. Validity bits of nullable output columns are
+// set with one atomicOr per valid value.
+constexpr int kFastRows = 4;
+constexpr int kFastThreads = 256;
+__global__ void __launch_bounds__(kFastThreads) probe_fast_kernel(KeysDev pk, KeysDev bk, int64_t n,
+                                                                  const unsigned long long *slots, uint64_t mask,
+                                                                  uint64_t seed, OutDev out, unsigned long long cap,
+                                                                  unsigned long long *count, int pad) {
+    constexpr int kWarps = kFastThreads / 32;
+    __shared__ unsigned s_warp[kWarps];
+    __shared__ unsigned long long s_base;
+    const long long *pkeys = static_cast<const long long *>(pk.c[0].data);
+    const long long *bkeys = static_cast<const long long *>(bk.c[0].data);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t tile = (int64_t)kFastThreads * kFastRows;
+    for (int64_t base = (int64_t)blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
+        int64_t row[kFastRows];
+        uint32_t head[kFastRows];
+        long long key[kFastRows];
+        uint64_t pos[kFastRows];
+        unsigned long long tag[kFastRows], slot[kFastRows];
+        bool live[kFastRows];
+#pragma unroll
+        for (int u = 0; u < kFastRows; u++) {
+            row[u] = base + (int64_t)u * kFastThreads + threadIdx.x;
+            live[u] = row[u] < n && key_valid(pk.c[0], row[u]);
+            key[u] = live[u] ? pkeys[row[u]] : 0;
+            const uint64_t g = finalize(hash_word((uint64_t)key[u]), seed);
+            tag[u] = g >> 32;
+            pos[u] = g & mask;
+        }
+#pragma unroll
+        for (int u = 0; u < kFastRows; u++) slot[u] = live[u] ? __ldg(slots + pos[u]) : 0ull;
+#pragma unroll
+        for (int u = 0; u < kFastRows; u++) {
+            head[u] = kNone;
+            if (!live[u]) continue;
+            unsigned long long sl = slot[u];
+            uint64_t p = pos[u];
+            for (uint64_t probes = 0; probes <= mask && sl != 0; probes++) {
+                if ((sl >> 32) == tag[u]) {
+                    const uint32_t o = (uint32_t)(sl & 0xFFFFFFFFull) - 1u;
+                    if (__ldg(bkeys + o) == key[u]) {
+                        head[u] = o;
+                        break;
+                    }
+                }
+                p = (p + 1) & mask;
+                sl = __ldg(slots + p);
+            }
+        }
+        bool emit[kFastRows];
+        unsigned mine = 0;
+#pragma unroll
+        for (int u = 0; u < kFastRows; u++) {
+            emit[u] = row[u] < n && (head[u] != kNone || pad);
+            mine += emit[u];
+        }
+        unsigned incl = mine;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned y = __shfl_up_sync(kFull, incl, d);
+            if (lane >= d) incl += y;
+        }
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned acc = 0;
+            for (int w = 0; w < kWarps; w++) {
+                const unsigned c = s_warp[w];
+                s_warp[w] = acc;
+                acc += c;
+            }
+            s_base = acc ? atomicAdd(count, (unsigned long long)acc) : 0ull;
+        }
+        __syncthreads();
+        unsigned long long at = s_base + s_warp[warp] + (incl - mine);
+        __syncthreads();  // s_warp and s_base are rewritten by the next tile
+#pragma unroll
+        for (int u = 0; u < kFastRows; u++) {
+            if (!emit[u]) continue;
+            const unsigned long long a = at++;
+            if (a >= cap) continue;
+            const uint32_t b = head[u];
+            for (int k = 0; k < out.n; k++) {
+                const OutColDev &c = out.c[k];
+                bool v = false;
+                if (c.side == 0) {
+                    copy_value(c.dst, c.src, (int64_t)a, row[u], c.width);
+                    v = bit_get(c.src_valid, c.src_voff, row[u]);
+                } else if (b != kNone) {
+                    copy_value(c.dst, c.src, (int64_t)a, b, c.width);
+                    v = bit_get(c.src_valid, c.src_voff, b);
+                } else {
+                    zero_value(c.dst, (int64_t)a, c.width);
+                }
+                if (c.dst_valid && v) atomicOr(c.dst_valid + (a >> 5), 1u << (a & 31));
+            }
+        }
+    }
+}
+
 // Probe rows once: semi, anti, null-aware anti (join/mod.rs:27-34).
 // kind 0 semi, 1 anti, 2 null-aware anti.
 template <bool FAST>
@@ -709,7 +817,14 @@ DevBatch HashJoin::probe(const DevBatch &in) {
                     auto *mc = counters_dev_.as<unsigned long long>() + 6;
                     uint8_t *marks = marks_.get() ? marks_.as<uint8_t>() : nullptr;
                     const int pad = jt == KRV_JOIN_LEFT_OUTER || jt == KRV_JOIN_FULL_OUTER;
-                    if (fast)
+                    // unique build keys: at most one output row per probe row
+                    const bool unique = build_rows_ > 0 && counters_.build_keys == indexed_rows_;
+                    if (fast && unique && !marks && pk.null_safe == 0 &&
+                        (jt == KRV_JOIN_INNER || jt == KRV_JOIN_LEFT_OUTER)) {
+                        const int fgrid = grid_for(rt_, ceil_div(n, kFastRows), kFastThreads, 8);
+                        probe_fast_kernel<<<fgrid, kFastThreads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, spec_.seed,
+                                                                                   od, cap, count, pad);
+                    } else if (fast)
                         probe_pairs_kernel<true><<<grid, threads, 0, rt_->stream>>>(
                             pk, bk, n, slots, mask_, next_.as<uint32_t>(), spec_.seed, od, cap, count, marks, pad,
                             spec_.single_match, status_word(rt_), mc);
