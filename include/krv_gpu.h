@@ -339,7 +339,11 @@ krv_status krv_star_build_device(krv_star *s, const struct ArrowDeviceArray *dim
                                  const struct ArrowSchema *schema_a,
                                  const struct ArrowDeviceArray *dim_b,
                                  const struct ArrowSchema *schema_b);
-/* Adds one fact batch to the running aggregate. */
+/* Adds one fact batch to the running aggregate. In the fused mode a
+ * page-locked host batch is not copied whole: fk_b (read whole) crosses the
+ * host link in bulk copies overlapping the kernels, fk_a, price and discount
+ * are read in place row by row; the call returns when none of the batch's
+ * buffers is read any more. */
 krv_status krv_star_probe(krv_star *s, const struct ArrowArray *fact,
                           const struct ArrowSchema *schema);
 krv_status krv_star_probe_device(krv_star *s, const struct ArrowDeviceArray *fact,

@@ -593,7 +593,8 @@ krv_status krv_star_probe(krv_star *s, const ArrowArray *fact, const ArrowSchema
         krv::HostBorrow hb(rt);
         // The fused probe streams fk_b once and reads fk_a, price and discount
         // only for the rows that pass the filters: page-locked columns are
-        // read in place, so only those bytes cross the host link.
+        // imported in place (fk_b then crosses in bulk copies, the others
+        // only by the sectors the kernels read).
         const krv::HostRead mode = krv::star_fused(s->s) ? krv::HostRead::InPlace : krv::HostRead::Copy;
         krv::star_probe(s->s, krv::import_host(rt, fact, schema, mode));
         return KRV_OK;

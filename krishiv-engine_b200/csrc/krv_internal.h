@@ -167,6 +167,7 @@ struct DevCol {
     DType type;
     int64_t length = 0;
     const void *data = nullptr;
+    const void *host = nullptr;  // a column read in place: its host address
     const uint8_t *valid = nullptr;
     int64_t valid_off = 0;
     bool nullable = true;

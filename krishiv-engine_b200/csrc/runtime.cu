@@ -324,6 +324,7 @@ static DevBatch import_impl(Runtime *rt, const ArrowArray *arr, const ArrowSchem
             const uint8_t *in_place = mode == HostRead::InPlace ? mapped_host(src, bytes) : nullptr;
             if (in_place) {
                 col.data = in_place;
+                col.host = src;
                 rt->host_borrowed = true;
             } else {
                 col.hold_data = std::make_shared<DBuf>(rt, bytes > 0 ? bytes : 8);

@@ -496,6 +496,54 @@ class StarPipeline {
         const size_t limit = (size_t)rt_->max_smem_optin - 1024;
         const bool staged = A.bits_b && star_scan_smem((int)bits_words_[1]) <= limit;
         A.bits_b_smem_words = staged ? (int)bits_words_[1] : 0;
+        const void *host_fk_b = f.cols[spec_.fact_fk_b].host;
+        if (host_fk_b && A.n >= 2 * kStreamRows) probe_streamed(A, static_cast<const long long *>(host_fk_b));
+        else scan_join(A);
+    }
+
+    // A fact batch in page-locked host memory: fk_b, read whole, crosses the
+    // host link as bulk copies into HBM (the link's copy rate, well above what
+    // kernel loads of host memory reach), kStreamRows rows at a time with
+    // kStreamStages chunks in flight on a copy stream; each chunk's scan and
+    // join run as the next chunks arrive and read fk_a, price and discount in
+    // place, so only the sectors of surviving rows cross the link.
+    void probe_streamed(const StarArgs &A0, const long long *host_fk_b) {
+        if (!cs_) {
+            KRV_CUDA(cudaStreamCreateWithFlags(&cs_, cudaStreamNonBlocking));
+            KRV_CUDA(cudaEventCreateWithFlags(&start_, cudaEventDisableTiming));
+            for (int s = 0; s < kStreamStages; s++) {
+                KRV_CUDA(cudaEventCreateWithFlags(&ready_[s], cudaEventDisableTiming));
+                KRV_CUDA(cudaEventCreateWithFlags(&free_[s], cudaEventDisableTiming));
+                stage_[s] = DBuf(rt_, (size_t)kStreamRows * 8);
+            }
+        }
+        // The copies start after the work queued before them (the staging
+        // buffers' readers in an earlier probe).
+        KRV_CUDA(cudaEventRecord(start_, rt_->stream));
+        KRV_CUDA(cudaStreamWaitEvent(cs_, start_, 0));
+        const int64_t chunks = ceil_div(A0.n, kStreamRows);
+        for (int64_t c = 0; c < chunks; c++) {
+            const int s = (int)(c % kStreamStages);
+            const int64_t r0 = c * kStreamRows, n = std::min(kStreamRows, A0.n - r0);
+            if (c >= kStreamStages) KRV_CUDA(cudaStreamWaitEvent(cs_, free_[s], 0));
+            KRV_CUDA(cudaMemcpyAsync(stage_[s].get(), host_fk_b + r0, (size_t)n * 8, cudaMemcpyHostToDevice, cs_));
+            KRV_CUDA(cudaEventRecord(ready_[s], cs_));
+            KRV_CUDA(cudaStreamWaitEvent(rt_->stream, ready_[s], 0));
+            StarArgs A = A0;
+            A.fk_b = stage_[s].as<long long>();
+            A.fk_a += r0;
+            A.price += r0;
+            A.disc += r0;
+            A.n = n;
+            // The join reads the survivor list, not fk_b: the stage is free
+            // once the scan is done.
+            scan_join(A, &free_[s]);
+        }
+    }
+
+    // The scan (stage 1) and the join (stage 2) over one range of fact rows;
+    // `scanned`, if given, is recorded between them.
+    void scan_join(StarArgs &A, cudaEvent_t *scanned = nullptr) {
         // The survivor list: one region per scan CTA, as large as the rows it scans.
         const int64_t tiles = ceil_div(A.n, kScanTile);
         const int grid = (int)std::min<int64_t>(rt_->sm_count, tiles);
@@ -518,7 +566,7 @@ class StarPipeline {
         // 16-byte vector loads of fk_b need a 16-byte aligned column.
         const bool vec = (reinterpret_cast<uintptr_t>(A.fk_b) & 15) == 0;
         const size_t smem = star_scan_smem(A.bits_b_smem_words);
-        if (staged) {
+        if (A.bits_b_smem_words > 0) {
             if (vec && kb32) launch_scan<1, true, true>(A, grid, smem);
             else if (vec) launch_scan<1, true, false>(A, grid, smem);
             else if (kb32) launch_scan<1, false, true>(A, grid, smem);
@@ -529,6 +577,7 @@ class StarPipeline {
             else if (kb32) launch_scan<0, false, true>(A, grid, smem);
             else launch_scan<0, false, false>(A, grid, smem);
         }
+        if (scanned) KRV_CUDA(cudaEventRecord(*scanned, rt_->stream));
         // Join over the survivors: several CTAs per region, so hundreds of
         // thousands of independent probes hide the memory latency.
         const int G = std::max(1, std::min(ngroups_host_, 256));
@@ -776,10 +825,26 @@ class StarPipeline {
     HashAggregate *plain_agg_ = nullptr;
     bool built_ = false;
     krv_star_counters counters_{};
+    // Staging of fk_b from host memory (probe_streamed).
+    static constexpr int64_t kStreamRows = 8ll << 20;  // 64 MiB of fk_b per chunk
+    static constexpr int kStreamStages = 3;
+    cudaStream_t cs_ = nullptr;
+    cudaEvent_t start_ = nullptr, ready_[kStreamStages] = {}, free_[kStreamStages] = {};
+    DBuf stage_[kStreamStages];
 
   public:
     ~StarPipeline() {
         if (plain_agg_) agg_destroy(plain_agg_);
+        if (cs_) {
+            cudaStreamSynchronize(cs_);
+            cudaStreamSynchronize(rt_->stream);
+            for (int s = 0; s < kStreamStages; s++) {
+                cudaEventDestroy(ready_[s]);
+                cudaEventDestroy(free_[s]);
+            }
+            cudaEventDestroy(start_);
+            cudaStreamDestroy(cs_);
+        }
     }
 };
 

@@ -118,3 +118,44 @@ def test_star_host_batches(kb, rt, oracle, pinned):
     assert sorted(got) == sorted(want)
     for k, (ws, _) in want.items():
         assert rel_err(got[k], ws) <= FLOAT_TOL, (k, got[k], ws)
+
+
+def test_star_host_batch_streamed(kb, rt, oracle):
+    """A page-locked fact batch of 36M rows: fk_b crosses the host link in
+    bulk copies of 8M rows, three in flight, while the kernels read the
+    other columns in place. Probed as one row and the rest (an odd Arrow
+    offset, five chunks, the last one ragged), then again after a reset:
+    the oracle's answer both times."""
+    import pyarrow as pa
+    import torch
+    W = importlib.import_module("krishiv-engine_b200.workloads")
+    data = W.star(rt, scale=0.12)
+    torch.cuda.synchronize()
+    assert data.fact_rows > 4 * (8 << 20)
+    passed, joined, want, _ = oracle_star(oracle, data, 0)
+    keep = []
+
+    def host(cols):
+        arrays = []
+        for name, t, _ in cols:
+            h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            h.copy_(t)
+            keep.append(h)
+            arrays.append(pa.array(h.numpy()))
+        return pa.RecordBatch.from_arrays(arrays, names=[n for n, _, _ in cols])
+
+    fact, dim_a, dim_b = host(data.fact), host(data.dim_a), host(data.dim_b)
+    s = kb.StarPipeline(rt, kb.star_spec(7, 7, group_by=0, mode=kb.STAR_FUSED))
+    s.build(dim_a, dim_b)
+    for parts in (((0, 1), (1, data.fact_rows - 1)), ((0, data.fact_rows),)):
+        s.reset()
+        for lo, n in parts:
+            s.probe(fact.slice(lo, n))
+        out = s.result()
+        c = s.counters()
+        assert c["fact_rows"] == data.fact_rows
+        assert c["passed_filters"] == passed and c["joined_rows"] == joined
+        got = dict(zip(out.column(0).to_pylist(), out.column(1).to_pylist()))
+        assert sorted(got) == sorted(want)
+        for k, (ws, _) in want.items():
+            assert rel_err(got[k], ws) <= FLOAT_TOL, (k, got[k], ws)
