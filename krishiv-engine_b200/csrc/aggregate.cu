@@ -320,11 +320,12 @@ __global__ void __launch_bounds__(256) agg_global_kernel(AggPlanDev P, TableDev 
 // Shared-memory pre-aggregation: a CTA-private table of `E` (power of two)
 // entries filled up to `fill` keys; rows of other keys go to the global table.
 // The `H` hottest keys (sampled on the host) also get one record per warp:
-// the lanes of a warp that hold rows of hot keys take turns updating their
-// warp's records with plain arithmetic (no atomics, no compare-and-swap float
-// adds), so a key that takes a large share of the rows is no longer updated
-// by every thread of the CTA through one record. The row loop runs the same
-// number of iterations on every lane, so the turns are taken by whole warps.
+// the lanes of a warp that hold rows of one hot key take turns updating
+// their warp's record of it with plain arithmetic (no atomics, no
+// compare-and-swap float adds), lanes of different hot keys in the same turn,
+// so a key that takes a large share of the rows is no longer updated by every
+// thread of the CTA through one record. The row loop runs the same number of
+// iterations on every lane, so the turns are taken by whole warps.
 constexpr int kHotKeys = 16;
 constexpr int kAggThreads = 1024;
 __global__ void __launch_bounds__(kAggThreads) agg_shared_kernel(AggPlanDev P, TableDev T, KeyIn key, int64_t n,
@@ -369,12 +370,16 @@ __global__ void __launch_bounds__(kAggThreads) agg_shared_kernel(AggPlanDev P, T
             for (int j = 0; j < kHotKeys; j++)
                 if (j < H && h < 0 && s_hot[j] == k && s_hot_gid[j] < kOverflowGid) h = j;
         }
-        unsigned turn = __ballot_sync(0xFFFFFFFFu, h >= 0);
-        while (turn) {
-            const int l = __ffs(turn) - 1;
-            turn &= turn - 1;
-            if (lane == l) update_record_plain(P, wrec + ((size_t)warp * H + h) * P.rec, r);
-            __syncwarp();
+        if (__ballot_sync(0xFFFFFFFFu, h >= 0)) {
+            // Lanes of one hot key take turns; lanes of different hot keys
+            // update their records in the same turn.
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, h);
+            const unsigned rank = __popc(peers & ((1u << lane) - 1u));
+            const unsigned turns = __reduce_max_sync(0xFFFFFFFFu, h >= 0 ? (unsigned)__popc(peers) : 0u);
+            for (unsigned t = 0; t < turns; t++) {
+                if (h >= 0 && rank == t) update_record_plain(P, wrec + ((size_t)warp * H + h) * P.rec, r);
+                __syncwarp();
+            }
         }
         if (!live || h >= 0) continue;
         if (!valid_key) {

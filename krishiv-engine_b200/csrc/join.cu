@@ -302,12 +302,33 @@ __global__ void __launch_bounds__(256) probe_pairs_kernel(KeysDev pk, KeysDev bk
 // shared memory and reserves its run of the output with one atomic per
 // kFastRows x 256 probe rows. Validity bits of nullable output columns are
 // set with one atomicOr per valid value.
+//
+// DIRECT: the build keys are also dense (their span at most a few times the
+// row count), and a direct index (key - lo -> build row) replaces the table:
+// one load per probe row instead of a slot load and a key compare.
 constexpr int kFastRows = 4;
 constexpr int kFastThreads = 256;
+struct DirectDev {
+    const uint32_t *row;  // build row of key lo + i, kNone where no row has it
+    long long lo;
+    unsigned long long span;  // hi - lo
+};
+
+__global__ void direct_build_kernel(KeysDev bk, int64_t n, DirectDev d) {
+    const long long *keys = static_cast<const long long *>(bk.c[0].data);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (!key_valid(bk.c[0], i)) continue;
+        const unsigned long long off = (unsigned long long)keys[i] - (unsigned long long)d.lo;
+        if (off <= d.span) const_cast<uint32_t *>(d.row)[off] = (uint32_t)i;
+    }
+}
+
+template <bool DIRECT>
 __global__ void __launch_bounds__(kFastThreads) probe_fast_kernel(KeysDev pk, KeysDev bk, int64_t n,
                                                                   const unsigned long long *slots, uint64_t mask,
-                                                                  uint64_t seed, OutDev out, unsigned long long cap,
-                                                                  unsigned long long *count, int pad) {
+                                                                  uint64_t seed, DirectDev dir, OutDev out,
+                                                                  unsigned long long cap, unsigned long long *count,
+                                                                  int pad) {
     constexpr int kWarps = kFastThreads / 32;
     __shared__ unsigned s_warp[kWarps];
     __shared__ unsigned long long s_base;
@@ -327,14 +348,23 @@ __global__ void __launch_bounds__(kFastThreads) probe_fast_kernel(KeysDev pk, Ke
             row[u] = base + (int64_t)u * kFastThreads + threadIdx.x;
             live[u] = row[u] < n && key_valid(pk.c[0], row[u]);
             key[u] = live[u] ? pkeys[row[u]] : 0;
+            if (DIRECT) continue;
             const uint64_t g = finalize(hash_word((uint64_t)key[u]), seed);
             tag[u] = g >> 32;
             pos[u] = g & mask;
         }
+        if (DIRECT) {
 #pragma unroll
-        for (int u = 0; u < kFastRows; u++) slot[u] = live[u] ? __ldg(slots + pos[u]) : 0ull;
+            for (int u = 0; u < kFastRows; u++) {
+                const unsigned long long off = (unsigned long long)key[u] - (unsigned long long)dir.lo;
+                head[u] = live[u] && off <= dir.span ? __ldg(dir.row + off) : kNone;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kFastRows; u++) slot[u] = !DIRECT && live[u] ? __ldg(slots + pos[u]) : 0ull;
 #pragma unroll
         for (int u = 0; u < kFastRows; u++) {
+            if (DIRECT) break;
             head[u] = kNone;
             if (!live[u]) continue;
             unsigned long long sl = slot[u];
@@ -659,6 +689,25 @@ void HashJoin::build_finish() {
     indexed_rows_ = (int64_t)host_ctr[4];
     key_lo_ = (long long)host_ctr[2];
     key_hi_ = (long long)host_ctr[3];
+    // Unique, dense int64 keys (a span of at most 4 values per row): a direct
+    // index, 4 bytes per key value, for the probe of inner and left outer joins.
+    direct_.reset();
+    direct_span_ = 0;
+    if (indexed_rows_ > 0 && counters_.build_keys == indexed_rows_ && spec_.n_keys == 1 && !spec_.null_safe[0] &&
+        arena_.cols[spec_.build_keys[0]].type.id == Type::I64 &&
+        (spec_.join_type == KRV_JOIN_INNER || spec_.join_type == KRV_JOIN_LEFT_OUTER)) {
+        const __int128 span = (__int128)key_hi_ - (__int128)key_lo_;
+        if (span >= 0 && span < ((__int128)1 << 31) && span < (__int128)4 * indexed_rows_ + 4096) {
+            direct_span_ = (unsigned long long)span;
+            direct_ = DBuf(rt_, (size_t)(span + 1) * 4);
+            KRV_CUDA(cudaMemsetAsync(direct_.get(), 0xFF, direct_.bytes(), rt_->stream));
+            KeysDev k = keys_of(arena_, spec_.build_keys, spec_.n_keys, spec_.null_safe);
+            direct_build_kernel<<<grid_for(rt_, build_rows_, 256, 8), 256, 0, rt_->stream>>>(
+                k, build_rows_, DirectDev{direct_.as<uint32_t>(), key_lo_, direct_span_});
+            rt_->launches++;
+            check_launch("direct_build_kernel");
+        }
+    }
     // The runtime filter of a one-key join (BuildSink::publish, join/build.rs:482).
     if (spec_.runtime_filter && spec_.n_keys == 1) {
         const DevCol &key = arena_.cols[spec_.build_keys[0]];
@@ -822,8 +871,13 @@ DevBatch HashJoin::probe(const DevBatch &in) {
                     if (fast && unique && !marks && pk.null_safe == 0 &&
                         (jt == KRV_JOIN_INNER || jt == KRV_JOIN_LEFT_OUTER)) {
                         const int fgrid = grid_for(rt_, ceil_div(n, kFastRows), kFastThreads, 8);
-                        probe_fast_kernel<<<fgrid, kFastThreads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, spec_.seed,
-                                                                                   od, cap, count, pad);
+                        const DirectDev dd{direct_.as<uint32_t>(), key_lo_, direct_span_};
+                        if (dd.row)
+                            probe_fast_kernel<true><<<fgrid, kFastThreads, 0, rt_->stream>>>(
+                                pk, bk, n, slots, mask_, spec_.seed, dd, od, cap, count, pad);
+                        else
+                            probe_fast_kernel<false><<<fgrid, kFastThreads, 0, rt_->stream>>>(
+                                pk, bk, n, slots, mask_, spec_.seed, dd, od, cap, count, pad);
                     } else if (fast)
                         probe_pairs_kernel<true><<<grid, threads, 0, rt_->stream>>>(
                             pk, bk, n, slots, mask_, next_.as<uint32_t>(), spec_.seed, od, cap, count, marks, pad,

@@ -135,6 +135,8 @@ class HashJoin {
     DevBatch arena_;                    // view of the arena
     bool have_schema_ = false;
     DBuf slots_, next_, marks_, counters_dev_;
+    DBuf direct_;  // unique dense keys: key - key_lo_ -> build row
+    unsigned long long direct_span_ = 0;
     uint64_t mask_ = 0;
     int64_t build_rows_ = 0;
     bool built_ = false;

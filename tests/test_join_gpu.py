@@ -189,3 +189,20 @@ def test_budget_need_memory(kb):
         j.build_push(batch(k=pa.array(np.arange(1 << 20, dtype=np.int64))))
     assert e.value.status == kb.NEED_MEMORY
     assert kb.lib().krv_last_need_bytes() > 0
+
+
+@pytest.mark.parametrize("jt", ["inner", "left_outer"])
+def test_dense_unique_build_keys(kb, rt, oracle, jt):
+    """Unique build keys over a dense range starting below zero, with holes
+    and NULL keys, probed by keys inside, just outside and far outside the
+    range (the int64 extremes) and NULLs: the oracle's pairs."""
+    rng = np.random.default_rng(15)
+    lo, span = -500_000, 140_000
+    keys = lo + rng.permutation(span)[:100_000]
+    build = [(int(k), 0) for k in keys] + [(None, 0)] * 50
+    rng.shuffle(build)
+    pk = rng.integers(lo - 1000, lo + span + 1000, 300_000)
+    probe = [(int(k), 0) for k in pk] + [(None, 0)] * 20 + [(-2**63, 0), (2**63 - 1, 0), (lo, 0), (lo - 1, 0)]
+    want = oracle_pairs(oracle, jt, probe, build, 1, False)
+    got = gpu_pairs(kb, rt, jt, probe, build, 1, False, build_batches=2)
+    assert got == want
