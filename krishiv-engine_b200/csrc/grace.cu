@@ -139,6 +139,130 @@ __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(PartArgs A, 
     }
 }
 
+// ---- the resident partitions' probe: one launch per input slice ------------------
+// Every resident partition's rows of the slice are probed against that
+// partition's table in one launch (tiles of 256 rows, each tile within one
+// partition), and all their output rows go to one output batch: no launch,
+// output count read or output copy per partition. The table lookups, chain
+// walks and output rounds are those of the unpartitioned join's probe
+// (pairs: newest build row first, left outer pads unmatched rows).
+constexpr int kGProbeThreads = 256;
+constexpr int kGMaxOut = 16;
+constexpr uint32_t kGNone = 0xFFFFFFFFu;
+struct GPartDev {
+    const unsigned long long *slots;
+    uint64_t mask;
+    const uint32_t *next;
+    const long long *bkey;
+    const void *bcol[kMaxCols];  // the partition's build columns
+    int64_t prow0, rows;         // its rows of the partitioned slice
+    int64_t tile0;               // its first tile
+};
+struct GOutCol {
+    void *dst;
+    uint32_t *dst_valid;  // zeroed bitmap words, or null
+    int32_t width;
+    int32_t side;  // 0: probe column `col`, 1: build column `col`
+    int32_t col;
+};
+struct GOutDev {
+    GOutCol c[kGMaxOut];
+    int32_t n;
+    const void *pcol[kMaxCols];  // the partitioned slice's columns
+    const long long *pkey;
+};
+
+__device__ __forceinline__ void gcopy(void *dst, const void *src, unsigned long long di, int64_t si, int w) {
+    if (w == 8) static_cast<unsigned long long *>(dst)[di] = static_cast<const unsigned long long *>(src)[si];
+    else static_cast<uint32_t *>(dst)[di] = static_cast<const uint32_t *>(src)[si];
+}
+
+__global__ void __launch_bounds__(kGProbeThreads) grace_probe_kernel(const GPartDev *parts, int nparts, int64_t tiles,
+                                                                     uint64_t seed, GOutDev out, unsigned long long cap,
+                                                                     unsigned long long *count, int pad,
+                                                                     int single_match, uint32_t *status) {
+    __shared__ GPartDev sp;
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        __syncthreads();  // the previous tile's partition is read no more
+        if (threadIdx.x == 0) {
+            int p = 0;
+            while (p + 1 < nparts && parts[p + 1].tile0 <= t) p++;
+            sp = parts[p];
+        }
+        __syncthreads();
+        const int64_t local = (t - sp.tile0) * kGProbeThreads + threadIdx.x;
+        const bool live = local < sp.rows;
+        const int64_t prow = sp.prow0 + local;
+        uint32_t cur = kGNone;
+        if (live) {
+            const long long k = out.pkey[prow];
+            const uint64_t g = finalize(hash_word((uint64_t)k), seed);
+            const unsigned long long tag = g >> 32;
+            uint64_t pos = g & sp.mask;
+            for (uint64_t probes = 0; probes <= sp.mask; probes++) {
+                const unsigned long long sl = __ldg(sp.slots + pos);
+                if (sl == 0) break;
+                if ((sl >> 32) == tag) {
+                    const uint32_t o = (uint32_t)(sl & 0xFFFFFFFFull) - 1u;
+                    if (__ldg(sp.bkey + o) == k) {
+                        cur = o;
+                        break;
+                    }
+                }
+                pos = (pos + 1) & sp.mask;
+            }
+        }
+        bool padrow = live && cur == kGNone && pad;
+        unsigned chain = 0;
+        while (__any_sync(0xFFFFFFFFu, cur != kGNone || padrow)) {
+            const bool want = cur != kGNone || padrow;
+            const unsigned ballot = __ballot_sync(0xFFFFFFFFu, want);
+            unsigned long long first = 0;
+            if (lane == 0) first = atomicAdd(count, (unsigned long long)__popc(ballot));
+            first = __shfl_sync(0xFFFFFFFFu, first, 0);
+            const unsigned rank = __popc(ballot & below);
+            const unsigned long long at = first + rank;
+            for (int c = 0; c < out.n; c++) {
+                const GOutCol C = out.c[c];
+                bool v = false;
+                if (want && at < cap) {
+                    if (C.side == 0) {
+                        gcopy(C.dst, out.pcol[C.col], at, prow, C.width);
+                        v = true;
+                    } else if (cur != kGNone) {
+                        gcopy(C.dst, sp.bcol[C.col], at, cur, C.width);
+                        v = true;
+                    } else if (C.width == 8) {
+                        static_cast<unsigned long long *>(C.dst)[at] = 0ull;
+                    } else {
+                        static_cast<uint32_t *>(C.dst)[at] = 0u;
+                    }
+                }
+                if (C.dst_valid) {
+                    // this round's bits in output order, OR-ed in with at most two atomics
+                    const unsigned m = __reduce_or_sync(0xFFFFFFFFu, v ? (1u << rank) : 0u);
+                    if (lane == 0 && m) {
+                        const unsigned long long w = first >> 5;
+                        const unsigned sh = (unsigned)(first & 31);
+                        const unsigned long long capw = (cap + 31) >> 5;
+                        if (w < capw) atomicOr(C.dst_valid + w, m << sh);
+                        if (sh && w + 1 < capw && (m >> (32 - sh))) atomicOr(C.dst_valid + w + 1, m >> (32 - sh));
+                    }
+                }
+            }
+            if (cur != kGNone) {
+                chain++;
+                cur = sp.next[cur];
+            } else {
+                padrow = false;
+            }
+        }
+        if (single_match && chain > 1) atomicOr(status, ST_TOO_MANY);
+    }
+}
+
 int radix_for(int64_t build_rows, int64_t row_bytes, int64_t budget) {
     // 2^radix partitions of at most a sixteenth of the budget each (3..6 bits).
     if (budget <= 0 || build_rows <= 0) return 3;
@@ -152,6 +276,12 @@ int radix_for(int64_t build_rows, int64_t row_bytes, int64_t budget) {
 
 // ---- the operator ------------------------------------------------------------------
 class GraceJoin {
+    // One partition's rows of a partitioned slice (views of its buffers).
+    struct Segment {
+        DevBatch batch;
+        int64_t rows = 0;
+    };
+
   public:
     GraceJoin(Runtime *rt, const krv_join_spec &spec, const krv_grace_options &opt) : rt_(rt), spec_(spec), opt_(opt) {
         if (spec.join_type != KRV_JOIN_INNER && spec.join_type != KRV_JOIN_LEFT_OUTER)
@@ -289,20 +419,132 @@ class GraceJoin {
             keep(out, null_join_->probe(with_null_keys(nulls)));
         }
         const int64_t out_cap = budget_ / 8 / out_row_bytes();
+        const double ratio = out_ratio();
+        std::vector<int> now;  // resident partitions joined by this slice's launch
+        double expect = 0;
         for (int p = 0; p < nparts_; p++) {
             Segment &s = segs[p];
             if (s.rows == 0) continue;
             Part &P = parts_[p];
             if (P.spilled) {
                 P.probe_host.push_back(spill(s));
-            } else if (out_rows >= out_cap) {
+            } else if ((double)out_rows + expect >= (double)out_cap) {
                 P.deferred.push_back(spill(s));
             } else {
-                DevBatch o = P.join->probe(s.batch);
-                out_rows += o.rows;
-                keep(out, std::move(o));
+                now.push_back(p);
+                expect += (double)s.rows * ratio;
             }
         }
+        if (!now.empty()) {
+            DevBatch o = probe_resident(segs, now, ratio);
+            out_rows += o.rows;
+            keep(out, std::move(o));
+        }
+    }
+
+    // Output rows per probe row of the resident partitions: as observed so
+    // far, else the build's mean rows per key (at least 1 for left outer).
+    double out_ratio() const {
+        if (res_probe_rows_ > 0) return (double)res_out_rows_ / (double)res_probe_rows_;
+        int64_t rows = 0, keys = 0;
+        for (const Part &P : parts_)
+            if (!P.spilled && P.join) {
+                rows += P.join->indexed_rows();
+                keys += P.join->counters().build_keys;
+            }
+        double r = keys > 0 ? (double)rows / (double)keys : 1.0;
+        if (spec_.join_type == KRV_JOIN_LEFT_OUTER) r = std::max(r, 1.0);
+        return r;
+    }
+
+    static std::vector<int> projection(int n, const int32_t *cols, int ncols) {
+        std::vector<int> v;
+        if (n < 0) {
+            for (int i = 0; i < ncols; i++) v.push_back(i);
+        } else {
+            for (int i = 0; i < n; i++) {
+                if (cols[i] < 0 || cols[i] >= ncols) fail(KRV_INVALID_ARGUMENT, "projection column out of range");
+                v.push_back(cols[i]);
+            }
+        }
+        return v;
+    }
+
+    // The segments `now` of one partitioned slice, each probed against its
+    // resident partition's table, in one launch and one output batch.
+    DevBatch probe_resident(const std::vector<Segment> &segs, const std::vector<int> &now, double ratio) {
+        const int key = spec_.probe_keys[0];
+        const std::vector<int> pcols = projection(spec_.n_probe_out, spec_.probe_out, (int)probe_types_.size());
+        const std::vector<int> bcols = projection(spec_.n_build_out, spec_.build_out, (int)build_types_.size());
+        if (pcols.size() + bcols.size() > (size_t)kGMaxOut) fail(KRV_UNSUPPORTED, "more than 16 output columns");
+        const DevBatch &first = segs[now[0]].batch;
+        GOutDev od{};
+        for (size_t c = 0; c < first.cols.size(); c++) od.pcol[c] = first.cols[c].hold_data->get();
+        od.pkey = static_cast<const long long *>(od.pcol[key]);
+        std::vector<GPartDev> hp;
+        int64_t tiles = 0, rows = 0;
+        for (int p : now) {
+            const Segment &s = segs[p];
+            const HashJoin &J = *parts_[p].join;
+            const HashJoin::TableDev tv = J.table_dev();
+            GPartDev d{};
+            d.slots = tv.slots;
+            d.mask = tv.mask;
+            d.next = tv.next;
+            const DevBatch &arena = J.arena();
+            d.bkey = arena.cols.empty() ? nullptr : static_cast<const long long *>(arena.cols[spec_.build_keys[0]].data);
+            for (size_t c = 0; c < arena.cols.size() && c < (size_t)kMaxCols; c++) d.bcol[c] = arena.cols[c].data;
+            d.prow0 = (static_cast<const uint8_t *>(s.batch.cols[key].data) - static_cast<const uint8_t *>(od.pcol[key])) / 8;
+            d.rows = s.rows;
+            d.tile0 = tiles;
+            tiles += ceil_div(s.rows, (int64_t)kGProbeThreads);
+            rows += s.rows;
+            hp.push_back(d);
+        }
+        DBuf dparts(rt_, hp.size() * sizeof(GPartDev));
+        KRV_CUDA(cudaMemcpyAsync(dparts.get(), hp.data(), hp.size() * sizeof(GPartDev), cudaMemcpyHostToDevice,
+                                 rt_->stream));
+        const bool left = spec_.join_type == KRV_JOIN_LEFT_OUTER;
+        unsigned long long cap = std::max<unsigned long long>(1, (unsigned long long)((double)rows * ratio * 1.05) + 1024);
+        DBuf cnt(rt_, 8);
+        for (int attempt = 0; attempt < 3; attempt++) {
+            DevBatch o;
+            od.n = 0;
+            for (int pc : pcols) {
+                const DevCol &m = probe_types_[pc];
+                DevCol d = make_col(rt_, m.type, (int64_t)cap, m.nullable, m.name);
+                if (d.valid) KRV_CUDA(cudaMemsetAsync(const_cast<uint8_t *>(d.valid), 0, d.hold_valid->bytes(), rt_->stream));
+                od.c[od.n++] = GOutCol{const_cast<void *>(d.data), (uint32_t *)d.valid, m.type.width(), 0, pc};
+                o.cols.push_back(d);
+            }
+            for (int bc : bcols) {
+                const DevCol &m = build_types_[bc];
+                DevCol d = make_col(rt_, m.type, (int64_t)cap, m.nullable || left, m.name);
+                if (d.valid) KRV_CUDA(cudaMemsetAsync(const_cast<uint8_t *>(d.valid), 0, d.hold_valid->bytes(), rt_->stream));
+                od.c[od.n++] = GOutCol{const_cast<void *>(d.data), (uint32_t *)d.valid, m.type.width(), 1, bc};
+                o.cols.push_back(d);
+            }
+            KRV_CUDA(cudaMemsetAsync(cnt.get(), 0, 8, rt_->stream));
+            clear_status(rt_);
+            const int grid = (int)std::min<int64_t>(tiles, (int64_t)rt_->sm_count * 8);
+            grace_probe_kernel<<<grid, kGProbeThreads, 0, rt_->stream>>>(
+                dparts.as<GPartDev>(), (int)hp.size(), tiles, spec_.seed, od, cap, cnt.as<unsigned long long>(),
+                left ? 1 : 0, spec_.single_match, status_word(rt_));
+            rt_->launches++;
+            check_launch("grace_probe_kernel");
+            const unsigned long long got = read_scalar<unsigned long long>(rt_, cnt.get());
+            if (take_status(rt_) & ST_TOO_MANY)
+                fail(KRV_TOO_MANY_ROWS, "SCALAR_SUBQUERY_TOO_MANY_ROWS: a probe row matched more than one build row");
+            if (got <= cap) {
+                o.rows = (int64_t)got;
+                for (DevCol &c : o.cols) c.length = o.rows;
+                res_probe_rows_ += rows;
+                res_out_rows_ += o.rows;
+                return o;
+            }
+            cap = got;  // more output than expected: again, with room for all of it
+        }
+        fail(KRV_INTERNAL, "partitioned probe output did not converge");
     }
 
     // Bytes of one output row: every column of both sides.
@@ -412,10 +654,6 @@ class GraceJoin {
     }
 
   private:
-    struct Segment {
-        DevBatch batch;
-        int64_t rows = 0;
-    };
     struct HostChunk {
         std::vector<uint8_t *> cols;
         int64_t rows = 0;
@@ -796,6 +1034,7 @@ class GraceJoin {
     std::unique_ptr<HashJoin> cur_join_;
     std::vector<std::pair<uint8_t *, size_t>> host_blocks_;
     cudaStream_t cs_ = nullptr;  // copies to and from the spill space
+    int64_t res_probe_rows_ = 0, res_out_rows_ = 0;  // the resident partitions' probes so far
     struct InFlight {
         cudaEvent_t done = nullptr;
         std::vector<std::shared_ptr<DBuf>> hold;

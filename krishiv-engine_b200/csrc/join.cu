@@ -829,7 +829,20 @@ DevBatch HashJoin::probe(const DevBatch &in) {
 
     const bool build_nullable = jt == KRV_JOIN_LEFT_OUTER || jt == KRV_JOIN_FULL_OUTER;
     const bool probe_nullable = jt == KRV_JOIN_RIGHT_OUTER || jt == KRV_JOIN_FULL_OUTER;
+    // The output's size is known only after the kernel. Unique build keys
+    // give at most one row per probe row; otherwise there is room for the
+    // rows that the earlier batches' output ratio predicts (before any, the
+    // build's mean rows per key), 5% more, and a batch with more output runs
+    // again with room for all of it.
     unsigned long long cap = (unsigned long long)std::max<int64_t>(n, 1);
+    const bool unique_keys = build_rows_ > 0 && counters_.build_keys == indexed_rows_;
+    if (pairs && !unique_keys && n > 0) {
+        const int64_t seen = counters_.probe_rows - n;
+        double ratio = seen > 0 ? (double)counters_.output_rows / (double)seen
+                       : counters_.build_keys > 0 ? (double)indexed_rows_ / (double)counters_.build_keys : 1.0;
+        if (jt == KRV_JOIN_LEFT_OUTER || jt == KRV_JOIN_FULL_OUTER) ratio = std::max(ratio, 1.0);
+        cap = std::max<unsigned long long>(1, (unsigned long long)((double)n * ratio * 1.05) + 1024);
+    }
     DBuf cnt(rt_, 8);
     for (int attempt = 0; attempt < 4; attempt++) {
         out = DevBatch{};
