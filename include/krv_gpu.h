@@ -205,16 +205,22 @@ int64_t krv_join_spilled_partitions(const krv_join *j);
 #define KRV_AGG_MODE_SHARED 2   /* shared-memory pre-aggregation + global table */
 
 #define KRV_MAX_AGGREGATES 32
+#define KRV_MAX_GROUP_KEYS 8
 
 typedef struct {
     int32_t function;  /* KRV_AGG_* */
     int32_t column;    /* input column (ignored by COUNT(*)) */
 } krv_agg_expr;
 
-/* AggregateSpec, aggregate/mod.rs:1083-1108 (final output, one group key) */
+/* AggregateSpec, aggregate/mod.rs:1083-1108 (final output). Group keys: one
+ * int32/int64/date32/decimal(18) column runs on the single-key tables
+ * directly; up to KRV_MAX_GROUP_KEYS columns of those types, decimal(38),
+ * float64, UTF-8 strings ("u") and binary ("z") are first given dense codes
+ * (NULL is a key value; float keys compare normalised). String and binary
+ * columns are taken as group keys only. */
 typedef struct {
-    int32_t n_group_by;             /* 1 (one int32/int64 key column) */
-    int32_t group_by[KRV_MAX_KEYS];
+    int32_t n_group_by;             /* 1..KRV_MAX_GROUP_KEYS */
+    int32_t group_by[KRV_MAX_GROUP_KEYS];
     int32_t n_aggregates;
     krv_agg_expr aggregates[KRV_MAX_AGGREGATES];
     int32_t ansi;                   /* spark.sql.ansi.enabled: overflow raises */

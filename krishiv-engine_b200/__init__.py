@@ -41,6 +41,7 @@ STAR_FUSED, STAR_PLAIN = 0, 1
 GEN_UNIFORM_I64, GEN_UNIFORM_I32, GEN_UNIT_F64, GEN_PERMUTATION, GEN_ZIPF = 0, 1, 2, 3, 4
 
 MAX_KEYS = 4
+MAX_GROUP_KEYS = 8
 MAX_OUT = 32
 MAX_AGGS = 32
 SCRATCH_MAX_GROUPS = 65536  # KRV_SCRATCH_MAX_GROUPS
@@ -108,7 +109,7 @@ class AggExpr(C.Structure):
 
 
 class AggSpec(C.Structure):
-    _fields_ = [("n_group_by", C.c_int32), ("group_by", C.c_int32 * MAX_KEYS), ("n_aggregates", C.c_int32),
+    _fields_ = [("n_group_by", C.c_int32), ("group_by", C.c_int32 * MAX_GROUP_KEYS), ("n_aggregates", C.c_int32),
                 ("aggregates", AggExpr * MAX_AGGS), ("ansi", C.c_int32), ("mode", C.c_int32),
                 ("expected_groups", C.c_int64), ("max_output_rows", C.c_int64)]
 
@@ -599,12 +600,15 @@ class HashJoin:
             pass
 
 
-def agg_spec(group_by: int, aggregates: Sequence, ansi=True, mode=MODE_AUTO, expected_groups=0,
+def agg_spec(group_by, aggregates: Sequence, ansi=True, mode=MODE_AUTO, expected_groups=0,
              max_output_rows=0) -> AggSpec:
+    """`group_by`: one column index or a sequence of up to MAX_GROUP_KEYS."""
     s = AggSpec()
     lib().krv_agg_spec_init(C.byref(s))
-    s.n_group_by = 1
-    s.group_by[0] = group_by
+    keys = [group_by] if isinstance(group_by, int) else list(group_by)
+    s.n_group_by = len(keys)
+    for i, k in enumerate(keys):
+        s.group_by[i] = k
     s.n_aggregates = len(aggregates)
     for i, (f, c) in enumerate(aggregates):
         s.aggregates[i].function = AGG_FUNCS[f] if isinstance(f, str) else int(f)

@@ -700,6 +700,19 @@ class HashAggregate {
     Runtime *rt_;
     krv_agg_spec spec_;
     bool planned_ = false, finished_ = false;
+    // Group keys other than one int32/int64/date32/decimal(18) column: the
+    // dictionary gives each key a dense int64 code, appended to every batch
+    // as column key_col_ and aggregated as the key.
+    KeyDict *dict_ = nullptr;
+    std::vector<int> dict_cols_;
+    int key_col_ = -1;
+
+  public:
+    ~HashAggregate() {
+        if (dict_) key_dict_destroy(dict_);
+    }
+
+  private:
     AggPlanDev P_{};
     std::vector<int> value_cols_;  // input column of each plan column
     std::vector<DType> input_types_;
@@ -722,7 +735,8 @@ class HashAggregate {
 };
 
 HashAggregate::HashAggregate(Runtime *rt, const krv_agg_spec &spec) : rt_(rt), spec_(spec) {
-    if (spec.n_group_by != 1) fail(KRV_UNSUPPORTED, "the GPU aggregate groups by exactly one key column");
+    if (spec.n_group_by < 1 || spec.n_group_by > KRV_MAX_GROUP_KEYS)
+        fail(KRV_UNSUPPORTED, "the GPU aggregate groups by 1 to 8 key columns");
     if (spec.n_aggregates < 0 || spec.n_aggregates > KRV_MAX_AGGREGATES)
         fail(KRV_INVALID_ARGUMENT, "aggregate count out of range");
     for (int e = 0; e < spec.n_aggregates; e++)
@@ -732,13 +746,30 @@ HashAggregate::HashAggregate(Runtime *rt, const krv_agg_spec &spec) : rt_(rt), s
 }
 
 void HashAggregate::plan(const DevBatch &b) {
+    for (int k = 0; k < spec_.n_group_by; k++)
+        if (spec_.group_by[k] < 0 || spec_.group_by[k] >= (int)b.cols.size())
+            fail(KRV_INVALID_ARGUMENT, "group-by column out of range");
     const int kc = spec_.group_by[0];
-    if (kc < 0 || kc >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "group-by column out of range");
-    key_type_ = b.cols[kc].type;
-    key_name_ = b.cols[kc].name;
-    if (key_type_.id != Type::I32 && key_type_.id != Type::I64 && key_type_.id != Type::Date32 &&
-        key_type_.id != Type::Dec64)
-        fail(KRV_UNSUPPORTED, "group key of type " + key_type_.format());
+    const Type t0 = b.cols[kc].type.id;
+    if (spec_.n_group_by == 1 && (t0 == Type::I32 || t0 == Type::I64 || t0 == Type::Date32 || t0 == Type::Dec64)) {
+        key_col_ = kc;
+        key_type_ = b.cols[kc].type;
+        key_name_ = b.cols[kc].name;
+    } else {
+        std::vector<DevCol> meta;
+        for (int k = 0; k < spec_.n_group_by; k++) {
+            dict_cols_.push_back(spec_.group_by[k]);
+            DevCol m;
+            m.type = b.cols[spec_.group_by[k]].type;
+            m.name = b.cols[spec_.group_by[k]].name;
+            m.nullable = b.cols[spec_.group_by[k]].nullable || b.cols[spec_.group_by[k]].valid;
+            meta.push_back(m);
+        }
+        dict_ = make_key_dict(rt_, meta);
+        key_col_ = (int)b.cols.size();
+        key_type_ = DType{Type::I64, 0, 0};
+        key_name_ = "#group";
+    }
     for (const DevCol &c : b.cols) {
         input_types_.push_back(c.type);
         input_names_.push_back(c.name);
@@ -751,7 +782,7 @@ void HashAggregate::plan(const DevBatch &b) {
         if (x.function == KRV_AGG_COUNT_STAR) continue;
         if (x.column < 0 || x.column >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "aggregate column out of range");
         const DType t = b.cols[x.column].type;
-        if (t.id == Type::Bool || t.id == Type::U8) fail(KRV_UNSUPPORTED, "aggregate over " + t.format());
+        if (t.id == Type::Bool || t.id == Type::U8 || t.var()) fail(KRV_UNSUPPORTED, "aggregate over " + t.format());
         if (t.id == Type::Dec128 && (x.function == KRV_AGG_MIN || x.function == KRV_AGG_MAX))
             fail(KRV_UNSUPPORTED, "MIN/MAX of decimal128 on the GPU aggregate");
         int at = -1;
@@ -951,17 +982,29 @@ void HashAggregate::sample_hot(const KeyIn &key, int64_t n) {
     KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // `hot` is a stack vector
 }
 
-void HashAggregate::push(const DevBatch &b) {
+void HashAggregate::push(const DevBatch &in) {
     if (finished_) fail(KRV_INVALID_ARGUMENT, "push after finish");
     DeviceGuard g(rt_);
-    if (!planned_) plan(b);
-    if (b.cols.size() != input_types_.size()) fail(KRV_INVALID_ARGUMENT, "batches differ in columns");
-    for (size_t i = 0; i < b.cols.size(); i++)
-        if (b.cols[i].type != input_types_[i]) fail(KRV_INVALID_ARGUMENT, "batches differ in types");
-    const int64_t n = b.rows;
+    if (!planned_) plan(in);
+    if (in.cols.size() != input_types_.size()) fail(KRV_INVALID_ARGUMENT, "batches differ in columns");
+    for (size_t i = 0; i < in.cols.size(); i++)
+        if (in.cols[i].type != input_types_[i]) fail(KRV_INVALID_ARGUMENT, "batches differ in types");
+    const int64_t n = in.rows;
     if (n == 0) return;
     if (n >= (int64_t)0xFFFFFFF0ll) fail(KRV_UNSUPPORTED, "aggregate batches of 2^32 rows or more");
-    const DevCol &kc = b.cols[spec_.group_by[0]];
+    DevBatch b = in;
+    DBuf codes;
+    if (dict_) {
+        codes = key_dict_encode(dict_, in, dict_cols_);
+        DevCol cc;
+        cc.type = DType{Type::I64, 0, 0};
+        cc.name = key_name_;
+        cc.nullable = false;
+        cc.length = n;
+        cc.data = codes.get();
+        b.cols.push_back(cc);
+    }
+    const DevCol &kc = b.cols[key_col_];
     KeyIn key{kc.data, kc.valid, kc.valid_off, kc.type.width(), 0};
     if (mode_ == KRV_AGG_MODE_SHARED && !sampled_) sample_hot(key, n);
     clear_status(rt_);
@@ -1080,6 +1123,14 @@ DevBatch HashAggregate::result() {
     const uint32_t st = take_status(rt_);
     if (st & ST_OVERFLOW)
         fail(KRV_ARITHMETIC_OVERFLOW, "ARITHMETIC_OVERFLOW: an aggregate overflowed its result type (ANSI mode)");
+    if (dict_) {
+        // the group-by columns in place of the codes
+        std::vector<DevCol> keys = key_dict_decode(dict_, static_cast<const long long *>(out.cols[0].data), out.rows);
+        DevCol codes = out.cols[0];
+        out.cols.erase(out.cols.begin());
+        out.cols.insert(out.cols.begin(), keys.begin(), keys.end());
+        KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // the codes are read by the decode
+    }
     return out;
 }
 

@@ -392,7 +392,7 @@ krv_status krv_agg_push(krv_agg *a, const ArrowArray *batch, const ArrowSchema *
         need(a, "aggregate");
         krv::DeviceGuard g(&a->owner->rt);
         krv::HostBorrow hb(&a->owner->rt);
-        krv::agg_push(a->a, krv::import_host(&a->owner->rt, batch, schema));
+        krv::agg_push(a->a, krv::import_host(&a->owner->rt, batch, schema, krv::HostRead::Copy, krv::Var::Allow));
         return KRV_OK;
     });
 }
@@ -400,7 +400,7 @@ krv_status krv_agg_push_device(krv_agg *a, const ArrowDeviceArray *batch, const 
     return guard([&] {
         need(a, "aggregate");
         krv::DeviceGuard g(&a->owner->rt);
-        krv::agg_push(a->a, krv::import_device(&a->owner->rt, batch, schema));
+        krv::agg_push(a->a, krv::import_device(&a->owner->rt, batch, schema, krv::Var::Allow));
         return KRV_OK;
     });
 }

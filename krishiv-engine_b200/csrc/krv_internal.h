@@ -146,13 +146,16 @@ enum class Type : int32_t {
     Dec128 = 6,  // "d:p,s" / "d:p,s,128"
     Date32 = 7,  // "tdD" (int32 days)
     U8 = 8,      // "C" (internal)
+    Utf8 = 9,    // "u" (int32 offsets + bytes)
+    Binary = 10, // "z" (int32 offsets + bytes)
 };
 
 struct DType {
     Type id = Type::I64;
     int32_t precision = 0;
     int32_t scale = 0;
-    int width() const;  // bytes per value (Bool: 0, bit-packed)
+    int width() const;  // bytes per value (Bool: 0, bit-packed; Utf8/Binary: 0, variable)
+    bool var() const { return id == Type::Utf8 || id == Type::Binary; }
     std::string format() const;
     bool operator==(const DType &o) const {
         return id == o.id && precision == o.precision && scale == o.scale;
@@ -166,7 +169,9 @@ DType parse_format(const char *fmt);
 struct DevCol {
     DType type;
     int64_t length = 0;
-    const void *data = nullptr;
+    const void *data = nullptr;  // values; Utf8/Binary: int32 offsets of rows 0..length
+    const void *bytes = nullptr; // Utf8/Binary: value i is bytes[offsets[i] .. offsets[i + 1])
+    int64_t var_bytes = -1;      // Utf8/Binary: offsets[length] when offsets[0] is 0 and it is known
     const void *host = nullptr;  // a column read in place: its host address
     const uint8_t *valid = nullptr;
     int64_t valid_off = 0;
@@ -174,6 +179,7 @@ struct DevCol {
     std::string name;
     std::shared_ptr<DBuf> hold_data;   // owned memory, if any
     std::shared_ptr<DBuf> hold_valid;
+    std::shared_ptr<DBuf> hold_bytes;
 };
 
 struct DevBatch {
@@ -186,10 +192,13 @@ struct DevBatch {
 // cudaHostRegister) become views that kernels read where they lie, over the
 // host link, and only the bytes a kernel touches cross it; other columns are
 // copied. Either way the calling entry point holds a HostBorrow.
+// Utf8/Binary columns are taken only where `var` is Var::Allow (an
+// aggregate's group keys); elsewhere they fail with KRV_UNSUPPORTED.
 enum class HostRead { Copy, InPlace };
+enum class Var { Reject, Allow };
 DevBatch import_host(Runtime *rt, const ArrowArray *arr, const ArrowSchema *schema,
-                     HostRead mode = HostRead::Copy);
-DevBatch import_device(Runtime *rt, const ArrowDeviceArray *arr, const ArrowSchema *schema);
+                     HostRead mode = HostRead::Copy, Var var = Var::Reject);
+DevBatch import_device(Runtime *rt, const ArrowDeviceArray *arr, const ArrowSchema *schema, Var var = Var::Reject);
 // Export: moves the batch's buffers to the caller.
 void export_host(Runtime *rt, const DevBatch &b, ArrowArray *out, ArrowSchema *out_schema);
 void export_device(Runtime *rt, const DevBatch &b, ArrowDeviceArray *out,

@@ -61,6 +61,14 @@ struct KeyFilterDev {
 };
 KeyFilterDev key_filter_dev(const KeyFilterImpl &f);
 
+// ---- group key codes (keydict.cu) ------------------------------------------------
+class KeyDict;
+KeyDict *make_key_dict(Runtime *rt, const std::vector<DevCol> &meta);
+void key_dict_destroy(KeyDict *d);
+DBuf key_dict_encode(KeyDict *d, const DevBatch &b, const std::vector<int> &cols);
+std::vector<DevCol> key_dict_decode(KeyDict *d, const long long *codes, int64_t n);
+int64_t key_dict_size(const KeyDict *d);
+
 // ---- hash join (crates/krishiv-exec/src/join/mod.rs:1014 HashJoin) -------------
 class HashJoin {
   public:

@@ -98,6 +98,8 @@ int DType::width() const {
     case Type::Dec128: return 16;
     case Type::Date32: return 4;
     case Type::U8: return 1;
+    case Type::Utf8: return 0;
+    case Type::Binary: return 0;
     }
     return 0;
 }
@@ -113,6 +115,8 @@ std::string DType::format() const {
     case Type::Dec128: return "d:" + std::to_string(precision) + "," + std::to_string(scale);
     case Type::Date32: return "tdD";
     case Type::U8: return "C";
+    case Type::Utf8: return "u";
+    case Type::Binary: return "z";
     }
     return "l";
 }
@@ -127,6 +131,8 @@ DType parse_format(const char *fmt) {
     else if (f == "g") t.id = Type::F64;
     else if (f == "tdD") t.id = Type::Date32;
     else if (f == "C") t.id = Type::U8;
+    else if (f == "u") t.id = Type::Utf8;
+    else if (f == "z") t.id = Type::Binary;
     else if (f.rfind("d:", 0) == 0) {
         int p = 0, s = 0, bits = 128;
         const int n = std::sscanf(f.c_str() + 2, "%d,%d,%d", &p, &s, &bits);
@@ -230,6 +236,9 @@ DevCol slice_col(const DevCol &c, int64_t from, int64_t n) {
         // Bit-packed data: keep byte alignment requirements simple.
         if (from % 8) fail(KRV_INTERNAL, "unaligned boolean slice");
         s.data = static_cast<const uint8_t *>(c.data) + from / 8;
+    } else if (c.type.var()) {
+        s.data = static_cast<const int32_t *>(c.data) + from;  // offsets stay absolute into `bytes`
+        s.var_bytes = -1;
     } else {
         s.data = static_cast<const uint8_t *>(c.data) + from * c.type.width();
     }
@@ -280,9 +289,38 @@ static bool page_locked(const void *p) {
     return a.type == cudaMemoryTypeHost;
 }
 
+// A Utf8/Binary column's offsets and bytes. A device column is viewed where
+// it lies; a host column is copied with its offsets rebased to start at 0.
+static void import_var(Runtime *rt, bool device, const ArrowArray *c, int64_t off, int64_t rows, DevCol &col) {
+    const int32_t *offs = static_cast<const int32_t *>(c->buffers[1]) + off;
+    const uint8_t *bytes = static_cast<const uint8_t *>(c->buffers[2]);
+    if (device) {
+        col.data = offs;
+        col.bytes = bytes;
+        return;
+    }
+    const int32_t o0 = rows > 0 ? offs[0] : 0, on = rows > 0 ? offs[rows] : 0;
+    if (on < o0) fail(KRV_INVALID_ARGUMENT, "column '" + col.name + "' has decreasing offsets");
+    col.hold_data = std::make_shared<DBuf>(rt, (size_t)(rows + 1) * 4);
+    std::vector<int32_t> rebased((size_t)rows + 1);
+    for (int64_t i = 0; i <= rows; i++) rebased[(size_t)i] = rows > 0 ? offs[i] - o0 : 0;
+    KRV_CUDA(cudaMemcpyAsync(col.hold_data->get(), rebased.data(), rebased.size() * 4, cudaMemcpyHostToDevice,
+                             rt->stream));
+    const size_t nb = (size_t)(on - o0);
+    col.hold_bytes = std::make_shared<DBuf>(rt, nb > 0 ? nb : 8);
+    if (nb) {
+        KRV_CUDA(cudaMemcpyAsync(col.hold_bytes->get(), bytes + o0, nb, cudaMemcpyHostToDevice, rt->stream));
+        if (page_locked(bytes + o0)) rt->host_borrowed = true;
+    }
+    KRV_CUDA(cudaStreamSynchronize(rt->stream));  // `rebased` is read by the copy
+    col.data = col.hold_data->get();
+    col.bytes = col.hold_bytes->get();
+    col.var_bytes = (int64_t)nb;
+}
+
 template <bool Device>
 static DevBatch import_impl(Runtime *rt, const ArrowArray *arr, const ArrowSchema *schema,
-                            HostRead mode = HostRead::Copy) {
+                            HostRead mode = HostRead::Copy, Var var = Var::Reject) {
     check_struct(arr, schema);
     DevBatch b;
     b.rows = arr->length;
@@ -301,19 +339,33 @@ static DevBatch import_impl(Runtime *rt, const ArrowArray *arr, const ArrowSchem
         const uint8_t *data = static_cast<const uint8_t *>(c->buffers[1]);
         const uint8_t *valid = c->null_count == 0 ? nullptr : static_cast<const uint8_t *>(c->buffers[0]);
         const int w = col.type.width();
+        if (col.type.var()) {
+            if (var != Var::Allow)
+                fail(KRV_UNSUPPORTED, "column '" + col.name + "': string and binary columns are taken as aggregate "
+                                      "group keys only");
+            if (c->n_buffers < 3) fail(KRV_INVALID_ARGUMENT, "column '" + col.name + "' has no value bytes buffer");
+            import_var(rt, Device, c, off, b.rows, col);
+        }
         if (Device) {
-            if (col.type.id == Type::Bool) {
+            if (col.type.var()) {
+                col.valid = valid;
+                col.valid_off = off;
+            } else if (col.type.id == Type::Bool) {
                 if (off % 8) fail(KRV_UNSUPPORTED, "boolean device column at an unaligned offset");
                 col.data = data + off / 8;
+                col.valid = valid;
+                col.valid_off = off;
             } else {
                 col.data = data + off * w;
+                col.valid = valid;
+                col.valid_off = off;
             }
-            col.valid = valid;
-            col.valid_off = off;
         } else {
-            size_t bytes;
-            const uint8_t *src;
-            if (col.type.id == Type::Bool) {
+            size_t bytes = 0;
+            const uint8_t *src = nullptr;
+            if (col.type.var()) {
+                // imported above
+            } else if (col.type.id == Type::Bool) {
                 if (off % 8) fail(KRV_UNSUPPORTED, "boolean column at an unaligned offset");
                 bytes = (size_t)ceil_div(b.rows, 8);
                 src = data + off / 8;
@@ -321,8 +373,10 @@ static DevBatch import_impl(Runtime *rt, const ArrowArray *arr, const ArrowSchem
                 bytes = (size_t)b.rows * (size_t)w;
                 src = data + off * w;
             }
-            const uint8_t *in_place = mode == HostRead::InPlace ? mapped_host(src, bytes) : nullptr;
-            if (in_place) {
+            const uint8_t *in_place = mode == HostRead::InPlace && src ? mapped_host(src, bytes) : nullptr;
+            if (col.type.var()) {
+                // offsets and bytes copied by import_var
+            } else if (in_place) {
                 col.data = in_place;
                 col.host = src;
                 rt->host_borrowed = true;
@@ -352,11 +406,11 @@ static DevBatch import_impl(Runtime *rt, const ArrowArray *arr, const ArrowSchem
     return b;
 }
 
-DevBatch import_host(Runtime *rt, const ArrowArray *arr, const ArrowSchema *schema, HostRead mode) {
-    return import_impl<false>(rt, arr, schema, mode);
+DevBatch import_host(Runtime *rt, const ArrowArray *arr, const ArrowSchema *schema, HostRead mode, Var var) {
+    return import_impl<false>(rt, arr, schema, mode, var);
 }
 
-DevBatch import_device(Runtime *rt, const ArrowDeviceArray *arr, const ArrowSchema *schema) {
+DevBatch import_device(Runtime *rt, const ArrowDeviceArray *arr, const ArrowSchema *schema, Var var) {
     if (!arr) fail(KRV_INVALID_ARGUMENT, "null ArrowDeviceArray");
     if (arr->device_type != ARROW_DEVICE_CUDA)
         fail(KRV_INVALID_ARGUMENT, "device batch is not ARROW_DEVICE_CUDA");
@@ -367,7 +421,7 @@ DevBatch import_device(Runtime *rt, const ArrowDeviceArray *arr, const ArrowSche
         cudaEvent_t ev = *static_cast<cudaEvent_t *>(arr->sync_event);
         KRV_CUDA(cudaStreamWaitEvent(rt->stream, ev, 0));
     }
-    return import_impl<true>(rt, &arr->array, schema);
+    return import_impl<true>(rt, &arr->array, schema, HostRead::Copy, var);
 }
 
 // ---------------------------------------------------------------------------------
@@ -482,10 +536,25 @@ void export_host(Runtime *rt, const DevBatch &b, ArrowArray *out, ArrowSchema *o
     std::vector<std::shared_ptr<DBuf>> keep;
     for (size_t i = 0; i < n; i++) {
         const DevCol &c = b.cols[i];
-        const size_t bytes = c.type.id == Type::Bool ? (size_t)ceil_div(b.rows, 8) : (size_t)b.rows * c.type.width();
+        const size_t bytes = c.type.id == Type::Bool ? (size_t)ceil_div(b.rows, 8)
+                             : c.type.var()          ? (size_t)(b.rows + 1) * 4
+                                                     : (size_t)b.rows * c.type.width();
         p->bufs.emplace_back(bytes + 64);
         std::vector<uint8_t> &data = p->bufs.back();
         if (bytes) KRV_CUDA(cudaMemcpyAsync(data.data(), c.data, bytes, cudaMemcpyDeviceToHost, rt->stream));
+        const uint8_t *bptr = nullptr;
+        if (c.type.var()) {
+            // the offsets first: they say which bytes to copy; rebased to 0
+            KRV_CUDA(cudaStreamSynchronize(rt->stream));
+            int32_t *offs = reinterpret_cast<int32_t *>(data.data());
+            const int32_t o0 = offs[0], on = offs[b.rows];
+            for (int64_t r = 0; r <= b.rows; r++) offs[r] -= o0;
+            p->bufs.emplace_back((size_t)(on - o0) + 64);
+            if (on > o0)
+                KRV_CUDA(cudaMemcpyAsync(p->bufs.back().data(), static_cast<const uint8_t *>(c.bytes) + o0,
+                                         (size_t)(on - o0), cudaMemcpyDeviceToHost, rt->stream));
+            bptr = p->bufs.back().data();
+        }
         const uint8_t *vptr = nullptr;
         auto v = aligned_validity(rt, c);
         if (v) {
@@ -496,6 +565,7 @@ void export_host(Runtime *rt, const DevBatch &b, ArrowArray *out, ArrowSchema *o
             vptr = p->bufs.back().data();
         }
         p->child_bufs[i] = {vptr, data.data()};
+        if (c.type.var()) p->child_bufs[i].push_back(bptr);
     }
     KRV_CUDA(cudaStreamSynchronize(rt->stream));
     for (size_t i = 0; i < n; i++) {
@@ -504,7 +574,7 @@ void export_host(Runtime *rt, const DevBatch &b, ArrowArray *out, ArrowSchema *o
         a.length = b.rows;
         // With a bitmap the count is left to the consumer (-1: unknown).
         a.null_count = p->child_bufs[i][0] ? -1 : 0;
-        a.n_buffers = 2;
+        a.n_buffers = (int64_t)p->child_bufs[i].size();
         a.buffers = p->child_bufs[i].data();
         a.release = release_child_array;
         p->children[i] = &a;
@@ -530,16 +600,18 @@ void export_device(Runtime *rt, const DevBatch &b, ArrowDeviceArray *out, ArrowS
     for (size_t i = 0; i < n; i++) {
         const DevCol &c = b.cols[i];
         if (c.hold_data) p->hold.push_back(c.hold_data);
+        if (c.hold_bytes) p->hold.push_back(c.hold_bytes);
         auto v = aligned_validity(rt, c);
         if (v) p->hold.push_back(v);
         p->child_bufs[i] = {v ? v->get() : nullptr, c.data};
+        if (c.type.var()) p->child_bufs[i].push_back(c.bytes);
     }
     for (size_t i = 0; i < n; i++) {
         ArrowArray &a = p->child_storage[i];
         std::memset(&a, 0, sizeof(a));
         a.length = b.rows;
         a.null_count = p->child_bufs[i][0] ? -1 : 0;  // unknown without a device pass
-        a.n_buffers = 2;
+        a.n_buffers = (int64_t)p->child_bufs[i].size();
         a.buffers = p->child_bufs[i].data();
         a.release = release_child_array;
         p->children[i] = &a;

@@ -14,6 +14,12 @@ Writes:
                          crates/krishiv-exec/tests/aggregate_tpch.rs (Q13,
                          Q18) with Spark 4.2.0's expected answers, from
                          crates/krishiv-exec/tests/fixtures/tpch-sf0.01/.
+  tpch_q1.npz / tpch_q18_keys.npz -- the inputs of Q1 (two string keys,
+                         decimal sums and averages) and of Q18's outer
+                         aggregate over all five keys (string, integers,
+                         date, decimal), column by column (strings as
+                         fixed-width unicode, decimals as unscaled (lo, hi)
+                         int64 words), with Spark's expected rows as text.
 """
 import csv
 import json
@@ -83,5 +89,37 @@ def main(ref):
                         expected=np.array(sorted(exp), dtype=np.int64))
 
 
+def columns_of(t):
+    """name -> numpy arrays of one Arrow table's columns (see the docstring)."""
+    out = {}
+    for f in t.schema:
+        c = t.column(f.name).combine_chunks()
+        out[f.name + "__valid"] = c.is_valid().to_numpy(zero_copy_only=False).astype(np.uint8)
+        if pa.types.is_string(f.type):
+            out[f.name + "__str"] = np.array([v if v is not None else "" for v in c.to_pylist()])
+        elif pa.types.is_decimal(f.type):
+            words = np.frombuffer(c.buffers()[1], dtype=np.int64)[2 * c.offset: 2 * (c.offset + len(c))]
+            out[f.name + "__dec_lo"] = words[0::2].copy()
+            out[f.name + "__dec_hi"] = words[1::2].copy()
+            out[f.name + "__dec_ps"] = np.array([f.type.precision, f.type.scale], dtype=np.int64)
+        elif pa.types.is_date32(f.type):
+            out[f.name + "__date32"] = c.cast(pa.int32()).fill_null(0).to_numpy(zero_copy_only=False)
+        else:
+            out[f.name + "__" + str(f.type)] = c.fill_null(0).to_numpy(zero_copy_only=False)
+    out["__order"] = np.array([f.name for f in t.schema])
+    return out
+
+
+def extra(ref):
+    fx = os.path.join(ref, "crates/krishiv-exec/tests/fixtures/tpch-sf0.01")
+    for q, name in (("q1", "tpch_q1.npz"), ("q18", "tpch_q18_keys.npz")):
+        t = read_arrow(os.path.join(fx, q + "_input.arrow"))
+        rows = [line.strip() for line in open(os.path.join(fx, q + "_expected.csv")) if line.strip()]
+        np.savez_compressed(os.path.join(HERE, name), expected=np.array(sorted(rows)), **columns_of(t))
+
+
 if __name__ == "__main__":
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    main(ref)
+    extra(ref)
     main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
