@@ -207,9 +207,27 @@ int64_t krv_join_spilled_partitions(const krv_join *j);
 #define KRV_MAX_AGGREGATES 32
 #define KRV_MAX_GROUP_KEYS 8
 
+/* AggInput (aggregate/mod.rs:413-419) and AggregateOutput (:421-427) */
+#define KRV_AGG_INPUT_RAW 0
+#define KRV_AGG_INPUT_STATE 1
+#define KRV_AGG_OUTPUT_FINAL 0
+#define KRV_AGG_OUTPUT_PARTIAL 1
+
+/* AggregateExpr (aggregate/mod.rs:431-454). With KRV_AGG_INPUT_STATE the
+ * arguments are the state columns a KRV_AGG_OUTPUT_PARTIAL aggregate wrote
+ * for the same function (AggregateExpr::merging, :561-569): `column` is the
+ * first, `column2` the second where the state has two (SUM of a decimal:
+ * sum, nonempty; AVG: sum, count), and arg_precision / arg_scale /
+ * arg_bits describe the raw decimal argument (AVG of a decimal, whose result
+ * type follows the raw type; 0: derived from the state's sum type). */
 typedef struct {
     int32_t function;  /* KRV_AGG_* */
-    int32_t column;    /* input column (ignored by COUNT(*)) */
+    int32_t column;    /* input column (ignored by raw COUNT(*)) */
+    int32_t input;     /* KRV_AGG_INPUT_* */
+    int32_t column2;   /* second state column, or -1 */
+    int32_t arg_precision, arg_scale;
+    int32_t arg_bits;  /* the raw decimal argument's width, 64 or 128 (0: the state sum's) */
+    int32_t reserved;
 } krv_agg_expr;
 
 /* AggregateSpec, aggregate/mod.rs:1083-1108 (final output). Group keys: one
@@ -227,6 +245,11 @@ typedef struct {
     int32_t mode;                   /* KRV_AGG_MODE_* */
     int64_t expected_groups;        /* planner estimate (0: unknown) */
     int64_t max_output_rows;        /* output batch bound; 0 = one batch */
+    int32_t output;                 /* KRV_AGG_OUTPUT_*: final values, or each aggregate's
+                                       state columns (AggregateExpr::state_fields, :747-800):
+                                       COUNT: count; SUM: sum (+ nonempty for decimals);
+                                       AVG: sum, count; MIN/MAX: value */
+    int32_t reserved;
 } krv_agg_spec;
 void krv_agg_spec_init(krv_agg_spec *spec);
 

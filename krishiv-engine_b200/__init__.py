@@ -34,6 +34,8 @@ JOIN_TYPES = {"inner": INNER, "left_outer": LEFT_OUTER, "left_semi": LEFT_SEMI, 
 COUNT_STAR, COUNT, SUM, MIN, MAX, AVG = 0, 1, 2, 3, 4, 5
 AGG_FUNCS = {"count_star": COUNT_STAR, "count": COUNT, "sum": SUM, "min": MIN, "max": MAX, "avg": AVG}
 MODE_AUTO, MODE_GLOBAL, MODE_SHARED = 0, 1, 2
+AGG_INPUT_RAW, AGG_INPUT_STATE = 0, 1
+AGG_OUTPUT_FINAL, AGG_OUTPUT_PARTIAL = 0, 1
 
 FILTER_RANGE, FILTER_EXACT, FILTER_BLOOM, FILTER_EMPTY = 0, 1, 2, 3
 STAR_FUSED, STAR_PLAIN = 0, 1
@@ -105,13 +107,16 @@ class JoinCounters(C.Structure):
 
 
 class AggExpr(C.Structure):
-    _fields_ = [("function", C.c_int32), ("column", C.c_int32)]
+    _fields_ = [("function", C.c_int32), ("column", C.c_int32), ("input", C.c_int32), ("column2", C.c_int32),
+                ("arg_precision", C.c_int32), ("arg_scale", C.c_int32), ("arg_bits", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class AggSpec(C.Structure):
     _fields_ = [("n_group_by", C.c_int32), ("group_by", C.c_int32 * MAX_GROUP_KEYS), ("n_aggregates", C.c_int32),
                 ("aggregates", AggExpr * MAX_AGGS), ("ansi", C.c_int32), ("mode", C.c_int32),
-                ("expected_groups", C.c_int64), ("max_output_rows", C.c_int64)]
+                ("expected_groups", C.c_int64), ("max_output_rows", C.c_int64), ("output", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class KeyFilterOptions(C.Structure):
@@ -601,8 +606,12 @@ class HashJoin:
 
 
 def agg_spec(group_by, aggregates: Sequence, ansi=True, mode=MODE_AUTO, expected_groups=0,
-             max_output_rows=0) -> AggSpec:
-    """`group_by`: one column index or a sequence of up to MAX_GROUP_KEYS."""
+             max_output_rows=0, partial=False) -> AggSpec:
+    """`group_by`: one column index or a sequence of up to MAX_GROUP_KEYS.
+    `aggregates`: (function, column) over raw input, or (function, "state",
+    column[, column2[, (arg_precision, arg_scale, arg_bits)]]) over the state
+    columns of a partial aggregate. `partial`: emit each aggregate's state
+    columns."""
     s = AggSpec()
     lib().krv_agg_spec_init(C.byref(s))
     keys = [group_by] if isinstance(group_by, int) else list(group_by)
@@ -610,9 +619,18 @@ def agg_spec(group_by, aggregates: Sequence, ansi=True, mode=MODE_AUTO, expected
     for i, k in enumerate(keys):
         s.group_by[i] = k
     s.n_aggregates = len(aggregates)
-    for i, (f, c) in enumerate(aggregates):
+    for i, a in enumerate(aggregates):
+        f = a[0]
         s.aggregates[i].function = AGG_FUNCS[f] if isinstance(f, str) else int(f)
-        s.aggregates[i].column = c
+        if len(a) > 2 and a[1] == "state":
+            s.aggregates[i].input = AGG_INPUT_STATE
+            s.aggregates[i].column = a[2]
+            s.aggregates[i].column2 = a[3] if len(a) > 3 and a[3] is not None else -1
+            if len(a) > 4:
+                s.aggregates[i].arg_precision, s.aggregates[i].arg_scale, s.aggregates[i].arg_bits = a[4]
+        else:
+            s.aggregates[i].column = a[1]
+    s.output = AGG_OUTPUT_PARTIAL if partial else AGG_OUTPUT_FINAL
     s.ansi = int(ansi)
     s.mode = mode
     s.expected_groups = expected_groups

@@ -35,7 +35,7 @@ constexpr long long kEmptyKey = (long long)0x8080808080808080ULL;
 constexpr uint32_t kPending = 0xFFFFFFFFu;
 constexpr uint32_t kOverflowGid = 0xFFFFFFFEu;
 constexpr uint32_t kNullGid = 0, kMarkerGid = 1, kFirstGid = 2;
-constexpr int kMaxValueCols = 8;
+constexpr int kMaxValueCols = 16;
 
 enum : int32_t { F_SUM = 1, F_MIN = 2, F_MAX = 4 };
 
@@ -466,9 +466,18 @@ __global__ void rehash_kernel(const long long *okeys, const uint32_t *ogids, uin
 }
 
 // ---- results -------------------------------------------------------------------
+// Output functions beyond KRV_AGG_*: the state columns of a partial
+// aggregate and the merges of state columns.
+enum : int32_t {
+    F_SUM_AS_F64 = 100,  // AVG's partial sum of a non-decimal column, as float64
+    F_NONEMPTY = 101,    // a decimal SUM's partial "nonempty" flag (Boolean)
+    F_COUNT_MERGE = 102, // COUNT over count states: their sum
+    F_AVG_MERGE = 103,   // AVG over (sum, count) states
+};
 struct OutExprDev {
     int32_t func;
     int32_t col;      // value column index in the plan (-1: COUNT(*))
+    int32_t aux;      // SUM of decimal states: the overflowed-state count; AVG merge: the counts (-1: none)
     int32_t otype;    // result Type
     int32_t rp, rs;   // result precision/scale (decimals)
     int32_t in_type;
@@ -577,18 +586,91 @@ __global__ void __launch_bounds__(256) finalize_kernel(AggPlanDev P, OutPlanDev 
         }
         for (int e = 0; e < O.n; e++) {
             const OutExprDev &X = O.e[e];
-            bool valid = false;
+            bool valid = false, bit = false;
             if (live) {
                 const unsigned long long rows = *reinterpret_cast<const unsigned long long *>(rec + P.off_rows);
+                // the states of an overflowed decimal sum seen in this group
+                const long long poisoned = X.aux >= 0 && X.func != F_AVG_MERGE
+                                               ? *reinterpret_cast<const long long *>(rec + P.c[X.aux].off_sum)
+                                               : 0;
                 if (X.func == KRV_AGG_COUNT_STAR) {
                     static_cast<long long *>(X.dst)[r] = (long long)rows;
                     valid = true;
+                } else if (X.func == F_COUNT_MERGE) {
+                    static_cast<long long *>(X.dst)[r] = *reinterpret_cast<const long long *>(rec + P.c[X.col].off_sum);
+                    valid = true;
+                } else if (X.func == F_NONEMPTY) {
+                    const unsigned long long cnt =
+                        *reinterpret_cast<const unsigned long long *>(rec + P.c[X.col].off_count);
+                    bit = cnt > 0 || poisoned > 0;
+                    valid = true;
+                } else if (X.func == F_AVG_MERGE) {
+                    const AggColDev &C = P.c[X.col];
+                    const long long cnt = *reinterpret_cast<const long long *>(rec + P.c[X.aux].off_sum);
+                    if (cnt > 0 && C.type == (int)Type::F64) {
+                        const double hi = *reinterpret_cast<const double *>(rec + C.off_sum);
+                        const double lo = *reinterpret_cast<const double *>(rec + C.off_sum + 8);
+                        static_cast<double *>(X.dst)[r] = __ddiv_rn(isfinite(hi) ? __dadd_rn(hi, lo) : hi, (double)cnt);
+                        valid = true;
+                    } else if (cnt > 0) {
+                        const unsigned long long lo = *reinterpret_cast<const unsigned long long *>(rec + C.off_sum);
+                        const long long hi = *reinterpret_cast<const long long *>(rec + C.off_sum + 8);
+                        const __int128 sum = (__int128)(((unsigned __int128)(unsigned long long)hi << 64) | lo);
+                        __int128 v = 0;
+                        if (avg_decimal(sum, X.in_scale, cnt, X.rp, X.rs, v)) {
+                            if (X.otype == (int)Type::Dec64) static_cast<long long *>(X.dst)[r] = (long long)v;
+                            else {
+                                long long *d = static_cast<long long *>(X.dst) + 2 * r;
+                                d[0] = (long long)(unsigned long long)v;
+                                d[1] = (long long)(v >> 64);
+                            }
+                            valid = true;
+                        } else if (X.ansi) {
+                            atomicOr(status, ST_OVERFLOW);
+                        }
+                    }
+                    if (!valid) {
+                        if (X.otype == (int)Type::Dec128) {
+                            static_cast<long long *>(X.dst)[2 * r] = 0;
+                            static_cast<long long *>(X.dst)[2 * r + 1] = 0;
+                        } else {
+                            static_cast<long long *>(X.dst)[r] = 0;
+                        }
+                    }
                 } else {
                     const AggColDev &C = P.c[X.col];
                     const unsigned long long cnt = *reinterpret_cast<const unsigned long long *>(rec + C.off_count);
                     if (X.func == KRV_AGG_COUNT) {
                         static_cast<long long *>(X.dst)[r] = (long long)cnt;
                         valid = true;
+                    } else if (X.func == F_SUM_AS_F64 && cnt > 0) {
+                        const bool i32 = C.type == (int)Type::I32 || C.type == (int)Type::Date32;
+                        double v;
+                        if (C.type == (int)Type::F64) {
+                            const double hi = *reinterpret_cast<const double *>(rec + C.off_sum);
+                            const double lo = *reinterpret_cast<const double *>(rec + C.off_sum + 8);
+                            v = isfinite(hi) ? __dadd_rn(hi, lo) : hi;
+                        } else if (i32) {
+                            v = (double)*reinterpret_cast<const long long *>(rec + C.off_sum);
+                        } else {
+                            const unsigned long long lo = *reinterpret_cast<const unsigned long long *>(rec + C.off_sum);
+                            const long long hi = *reinterpret_cast<const long long *>(rec + C.off_sum + 8);
+                            const bool fits64 = (hi == 0 && !(lo >> 63)) || (hi == -1 && (lo >> 63));
+                            v = fits64 ? (double)(long long)lo : (double)hi * 18446744073709551616.0 + (double)lo;
+                        }
+                        static_cast<double *>(X.dst)[r] = v;
+                        valid = true;
+                    } else if (X.func == F_SUM_AS_F64) {
+                        static_cast<double *>(X.dst)[r] = 0.0;
+                    } else if (poisoned > 0) {
+                        // a state's sum overflowed: NULL, or the ANSI error
+                        if (X.ansi) atomicOr(status, ST_OVERFLOW);
+                        if (X.otype == (int)Type::Dec128) {
+                            static_cast<long long *>(X.dst)[2 * r] = 0;
+                            static_cast<long long *>(X.dst)[2 * r + 1] = 0;
+                        } else {
+                            static_cast<long long *>(X.dst)[r] = 0;
+                        }
                     } else if (cnt > 0) {
                         const bool i32 = C.type == (int)Type::I32 || C.type == (int)Type::Date32;
                         if (X.func == KRV_AGG_MIN || X.func == KRV_AGG_MAX) {
@@ -672,12 +754,24 @@ __global__ void __launch_bounds__(256) finalize_kernel(AggPlanDev P, OutPlanDev 
                     }
                 }
             }
+            if (X.func == F_NONEMPTY) {  // Boolean data: one bit per row
+                const unsigned w = __ballot_sync(0xFFFFFFFFu, bit);
+                if ((threadIdx.x & 31) == 0 && live) static_cast<uint32_t *>(X.dst)[r >> 5] = w;
+            }
             if (X.dst_valid) {
                 const unsigned w = __ballot_sync(0xFFFFFFFFu, valid);
                 if ((threadIdx.x & 31) == 0 && live) X.dst_valid[r >> 5] = w;
             }
         }
     }
+}
+
+// The overflowed decimal SUM states of a batch: 1 where the state's sum is
+// NULL but its `nonempty` flag is set (Boolean data, bit i = row i).
+__global__ void poison_kernel(const uint8_t *sum_valid, int64_t sum_voff, const uint8_t *nonempty,
+                              int64_t nonempty_off, int64_t n, long long *out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (!bit_get(sum_valid, sum_voff, i) && bit_get(nonempty, nonempty_off, i)) ? 1 : 0;
 }
 
 }  // namespace
@@ -706,6 +800,11 @@ class HashAggregate {
     KeyDict *dict_ = nullptr;
     std::vector<int> dict_cols_;
     int key_col_ = -1;
+    // Plan columns of each aggregate (col, aux: see OutExprDev) and the
+    // (sum, nonempty) columns of the decimal SUM states whose overflow flags
+    // are appended to every batch after the code column.
+    std::vector<int> expr_col_, expr_aux_;
+    std::vector<std::pair<int, int>> poison_src_;
 
   public:
     ~HashAggregate() {
@@ -775,34 +874,89 @@ void HashAggregate::plan(const DevBatch &b) {
         input_names_.push_back(c.name);
     }
     // One plan column per distinct input column; flags from its aggregates.
+    // Merges of decimal SUM states add a hidden int64 column per state pair:
+    // 1 where the state overflowed (its sum NULL, its nonempty flag set).
+    const int hidden_base = (int)b.cols.size() + (dict_ ? 1 : 0);
+    auto type_of = [&](int col) -> DType {
+        if (col >= hidden_base) return DType{Type::I64, 0, 0};
+        return b.cols[col].type;
+    };
     P_.ncols = 0;
     std::vector<int32_t> flags;
-    for (int e = 0; e < spec_.n_aggregates; e++) {
-        const krv_agg_expr &x = spec_.aggregates[e];
-        if (x.function == KRV_AGG_COUNT_STAR) continue;
-        if (x.column < 0 || x.column >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "aggregate column out of range");
-        const DType t = b.cols[x.column].type;
-        if (t.id == Type::Bool || t.id == Type::U8 || t.var()) fail(KRV_UNSUPPORTED, "aggregate over " + t.format());
-        if (t.id == Type::Dec128 && (x.function == KRV_AGG_MIN || x.function == KRV_AGG_MAX))
-            fail(KRV_UNSUPPORTED, "MIN/MAX of decimal128 on the GPU aggregate");
+    auto plan_col = [&](int col, int32_t flag) -> int {
         int at = -1;
         for (size_t i = 0; i < value_cols_.size(); i++)
-            if (value_cols_[i] == x.column) at = (int)i;
+            if (value_cols_[i] == col) at = (int)i;
         if (at < 0) {
-            if ((int)value_cols_.size() == kMaxValueCols) fail(KRV_UNSUPPORTED, "more than 8 aggregated columns");
-            value_cols_.push_back(x.column);
+            if ((int)value_cols_.size() == kMaxValueCols) fail(KRV_UNSUPPORTED, "more than 16 aggregated columns");
+            value_cols_.push_back(col);
             flags.push_back(0);
             at = (int)value_cols_.size() - 1;
         }
-        if (x.function == KRV_AGG_SUM || x.function == KRV_AGG_AVG) flags[at] |= F_SUM;
-        if (x.function == KRV_AGG_MIN) flags[at] |= F_MIN;
-        if (x.function == KRV_AGG_MAX) flags[at] |= F_MAX;
+        flags[at] |= flag;
+        return at;
+    };
+    auto check_col = [&](int col) {
+        if (col < 0 || col >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "aggregate column out of range");
+        const DType t = b.cols[col].type;
+        if (t.id == Type::Bool || t.id == Type::U8 || t.var()) fail(KRV_UNSUPPORTED, "aggregate over " + t.format());
+        return t;
+    };
+    expr_col_.assign(spec_.n_aggregates, -1);
+    expr_aux_.assign(spec_.n_aggregates, -1);
+    for (int e = 0; e < spec_.n_aggregates; e++) {
+        const krv_agg_expr &x = spec_.aggregates[e];
+        const bool state = x.input == KRV_AGG_INPUT_STATE;
+        if (x.input != KRV_AGG_INPUT_RAW && !state) fail(KRV_INVALID_ARGUMENT, "unknown aggregate input");
+        if (!state) {
+            if (x.function == KRV_AGG_COUNT_STAR) continue;
+            const DType t = check_col(x.column);
+            if (t.id == Type::Dec128 && (x.function == KRV_AGG_MIN || x.function == KRV_AGG_MAX))
+                fail(KRV_UNSUPPORTED, "MIN/MAX of decimal128 on the GPU aggregate");
+            int32_t f = 0;
+            if (x.function == KRV_AGG_SUM || x.function == KRV_AGG_AVG) f = F_SUM;
+            if (x.function == KRV_AGG_MIN) f = F_MIN;
+            if (x.function == KRV_AGG_MAX) f = F_MAX;
+            expr_col_[e] = plan_col(x.column, f);
+            continue;
+        }
+        // Partial states (AggregateExpr::merging, aggregate/mod.rs:561-569).
+        const DType t = check_col(x.column);
+        const bool dec = t.id == Type::Dec64 || t.id == Type::Dec128;
+        switch (x.function) {
+        case KRV_AGG_COUNT_STAR:
+        case KRV_AGG_COUNT:
+            if (t.id != Type::I64) fail(KRV_INVALID_ARGUMENT, "a COUNT state is an int64 column");
+            expr_col_[e] = plan_col(x.column, F_SUM);
+            break;
+        case KRV_AGG_SUM:
+            expr_col_[e] = plan_col(x.column, F_SUM);
+            if (dec) {
+                if (x.column2 < 0 || x.column2 >= (int)b.cols.size() || b.cols[x.column2].type.id != Type::Bool)
+                    fail(KRV_INVALID_ARGUMENT, "a decimal SUM state is (sum, nonempty Boolean)");
+                poison_src_.push_back({x.column, x.column2});
+                expr_aux_[e] = plan_col(hidden_base + (int)poison_src_.size() - 1, F_SUM);
+            }
+            break;
+        case KRV_AGG_AVG:
+            if (!dec && t.id != Type::F64) fail(KRV_INVALID_ARGUMENT, "an AVG state's sum is decimal or float64");
+            if (x.column2 < 0 || check_col(x.column2).id != Type::I64)
+                fail(KRV_INVALID_ARGUMENT, "an AVG state is (sum, int64 count)");
+            expr_col_[e] = plan_col(x.column, F_SUM);
+            expr_aux_[e] = plan_col(x.column2, F_SUM);
+            break;
+        case KRV_AGG_MIN:
+        case KRV_AGG_MAX:
+            if (t.id == Type::Dec128) fail(KRV_UNSUPPORTED, "MIN/MAX of decimal128 on the GPU aggregate");
+            expr_col_[e] = plan_col(x.column, x.function == KRV_AGG_MIN ? F_MIN : F_MAX);
+            break;
+        }
     }
     // Record layout: 16-byte sums first, then 8-byte fields, then 4-byte ones.
     int off = 0;
     P_.ncols = (int)value_cols_.size();
     for (int c = 0; c < P_.ncols; c++) {
-        const DType t = b.cols[value_cols_[c]].type;
+        const DType t = type_of(value_cols_[c]);
         AggColDev &C = P_.c[c];
         C.type = (int)t.id;
         C.flags = flags[c];
@@ -1004,6 +1158,22 @@ void HashAggregate::push(const DevBatch &in) {
         cc.data = codes.get();
         b.cols.push_back(cc);
     }
+    std::vector<DBuf> hidden;
+    for (const auto &ps : poison_src_) {
+        const DevCol &sc = in.cols[ps.first], &nc = in.cols[ps.second];
+        hidden.emplace_back(rt_, (size_t)n * 8);
+        poison_kernel<<<grid_for(rt_, n, 256, 8), 256, 0, rt_->stream>>>(
+            sc.valid, sc.valid_off, static_cast<const uint8_t *>(nc.data), 0, n, hidden.back().as<long long>());
+        rt_->launches++;
+        check_launch("poison_kernel");
+        DevCol hc;
+        hc.type = DType{Type::I64, 0, 0};
+        hc.name = "#overflowed";
+        hc.nullable = false;
+        hc.length = n;
+        hc.data = hidden.back().get();
+        b.cols.push_back(hc);
+    }
     const DevCol &kc = b.cols[key_col_];
     KeyIn key{kc.data, kc.valid, kc.valid_off, kc.type.width(), 0};
     if (mode_ == KRV_AGG_MODE_SHARED && !sampled_) sample_hot(key, n);
@@ -1057,58 +1227,109 @@ DevBatch HashAggregate::result() {
     const bool key_nullable = special_rows[0] != 0;
     DevCol kcol = make_col(rt_, key_type_, nout, key_nullable, key_name_);
     out.cols.push_back(kcol);
-    O.n = spec_.n_aggregates;
+    // Output expressions: one per aggregate (final), or each aggregate's
+    // state columns (partial; AggregateExpr::state_fields, aggregate/mod.rs:747-800).
+    struct OutSpec {
+        int32_t func, col, aux;
+        DType in, type;
+        std::string name;
+        bool nullable;
+    };
+    std::vector<OutSpec> outs;
+    static const char *fname[] = {"count(1)", "count", "sum", "min", "max", "avg"};
+    const bool partial = spec_.output == KRV_AGG_OUTPUT_PARTIAL;
     for (int e = 0; e < spec_.n_aggregates; e++) {
         const krv_agg_expr &x = spec_.aggregates[e];
-        OutExprDev &X = O.e[e];
-        X.func = x.function;
-        X.ansi = spec_.ansi;
-        X.col = -1;
-        DType ot{Type::I64, 0, 0};
-        std::string name;
-        static const char *fname[] = {"count(1)", "count", "sum", "min", "max", "avg"};
-        if (x.function == KRV_AGG_COUNT_STAR) {
-            name = "count(1)";
-        } else {
-            for (size_t i = 0; i < value_cols_.size(); i++)
-                if (value_cols_[i] == x.column) X.col = (int)i;
-            const DType it = input_types_[x.column];
-            X.in_type = (int)it.id;
-            X.in_scale = it.scale;
-            name = std::string(fname[x.function]) + "(" + input_names_[x.column] + ")";
-            const bool dec = it.id == Type::Dec64 || it.id == Type::Dec128;
-            switch (x.function) {
-            case KRV_AGG_COUNT: ot = DType{Type::I64, 0, 0}; break;
-            case KRV_AGG_MIN:
-            case KRV_AGG_MAX: ot = it; break;
-            case KRV_AGG_SUM:
-                if (dec) {
-                    // sum_decimal (aggregate/mod.rs:929-931) on decimal_on's carrier (:1018-1024)
-                    const int p = std::min(38, it.precision + 10);
-                    ot = DType{(it.id == Type::Dec64 && p <= 18) ? Type::Dec64 : Type::Dec128, p, it.scale};
-                } else if (it.id == Type::F64) {
-                    ot = DType{Type::F64, 0, 0};
-                } else {
-                    ot = DType{Type::I64, 0, 0};
-                }
-                break;
-            case KRV_AGG_AVG:
-                if (dec) {
-                    const int p = std::min(38, it.precision + 4), s = std::min(38, it.scale + 4);
-                    ot = DType{(it.id == Type::Dec64 && p <= 18) ? Type::Dec64 : Type::Dec128, p, s};
-                } else {
-                    ot = DType{Type::F64, 0, 0};
-                }
-                break;
+        const bool state = x.input == KRV_AGG_INPUT_STATE;
+        const int col = expr_col_[e], aux = expr_aux_[e];
+        const DType it = col >= 0 ? input_types_[x.column] : DType{Type::I64, 0, 0};
+        const std::string name = x.function == KRV_AGG_COUNT_STAR
+                                     ? std::string("count(1)")
+                                     : std::string(fname[x.function]) + "(" + input_names_[x.column] + ")";
+        const bool dec = it.id == Type::Dec64 || it.id == Type::Dec128;
+        const DType i64{Type::I64, 0, 0}, f64{Type::F64, 0, 0};
+        // sum_decimal (aggregate/mod.rs:929-931) on decimal_on's carrier (:1018-1024); a
+        // merge of decimal sums keeps the state's type
+        auto sum_type = [&]() -> DType {
+            if (dec && state) return it;
+            if (dec) {
+                const int p = std::min(38, it.precision + 10);
+                return DType{(it.id == Type::Dec64 && p <= 18) ? Type::Dec64 : Type::Dec128, p, it.scale};
             }
+            return it.id == Type::F64 ? f64 : i64;
+        };
+        // AVG of a decimal: (p + 4, s + 4) of the raw argument
+        auto avg_type = [&]() -> DType {
+            if (!dec) return f64;
+            int rp = it.precision, rs = it.scale;
+            bool r64 = it.id == Type::Dec64;
+            if (state) {
+                rp = x.arg_precision > 0 ? x.arg_precision : it.precision < 38 ? it.precision - 10 : -1;
+                if (rp <= 0) fail(KRV_INVALID_ARGUMENT, "AVG over decimal states of precision 38 needs arg_precision");
+                rs = x.arg_precision > 0 ? x.arg_scale : it.scale;
+                r64 = x.arg_bits ? x.arg_bits == 64 : it.id == Type::Dec64;
+            }
+            const int p = std::min(38, rp + 4), sc = std::min(38, rs + 4);
+            return DType{(r64 && p <= 18) ? Type::Dec64 : Type::Dec128, p, sc};
+        };
+        auto add = [&](int32_t func, int c, int a, DType type, const std::string &nm, bool nullable) {
+            outs.push_back(OutSpec{func, c, a, it, type, nm, nullable});
+        };
+        const int32_t count_f = state ? F_COUNT_MERGE : x.function;
+        switch (x.function) {
+        case KRV_AGG_COUNT_STAR:
+        case KRV_AGG_COUNT:
+            add(count_f, col, -1, i64, partial ? name + "#count" : name, false);
+            break;
+        case KRV_AGG_MIN:
+        case KRV_AGG_MAX:
+            add(x.function, col, -1, it, partial ? name + "#value" : name, true);
+            break;
+        case KRV_AGG_SUM:
+            add(KRV_AGG_SUM, col, aux, sum_type(), partial ? name + "#sum" : name, true);
+            if (partial && dec) add(F_NONEMPTY, col, aux, DType{Type::Bool, 0, 0}, name + "#nonempty", false);
+            break;
+        case KRV_AGG_AVG:
+            if (!partial) {
+                add(state ? F_AVG_MERGE : KRV_AGG_AVG, col, aux, avg_type(), name, true);
+            } else if (state) {
+                add(KRV_AGG_SUM, col, -1, sum_type(), name + "#sum", true);
+                add(F_COUNT_MERGE, aux, -1, i64, name + "#count", false);
+            } else {
+                add(dec ? KRV_AGG_SUM : F_SUM_AS_F64, col, -1, dec ? sum_type() : f64, name + "#sum", true);
+                add(KRV_AGG_COUNT, col, -1, i64, name + "#count", false);
+            }
+            break;
         }
-        X.otype = (int)ot.id;
-        X.rp = ot.precision;
-        X.rs = ot.scale;
-        const bool nullable = !(x.function == KRV_AGG_COUNT_STAR || x.function == KRV_AGG_COUNT);
-        DevCol c = make_col(rt_, ot, nout, nullable, name);
+    }
+    if ((int)outs.size() > kMaxExprs) fail(KRV_UNSUPPORTED, "more than 32 output columns of aggregates");
+    O.n = (int)outs.size();
+    for (int e = 0; e < O.n; e++) {
+        const OutSpec &o = outs[e];
+        OutExprDev &X = O.e[e];
+        X.func = o.func;
+        X.col = o.col;
+        X.aux = o.aux;
+        X.ansi = spec_.ansi;
+        X.in_type = (int)o.in.id;
+        X.in_scale = o.in.scale;
+        X.otype = (int)o.type.id;
+        X.rp = o.type.precision;
+        X.rs = o.type.scale;
+        DevCol c;
+        if (o.type.id == Type::Bool) {
+            // whole 32-bit words: the kernel stores one word per 32 rows
+            c.type = o.type;
+            c.name = o.name;
+            c.nullable = false;
+            c.length = nout;
+            c.hold_data = std::make_shared<DBuf>(rt_, (size_t)ceil_div(std::max<int64_t>(nout, 1), 32) * 4);
+            c.data = c.hold_data->get();
+        } else {
+            c = make_col(rt_, o.type, nout, o.nullable, o.name);
+        }
         X.dst = const_cast<void *>(c.data);
-        X.dst_valid = nullable ? (uint32_t *)c.valid : nullptr;
+        X.dst_valid = o.nullable ? (uint32_t *)c.valid : nullptr;
         out.cols.push_back(c);
     }
     out.rows = nout;

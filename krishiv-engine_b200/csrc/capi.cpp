@@ -372,6 +372,7 @@ void krv_agg_spec_init(krv_agg_spec *s) {
     *s = krv_agg_spec{};
     s->n_group_by = 1;
     s->ansi = 1;
+    for (int e = 0; e < KRV_MAX_AGGREGATES; e++) s->aggregates[e].column2 = -1;
 }
 
 krv_status krv_agg_create(krv_runtime *rt, const krv_agg_spec *spec, krv_agg **out) {

@@ -145,7 +145,8 @@ __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(PartArgs A, 
 // partition), and all their output rows go to one output batch: no launch,
 // output count read or output copy per partition. The table lookups, chain
 // walks and output rounds are those of the unpartitioned join's probe
-// (pairs: newest build row first, left outer pads unmatched rows).
+// (pairs: newest build row first, left outer pads unmatched rows). Tiles of
+// 32 rows, each within one partition, are taken one per warp.
 constexpr int kGProbeThreads = 256;
 constexpr int kGMaxOut = 16;
 constexpr uint32_t kGNone = 0xFFFFFFFFu;
@@ -156,7 +157,7 @@ struct GPartDev {
     const long long *bkey;
     const void *bcol[kMaxCols];  // the partition's build columns
     int64_t prow0, rows;         // its rows of the partitioned slice
-    int64_t tile0;               // its first tile
+    int64_t tile0;               // its first tile (of 32 rows)
 };
 struct GOutCol {
     void *dst;
@@ -181,39 +182,45 @@ __global__ void __launch_bounds__(kGProbeThreads) grace_probe_kernel(const GPart
                                                                      uint64_t seed, GOutDev out, unsigned long long cap,
                                                                      unsigned long long *count, int pad,
                                                                      int single_match, uint32_t *status) {
-    __shared__ GPartDev sp;
     const unsigned lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
-    for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-        __syncthreads();  // the previous tile's partition is read no more
-        if (threadIdx.x == 0) {
-            int p = 0;
-            while (p + 1 < nparts && parts[p + 1].tile0 <= t) p++;
-            sp = parts[p];
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    // Tiles of 32 rows, one warp each: no block-wide synchronization.
+    for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < tiles; t += nwarps) {
+        // the tile's partition: the last one whose first tile is at most t
+        int p = 0;
+        for (int base = 0; base < nparts; base += 32) {
+            const int q = base + (int)lane;
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, q < nparts && parts[q].tile0 <= t);
+            if (m) p = base + 31 - __clz(m);
         }
-        __syncthreads();
-        const int64_t local = (t - sp.tile0) * kGProbeThreads + threadIdx.x;
-        const bool live = local < sp.rows;
-        const int64_t prow = sp.prow0 + local;
+        const GPartDev *sp = parts + p;
+        const unsigned long long *slots = sp->slots;
+        const uint64_t mask = sp->mask;
+        const int64_t local = (t - sp->tile0) * 32 + lane;
+        const bool live = local < sp->rows;
+        const int64_t prow = sp->prow0 + local;
         uint32_t cur = kGNone;
         if (live) {
             const long long k = out.pkey[prow];
             const uint64_t g = finalize(hash_word((uint64_t)k), seed);
             const unsigned long long tag = g >> 32;
-            uint64_t pos = g & sp.mask;
-            for (uint64_t probes = 0; probes <= sp.mask; probes++) {
-                const unsigned long long sl = __ldg(sp.slots + pos);
+            uint64_t pos = g & mask;
+            const long long *bkey = sp->bkey;
+            for (uint64_t probes = 0; probes <= mask; probes++) {
+                const unsigned long long sl = __ldg(slots + pos);
                 if (sl == 0) break;
                 if ((sl >> 32) == tag) {
                     const uint32_t o = (uint32_t)(sl & 0xFFFFFFFFull) - 1u;
-                    if (__ldg(sp.bkey + o) == k) {
+                    if (__ldg(bkey + o) == k) {
                         cur = o;
                         break;
                     }
                 }
-                pos = (pos + 1) & sp.mask;
+                pos = (pos + 1) & mask;
             }
         }
+        const uint32_t *next = sp->next;
         bool padrow = live && cur == kGNone && pad;
         unsigned chain = 0;
         while (__any_sync(0xFFFFFFFFu, cur != kGNone || padrow)) {
@@ -232,7 +239,7 @@ __global__ void __launch_bounds__(kGProbeThreads) grace_probe_kernel(const GPart
                         gcopy(C.dst, out.pcol[C.col], at, prow, C.width);
                         v = true;
                     } else if (cur != kGNone) {
-                        gcopy(C.dst, sp.bcol[C.col], at, cur, C.width);
+                        gcopy(C.dst, sp->bcol[C.col], at, cur, C.width);
                         v = true;
                     } else if (C.width == 8) {
                         static_cast<unsigned long long *>(C.dst)[at] = 0ull;
@@ -254,7 +261,7 @@ __global__ void __launch_bounds__(kGProbeThreads) grace_probe_kernel(const GPart
             }
             if (cur != kGNone) {
                 chain++;
-                cur = sp.next[cur];
+                cur = next[cur];
             } else {
                 padrow = false;
             }
@@ -497,7 +504,7 @@ class GraceJoin {
             d.prow0 = (static_cast<const uint8_t *>(s.batch.cols[key].data) - static_cast<const uint8_t *>(od.pcol[key])) / 8;
             d.rows = s.rows;
             d.tile0 = tiles;
-            tiles += ceil_div(s.rows, (int64_t)kGProbeThreads);
+            tiles += ceil_div(s.rows, (int64_t)32);
             rows += s.rows;
             hp.push_back(d);
         }
@@ -526,7 +533,7 @@ class GraceJoin {
             }
             KRV_CUDA(cudaMemsetAsync(cnt.get(), 0, 8, rt_->stream));
             clear_status(rt_);
-            const int grid = (int)std::min<int64_t>(tiles, (int64_t)rt_->sm_count * 8);
+            const int grid = (int)std::min<int64_t>(ceil_div(tiles, (int64_t)kGProbeThreads / 32), (int64_t)rt_->sm_count * 8);
             grace_probe_kernel<<<grid, kGProbeThreads, 0, rt_->stream>>>(
                 dparts.as<GPartDev>(), (int)hp.size(), tiles, spec_.seed, od, cap, cnt.as<unsigned long long>(),
                 left ? 1 : 0, spec_.single_match, status_word(rt_));

@@ -906,8 +906,8 @@ class Server {
         as.n_group_by = 1;
         as.group_by[0] = 1;
         as.n_aggregates = 2;
-        as.aggregates[0] = krv_agg_expr{KRV_AGG_SUM, 0};
-        as.aggregates[1] = krv_agg_expr{KRV_AGG_COUNT_STAR, 0};
+        as.aggregates[0] = krv_agg_expr{KRV_AGG_SUM, 0, KRV_AGG_INPUT_RAW, -1, 0, 0, 0, 0};
+        as.aggregates[1] = krv_agg_expr{KRV_AGG_COUNT_STAR, 0, KRV_AGG_INPUT_RAW, -1, 0, 0, 0, 0};
         as.ansi = opt_.ansi;
         as.expected_groups = std::max<int64_t>(r.table->ngroups, 1);
         std::unique_ptr<HashAggregate, void (*)(HashAggregate *)> a(make_aggregate(rt_, as), agg_destroy);

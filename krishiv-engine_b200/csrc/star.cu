@@ -707,8 +707,8 @@ class StarPipeline {
             as.n_group_by = 1;
             as.group_by[0] = 0;
             as.n_aggregates = 2;
-            as.aggregates[0] = krv_agg_expr{KRV_AGG_SUM, 1};
-            as.aggregates[1] = krv_agg_expr{KRV_AGG_COUNT_STAR, 0};
+            as.aggregates[0] = krv_agg_expr{KRV_AGG_SUM, 1, KRV_AGG_INPUT_RAW, -1, 0, 0, 0, 0};
+            as.aggregates[1] = krv_agg_expr{KRV_AGG_COUNT_STAR, 0, KRV_AGG_INPUT_RAW, -1, 0, 0, 0, 0};
             as.expected_groups = std::max(ngroups_host_, 1);
             as.mode = KRV_AGG_MODE_GLOBAL;
             plain_agg_ = make_aggregate(rt_, as);
