@@ -239,7 +239,7 @@ krv_status krv_join_build_push(krv_join *j, const ArrowArray *batch, const Arrow
         need(j, "join");
         krv::DeviceGuard g(&j->owner->rt);
         krv::HostBorrow hb(&j->owner->rt);
-        DevBatch b = krv::import_host(&j->owner->rt, batch, schema);
+        DevBatch b = krv::import_host(&j->owner->rt, batch, schema, krv::HostRead::Copy, krv::Var::Allow);
         if (j->g) krv::grace_build_push(j->g, b);
         else j->j->build_push(b);
         return KRV_OK;
@@ -249,7 +249,7 @@ krv_status krv_join_build_push_device(krv_join *j, const ArrowDeviceArray *batch
     return guard([&] {
         need(j, "join");
         krv::DeviceGuard g(&j->owner->rt);
-        DevBatch b = krv::import_device(&j->owner->rt, batch, schema);
+        DevBatch b = krv::import_device(&j->owner->rt, batch, schema, krv::Var::Allow);
         if (j->g) krv::grace_build_push(j->g, b);
         else j->j->build_push(b);
         return KRV_OK;
@@ -279,10 +279,10 @@ static krv_status join_probe_impl(krv_join *j, const In *in, const ArrowSchema *
             DevBatch inb;
             std::unique_ptr<krv::HostBorrow> hb;
             if constexpr (Device) {
-                inb = krv::import_device(rt, in, in_schema);
+                inb = krv::import_device(rt, in, in_schema, krv::Var::Allow);
             } else {
                 hb.reset(new krv::HostBorrow(rt));
-                inb = krv::import_host(rt, in, in_schema);
+                inb = krv::import_host(rt, in, in_schema, krv::HostRead::Copy, krv::Var::Allow);
             }
             if (j->g) {
                 std::vector<DevBatch> outs = krv::grace_probe(j->g, inb);

@@ -602,9 +602,131 @@ void HashJoin::build_adopt(DevBatch b) {
     arena_cap_ = b.rows;
 }
 
+HashJoin::~HashJoin() = default;
+
+static void reject_var(const DevBatch &b) {
+    for (const DevCol &c : b.cols)
+        if (c.type.var()) fail(KRV_UNSUPPORTED, "column '" + c.name + "': string and binary columns are taken as keys only");
+}
+
+// Whether the keys are coded: some key column of the first build batch is
+// a string or binary column.
+void HashJoin::decide(const DevBatch &b) {
+    decided_ = true;
+    bool var = false;
+    for (int k = 0; k < spec_.n_keys; k++) {
+        const int c = spec_.build_keys[k];
+        if (c < 0 || c >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "build key column out of range");
+        var = var || b.cols[c].type.var();
+    }
+    if (!var) return;
+    coded_.reset(new Coded());
+    coded_->outer = spec_;
+    std::vector<DevCol> meta;
+    for (int k = 0; k < spec_.n_keys; k++) {
+        const DevCol &c = b.cols[spec_.build_keys[k]];
+        DevCol m;
+        m.type = c.type;
+        m.name = c.name;
+        m.nullable = c.nullable || c.valid;
+        meta.push_back(m);
+    }
+    coded_->dict = make_key_dict(rt_, meta);
+    // the build side's columns without its string columns, then the code
+    std::vector<int> map;
+    int inner = 0;
+    for (const DevCol &c : b.cols) map.push_back(c.type.var() ? -1 : inner++);
+    const krv_join_spec &o = coded_->outer;
+    spec_.n_keys = 1;
+    spec_.build_keys[0] = inner;
+    spec_.null_safe[0] = 0;
+    spec_.runtime_filter = 0;  // a filter over codes answers nothing outside
+    const int nb = o.n_build_out < 0 ? (int)b.cols.size() : o.n_build_out;
+    for (int i = 0; i < nb; i++) {
+        const int c = o.n_build_out < 0 ? i : o.build_out[i];
+        if (c < 0 || c >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "projection column out of range");
+        if (map[c] < 0) fail(KRV_UNSUPPORTED, "string and binary columns in a join's output");
+        spec_.build_out[i] = map[c];
+    }
+    spec_.n_build_out = nb;
+}
+
+__global__ void code_valid_kernel(KeysDev k, int64_t n, uint32_t *bits) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i - (threadIdx.x & 31) < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        bool v = i < n;
+        for (int c = 0; c < k.n && v; c++)
+            if (!((k.null_safe >> c) & 1u) && !bit_get(k.c[c].valid, k.c[c].voff, i)) v = false;
+        const unsigned w = __ballot_sync(0xFFFFFFFFu, v);
+        if ((threadIdx.x & 31) == 0) bits[i >> 5] = w;
+    }
+}
+
+// The batch the table sees: b without its string columns, then the key
+// code (NULL where an `=` key is NULL: such a row never matches).
+DevBatch HashJoin::coded_batch(const DevBatch &b, bool build) {
+    const krv_join_spec &o = coded_->outer;
+    const int32_t *keys = build ? o.build_keys : o.probe_keys;
+    std::vector<int> cols;
+    for (int k = 0; k < o.n_keys; k++) {
+        if (keys[k] < 0 || keys[k] >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "key column out of range");
+        cols.push_back(keys[k]);
+    }
+    auto codes = std::make_shared<DBuf>(key_dict_encode(coded_->dict, b, cols, build));
+    DevBatch in;
+    in.rows = b.rows;
+    std::vector<int> map;
+    int inner = 0;
+    for (const DevCol &c : b.cols) {
+        map.push_back(c.type.var() ? -1 : inner++);
+        if (!c.type.var()) in.cols.push_back(c);
+    }
+    // validity of the code: every `=` key component valid
+    KeysDev kd{};
+    kd.n = o.n_keys;
+    for (int k = 0; k < o.n_keys; k++) {
+        const DevCol &c = b.cols[keys[k]];
+        kd.c[k] = KeyColDev{c.data, c.valid, c.valid_off, 8, 0};
+        if (o.null_safe[k]) kd.null_safe |= 1u << k;
+    }
+    auto bits = std::make_shared<DBuf>(rt_, (size_t)ceil_div(std::max<int64_t>(b.rows, 1), 32) * 4 + 8);
+    if (b.rows > 0) {
+        code_valid_kernel<<<grid_for(rt_, b.rows, 256, 8), 256, 0, rt_->stream>>>(kd, b.rows, bits->as<uint32_t>());
+        rt_->launches++;
+        check_launch("code_valid_kernel");
+    }
+    DevCol cc;
+    cc.type = DType{Type::I64, 0, 0};
+    cc.name = "#key";
+    cc.nullable = true;
+    cc.length = b.rows;
+    cc.hold_data = codes;
+    cc.data = codes->get();
+    cc.hold_valid = bits;
+    cc.valid = bits->as<uint8_t>();
+    cc.valid_off = 0;
+    in.cols.push_back(cc);
+    if (!build && !coded_->probe_mapped) {
+        coded_->probe_mapped = true;
+        spec_.probe_keys[0] = inner;
+        const int np = o.n_probe_out < 0 ? (int)b.cols.size() : o.n_probe_out;
+        for (int i = 0; i < np; i++) {
+            const int c = o.n_probe_out < 0 ? i : o.probe_out[i];
+            if (c < 0 || c >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "projection column out of range");
+            if (map[c] < 0) fail(KRV_UNSUPPORTED, "string and binary columns in a join's output");
+            spec_.probe_out[i] = map[c];
+        }
+        spec_.n_probe_out = np;
+    }
+    return in;
+}
+
 void HashJoin::build_push(DevBatch b) {
     if (built_) fail(KRV_INVALID_ARGUMENT, "build_push after build_finish");
     DeviceGuard g(rt_);
+    if (!decided_) decide(b);
+    if (coded_) b = coded_batch(b, true);
+    else reject_var(b);
     append_arena(b);
 }
 
@@ -736,9 +858,13 @@ static std::vector<int> projection(int n, const int32_t *cols, int ncols) {
     return v;
 }
 
-DevBatch HashJoin::probe(const DevBatch &in) {
+DevBatch HashJoin::probe(const DevBatch &outer_in) {
     if (!built_) fail(KRV_INVALID_ARGUMENT, "probe before build_finish");
     DeviceGuard g(rt_);
+    DevBatch coded_in;
+    if (coded_) coded_in = coded_batch(outer_in, false);
+    else reject_var(outer_in);
+    const DevBatch &in = coded_ ? coded_in : outer_in;
     const int jt = spec_.join_type;
     const int64_t n = in.rows;
     counters_.probe_rows += n;

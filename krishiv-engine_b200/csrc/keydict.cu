@@ -7,7 +7,8 @@
 // :24-31, :906-1030). Here: a group key of up to eight columns (int32/int64/
 // date32/decimal/float64 values, UTF-8 strings and binary) is mapped to a
 // dense int64 code by one open-addressing table in HBM, and the aggregate
-// runs on that code with its single-key kernels. The table keeps each code's
+// runs on that code with its single-key kernels (a join with string or
+// binary keys likewise: the build side inserts, the probe side looks up). The table keeps each code's
 // key (fixed-width values by column, strings in a byte heap) and 64-bit
 // hash. NULL is a key value of its own (GROUP BY puts NULLs in one group);
 // float keys compare after normalisation (-0.0 is 0.0, one NaN), as the
@@ -301,11 +302,27 @@ class KeyDict {
     int64_t size() const { return count_; }
 
     // The int64 code of each row's key (columns `cols` of b); unseen keys get
-    // new codes.
-    DBuf encode(const DevBatch &b, const std::vector<int> &cols) {
+    // new codes (insert) or -1 (lookup only).
+    DBuf encode(const DevBatch &b, const std::vector<int> &cols, bool insert = true) {
         const int64_t n = b.rows;
+        if (cols.size() != meta_.size()) fail(KRV_INTERNAL, "key dictionary: column count");
+        for (size_t k = 0; k < cols.size(); k++)
+            if (b.cols[cols[k]].type != meta_[k].type) fail(KRV_INVALID_ARGUMENT, "key columns differ in types");
         DBuf codes(rt_, (size_t)std::max<int64_t>(n, 1) * 8);
         if (n == 0) return codes;
+        if (!insert) {
+            if (slot_count_ == 0) {
+                KRV_CUDA(cudaMemsetAsync(codes.get(), 0xFF, (size_t)n * 8, rt_->stream));
+                return codes;
+            }
+            DictDev D = dev(b, cols);
+            clear_status(rt_);
+            dict_encode_kernel<<<grid_for(rt_, n, 256, 8), 256, 0, rt_->stream>>>(D, n, 0, codes.as<long long>());
+            rt_->launches++;
+            check_launch("dict_encode_kernel");
+            if (take_status(rt_) & ST_TIMEOUT) fail(KRV_TIMEOUT, "group keys: a wait for a code gave up");
+            return codes;
+        }
         int64_t heap_need = 0;
         for (int c : cols) {
             const DevCol &col = b.cols[c];
@@ -511,7 +528,9 @@ class KeyDict {
 
 KeyDict *make_key_dict(Runtime *rt, const std::vector<DevCol> &meta) { return new KeyDict(rt, meta); }
 void key_dict_destroy(KeyDict *d) { delete d; }
-DBuf key_dict_encode(KeyDict *d, const DevBatch &b, const std::vector<int> &cols) { return d->encode(b, cols); }
+DBuf key_dict_encode(KeyDict *d, const DevBatch &b, const std::vector<int> &cols, bool insert) {
+    return d->encode(b, cols, insert);
+}
 std::vector<DevCol> key_dict_decode(KeyDict *d, const long long *codes, int64_t n) { return d->decode(codes, n); }
 int64_t key_dict_size(const KeyDict *d) { return d->size(); }
 

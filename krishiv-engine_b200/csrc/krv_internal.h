@@ -193,7 +193,8 @@ struct DevBatch {
 // host link, and only the bytes a kernel touches cross it; other columns are
 // copied. Either way the calling entry point holds a HostBorrow.
 // Utf8/Binary columns are taken only where `var` is Var::Allow (an
-// aggregate's group keys); elsewhere they fail with KRV_UNSUPPORTED.
+// aggregate's group keys, a join's keys); elsewhere they fail with
+// KRV_UNSUPPORTED.
 enum class HostRead { Copy, InPlace };
 enum class Var { Reject, Allow };
 DevBatch import_host(Runtime *rt, const ArrowArray *arr, const ArrowSchema *schema,

@@ -65,7 +65,7 @@ KeyFilterDev key_filter_dev(const KeyFilterImpl &f);
 class KeyDict;
 KeyDict *make_key_dict(Runtime *rt, const std::vector<DevCol> &meta);
 void key_dict_destroy(KeyDict *d);
-DBuf key_dict_encode(KeyDict *d, const DevBatch &b, const std::vector<int> &cols);
+DBuf key_dict_encode(KeyDict *d, const DevBatch &b, const std::vector<int> &cols, bool insert = true);
 std::vector<DevCol> key_dict_decode(KeyDict *d, const long long *codes, int64_t n);
 int64_t key_dict_size(const KeyDict *d);
 
@@ -102,6 +102,7 @@ class HashJoin {
 
     // Pending output batches for the bounded-output protocol.
     std::vector<DevBatch> pending;
+    ~HashJoin();
 
     // Device view of the built table (for fused pipelines).
     struct TableDev {
@@ -121,6 +122,24 @@ class HashJoin {
 
   private:
     void append_arena(const DevBatch &b);
+    // String or binary join keys: the key dictionary codes each key tuple as
+    // one int64 (the build side inserts, the probe side looks up, -1 for a
+    // key the build never saw); the table and kernels then join on that code.
+    // String columns leave the batches the table sees, so none may be
+    // projected into the output. spec_ then describes those batches; outer
+    // is the caller's spec.
+    struct Coded {
+        KeyDict *dict = nullptr;
+        krv_join_spec outer{};
+        bool probe_mapped = false;
+        ~Coded() {
+            if (dict) key_dict_destroy(dict);
+        }
+    };
+    std::unique_ptr<Coded> coded_;
+    bool decided_ = false;
+    void decide(const DevBatch &b);
+    DevBatch coded_batch(const DevBatch &b, bool build);
     // The column shape (types, names, nullability) of the probe output.
     void remember_shape(const DevBatch &out) {
         out_meta_.clear();

@@ -342,7 +342,7 @@ static DevBatch import_impl(Runtime *rt, const ArrowArray *arr, const ArrowSchem
         if (col.type.var()) {
             if (var != Var::Allow)
                 fail(KRV_UNSUPPORTED, "column '" + col.name + "': string and binary columns are taken as aggregate "
-                                      "group keys only");
+                                      "group keys and join keys only");
             if (c->n_buffers < 3) fail(KRV_INVALID_ARGUMENT, "column '" + col.name + "' has no value bytes buffer");
             import_var(rt, Device, c, off, b.rows, col);
         }

@@ -206,3 +206,68 @@ def test_dense_unique_build_keys(kb, rt, oracle, jt):
     want = oracle_pairs(oracle, jt, probe, build, 1, False)
     got = gpu_pairs(kb, rt, jt, probe, build, 1, False, build_batches=2)
     assert got == want
+
+
+def str_of(v):
+    """A string key per int key (one to one, some over 8 bytes), None kept."""
+    return None if v is None else ("key-%d-" % v) * (1 + abs(v) % 3)
+
+
+def rows_batch_str(rows, idname):
+    k1 = pa.array([str_of(r[0]) for r in rows], type=pa.string())
+    k2 = pa.array([r[1] for r in rows], type=pa.int32())
+    return batch(k1=k1, k2=k2, **{idname: pa.array(np.arange(len(rows), dtype=np.int64))})
+
+
+def gpu_pairs_str(kb, rt, jt, probe, build, nkeys, null_safe, build_batches=1):
+    """gpu_pairs with a string first key: the id columns are projected, the
+    string key is not (string columns never reach a join's output)."""
+    spec = kb.join_spec(jt, probe_keys=tuple(range(nkeys)), build_keys=tuple(range(nkeys)),
+                        null_safe=[null_safe] * nkeys, probe_out=[2], build_out=[2])
+    j = kb.HashJoin(rt, spec)
+    b = rows_batch_str(build, "bid")
+    step = max(1, -(-len(build) // build_batches))
+    if len(build) == 0:
+        j.build_push(b)
+    for s in range(0, len(build), step):
+        j.build_push(b.slice(s, step))
+    j.build_finish()
+    outs = j.probe(rows_batch_str(probe, "pid"))
+    outs += j.finish()
+    t = concat(outs)
+    if jt == "existence":
+        return collections.Counter(zip(t.column("pid").to_pylist(), [int(x) for x in t.column("exists").to_pylist()]))
+    return pairs_from_output(t)
+
+
+@pytest.mark.parametrize("jt", TYPES)
+def test_string_keys_match_the_oracle(kb, rt, oracle, jt):
+    """String join keys (one string key, or a string and an int32 key, `=`
+    and `<=>`), coded by the key dictionary: every join type gives the
+    oracle's pairs on the edge cases and on random keys with duplicates and
+    NULLs (the oracle joins the int keys the strings stand for)."""
+    rng = np.random.default_rng(16)
+    probe_r = [(int(x) if x >= 0 else None, int(y)) for x, y in zip(rng.integers(-20, 3000, 20000),
+                                                                     rng.integers(0, 3, 20000))]
+    build_r = [(int(x) if x >= 0 else None, int(y)) for x, y in zip(rng.integers(-20, 3000, 9000),
+                                                                     rng.integers(0, 3, 9000))]
+    inputs = [(EDGE_PROBE, EDGE_BUILD), (EDGE_PROBE, []), ([], EDGE_BUILD), (EDGE_PROBE, ALL_NULL),
+              (ALL_NULL, EDGE_BUILD), (probe_r, build_r)]
+    for nkeys in (1, 2):
+        for safe in (False, True):
+            if jt == "null_aware_anti" and (nkeys > 1 or safe):
+                continue
+            for probe, build in inputs:
+                want = oracle_pairs(oracle, jt, probe, build, nkeys, safe)
+                got = gpu_pairs_str(kb, rt, jt, probe, build, nkeys, safe, build_batches=3 if len(build) > 100 else 1)
+                assert got == want, (jt, nkeys, safe, len(probe), len(build))
+
+
+def test_string_key_types_must_agree(kb, rt):
+    spec = kb.join_spec("inner", probe_out=[1], build_out=[1])
+    j = kb.HashJoin(rt, spec)
+    j.build_push(batch(k=pa.array(["a", "b"]), bid=pa.array([0, 1])))
+    j.build_finish()
+    with pytest.raises(kb.KrvError) as e:
+        j.probe(batch(k=pa.array([1, 2]), pid=pa.array([0, 1])))
+    assert e.value.status in (kb.INVALID_ARGUMENT, kb.UNSUPPORTED)
