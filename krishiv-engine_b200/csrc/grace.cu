@@ -146,8 +146,10 @@ __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(PartArgs A, 
 // output count read or output copy per partition. The table lookups, chain
 // walks and output rounds are those of the unpartitioned join's probe
 // (pairs: newest build row first, left outer pads unmatched rows). Tiles of
-// 32 rows, each within one partition, are taken one per warp.
+// 64 rows, each within one partition, are taken one per warp, two rows per
+// lane with their first lookups in flight together.
 constexpr int kGProbeThreads = 256;
+constexpr int kGRows = 2;  // probe rows per lane
 constexpr int kGMaxOut = 16;
 constexpr uint32_t kGNone = 0xFFFFFFFFu;
 struct GPartDev {
@@ -157,7 +159,7 @@ struct GPartDev {
     const long long *bkey;
     const void *bcol[kMaxCols];  // the partition's build columns
     int64_t prow0, rows;         // its rows of the partitioned slice
-    int64_t tile0;               // its first tile (of 32 rows)
+    int64_t tile0;               // its first tile (of 32 x kGRows rows)
 };
 struct GOutCol {
     void *dst;
@@ -185,7 +187,7 @@ __global__ void __launch_bounds__(kGProbeThreads) grace_probe_kernel(const GPart
     const unsigned lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    // Tiles of 32 rows, one warp each: no block-wide synchronization.
+    // Tiles of 32 x kGRows rows, one warp each: no block-wide synchronization.
     for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < tiles; t += nwarps) {
         // the tile's partition: the last one whose first tile is at most t
         int p = 0;
@@ -197,76 +199,107 @@ __global__ void __launch_bounds__(kGProbeThreads) grace_probe_kernel(const GPart
         const GPartDev *sp = parts + p;
         const unsigned long long *slots = sp->slots;
         const uint64_t mask = sp->mask;
-        const int64_t local = (t - sp->tile0) * 32 + lane;
-        const bool live = local < sp->rows;
-        const int64_t prow = sp->prow0 + local;
-        uint32_t cur = kGNone;
-        if (live) {
-            const long long k = out.pkey[prow];
-            const uint64_t g = finalize(hash_word((uint64_t)k), seed);
-            const unsigned long long tag = g >> 32;
-            uint64_t pos = g & mask;
-            const long long *bkey = sp->bkey;
-            for (uint64_t probes = 0; probes <= mask; probes++) {
-                const unsigned long long sl = __ldg(slots + pos);
-                if (sl == 0) break;
-                if ((sl >> 32) == tag) {
-                    const uint32_t o = (uint32_t)(sl & 0xFFFFFFFFull) - 1u;
-                    if (__ldg(bkey + o) == k) {
-                        cur = o;
+        const long long *bkey = sp->bkey;
+        // kGRows rows per lane: their first slot loads, then their first
+        // candidates' key loads, are in flight together
+        bool live[kGRows];
+        int64_t prow[kGRows];
+        long long key[kGRows], bk[kGRows];
+        unsigned long long tag[kGRows], sl[kGRows];
+        uint64_t pos[kGRows];
+        uint32_t cand[kGRows], cur[kGRows];
+#pragma unroll
+        for (int u = 0; u < kGRows; u++) {
+            const int64_t local = (t - sp->tile0) * (32 * kGRows) + u * 32 + lane;
+            live[u] = local < sp->rows;
+            prow[u] = sp->prow0 + local;
+            key[u] = live[u] ? out.pkey[prow[u]] : 0;
+            const uint64_t g = finalize(hash_word((uint64_t)key[u]), seed);
+            tag[u] = g >> 32;
+            pos[u] = g & mask;
+        }
+#pragma unroll
+        for (int u = 0; u < kGRows; u++) sl[u] = live[u] ? __ldg(slots + pos[u]) : 0ull;
+#pragma unroll
+        for (int u = 0; u < kGRows; u++) {
+            cand[u] = (sl[u] != 0 && (sl[u] >> 32) == tag[u]) ? (uint32_t)(sl[u] & 0xFFFFFFFFull) - 1u : kGNone;
+            bk[u] = cand[u] != kGNone ? __ldg(bkey + cand[u]) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kGRows; u++) {
+            cur[u] = kGNone;
+            if (!live[u] || sl[u] == 0) continue;  // an empty first slot: no match
+            if (cand[u] != kGNone && bk[u] == key[u]) {
+                cur[u] = cand[u];
+                continue;
+            }
+            // the rest of the probe sequence, a slot at a time
+            uint64_t q = (pos[u] + 1) & mask;
+            for (uint64_t probes = 1; probes <= mask; probes++) {
+                const unsigned long long s2 = __ldg(slots + q);
+                if (s2 == 0) break;
+                if ((s2 >> 32) == tag[u]) {
+                    const uint32_t o = (uint32_t)(s2 & 0xFFFFFFFFull) - 1u;
+                    if (__ldg(bkey + o) == key[u]) {
+                        cur[u] = o;
                         break;
                     }
                 }
-                pos = (pos + 1) & mask;
+                q = (q + 1) & mask;
             }
         }
         const uint32_t *next = sp->next;
-        bool padrow = live && cur == kGNone && pad;
-        unsigned chain = 0;
-        while (__any_sync(0xFFFFFFFFu, cur != kGNone || padrow)) {
-            const bool want = cur != kGNone || padrow;
-            const unsigned ballot = __ballot_sync(0xFFFFFFFFu, want);
-            unsigned long long first = 0;
-            if (lane == 0) first = atomicAdd(count, (unsigned long long)__popc(ballot));
-            first = __shfl_sync(0xFFFFFFFFu, first, 0);
-            const unsigned rank = __popc(ballot & below);
-            const unsigned long long at = first + rank;
-            for (int c = 0; c < out.n; c++) {
-                const GOutCol C = out.c[c];
-                bool v = false;
-                if (want && at < cap) {
-                    if (C.side == 0) {
-                        gcopy(C.dst, out.pcol[C.col], at, prow, C.width);
-                        v = true;
-                    } else if (cur != kGNone) {
-                        gcopy(C.dst, sp->bcol[C.col], at, cur, C.width);
-                        v = true;
-                    } else if (C.width == 8) {
-                        static_cast<unsigned long long *>(C.dst)[at] = 0ull;
-                    } else {
-                        static_cast<uint32_t *>(C.dst)[at] = 0u;
+#pragma unroll
+        for (int u = 0; u < kGRows; u++) {
+            const int64_t pr = prow[u];
+            uint32_t c0 = cur[u];
+            bool padrow = live[u] && c0 == kGNone && pad;
+            unsigned chain = 0;
+            while (__any_sync(0xFFFFFFFFu, c0 != kGNone || padrow)) {
+                const bool want = c0 != kGNone || padrow;
+                const unsigned ballot = __ballot_sync(0xFFFFFFFFu, want);
+                unsigned long long first = 0;
+                if (lane == 0) first = atomicAdd(count, (unsigned long long)__popc(ballot));
+                first = __shfl_sync(0xFFFFFFFFu, first, 0);
+                const unsigned rank = __popc(ballot & below);
+                const unsigned long long at = first + rank;
+                for (int c = 0; c < out.n; c++) {
+                    const GOutCol C = out.c[c];
+                    bool v = false;
+                    if (want && at < cap) {
+                        if (C.side == 0) {
+                            gcopy(C.dst, out.pcol[C.col], at, pr, C.width);
+                            v = true;
+                        } else if (c0 != kGNone) {
+                            gcopy(C.dst, sp->bcol[C.col], at, c0, C.width);
+                            v = true;
+                        } else if (C.width == 8) {
+                            static_cast<unsigned long long *>(C.dst)[at] = 0ull;
+                        } else {
+                            static_cast<uint32_t *>(C.dst)[at] = 0u;
+                        }
+                    }
+                    if (C.dst_valid) {
+                        // this round's bits in output order, OR-ed in with at most two atomics
+                        const unsigned m = __reduce_or_sync(0xFFFFFFFFu, v ? (1u << rank) : 0u);
+                        if (lane == 0 && m) {
+                            const unsigned long long w = first >> 5;
+                            const unsigned sh = (unsigned)(first & 31);
+                            const unsigned long long capw = (cap + 31) >> 5;
+                            if (w < capw) atomicOr(C.dst_valid + w, m << sh);
+                            if (sh && w + 1 < capw && (m >> (32 - sh))) atomicOr(C.dst_valid + w + 1, m >> (32 - sh));
+                        }
                     }
                 }
-                if (C.dst_valid) {
-                    // this round's bits in output order, OR-ed in with at most two atomics
-                    const unsigned m = __reduce_or_sync(0xFFFFFFFFu, v ? (1u << rank) : 0u);
-                    if (lane == 0 && m) {
-                        const unsigned long long w = first >> 5;
-                        const unsigned sh = (unsigned)(first & 31);
-                        const unsigned long long capw = (cap + 31) >> 5;
-                        if (w < capw) atomicOr(C.dst_valid + w, m << sh);
-                        if (sh && w + 1 < capw && (m >> (32 - sh))) atomicOr(C.dst_valid + w + 1, m >> (32 - sh));
-                    }
+                if (c0 != kGNone) {
+                    chain++;
+                    c0 = next[c0];
+                } else {
+                    padrow = false;
                 }
             }
-            if (cur != kGNone) {
-                chain++;
-                cur = next[cur];
-            } else {
-                padrow = false;
-            }
+            if (single_match && chain > 1) atomicOr(status, ST_TOO_MANY);
         }
-        if (single_match && chain > 1) atomicOr(status, ST_TOO_MANY);
     }
 }
 
@@ -504,7 +537,7 @@ class GraceJoin {
             d.prow0 = (static_cast<const uint8_t *>(s.batch.cols[key].data) - static_cast<const uint8_t *>(od.pcol[key])) / 8;
             d.rows = s.rows;
             d.tile0 = tiles;
-            tiles += ceil_div(s.rows, (int64_t)32);
+            tiles += ceil_div(s.rows, (int64_t)(32 * kGRows));
             rows += s.rows;
             hp.push_back(d);
         }
