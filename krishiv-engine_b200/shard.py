@@ -4,7 +4,15 @@ fact rows a rank owns and how the ranks' partial results combine.
 The star query shards by fact rows. Dimensions are replicated (every rank
 builds the same tables and filters), each rank probes its own rows, and the
 partial grouped sums merge once at the end: a gather of a few groups per
-rank, no exchange on the data path."""
+rank, no exchange on the data path.
+
+A grouped aggregate with many groups has a real exchange step: each rank
+aggregates its own rows into partial states (krv_agg with
+KRV_AGG_OUTPUT_PARTIAL), `exchange` sends every state row to the rank that
+owns its key (`key_owner`) with one all-to-all per column (NCCL over NVLink
+for device tensors, gloo for host tensors), and each rank merges the states
+of the keys it owns (KRV_AGG_INPUT_STATE): every group ends on exactly one
+rank."""
 from __future__ import annotations
 
 import math
@@ -58,3 +66,46 @@ def max_over_ranks(dist, value: float, device="cpu") -> float:
     t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+_MASK32 = (1 << 32) - 1
+
+
+def _shr(z, s: int):
+    """Logical right shift of an int64 tensor (its bits as unsigned)."""
+    return (z >> s) & ((1 << (64 - s)) - 1)
+
+
+def key_owner(keys, world: int):
+    """The rank owning each int64 key's group: the top 32 bits of a
+    SplitMix64 finalisation of the key, scaled to `world` (any mixing
+    function would do: owners only decide where a group is merged, never its
+    result). `keys` is an int64 torch tensor on any device."""
+    import torch
+    z = keys.to(torch.int64)
+    z = (z ^ _shr(z, 30)) * -4658895280553007687   # 0xbf58476d1ce4e5b9
+    z = (z ^ _shr(z, 27)) * -7723592293110705685   # 0x94d049bb133111eb
+    z = z ^ _shr(z, 31)
+    return (_shr(z, 32) * world) >> 32
+
+
+def exchange(dist, columns, owner):
+    """Sends row i of every column (equal-length torch tensors, one device)
+    to rank owner[i]; returns this rank's received rows of every column,
+    grouped by sending rank in rank order. One all_to_all_single for the
+    counts, one per column."""
+    import torch
+    world = dist.get_world_size()
+    owner = owner.to(torch.int64)
+    order = torch.argsort(owner, stable=True)
+    send = torch.bincount(owner, minlength=world).to(torch.int64)
+    recv = torch.empty_like(send)
+    dist.all_to_all_single(recv, send)
+    send_l, recv_l = send.tolist(), recv.tolist()
+    out = []
+    for c in columns:
+        src = c[order].contiguous()
+        dst = torch.empty((sum(recv_l),) + tuple(c.shape[1:]), dtype=c.dtype, device=c.device)
+        dist.all_to_all_single(dst, src, recv_l, send_l)
+        out.append(dst)
+    return out

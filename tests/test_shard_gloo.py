@@ -89,3 +89,104 @@ def test_two_gloo_ranks_match_one(oracle):
         for g, (s, n) in want.items():
             assert merged[g][1] == n
             assert rel_err(merged[g][0], s) <= 1e-12
+
+
+def _agg_rank(rank, world, port, queue):
+    """One rank of a two-phase grouped aggregate: partial states of its own
+    rows (the oracle stands in for the device's partial aggregate), the
+    exchange by key owner, the merge of the states of the keys it owns."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import oracle as O
+    shard = importlib.import_module("krishiv-engine_b200.shard")
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        keys, x, y, yv = _agg_rows(rank)
+        cols = [{"values": x, "type": O.T_I64}, {"values": y, "valid": yv.astype(np.uint8), "type": O.T_F64}]
+        wk, _, wr = O.hash_aggregate(keys, None, cols, [(O.COUNT_STAR, 0), (O.SUM, 0), (O.MIN, 0), (O.MAX, 0),
+                                                        (O.SUM, 1), (O.COUNT, 1)])
+        state = [torch.tensor(wk), torch.tensor(wr[0]["i64"]), torch.tensor(wr[1]["i64"]), torch.tensor(wr[2]["i64"]),
+                 torch.tensor(wr[3]["i64"]), torch.tensor(wr[4]["f64"]),
+                 torch.tensor(wr[4]["valid"].astype(np.uint8)), torch.tensor(wr[5]["i64"])]
+        owner = shard.key_owner(state[0], world)
+        got = [t.numpy() for t in shard.exchange(dist, state, owner)]
+        mine = bool((shard.key_owner(torch.tensor(got[0]), world) == rank).all())
+        mcols = [{"values": got[1], "type": O.T_I64}, {"values": got[2], "type": O.T_I64},
+                 {"values": got[3], "type": O.T_I64}, {"values": got[4], "type": O.T_I64},
+                 {"values": got[5], "valid": got[6], "type": O.T_F64}, {"values": got[7], "type": O.T_I64}]
+        mk, _, mr = O.hash_aggregate(got[0], None, mcols, [(O.SUM, 0), (O.SUM, 1), (O.MIN, 2), (O.MAX, 3),
+                                                            (O.SUM, 4), (O.SUM, 5)])
+        merged = {}
+        for j, k in enumerate(mk.tolist()):
+            sy = float(mr[4]["f64"][j]) if mr[4]["valid"][j] else None
+            merged[k] = (int(mr[0]["i64"][j]), int(mr[1]["i64"][j]), int(mr[2]["i64"][j]), int(mr[3]["i64"][j]), sy,
+                         int(mr[5]["i64"][j]))
+        dist.barrier()
+        queue.put((rank, merged, mine))
+    finally:
+        dist.destroy_process_group()
+
+
+def _agg_rows(rank):
+    import numpy as np
+    rng = np.random.default_rng(100 + rank)
+    n = 40_000
+    keys = rng.integers(-3000, 3000, n).astype(np.int64)
+    x = rng.integers(-10**12, 10**12, n).astype(np.int64)
+    y = rng.random(n) * 200 - 100
+    yv = rng.random(n) > 0.05
+    return keys, x, y, yv
+
+
+def test_two_phase_aggregate_exchange_on_two_gloo_ranks(oracle):
+    """Partial states exchanged by key owner (shard.key_owner / exchange):
+    every group is merged on exactly one rank, the rank that owns it, and the
+    merged groups equal the one-phase aggregate of both ranks' rows."""
+    import numpy as np
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_agg_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    # the results are read before the joins: a rank blocks on its put until
+    # its (large) result is taken from the pipe
+    got = sorted([q.get(timeout=240) for _ in procs], key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    assert all(mine for _, _, mine in got)
+    assert not set(got[0][1]) & set(got[1][1])
+    merged = {**got[0][1], **got[1][1]}
+    rows = [_agg_rows(r) for r in range(2)]
+    keys = np.concatenate([r[0] for r in rows])
+    cols = [{"values": np.concatenate([r[1] for r in rows]), "type": oracle.T_I64},
+            {"values": np.concatenate([r[2] for r in rows]), "valid": np.concatenate([r[3] for r in rows]).astype(np.uint8),
+             "type": oracle.T_F64}]
+    wk, _, wr = oracle.hash_aggregate(keys, None, cols, [(oracle.COUNT_STAR, 0), (oracle.SUM, 0), (oracle.MIN, 0),
+                                                        (oracle.MAX, 0), (oracle.SUM, 1), (oracle.COUNT, 1)])
+    assert len(merged) == len(wk)
+    for j, k in enumerate(wk.tolist()):
+        m = merged[k]
+        assert m[:4] == (int(wr[0]["i64"][j]), int(wr[1]["i64"][j]), int(wr[2]["i64"][j]), int(wr[3]["i64"][j]))
+        assert m[5] == int(wr[5]["i64"][j])
+        if wr[4]["valid"][j]:
+            assert rel_err(m[4], float(wr[4]["f64"][j])) <= 1e-12
+        else:
+            assert m[4] is None
+
+
+def test_key_owner_is_balanced_and_stable():
+    import torch
+    shard = importlib.import_module("krishiv-engine_b200.shard")
+    k = torch.arange(-50_000, 50_000, dtype=torch.int64)
+    for world in (2, 3, 8):
+        o = shard.key_owner(k, world)
+        assert int(o.min()) == 0 and int(o.max()) == world - 1
+        counts = torch.bincount(o, minlength=world).tolist()
+        assert max(counts) - min(counts) < 0.05 * len(k) / world * world
+        assert torch.equal(o, shard.key_owner(k.clone(), world))
