@@ -58,3 +58,49 @@ def test_no_device_is_an_error_status(kb):
 
 def test_version(kb):
     assert b"sm_100a" in kb.lib().krv_version()
+
+
+# Each C struct of include/krv_gpu.h and its ctypes mirror in the binding.
+STRUCTS = {"krv_join_spec": "JoinSpec", "krv_join_counters": "JoinCounters", "krv_grace_options": "GraceOptions",
+           "krv_agg_expr": "AggExpr", "krv_agg_spec": "AggSpec", "krv_key_filter_options": "KeyFilterOptions",
+           "krv_key_filter_info": "KeyFilterInfo", "krv_star_spec": "StarSpec", "krv_star_counters": "StarCounters",
+           "krv_gen_spec": "GenSpec", "krv_server_options": "ServerOptions", "krv_server_stats": "ServerStats"}
+
+
+def test_header_is_c_and_structs_match_the_binding(kb, tmp_path):
+    """The header compiles as C11, and every struct's size and every field's
+    offset seen by a C compiler equal the Python binding's ctypes layout."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "krv_gpu.h"', "int main(void) {"]
+    for cname, pyname in STRUCTS.items():
+        cls = getattr(kb, pyname)
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for f in cls._fields_:
+            lines.append(f'printf("{cname}.{f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True, capture_output=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                           text=True).stdout.splitlines())
+    for cname, pyname in STRUCTS.items():
+        cls = getattr(kb, pyname)
+        assert int(got[cname]) == C.sizeof(cls), cname
+        for f in cls._fields_:
+            assert int(got[f"{cname}.{f[0]}"]) == getattr(cls, f[0]).offset, (cname, f[0])
+
+
+def test_state_aggregate_specs(kb):
+    s = kb.agg_spec([0, 1], [("sum", "state", 2, 3), ("avg", "state", 4, 5, (15, 2, 128)), ("count_star", "state", 6),
+                             ("min", 7)], partial=True)
+    assert s.n_group_by == 2 and s.output == kb.AGG_OUTPUT_PARTIAL
+    a = s.aggregates
+    assert (a[0].input, a[0].column, a[0].column2) == (kb.AGG_INPUT_STATE, 2, 3)
+    assert (a[1].arg_precision, a[1].arg_scale, a[1].arg_bits) == (15, 2, 128)
+    assert (a[2].input, a[2].column, a[2].column2) == (kb.AGG_INPUT_STATE, 6, -1)
+    assert (a[3].input, a[3].column, a[3].column2) == (kb.AGG_INPUT_RAW, 7, -1)
