@@ -121,6 +121,9 @@ __device__ __forceinline__ void update_record(const AggPlanDev &P, uint8_t *r, i
             if (C.flags & F_SUM)
                 atomic_add_i128(reinterpret_cast<unsigned long long *>(r + C.off_sum),
                                 reinterpret_cast<long long *>(r + C.off_sum + 8), p[0], p[1]);
+            // MIN/MAX only for precision <= 18: the value is its low word
+            if (C.flags & F_MIN) atomicMin(reinterpret_cast<long long *>(r + C.off_min), p[0]);
+            if (C.flags & F_MAX) atomicMax(reinterpret_cast<long long *>(r + C.off_max), p[0]);
         } else {  // I64, Dec64
             const long long v = static_cast<const long long *>(C.data)[i];
             if (C.flags & F_SUM)
@@ -180,6 +183,14 @@ __device__ __forceinline__ void update_record_plain(const AggPlanDev &P, uint8_t
                 *lo = old + (unsigned long long)p[0];
                 *hi += p[1] + (long long)(*lo < old);
             }
+            if (C.flags & F_MIN) {
+                long long *m = reinterpret_cast<long long *>(r + C.off_min);
+                *m = p[0] < *m ? p[0] : *m;
+            }
+            if (C.flags & F_MAX) {
+                long long *m = reinterpret_cast<long long *>(r + C.off_max);
+                *m = p[0] > *m ? p[0] : *m;
+            }
         } else {  // I64, Dec64
             const long long v = static_cast<const long long *>(C.data)[i];
             if (C.flags & F_SUM) {
@@ -235,12 +246,10 @@ __device__ __forceinline__ void merge_record(const AggPlanDev &P, uint8_t *dst, 
                                 reinterpret_cast<long long *>(dst + C.off_sum + 8),
                                 *reinterpret_cast<const long long *>(src + C.off_sum),
                                 *reinterpret_cast<const long long *>(src + C.off_sum + 8));
-            if (C.type != (int)Type::Dec128) {
-                if (C.flags & F_MIN)
-                    atomicMin(reinterpret_cast<long long *>(dst + C.off_min), *reinterpret_cast<const long long *>(src + C.off_min));
-                if (C.flags & F_MAX)
-                    atomicMax(reinterpret_cast<long long *>(dst + C.off_max), *reinterpret_cast<const long long *>(src + C.off_max));
-            }
+            if (C.flags & F_MIN)
+                atomicMin(reinterpret_cast<long long *>(dst + C.off_min), *reinterpret_cast<const long long *>(src + C.off_min));
+            if (C.flags & F_MAX)
+                atomicMax(reinterpret_cast<long long *>(dst + C.off_max), *reinterpret_cast<const long long *>(src + C.off_max));
         }
     }
 }
@@ -679,7 +688,11 @@ __global__ void __launch_bounds__(256) finalize_kernel(AggPlanDev P, OutPlanDev 
                             else if (C.type == (int)Type::F64)
                                 static_cast<double *>(X.dst)[r] =
                                     f64_from_order_key(*reinterpret_cast<const unsigned long long *>(rec + off));
-                            else static_cast<long long *>(X.dst)[r] = *reinterpret_cast<const long long *>(rec + off);
+                            else if (X.otype == (int)Type::Dec128) {
+                                const long long v = *reinterpret_cast<const long long *>(rec + off);
+                                static_cast<long long *>(X.dst)[2 * r] = v;
+                                static_cast<long long *>(X.dst)[2 * r + 1] = v < 0 ? -1 : 0;
+                            } else static_cast<long long *>(X.dst)[r] = *reinterpret_cast<const long long *>(rec + off);
                             valid = true;
                         } else if (C.type == (int)Type::F64) {
                             const double hi = *reinterpret_cast<const double *>(rec + C.off_sum);
@@ -911,8 +924,8 @@ void HashAggregate::plan(const DevBatch &b) {
         if (!state) {
             if (x.function == KRV_AGG_COUNT_STAR) continue;
             const DType t = check_col(x.column);
-            if (t.id == Type::Dec128 && (x.function == KRV_AGG_MIN || x.function == KRV_AGG_MAX))
-                fail(KRV_UNSUPPORTED, "MIN/MAX of decimal128 on the GPU aggregate");
+            if (t.id == Type::Dec128 && t.precision > 18 && (x.function == KRV_AGG_MIN || x.function == KRV_AGG_MAX))
+                fail(KRV_UNSUPPORTED, "MIN/MAX of decimals of precision 19 to 38 on the GPU aggregate");
             int32_t f = 0;
             if (x.function == KRV_AGG_SUM || x.function == KRV_AGG_AVG) f = F_SUM;
             if (x.function == KRV_AGG_MIN) f = F_MIN;
@@ -947,7 +960,8 @@ void HashAggregate::plan(const DevBatch &b) {
             break;
         case KRV_AGG_MIN:
         case KRV_AGG_MAX:
-            if (t.id == Type::Dec128) fail(KRV_UNSUPPORTED, "MIN/MAX of decimal128 on the GPU aggregate");
+            if (t.id == Type::Dec128 && t.precision > 18)
+                fail(KRV_UNSUPPORTED, "MIN/MAX of decimals of precision 19 to 38 on the GPU aggregate");
             expr_col_[e] = plan_col(x.column, x.function == KRV_AGG_MIN ? F_MIN : F_MAX);
             break;
         }

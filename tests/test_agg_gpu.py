@@ -3,6 +3,7 @@ answers, through the C ABI. Integer and decimal results are bit-exact;
 float64 SUM/AVG are within 1e-12 relative of the oracle's compensated sum;
 MIN/MAX and COUNT are exact."""
 import os
+from decimal import Decimal
 
 import numpy as np
 import pyarrow as pa
@@ -190,3 +191,49 @@ def test_device_path(kb, rt, oracle):
                                        [(oracle.SUM, 0), (oracle.MIN, 0), (oracle.COUNT_STAR, 0)])
     want = dict(zip(keys.tolist(), r[0]["i64"].tolist()))
     assert dict(zip(got_k.tolist(), got_s.tolist())) == want
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_decimal128_columns(kb, rt, oracle, mode):
+    """decimal128(15,2) values (the carrier Spark-written Arrow files use for
+    decimal(15,2)), negative and NULL: SUM, COUNT, MIN, MAX and AVG exact
+    against the oracle; MIN/MAX keep the input type. MIN/MAX of a
+    decimal(20,2) column are not taken (UNSUPPORTED)."""
+    rng = np.random.default_rng(41)
+    n = 200_000
+    key = rng.integers(0, 3000, n, dtype=np.int64)
+    v = rng.integers(-10**13, 10**13, n, dtype=np.int64)
+    valid = rng.random(n) > 0.03
+    words = np.stack([v, np.where(v < 0, -1, 0)], 1).astype(np.int64).reshape(-1)
+    dec = pa.Array.from_buffers(pa.decimal128(15, 2), n, [pa.py_buffer(np.packbits(valid, bitorder="little").tobytes()),
+                                                         pa.py_buffer(words.tobytes())])
+    b = batch(k=pa.array(key), d=dec)
+    aggs = [(f, 1) for f in FUNCS]
+    out = run(kb, rt, b, 0, aggs, mode, batches=3)
+    assert [out.schema.field(i).type for i in range(1, 6)] == [pa.decimal128(25, 2), pa.int64(), pa.decimal128(15, 2),
+                                                              pa.decimal128(15, 2), pa.decimal128(19, 6)]
+    cols = [{"values": words, "valid": valid.astype(np.uint8), "type": oracle.T_DEC128, "precision": 15, "scale": 2}]
+    F = {"sum": oracle.SUM, "count": oracle.COUNT, "min": oracle.MIN, "max": oracle.MAX, "avg": oracle.AVG}
+    keys, _, res = oracle.hash_aggregate(key, None, cols, [(F[f], 0) for f, _ in aggs])
+    order = {int(k): i for i, k in enumerate(keys)}
+    got = {k: r for k, *r in zip(*[c.to_pylist() for c in out.columns])}
+    assert sorted(got) == sorted(order)
+    for k, vals in got.items():
+        gi = order[k]
+        for e, (f, _) in enumerate(aggs):
+            r = res[e]
+            if not r["valid"][gi]:
+                assert vals[e] is None
+                continue
+            if f == "count":
+                assert vals[e] == r["i64"][gi]
+            elif f in ("sum", "avg"):
+                scale = out.schema.field(1 + e).type.scale
+                assert int(vals[e].scaleb(scale)) == int(r["lo"][gi]) + (int(r["hi"][gi]) << 64), (f, k)
+            else:
+                assert int(vals[e].scaleb(2)) == int(r["i64"][gi]), (f, k)
+    wide = batch(k=pa.array([1, 2]), d=pa.array([Decimal(1), Decimal(2)], pa.decimal128(20, 2)))
+    a = kb.HashAggregate(rt, kb.agg_spec(0, [("min", 1)]))
+    with pytest.raises(kb.KrvError) as e:
+        a.push(wide)
+    assert e.value.status == kb.UNSUPPORTED
