@@ -196,7 +196,8 @@ krv_status krv_join_create_partitioned(krv_runtime *rt, const krv_join_spec *spe
 int64_t krv_join_spilled_partitions(const krv_join *j);
 
 /* ---- grouped hash aggregate ---------------------------------------------- */
-/* AggregateFunction (aggregate/mod.rs:134), the core five */
+/* AggregateFunction (aggregate/mod.rs:134), the core five. MIN/MAX take
+ * decimals of precision up to 18 (decimal64 or decimal128 carrier). */
 #define KRV_AGG_COUNT_STAR 0
 #define KRV_AGG_COUNT 1
 #define KRV_AGG_SUM 2
