@@ -104,3 +104,37 @@ def test_state_aggregate_specs(kb):
     assert (a[1].arg_precision, a[1].arg_scale, a[1].arg_bits) == (15, 2, 128)
     assert (a[2].input, a[2].column, a[2].column2) == (kb.AGG_INPUT_STATE, 6, -1)
     assert (a[3].input, a[3].column, a[3].column2) == (kb.AGG_INPUT_RAW, 7, -1)
+
+
+def test_a_c_program_links_and_calls_the_library(kb, tmp_path):
+    """A plain C caller (no Python, no PyTorch) links libkrv_gpu.so through the
+    header, reads the version and gets a status, not a crash, from a call
+    that needs a device (here: none, or the box's first GPU)."""
+    import shutil
+    import subprocess
+    import torch
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "caller.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include "krv_gpu.h"
+int main(void) {
+    krv_runtime *rt = NULL;
+    krv_status st = krv_runtime_create(0, 0, NULL, &rt);
+    printf("%s\n%d\n", krv_version(), (int)st);
+    if (st == KRV_OK) krv_runtime_destroy(rt);
+    else printf("%s\n", krv_last_error());
+    return 0;
+}
+''')
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(kb.LIB_PATH)
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", libdir, "-lkrv_gpu", "-Wl,-rpath," + libdir], check=True, capture_output=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines()
+    assert "sm_100a" in out[0]
+    if torch.cuda.is_available():
+        assert int(out[1]) == kb.OK
+    else:
+        assert int(out[1]) in (kb.CUDA_ERROR, kb.INVALID_ARGUMENT) and out[2]
