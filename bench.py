@@ -532,7 +532,7 @@ def cpu_grace(scale):
 
 
 def run_grace(args, kb, W, rt, rank, world, pg, device):
-    """Survey config 4: left outer join, 500M build rows x 2B probe rows, under
+    """The partitioned join workload: left outer join, 500M build rows x 2B probe rows, under
     a 24 GB device budget (a runtime whose allocations are capped), inputs
     resident in HBM, every output batch consumed by a checksum."""
     import torch

@@ -122,4 +122,3 @@ if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     main(ref)
     extra(ref)
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
