@@ -638,6 +638,35 @@ def agg_spec(group_by, aggregates: Sequence, ansi=True, mode=MODE_AUTO, expected
     return s
 
 
+def merging(aggregates: Sequence, first: int, arg_types: Sequence) -> list:
+    """The second-phase aggregates over the state columns that a partial
+    aggregate (agg_spec(..., partial=True)) writes for `aggregates`, those
+    columns starting at column `first` (after the group keys), in the
+    reference's order (AggregateExpr::merging, aggregate/mod.rs:561-569, over
+    AggregateExpr::state_fields, :747-800): COUNT one column, SUM one (two
+    for a decimal argument: sum, nonempty), AVG two (sum, count), MIN/MAX
+    one. `arg_types` gives each aggregate's raw argument type (pyarrow;
+    None for COUNT(*)): decimals decide SUM's state and AVG's result type."""
+    import pyarrow as pa
+    out, at = [], first
+    for a, t in zip(aggregates, arg_types):
+        f = a[0]
+        dec = t is not None and pa.types.is_decimal(t)
+        if f in ("count", "count_star", "min", "max"):
+            out.append((f, "state", at))
+            at += 1
+        elif f == "sum":
+            out.append((f, "state", at, at + 1) if dec else (f, "state", at))
+            at += 2 if dec else 1
+        elif f == "avg":
+            raw = (t.precision, t.scale, t.bit_width) if dec else None
+            out.append((f, "state", at, at + 1, raw) if raw else (f, "state", at, at + 1))
+            at += 2
+        else:
+            raise ValueError("unknown aggregate function %r" % (f,))
+    return out
+
+
 class HashAggregate:
     """The grouped hash aggregate (HashAggregate, crates/krishiv-exec/src/aggregate/sink.rs:181)."""
 

@@ -138,3 +138,22 @@ int main(void) {
         assert int(out[1]) == kb.OK
     else:
         assert int(out[1]) in (kb.CUDA_ERROR, kb.INVALID_ARGUMENT) and out[2]
+
+
+def test_merging_specs(kb):
+    """merging() lays out the second phase over the partial states as the
+    reference's AggregateExpr::merging does: TPC-H Q1's aggregates after two
+    group keys, and integer / float / decimal mixes."""
+    import pyarrow as pa
+    d15 = pa.decimal128(15, 2)
+    q1 = [("sum", 2), ("sum", 3), ("sum", 4), ("sum", 5), ("avg", 2), ("avg", 3), ("avg", 6), ("count_star", 0)]
+    types = [d15, d15, pa.decimal128(32, 4), pa.decimal128(38, 6), d15, d15, d15, None]
+    assert kb.merging(q1, 2, types) == [
+        ("sum", "state", 2, 3), ("sum", "state", 4, 5), ("sum", "state", 6, 7), ("sum", "state", 8, 9),
+        ("avg", "state", 10, 11, (15, 2, 128)), ("avg", "state", 12, 13, (15, 2, 128)),
+        ("avg", "state", 14, 15, (15, 2, 128)), ("count_star", "state", 16)]
+    mix = [("sum", 1), ("min", 1), ("avg", 2), ("count", 3), ("max", 3)]
+    assert kb.merging(mix, 1, [pa.int64(), pa.int64(), pa.float64(), pa.int32(), pa.int32()]) == [
+        ("sum", "state", 1), ("min", "state", 2), ("avg", "state", 3, 4), ("count", "state", 5), ("max", "state", 6)]
+    s = kb.agg_spec([0, 1], kb.merging(q1, 2, types))
+    assert s.aggregates[4].arg_bits == 128 and s.aggregates[0].column2 == 3
