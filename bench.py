@@ -138,22 +138,86 @@ def _shard():
 
 
 # ---- the CPU baseline (the oracle's multi-threaded restatement) ---------------------------
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    return O
+
+
+def host_bytes_available():
+    try:
+        import psutil
+        return int(psutil.virtual_memory().available)
+    except Exception:
+        return 0
+
+
+def cpu_star_inputs(scale, fact_scale, threads):
+    """The star query's whole input on the host, generated by the oracle's
+    counter-based generators (the device generators' functions) on `threads`
+    host threads; None when the host has too little free memory for it."""
+    O = _oracle()
+    W = importlib.import_module("krishiv-engine_b200.workloads")
+    nf = int(300_000_000 * fact_scale)
+    need = 32 * nf + 16 * int(20_000_000 * scale)
+    if host_bytes_available() < 2 * need:
+        return None
+    fact, dims = O.star_inputs_mt(scale, W.STAR_SEED, threads, fact_rows=nf, pred=W.PRED_VALUE)
+    return fact, dims
+
+
+def cpu_star_full(fact, dims, threads, runs):
+    """The CPU oracle's star query (dimension builds with their key filters,
+    the fact probe split over `threads` host threads, compensated group sums)
+    over every fact row given, `runs` times: (median whole-query seconds,
+    the last answer)."""
+    O = _oracle()
+    W = importlib.import_module("krishiv-engine_b200.workloads")
+    times, ans = [], None
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        ans = O.star_query(fact, dims, pred=W.PRED_VALUE, threads=threads)
+        times.append(time.perf_counter() - t0)
+    return statistics.median(times), ans
+
+
 def cpu_star(scale, sample_rows, threads, seed=None):
     """Times the star query on the host cores with the CPU oracle on the first
     `sample_rows` fact rows (dimensions at full size); returns the whole-query
-    rate extrapolated to the full fact table (build time + full probe)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+    rate extrapolated to the full fact table (build time + full probe). Used
+    only when the host cannot hold the whole fact table."""
+    O = _oracle()
     W = importlib.import_module("krishiv-engine_b200.workloads")
     seed = W.STAR_SEED if seed is None else seed
     nf = int(300_000_000 * scale)
     s = min(sample_rows, nf)
-    fact, dims = O.star_inputs(scale, seed, fact_rows=s, pred=W.PRED_VALUE)
+    fact, dims = O.star_inputs_mt(scale, seed, threads, fact_rows=s, pred=W.PRED_VALUE)
     groups, passed, joined, tb, tp = O.star_query(fact, dims, pred=W.PRED_VALUE, threads=threads)
     probe_rate = s / tp
     whole = tb + nf / probe_rate
     return {"value": nf / whole / 1e6, "build_s": tb, "probe_rows_per_s": probe_rate, "sample_rows": s,
             "threads": threads, "groups": len(groups), "joined": joined}
+
+
+def star_parity(gpu_groups, gpu_counters, oracle_answer, rows, tol=1e-12):
+    """The GPU's answer against the oracle's on the same rows: the rows passing
+    both key filters and the joined rows exactly, the same groups, and each
+    group's sum within `tol` relative of the oracle's compensated sum."""
+    groups, passed, joined, _, _ = oracle_answer
+    worst = 0.0
+    for k, (want, _) in groups.items():
+        got = gpu_groups.get(k)
+        if got is None:
+            worst = float("inf")
+            break
+        worst = max(worst, abs(got - want) / max(abs(want), 1e-300))
+    same_groups = sorted(groups) == sorted(gpu_groups)
+    ok = (passed == gpu_counters["passed_filters"] and joined == gpu_counters["joined_rows"] and same_groups
+          and worst <= tol)
+    return {"checker": "CPU oracle star query (the reference's algorithms restated in C) on the same rows",
+            "fact_rows": rows, "passed_filters": [gpu_counters["passed_filters"], passed],
+            "joined_rows": [gpu_counters["joined_rows"], joined], "groups": [len(gpu_groups), len(groups)],
+            "max_rel_err": worst, "tolerance": tol, "ok": bool(ok)}
 
 
 def cpu_join(scale, threads=1):
@@ -242,6 +306,8 @@ def run_star(args, kb, W, rt, rank, world, pg, device):
         if kernel_events is not None:
             kernel_events.extend(ev[2].elapsed_time(ev[3]) for ev in kev)
             if phases is not None:
+                phases["_steps"] = [ev[0].elapsed_time(ev[4]) for ev in kev]
+            if phases is not None:
                 for name, i in (("reset", 0), ("build", 1), ("probe", 2), ("result", 3)):
                     phases[name] = statistics.median(ev[i].elapsed_time(ev[i + 1]) for ev in kev)
         return ms, rt.launches - launches0
@@ -252,6 +318,11 @@ def run_star(args, kb, W, rt, rank, world, pg, device):
     with Clocks(device) as clk:
         ms, launches = timed(fused, args.steps, args.warmup, kernel_ms, phases)
     ms_max = max_over_ranks(pg, ms, device)
+    step_ms = sorted(phases.pop("_steps"))
+    latency = {"p50": max_over_ranks(pg, percentile(step_ms, 50), device),
+               "p99": max_over_ranks(pg, percentile(step_ms, 99), device),
+               "max": max_over_ranks(pg, step_ms[-1], device), "steps": len(step_ms),
+               "what": "whole-query step time (device events), max over ranks"}
     counters = fused.counters()
     result = fused.result()
     # Each rank holds the groups of its own fact rows; the job's answer is
@@ -295,10 +366,13 @@ def run_star(args, kb, W, rt, rank, world, pg, device):
         "mode": "fused (batched) pipeline",
         "groups": len(merged),
         "gpu_launches": launches,
+        "latency_ms": latency,
         "phases_ms": phases,
         "roofline": {"bound": "hbm", "kernel": "star_scan_kernel + star_join_kernel (fact probe)",
                      "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": profile_traffic("star_probe", nf),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the scan + join pair "
+                                       "on the 30M-fact-row case (profiles/star_probe_traffic.txt), scaled by fact rows",
                      "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": kern_ms,
                      "sectors_read_bytes": sector_bytes,
                      "sectors_read_GBps": sector_bytes / (kern_ms * 1e-3) / 1e9},
@@ -309,30 +383,65 @@ def run_star(args, kb, W, rt, rank, world, pg, device):
         "clocks": clk.summary(),
     }
     del plain
+    host = None
+    if not args.no_e2e or (rank == 0 and not args.no_cpu):
+        host = HostStar(data)
     if not args.no_e2e:
-        out["e2e"] = run_star_e2e(args, kb, W, rt, data, pg, device)
+        out["e2e"] = run_star_e2e(args, kb, W, rt, data, host, pg, device)
+    if rank == 0 and not args.no_cpu:
+        # The CPU leg: the oracle's star query on the host cores over every
+        # fact row of this rank (the same host buffers the e2e leg reads),
+        # timed, and its answer checked against the GPU's.
+        threads = os.cpu_count() or 1
+        kind = _oracle().use_native()
+        fact = tuple(h.numpy() for h in host.fact_cols)
+        dims = [tuple(h.numpy() for h in cols) for cols in (host.dim_a_cols, host.dim_b_cols)]
+        secs, ans = cpu_star_full(fact, dims, threads, runs=3)
+        out["cpu_baseline"] = {"value": nf / secs / 1e6, "unit": "Mrows/s", "cores": threads, "kind": "port",
+                               "sample": f"the whole query over all {nf} fact rows (no extrapolation), median of 3 "
+                                         f"runs; oracle built -O3 ({kind})",
+                               "build_s": ans[3], "probe_s": ans[4]}
+        out["parity"] = star_parity(fr, counters, ans, nf)
     return out
 
 
-def run_star_e2e(args, kb, W, rt, data, pg, device):
+class HostStar:
+    """Page-locked host copies of the star query's columns (Arrow batches
+    over them, and the tensors that own the memory)."""
+
+    def __init__(self, data):
+        import pyarrow as pa
+        import torch
+
+        def host_batch(cols):
+            arrays, names, keep = [], [], []
+            for name, t, _ in cols:
+                h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+                h.copy_(t)
+                keep.append(h)
+                arrays.append(pa.array(h.numpy()))
+                names.append(name)
+            return pa.RecordBatch.from_arrays(arrays, names=names), keep
+
+        self.fact, self.fact_cols = host_batch(data.fact)
+        self.dim_a, self.dim_a_cols = host_batch(data.dim_a)
+        self.dim_b, self.dim_b_cols = host_batch(data.dim_b)
+
+
+def percentile(sorted_values, q):
+    """The q-th percentile (nearest rank) of an ascending list."""
+    if not sorted_values:
+        return None
+    i = min(len(sorted_values) - 1, max(0, int(round(q / 100.0 * len(sorted_values) + 0.5)) - 1))
+    return sorted_values[i]
+
+
+def run_star_e2e(args, kb, W, rt, data, host, pg, device):
     """The same query through the C ABI with host (pinned) Arrow buffers; the
     host-to-device copies and the result's device-to-host read are timed."""
-    import pyarrow as pa
     import torch
 
-    def host_batch(cols):
-        arrays, names, keep = [], [], []
-        for name, t, _ in cols:
-            h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
-            h.copy_(t)
-            keep.append(h)
-            arrays.append(pa.array(h.numpy()))
-            names.append(name)
-        return pa.RecordBatch.from_arrays(arrays, names=names), keep
-
-    fact, k1 = host_batch(data.fact)
-    dim_a, k2 = host_batch(data.dim_a)
-    dim_b, k3 = host_batch(data.dim_b)
+    fact, dim_a, dim_b = host.fact, host.dim_a, host.dim_b
     pipe = kb.StarPipeline(rt, kb.star_spec(W.PRED_VALUE, W.PRED_VALUE, group_by=0, mode=kb.STAR_FUSED))
     steps = max(2, args.steps // 2)
     for _ in range(args.warmup):
@@ -632,9 +741,9 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
 
 def profile_traffic(name, rows):
     """DRAM bytes (read + write) of one launch of `name` over `rows` fact
-    rows, from the committed ncu summary (profiles/<name>_dram.md, line
+    rows, from the committed ncu summary profiles/<name>_traffic.txt (line
     'dram_bytes_per_fact_row: X'), scaled to `rows`."""
-    path = os.path.join(ROOT, "profiles", f"{name}_dram.md")
+    path = os.path.join(ROOT, "profiles", f"{name}_traffic.txt")
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_fact_row:"):
@@ -786,19 +895,36 @@ def main():
         # (no process group; the other ranks exit at once).
         if int(os.environ.get("RANK", "0")) != 0:
             return
-        steps = []
-        info = None
-        for _ in range(args.warmup + args.steps):
-            info = cpu_star(args.scale, min(args.cpu_sample, 5_000_000), threads)
-            steps.append(info["value"])
-        v = statistics.median(steps[args.warmup:])
+        O = _oracle()
+        kind = O.use_native()
+        fs = args.fact_scale if args.fact_scale is not None else args.scale
+        nf = int(300_000_000 * fs)
+        inputs = cpu_star_inputs(args.scale, fs, threads)
+        if inputs is not None:
+            fact, dims = inputs
+            # each step: the whole query over every fact row (no extrapolation)
+            secs, _ = cpu_star_full(fact, dims, threads, runs=args.warmup)
+            times = []
+            for _ in range(args.steps):
+                t, _ = cpu_star_full(fact, dims, threads, runs=1)
+                times.append(t)
+            v = nf / statistics.median(times) / 1e6
+            sample = (f"the whole query over all {nf} fact rows per step (dimension builds, key filters, probe, "
+                      f"grouped sums; no extrapolation); median of {args.steps} steps; oracle built -O3 ({kind})")
+        else:
+            steps = []
+            info = None
+            for _ in range(args.warmup + args.steps):
+                info = cpu_star(args.scale, min(args.cpu_sample, 5_000_000), threads)
+                steps.append(info["value"])
+            v = statistics.median(steps[args.warmup:])
+            sample = (f"full dimensions, first {info['sample_rows']} fact rows per step, whole-query rate "
+                      f"extrapolated (build + full probe): too little free host memory for all {nf} rows")
         line = {"impl": "reference", "metric": "star join+agg probe Mrows/s (fact rows per second, whole query)",
-                "value": v, "unit": "Mrows/s", "n_gpus": args.gpus, "device": "host CPU cores", "steps": args.steps, "warmup": args.warmup,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "config": star_config(args.scale, args.fact_scale if args.fact_scale is not None else args.scale),
-                "cpu_baseline": {"value": v, "unit": "Mrows/s", "cores": threads, "kind": "port",
-                                 "sample": f"full dimensions, first {info['sample_rows']} fact rows per step, "
-                                           "whole-query rate extrapolated (build + full probe)"},
+                "value": v, "unit": "Mrows/s", "n_gpus": args.gpus, "device": "host CPU cores", "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "config": star_config(args.scale, fs),
+                "cpu_baseline": {"value": v, "unit": "Mrows/s", "cores": threads, "kind": "port", "sample": sample},
                 "e2e": {"value": v, "unit": "Mrows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -812,12 +938,6 @@ def main():
     rt = kb.Runtime.on_torch_stream(local)
     runner = {"star": run_star, "join": run_join, "agg": run_agg, "serve": run_serve, "grace": run_grace}[args.workload]
     out = runner(args, kb, W, rt, rank, world, pg, device)
-    if rank == 0 and args.workload == "star" and not args.no_cpu:
-        c = cpu_star(args.scale, args.cpu_sample, threads)
-        out["cpu_baseline"] = {"value": c["value"], "unit": "Mrows/s", "cores": threads, "kind": "port",
-                               "sample": f"full dimensions + first {c['sample_rows']} fact rows, whole-query "
-                                         f"rate extrapolated to {int(300_000_000 * args.scale)} rows "
-                                         f"(build {c['build_s']:.2f} s, probe {c['probe_rows_per_s'] / 1e6:.1f} Mrows/s)"}
     if rank == 0:
         print(json.dumps(out))
     if pg is not None:

@@ -173,6 +173,21 @@ krv_status krv_join_key_filter(krv_join *j, krv_key_filter **out);
 krv_status krv_join_counters_get(const krv_join *j, krv_join_counters *out);
 void krv_join_destroy(krv_join *j);
 
+/* The key hash the join tables and partitions use, for every row of a device
+ * batch: the seedless row hash h of the key columns (RowLayout::encode +
+ * fold/mix, rows/layout.rs:487-555, 1131-1144: a NULL key mixes NULL_HASH when
+ * null_safe[k] is set and is skipped otherwise), g = fin(h ^ seed)
+ * (rows/layout.rs:1080), and the partition id at `depth` (Hashing::partition,
+ * join/keys.rs:118-128, and the grace levels of hash.rs:139-148: depth 0 takes
+ * the top `radix` bits of h, radix clamped to 3..6; depth d >= 1 takes bits
+ * [48-3d, 51-3d) of g, d clamped to 6). out_h, out_g (uint64) and out_part
+ * (int32) are device arrays of the batch's length on the runtime's device;
+ * any of them may be NULL. Asynchronous on the runtime's stream. */
+krv_status krv_hash_rows_device(krv_runtime *rt, const struct ArrowDeviceArray *batch,
+                                const struct ArrowSchema *schema, const int32_t *key_columns,
+                                const int32_t *null_safe, int32_t n_keys, uint64_t seed, int32_t depth,
+                                int32_t radix, uint64_t *out_h, uint64_t *out_g, int32_t *out_part);
+
 /* ---- partitioned (grace) hash join -----------------------------------------
  * The engine's grace join (join/grace.rs:828-1481): both sides are radix
  * partitioned by the key hash (level 0: top radix_bits of h, 3..6; a partition

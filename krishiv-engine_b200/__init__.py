@@ -193,6 +193,8 @@ _SIGS = {
     "krv_join_finish_device": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema)]),
     "krv_join_key_filter": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "krv_join_counters_get": (C.c_int32, [C.c_void_p, C.POINTER(JoinCounters)]),
+    "krv_hash_rows_device": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                         C.c_uint64, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "krv_join_destroy": (None, [C.c_void_p]),
     "krv_agg_spec_init": (None, [C.POINTER(AggSpec)]),
     "krv_agg_create": (C.c_int32, [C.c_void_p, C.POINTER(AggSpec), C.POINTER(C.c_void_p)]),
@@ -360,6 +362,7 @@ class DeviceBatch:
             self.children[i] = C.pointer(a)
         top_bufs = (C.c_void_p * 1)(None)
         self._keep.append(top_bufs)
+        self.rows = n
         self.dev = ArrowDeviceArray()
         self.dev.array = ArrowArray(length=n, null_count=0, offset=0, n_buffers=1, n_children=len(columns),
                                     buffers=top_bufs, children=self.children, dictionary=None,
@@ -473,6 +476,25 @@ class Runtime:
             self.close()
         except Exception:
             pass
+
+
+def hash_rows(rt: "Runtime", db: "DeviceBatch", key_columns=(0,), null_safe=None, seed: int = 0, depth: int = 0,
+              radix: int = 4):
+    """The join's key hash of every row of a DeviceBatch (krv_hash_rows_device):
+    (h, g, partition) as CUDA tensors (uint64 values in int64 tensors, int32
+    partition ids)."""
+    import torch
+    n = db.rows
+    dev = f"cuda:{rt.device}"
+    h = torch.empty(n, dtype=torch.int64, device=dev)
+    g = torch.empty(n, dtype=torch.int64, device=dev)
+    p = torch.empty(n, dtype=torch.int32, device=dev)
+    cols = (C.c_int32 * len(key_columns))(*key_columns)
+    ns = (C.c_int32 * len(key_columns))(*(null_safe or [0] * len(key_columns)))
+    check(lib().krv_hash_rows_device(rt.h, C.byref(db.dev), C.byref(db.schema), cols, ns, len(key_columns),
+                                     seed & 0xFFFFFFFFFFFFFFFF, depth, radix, h.data_ptr() if n else None,
+                                     g.data_ptr() if n else None, p.data_ptr() if n else None))
+    return h, g, p
 
 
 def join_spec(join_type="inner", probe_keys=(0,), build_keys=(0,), null_safe=None, single_match=False,
@@ -856,10 +878,27 @@ def agg_sum_i64_scratch(keys, values, out_keys, out_sums, out_counts, out_info, 
     (at most SCRATCH_MAX_GROUPS) and out_info two: the group count (-1 when the
     keys had more distinct values than max_groups) and a wrap flag. `stream`
     is a raw cudaStream_t handle (None: the default stream). Asynchronous."""
+    import torch
+    named = {"keys": keys, "values": values, "out_keys": out_keys, "out_sums": out_sums,
+             "out_counts": out_counts, "out_info": out_info}
+    for name, t in named.items():
+        if t.dtype != torch.int64:
+            raise ValueError(f"{name} must be int64, not {t.dtype}")
+        if not t.is_cuda:
+            raise ValueError(f"{name} must be a CUDA tensor")
+        if t.dim() != 1 or not t.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous 1-D tensor")
+    devices = {t.device for t in named.values()}
+    if len(devices) != 1:
+        raise ValueError("all tensors must be on one device")
     n = int(keys.shape[0])
     if int(values.shape[0]) != n:
         raise ValueError("keys and values differ in length")
     g = int(out_keys.shape[0])
+    if int(out_sums.shape[0]) < g or int(out_counts.shape[0]) < g:
+        raise ValueError("out_sums and out_counts must hold at least len(out_keys) values")
+    if int(out_info.shape[0]) < 2:
+        raise ValueError("out_info must hold two values")
     check(lib().krv_agg_sum_i64_scratch(keys.data_ptr() if n else None, values.data_ptr() if n else None, n, g,
                                         out_keys.data_ptr() if g else None, out_sums.data_ptr() if g else None,
                                         out_counts.data_ptr() if g else None, out_info.data_ptr(), stream))

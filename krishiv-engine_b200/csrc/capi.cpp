@@ -360,6 +360,19 @@ krv_status krv_join_counters_get(const krv_join *j, krv_join_counters *out) {
         return KRV_OK;
     });
 }
+krv_status krv_hash_rows_device(krv_runtime *rt, const ArrowDeviceArray *batch, const ArrowSchema *schema,
+                                const int32_t *key_columns, const int32_t *null_safe, int32_t n_keys, uint64_t seed,
+                                int32_t depth, int32_t radix, uint64_t *out_h, uint64_t *out_g, int32_t *out_part) {
+    return guard([&] {
+        need(rt, "runtime");
+        need(key_columns, "key_columns");
+        krv::Runtime *r = &rt->rt;
+        krv::DeviceGuard g(r);
+        DevBatch b = krv::import_device(r, batch, schema);
+        krv::hash_rows(r, b, key_columns, n_keys, null_safe, seed, depth, radix, out_h, out_g, out_part);
+        return KRV_OK;
+    });
+}
 void krv_join_destroy(krv_join *j) {
     if (!j) return;
     krv::DeviceGuard g(&j->owner->rt);

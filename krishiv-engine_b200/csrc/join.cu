@@ -511,6 +511,38 @@ KeysDev keys_of(const DevBatch &b, const int32_t *cols, int n, const int32_t *nu
     return k;
 }
 
+namespace {
+// The join's own key hash for every row, as the build and probe kernels
+// compute it: h (row_hash), g = fin(h ^ seed), and the partition at `depth`
+// (0: the top `radix` bits of h; d >= 1: bits [48-3d, 51-3d) of g).
+__global__ void __launch_bounds__(256) hash_rows_kernel(KeysDev k, int64_t n, uint64_t seed, int depth, int radix,
+                                                        uint64_t *out_h, uint64_t *out_g, int32_t *out_part) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t h = row_hash(k, i);
+        const uint64_t g = finalize(h, seed);
+        if (out_h) out_h[i] = h;
+        if (out_g) out_g[i] = g;
+        if (out_part) out_part[i] = depth == 0 ? (int32_t)(h >> (64 - radix)) : (int32_t)((g >> (48 - 3 * depth)) & 7u);
+    }
+}
+}  // namespace
+
+void hash_rows(Runtime *rt, const DevBatch &b, const int32_t *cols, int n, const int32_t *null_safe, uint64_t seed,
+               int depth, int radix, uint64_t *out_h, uint64_t *out_g, int32_t *out_part) {
+    if (n < 1 || n > KRV_MAX_KEYS) fail(KRV_INVALID_ARGUMENT, "1 to 4 key columns");
+    // Hashing::partition (join/keys.rs:92-95, 118-128): radix 3..6, depth 0..6
+    radix = std::min(6, std::max(3, radix));
+    if (depth < 0) fail(KRV_INVALID_ARGUMENT, "negative partition depth");
+    depth = std::min(depth, 6);
+    const KeysDev k = keys_of(b, cols, n, null_safe);
+    if (b.rows == 0) return;
+    hash_rows_kernel<<<grid_for(rt, b.rows, 256, 8), 256, 0, rt->stream>>>(k, b.rows, seed, depth, radix, out_h, out_g,
+                                                                          out_part);
+    rt->launches++;
+    check_launch("hash_rows_kernel");
+}
+
 static bool fast_keys(const KeysDev &k) { return k.n == 1 && k.c[0].width == 8 && !k.c[0].is_float; }
 
 HashJoin::HashJoin(Runtime *rt, const krv_join_spec &spec) : rt_(rt), spec_(spec) {

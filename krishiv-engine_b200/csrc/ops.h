@@ -24,6 +24,10 @@ struct KeysDev {
     uint32_t null_safe;  // bit k: key k is compared with <=>
 };
 KeysDev keys_of(const DevBatch &b, const int32_t *cols, int n, const int32_t *null_safe);
+// The join's key hash of every row (h, g = fin(h ^ seed), partition id at
+// depth / radix); any output may be null. Device outputs of b.rows values.
+void hash_rows(Runtime *rt, const DevBatch &b, const int32_t *cols, int n, const int32_t *null_safe, uint64_t seed,
+               int depth, int radix, uint64_t *out_h, uint64_t *out_g, int32_t *out_part);
 
 // ---- runtime key filter (crates/krishiv-io/src/runtime_filter/filter.rs:627) ----
 struct KeyFilterImpl {

@@ -51,7 +51,8 @@ constexpr int kProbeLimit = 8192;
 //   cnt[kSlots + 1]     COUNT(*) per slot; slot kSlots holds key kEmpty
 //   lo[kSlots + 1]      128-bit SUM per slot, low word
 //   hi[kSlots + 1]      128-bit SUM per slot, high word
-//   ctl[8]              [0] groups written, [1] a key found no slot, [2] a sum left int64
+//   ctl[8]              [0] groups written, [1] a key found no slot, [2] a sum left int64,
+//                       [3] slots claimed (distinct keys seen, the marker key aside)
 constexpr int64_t kOffCnt = kSlots;
 constexpr int64_t kOffLo = kOffCnt + kSlots + 1;
 constexpr int64_t kOffHi = kOffLo + kSlots + 1;
@@ -76,16 +77,28 @@ __global__ void clear_kernel(unsigned long long *s) {
         s[i] = i < kSlots ? kEmpty : 0ull;
 }
 
+// How often (in rows of one thread) the row loop looks at the void flags.
+constexpr int kVoidCheckEvery = 8;
+
 // One row: find or claim the key's slot, then add to its count and sum.
+// Once the answer is void (a key found no slot, or more than max_groups keys
+// claimed slots) the remaining rows are skipped: the kernel would otherwise
+// keep walking long probe runs of a full table only to report -1.
 __global__ void rows_kernel(unsigned long long *s, const int64_t *__restrict__ keys,
-                            const int64_t *__restrict__ values, int64_t n) {
+                            const int64_t *__restrict__ values, int64_t n, int64_t max_groups) {
     unsigned long long *slot_key = s;
     unsigned long long *cnt = s + kOffCnt;
     unsigned long long *lo = s + kOffLo;
     long long *hi = reinterpret_cast<long long *>(s + kOffHi);
     unsigned long long *ctl = s + kOffCtl;
+    const volatile unsigned long long *vctl = ctl;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int since_check = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        if (++since_check == kVoidCheckEvery) {
+            since_check = 0;
+            if (vctl[1] != 0 || (int64_t)vctl[3] > max_groups) break;
+        }
         const unsigned long long k = (unsigned long long)keys[i];
         const int64_t v = values[i];
         int64_t slot = -1;
@@ -95,7 +108,14 @@ __global__ void rows_kernel(unsigned long long *s, const int64_t *__restrict__ k
             uint64_t p = krv::finalize(krv::hash_word(k), kSeed) & (uint64_t)(kSlots - 1);
             for (int t = 0; t < kProbeLimit; t++) {
                 unsigned long long cur = slot_key[p];
-                if (cur == kEmpty) cur = atomicCAS(&slot_key[p], kEmpty, k);
+                if (cur == kEmpty) {
+                    cur = atomicCAS(&slot_key[p], kEmpty, k);
+                    if (cur == kEmpty && (int64_t)atomicAdd(&ctl[3], 1ull) >= max_groups) {
+                        // one key more than the caller's outputs hold
+                        atomicOr(&ctl[1], 1ull);
+                        break;
+                    }
+                }
                 if (cur == kEmpty || cur == k) {
                     slot = (int64_t)p;
                     break;
@@ -203,7 +223,7 @@ krv_status krv_agg_sum_i64_scratch(const int64_t *keys, const int64_t *values, i
     clear_kernel<<<std::min(slot_blocks, d.blocks), kThreads, 0, s>>>(d.words);
     if (n > 0) {
         const int row_blocks = (int)std::min<int64_t>(d.blocks, (n + kThreads - 1) / kThreads);
-        rows_kernel<<<row_blocks, kThreads, 0, s>>>(d.words, keys, values, n);
+        rows_kernel<<<row_blocks, kThreads, 0, s>>>(d.words, keys, values, n, max_groups);
     }
     emit_kernel<<<std::min(slot_blocks, d.blocks), kThreads, 0, s>>>(d.words, max_groups, out_keys, out_sums,
                                                                       out_counts);

@@ -15,6 +15,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_NATIVE_PATH = os.path.join(_HERE, "_native", "liboracle.so")
 
 INNER, LEFT_OUTER, LEFT_SEMI, LEFT_ANTI, NULL_AWARE_ANTI, EXISTENCE = 0, 1, 2, 3, 4, 5
 RIGHT_SEMI, RIGHT_ANTI, RIGHT_OUTER, FULL_OUTER = 6, 7, 8, 9
@@ -58,6 +59,23 @@ class OrcKeyFilter(C.Structure):
 
 
 _lib = None
+_lib_kind = "generic"
+
+
+def use_native() -> str:
+    """Loads a copy of the oracle compiled for this host (-O3 -march=native),
+    built here with `make native`; falls back to the generic -O3 copy when
+    that build fails. Must come before the first use. Returns which copy is
+    loaded ("native" or "generic")."""
+    global _lib_kind
+    if _lib is not None:
+        return _lib_kind
+    try:
+        subprocess.run(["make", "-s", "-C", _HERE, "native"], check=True, capture_output=True)
+        _lib_kind = "native"
+    except (OSError, subprocess.CalledProcessError):
+        _lib_kind = "generic"
+    return _lib_kind
 
 
 def lib():
@@ -65,7 +83,7 @@ def lib():
     if _lib is None:
         if not os.path.exists(_LIB_PATH):
             build()
-        L = C.CDLL(_LIB_PATH)
+        L = C.CDLL(_NATIVE_PATH if _lib_kind == "native" else _LIB_PATH)
         u64, i64, i32, vp = C.c_uint64, C.c_int64, C.c_int32, C.c_void_p
         L.orc_fold.restype = u64
         L.orc_fold.argtypes = [u64, u64]
@@ -318,6 +336,36 @@ def star_inputs(scale, seed, fact_row0=0, fact_rows=None, pred=7):
     r0 = dict(row0=fact_row0)
     fact = (gen_column(0, seed, 1, n, lo=0, hi=na - 1, **r0)[0], gen_column(0, seed, 2, n, lo=0, hi=nb - 1, **r0)[0],
             gen_column(0, seed, 3, n, lo=1000, hi=10_000_000, **r0)[0], gen_column(2, seed, 4, n, x0=0.0, x1=0.1, **r0)[0])
+    dims = []
+    for base, m in ((10, na), (20, nb)):
+        dims.append((gen_column(3, seed + base, base + 1, m, lo=0, hi=m)[0], gen_column(1, seed, base + 2, m, lo=0, hi=19)[0],
+                     gen_column(1, seed, base + 3, m, lo=0, hi=24)[0]))
+    return fact, dims
+
+
+def gen_column_mt(kind, seed, column, n, threads, lo=0, hi=0, x0=0.0, x1=0.0, row0=0, chunk=1 << 22):
+    """gen_column over `threads` host threads (chunks of rows; the C calls
+    release the interpreter lock). No NULLs."""
+    from concurrent.futures import ThreadPoolExecutor
+    out = np.empty(n, dtype=GEN_DTYPE[kind])
+    L = lib()
+
+    def work(a):
+        b = min(n, a + chunk)
+        L.orc_gen_column(seed, column, kind, lo, hi, x0, x1, row0 + a, b - a, 0.0, out[a:].ctypes.data, None)
+
+    with ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
+        list(ex.map(work, range(0, n, chunk)))
+    return out
+
+
+def star_inputs_mt(scale, seed, threads, fact_rows=None, pred=7):
+    """star_inputs with the fact columns generated on `threads` host threads."""
+    nf, na, nb = int(300_000_000 * scale), int(20_000_000 * scale), int(1_000_000 * scale)
+    n = nf if fact_rows is None else fact_rows
+    fact = (gen_column_mt(0, seed, 1, n, threads, lo=0, hi=na - 1), gen_column_mt(0, seed, 2, n, threads, lo=0, hi=nb - 1),
+            gen_column_mt(0, seed, 3, n, threads, lo=1000, hi=10_000_000),
+            gen_column_mt(2, seed, 4, n, threads, x0=0.0, x1=0.1))
     dims = []
     for base, m in ((10, na), (20, nb)):
         dims.append((gen_column(3, seed + base, base + 1, m, lo=0, hi=m)[0], gen_column(1, seed, base + 2, m, lo=0, hi=19)[0],
