@@ -487,6 +487,9 @@ def run_star_e2e(args, kb, W, rt, data, host, pg, device):
             "timing": "host wall clock around synchronous C-ABI calls"}
 
 
+SWEEP_LOADS = (0.25, 0.5, 1.0, 1.5)
+
+
 def run_serve(args, kb, W, rt, rank, world, pg, device):
     """The served request stream: join + grouped aggregate requests against
     resident tables, batched (ticks over a device work queue) against plain
@@ -549,6 +552,7 @@ def run_serve(args, kb, W, rt, rank, world, pg, device):
     n = args.requests
     zero, which = W.serve_arrivals(n, 0.0, len(temps))
     zero = np.zeros(n)
+    sweep = None
     with Clocks(device) as clk:
         cap_b = stream(kb.SERVE_BATCHED, zero, which, warm=len(temps))
         cap_p = stream(kb.SERVE_PLAIN, zero[: args.plain_requests], which[: args.plain_requests], warm=2)
@@ -560,6 +564,21 @@ def run_serve(args, kb, W, rt, rank, world, pg, device):
         rate_b = load * cap_b["requests_per_s"]
         arr_b, wh_b = W.serve_arrivals(n, rate_b, len(temps))
         at_batched = stream(kb.SERVE_BATCHED, arr_b, wh_b, warm=len(temps))
+        if args.serve_sweep:
+            # Offered load swept from 0.25x to 1.5x of each mode's measured
+            # capacity (Poisson arrivals, the same template mix): requests
+            # served per second, p50 / p99 latency at each point.
+            sweep = {"loads": list(SWEEP_LOADS), "batched": [], "plain": []}
+            for mode, cap, count, key in ((kb.SERVE_BATCHED, cap_b, n, "batched"),
+                                          (kb.SERVE_PLAIN, cap_p, args.plain_requests, "plain")):
+                for f in SWEEP_LOADS:
+                    r = f * cap["requests_per_s"]
+                    a_s, w_s = W.serve_arrivals(count, r, len(temps))
+                    pt = stream(mode, a_s, w_s, warm=len(temps) if mode == kb.SERVE_BATCHED else 2)
+                    pt["offered_requests_per_s"] = r
+                    pt["offered_load"] = f
+                    pt.pop("stats", None)
+                    sweep[key].append(pt)
     # the same request alone and in the mix
     s, tids = server(kb.SERVE_BATCHED)
     j = int(which[0])
@@ -595,6 +614,7 @@ def run_serve(args, kb, W, rt, rank, world, pg, device):
         "open_loop_at_plain_load": {"requests_per_s_offered": rate, "plain": at_plain_p, "batched": at_plain_b},
         "open_loop_at_batched_load": {"requests_per_s_offered": rate_b, "batched": at_batched},
         "same_alone_and_in_mix": alone == in_mix,
+        "load_sweep": sweep,
         "roofline": {"bound": "hbm", "achieved": alg, "peak": peak, "peak_source": kind, "unit": "GB/s",
                      "frac": alg / peak, "traffic": None,
                      "note": "16 B (k, x) per probe row over the closed-loop batched run"},
@@ -885,6 +905,8 @@ def main():
     ap.add_argument("--tick-rows", type=int, default=16 << 20, help="serve: probe rows per tick")
     ap.add_argument("--serve-budget", type=int, default=8 << 30, help="serve: HBM budget of running requests")
     ap.add_argument("--serve-load", type=float, default=0.7, help="serve: offered load / capacity")
+    ap.add_argument("--serve-sweep", action="store_true",
+                    help="serve: also sweep the offered load over 0.25x..1.5x of each mode's capacity")
     ap.add_argument("--grace-budget", type=int, default=24 << 30, help="grace: device budget of the join")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -450,6 +450,412 @@ __global__ void __launch_bounds__(kAggThreads) agg_shared_kernel(AggPlanDev P, T
     }
 }
 
+// ---- partitioned aggregation ------------------------------------------------------
+// Two passes over a batch, so that no row updates a record through a global
+// atomic:
+//  1. agg_split_kernel streams every row once. Rows of the hot keys (sampled
+//     from the first batch), of the NULL key and of the marker key are combined
+//     within the warp (lanes of one key reduce to one leader) and folded into
+//     the CTA's shared-memory records of those keys; every other row is written
+//     as one fixed-size row record into its hash partition.
+//  2. agg_part_kernel runs one CTA per partition: the partition's rows are
+//     folded into a shared-memory table of its keys (each cold key lives in one
+//     partition only), and each key's record is merged once into the global
+//     record of its group. A full local table is merged and emptied (a window);
+//     a window whose keys find no room in the global table is not merged at all,
+//     and the partition stops there to run again after the host grows the table.
+// Row records: key (8 B) at 0, the validity word (bit c: plan column c valid)
+// at 8, values at off_val[c] (4-byte values from 12, then 8- and 16-byte ones).
+constexpr int kHotMax = 512;
+constexpr int kSplitThreads = 512;
+constexpr int kPartThreads = 512;
+constexpr int kCntStride = 32;  // partition counters one 128-byte line apart
+constexpr unsigned kFullMask = 0xFFFFFFFFu;
+
+struct SplitDev {
+    const long long *hot_keys;  // H distinct keys, none equal to kEmptyKey
+    const uint32_t *hot_gids;   // H + 2 global group ids (then the NULL and marker groups)
+    int H;
+    int hot_slots;  // power of two >= 2H (0 when H == 0)
+    int part_bits;  // >= 1
+    int row_bytes;
+    int16_t off_val[kMaxValueCols];
+    uint8_t *part_buf;          // partition p: rows [p * cap, (p + 1) * cap)
+    unsigned int *part_cnt;     // partition p's row count at part_cnt[p * kCntStride]
+    uint32_t cap;
+    uint32_t *ovf_rows;         // rows that met a full partition (aggregated afterwards)
+    unsigned long long *ovf_count;
+    int64_t row0;               // the batch row of this slice's row 0 (ovf_rows hold batch rows)
+};
+
+// A value as the accumulators take it: `lo`/`hi` the 128-bit sum operand of
+// integer and decimal types (f64: the value's bits in lo); `mm` a signed
+// 64-bit key whose order is the value's (f64: the order key with its top bit
+// flipped; decimal128: the low word, MIN/MAX being for precision <= 18).
+__device__ __forceinline__ void value_words(const AggColDev &C, const void *data, int64_t i, uint64_t &lo,
+                                            uint64_t &hi) {
+    if (C.type == (int)Type::I32 || C.type == (int)Type::Date32) {
+        const long long v = static_cast<const int *>(data)[i];
+        lo = (uint64_t)v;
+        hi = v < 0 ? ~0ull : 0ull;
+    } else if (C.type == (int)Type::Dec128) {
+        const long long *p = static_cast<const long long *>(data) + 2 * i;
+        lo = (uint64_t)p[0];
+        hi = (uint64_t)p[1];
+    } else {  // I64, Dec64, F64 (bits)
+        const long long v = static_cast<const long long *>(data)[i];
+        lo = (uint64_t)v;
+        hi = v < 0 ? ~0ull : 0ull;
+    }
+}
+__device__ __forceinline__ long long mm_key(const AggColDev &C, uint64_t lo) {
+    if (C.type == (int)Type::F64) return (long long)(f64_order_key(__longlong_as_double((long long)lo)) ^ 0x8000000000000000ull);
+    return (long long)lo;
+}
+
+// Folds (count, 128-bit sum or double-double sum, min and max keys) of one
+// key's rows into its record; shared or global memory, concurrent updaters.
+__device__ __forceinline__ void fold_partial(const AggColDev &C, uint8_t *r, unsigned long long cnt, uint64_t slo,
+                                             uint64_t shi, double ds, double de, long long mn, long long mx) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(r + C.off_count), cnt);
+    const bool i32 = C.type == (int)Type::I32 || C.type == (int)Type::Date32;
+    if (C.flags & F_SUM) {
+        if (C.type == (int)Type::F64) {
+            atomic_add_dd2(reinterpret_cast<double *>(r + C.off_sum), reinterpret_cast<double *>(r + C.off_sum + 8), ds,
+                           de);
+        } else if (i32) {
+            atomicAdd(reinterpret_cast<unsigned long long *>(r + C.off_sum), (unsigned long long)slo);
+        } else {
+            atomic_add_i128(reinterpret_cast<unsigned long long *>(r + C.off_sum),
+                            reinterpret_cast<long long *>(r + C.off_sum + 8), (int64_t)slo, (int64_t)shi);
+        }
+    }
+    if (C.flags & F_MIN) {
+        if (i32) atomicMin(reinterpret_cast<int *>(r + C.off_min), (int)mn);
+        else if (C.type == (int)Type::F64)
+            atomicMin(reinterpret_cast<unsigned long long *>(r + C.off_min), (unsigned long long)mn ^ 0x8000000000000000ull);
+        else atomicMin(reinterpret_cast<long long *>(r + C.off_min), mn);
+    }
+    if (C.flags & F_MAX) {
+        if (i32) atomicMax(reinterpret_cast<int *>(r + C.off_max), (int)mx);
+        else if (C.type == (int)Type::F64)
+            atomicMax(reinterpret_cast<unsigned long long *>(r + C.off_max), (unsigned long long)mx ^ 0x8000000000000000ull);
+        else atomicMax(reinterpret_cast<long long *>(r + C.off_max), mx);
+    }
+}
+
+// The hot rows of one warp step: the lanes of each hot key (`hi`, -1 when the
+// lane has none) reduce their values to the key's lowest lane, which folds
+// them into the key's shared-memory record: one update per key and warp step.
+__device__ __forceinline__ void hot_rows(const AggPlanDev &P, uint8_t *hrec, int64_t r, int hi, unsigned lane) {
+    const bool hot = hi >= 0;
+    const unsigned peers = __match_any_sync(kFullMask, hot ? hi : 0x40000 + (int)lane);
+    const unsigned lead_lane = __ffs(peers) - 1;
+    const bool lead = hot && lane == lead_lane;
+    const unsigned turns = __reduce_max_sync(kFullMask, hot ? (unsigned)__popc(peers) : 1u);
+    uint8_t *rec = hrec + (size_t)(hot ? hi : 0) * P.rec;
+    if (lead) atomicAdd(reinterpret_cast<unsigned long long *>(rec + P.off_rows), (unsigned long long)__popc(peers));
+    for (int c = 0; c < P.ncols; c++) {
+        const AggColDev &C = P.c[c];
+        const bool v = hot && bit_get(C.valid, C.voff, r);
+        const unsigned vm = __ballot_sync(kFullMask, v) & peers;
+        const bool any = (C.flags & (F_SUM | F_MIN | F_MAX)) != 0;
+        uint64_t lo = 0, hw = 0;
+        if (v && any) value_words(C, C.data, r, lo, hw);
+        const bool f64 = C.type == (int)Type::F64;
+        // this lane's value, then the other lanes of its key
+        uint64_t slo = v ? lo : 0, shi = v ? hw : 0;
+        double ds = (v && f64) ? __longlong_as_double((long long)lo) : 0.0, de = 0.0;
+        long long mn = v ? mm_key(C, lo) : LLONG_MAX, mx = v ? mm_key(C, lo) : LLONG_MIN;
+        if (any) {
+            unsigned rest = peers & (peers - 1u);
+            for (unsigned t = 1; t < turns; t++) {
+                const unsigned src = rest ? (unsigned)__ffs(rest) - 1u : lane;
+                rest &= rest - 1u;
+                const uint64_t xlo = __shfl_sync(kFullMask, lo, src);
+                const uint64_t xhi = __shfl_sync(kFullMask, hw, src);
+                if (src != lane && ((vm >> src) & 1u)) {
+                    if (f64) {
+                        double s, e;
+                        two_sum(ds, __longlong_as_double((long long)xlo), s, e);
+                        ds = s;
+                        de = __dadd_rn(de, e);
+                    } else {
+                        const uint64_t o = slo;
+                        slo += xlo;
+                        shi += xhi + (slo < o ? 1ull : 0ull);
+                    }
+                    const long long k = mm_key(C, xlo);
+                    mn = k < mn ? k : mn;
+                    mx = k > mx ? k : mx;
+                }
+            }
+        }
+        if (lead && vm) fold_partial(C, rec, (unsigned long long)__popc(vm), slo, shi, ds, de, mn, mx);
+    }
+}
+
+// The cold rows of one warp step: each lane's row into its partition (one
+// counter update per partition and warp step); a row that meets a full
+// partition is listed for the global table instead.
+__device__ __forceinline__ void cold_rows(const AggPlanDev &P, const SplitDev &S, int64_t r, long long k, uint64_t h,
+                                          bool cold, unsigned lane) {
+    const int p = cold ? (int)(h >> (64 - S.part_bits)) : -1 - (int)lane;
+    const unsigned peers = __match_any_sync(kFullMask, p);
+    const unsigned lead_lane = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (cold && lane == lead_lane) base = atomicAdd(S.part_cnt + (size_t)p * kCntStride, (unsigned)__popc(peers));
+    base = __shfl_sync(kFullMask, base, lead_lane);
+    if (!cold) return;
+    const unsigned at = base + __popc(peers & ((1u << lane) - 1u));
+    if (at >= S.cap) {
+        S.ovf_rows[atomicAdd(S.ovf_count, 1ull)] = (uint32_t)(S.row0 + r);
+        return;
+    }
+    uint8_t *row = S.part_buf + ((size_t)p * S.cap + at) * S.row_bytes;
+    *reinterpret_cast<long long *>(row) = k;
+    uint32_t bits = 0;
+    for (int c = 0; c < P.ncols; c++) {
+        const AggColDev &C = P.c[c];
+        if (!bit_get(C.valid, C.voff, r)) continue;
+        bits |= 1u << c;
+        if (!(C.flags & (F_SUM | F_MIN | F_MAX))) continue;
+        uint8_t *dst = row + S.off_val[c];
+        if (C.type == (int)Type::I32 || C.type == (int)Type::Date32)
+            *reinterpret_cast<int *>(dst) = static_cast<const int *>(C.data)[r];
+        else if (C.type == (int)Type::Dec128)
+            *reinterpret_cast<longlong2 *>(dst) = static_cast<const longlong2 *>(C.data)[r];
+        else
+            *reinterpret_cast<long long *>(dst) = static_cast<const long long *>(C.data)[r];
+    }
+    *reinterpret_cast<uint32_t *>(row + 8) = bits;
+}
+
+__global__ void __launch_bounds__(kSplitThreads) agg_split_kernel(AggPlanDev P, TableDev T, KeyIn key, int64_t n,
+                                                                  SplitDev S) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int NH = S.H + 2;
+    uint8_t *hrec = smem;                                                          // NH records
+    long long *hkeys = reinterpret_cast<long long *>(hrec + (size_t)NH * P.rec);   // hot_slots
+    int16_t *hidx = reinterpret_cast<int16_t *>(hkeys + S.hot_slots);              // hot_slots
+    const unsigned lane = threadIdx.x & 31u;
+    for (int e = threadIdx.x; e < NH; e += blockDim.x) init_record(P, hrec + (size_t)e * P.rec);
+    for (int e = threadIdx.x; e < S.hot_slots; e += blockDim.x) {
+        hkeys[e] = kEmptyKey;
+        hidx[e] = -1;
+    }
+    __syncthreads();
+    const int hmask = S.hot_slots - 1;
+    for (int j = threadIdx.x; j < S.H; j += blockDim.x) {
+        const long long k = S.hot_keys[j];
+        int pos = (int)(hash_word((uint64_t)k) & (uint64_t)hmask);
+        for (int t = 0; t < S.hot_slots; t++) {
+            if ((long long)atomicCAS(reinterpret_cast<unsigned long long *>(hkeys + pos), (unsigned long long)kEmptyKey,
+                                     (unsigned long long)k) == kEmptyKey) {
+                hidx[pos] = (int16_t)j;
+                break;
+            }
+            pos = (pos + 1) & hmask;
+        }
+    }
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int64_t r = base + threadIdx.x;
+        const bool live = r < n;
+        const bool kv = live && bit_get(key.valid, key.voff, r);
+        const long long k = kv ? key_at(key, r) : 0;
+        const uint64_t h = hash_word((uint64_t)k);
+        int hi = -1;
+        if (live) {
+            if (!kv) hi = S.H;
+            else if (k == kEmptyKey) hi = S.H + 1;
+            else if (S.H) {
+                int pos = (int)(h & (uint64_t)hmask);
+                for (int t = 0; t < S.hot_slots; t++) {
+                    const long long c = hkeys[pos];
+                    if (c == k) {
+                        hi = hidx[pos];
+                        break;
+                    }
+                    if (c == kEmptyKey) break;
+                    pos = (pos + 1) & hmask;
+                }
+            }
+        }
+        if (__any_sync(kFullMask, hi >= 0)) hot_rows(P, hrec, r, hi, lane);
+        const bool cold = live && hi < 0;
+        if (__any_sync(kFullMask, cold)) cold_rows(P, S, r, k, h, cold, lane);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < NH; e += blockDim.x) {
+        if (S.hot_gids[e] < kOverflowGid) merge_record(P, T.states + (size_t)S.hot_gids[e] * P.rec, hrec + (size_t)e * P.rec);
+        else atomicOr(T.status, ST_CAPACITY);
+    }
+}
+
+struct PartDev {
+    const uint8_t *part_buf;
+    const unsigned int *part_cnt;
+    uint32_t cap;
+    int row_bytes;
+    int16_t off_val[kMaxValueCols];
+    const int *todo;   // the partitions to run: CTA b runs partition todo[b]
+    uint32_t *start;   // per partition: its first row not yet merged (read and written)
+    int *failed;       // partitions that stopped for want of room in the global table
+    int L;             // local records per CTA (>= the block size)
+    int slots;         // local table slots: a power of two >= 2L
+};
+
+// One row record folded into a (shared-memory) record.
+__device__ __forceinline__ void fold_row(const AggPlanDev &P, const int16_t *off_val, uint8_t *rec, const uint8_t *row) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(rec + P.off_rows), 1ull);
+    const uint32_t bits = *reinterpret_cast<const uint32_t *>(row + 8);
+    for (int c = 0; c < P.ncols; c++) {
+        if (!((bits >> c) & 1u)) continue;
+        const AggColDev &C = P.c[c];
+        if (!(C.flags & (F_SUM | F_MIN | F_MAX))) {
+            atomicAdd(reinterpret_cast<unsigned long long *>(rec + C.off_count), 1ull);
+            continue;
+        }
+        uint64_t lo, hi;
+        value_words(C, row + off_val[c], 0, lo, hi);
+        const bool f64 = C.type == (int)Type::F64;
+        const long long m = mm_key(C, lo);
+        fold_partial(C, rec, 1ull, lo, hi, f64 ? __longlong_as_double((long long)lo) : 0.0, 0.0, m, m);
+    }
+}
+
+// The local record of key k, claimed (and initialised) when new; -1 when the
+// table has no record left or a wait gave up.
+__device__ __forceinline__ int local_record(const AggPlanDev &P, const PartDev &D, long long *skeys, uint16_t *sidx,
+                                            long long *rkeys, uint8_t *lrec, int *fill, long long k, uint64_t h,
+                                            uint32_t *status) {
+    const int mask = D.slots - 1;
+    int pos = (int)(h & (uint64_t)mask);
+    for (int t = 0; t < D.slots; t++) {
+        long long cur = *reinterpret_cast<volatile long long *>(skeys + pos);
+        if (cur == kEmptyKey) {
+            const int e = atomicAdd(fill, 1);
+            if (e >= D.L) return -1;
+            init_record(P, lrec + (size_t)e * P.rec);
+            rkeys[e] = k;
+            __threadfence_block();
+            cur = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(skeys + pos), (unsigned long long)kEmptyKey,
+                                       (unsigned long long)k);
+            if (cur == kEmptyKey) {
+                *reinterpret_cast<volatile uint16_t *>(sidx + pos) = (uint16_t)e;
+                return e;
+            }
+            // another thread claimed the slot: record e stays empty (no rows)
+        }
+        if (cur == k) {
+            for (int it = 0; it < (1 << 20); it++) {
+                const uint16_t e = *reinterpret_cast<volatile uint16_t *>(sidx + pos);
+                if (e != 0xFFFFu) {
+                    __threadfence_block();
+                    return e;
+                }
+            }
+            atomicOr(status, ST_TIMEOUT);
+            return -1;
+        }
+        pos = (pos + 1) & mask;
+    }
+    return -1;
+}
+
+// Merges the non-empty local records into the global table: first every key's
+// group id (inserting new keys), and only when all found one, the records.
+__device__ bool flush_local(const AggPlanDev &P, const TableDev &T, const PartDev &D, const long long *rkeys,
+                            uint8_t *lrec, uint32_t *lgid, int m, int *fail) {
+    for (int e = threadIdx.x; e < m; e += blockDim.x) {
+        uint32_t g = kPending;
+        if (*reinterpret_cast<const unsigned long long *>(lrec + (size_t)e * P.rec + P.off_rows)) {
+            g = find_or_insert(T, P, rkeys[e]);
+            if (g == kOverflowGid) atomicOr(fail, 1);
+        }
+        lgid[e] = g;
+    }
+    __syncthreads();
+    const bool ok = *reinterpret_cast<volatile int *>(fail) == 0;
+    if (ok)
+        for (int e = threadIdx.x; e < m; e += blockDim.x)
+            if (lgid[e] != kPending) merge_record(P, T.states + (size_t)lgid[e] * P.rec, lrec + (size_t)e * P.rec);
+    __syncthreads();
+    return ok;
+}
+
+__global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, TableDev T, PartDev D) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint8_t *lrec = smem;                                                            // L records
+    long long *rkeys = reinterpret_cast<long long *>(lrec + (size_t)D.L * P.rec);    // L keys
+    long long *skeys = rkeys + D.L;                                                  // slots
+    uint16_t *sidx = reinterpret_cast<uint16_t *>(skeys + D.slots);                  // slots
+    uint32_t *lgid = reinterpret_cast<uint32_t *>(sidx + D.slots);                   // L
+    __shared__ int s_fill, s_fail;
+    const int p = D.todo[blockIdx.x];
+    const uint32_t cnt = D.part_cnt[(size_t)p * kCntStride];
+    const uint32_t rows = cnt < D.cap ? cnt : D.cap;
+    const uint8_t *buf = D.part_buf + (size_t)p * D.cap * D.row_bytes;
+    uint32_t window = D.start[p];
+    auto reset = [&]() {
+        for (int s = threadIdx.x; s < D.slots; s += blockDim.x) {
+            skeys[s] = kEmptyKey;
+            sidx[s] = 0xFFFFu;
+        }
+        if (threadIdx.x == 0) {
+            s_fill = 0;
+            s_fail = 0;
+        }
+        __syncthreads();
+    };
+    reset();
+    for (uint32_t base = window; base < rows; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const bool live = i < rows;
+        const uint8_t *row = buf + (size_t)i * D.row_bytes;
+        const long long k = live ? *reinterpret_cast<const long long *>(row) : 0;
+        const uint64_t h = hash_word((uint64_t)k);
+        for (int attempt = 0; attempt < 2; attempt++) {
+            const int e = live ? local_record(P, D, skeys, sidx, rkeys, lrec, &s_fill, k, h, T.status) : 0;
+            if (!__syncthreads_or(e < 0)) {
+                if (live) fold_row(P, D.off_val, lrec + (size_t)e * P.rec, row);
+                break;
+            }
+            // The table is full: merge the window's rows (those before this
+            // tile; the tile's new records are still empty) and retry the tile.
+            const int m = s_fill < D.L ? s_fill : D.L;
+            if (!flush_local(P, T, D, rkeys, lrec, lgid, m, &s_fail)) {
+                if (threadIdx.x == 0) {
+                    D.start[p] = window;
+                    atomicAdd(D.failed, 1);
+                }
+                return;
+            }
+            window = base;
+            reset();
+        }
+    }
+    __syncthreads();
+    const int m = s_fill < D.L ? s_fill : D.L;
+    if (!flush_local(P, T, D, rkeys, lrec, lgid, m, &s_fail)) {
+        if (threadIdx.x == 0) {
+            D.start[p] = window;
+            atomicAdd(D.failed, 1);
+        }
+        return;
+    }
+    if (threadIdx.x == 0) D.start[p] = rows;
+}
+
+// Group ids of the hot keys (inserted into the global table), then the NULL
+// and the marker group.
+__global__ void hot_gid_kernel(AggPlanDev P, TableDev T, const long long *hot_keys, int H, uint32_t *hot_gids) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < H + 2; j += gridDim.x * blockDim.x)
+        hot_gids[j] = j < H ? find_or_insert(T, P, hot_keys[j]) : (j == H ? kNullGid : kMarkerGid);
+}
+
 __global__ void init_special_kernel(AggPlanDev P, uint8_t *states) {
     if (threadIdx.x < 2) init_record(P, states + (size_t)threadIdx.x * P.rec);
 }
@@ -844,6 +1250,22 @@ class HashAggregate {
     bool sampled_ = false;
     DBuf hot_;
     int hot_count_ = 0;
+    // The partitioned path (agg_split_kernel + agg_part_kernel) for large
+    // batches: its hot keys, their group ids and the estimate of distinct
+    // keys, taken from the first large batch.
+    bool use_partitioned(int64_t n) const;
+    void push_partitioned(const DevBatch &b, const KeyIn &key, int64_t n);
+    void plan_partitioned(const KeyIn &key, int64_t n);
+    void drain_deferred(const DevBatch &b, const KeyIn &key, DBuf &ovf, DBuf &ovf_count, unsigned long long deferred);
+    bool part_planned_ = false;
+    DBuf part_hot_keys_, part_hot_gids_;
+    int part_hot_ = 0;
+    double part_cold_frac_ = 1.0;
+    int64_t part_groups_est_ = 0;
+    int part_row_bytes_ = 0;
+    int16_t part_off_val_[kMaxValueCols] = {};
+    int part_local_ = 0;      // local records per agg_part_kernel CTA
+    size_t part_smem_ = 0;    // its shared memory
 };
 
 HashAggregate::HashAggregate(Runtime *rt, const krv_agg_spec &spec) : rt_(rt), spec_(spec) {
@@ -1025,6 +1447,14 @@ void HashAggregate::plan(const DevBatch &b) {
     while ((e * 2) * per + 64 <= std::min(rt_->max_smem_optin, 200 * 1024)) e *= 2;
     smem_entries_ = e >= 64 ? e : 0;
     if (smem_entries_ == 0) mode_ = KRV_AGG_MODE_GLOBAL;
+    // The partitioned path's local table: at least one record per thread of
+    // agg_part_kernel, with slots for twice as many keys.
+    {
+        const int L = kPartThreads;
+        const size_t smem = (size_t)L * (P_.rec + 8 + 4) + (size_t)next_pow2((uint64_t)2 * L) * 10;
+        part_local_ = smem <= (size_t)rt_->max_smem_optin - 1024 ? L : 0;
+        part_smem_ = smem;
+    }
     const uint64_t hint = spec_.expected_groups > 0 ? (uint64_t)spec_.expected_groups : 65536;
     alloc_table(std::max<uint64_t>(1024, next_pow2((uint64_t)(hint * 2))));
     planned_ = true;
@@ -1150,6 +1580,276 @@ void HashAggregate::sample_hot(const KeyIn &key, int64_t n) {
     KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // `hot` is a stack vector
 }
 
+// ---- the partitioned path ----------------------------------------------------------
+namespace {
+constexpr int64_t kPartMinRows = 1 << 18;    // smaller batches take the one-pass kernels
+constexpr int64_t kPartSliceRows = 1 << 27;  // rows per split + partition round
+constexpr int kPartSample = 1 << 16;
+
+// The plan's columns sliced to start at row `row0`.
+AggPlanDev slice_plan(const AggPlanDev &P, int64_t row0, const std::vector<int> &widths) {
+    AggPlanDev S = P;
+    for (int c = 0; c < P.ncols; c++) {
+        S.c[c].data = static_cast<const uint8_t *>(P.c[c].data) + row0 * widths[c];
+        S.c[c].voff = P.c[c].voff + row0;
+    }
+    return S;
+}
+}  // namespace
+
+bool HashAggregate::use_partitioned(int64_t n) const {
+    return mode_ == KRV_AGG_MODE_SHARED && n >= kPartMinRows && part_local_ > 0;
+}
+
+void HashAggregate::plan_partitioned(const KeyIn &key, int64_t n) {
+    part_planned_ = true;
+    // Row records: key, validity word, then the values the accumulators read.
+    int off = 12;
+    for (int c = 0; c < P_.ncols; c++) part_off_val_[c] = 0;
+    for (int pass = 0; pass < 3; pass++) {
+        const int want = pass == 0 ? 4 : pass == 1 ? 8 : 16;
+        if (want > 4) off = (off + want - 1) / want * want;
+        for (int c = 0; c < P_.ncols; c++) {
+            const AggColDev &C = P_.c[c];
+            if (!(C.flags & (F_SUM | F_MIN | F_MAX))) continue;
+            const int w = (C.type == (int)Type::I32 || C.type == (int)Type::Date32) ? 4
+                          : C.type == (int)Type::Dec128                             ? 16
+                                                                                    : 8;
+            if (w != want) continue;
+            part_off_val_[c] = (int16_t)off;
+            off += w;
+        }
+    }
+    part_row_bytes_ = (off + 15) / 16 * 16;
+    // The sample: a strided 64K rows of the first large batch.
+    const int m = (int)std::min<int64_t>(n, kPartSample);
+    const int64_t step = std::max<int64_t>(1, n / m);
+    DBuf keys(rt_, (size_t)m * 8), ok(rt_, (size_t)m);
+    sample_keys_kernel<<<grid_for(rt_, m, 256, 4), 256, 0, rt_->stream>>>(key, n, step, m, keys.as<long long>(),
+                                                                          ok.as<uint8_t>());
+    rt_->launches++;
+    check_launch("sample_keys_kernel");
+    std::vector<long long> hk(m);
+    std::vector<uint8_t> hv(m);
+    KRV_CUDA(cudaMemcpyAsync(hk.data(), keys.get(), (size_t)m * 8, cudaMemcpyDeviceToHost, rt_->stream));
+    KRV_CUDA(cudaMemcpyAsync(hv.data(), ok.get(), (size_t)m, cudaMemcpyDeviceToHost, rt_->stream));
+    KRV_CUDA(cudaStreamSynchronize(rt_->stream));
+    std::vector<long long> v;
+    int special = 0;
+    for (int j = 0; j < m; j++) {
+        if (hv[j] && hk[j] != kEmptyKey) v.push_back(hk[j]);
+        else special++;
+    }
+    std::sort(v.begin(), v.end());
+    std::vector<std::pair<int, long long>> runs;  // (count, key)
+    for (size_t a = 0; a < v.size();) {
+        size_t b = a;
+        while (b < v.size() && v[b] == v[a]) b++;
+        runs.push_back({(int)(b - a), v[a]});
+        a = b;
+    }
+    std::sort(runs.begin(), runs.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    // Hot: seen at least 3 times, as many as the split kernel's shared memory
+    // holds records for beside its lookup table.
+    const int smem_cap = std::min(rt_->max_smem_optin - 2048, 72 * 1024);
+    int hmax = kHotMax;
+    while (hmax > 0 && (size_t)(hmax + 2) * P_.rec + (size_t)2 * next_pow2(hmax) * 10 > (size_t)smem_cap) hmax /= 2;
+    std::vector<long long> hot;
+    int hot_rows = 0;
+    for (const auto &rk : runs) {
+        if ((int)hot.size() == hmax || rk.first < 3) break;
+        hot.push_back(rk.second);
+        hot_rows += rk.first;
+    }
+    part_hot_ = (int)hot.size();
+    part_cold_frac_ = m ? std::max(0.0, 1.0 - (double)(hot_rows + special) / m) : 1.0;
+    // Distinct cold keys (the guaranteed-error estimator: keys seen once in
+    // the sample stand for sqrt(n / m) keys each).
+    int64_t d = 0, f1 = 0;
+    for (size_t i = hot.size(); i < runs.size(); i++) {
+        d++;
+        if (runs[i].first == 1) f1++;
+    }
+    const double est = (double)d + (double)f1 * (std::sqrt((double)n / std::max(1, m)) - 1.0);
+    part_groups_est_ = std::max<int64_t>({(int64_t)est, spec_.expected_groups, 1});
+    // Hot keys' group ids: the table first gets room for them.
+    part_hot_keys_ = DBuf(rt_, (size_t)std::max(1, part_hot_) * 8);
+    part_hot_gids_ = DBuf(rt_, (size_t)(part_hot_ + 2) * 4);
+    if (part_hot_)
+        KRV_CUDA(cudaMemcpyAsync(part_hot_keys_.get(), hot.data(), hot.size() * 8, cudaMemcpyHostToDevice, rt_->stream));
+    if (known_groups_ + part_hot_ + 2 > (int64_t)limit_) grow((uint64_t)known_groups_ + part_hot_ + 2);
+    TableDev T{keys_.as<long long>(), gids_.as<uint32_t>(), slots_ - 1, states_.as<uint8_t>(), gkeys_.as<long long>(),
+               ngroups_.as<unsigned long long>(), limit_, status_word(rt_)};
+    hot_gid_kernel<<<grid_for(rt_, part_hot_ + 2, 128, 1), 128, 0, rt_->stream>>>(P_, T, part_hot_keys_.as<long long>(),
+                                                                                  part_hot_, part_hot_gids_.as<uint32_t>());
+    rt_->launches++;
+    check_launch("hot_gid_kernel");
+    KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // `hot` is a stack vector
+}
+
+// Rows listed in `ovf` (deferred: their partition was full) through the
+// global-table kernel, growing the table when they need room.
+void HashAggregate::drain_deferred(const DevBatch &b, const KeyIn &key, DBuf &ovf, DBuf &ovf_count,
+                                   unsigned long long deferred) {
+    AggPlanDev P = P_;
+    for (int c = 0; c < P.ncols; c++) {
+        const DevCol &col = b.cols[value_cols_[c]];
+        P.c[c].data = col.data;
+        P.c[c].valid = col.valid;
+        P.c[c].voff = col.valid_off;
+    }
+    DBuf idx;
+    for (int round = 0; round < 16; round++) {
+        if (deferred == 0) return;
+        known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());
+        if (known_groups_ + (int64_t)deferred > (int64_t)limit_) grow((uint64_t)known_groups_ + deferred);
+        idx = DBuf(rt_, (size_t)deferred * 4);
+        KRV_CUDA(cudaMemcpyAsync(idx.get(), ovf.get(), (size_t)deferred * 4, cudaMemcpyDeviceToDevice, rt_->stream));
+        KRV_CUDA(cudaMemsetAsync(ovf_count.get(), 0, 8, rt_->stream));
+        TableDev T{keys_.as<long long>(), gids_.as<uint32_t>(), slots_ - 1, states_.as<uint8_t>(), gkeys_.as<long long>(),
+                   ngroups_.as<unsigned long long>(), limit_, status_word(rt_)};
+        agg_global_kernel<<<grid_for(rt_, (int64_t)deferred, 256, 8), 256, 0, rt_->stream>>>(
+            P, T, key, (int64_t)deferred, idx.as<uint32_t>(), ovf.as<uint32_t>(), ovf_count.as<unsigned long long>());
+        rt_->launches++;
+        check_launch("agg_global_kernel");
+        deferred = read_scalar<unsigned long long>(rt_, ovf_count.get());
+    }
+    fail(KRV_INTERNAL, "aggregate: table growth did not converge");
+}
+
+void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_t n) {
+    clear_status(rt_);
+    known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());
+    pending_rows_ = 0;
+    if (!part_planned_) plan_partitioned(key, n);
+    AggPlanDev P = P_;
+    std::vector<int> widths(P.ncols);
+    for (int c = 0; c < P.ncols; c++) {
+        const DevCol &col = b.cols[value_cols_[c]];
+        P.c[c].data = col.data;
+        P.c[c].valid = col.valid;
+        P.c[c].voff = col.valid_off;
+        widths[c] = col.type.width();
+    }
+    const int L = part_local_;
+    // Partitions: each to hold about L/2 distinct keys.
+    int bits = 5;
+    while (bits < 14 && ((int64_t)1 << bits) * (L / 2) < part_groups_est_) bits++;
+    const int nparts = 1 << bits;
+    const int H = part_hot_;
+    const int hot_slots = H ? (int)next_pow2((uint64_t)2 * H) : 0;
+    const size_t split_smem = (size_t)(H + 2) * P.rec + (size_t)hot_slots * 10;
+    KRV_CUDA(cudaFuncSetAttribute(agg_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)split_smem));
+    KRV_CUDA(cudaFuncSetAttribute(agg_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)part_smem_));
+    int split_blocks = 0, part_blocks = 0;
+    KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&split_blocks, agg_split_kernel, kSplitThreads, split_smem));
+    KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&part_blocks, agg_part_kernel, kPartThreads, part_smem_));
+    if (split_blocks < 1 || part_blocks < 1) fail(KRV_INTERNAL, "aggregate: partitioned kernels do not fit an SM");
+    DBuf todo_all(rt_, (size_t)nparts * 4);
+    {
+        std::vector<int> iota(nparts);
+        for (int p = 0; p < nparts; p++) iota[p] = p;
+        KRV_CUDA(cudaMemcpyAsync(todo_all.get(), iota.data(), (size_t)nparts * 4, cudaMemcpyHostToDevice, rt_->stream));
+        KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // `iota` is a stack vector
+    }
+    const KeyIn key0 = key;
+    for (int64_t row0 = 0; row0 < n; row0 += kPartSliceRows) {
+        const int64_t ns = std::min<int64_t>(kPartSliceRows, n - row0);
+        const uint64_t cap64 =
+            std::min<uint64_t>((uint64_t)ns, ((uint64_t)((double)ns * part_cold_frac_ * 1.25 / nparts) + 256 + 31) / 32 * 32);
+        const uint32_t cap = (uint32_t)cap64;
+        DBuf part_buf(rt_, (size_t)nparts * cap * part_row_bytes_);
+        DBuf part_cnt(rt_, (size_t)nparts * kCntStride * 4);
+        DBuf start(rt_, (size_t)nparts * 4);
+        DBuf ctl(rt_, 16);  // [0] deferred rows (u64), [8] failed partitions (int)
+        DBuf ovf(rt_, (size_t)ns * 4);
+        KRV_CUDA(cudaMemsetAsync(part_cnt.get(), 0, part_cnt.bytes(), rt_->stream));
+        KRV_CUDA(cudaMemsetAsync(start.get(), 0, start.bytes(), rt_->stream));
+        KRV_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, rt_->stream));
+        // Room in the table for the keys this slice may add (an estimate; a
+        // partition that finds none stops and runs again after a grow).
+        const int64_t want = known_groups_ + std::min<int64_t>(ns, part_groups_est_) + H + 2;
+        if (want > (int64_t)limit_) grow((uint64_t)want);
+        TableDev T{keys_.as<long long>(), gids_.as<uint32_t>(), slots_ - 1, states_.as<uint8_t>(), gkeys_.as<long long>(),
+                   ngroups_.as<unsigned long long>(), limit_, status_word(rt_)};
+        SplitDev S{};
+        S.hot_keys = part_hot_keys_.as<long long>();
+        S.hot_gids = part_hot_gids_.as<uint32_t>();
+        S.H = H;
+        S.hot_slots = hot_slots;
+        S.part_bits = bits;
+        S.row_bytes = part_row_bytes_;
+        for (int c = 0; c < kMaxValueCols; c++) S.off_val[c] = part_off_val_[c];
+        S.part_buf = part_buf.as<uint8_t>();
+        S.part_cnt = part_cnt.as<unsigned int>();
+        S.cap = cap;
+        S.ovf_rows = ovf.as<uint32_t>();
+        S.ovf_count = ctl.as<unsigned long long>();
+        S.row0 = row0;
+        const AggPlanDev PS = slice_plan(P, row0, widths);
+        KeyIn ks = key0;
+        ks.data = static_cast<const uint8_t *>(key0.data) + row0 * key0.width;
+        ks.voff = key0.voff + row0;
+        const int grid1 = (int)std::min<int64_t>((int64_t)split_blocks * rt_->sm_count, ceil_div(ns, kSplitThreads));
+        agg_split_kernel<<<grid1, kSplitThreads, split_smem, rt_->stream>>>(PS, T, ks, ns, S);
+        rt_->launches++;
+        check_launch("agg_split_kernel");
+        PartDev D{};
+        D.part_buf = part_buf.as<uint8_t>();
+        D.part_cnt = part_cnt.as<unsigned int>();
+        D.cap = cap;
+        D.row_bytes = part_row_bytes_;
+        for (int c = 0; c < kMaxValueCols; c++) D.off_val[c] = part_off_val_[c];
+        D.todo = todo_all.as<int>();
+        D.start = start.as<uint32_t>();
+        D.failed = reinterpret_cast<int *>(ctl.as<uint8_t>() + 8);
+        D.L = L;
+        D.slots = (int)next_pow2((uint64_t)2 * L);
+        agg_part_kernel<<<nparts, kPartThreads, part_smem_, rt_->stream>>>(P, T, D);
+        rt_->launches++;
+        check_launch("agg_part_kernel");
+        DBuf todo;
+        for (int round = 0;; round++) {
+            struct {
+                unsigned long long deferred;
+                int failed, pad;
+            } c{};
+            read_device(rt_, ctl.get(), sizeof(c), &c);
+            const uint32_t st = take_status(rt_);
+            if (st & ST_TIMEOUT) fail(KRV_TIMEOUT, "aggregate: a wait for a group id gave up");
+            if (st & ST_CAPACITY) fail(KRV_INTERNAL, "aggregate: a hot key has no group");
+            known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());
+            if (c.failed == 0) {
+                drain_deferred(b, key0, ovf, ctl, c.deferred);
+                break;
+            }
+            if (round == 16) fail(KRV_INTERNAL, "aggregate: table growth did not converge");
+            // Partitions that stopped: their windows run again on a bigger table.
+            std::vector<uint32_t> hs(nparts), hc((size_t)nparts * kCntStride);
+            KRV_CUDA(cudaMemcpyAsync(hs.data(), start.get(), (size_t)nparts * 4, cudaMemcpyDeviceToHost, rt_->stream));
+            KRV_CUDA(cudaMemcpyAsync(hc.data(), part_cnt.get(), part_cnt.bytes(), cudaMemcpyDeviceToHost, rt_->stream));
+            KRV_CUDA(cudaStreamSynchronize(rt_->stream));
+            std::vector<int> again;
+            for (int p = 0; p < nparts; p++)
+                if (hs[p] < std::min<uint32_t>(hc[(size_t)p * kCntStride], cap)) again.push_back(p);
+            grow((uint64_t)known_groups_ + (uint64_t)again.size() * L + 1);
+            todo = DBuf(rt_, again.size() * 4);
+            KRV_CUDA(cudaMemcpyAsync(todo.get(), again.data(), again.size() * 4, cudaMemcpyHostToDevice, rt_->stream));
+            KRV_CUDA(cudaMemsetAsync(ctl.as<uint8_t>() + 8, 0, 4, rt_->stream));
+            TableDev T2{keys_.as<long long>(), gids_.as<uint32_t>(), slots_ - 1, states_.as<uint8_t>(),
+                        gkeys_.as<long long>(), ngroups_.as<unsigned long long>(), limit_, status_word(rt_)};
+            D.todo = todo.as<int>();
+            agg_part_kernel<<<(int)again.size(), kPartThreads, part_smem_, rt_->stream>>>(P, T2, D);
+            rt_->launches++;
+            check_launch("agg_part_kernel");
+            KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // `again` is a stack vector
+        }
+    }
+    const uint32_t st = take_status(rt_);
+    if (st & ST_TIMEOUT) fail(KRV_TIMEOUT, "aggregate: a wait for a group id gave up");
+    known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());
+}
+
 void HashAggregate::push(const DevBatch &in) {
     if (finished_) fail(KRV_INVALID_ARGUMENT, "push after finish");
     DeviceGuard g(rt_);
@@ -1190,6 +1890,10 @@ void HashAggregate::push(const DevBatch &in) {
     }
     const DevCol &kc = b.cols[key_col_];
     KeyIn key{kc.data, kc.valid, kc.valid_off, kc.type.width(), 0};
+    if (use_partitioned(n)) {
+        push_partitioned(b, key, n);
+        return;
+    }
     if (mode_ == KRV_AGG_MODE_SHARED && !sampled_) sample_hot(key, n);
     clear_status(rt_);
     DBuf ovf_count(rt_, 8);
