@@ -112,7 +112,7 @@ typedef struct {
     int32_t build_keys[KRV_MAX_KEYS];      /* build (right) key columns */
     int32_t null_safe[KRV_MAX_KEYS];       /* `<=>` instead of `=` */
     int32_t single_match;                  /* LeftOuter only: > 1 match fails */
-    int32_t has_residual_filter;           /* must be 0: residual filters are unsupported */
+    int32_t has_residual_filter;           /* 1: krv_join_set_filter gives the filter before the build */
     /* Output projection: probe columns then build columns. -1 = every column. */
     int32_t n_probe_out;
     int32_t probe_out[KRV_MAX_OUT_COLUMNS];
@@ -128,6 +128,50 @@ typedef struct {
     int64_t max_output_rows;   /* output batch bound; 0 = one batch per input */
 } krv_join_spec;
 void krv_join_spec_init(krv_join_spec *spec);
+
+/* ---- residual join filters ----------------------------------------------
+ * JoinSpec::filter (join/mod.rs:327-350), applied to every candidate pair of
+ * equal keys before it counts (join/probe.rs:393-489, the filter at
+ * :425-436): a pair matches only where the filter is TRUE (NULL is not a
+ * match), and the outer, semi, anti and existence results and the build-side
+ * marks of right/full joins follow the filtered matches; single_match counts
+ * filtered matches. The filter is a conjunction of comparisons between
+ * probe columns, build columns and constants (columns of the input batches,
+ * by index). Operands are int32/int64/date32 columns, decimal64 columns
+ * (compared as unscaled values: both sides of a comparison of two decimal
+ * columns must have one scale; a constant is unscaled at the column's
+ * scale), or float64 columns; a comparison with a float64 operand compares
+ * as float64 with Spark's order (NaN equal to NaN and above every other
+ * value, -0.0 equal to 0.0). A NULL operand makes its comparison, and so the
+ * filter, not TRUE. Not for null-aware anti joins (as the reference, which
+ * rejects that combination), partitioned joins, or joins on string keys. */
+#define KRV_MAX_FILTER_TERMS 8
+#define KRV_CMP_EQ 0
+#define KRV_CMP_NE 1
+#define KRV_CMP_LT 2
+#define KRV_CMP_LE 3
+#define KRV_CMP_GT 4
+#define KRV_CMP_GE 5
+#define KRV_OPERAND_PROBE 0      /* column `column` of the probe batch */
+#define KRV_OPERAND_BUILD 1      /* column `column` of the build batch */
+#define KRV_OPERAND_CONST_I64 2  /* the constant i64 */
+#define KRV_OPERAND_CONST_F64 3  /* the constant f64 */
+typedef struct {
+    int32_t kind;    /* KRV_OPERAND_* */
+    int32_t column;
+    int64_t i64;
+    double f64;
+} krv_filter_operand;
+typedef struct {
+    int32_t op;      /* KRV_CMP_*: left op right */
+    int32_t pad0;
+    krv_filter_operand left, right;
+} krv_filter_term;
+typedef struct {
+    int32_t n_terms; /* 1..KRV_MAX_FILTER_TERMS, all of which must be TRUE */
+    int32_t pad0;
+    krv_filter_term terms[KRV_MAX_FILTER_TERMS];
+} krv_join_filter;
 
 /* Counters (join/mod.rs:353-607) */
 typedef struct {
@@ -145,6 +189,10 @@ typedef struct krv_key_filter krv_key_filter;
 
 /* HashJoin::try_new (join/mod.rs:1014) */
 krv_status krv_join_create(krv_runtime *rt, const krv_join_spec *spec, krv_join **out);
+/* Sets the join's residual filter (see krv_join_filter); before the first
+ * build push. Column operands are checked against the batches' schemas at
+ * the first probe. */
+krv_status krv_join_set_filter(krv_join *j, const krv_join_filter *filter);
 /* BuildSink::sink (join/build.rs:1225-1335) */
 krv_status krv_join_build_push(krv_join *j, const struct ArrowArray *batch,
                                const struct ArrowSchema *schema);

@@ -101,6 +101,42 @@ class JoinSpec(C.Structure):
                 ("max_output_rows", C.c_int64)]
 
 
+CMP = {"=": 0, "!=": 1, "<": 2, "<=": 3, ">": 4, ">=": 5}
+OPERAND_PROBE, OPERAND_BUILD, OPERAND_CONST_I64, OPERAND_CONST_F64 = 0, 1, 2, 3
+MAX_FILTER_TERMS = 8
+
+
+class FilterOperand(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("column", C.c_int32), ("i64", C.c_int64), ("f64", C.c_double)]
+
+
+class FilterTerm(C.Structure):
+    _fields_ = [("op", C.c_int32), ("pad0", C.c_int32), ("left", FilterOperand), ("right", FilterOperand)]
+
+
+class JoinFilter(C.Structure):
+    _fields_ = [("n_terms", C.c_int32), ("pad0", C.c_int32), ("terms", FilterTerm * MAX_FILTER_TERMS)]
+
+
+def join_filter(terms) -> JoinFilter:
+    """A residual join filter (krv_join_filter): `terms` is a list of
+    (left, op, right), op one of = != < <= > >=, each operand ("probe", col),
+    ("build", col), an int (int64 constant) or a float (float64 constant).
+    Every term must be TRUE for a pair to match."""
+    f = JoinFilter()
+    f.n_terms = len(terms)
+
+    def operand(o):
+        if isinstance(o, tuple):
+            return FilterOperand(kind=OPERAND_PROBE if o[0] == "probe" else OPERAND_BUILD, column=o[1])
+        if isinstance(o, float):
+            return FilterOperand(kind=OPERAND_CONST_F64, f64=o)
+        return FilterOperand(kind=OPERAND_CONST_I64, i64=int(o))
+    for i, (l, op, r) in enumerate(terms):
+        f.terms[i] = FilterTerm(op=CMP[op], left=operand(l), right=operand(r))
+    return f
+
+
 class JoinCounters(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("build_rows", "build_keys", "table_slots", "probe_rows",
                                          "output_rows", "max_chain", "partitions")]
@@ -193,6 +229,7 @@ _SIGS = {
     "krv_join_finish_device": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema)]),
     "krv_join_key_filter": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "krv_join_counters_get": (C.c_int32, [C.c_void_p, C.POINTER(JoinCounters)]),
+    "krv_join_set_filter": (C.c_int32, [C.c_void_p, C.POINTER(JoinFilter)]),
     "krv_hash_rows_device": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                          C.c_uint64, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "krv_join_destroy": (None, [C.c_void_p]),
@@ -532,7 +569,8 @@ class HashJoin:
     or left outer on one int64 key, within `device_budget` bytes (0: the
     runtime's budget), spilling partitions to page-locked host memory."""
 
-    def __init__(self, rt: Runtime, spec: JoinSpec, partitioned: bool = False, device_budget: int = 0):
+    def __init__(self, rt: Runtime, spec: JoinSpec, partitioned: bool = False, device_budget: int = 0,
+                 filter=None):
         self.rt = rt
         h = C.c_void_p()
         if partitioned:
@@ -543,6 +581,10 @@ class HashJoin:
         else:
             check(lib().krv_join_create(rt.h, C.byref(spec), C.byref(h)))
         self.h = h
+        if filter is not None:
+            # a residual filter (join_filter(...) or its list of terms)
+            f = filter if isinstance(filter, JoinFilter) else join_filter(filter)
+            check(lib().krv_join_set_filter(self.h, C.byref(f)))
 
     def build_push(self, batch):
         with HostBatch(batch) as hb:

@@ -352,6 +352,16 @@ krv_status krv_join_key_filter(krv_join *j, krv_key_filter **out) {
         return KRV_OK;
     });
 }
+krv_status krv_join_set_filter(krv_join *j, const krv_join_filter *filter) {
+    return guard([&] {
+        need(j, "join");
+        need(filter, "filter");
+        if (j->g) krv::fail(KRV_UNSUPPORTED, "a residual filter on a partitioned join");
+        krv::DeviceGuard g(&j->owner->rt);
+        j->j->set_filter(*filter);
+        return KRV_OK;
+    });
+}
 krv_status krv_join_counters_get(const krv_join *j, krv_join_counters *out) {
     return guard([&] {
         need(j, "join");

@@ -179,6 +179,56 @@ __device__ __forceinline__ uint32_t lookup(const KeysDev &pk, int64_t i, const K
     return kNone;
 }
 
+// ---- residual filter (JoinSpec::filter, join/probe.rs:425-436) -------------------
+__device__ __forceinline__ bool filter_operand(const FilterOpDev &o, int64_t p, uint32_t b, long long &iv, double &fv) {
+    if (o.side == 2) {
+        iv = o.ci;
+        fv = o.is_float ? o.cf : (double)o.ci;
+        return true;
+    }
+    const int64_t r = o.side == 0 ? p : (int64_t)b;
+    if (!bit_get(o.valid, o.voff, r)) return false;
+    if (o.width == 4) {
+        iv = static_cast<const int *>(o.data)[r];
+        fv = (double)iv;
+    } else if (o.is_float) {
+        fv = static_cast<const double *>(o.data)[r];
+        iv = 0;
+    } else {
+        iv = static_cast<const long long *>(o.data)[r];
+        fv = (double)iv;
+    }
+    return true;
+}
+template <class T>
+__device__ __forceinline__ bool compare(int op, T a, T b) {
+    switch (op) {
+    case KRV_CMP_EQ: return a == b;
+    case KRV_CMP_NE: return a != b;
+    case KRV_CMP_LT: return a < b;
+    case KRV_CMP_LE: return a <= b;
+    case KRV_CMP_GT: return a > b;
+    default: return a >= b;
+    }
+}
+__device__ bool filter_true(const FilterDev &F, int64_t p, uint32_t b) {
+    for (int t = 0; t < F.n; t++) {
+        const FilterTermDev &T = F.t[t];
+        long long li, ri;
+        double lf, rf;
+        if (!filter_operand(T.l, p, b, li, lf) || !filter_operand(T.r, p, b, ri, rf)) return false;
+        const bool ok = T.as_float ? compare(T.op, f64_order_key(lf), f64_order_key(rf)) : compare(T.op, li, ri);
+        if (!ok) return false;
+    }
+    return true;
+}
+// The first build row of the chain from `cur` (newest first) whose pair
+// with probe row p passes the filter.
+__device__ __forceinline__ uint32_t first_true(const FilterDev &F, int64_t p, uint32_t cur, const uint32_t *next) {
+    while (cur != kNone && !filter_true(F, p, cur)) cur = next[cur];
+    return cur;
+}
+
 struct OutColDev {
     const void *src;
     const uint8_t *src_valid;
@@ -261,19 +311,21 @@ __device__ __forceinline__ unsigned long long round_alloc(unsigned long long *co
 }
 
 // Pairs: inner, left outer, right outer, full outer (join/probe.rs:266-502).
-template <bool FAST>
+template <bool FAST, bool FILT>
 __global__ void __launch_bounds__(256) probe_pairs_kernel(KeysDev pk, KeysDev bk, int64_t n,
                                                           const unsigned long long *slots, uint64_t mask,
                                                           const uint32_t *next, uint64_t seed, OutDev out,
                                                           unsigned long long cap, unsigned long long *count,
                                                           uint8_t *marks, int pads_probe, int single_match,
-                                                          uint32_t *status, unsigned long long *max_chain) {
+                                                          uint32_t *status, unsigned long long *max_chain,
+                                                          FilterDev F) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += stride) {
         const int64_t i = base + threadIdx.x;
         const bool live = i < n;
         uint32_t cur = kNone;
         if (live && matchable(pk, i)) cur = lookup<FAST>(pk, i, bk, slots, mask, seed);
+        if (FILT) cur = first_true(F, i, cur, next);
         bool pad = live && cur == kNone && pads_probe;
         unsigned chain = 0;
         while (__any_sync(kFull, cur != kNone || pad)) {
@@ -285,6 +337,7 @@ __global__ void __launch_bounds__(256) probe_pairs_kernel(KeysDev pk, KeysDev bk
                 if (marks) marks[cur] = 1;
                 chain++;
                 cur = next[cur];
+                if (FILT) cur = first_true(F, i, cur, next);
             } else {
                 pad = false;
             }
@@ -434,12 +487,12 @@ __global__ void __launch_bounds__(kFastThreads) probe_fast_kernel(KeysDev pk, Ke
 
 // Probe rows once: semi, anti, null-aware anti (join/mod.rs:27-34).
 // kind 0 semi, 1 anti, 2 null-aware anti.
-template <bool FAST>
+template <bool FAST, bool FILT>
 __global__ void __launch_bounds__(256) probe_rows_kernel(KeysDev pk, KeysDev bk, int64_t n,
                                                          const unsigned long long *slots, uint64_t mask,
                                                          uint64_t seed, OutDev out, unsigned long long cap,
                                                          unsigned long long *count, int kind, int build_empty,
-                                                         int build_has_null) {
+                                                         int build_has_null, const uint32_t *next, FilterDev F) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += stride) {
         const int64_t i = base + threadIdx.x;
@@ -447,7 +500,9 @@ __global__ void __launch_bounds__(256) probe_rows_kernel(KeysDev pk, KeysDev bk,
         bool ok = false;
         if (live) {
             const bool m = matchable(pk, i);
-            const bool hit = m && !build_empty && lookup<FAST>(pk, i, bk, slots, mask, seed) != kNone;
+            uint32_t c = m && !build_empty ? lookup<FAST>(pk, i, bk, slots, mask, seed) : kNone;
+            if (FILT) c = first_true(F, i, c, next);
+            const bool hit = c != kNone;
             if (kind == 0) ok = hit;
             else if (kind == 1) ok = !hit;
             else ok = build_empty || (!build_has_null && m && !hit);
@@ -460,15 +515,20 @@ __global__ void __launch_bounds__(256) probe_rows_kernel(KeysDev pk, KeysDev bk,
 
 // Existence: every probe row once plus `exists` (join/mod.rs:35-45). Rows
 // keep their positions; the flag of rows [base, base + 32) is one word.
-template <bool FAST>
+template <bool FAST, bool FILT>
 __global__ void __launch_bounds__(256) probe_exists_kernel(KeysDev pk, KeysDev bk, int64_t n,
                                                            const unsigned long long *slots, uint64_t mask,
-                                                           uint64_t seed, uint32_t *exists, int build_empty) {
+                                                           uint64_t seed, uint32_t *exists, int build_empty,
+                                                           const uint32_t *next, FilterDev F) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += stride) {
         const int64_t i = base + threadIdx.x;
         bool hit = false;
-        if (i < n && !build_empty && matchable(pk, i)) hit = lookup<FAST>(pk, i, bk, slots, mask, seed) != kNone;
+        if (i < n && !build_empty && matchable(pk, i)) {
+            uint32_t c = lookup<FAST>(pk, i, bk, slots, mask, seed);
+            if (FILT) c = first_true(F, i, c, next);
+            hit = c != kNone;
+        }
         const unsigned word = __ballot_sync(kFull, hit);
         if (lane_id() == 0 && (i < n)) exists[i >> 5] = word;
     }
@@ -549,8 +609,8 @@ HashJoin::HashJoin(Runtime *rt, const krv_join_spec &spec) : rt_(rt), spec_(spec
     if (spec.n_keys < 1 || spec.n_keys > KRV_MAX_KEYS) fail(KRV_INVALID_ARGUMENT, "join needs 1..4 keys");
     if (spec.join_type < KRV_JOIN_INNER || spec.join_type > KRV_JOIN_FULL_OUTER)
         fail(KRV_INVALID_ARGUMENT, "unknown join type");
-    if (spec.has_residual_filter)
-        fail(KRV_UNSUPPORTED, "KRISHIV_UNSUPPORTED_FEATURE: residual join filters on the GPU join");
+    if (spec.has_residual_filter && spec.join_type == KRV_JOIN_NULL_AWARE_ANTI)
+        fail(KRV_UNSUPPORTED, "KRISHIV_UNSUPPORTED_FEATURE: null-aware anti join with a residual condition");
     if (spec.single_match && spec.join_type != KRV_JOIN_LEFT_OUTER)
         fail(KRV_INVALID_ARGUMENT, "single_match is for left outer joins only");
     if (spec.join_type == KRV_JOIN_NULL_AWARE_ANTI && (spec.n_keys != 1 || spec.null_safe[0]))
@@ -641,6 +701,73 @@ static void reject_var(const DevBatch &b) {
         if (c.type.var()) fail(KRV_UNSUPPORTED, "column '" + c.name + "': string and binary columns are taken as keys only");
 }
 
+void HashJoin::set_filter(const krv_join_filter &f) {
+    if (decided_) fail(KRV_INVALID_ARGUMENT, "krv_join_set_filter after the first build push");
+    if (spec_.join_type == KRV_JOIN_NULL_AWARE_ANTI)
+        fail(KRV_UNSUPPORTED, "KRISHIV_UNSUPPORTED_FEATURE: null-aware anti join with a residual condition");
+    if (f.n_terms < 1 || f.n_terms > KRV_MAX_FILTER_TERMS)
+        fail(KRV_INVALID_ARGUMENT, "a residual filter has 1 to 8 comparisons");
+    for (int t = 0; t < f.n_terms; t++) {
+        const krv_filter_term &T = f.terms[t];
+        if (T.op < KRV_CMP_EQ || T.op > KRV_CMP_GE) fail(KRV_INVALID_ARGUMENT, "unknown comparison");
+        for (const krv_filter_operand *o : {&T.left, &T.right})
+            if (o->kind < KRV_OPERAND_PROBE || o->kind > KRV_OPERAND_CONST_F64)
+                fail(KRV_INVALID_ARGUMENT, "unknown filter operand kind");
+    }
+    residual_ = f;
+    residual_set_ = true;
+    spec_.has_residual_filter = 1;
+}
+
+// The device form of the residual filter over probe batch `in` and the arena.
+FilterDev HashJoin::filter_dev(const DevBatch &in) const {
+    FilterDev F{};
+    F.n = residual_.n_terms;
+    auto operand = [&](const krv_filter_operand &o, FilterOpDev &d, DType &t) {
+        d.side = o.kind == KRV_OPERAND_PROBE ? 0 : o.kind == KRV_OPERAND_BUILD ? 1 : 2;
+        if (d.side == 2) {
+            d.is_float = o.kind == KRV_OPERAND_CONST_F64;
+            d.ci = o.i64;
+            d.cf = o.f64;
+            t = DType{d.is_float ? Type::F64 : Type::I64, 0, 0};
+            return;
+        }
+        const int ncol = d.side == 0 ? (int)in.cols.size() : (int)arena_cols_.size();
+        if (o.column < 0 || o.column >= ncol) fail(KRV_INVALID_ARGUMENT, "residual filter column out of range");
+        const DevCol &meta = d.side == 0 ? in.cols[o.column] : arena_cols_[o.column];
+        t = meta.type;
+        if (t.id != Type::I32 && t.id != Type::Date32 && t.id != Type::I64 && t.id != Type::Dec64 && t.id != Type::F64)
+            fail(KRV_UNSUPPORTED, "a residual filter over " + t.format() + " columns");
+        d.width = t.width();
+        d.is_float = t.id == Type::F64;
+        if (d.side == 0) {
+            d.data = meta.data;
+            d.valid = meta.valid;
+            d.voff = meta.valid_off;
+        } else if (!arena_.cols.empty()) {
+            const DevCol &c = arena_.cols[o.column];
+            d.data = c.data;
+            d.valid = meta.nullable ? c.valid : nullptr;
+            d.voff = c.valid_off;
+        }
+    };
+    for (int t = 0; t < F.n; t++) {
+        const krv_filter_term &T = residual_.terms[t];
+        FilterTermDev &D = F.t[t];
+        D.op = T.op;
+        DType lt, rt;
+        operand(T.left, D.l, lt);
+        operand(T.right, D.r, rt);
+        D.as_float = D.l.is_float || D.r.is_float;
+        const bool ldec = lt.id == Type::Dec64, rdec = rt.id == Type::Dec64;
+        if (!D.as_float && D.l.side != 2 && D.r.side != 2 && ldec != rdec)
+            fail(KRV_UNSUPPORTED, "a residual filter compares a decimal column with an integer column");
+        if (ldec && rdec && lt.scale != rt.scale)
+            fail(KRV_UNSUPPORTED, "a residual filter compares decimal columns of different scales");
+    }
+    return F;
+}
+
 // Whether the keys are coded: some key column of the first build batch is
 // a string or binary column.
 void HashJoin::decide(const DevBatch &b) {
@@ -652,6 +779,7 @@ void HashJoin::decide(const DevBatch &b) {
         var = var || b.cols[c].type.var();
     }
     if (!var) return;
+    if (residual_set_) fail(KRV_UNSUPPORTED, "a residual filter on a join over string or binary keys");
     coded_.reset(new Coded());
     coded_->outer = spec_;
     std::vector<DevCol> meta;
@@ -917,6 +1045,29 @@ DevBatch HashJoin::probe(const DevBatch &outer_in) {
             fail(KRV_INVALID_ARGUMENT, "probe and build key types differ");
     }
     const bool fast = fast_keys(pk);
+    if (spec_.has_residual_filter && !residual_set_)
+        fail(KRV_INVALID_ARGUMENT, "has_residual_filter is set but no filter was given (krv_join_set_filter)");
+    const bool filt = residual_set_;
+    const FilterDev fd = filt ? filter_dev(in) : FilterDev{};
+    auto launch_pairs = [&](bool fast_, bool filt_, int grid_, int threads_, const KeysDev &pk_, const KeysDev &bk_,
+                            int64_t n_, const OutDev &od_, unsigned long long cap_, unsigned long long *count_,
+                            uint8_t *marks_p, int pad_, int single_, unsigned long long *mc_, const FilterDev &fd_) {
+        const auto *sl = slots_.as<unsigned long long>();
+        const uint32_t *nx = next_.as<uint32_t>();
+        uint32_t *st = status_word(rt_);
+        if (fast_ && filt_)
+            probe_pairs_kernel<true, true><<<grid_, threads_, 0, rt_->stream>>>(
+                pk_, bk_, n_, sl, mask_, nx, spec_.seed, od_, cap_, count_, marks_p, pad_, single_, st, mc_, fd_);
+        else if (fast_)
+            probe_pairs_kernel<true, false><<<grid_, threads_, 0, rt_->stream>>>(
+                pk_, bk_, n_, sl, mask_, nx, spec_.seed, od_, cap_, count_, marks_p, pad_, single_, st, mc_, fd_);
+        else if (filt_)
+            probe_pairs_kernel<false, true><<<grid_, threads_, 0, rt_->stream>>>(
+                pk_, bk_, n_, sl, mask_, nx, spec_.seed, od_, cap_, count_, marks_p, pad_, single_, st, mc_, fd_);
+        else
+            probe_pairs_kernel<false, false><<<grid_, threads_, 0, rt_->stream>>>(
+                pk_, bk_, n_, sl, mask_, nx, spec_.seed, od_, cap_, count_, marks_p, pad_, single_, st, mc_, fd_);
+    };
     const auto pcols = projection(spec_.n_probe_out, spec_.probe_out, (int)in.cols.size());
     const auto bcols = projection(spec_.n_build_out, spec_.build_out, (int)arena_cols_.size());
     const int threads = 256;
@@ -940,12 +1091,21 @@ DevBatch HashJoin::probe(const DevBatch &outer_in) {
         DevCol ex = make_col(rt_, DType{Type::Bool, 0, 0}, n, false, "exists");
         zero(rt_, const_cast<void *>(ex.data), ex.hold_data->bytes());
         if (n > 0) {
-            if (fast)
-                probe_exists_kernel<true><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, spec_.seed,
-                                                                             (uint32_t *)ex.data, build_rows_ == 0);
+            const uint32_t *nx = next_.as<uint32_t>();
+            uint32_t *exw = (uint32_t *)ex.data;
+            const int empty = build_rows_ == 0;
+            if (fast && filt)
+                probe_exists_kernel<true, true><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, spec_.seed,
+                                                                                   exw, empty, nx, fd);
+            else if (fast)
+                probe_exists_kernel<true, false><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, spec_.seed,
+                                                                                    exw, empty, nx, fd);
+            else if (filt)
+                probe_exists_kernel<false, true><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, spec_.seed,
+                                                                                    exw, empty, nx, fd);
             else
-                probe_exists_kernel<false><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, spec_.seed,
-                                                                              (uint32_t *)ex.data, build_rows_ == 0);
+                probe_exists_kernel<false, false><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, slots, mask_,
+                                                                                     spec_.seed, exw, empty, nx, fd);
             rt_->launches++;
             check_launch("probe_exists_kernel");
         }
@@ -965,14 +1125,8 @@ DevBatch HashJoin::probe(const DevBatch &outer_in) {
             DBuf cnt(rt_, 8);
             zero(rt_, cnt.get(), 8);
             auto *mc = counters_dev_.as<unsigned long long>() + 6;
-            if (fast)
-                probe_pairs_kernel<true><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, next_.as<uint32_t>(),
-                                                                            spec_.seed, od, 0, cnt.as<unsigned long long>(),
-                                                                            marks_.as<uint8_t>(), 0, 0, status_word(rt_), mc);
-            else
-                probe_pairs_kernel<false><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, slots, mask_, next_.as<uint32_t>(),
-                                                                             spec_.seed, od, 0, cnt.as<unsigned long long>(),
-                                                                             marks_.as<uint8_t>(), 0, 0, status_word(rt_), mc);
+            launch_pairs(fast, filt, grid, threads, pk, bk, n, od, 0, cnt.as<unsigned long long>(), marks_.as<uint8_t>(), 0,
+                         0, mc, fd);
             rt_->launches++;
             check_launch("probe_pairs_kernel");
         }
@@ -1039,7 +1193,7 @@ DevBatch HashJoin::probe(const DevBatch &outer_in) {
                     const int pad = jt == KRV_JOIN_LEFT_OUTER || jt == KRV_JOIN_FULL_OUTER;
                     // unique build keys: at most one output row per probe row
                     const bool unique = build_rows_ > 0 && counters_.build_keys == indexed_rows_;
-                    if (fast && unique && !marks && pk.null_safe == 0 &&
+                    if (fast && unique && !marks && pk.null_safe == 0 && !filt &&
                         (jt == KRV_JOIN_INNER || jt == KRV_JOIN_LEFT_OUTER)) {
                         const int fgrid = grid_for(rt_, ceil_div(n, kFastRows), kFastThreads, 8);
                         const DirectDev dd{direct_.as<uint32_t>(), key_lo_, direct_span_};
@@ -1049,14 +1203,10 @@ DevBatch HashJoin::probe(const DevBatch &outer_in) {
                         else
                             probe_fast_kernel<false><<<fgrid, kFastThreads, 0, rt_->stream>>>(
                                 pk, bk, n, slots, mask_, spec_.seed, dd, od, cap, count, pad);
-                    } else if (fast)
-                        probe_pairs_kernel<true><<<grid, threads, 0, rt_->stream>>>(
-                            pk, bk, n, slots, mask_, next_.as<uint32_t>(), spec_.seed, od, cap, count, marks, pad,
-                            spec_.single_match, status_word(rt_), mc);
-                    else
-                        probe_pairs_kernel<false><<<grid, threads, 0, rt_->stream>>>(
-                            pk, bk, n, slots, mask_, next_.as<uint32_t>(), spec_.seed, od, cap, count, marks, pad,
-                            spec_.single_match, status_word(rt_), mc);
+                    } else {
+                        launch_pairs(fast, filt, grid, threads, pk, bk, n, od, cap, count, marks, pad,
+                                     spec_.single_match, mc, fd);
+                    }
                     rt_->launches++;
                     check_launch("probe_pairs_kernel");
                 }
@@ -1064,14 +1214,20 @@ DevBatch HashJoin::probe(const DevBatch &outer_in) {
                 const int kind = jt == KRV_JOIN_LEFT_SEMI ? 0 : jt == KRV_JOIN_LEFT_ANTI ? 1 : 2;
                 const unsigned long long *sl = slots;
                 const uint64_t mask = mask_;
-                if (fast)
-                    probe_rows_kernel<true><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, sl, mask, spec_.seed, od, cap,
-                                                                               count, kind, build_rows_ == 0,
-                                                                               any_null_build_);
+                const uint32_t *nx = next_.as<uint32_t>();
+                const int empty = build_rows_ == 0, hn = any_null_build_;
+                if (fast && filt)
+                    probe_rows_kernel<true, true><<<grid, threads, 0, rt_->stream>>>(
+                        pk, bk, n, sl, mask, spec_.seed, od, cap, count, kind, empty, hn, nx, fd);
+                else if (fast)
+                    probe_rows_kernel<true, false><<<grid, threads, 0, rt_->stream>>>(
+                        pk, bk, n, sl, mask, spec_.seed, od, cap, count, kind, empty, hn, nx, fd);
+                else if (filt)
+                    probe_rows_kernel<false, true><<<grid, threads, 0, rt_->stream>>>(
+                        pk, bk, n, sl, mask, spec_.seed, od, cap, count, kind, empty, hn, nx, fd);
                 else
-                    probe_rows_kernel<false><<<grid, threads, 0, rt_->stream>>>(pk, bk, n, sl, mask, spec_.seed, od, cap,
-                                                                                count, kind, build_rows_ == 0,
-                                                                                any_null_build_);
+                    probe_rows_kernel<false, false><<<grid, threads, 0, rt_->stream>>>(
+                        pk, bk, n, sl, mask, spec_.seed, od, cap, count, kind, empty, hn, nx, fd);
                 rt_->launches++;
                 check_launch("probe_rows_kernel");
             }

@@ -73,6 +73,30 @@ DBuf key_dict_encode(KeyDict *d, const DevBatch &b, const std::vector<int> &cols
 std::vector<DevCol> key_dict_decode(KeyDict *d, const long long *codes, int64_t n);
 int64_t key_dict_size(const KeyDict *d);
 
+// ---- residual join filter, device form (join/probe.rs:425-436) -------------------
+// A conjunction of comparisons; a pair counts only where every one is TRUE
+// (a NULL operand is not TRUE).
+struct FilterOpDev {
+    int32_t side;      // 0 the probe row's column, 1 the build row's, 2 a constant
+    int32_t width;     // 4 or 8 (columns)
+    int32_t is_float;  // a float64 column or constant
+    int32_t pad;
+    const void *data;
+    const uint8_t *valid;
+    int64_t voff;
+    long long ci;
+    double cf;
+};
+struct FilterTermDev {
+    int32_t op;        // KRV_CMP_*
+    int32_t as_float;  // compare as float64 (Spark's order)
+    FilterOpDev l, r;
+};
+struct FilterDev {
+    FilterTermDev t[KRV_MAX_FILTER_TERMS];
+    int32_t n;
+};
+
 // ---- hash join (crates/krishiv-exec/src/join/mod.rs:1014 HashJoin) -------------
 class HashJoin {
   public:
@@ -103,6 +127,9 @@ class HashJoin {
         probe_names_.clear();
         probe_nullable_.clear();
     }
+
+    // Sets the residual filter (before the first build push).
+    void set_filter(const krv_join_filter &f);
 
     // Pending output batches for the bounded-output protocol.
     std::vector<DevBatch> pending;
@@ -142,6 +169,10 @@ class HashJoin {
     };
     std::unique_ptr<Coded> coded_;
     bool decided_ = false;
+    // The residual filter (JoinSpec::filter), set before the build.
+    krv_join_filter residual_{};
+    bool residual_set_ = false;
+    FilterDev filter_dev(const DevBatch &in) const;
     void decide(const DevBatch &b);
     DevBatch coded_batch(const DevBatch &b, bool build);
     // The column shape (types, names, nullability) of the probe output.

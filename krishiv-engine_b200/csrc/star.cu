@@ -36,67 +36,96 @@ namespace {
 constexpr long long kAttrEmpty = (long long)0x8080808080808080ULL;
 
 // Rows of a dimension with pred == value: their key and attribute, compacted
-// (the filter below the join build).
-// Each warp takes chunks of 16 x 32 rows: it reads pred for the chunk (one
-// ballot per 32 rows), reserves the chunk's output with one atomic, then
-// writes the survivors in row order.
+// (the filter below the join build). Each warp takes 16 x 32 rows of the
+// block's tile, reading pred once per row (one ballot per 32 rows); the
+// block reserves its tile's output with one atomic, so the shared counter
+// sees one update per 16K rows; the survivors are written in row order.
+// `range` (when given) gets the selected keys' min and max, `arange` the
+// selected attributes' (one update per block each).
 constexpr int kSelectSteps = 16;
-__global__ void __launch_bounds__(256) dim_select_kernel(const long long *key, const int32_t *pred, const int32_t *attr,
-                                                         int64_t n, int32_t value, long long *okey, int32_t *oattr,
-                                                         unsigned long long *count, long long *range) {
-    const int lane = threadIdx.x & 31;
-    long long lo = LLONG_MAX, hi = LLONG_MIN;  // selected keys' range (when `range`)
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
-    const int64_t chunk = 32 * kSelectSteps;
-    for (int64_t c0 = ((int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5)) * chunk; c0 < n;
-         c0 += warps * chunk) {
+constexpr int kSelectThreads = 1024;
+constexpr int kSelectTile = kSelectThreads * kSelectSteps;
+__global__ void __launch_bounds__(kSelectThreads) dim_select_kernel(const long long *key, const int32_t *pred,
+                                                                    const int32_t *attr, int64_t n, int32_t value,
+                                                                    long long *okey, int32_t *oattr,
+                                                                    unsigned long long *count, long long *range,
+                                                                    long long *arange) {
+    __shared__ unsigned s_tot[kSelectThreads / 32];
+    __shared__ unsigned long long s_base;
+    __shared__ long long s_rng[4][kSelectThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long lo = LLONG_MAX, hi = LLONG_MIN, alo = LLONG_MAX, ahi = LLONG_MIN;
+    for (int64_t t0 = (int64_t)blockIdx.x * kSelectTile; t0 < n; t0 += (int64_t)gridDim.x * kSelectTile) {
+        const int64_t c0 = t0 + (int64_t)warp * 32 * kSelectSteps;
         unsigned ballots[kSelectSteps];
-        int total = 0;
+        unsigned total = 0;
 #pragma unroll
         for (int s = 0; s < kSelectSteps; s++) {
             const int64_t i = c0 + s * 32 + lane;
             ballots[s] = __ballot_sync(0xFFFFFFFFu, i < n && pred[i] == value);
             total += __popc(ballots[s]);
         }
-        unsigned long long base = 0;
-        if (lane == 0 && total) base = atomicAdd(count, (unsigned long long)total);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (lane == 0) s_tot[warp] = total;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned acc = 0;
+            for (int w = 0; w < kSelectThreads / 32; w++) {
+                const unsigned t = s_tot[w];
+                s_tot[w] = acc;
+                acc += t;
+            }
+            s_base = acc ? atomicAdd(count, (unsigned long long)acc) : 0ull;
+        }
+        __syncthreads();
+        unsigned long long base = s_base + s_tot[warp];
 #pragma unroll
         for (int s = 0; s < kSelectSteps; s++) {
             if ((ballots[s] >> lane) & 1u) {
                 const int64_t i = c0 + s * 32 + lane;
                 const unsigned long long pos = base + __popc(ballots[s] & lanemask_lt());
                 const long long k = key[i];
+                const int32_t a = attr[i];
                 okey[pos] = k;
-                oattr[pos] = attr[i];
+                oattr[pos] = a;
                 lo = k < lo ? k : lo;
                 hi = k > hi ? k : hi;
+                alo = a < alo ? a : alo;
+                ahi = a > ahi ? a : ahi;
             }
             base += __popc(ballots[s]);
         }
+        __syncthreads();  // s_tot is rewritten by the next tile
     }
-    if (range) {
+    if (!range && !arange) return;
 #pragma unroll
-        for (int d = 16; d > 0; d >>= 1) {
-            const long long a = __shfl_xor_sync(0xFFFFFFFFu, lo, d), b = __shfl_xor_sync(0xFFFFFFFFu, hi, d);
-            lo = a < lo ? a : lo;
-            hi = b > hi ? b : hi;
+    for (int d = 16; d > 0; d >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, d));
+        hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, d));
+        alo = min(alo, __shfl_xor_sync(0xFFFFFFFFu, alo, d));
+        ahi = max(ahi, __shfl_xor_sync(0xFFFFFFFFu, ahi, d));
+    }
+    if (lane == 0) {
+        s_rng[0][warp] = lo;
+        s_rng[1][warp] = hi;
+        s_rng[2][warp] = alo;
+        s_rng[3][warp] = ahi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kSelectThreads / 32; w++) {
+            lo = min(lo, s_rng[0][w]);
+            hi = max(hi, s_rng[1][w]);
+            alo = min(alo, s_rng[2][w]);
+            ahi = max(ahi, s_rng[3][w]);
         }
-        if (lane == 0 && lo <= hi) {
+        if (lo <= hi && range) {
             atomicMin(range, lo);
             atomicMax(range + 1, hi);
         }
-    }
-}
-
-// A dimension with unique keys: group id (int16, -1 = no key) at key - lo.
-// Two rows with one key leave the index incomplete and set *dup.
-__global__ void dim_index_kernel(const long long *key, const int32_t *gid, int64_t n, long long lo,
-                                 unsigned short *direct, unsigned int *dup) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const unsigned long long off = (unsigned long long)(key[i] - lo);
-        const unsigned short old = atomicCAS(direct + off, (unsigned short)0xFFFFu, (unsigned short)gid[i]);
-        if (old != (unsigned short)0xFFFFu) atomicOr(dup, 1u);
+        if (alo <= ahi && arange) {
+            atomicMin(arange, alo);
+            atomicMax(arange + 1, ahi);
+        }
     }
 }
 
@@ -136,16 +165,159 @@ __global__ void attr_gid_kernel(const int32_t *attr, int64_t n, long long *tkeys
     }
 }
 
-// Plain form helpers: the scan's row stage keeps rows passing both filters.
+// The fast build's device-driven steps. `ctl` words (int64): [0..1] selected
+// rows per dimension, [2..5] their key (lo, hi), [6..7] the attribute (lo, hi)
+// of both dimensions, [8..9] duplicate-key flags, [10] group ids handed out by
+// the attribute table, [11] status bits.
+constexpr int kCtlWords = 12;
+constexpr unsigned long long kMaxDirectSpan = 1ull << 26;  // key values a direct index covers
+constexpr long long kDirectAttrSpan = 1024;                // attribute values that are their own group id
+
+// Marks [0, hi - lo] of a direct index empty (-1), when the span qualifies.
+__global__ void direct_fill_kernel(unsigned long long *direct, const long long *range) {
+    const long long lo = range[0], hi = range[1];
+    if (lo > hi) return;
+    const unsigned long long span = (unsigned long long)(hi - lo);
+    if (span >= kMaxDirectSpan) return;
+    const unsigned long long words = span / 4 + 1;  // four int16 entries per word
+    for (unsigned long long w = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; w < words;
+         w += (unsigned long long)gridDim.x * blockDim.x)
+        direct[w] = ~0ull;
+}
+
+// The group id of attribute value k in the shared attribute table (claimed
+// when new; readers wait, bounded, for its id).
+__device__ __forceinline__ int32_t attr_gid_of(long long k, long long *tkeys, int32_t *tgid, uint64_t mask,
+                                               int32_t *gattr, unsigned int *ngroups, uint32_t *status) {
+    uint64_t pos = hash_word((uint64_t)k) & mask;
+    for (uint64_t p = 0; p <= mask; p++) {
+        long long cur = __ldcg(tkeys + pos);
+        if (cur == kAttrEmpty)
+            cur = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(tkeys + pos),
+                                       (unsigned long long)kAttrEmpty, (unsigned long long)k);
+        if (cur == kAttrEmpty) {
+            const int32_t g = (int32_t)atomicAdd(ngroups, 1u);
+            gattr[g] = (int32_t)k;
+            __threadfence();
+            atomicExch(tgid + pos, g);
+            return g;
+        }
+        if (cur == k) {
+            for (int it = 0; it < (1 << 22); it++) {
+                const int32_t g = *reinterpret_cast<volatile int32_t *>(tgid + pos);
+                if (g >= 0) return g;
+                __nanosleep(20);
+            }
+            atomicOr(status, ST_TIMEOUT);
+            return 0;
+        }
+        pos = (pos + 1) & mask;
+    }
+    return 0;
+}
+
+// Each selected row's group id at its key's place of the direct index: the
+// attribute itself (minus the lowest) when both dimensions' attributes span
+// fewer than kDirectAttrSpan values, else the attribute table's id. Two rows
+// with one key set the dimension's duplicate flag.
+__global__ void dim_index_fast_kernel(const long long *key, const int32_t *attr, long long *ctl, int d,
+                                      unsigned short *direct, long long *tkeys, int32_t *tgid, uint64_t mask,
+                                      int32_t *gattr) {
+    const unsigned long long n = (unsigned long long)ctl[d];
+    const long long lo = ctl[2 + 2 * d], hi = ctl[3 + 2 * d];
+    if (lo > hi || (unsigned long long)(hi - lo) >= kMaxDirectSpan) return;
+    const long long alo = ctl[6], ahi = ctl[7];
+    const bool own = ahi - alo < kDirectAttrSpan;
+    unsigned int *dup = reinterpret_cast<unsigned int *>(ctl + 8 + d);
+    unsigned int *ngroups = reinterpret_cast<unsigned int *>(ctl + 10);
+    uint32_t *status = reinterpret_cast<uint32_t *>(ctl + 11);
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const long long a = attr[i];
+        const int32_t g = own ? (int32_t)(a - alo) : attr_gid_of(a, tkeys, tgid, mask, gattr, ngroups, status);
+        const unsigned long long off = (unsigned long long)(key[i] - lo);
+        const unsigned short old = atomicCAS(direct + off, (unsigned short)0xFFFFu, (unsigned short)g);
+        if (old != (unsigned short)0xFFFFu) atomicOr(dup, 1u);
+    }
+}
+
+// gattr[g] = lo + g: the attribute values that are their own group ids.
+__global__ void attr_iota_kernel(int32_t *gattr, long long lo, int G) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) gattr[g] = (int32_t)(lo + g);
+}
+
+// The result rows: groups with joined rows in group-id order, (attr, sum of
+// the double-double accumulator rounded once, sum valid unless every value
+// was NULL). One block; out[0] = rows, out[1] = NULL sums, out[2..4] the
+// scan statistics.
+constexpr int kResultThreads = 1024;
+__global__ void __launch_bounds__(kResultThreads) star_result_kernel(int G, const int32_t *gattr, const double *hi,
+                                                                     const double *lo, const unsigned long long *cnt,
+                                                                     const unsigned long long *nulls,
+                                                                     const unsigned long long *stats, int32_t *oattr,
+                                                                     double *osum, uint32_t *ovalid,
+                                                                     unsigned long long *out) {
+    __shared__ unsigned s_warp[kResultThreads / 32];
+    __shared__ unsigned s_base, s_nulls;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        s_base = 0;
+        s_nulls = 0;
+    }
+    for (int w = threadIdx.x; w < (G + 31) / 32; w += kResultThreads) ovalid[w] = 0;
+    __syncthreads();
+    for (int g0 = 0; g0 < G; g0 += kResultThreads) {
+        const int g = g0 + threadIdx.x;
+        const bool has = g < G && cnt[g] > 0;
+        const unsigned b = __ballot_sync(0xFFFFFFFFu, has);
+        if (lane == 0) s_warp[warp] = __popc(b);
+        __syncthreads();
+        unsigned before = s_base;
+        for (int w = 0; w < warp; w++) before += s_warp[w];
+        const unsigned pos = before + __popc(b & lanemask_lt());
+        if (has) {
+            const double h = hi[g];
+            oattr[pos] = gattr[g];
+            osum[pos] = isfinite(h) ? __dadd_rn(h, lo[g]) : h;
+            if (cnt[g] > nulls[g]) atomicOr(ovalid + (pos >> 5), 1u << (pos & 31));
+            else atomicAdd(&s_nulls, 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int w = 0; w < kResultThreads / 32; w++) s_base += s_warp[w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = s_base;
+        out[1] = s_nulls;
+        out[2] = stats[0];
+        out[3] = stats[1];
+        out[4] = stats[2];
+    }
+}
+
+// Plain form helpers: the scan's row stage keeps rows passing both filters
+// (a null `pass_*` passes every row) whose keys are both valid (a NULL key
+// never joins). `ovv`, when given (zeroed words), gets bit `pos` set where
+// the kept row's price and discount are both valid.
+struct FactValid {
+    const uint8_t *v[4];  // fk_a, fk_b, price, discount (null: no NULLs)
+    int64_t o[4];
+};
 __global__ void __launch_bounds__(256) compact4_kernel(const uint32_t *pass_a, const uint32_t *pass_b, int64_t n,
-                                                       const long long *c0, const long long *c1, const long long *c2,
-                                                       const double *c3, long long *o0, long long *o1, long long *o2,
-                                                       double *o3, unsigned long long *count) {
+                                                       FactValid V, const long long *c0, const long long *c1,
+                                                       const long long *c2, const double *c3, long long *o0,
+                                                       long long *o1, long long *o2, double *o3, uint32_t *ovv,
+                                                       unsigned long long *count) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += stride) {
         const int64_t i = base + threadIdx.x;
         bool ok = false;
-        if (i < n) ok = ((pass_a[i >> 5] & pass_b[i >> 5]) >> (i & 31)) & 1u;
+        if (i < n) {
+            const uint32_t a = pass_a ? pass_a[i >> 5] : ~0u, b = pass_b ? pass_b[i >> 5] : ~0u;
+            ok = ((a & b) >> (i & 31)) & 1u;
+            ok = ok && bit_get(V.v[0], V.o[0], i) && bit_get(V.v[1], V.o[1], i);
+        }
         const unsigned ballot = __ballot_sync(0xFFFFFFFFu, ok);
         unsigned long long first = 0;
         if (lane_id() == 0 && ballot) first = atomicAdd(count, (unsigned long long)__popc(ballot));
@@ -156,6 +328,8 @@ __global__ void __launch_bounds__(256) compact4_kernel(const uint32_t *pass_a, c
             o1[pos] = c1[i];
             o2[pos] = c2[i];
             o3[pos] = c3[i];
+            if (ovv && bit_get(V.v[2], V.o[2], i) && bit_get(V.v[3], V.o[3], i))
+                atomicOr(ovv + (pos >> 5), 1u << (pos & 31));
         }
     }
 }
@@ -194,20 +368,24 @@ class StarPipeline {
     }
 
     // The fused plan's build when both dimensions have unique keys over spans
-    // of at most 2^26 values (the common star schema): select both, then
-    // dense group ids, an int16 direct index and the key filter from the
-    // selection's count and range; two host reads in all. False (nothing
-    // kept) when a dimension does not qualify: the join-table build runs.
+    // of at most 2^26 values (the common star schema): select both, then the
+    // direct indexes (key -> group id, int16), with every step sized from the
+    // selection on the device; one host read of the counts, ranges and
+    // duplicate flags; then the key filters from the selection's count and
+    // range. False (nothing kept) when a dimension does not qualify: the
+    // join-table build runs.
+    int select_grid(int64_t n) const {
+        return (int)std::max<int64_t>(1, std::min<int64_t>(2 * rt_->sm_count, ceil_div(n, kSelectTile)));
+    }
     bool build_fast(const DevBatch *dims[2], const int32_t values[2]) {
         struct Sel {
-            DBuf key, attr, gid;
+            DBuf key, attr;
             int64_t rows = 0;
             long long lo = 0, hi = -1;
         } sel[2];
-        // [0..1] counts, [2..5] (lo, hi) per dimension
-        DBuf ctl(rt_, 6 * 8);
-        const unsigned long long init[6] = {0, 0, (unsigned long long)LLONG_MAX, (unsigned long long)LLONG_MIN,
-                                            (unsigned long long)LLONG_MAX, (unsigned long long)LLONG_MIN};
+        DBuf ctl(rt_, kCtlWords * 8);
+        const long long init[kCtlWords] = {0, 0, LLONG_MAX, LLONG_MIN, LLONG_MAX, LLONG_MIN, LLONG_MAX, LLONG_MIN,
+                                           0, 0, 0, 0};
         KRV_CUDA(cudaMemcpyAsync(ctl.get(), init, sizeof(init), cudaMemcpyHostToDevice, rt_->stream));
         for (int d = 0; d < 2; d++) {
             const DevBatch &b = *dims[d];
@@ -215,47 +393,55 @@ class StarPipeline {
             sel[d].key = DBuf(rt_, (size_t)std::max<int64_t>(n, 1) * 8);
             sel[d].attr = DBuf(rt_, (size_t)std::max<int64_t>(n, 1) * 4);
             if (n > 0) {
-                dim_select_kernel<<<grid_for(rt_, n, 256, 8), 256, 0, rt_->stream>>>(
+                dim_select_kernel<<<select_grid(n), kSelectThreads, 0, rt_->stream>>>(
                     static_cast<const long long *>(b.cols[spec_.dim_key].data),
                     static_cast<const int32_t *>(b.cols[spec_.dim_pred].data),
                     static_cast<const int32_t *>(b.cols[spec_.dim_attr].data), n, values[d], sel[d].key.as<long long>(),
-                    sel[d].attr.as<int32_t>(), ctl.as<unsigned long long>() + d, ctl.as<long long>() + 2 + 2 * d);
+                    sel[d].attr.as<int32_t>(), ctl.as<unsigned long long>() + d, ctl.as<long long>() + 2 + 2 * d,
+                    ctl.as<long long>() + 6);
                 rt_->launches++;
                 check_launch("dim_select_kernel");
             }
         }
-        unsigned long long got[6];
-        KRV_CUDA(cudaMemcpyAsync(got, ctl.get(), sizeof(got), cudaMemcpyDeviceToHost, rt_->stream));
-        KRV_CUDA(cudaStreamSynchronize(rt_->stream));
         for (int d = 0; d < 2; d++) {
-            sel[d].rows = (int64_t)got[d];
-            sel[d].lo = (long long)got[2 + 2 * d];
-            sel[d].hi = (long long)got[3 + 2 * d];
+            if (!direct_full_[d].get()) direct_full_[d] = DBuf(rt_, (size_t)(kMaxDirectSpan + 4) * 2);
+            direct_fill_kernel<<<2 * rt_->sm_count, 256, 0, rt_->stream>>>(direct_full_[d].as<unsigned long long>(),
+                                                                           ctl.as<long long>() + 2 + 2 * d);
+            rt_->launches++;
+            check_launch("direct_fill_kernel");
+        }
+        for (int d = 0; d < 2; d++) {
+            const int64_t n = dims[d]->rows;
+            if (n <= 0) continue;
+            dim_index_fast_kernel<<<grid_for(rt_, std::max<int64_t>(1, n / 16), 256, 8), 256, 0, rt_->stream>>>(
+                sel[d].key.as<long long>(), sel[d].attr.as<int32_t>(), ctl.as<long long>(), d,
+                direct_full_[d].as<unsigned short>(), gkeys_.as<long long>(), gtab_.as<int32_t>(), gmask_,
+                gattr_.as<int32_t>());
+            rt_->launches++;
+            check_launch("dim_index_fast_kernel");
+        }
+        long long got[kCtlWords];
+        read_device(rt_, ctl.get(), sizeof(got), got);
+        if ((uint32_t)got[11] & ST_TIMEOUT) fail(KRV_TIMEOUT, "star build: a wait for a group id gave up");
+        for (int d = 0; d < 2; d++) {
+            sel[d].rows = got[d];
+            sel[d].lo = got[2 + 2 * d];
+            sel[d].hi = got[3 + 2 * d];
             if (sel[d].rows <= 0) return false;
             const __int128 span = (__int128)sel[d].hi - (__int128)sel[d].lo;
-            if (span < 0 || span >= ((__int128)1 << 26)) return false;
+            if (span < 0 || span >= (__int128)kMaxDirectSpan) return false;
+            if ((uint32_t)got[8 + d]) return false;  // duplicate dimension keys: the join-table build
         }
-        // dense group ids, then the direct indexes (duplicates flagged)
-        DBuf flags(rt_, 4 * 4);  // [0] ngroups, [1..2] duplicate keys, [3] status
-        KRV_CUDA(cudaMemsetAsync(flags.get(), 0, 16, rt_->stream));
-        DBuf direct[2];
-        for (int d = 0; d < 2; d++) {
-            const int64_t rows = sel[d].rows;
-            sel[d].gid = DBuf(rt_, (size_t)rows * 4);
-            attr_gid_kernel<<<grid_for(rt_, rows, 256, 8), 256, 0, rt_->stream>>>(
-                sel[d].attr.as<int32_t>(), rows, gkeys_.as<long long>(), gtab_.as<int32_t>(), gmask_, sel[d].gid.as<int32_t>(),
-                gattr_.as<int32_t>(), flags.as<unsigned int>(), flags.as<uint32_t>() + 3);
+        const long long alo = got[6], ahi = got[7];
+        if (ahi - alo < kDirectAttrSpan) {
+            ngroups_host_ = (int)(ahi - alo + 1);
+            attr_iota_kernel<<<1, 1024, 0, rt_->stream>>>(gattr_.as<int32_t>(), alo, ngroups_host_);
             rt_->launches++;
-            check_launch("attr_gid_kernel");
-            const size_t span = (size_t)(sel[d].hi - sel[d].lo) + 1;
-            direct[d] = DBuf(rt_, span * 2);
-            KRV_CUDA(cudaMemsetAsync(direct[d].get(), 0xFF, span * 2, rt_->stream));
-            dim_index_kernel<<<grid_for(rt_, rows, 256, 8), 256, 0, rt_->stream>>>(
-                sel[d].key.as<long long>(), sel[d].gid.as<int32_t>(), rows, sel[d].lo, direct[d].as<unsigned short>(),
-                flags.as<unsigned int>() + 1 + d);
-            rt_->launches++;
-            check_launch("dim_index_kernel");
+            check_launch("attr_iota_kernel");
+        } else {
+            ngroups_host_ = (int)(uint32_t)got[10];
         }
+        if (ngroups_host_ > (int)gmask_ / 2) fail(KRV_UNSUPPORTED, "more than 32768 distinct attribute values");
         // key filters from the selection's stats (keys unique: distinct = rows)
         std::shared_ptr<KeyFilterImpl> filt[2];
         if (spec_.use_filters) {
@@ -271,19 +457,11 @@ class StarPipeline {
                 filt[d] = build_key_filter(rt_, fo, kc, &ks);
             }
         }
-        uint32_t fl[4];
-        KRV_CUDA(cudaMemcpyAsync(fl, flags.get(), sizeof(fl), cudaMemcpyDeviceToHost, rt_->stream));
-        KRV_CUDA(cudaStreamSynchronize(rt_->stream));
-        if (fl[3] & ST_TIMEOUT) fail(KRV_TIMEOUT, "star build: a wait for a group id gave up");
-        if (fl[1] || fl[2]) return false;  // duplicate dimension keys: the join-table build
-        ngroups_host_ = (int)fl[0];
-        if (ngroups_host_ > (int)gmask_ / 2) fail(KRV_UNSUPPORTED, "more than 32768 distinct attribute values");
         for (int d = 0; d < 2; d++) {
             dims_[d] = Dim{};
             dims_[d].rows = sel[d].rows;
             filt_[d] = filt[d];
-            direct_buf_[d] = std::move(direct[d]);
-            direct_[d] = StarDirect{direct_buf_[d].get(), sel[d].lo, (unsigned long long)(sel[d].hi - sel[d].lo), 2};
+            direct_[d] = StarDirect{direct_full_[d].get(), sel[d].lo, (unsigned long long)(sel[d].hi - sel[d].lo), 2};
         }
         counters_.dim_a_keys = sel[0].rows;
         counters_.dim_b_keys = sel[1].rows;
@@ -299,10 +477,10 @@ class StarPipeline {
         DBuf cnt(rt_, 8);
         KRV_CUDA(cudaMemsetAsync(cnt.get(), 0, 8, rt_->stream));
         if (n > 0) {
-            dim_select_kernel<<<grid_for(rt_, n, 256, 8), 256, 0, rt_->stream>>>(
+            dim_select_kernel<<<select_grid(n), kSelectThreads, 0, rt_->stream>>>(
                 static_cast<const long long *>(d.cols[c_key].data), static_cast<const int32_t *>(d.cols[c_pred].data),
                 static_cast<const int32_t *>(d.cols[c_attr].data), n, value, out.key.as<long long>(),
-                out.attr.as<int32_t>(), cnt.as<unsigned long long>(), nullptr);
+                out.attr.as<int32_t>(), cnt.as<unsigned long long>(), nullptr, nullptr);
             rt_->launches++;
             check_launch("dim_select_kernel");
         }
@@ -388,6 +566,7 @@ class StarPipeline {
         sum_hi_ = DBuf(rt_, G * 8);
         sum_lo_ = DBuf(rt_, G * 8);
         cnt_ = DBuf(rt_, G * 8);
+        nulls_ = DBuf(rt_, G * 8);
         stats_ = DBuf(rt_, 32);
         reset();
         if (!fast) {
@@ -419,6 +598,7 @@ class StarPipeline {
         KRV_CUDA(cudaMemsetAsync(sum_hi_.get(), 0, G * 8, rt_->stream));
         KRV_CUDA(cudaMemsetAsync(sum_lo_.get(), 0, G * 8, rt_->stream));
         KRV_CUDA(cudaMemsetAsync(cnt_.get(), 0, G * 8, rt_->stream));
+        KRV_CUDA(cudaMemsetAsync(nulls_.get(), 0, G * 8, rt_->stream));
         KRV_CUDA(cudaMemsetAsync(stats_.get(), 0, 32, rt_->stream));
         counters_.fact_rows = 0;
         if (plain_agg_) {
@@ -435,7 +615,6 @@ class StarPipeline {
             if (c[i] < 0 || c[i] >= nc) fail(KRV_INVALID_ARGUMENT, "fact column out of range");
             if (f.cols[c[i]].type.id != t[i])
                 fail(KRV_UNSUPPORTED, "star fact columns are (int64 fk_a, int64 fk_b, int64 price, float64 discount)");
-            if (f.cols[c[i]].valid) fail(KRV_UNSUPPORTED, "star fact columns without NULLs");
         }
     }
 
@@ -489,7 +668,18 @@ class StarPipeline {
         A.sum_hi = sum_hi_.as<double>();
         A.sum_lo = sum_lo_.as<double>();
         A.cnt = cnt_.as<unsigned long long>();
+        A.nulls = nulls_.as<unsigned long long>();
         A.stats = stats_.as<unsigned long long>();
+        const DevCol &ca = f.cols[spec_.fact_fk_a], &cb = f.cols[spec_.fact_fk_b];
+        const DevCol &cp = f.cols[spec_.fact_price], &cd = f.cols[spec_.fact_discount];
+        A.v_fk_a = ca.valid;
+        A.o_fk_a = ca.valid_off;
+        A.v_fk_b = cb.valid;
+        A.o_fk_b = cb.valid_off;
+        A.v_price = cp.valid;
+        A.o_price = cp.valid_off;
+        A.v_disc = cd.valid;
+        A.o_disc = cd.valid_off;
         // B's filter answer bitmap (built with the dimensions) is staged in
         // shared memory when it fits.
         A.bits_b = A.use_filters && bits_[1].get() ? bits_[1].as<uint32_t>() : nullptr;
@@ -534,6 +724,10 @@ class StarPipeline {
             A.fk_a += r0;
             A.price += r0;
             A.disc += r0;
+            A.o_fk_a += r0;
+            A.o_fk_b += r0;
+            A.o_price += r0;
+            A.o_disc += r0;
             A.n = n;
             // The join reads the survivor list, not fk_b: the stage is free
             // once the scan is done.
@@ -644,27 +838,46 @@ class StarPipeline {
         const int64_t n = f.rows;
         const DevCol &ca = f.cols[spec_.fact_fk_a], &cb = f.cols[spec_.fact_fk_b];
         const DevCol &cp = f.cols[spec_.fact_price], &cd = f.cols[spec_.fact_discount];
-        // 1-2. the row stage: both runtime filters, then compaction
+        // 1-2. the row stage: both runtime filters, then compaction (also
+        // when columns have NULLs: rows with a NULL key go, and the price
+        // column of the kept rows carries whether their value is valid)
         DevBatch kept;
-        if (spec_.use_filters && fa && fb) {
-            DevCol pb = evaluate_key_filter(*fb, cb);
-            DevCol pa = evaluate_key_filter(*fa, ca);
+        const bool filters = spec_.use_filters && fa && fb;
+        const bool nullable = ca.valid || cb.valid || cp.valid || cd.valid;
+        if (filters || nullable) {
+            DevCol pb, pa;
+            if (filters) {
+                pb = evaluate_key_filter(*fb, cb);
+                pa = evaluate_key_filter(*fa, ca);
+            }
             DevCol o0 = make_col(rt_, ca.type, n, false, "fk_a"), o1 = make_col(rt_, cb.type, n, false, "fk_b");
             DevCol o2 = make_col(rt_, cp.type, n, false, "price"), o3 = make_col(rt_, cd.type, n, false, "discount");
+            const bool value_nulls = cp.valid || cd.valid;
+            if (value_nulls) {
+                o2.hold_valid = std::make_shared<DBuf>(rt_, (size_t)ceil_div(std::max<int64_t>(n, 1), 32) * 4);
+                KRV_CUDA(cudaMemsetAsync(o2.hold_valid->get(), 0, o2.hold_valid->bytes(), rt_->stream));
+                o2.valid = o2.hold_valid->as<uint8_t>();
+                o2.valid_off = 0;
+                o2.nullable = true;
+            }
             DBuf cnt(rt_, 8);
             KRV_CUDA(cudaMemsetAsync(cnt.get(), 0, 8, rt_->stream));
             if (n > 0) {
+                const FactValid V{{ca.valid, cb.valid, cp.valid, cd.valid},
+                                  {ca.valid_off, cb.valid_off, cp.valid_off, cd.valid_off}};
                 compact4_kernel<<<grid_for(rt_, n, 256, 8), 256, 0, rt_->stream>>>(
-                    (const uint32_t *)pa.data, (const uint32_t *)pb.data, n, (const long long *)ca.data,
-                    (const long long *)cb.data, (const long long *)cp.data, (const double *)cd.data, (long long *)o0.data,
-                    (long long *)o1.data, (long long *)o2.data, (double *)o3.data, cnt.as<unsigned long long>());
+                    filters ? (const uint32_t *)pa.data : nullptr, filters ? (const uint32_t *)pb.data : nullptr, n, V,
+                    (const long long *)ca.data, (const long long *)cb.data, (const long long *)cp.data,
+                    (const double *)cd.data, (long long *)o0.data, (long long *)o1.data, (long long *)o2.data,
+                    (double *)o3.data, value_nulls ? o2.hold_valid->as<uint32_t>() : nullptr,
+                    cnt.as<unsigned long long>());
                 rt_->launches++;
                 check_launch("compact4_kernel");
             }
             kept.rows = (int64_t)read_scalar<unsigned long long>(rt_, cnt.get());
             kept.cols = {o0, o1, o2, o3};
             for (auto &c : kept.cols) c.length = kept.rows;
-            counters_.passed_filters += kept.rows;
+            if (filters) counters_.passed_filters += kept.rows;
         } else {
             kept.rows = n;
             kept.cols = {ca, cb, cp, cd};
@@ -696,6 +909,12 @@ class StarPipeline {
                 (const long long *)j2.cols[0].data, (const double *)j2.cols[1].data, j2.rows, (double *)val.data);
             rt_->launches++;
             check_launch("project_kernel");
+        }
+        if (j2.cols[0].valid) {  // a NULL price or discount: a NULL value, skipped by SUM
+            val.valid = j2.cols[0].valid;
+            val.valid_off = j2.cols[0].valid_off;
+            val.hold_valid = j2.cols[0].hold_valid;
+            val.nullable = true;
         }
         DevBatch proj;
         proj.rows = j2.rows;
@@ -738,38 +957,45 @@ class StarPipeline {
         DeviceGuard g(rt_);
         DevBatch out;
         const int G = std::max(ngroups_host_, 0);
-        std::vector<double> hi(G), lo(G);
-        std::vector<unsigned long long> cnt(G);
         std::vector<int32_t> gattr(G);
+        if (spec_.mode == KRV_STAR_FUSED) {
+            // Compacted on the device; one host read of the row count and the
+            // statistics.
+            const int64_t cap = std::max(G, 1);
+            DevCol a = make_col(rt_, DType{Type::I32, 0, 0}, cap, false, "attr");
+            DevCol sc = make_col(rt_, DType{Type::F64, 0, 0}, cap, false, "sum");
+            auto valid = std::make_shared<DBuf>(rt_, (size_t)ceil_div(cap, 32) * 4);
+            DBuf info(rt_, 5 * 8);
+            star_result_kernel<<<1, kResultThreads, 0, rt_->stream>>>(
+                G, gattr_.as<int32_t>(), sum_hi_.as<double>(), sum_lo_.as<double>(), cnt_.as<unsigned long long>(),
+                nulls_.as<unsigned long long>(), stats_.as<unsigned long long>(), const_cast<int32_t *>(
+                    static_cast<const int32_t *>(a.data)), const_cast<double *>(static_cast<const double *>(sc.data)),
+                valid->as<uint32_t>(), info.as<unsigned long long>());
+            rt_->launches++;
+            check_launch("star_result_kernel");
+            unsigned long long r[5];
+            read_device(rt_, info.get(), sizeof(r), r);
+            counters_.passed_filters = (int64_t)r[2];
+            counters_.joined_rows = (int64_t)r[3];
+            counters_.fk_a_sectors = (int64_t)r[4];
+            a.length = sc.length = (int64_t)r[0];
+            if (r[1]) {
+                sc.hold_valid = valid;
+                sc.valid = valid->as<uint8_t>();
+                sc.valid_off = 0;
+                sc.nullable = true;
+            }
+            out.rows = (int64_t)r[0];
+            out.cols = {a, sc};
+            return out;
+        }
         if (G > 0) {
             KRV_CUDA(cudaMemcpyAsync(gattr.data(), gattr_.get(), (size_t)G * 4, cudaMemcpyDeviceToHost, rt_->stream));
-        }
-        if (spec_.mode == KRV_STAR_FUSED) {
-            if (G > 0) {
-                KRV_CUDA(cudaMemcpyAsync(hi.data(), sum_hi_.get(), (size_t)G * 8, cudaMemcpyDeviceToHost, rt_->stream));
-                KRV_CUDA(cudaMemcpyAsync(lo.data(), sum_lo_.get(), (size_t)G * 8, cudaMemcpyDeviceToHost, rt_->stream));
-                KRV_CUDA(cudaMemcpyAsync(cnt.data(), cnt_.get(), (size_t)G * 8, cudaMemcpyDeviceToHost, rt_->stream));
-            }
-            unsigned long long st[3];
-            KRV_CUDA(cudaMemcpyAsync(st, stats_.get(), 24, cudaMemcpyDeviceToHost, rt_->stream));
-            KRV_CUDA(cudaStreamSynchronize(rt_->stream));
-            counters_.passed_filters = (int64_t)st[0];
-            counters_.joined_rows = (int64_t)st[1];
-            counters_.fk_a_sectors = (int64_t)st[2];
-            // The groups with rows, in group-id order: (attr, hi + lo), the
-            // double-double sum rounded once.
-            std::vector<int32_t> oa;
-            std::vector<double> os;
-            for (int g = 0; g < G; g++)
-                if (cnt[g]) {
-                    oa.push_back(gattr[g]);
-                    os.push_back(std::isfinite(hi[g]) ? hi[g] + lo[g] : hi[g]);
-                }
-            return host_result(oa, os);
         }
         KRV_CUDA(cudaStreamSynchronize(rt_->stream));
         std::vector<int32_t> oa;
         std::vector<double> os;
+        std::vector<uint8_t> ov;
         if (plain_agg_) {
             DevBatch r = agg_result(plain_agg_);
             const int64_t m = r.rows;
@@ -780,22 +1006,40 @@ class StarPipeline {
                 KRV_CUDA(cudaMemcpyAsync(sum.data(), r.cols[1].data, (size_t)m * 8, cudaMemcpyDeviceToHost, rt_->stream));
                 KRV_CUDA(cudaStreamSynchronize(rt_->stream));
             }
+            const int64_t sv_bytes = ceil_div(std::max<int64_t>(r.cols[1].valid_off + m, 1), 8);
+            std::vector<uint8_t> sv((size_t)sv_bytes, 0xFF);
+            if (m > 0 && r.cols[1].valid)
+                KRV_CUDA(cudaMemcpyAsync(sv.data(), r.cols[1].valid, (size_t)sv_bytes, cudaMemcpyDeviceToHost,
+                                         rt_->stream));
+            KRV_CUDA(cudaStreamSynchronize(rt_->stream));
             for (int64_t i = 0; i < m; i++) {
                 oa.push_back(gattr[gid[i]]);
                 os.push_back(sum[i]);
+                const int64_t b = r.cols[1].valid_off + i;
+                ov.push_back(r.cols[1].valid ? (uint8_t)((sv[b >> 3] >> (b & 7)) & 1) : (uint8_t)1);
             }
         }
-        return host_result(oa, os);
+        return host_result(oa, os, ov);
     }
 
-    DevBatch host_result(const std::vector<int32_t> &attr, const std::vector<double> &sum) {
+    // The result batch (attr, sum); `valid[i]` = 0 makes sum i NULL.
+    DevBatch host_result(const std::vector<int32_t> &attr, const std::vector<double> &sum,
+                         const std::vector<uint8_t> &valid) {
         DevBatch out;
         const int64_t m = (int64_t)attr.size();
+        bool any_null = false;
+        for (uint8_t v : valid) any_null |= !v;
         DevCol a = make_col(rt_, DType{Type::I32, 0, 0}, m, false, "attr");
-        DevCol s = make_col(rt_, DType{Type::F64, 0, 0}, m, false, "sum");
+        DevCol s = make_col(rt_, DType{Type::F64, 0, 0}, m, any_null, "sum");
+        std::vector<uint8_t> bits((size_t)ceil_div(std::max<int64_t>(m, 1), 8), 0);
+        for (int64_t i = 0; i < m; i++)
+            if (valid[i]) bits[i >> 3] |= (uint8_t)(1u << (i & 7));
         if (m > 0) {
             KRV_CUDA(cudaMemcpyAsync(const_cast<void *>(a.data), attr.data(), (size_t)m * 4, cudaMemcpyHostToDevice, rt_->stream));
             KRV_CUDA(cudaMemcpyAsync(const_cast<void *>(s.data), sum.data(), (size_t)m * 8, cudaMemcpyHostToDevice, rt_->stream));
+            if (any_null)
+                KRV_CUDA(cudaMemcpyAsync(const_cast<uint8_t *>(s.valid), bits.data(), bits.size(), cudaMemcpyHostToDevice,
+                                         rt_->stream));
             KRV_CUDA(cudaStreamSynchronize(rt_->stream));
         }
         out.rows = m;
@@ -814,13 +1058,14 @@ class StarPipeline {
     DBuf gkeys_, gtab_, gattr_, ngroups_;
     uint32_t gmask_ = 0;
     int ngroups_host_ = 0;
-    DBuf sum_hi_, sum_lo_, cnt_, stats_;
+    DBuf sum_hi_, sum_lo_, cnt_, nulls_, stats_;
     DBuf bits_[2];               // filter answer bitmaps of dimensions a and b
     DBuf direct_buf_[2];         // direct key -> group id indexes
     DBuf surv_row_, surv_kb_, region_count_;  // fact rows that passed B's filter
     uint64_t surv_cap_ = 0;
     bool surv_kb64_ = false;
     StarDirect direct_[2] = {};
+    DBuf direct_full_[2];  // the fast build's direct indexes (kMaxDirectSpan entries each)
     int64_t bits_words_[2] = {0, 0};
     HashAggregate *plain_agg_ = nullptr;
     bool built_ = false;

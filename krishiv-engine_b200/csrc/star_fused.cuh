@@ -75,6 +75,13 @@ struct StarArgs {
     long long *surv_kb64;  // fk_b (otherwise)
     uint64_t region;
     unsigned long long *region_count;
+    // Validity bitmaps of the fact columns (null: no NULLs) and the bit of
+    // row 0 in each. A NULL key never joins (join/keys.rs:17-19); a NULL
+    // price or discount makes the row's value NULL, which SUM skips: the row
+    // still joins and counts, and adds one to its group's `nulls`.
+    const uint8_t *v_fk_a, *v_fk_b, *v_price, *v_disc;
+    int64_t o_fk_a, o_fk_b, o_price, o_disc;
+    unsigned long long *nulls;
 };
 
 __device__ __forceinline__ uint32_t star_lookup(const StarTable &t, long long k) {
@@ -174,6 +181,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) star_scan_kernel(StarArgs A) 
                 p = filter_pass(A.fb, cur[u]);
             }
             if (!full && r0 + u >= A.n) p = false;
+            if (A.v_fk_b && p && !bit_get(A.v_fk_b, A.o_fk_b, r0 + u)) p = false;
             m |= (unsigned)p << u;
         }
         // fk_a's 32-byte sectors of the passing rows will be read by stage 2.
@@ -212,6 +220,11 @@ __global__ void __launch_bounds__(kScanThreads, 1) star_scan_kernel(StarArgs A) 
 }
 
 // ---- stage 2 ------------------------------------------------------------------------
+// price * (1 - discount) of a row is NULL.
+__device__ __forceinline__ bool star_value_null(const StarArgs &A, uint32_t row) {
+    return (A.v_price && !bit_get(A.v_price, A.o_price, row)) || (A.v_disc && !bit_get(A.v_disc, A.o_disc, row));
+}
+
 // Adds v to the group of one joined pair: this warp's own accumulators in
 // shared memory (lanes take turns, plain compensated adds: float64 atomics
 // in shared memory are compare-and-swap loops) or, past them, the global ones.
@@ -320,6 +333,10 @@ __global__ void __launch_bounds__(kJoinThreads, 2) star_join_kernel(StarArgs A, 
 #pragma unroll
             for (int j = 0; j < kK; j++) pa[j] = has[j];
         }
+        if (A.v_fk_a) {
+#pragma unroll
+            for (int j = 0; j < kK; j++) pa[j] = pa[j] && bit_get(A.v_fk_a, A.o_fk_a, row[j]);
+        }
         if (DIRECT) {
 #pragma unroll
             for (int j = 0; j < kK; j++) {
@@ -327,7 +344,10 @@ __global__ void __launch_bounds__(kJoinThreads, 2) star_join_kernel(StarArgs A, 
                 hit[j] = pa[j] && ga[j] >= 0 && gb[j] >= 0;
                 g[j] = A.group_by == 0 ? ga[j] : gb[j];
                 v[j] = 0.0;
-                if (hit[j]) v[j] = __dmul_rn((double)__ldcs(A.price + row[j]), __dsub_rn(1.0, __ldcs(A.disc + row[j])));
+                if (hit[j]) {
+                    if (star_value_null(A, row[j])) atomicAdd(A.nulls + g[j], 1ull);
+                    else v[j] = __dmul_rn((double)__ldcs(A.price + row[j]), __dsub_rn(1.0, __ldcs(A.disc + row[j])));
+                }
             }
 #pragma unroll
             for (int j = 0; j < kK; j++) {
@@ -353,8 +373,9 @@ __global__ void __launch_bounds__(kJoinThreads, 2) star_join_kernel(StarArgs A, 
                     if (ra != kStarNone) rb0 = star_lookup(A.tb, kb[j]);
                 }
                 const bool h = ra != kStarNone && rb0 != kStarNone;
+                const bool vnull = h && star_value_null(A, row[j]);
                 double vv = 0.0;
-                if (h) vv = __dmul_rn((double)__ldcs(A.price + row[j]), __dsub_rn(1.0, __ldcs(A.disc + row[j])));
+                if (h && !vnull) vv = __dmul_rn((double)__ldcs(A.price + row[j]), __dsub_rn(1.0, __ldcs(A.disc + row[j])));
                 unsigned pend = __ballot_sync(0xFFFFFFFFu, h);
                 while (pend) {
                     const int l = __ffs(pend) - 1;
@@ -365,8 +386,9 @@ __global__ void __launch_bounds__(kJoinThreads, 2) star_join_kernel(StarArgs A, 
                             int cb = 0;
                             for (uint32_t rb = rb0; rb != kStarNone && cb < (1 << 20); cb++, rb = A.tb.next[rb]) {
                                 joined++;
-                                star_add_plain(A, A.group_by == 0 ? A.ta.gid[ra] : A.tb.gid[rb], vv, w_hi, w_lo,
-                                               w_cnt, G);
+                                const int gg = A.group_by == 0 ? A.ta.gid[ra] : A.tb.gid[rb];
+                                if (vnull) atomicAdd(A.nulls + gg, 1ull);
+                                star_add_plain(A, gg, vv, w_hi, w_lo, w_cnt, G);
                             }
                         }
                     }

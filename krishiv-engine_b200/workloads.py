@@ -62,26 +62,29 @@ class StarData:
     dim_b_rows: int
 
 
-def star(rt, scale: float = 1.0, seed: int = STAR_SEED, fact_row0: int = 0, fact_scale=None) -> StarData:
+def star(rt, scale: float = 1.0, seed: int = STAR_SEED, fact_row0: int = 0, fact_scale=None,
+         fact_nulls: float = 0.0) -> StarData:
     """The star-join inputs; `fact_row0` selects which fact rows (a shard of
     the fact stream for one of several devices); `fact_scale` (default
-    `scale`) sizes the fact table alone, the dimensions keep `scale`."""
+    `scale`) sizes the fact table alone, the dimensions keep `scale`;
+    `fact_nulls` > 0 makes that fraction of each fact column NULL
+    (independently per column)."""
     import torch
     kb = _kb()
     fs = scale if fact_scale is None else fact_scale
     nf, na, nb = int(300_000_000 * fs), int(20_000_000 * scale), int(1_000_000 * scale)
-    r0 = dict(row0=fact_row0)
-    fk_a, _ = _col(rt, nf, torch.int64, kb.GEN_UNIFORM_I64, seed, 1, lo=0, hi=na - 1, **r0)
-    fk_b, _ = _col(rt, nf, torch.int64, kb.GEN_UNIFORM_I64, seed, 2, lo=0, hi=nb - 1, **r0)
-    price, _ = _col(rt, nf, torch.int64, kb.GEN_UNIFORM_I64, seed, 3, lo=1000, hi=10_000_000, **r0)
-    disc, _ = _col(rt, nf, torch.float64, kb.GEN_UNIT_F64, seed, 4, x0=0.0, x1=0.1, **r0)
+    r0 = dict(row0=fact_row0, null_fraction=fact_nulls)
+    fk_a, v1 = _col(rt, nf, torch.int64, kb.GEN_UNIFORM_I64, seed, 1, lo=0, hi=na - 1, **r0)
+    fk_b, v2 = _col(rt, nf, torch.int64, kb.GEN_UNIFORM_I64, seed, 2, lo=0, hi=nb - 1, **r0)
+    price, v3 = _col(rt, nf, torch.int64, kb.GEN_UNIFORM_I64, seed, 3, lo=1000, hi=10_000_000, **r0)
+    disc, v4 = _col(rt, nf, torch.float64, kb.GEN_UNIT_F64, seed, 4, x0=0.0, x1=0.1, **r0)
     dims = []
     for base, n in ((10, na), (20, nb)):
         key, _ = _col(rt, n, torch.int64, kb.GEN_PERMUTATION, seed + base, base + 1, lo=0, hi=n)
         pred, _ = _col(rt, n, torch.int32, kb.GEN_UNIFORM_I32, seed, base + 2, lo=0, hi=19)
         attr, _ = _col(rt, n, torch.int32, kb.GEN_UNIFORM_I32, seed, base + 3, lo=0, hi=24)
         dims.append([("key", key, None), ("pred", pred, None), ("attr", attr, None)])
-    fact = [("fk_a", fk_a, None), ("fk_b", fk_b, None), ("price", price, None), ("discount", disc, None)]
+    fact = [("fk_a", fk_a, v1), ("fk_b", fk_b, v2), ("price", price, v3), ("discount", disc, v4)]
     return StarData(fact, dims[0], dims[1], nf, na, nb)
 
 

@@ -16,7 +16,7 @@
  *   - crates/krishiv-exec/tests/hash_join/main.rs:128-181 (nested-loop join
  *     oracle over every join type, NULLs, duplicates, empty inputs).
  *
- * Build: oracle/Makefile (gcc -O2 -ffp-contract=off, so float arithmetic is
+ * Build: oracle/Makefile (gcc -O3 -ffp-contract=off, so float arithmetic is
  * plain IEEE double with no contraction).
  */
 #include "krv_oracle.h"
@@ -410,9 +410,72 @@ static void push_pair(pairs_t *o, int64_t p, int64_t b) {
     o->n++;
 }
 
+/* One operand of a filter comparison for the pair (probe row p, build row
+ * b): 0 when NULL. */
+static int filter_operand(const orc_operand *o, int64_t p, int64_t b, int64_t *iv, double *fv) {
+    if (o->side == ORC_SIDE_CONST) {
+        *iv = o->i64;
+        *fv = o->is_float ? o->f64 : (double)o->i64;
+        return 1;
+    }
+    int64_t r = o->side == ORC_SIDE_PROBE ? p : b;
+    if (o->col.valid && !o->col.valid[r]) return 0;
+    if (o->col.width == 4) {
+        int32_t v;
+        memcpy(&v, (const uint8_t *)o->col.data + 4 * r, 4);
+        *iv = v;
+        *fv = (double)v;
+    } else if (o->col.is_float) {
+        memcpy(fv, (const uint8_t *)o->col.data + 8 * r, 8);
+        *iv = 0;
+    } else {
+        memcpy(iv, (const uint8_t *)o->col.data + 8 * r, 8);
+        *fv = (double)*iv;
+    }
+    return 1;
+}
+/* Spark's double order (aggregate/accumulator/helpers.rs:498): NaN equals
+ * NaN and is above everything, -0.0 equals 0.0: -1, 0, 1. */
+static int spark_cmp(double a, double b) {
+    int an = a != a, bn = b != b;
+    if (an || bn) return an == bn ? 0 : an ? 1 : -1;
+    return a < b ? -1 : a > b ? 1 : 0;
+}
+static int cmp_holds(int op, int c) {
+    switch (op) {
+    case 0: return c == 0;
+    case 1: return c != 0;
+    case 2: return c < 0;
+    case 3: return c <= 0;
+    case 4: return c > 0;
+    default: return c >= 0;
+    }
+}
+static int filter_true(const orc_filter *f, int64_t p, int64_t b) {
+    for (int t = 0; t < f->n; t++) {
+        const orc_term *T = &f->t[t];
+        int64_t li, ri;
+        double lf, rf;
+        if (!filter_operand(&T->l, p, b, &li, &lf) || !filter_operand(&T->r, p, b, &ri, &rf)) return 0;
+        int as_float = (T->l.side == ORC_SIDE_CONST ? T->l.is_float : T->l.col.is_float) ||
+                       (T->r.side == ORC_SIDE_CONST ? T->r.is_float : T->r.col.is_float);
+        int c = as_float ? spark_cmp(lf, rf) : (li < ri ? -1 : li > ri ? 1 : 0);
+        if (!cmp_holds(T->op, c)) return 0;
+    }
+    return 1;
+}
+
 int64_t orc_hash_join(int32_t jt, const orc_col *bk, int64_t nb, const orc_col *pk, int64_t np,
                       int32_t nkeys, const int32_t *null_safe, int32_t single_match,
                       uint64_t seed, int32_t radix, int64_t **out_probe, int64_t **out_build) {
+    return orc_hash_join_filtered(jt, bk, nb, pk, np, nkeys, null_safe, single_match, seed, radix, NULL,
+                                  out_probe, out_build);
+}
+
+int64_t orc_hash_join_filtered(int32_t jt, const orc_col *bk, int64_t nb, const orc_col *pk, int64_t np,
+                               int32_t nkeys, const int32_t *null_safe, int32_t single_match,
+                               uint64_t seed, int32_t radix, const orc_filter *filter, int64_t **out_probe,
+                               int64_t **out_build) {
     if (radix < 3) radix = 3;
     if (radix > 6) radix = 6;
     int nparts = 1 << radix;
@@ -517,6 +580,8 @@ int64_t orc_hash_join(int32_t jt, const orc_col *bk, int64_t nb, const orc_col *
             }
             for (uint32_t o = head; o != NO_MATCH; o = P->next[o]) {
                 int64_t r = P->rows[o];
+                /* a pair counts only where the filter is TRUE (join/probe.rs:425-436) */
+                if (filter && !filter_true(filter, i, r)) continue;
                 matched++;
                 if (builds_preserved) bmark[r] = 1;
                 if (jt == ORC_INNER || jt == ORC_LEFT_OUTER || jt == ORC_RIGHT_OUTER ||

@@ -101,6 +101,36 @@ int64_t orc_hash_join(int32_t join_type, const orc_col *build_keys, int64_t nb,
                       const orc_col *probe_keys, int64_t np, int32_t nkeys,
                       const int32_t *null_safe, int32_t single_match, uint64_t seed,
                       int32_t radix, int64_t **out_probe, int64_t **out_build);
+/* JoinSpec::filter (join/mod.rs:327-350) applied to candidate pairs
+ * (join/probe.rs:393-489, :425-436): a conjunction of comparisons whose
+ * operands are a probe column, a build column (ORC_SIDE_*: `col`) or a
+ * constant (i64, or f64 when is_float); comparisons with a float operand
+ * compare as double in Spark's order (NaN equal to NaN and largest, -0.0
+ * equal to 0.0); a NULL operand is not TRUE. */
+enum { ORC_SIDE_PROBE = 0, ORC_SIDE_BUILD = 1, ORC_SIDE_CONST = 2 };
+typedef struct {
+    int32_t side;
+    int32_t is_float;
+    orc_col col;
+    int64_t i64;
+    double f64;
+} orc_operand;
+typedef struct {
+    int32_t op; /* 0 =, 1 !=, 2 <, 3 <=, 4 >, 5 >= */
+    int32_t pad;
+    orc_operand l, r;
+} orc_term;
+typedef struct {
+    int32_t n;
+    int32_t pad;
+    orc_term t[8];
+} orc_filter;
+/* orc_hash_join with a residual filter (NULL: none). */
+int64_t orc_hash_join_filtered(int32_t join_type, const orc_col *build_keys, int64_t nb,
+                               const orc_col *probe_keys, int64_t np, int32_t nkeys,
+                               const int32_t *null_safe, int32_t single_match, uint64_t seed,
+                               int32_t radix, const orc_filter *filter, int64_t **out_probe,
+                               int64_t **out_build);
 void orc_free(void *p);
 
 /* ---- grouped aggregate (crates/krishiv-exec/src/aggregate/) ---------------- */

@@ -217,11 +217,51 @@ class KeyFilter:
         return out.astype(bool)
 
 
+class OrcOperand(C.Structure):
+    _fields_ = [("side", C.c_int32), ("is_float", C.c_int32), ("col", OrcCol), ("i64", C.c_int64),
+                ("f64", C.c_double)]
+
+
+class OrcTerm(C.Structure):
+    _fields_ = [("op", C.c_int32), ("pad", C.c_int32), ("l", OrcOperand), ("r", OrcOperand)]
+
+
+class OrcFilter(C.Structure):
+    _fields_ = [("n", C.c_int32), ("pad", C.c_int32), ("t", OrcTerm * 8)]
+
+
+CMP = {"=": 0, "!=": 1, "<": 2, "<=": 3, ">": 4, ">=": 5}
+
+
+def make_filter(terms, probe_cols, build_cols):
+    """A residual filter: `terms` as (left, op, right) with operands
+    ("probe", i) / ("build", i) naming entries of `probe_cols` /
+    `build_cols` ((values, valid-or-None) numpy pairs), an int or a float.
+    Returns (OrcFilter, keep-alive list)."""
+    f = OrcFilter()
+    f.n = len(terms)
+    keep = []
+
+    def operand(o):
+        if isinstance(o, tuple):
+            values, valid = (probe_cols if o[0] == "probe" else build_cols)[o[1]]
+            c, k = _col(values, valid, values.dtype == np.float64)
+            keep.append(k)
+            return OrcOperand(side=0 if o[0] == "probe" else 1, is_float=int(values.dtype == np.float64), col=c)
+        if isinstance(o, float):
+            return OrcOperand(side=2, is_float=1, f64=o)
+        return OrcOperand(side=2, is_float=0, i64=int(o))
+    for i, (l, op, r) in enumerate(terms):
+        f.t[i] = OrcTerm(op=CMP[op], l=operand(l), r=operand(r))
+    return f, keep
+
+
 def hash_join(join_type, build_keys, probe_keys, null_safe=None, single_match=False, seed=7,
-              radix=3):
+              radix=3, filter=None):
     """Index pairs of probe ⋈ build. `build_keys`/`probe_keys`: lists of
     (values, valid-or-None, is_float). Returns (probe_rows, build_rows) int64
-    arrays with -1 for a NULL-padded side (existence: build_rows = flag)."""
+    arrays with -1 for a NULL-padded side (existence: build_rows = flag).
+    `filter`: a residual filter from make_filter (or None)."""
     nk = len(build_keys)
     nb = len(build_keys[0][0])
     np_ = len(probe_keys[0][0])
@@ -238,9 +278,15 @@ def hash_join(join_type, build_keys, probe_keys, null_safe=None, single_match=Fa
     ns = np.array(null_safe if null_safe is not None else [0] * nk, dtype=np.int32)
     op = C.POINTER(C.c_int64)()
     ob = C.POINTER(C.c_int64)()
-    n = lib().orc_hash_join(join_type, C.addressof(ba), nb, C.addressof(pa), np_, nk,
-                            ns.ctypes.data, int(single_match), seed, radix, C.byref(op),
-                            C.byref(ob))
+    L = lib()
+    L.orc_hash_join_filtered.restype = C.c_int64
+    L.orc_hash_join_filtered.argtypes = [C.c_int32, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32,
+                                         C.c_void_p, C.c_int32, C.c_uint64, C.c_int32, C.c_void_p,
+                                         C.POINTER(C.POINTER(C.c_int64)), C.POINTER(C.POINTER(C.c_int64))]
+    n = L.orc_hash_join_filtered(join_type, C.addressof(ba), nb, C.addressof(pa), np_, nk,
+                                 ns.ctypes.data, int(single_match), seed, radix,
+                                 C.addressof(filter[0]) if filter is not None else None, C.byref(op),
+                                 C.byref(ob))
     if n == -2:
         raise RuntimeError("SCALAR_SUBQUERY_TOO_MANY_ROWS")
     if n < 0:

@@ -108,11 +108,25 @@ def test_single_match_error(kb, rt):
     assert e.value.status == kb.TOO_MANY_ROWS
 
 
-def test_residual_filter_unsupported(kb, rt):
+def test_residual_filter_flag_needs_a_filter(kb, rt):
+    """has_residual_filter without krv_join_set_filter is an error at the first
+    probe; a null-aware anti join takes no residual condition (the reference
+    rejects that combination, join/mod.rs:746-752)."""
     spec = kb.join_spec("inner")
+    spec.has_residual_filter = 1
+    j = kb.HashJoin(rt, spec)
+    j.build_push(rows_batch([(1, 0)], "bid"))
+    j.build_finish()
+    with pytest.raises(kb.KrvError) as e:
+        j.probe(rows_batch([(1, 0)], "pid"))
+    assert e.value.status == kb.INVALID_ARGUMENT
+    spec = kb.join_spec("null_aware_anti")
     spec.has_residual_filter = 1
     with pytest.raises(kb.KrvError) as e:
         kb.HashJoin(rt, spec)
+    assert e.value.status == kb.UNSUPPORTED
+    with pytest.raises(kb.KrvError) as e:
+        kb.HashJoin(rt, kb.join_spec("null_aware_anti"), filter=[(("probe", 1), "<", ("build", 1))])
     assert e.value.status == kb.UNSUPPORTED
 
 

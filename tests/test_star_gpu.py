@@ -13,8 +13,16 @@ pytestmark = pytest.mark.gpu
 FLOAT_TOL = 1e-12
 
 
+def unpack(valid, n):
+    """A device validity bitmap as a boolean array (all True when None)."""
+    if valid is None:
+        return np.ones(n, dtype=bool)
+    return np.unpackbits(valid.cpu().numpy(), bitorder="little")[:n].astype(bool)
+
+
 def oracle_star(oracle, data, group_by=0):
     fk_a, fk_b, price, disc = [c[1].cpu().numpy() for c in data.fact]
+    va, vb, vp, vd = [unpack(c[2], data.fact_rows) for c in data.fact]
     dims = []
     for d in (data.dim_a, data.dim_b):
         key, pred, attr = [c[1].cpu().numpy() for c in d]
@@ -22,19 +30,23 @@ def oracle_star(oracle, data, group_by=0):
         dims.append((key[sel], attr[sel]))
     (ka, aa), (kb_, ab) = dims
     fa, fb = oracle.KeyFilter(ka), oracle.KeyFilter(kb_)
-    passed = fa.evaluate(fk_a) & fb.evaluate(fk_b)
+    passed = fa.evaluate(fk_a, va) & fb.evaluate(fk_b, vb)
     oa, ob = np.argsort(ka), np.argsort(kb_)
     ia = np.searchsorted(ka, fk_a, sorter=oa)
     ib = np.searchsorted(kb_, fk_b, sorter=ob)
     ia = np.minimum(ia, len(ka) - 1)
     ib = np.minimum(ib, len(kb_) - 1)
-    hit = (ka[oa[ia]] == fk_a) & (kb_[ob[ib]] == fk_b)
+    # a NULL key never joins (join/keys.rs:17-19)
+    hit = (ka[oa[ia]] == fk_a) & (kb_[ob[ib]] == fk_b) & va & vb
     assert not (hit & ~passed).any(), "a runtime filter dropped a joining row"
     group = (aa[oa[ia]] if group_by == 0 else ab[ob[ib]])[hit].astype(np.int64)
     value = price[hit].astype(np.float64) * (1.0 - disc[hit])
-    keys, _, res = oracle.hash_aggregate(group, None, [{"values": value, "type": oracle.T_F64}],
+    value_valid = (vp & vd)[hit]  # a NULL price or discount: a NULL value, skipped by SUM
+    keys, _, res = oracle.hash_aggregate(group, None,
+                                         [{"values": value, "valid": value_valid.astype(np.uint8), "type": oracle.T_F64}],
                                          [(oracle.SUM, 0), (oracle.COUNT_STAR, 0)])
-    return int(passed.sum()), int(hit.sum()), {int(k): (s, c) for k, s, c in zip(keys, res[0]["f64"], res[1]["i64"])}, (fa, fb)
+    return int(passed.sum()), int(hit.sum()), {int(k): (s if ok else None, c) for k, s, ok, c in
+                                               zip(keys, res[0]["f64"], res[0]["valid"], res[1]["i64"])}, (fa, fb)
 
 
 @pytest.mark.parametrize("mode", [0, 1])
@@ -61,6 +73,47 @@ def test_star_matches_oracle(kb, rt, oracle, mode, group_by):
     assert sorted(got) == sorted(want)
     for k, (ws, _) in want.items():
         assert rel_err(got[k], ws) <= FLOAT_TOL, (k, got[k], ws)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("group_by", [0, 1])
+def test_star_with_null_fact_columns(kb, rt, oracle, mode, group_by):
+    """2% NULLs in every fact column: NULL keys never join, a NULL price or
+    discount makes the row's value NULL (the row still joins; SUM skips it).
+    Fused and plain forms against the oracle, in two device probe batches
+    (the second cut at an odd row)."""
+    W = importlib.import_module("krishiv-engine_b200.workloads")
+    import torch
+    data = W.star(rt, scale=0.01, fact_nulls=0.02)
+    torch.cuda.synchronize()
+    assert all(c[2] is not None for c in data.fact)
+    s = kb.StarPipeline(rt, kb.star_spec(7, 7, group_by=group_by, mode=mode))
+    s.build_device(kb.DeviceBatch(data.dim_a), kb.DeviceBatch(data.dim_b))
+    n = data.fact_rows
+    cut = n // 2 + 3
+    full = [(name, t, v) for name, t, v in data.fact]
+    # the second part as its own device columns: values and bitmaps realigned at row 0
+    second = []
+    for name, t, v in full:
+        bits = np.unpackbits(v.cpu().numpy(), bitorder="little")[cut:n]
+        packed = torch.tensor(np.packbits(bits, bitorder="little"), device="cuda")
+        second.append((name, t[cut:].contiguous(), packed))
+    first = [(name, t[:cut], v) for name, t, v in full]
+    s.probe_device(kb.DeviceBatch(first))
+    s.probe_device(kb.DeviceBatch(second))
+    out = s.result()
+    c = s.counters()
+    passed, joined, want, _ = oracle_star(oracle, data, group_by)
+    if mode == 0:
+        assert c["passed_filters"] == passed
+    assert c["joined_rows"] == joined
+    got = dict(zip(out.column(0).to_pylist(), out.column(1).to_pylist()))
+    assert sorted(got) == sorted(want)
+    for k, (ws, _) in want.items():
+        if ws is None:
+            assert got[k] is None, k
+        else:
+            assert rel_err(got[k], ws) <= FLOAT_TOL, (k, got[k], ws)
 
 
 def test_star_same_alone_and_after_reset(kb, rt):
@@ -158,4 +211,51 @@ def test_star_host_batch_streamed(kb, rt, oracle):
         got = dict(zip(out.column(0).to_pylist(), out.column(1).to_pylist()))
         assert sorted(got) == sorted(want)
         for k, (ws, _) in want.items():
+            assert rel_err(got[k], ws) <= FLOAT_TOL, (k, got[k], ws)
+
+
+def test_star_host_batch_streamed_with_nulls(kb, rt, oracle):
+    """Page-locked host columns with 2% NULLs each, 36M fact rows: fk_b moves
+    in bulk copies of 8M rows, the other values are read in place, and the
+    validity bitmaps (copied to the device) are read at the bit offset of an
+    Arrow slice that starts at row 5 plus that of each chunk."""
+    import pyarrow as pa
+    import torch
+    W = importlib.import_module("krishiv-engine_b200.workloads")
+    data = W.star(rt, scale=0.12, fact_nulls=0.02)
+    torch.cuda.synchronize()
+    passed, joined, want, _ = oracle_star(oracle, data, 0)
+    keep = []
+    n = data.fact_rows
+
+    def pinned(t):
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        h.copy_(t)
+        keep.append(h)
+        return h
+
+    arrays = []
+    for name, t, v in data.fact:
+        ht, hv = pinned(t), pinned(v)
+        typ = pa.float64() if t.dtype == torch.float64 else pa.int64()
+        arrays.append(pa.Array.from_buffers(typ, n, [pa.foreign_buffer(hv.data_ptr(), hv.numel()),
+                                                     pa.foreign_buffer(ht.data_ptr(), ht.numel() * 8)]))
+    fact = pa.RecordBatch.from_arrays(arrays, names=[c[0] for c in data.fact])
+
+    def host(cols):
+        return pa.RecordBatch.from_arrays([pa.array(pinned(t).numpy()) for _, t, _ in cols], names=[c[0] for c in cols])
+
+    s = kb.StarPipeline(rt, kb.star_spec(7, 7, group_by=0, mode=kb.STAR_FUSED))
+    s.build(host(data.dim_a), host(data.dim_b))
+    s.probe(fact.slice(0, 5))
+    s.probe(fact.slice(5, n - 5))
+    out = s.result()
+    c = s.counters()
+    assert c["passed_filters"] == passed and c["joined_rows"] == joined
+    got = dict(zip(out.column(0).to_pylist(), out.column(1).to_pylist()))
+    assert sorted(got) == sorted(want)
+    for k, (ws, _) in want.items():
+        if ws is None:
+            assert got[k] is None, k
+        else:
             assert rel_err(got[k], ws) <= FLOAT_TOL, (k, got[k], ws)
