@@ -236,7 +236,8 @@ struct OutColDev {
     void *dst;
     uint32_t *dst_valid;  // zeroed bitmap words, or null (non-nullable output)
     int32_t width;
-    int32_t side;         // 0 probe row, 1 build row, 2 constant NULL
+    int32_t side;         // 0 probe row, 1 build row, 2 constant NULL; 3 / 4 the probe / build row
+                          // index itself (int64, -1 for a NULL side): the rows string columns are gathered from
 };
 struct OutDev {
     OutColDev c[2 * KRV_MAX_OUT_COLUMNS];
@@ -275,7 +276,11 @@ __device__ __forceinline__ void emit_round(const OutDev &out, bool want, unsigne
         const OutColDev &c = out.c[k];
         bool v = false;
         if (want && pos < cap) {
-            if (c.side == 0 && prow >= 0) {
+            if (c.side == 3) {
+                static_cast<long long *>(c.dst)[pos] = prow >= 0 ? prow : -1;
+            } else if (c.side == 4) {
+                static_cast<long long *>(c.dst)[pos] = brow != kNone ? (long long)brow : -1;
+            } else if (c.side == 0 && prow >= 0) {
                 copy_value(c.dst, c.src, (int64_t)pos, prow, c.width);
                 v = bit_get(c.src_valid, c.src_voff, prow);
             } else if (c.side == 1 && brow != kNone) {
@@ -470,7 +475,11 @@ __global__ void __launch_bounds__(kFastThreads) probe_fast_kernel(KeysDev pk, Ke
             for (int k = 0; k < out.n; k++) {
                 const OutColDev &c = out.c[k];
                 bool v = false;
-                if (c.side == 0) {
+                if (c.side == 3) {
+                    static_cast<long long *>(c.dst)[a] = row[u];
+                } else if (c.side == 4) {
+                    static_cast<long long *>(c.dst)[a] = b != kNone ? (long long)b : -1;
+                } else if (c.side == 0) {
                     copy_value(c.dst, c.src, (int64_t)a, row[u], c.width);
                     v = bit_get(c.src_valid, c.src_voff, row[u]);
                 } else if (b != kNone) {
@@ -643,20 +652,32 @@ void HashJoin::append_arena(const DevBatch &b) {
     if (need > (int64_t)0xFFFFFFFEll) fail(KRV_UNSUPPORTED, "more than 2^32-2 build rows in one table");
     if (need > arena_cap_) {
         int64_t cap = std::max<int64_t>({need, arena_cap_ * 2, spec_.build_rows_hint, 1024});
+        if (arena_var_.size() < arena_cols_.size()) arena_var_.resize(arena_cols_.size());
         for (size_t i = 0; i < arena_cols_.size(); i++) {
             const DType t = arena_cols_[i].type;
-            const size_t bytes = t.id == Type::Bool ? (size_t)ceil_div(cap, 8) : (size_t)cap * t.width();
+            // a string column keeps a start (int64) per row here and its length beside
+            const size_t w = t.var() ? 8 : (size_t)t.width();
+            const size_t bytes = t.id == Type::Bool ? (size_t)ceil_div(cap, 8) : (size_t)cap * w;
             auto nd = std::make_shared<DBuf>(rt_, bytes);
             auto nv = std::make_shared<DBuf>(rt_, (size_t)ceil_div(cap, 32) * 4 + 8);
             zero(rt_, nv->get(), nv->bytes());
+            std::shared_ptr<DBuf> nl;
+            if (t.var()) nl = std::make_shared<DBuf>(rt_, (size_t)cap * 4);
             if (build_rows_) {
-                const size_t old = t.id == Type::Bool ? (size_t)ceil_div(build_rows_, 8) : (size_t)build_rows_ * t.width();
+                const size_t old = t.id == Type::Bool ? (size_t)ceil_div(build_rows_, 8) : (size_t)build_rows_ * w;
                 KRV_CUDA(cudaMemcpyAsync(nd->get(), arena_data_[i]->get(), old, cudaMemcpyDeviceToDevice, rt_->stream));
                 KRV_CUDA(cudaMemcpyAsync(nv->get(), arena_valid_[i]->get(), (size_t)ceil_div(build_rows_, 8),
                                          cudaMemcpyDeviceToDevice, rt_->stream));
+                if (nl)
+                    KRV_CUDA(cudaMemcpyAsync(nl->get(), arena_var_[i].lens->get(), (size_t)build_rows_ * 4,
+                                             cudaMemcpyDeviceToDevice, rt_->stream));
             }
             arena_data_[i] = nd;
             arena_valid_[i] = nv;
+            if (nl) {
+                arena_var_[i].starts = nd;
+                arena_var_[i].lens = nl;
+            }
         }
         arena_cap_ = cap;
     }
@@ -664,11 +685,15 @@ void HashJoin::append_arena(const DevBatch &b) {
         const DevCol &c = b.cols[i];
         const DType t = c.type;
         if (t.id == Type::Bool) fail(KRV_UNSUPPORTED, "boolean build columns");
-        const size_t w = (size_t)t.width();
         if (c.valid) arena_cols_[i].nullable = true;
         if (b.rows == 0) continue;  // an empty batch only fixes the schema
-        KRV_CUDA(cudaMemcpyAsync(arena_data_[i]->as<uint8_t>() + build_rows_ * w, c.data, (size_t)b.rows * w,
-                                 cudaMemcpyDeviceToDevice, rt_->stream));
+        if (t.var()) {
+            var_arena_append(rt_, arena_var_[i], c, build_rows_, b.rows);
+        } else {
+            const size_t w = (size_t)t.width();
+            KRV_CUDA(cudaMemcpyAsync(arena_data_[i]->as<uint8_t>() + build_rows_ * w, c.data, (size_t)b.rows * w,
+                                     cudaMemcpyDeviceToDevice, rt_->stream));
+        }
         append_bits(rt_, c.valid, c.valid_off, b.rows, arena_valid_[i]->as<uint8_t>(), build_rows_);
     }
     build_rows_ = need;
@@ -696,9 +721,28 @@ void HashJoin::build_adopt(DevBatch b) {
 
 HashJoin::~HashJoin() = default;
 
-static void reject_var(const DevBatch &b) {
-    for (const DevCol &c : b.cols)
-        if (c.type.var()) fail(KRV_UNSUPPORTED, "column '" + c.name + "': string and binary columns are taken as keys only");
+VarSrc HashJoin::var_src(int side, int col, const DevBatch *probe) const {
+    VarSrc v{};
+    if (side == 0) {
+        const DevCol &c = probe->cols[col];
+        v.offs = static_cast<const int32_t *>(c.data);
+        v.bytes = static_cast<const uint8_t *>(c.bytes);
+        v.valid = c.valid;
+        v.voff = c.valid_off;
+        return v;
+    }
+    if (col >= (int)arena_var_.size() || !arena_var_[col].starts) return v;  // no build rows: never read
+    const VarArena &a = arena_var_[col];
+    v.starts = a.starts->as<long long>();
+    v.lens = a.lens->as<int32_t>();
+    v.bytes = a.heap ? a.heap->as<uint8_t>() : nullptr;
+    v.valid = arena_cols_[col].nullable ? arena_valid_[col]->as<uint8_t>() : nullptr;
+    return v;
+}
+
+DevCol HashJoin::empty_col(const DevCol &meta) const {
+    if (meta.type.var()) return var_gather(rt_, VarSrc{}, nullptr, 0, meta.type, meta.nullable, meta.name);
+    return make_col(rt_, meta.type, 0, meta.nullable, meta.name);
 }
 
 void HashJoin::set_filter(const krv_join_filter &f) {
@@ -886,7 +930,6 @@ void HashJoin::build_push(DevBatch b) {
     DeviceGuard g(rt_);
     if (!decided_) decide(b);
     if (coded_) b = coded_batch(b, true);
-    else reject_var(b);
     append_arena(b);
 }
 
@@ -1023,7 +1066,6 @@ DevBatch HashJoin::probe(const DevBatch &outer_in) {
     DeviceGuard g(rt_);
     DevBatch coded_in;
     if (coded_) coded_in = coded_batch(outer_in, false);
-    else reject_var(outer_in);
     const DevBatch &in = coded_ ? coded_in : outer_in;
     const int jt = spec_.join_type;
     const int64_t n = in.rows;
@@ -1079,6 +1121,10 @@ DevBatch HashJoin::probe(const DevBatch &outer_in) {
         out.rows = n;
         for (int pc : pcols) {
             const DevCol &s = in.cols[pc];
+            if (s.type.var()) {
+                out.cols.push_back(var_gather(rt_, var_src(0, pc, &in), nullptr, n, s.type, s.nullable || s.valid, s.name));
+                continue;
+            }
             DevCol d = make_col(rt_, s.type, n, s.nullable || s.valid, s.name);
             const size_t bytes = s.type.id == Type::Bool ? (size_t)ceil_div(n, 8) : (size_t)n * s.type.width();
             if (bytes) KRV_CUDA(cudaMemcpyAsync(const_cast<void *>(d.data), s.data, bytes, cudaMemcpyDeviceToDevice, rt_->stream));
@@ -1132,10 +1178,7 @@ DevBatch HashJoin::probe(const DevBatch &outer_in) {
         }
         // Nothing is emitted by this batch: an empty batch of the output shape.
         DevBatch empty;
-        for (int bc : bcols) {
-            const DevCol &meta = arena_cols_[bc];
-            empty.cols.push_back(make_col(rt_, meta.type, 0, meta.nullable, meta.name));
-        }
+        for (int bc : bcols) empty.cols.push_back(empty_col(arena_cols_[bc]));
         return empty;
     }
 
@@ -1159,10 +1202,20 @@ DevBatch HashJoin::probe(const DevBatch &outer_in) {
     for (int attempt = 0; attempt < 4; attempt++) {
         out = DevBatch{};
         OutDev od{};
+        std::vector<VarOut> vars;  // string columns, gathered once the row indexes are known
         for (int pc : pcols) {
             const DevCol &s = in.cols[pc];
             if (s.type.id == Type::Bool) fail(KRV_UNSUPPORTED, "boolean probe payload columns");
             const bool nullable = s.nullable || s.valid || probe_nullable;
+            if (s.type.var()) {
+                DevCol m;
+                m.type = s.type;
+                m.name = s.name;
+                m.nullable = nullable;
+                vars.push_back(VarOut{(int)out.cols.size(), 0, pc});
+                out.cols.push_back(m);
+                continue;
+            }
             DevCol d = make_col(rt_, s.type, (int64_t)cap, nullable, s.name);
             if (d.valid) zero(rt_, const_cast<uint8_t *>(d.valid), d.hold_valid->bytes());
             od.c[od.n++] = OutColDev{s.data, s.valid, s.valid_off, const_cast<void *>(d.data),
@@ -1174,6 +1227,15 @@ DevBatch HashJoin::probe(const DevBatch &outer_in) {
                 const DevCol &s = arena_.cols.empty() ? DevCol{} : arena_.cols[bc];
                 const DevCol &meta = arena_cols_[bc];
                 const bool nullable = meta.nullable || build_nullable;
+                if (meta.type.var()) {
+                    DevCol m;
+                    m.type = meta.type;
+                    m.name = meta.name;
+                    m.nullable = nullable;
+                    vars.push_back(VarOut{(int)out.cols.size(), 1, bc});
+                    out.cols.push_back(m);
+                    continue;
+                }
                 DevCol d = make_col(rt_, meta.type, (int64_t)cap, nullable, meta.name);
                 if (d.valid) zero(rt_, const_cast<uint8_t *>(d.valid), d.hold_valid->bytes());
                 od.c[od.n++] = OutColDev{s.data, meta.nullable ? s.valid : nullptr, 0, const_cast<void *>(d.data),
@@ -1181,6 +1243,12 @@ DevBatch HashJoin::probe(const DevBatch &outer_in) {
                 out.cols.push_back(d);
             }
         }
+        DBuf idx[2];
+        for (const VarOut &v : vars)
+            if (!idx[v.side].get()) {
+                idx[v.side] = DBuf(rt_, (size_t)cap * 8);
+                od.c[od.n++] = OutColDev{nullptr, nullptr, 0, idx[v.side].get(), nullptr, 8, 3 + v.side};
+            }
         zero(rt_, cnt.get(), 8);
         clear_status(rt_);
         if (n > 0) {
@@ -1238,6 +1306,11 @@ DevBatch HashJoin::probe(const DevBatch &outer_in) {
         if (got <= cap) {
             out.rows = (int64_t)got;
             for (DevCol &c : out.cols) c.length = out.rows;
+            for (const VarOut &v : vars) {
+                const DevCol m = out.cols[v.pos];
+                out.cols[v.pos] = var_gather(rt_, var_src(v.side, v.col, &in), idx[v.side].as<long long>(), out.rows,
+                                             m.type, m.nullable, m.name);
+            }
             counters_.output_rows += out.rows;
             remember_shape(out);
             return out;
@@ -1257,7 +1330,7 @@ DevBatch HashJoin::finish() {
         // Nothing waits for the end: an empty batch of the probe output's shape.
         finished_ = true;
         DevBatch empty;
-        for (const DevCol &m : out_meta_) empty.cols.push_back(make_col(rt_, m.type, 0, m.nullable, m.name));
+        for (const DevCol &m : out_meta_) empty.cols.push_back(empty_col(m));
         return empty;
     }
     finished_ = true;
@@ -1270,7 +1343,17 @@ DevBatch HashJoin::finish() {
     const unsigned long long cap = (unsigned long long)std::max<int64_t>(build_rows_, 1);
     DevBatch out;
     OutDev od{};
+    std::vector<VarOut> vars;
     for (int pc : pcols) {
+        if (probe_types_[pc].var()) {
+            DevCol m;
+            m.type = probe_types_[pc];
+            m.name = probe_names_[pc];
+            m.nullable = true;
+            vars.push_back(VarOut{(int)out.cols.size(), 0, pc});
+            out.cols.push_back(m);
+            continue;
+        }
         DevCol d = make_col(rt_, probe_types_[pc], (int64_t)cap, true, probe_names_[pc]);
         zero(rt_, const_cast<uint8_t *>(d.valid), d.hold_valid->bytes());
         od.c[od.n++] = OutColDev{nullptr, nullptr, 0, const_cast<void *>(d.data), (uint32_t *)d.valid,
@@ -1281,12 +1364,27 @@ DevBatch HashJoin::finish() {
         const DevCol &meta = arena_cols_[bc];
         const DevCol &s = arena_.cols[bc];
         const bool nullable = meta.nullable || jt == KRV_JOIN_FULL_OUTER;
+        if (meta.type.var()) {
+            DevCol m;
+            m.type = meta.type;
+            m.name = meta.name;
+            m.nullable = nullable;
+            vars.push_back(VarOut{(int)out.cols.size(), 1, bc});
+            out.cols.push_back(m);
+            continue;
+        }
         DevCol d = make_col(rt_, meta.type, (int64_t)cap, nullable, meta.name);
         if (d.valid) zero(rt_, const_cast<uint8_t *>(d.valid), d.hold_valid->bytes());
         od.c[od.n++] = OutColDev{s.data, meta.nullable ? s.valid : nullptr, 0, const_cast<void *>(d.data),
                                  (uint32_t *)d.valid, meta.type.width(), 1};
         out.cols.push_back(d);
     }
+    DBuf idx[2];
+    for (const VarOut &v : vars)
+        if (!idx[v.side].get()) {
+            idx[v.side] = DBuf(rt_, (size_t)cap * 8);
+            od.c[od.n++] = OutColDev{nullptr, nullptr, 0, idx[v.side].get(), nullptr, 8, 3 + v.side};
+        }
     DBuf cnt(rt_, 8);
     zero(rt_, cnt.get(), 8);
     if (build_rows_ > 0) {
@@ -1300,6 +1398,12 @@ DevBatch HashJoin::finish() {
     }
     out.rows = (int64_t)read_scalar<unsigned long long>(rt_, cnt.get());
     for (DevCol &c : out.cols) c.length = out.rows;
+    for (const VarOut &v : vars) {
+        const DevCol m = out.cols[v.pos];
+        // the tail's probe side is all NULL: its string columns read nothing
+        const VarSrc src = v.side == 1 ? var_src(1, v.col, nullptr) : VarSrc{};
+        out.cols[v.pos] = var_gather(rt_, src, idx[v.side].as<long long>(), out.rows, m.type, m.nullable, m.name);
+    }
     counters_.output_rows += out.rows;
     return out;
 }

@@ -97,6 +97,31 @@ struct FilterDev {
     int32_t n;
 };
 
+// ---- string and binary columns on the join path (varcol.cu) ----------------------
+// A source of string values by row: Arrow int32 offsets into `bytes` (offs,
+// value r = bytes[offs[r] .. offs[r + 1])), or a start and a length per row
+// (starts / lens, the build arena's form).
+struct VarSrc {
+    const int32_t *offs;
+    const long long *starts;
+    const int32_t *lens;
+    const uint8_t *bytes;
+    const uint8_t *valid;
+    int64_t voff;
+};
+// The build arena's form of one string column.
+struct VarArena {
+    std::shared_ptr<DBuf> starts, lens, heap;
+    int64_t heap_size = 0, heap_cap = 0;
+};
+// Appends n rows of string column c at arena row base_row (starts and lens
+// must hold base_row + n rows).
+void var_arena_append(Runtime *rt, VarArena &a, const DevCol &c, int64_t base_row, int64_t n);
+// The string column of m output rows whose values are src's rows idx[j]
+// (idx null: row j; -1: NULL).
+DevCol var_gather(Runtime *rt, const VarSrc &src, const long long *idx, int64_t m, DType type, bool nullable,
+                  const std::string &name);
+
 // ---- hash join (crates/krishiv-exec/src/join/mod.rs:1014 HashJoin) -------------
 class HashJoin {
   public:
@@ -193,6 +218,16 @@ class HashJoin {
     krv_join_spec spec_;
     std::vector<DevCol> arena_cols_;    // growable build arena
     std::vector<std::shared_ptr<DBuf>> arena_data_, arena_valid_;
+    std::vector<VarArena> arena_var_;   // string columns: per-row starts, lengths and the byte heap
+    // The string columns of an output batch: gathered from the probe batch
+    // or the arena by the row index columns the kernels wrote.
+    struct VarOut {
+        int pos;        // output column
+        int side;       // 0 probe, 1 build
+        int col;        // source column
+    };
+    VarSrc var_src(int side, int col, const DevBatch *probe) const;
+    DevCol empty_col(const DevCol &meta) const;
     int64_t arena_cap_ = 0;
     DevBatch arena_;                    // view of the arena
     bool have_schema_ = false;
