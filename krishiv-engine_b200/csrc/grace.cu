@@ -139,6 +139,35 @@ __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(PartArgs A, 
     }
 }
 
+// ---- the fallback for a partition that splitting cannot shrink ------------------
+// Probe row ids of a chunk: base, base + 1, ...
+__global__ void iota_kernel(long long *out, int64_t n, long long base) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = base + i;
+}
+// The probe rows that matched some build row (their ids in an output batch).
+__global__ void mark_matched_kernel(const long long *ids, int64_t n, uint8_t *matched) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        matched[ids[i]] = 1;
+}
+// The rows of a chunk (ids base..) that matched nothing, compacted (any order).
+__global__ void compact_unmatched_kernel(PartArgs A, const uint8_t *matched, long long base,
+                                         unsigned long long *count) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t b0 = blockIdx.x * (int64_t)blockDim.x; b0 < A.n; b0 += stride) {
+        const int64_t r = b0 + threadIdx.x;
+        const bool keep = r < A.n && !matched[base + r];
+        const unsigned long long at = warp_alloc(count, keep, 0xFFFFFFFFu);
+        if (!keep) continue;
+        for (int c = 0; c < A.ncols; c++) {
+            if (A.c[c].width == 4)
+                static_cast<uint32_t *>(A.c[c].dst)[at] = static_cast<const uint32_t *>(A.c[c].src)[r];
+            else
+                static_cast<uint64_t *>(A.c[c].dst)[at] = static_cast<const uint64_t *>(A.c[c].src)[r];
+        }
+    }
+}
+
 // ---- the resident partitions' probe: one launch per input slice ------------------
 // Every resident partition's rows of the slice are probed against that
 // partition's table in one launch (tiles of 256 rows, each tile within one
@@ -635,6 +664,10 @@ class GraceJoin {
             P.join.reset();  // this resident table is done
         }
         for (;;) {
+            if (fb_.active) {
+                if (fallback_next(out)) return true;
+                continue;
+            }
             if (cur_join_) {
                 if (prefetch_.pending || cur_probe_ < cur_.probe_host.size()) {
                     DevBatch pb = prefetch_.pending ? take_prefetch() : load_group(cur_.probe_host, cur_probe_);
@@ -655,13 +688,15 @@ class GraceJoin {
             int64_t rows = 0;
             for (const HostChunk &c : t.build_host) rows += c.rows;
             if (t.probe_host.empty()) continue;  // no probe rows: nothing to emit
-            if (est_part_bytes(rows) > resident_cap() && t.level < kMaxLevel) {
+            if (est_part_bytes(rows) > resident_cap() && t.level < kMaxLevel && !no_shrink(t, rows)) {
                 split(t);
                 continue;
             }
-            if (est_part_bytes(rows) > resident_cap())
-                fail(KRV_NEED_MEMORY, "a partition of the build side stays above the memory budget after " +
-                                          std::to_string(kMaxLevel) + " levels of splits (one heavy key)");
+            if (est_part_bytes(rows) > resident_cap()) {
+                // Splitting cannot shrink it (one heavy key): the fallback.
+                start_fallback(std::move(t));
+                continue;
+            }
             krv_join_spec js = spec_;
             js.build_rows_hint = rows;
             cur_join_.reset(new HashJoin(rt_, js));
@@ -675,7 +710,9 @@ class GraceJoin {
         }
     }
 
-    bool done() const { return finishing_ && deferred_part_ >= nparts_ && !cur_join_ && tasks_.empty(); }
+    bool done() const {
+        return finishing_ && deferred_part_ >= nparts_ && !cur_join_ && tasks_.empty() && !fb_.active;
+    }
     // A zero-row batch of the output's shape.
     DevBatch empty_output() {
         if (!built_ || probe_types_.empty()) return DevBatch{};
@@ -1033,6 +1070,175 @@ class GraceJoin {
         DevBatch b = alloc_like(types, rows);
         copy_in(hs, b, rt_->stream);
         return b;
+    }
+
+    // ---- the fallback (join/fallback.rs: a partition that splitting
+    // cannot shrink joins by sort-merge, started at join/grace.rs:1006-1013)
+    // Here the same rows come from the build side in groups of chunks that
+    // each fit the resident share of the budget: every group's table joins
+    // every probe chunk (inner pairs, each probe row carrying its id), the
+    // ids of matched probe rows are marked, and for a left outer join the
+    // probe rows no group matched are padded at the end.
+    struct Fallback {
+        bool active = false;
+        std::vector<std::vector<HostChunk>> groups;
+        size_t group = 0;
+        std::unique_ptr<HashJoin> join;
+        std::vector<HostChunk> probe_host;
+        std::vector<long long> probe_base;  // id of each probe chunk's first row
+        size_t probe_at = 0;
+        DBuf matched;                        // a byte per probe row: matched by some group
+        bool padding = false;
+    } fb_;
+    int64_t fallbacks_ = 0;
+
+    // Whether the task's build side would not shrink: its rows all share one key.
+    bool no_shrink(const Task &t, int64_t rows) {
+        if (rows < 2) return true;
+        reap(true);  // the chunks' spill copies have landed
+        long long first = 0;
+        bool have = false;
+        for (const HostChunk &c : t.build_host)
+            if (c.rows) {
+                first = reinterpret_cast<const long long *>(c.cols[spec_.build_keys[0]])[0];
+                have = true;
+                break;
+            }
+        if (!have) return true;
+        for (const HostChunk &c : t.build_host) {
+            const long long *k = reinterpret_cast<const long long *>(c.cols[spec_.build_keys[0]]);
+            for (int64_t i = 0; i < c.rows; i++)
+                if (k[i] != first) return false;
+        }
+        return true;
+    }
+
+    void start_fallback(Task t) {
+        fallbacks_++;
+        fb_ = Fallback{};
+        fb_.active = true;
+        std::vector<HostChunk> g;
+        int64_t grows = 0;
+        for (HostChunk &c : t.build_host) {
+            if (!g.empty() && est_part_bytes(grows + c.rows) > resident_cap()) {
+                fb_.groups.push_back(std::move(g));
+                g.clear();
+                grows = 0;
+            }
+            grows += c.rows;
+            g.push_back(c);
+        }
+        if (!g.empty()) fb_.groups.push_back(std::move(g));
+        long long base = 0;
+        for (const HostChunk &c : t.probe_host) {
+            fb_.probe_base.push_back(base);
+            base += c.rows;
+        }
+        fb_.probe_host = std::move(t.probe_host);
+        if (spec_.join_type == KRV_JOIN_LEFT_OUTER) {
+            fb_.matched = DBuf(rt_, (size_t)std::max<long long>(base, 1));
+            KRV_CUDA(cudaMemsetAsync(fb_.matched.get(), 0, fb_.matched.bytes(), rt_->stream));
+        }
+    }
+
+    // The probe chunk at `at` with its row ids as a last column.
+    DevBatch load_with_ids(size_t at) {
+        DevBatch b = load(fb_.probe_host[at], probe_types_);
+        DevCol id;
+        id.type = DType{Type::I64, 0, 0};
+        id.name = "#row";
+        id.nullable = false;
+        id.length = b.rows;
+        id.hold_data = std::make_shared<DBuf>(rt_, (size_t)std::max<int64_t>(b.rows, 1) * 8);
+        id.data = id.hold_data->get();
+        if (b.rows) {
+            iota_kernel<<<grid_for(rt_, b.rows, 256, 4), 256, 0, rt_->stream>>>(id.hold_data->as<long long>(), b.rows,
+                                                                                fb_.probe_base[at]);
+            rt_->launches++;
+            check_launch("iota_kernel");
+        }
+        b.cols.push_back(id);
+        return b;
+    }
+
+    // The next output batch of the fallback; false when it produced none
+    // this step (the caller calls again until it is no longer active).
+    bool fallback_next(DevBatch &out) {
+        if (!fb_.padding) {
+            if (!fb_.join) {
+                if (fb_.group == fb_.groups.size()) {
+                    fb_.padding = spec_.join_type == KRV_JOIN_LEFT_OUTER;
+                    fb_.probe_at = 0;
+                    if (!fb_.padding) fb_ = Fallback{};
+                    return false;
+                }
+                // inner pairs of this group; the probe rows keep their id
+                krv_join_spec js = spec_;
+                js.join_type = KRV_JOIN_INNER;
+                js.runtime_filter = 0;
+                const int np = (int)probe_types_.size();
+                if (spec_.n_probe_out < 0) {
+                    js.n_probe_out = np + 1;
+                    for (int c = 0; c <= np; c++) js.probe_out[c] = c;
+                } else {
+                    js.probe_out[js.n_probe_out++] = np;
+                }
+                int64_t rows = 0;
+                for (const HostChunk &c : fb_.groups[fb_.group]) rows += c.rows;
+                js.build_rows_hint = rows;
+                fb_.join.reset(new HashJoin(rt_, js));
+                fb_.join->build_adopt(load_all(fb_.groups[fb_.group], build_types_));
+                fb_.join->build_finish();
+                fb_.probe_at = 0;
+            }
+            if (fb_.probe_at == fb_.probe_host.size()) {
+                fb_.join.reset();
+                fb_.group++;
+                return false;
+            }
+            const size_t at = fb_.probe_at++;
+            DevBatch o = fb_.join->probe(load_with_ids(at));
+            // the id column follows the probe columns
+            const int idc = spec_.n_probe_out < 0 ? (int)probe_types_.size() : spec_.n_probe_out;
+            if (fb_.matched.get() && o.rows) {
+                mark_matched_kernel<<<grid_for(rt_, o.rows, 256, 4), 256, 0, rt_->stream>>>(
+                    static_cast<const long long *>(o.cols[idc].data), o.rows, fb_.matched.as<uint8_t>());
+                rt_->launches++;
+                check_launch("mark_matched_kernel");
+            }
+            o.cols.erase(o.cols.begin() + idc);
+            counters_.output_rows += o.rows;
+            if (o.rows == 0) return false;
+            out = o;
+            return true;
+        }
+        // left outer: the probe rows no group matched, the build side NULL
+        if (fb_.probe_at == fb_.probe_host.size()) {
+            fb_ = Fallback{};
+            return false;
+        }
+        const size_t at = fb_.probe_at++;
+        DevBatch b = load(fb_.probe_host[at], probe_types_);
+        DevBatch keep = alloc_like(probe_types_, b.rows);
+        PartArgs A{};
+        A.n = b.rows;
+        A.ncols = (int)b.cols.size();
+        for (int c = 0; c < A.ncols; c++) A.c[c] = PartCol{b.cols[c].data, keep.cols[c].hold_data->get(), b.cols[c].type.width()};
+        DBuf cnt(rt_, 8);
+        KRV_CUDA(cudaMemsetAsync(cnt.get(), 0, 8, rt_->stream));
+        if (b.rows) {
+            compact_unmatched_kernel<<<grid_for(rt_, b.rows, 256, 4), 256, 0, rt_->stream>>>(
+                A, fb_.matched.as<uint8_t>(), fb_.probe_base[at], cnt.as<unsigned long long>());
+            rt_->launches++;
+            check_launch("compact_unmatched_kernel");
+        }
+        keep.rows = (int64_t)read_scalar<unsigned long long>(rt_, cnt.get());
+        for (DevCol &c : keep.cols) c.length = keep.rows;
+        if (keep.rows == 0) return false;
+        DevBatch o = null_join_->probe(keep);
+        counters_.output_rows += o.rows;
+        out = o;
+        return true;
     }
 
     // Splits task `t` 8 ways with the next level of hash bits, chunk by chunk.

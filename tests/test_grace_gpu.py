@@ -2,7 +2,10 @@
 unpartitioned join: the output multiset is exact for left outer and inner
 joins with NULL keys, heavy probe keys and duplicate build keys, whether the
 partitions stay in HBM, spill to host memory, or spill and split again; a
-partition of one key that cannot fit fails with NEED_MEMORY."""
+partition of one key that cannot fit joins by the fallback (the build side in
+groups that fit, probe rows padded once no group matched them) and gives the
+oracle's rows, where the reference falls back to a sort-merge join
+(crates/krishiv-exec/src/join/fallback.rs, started at join/grace.rs:1006-1013)."""
 import collections
 
 import numpy as np
@@ -113,10 +116,19 @@ def test_partitioned_equals_unpartitioned(kb, rt):
     assert a == b
 
 
-def test_one_heavy_build_key_that_cannot_fit(kb, rt):
+@pytest.mark.parametrize("jt", ["left_outer", "inner"])
+def test_one_heavy_build_key_that_cannot_fit(kb, rt, oracle, jt):
+    """50,000 build rows of one key under a 256 KiB budget: no split can shrink
+    that partition, so it joins by the fallback; the output is the oracle's
+    (every probe row of the key pairs with all 50,000 rows, the others are
+    padded or dropped)."""
     n = 50_000
-    build = (np.full(n, 42, np.int64), np.ones(n, bool), np.arange(n, dtype=np.int64), np.arange(n, dtype=np.int64))
-    probe = (np.array([42, 7], np.int64), np.ones(2, bool), np.array([1, 2], np.int64))
-    with pytest.raises(kb.KrvError) as e:
-        run(kb, rt, build, probe, "left_outer", True, budget=256 << 10)
-    assert e.value.status == kb.NEED_MEMORY
+    rng = np.random.default_rng(3)
+    build = (np.full(n, 42, np.int64), np.ones(n, bool), np.arange(n, dtype=np.int64),
+             rng.integers(-(2**62), 2**62, n).astype(np.int64))
+    pk = np.array([42, 7, 42, 9, 42] * 3, np.int64)
+    probe = (pk, np.ones(pk.size, bool), np.arange(pk.size, dtype=np.int64))
+    got, j = run(kb, rt, build, probe, jt, True, budget=256 << 10, batches=1)
+    want = oracle_rows(oracle, build, probe, jt)
+    assert got == want
+    assert sum(got.values()) == 9 * n + (6 if jt == "left_outer" else 0)
