@@ -683,7 +683,7 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
 
     def run_join(partitioned, r):
         spec = kb.join_spec("left_outer", probe_out=[0, 1], build_out=[1, 2], build_rows_hint=nb,
-                            max_output_rows=64 << 20)
+                            max_output_rows=64 << 20, max_load=args.max_load, radix_bits=args.radix_bits)
         j = kb.HashJoin(r, spec, partitioned=partitioned, device_budget=budget if partitioned else 0)
         t = [time.perf_counter()]
         for db in batches(build, nb, bstep):
@@ -784,7 +784,8 @@ def run_join(args, kb, W, rt, rank, world, pg, device):
     phase = {"build": [], "probe": []}
 
     def step(ev=None):
-        j = kb.HashJoin(rt, kb.join_spec("inner", probe_out=[0, 1], build_out=[1], build_rows_hint=nb))
+        j = kb.HashJoin(rt, kb.join_spec("inner", probe_out=[0, 1], build_out=[1], build_rows_hint=nb,
+                                         max_load=args.max_load))
         e = [torch.cuda.Event(enable_timing=True) for _ in range(3)] if ev is not None else None
         if e:
             e[0].record(stream)
@@ -822,6 +823,7 @@ def run_join(args, kb, W, rt, rank, world, pg, device):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64 keys", "data": "synthetic",
             "config": {"workload": "inner join 1M build x 10M probe (50% match), output (k, v, w)",
+                       "max_load": args.max_load or 0.5,
                        "build_rows": nb, "probe_rows": np_, "output_rows": out_rows,
                        "l2": "inputs (136 MB) larger than L2; each step rebuilds the table"},
             "gpu_launches": rt.launches - launches0,
@@ -908,6 +910,8 @@ def main():
     ap.add_argument("--serve-sweep", action="store_true",
                     help="serve: also sweep the offered load over 0.25x..1.5x of each mode's capacity")
     ap.add_argument("--grace-budget", type=int, default=24 << 30, help="grace: device budget of the join")
+    ap.add_argument("--max-load", type=float, default=0.0, help="join, grace: hash table load factor (0: default)")
+    ap.add_argument("--radix-bits", type=int, default=0, help="grace: level-0 partition bits (0: chosen)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     threads = os.cpu_count() or 1
