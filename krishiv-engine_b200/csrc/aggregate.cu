@@ -750,12 +750,15 @@ __device__ __forceinline__ int local_record(const AggPlanDev &P, const PartDev &
             // another thread claimed the slot: record e stays empty (no rows)
         }
         if (cur == k) {
+            // claimed by a lane of another warp (one lane per key and warp
+            // looks keys up): wait, bounded, for its record id
             for (int it = 0; it < (1 << 20); it++) {
                 const uint16_t e = *reinterpret_cast<volatile uint16_t *>(sidx + pos);
                 if (e != 0xFFFFu) {
                     __threadfence_block();
                     return e;
                 }
+                __nanosleep(20);
             }
             atomicOr(status, ST_TIMEOUT);
             return -1;
@@ -817,8 +820,15 @@ __global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, Ta
         const uint8_t *row = buf + (size_t)i * D.row_bytes;
         const long long k = live ? *reinterpret_cast<const long long *>(row) : 0;
         const uint64_t h = hash_word((uint64_t)k);
+        const unsigned lane = threadIdx.x & 31u;
         for (int attempt = 0; attempt < 2; attempt++) {
-            const int e = live ? local_record(P, D, skeys, sidx, rkeys, lrec, &s_fill, k, h, T.status) : 0;
+            // One lane per distinct key of the warp looks it up; the lanes of
+            // that key take its record (no lane waits on its own warp).
+            const unsigned peers = __match_any_sync(kFullMask, live ? k : kEmptyKey);
+            const int lead = __ffs(peers) - 1;
+            int e = 0;
+            if (live && (int)lane == lead) e = local_record(P, D, skeys, sidx, rkeys, lrec, &s_fill, k, h, T.status);
+            e = __shfl_sync(kFullMask, e, lead);
             if (!__syncthreads_or(e < 0)) {
                 if (live) fold_row(P, D.off_val, lrec + (size_t)e * P.rec, row);
                 break;

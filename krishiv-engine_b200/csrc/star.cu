@@ -627,7 +627,8 @@ class StarPipeline {
 
     template <int BMODE, bool VEC, bool KB32>
     void launch_scan(const StarArgs &A, int grid, size_t smem) {
-        auto kern = star_scan_kernel<BMODE, VEC, KB32>;
+        const bool nulls = A.v_fk_a || A.v_fk_b || A.v_price || A.v_disc;
+        auto kern = nulls ? star_scan_kernel<BMODE, VEC, KB32, true> : star_scan_kernel<BMODE, VEC, KB32, false>;
         KRV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<grid, kScanThreads, smem, rt_->stream>>>(A);
         rt_->launches++;
@@ -636,7 +637,8 @@ class StarPipeline {
 
     template <bool DIRECT, bool KB32>
     void launch_join(const StarArgs &A, int regions, int slices, int G) {
-        auto kern = star_join_kernel<DIRECT, KB32>;
+        const bool nulls = A.v_fk_a || A.v_fk_b || A.v_price || A.v_disc;
+        auto kern = nulls ? star_join_kernel<DIRECT, KB32, true> : star_join_kernel<DIRECT, KB32, false>;
         const size_t smem = star_join_smem(G);
         KRV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<regions * slices, kJoinThreads, smem, rt_->stream>>>(A, regions, slices, G);

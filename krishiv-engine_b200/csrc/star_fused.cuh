@@ -132,7 +132,9 @@ __device__ __forceinline__ void star_load_tile(const StarArgs &A, int64_t r0, lo
 // ---- stage 1 ------------------------------------------------------------------------
 // BMODE 1: B's answer bitmap in shared memory; 0: B's filter probed per row.
 // KB32: survivors keep fk_b - lo in 32 bits.
-template <int BMODE, bool VEC, bool KB32>
+// NULLS: fact columns with validity bitmaps (compiled apart, so the kernel for
+// columns without NULLs tests no bits).
+template <int BMODE, bool VEC, bool KB32, bool NULLS>
 __global__ void __launch_bounds__(kScanThreads, 1) star_scan_kernel(StarArgs A) {
     extern __shared__ __align__(16) uint8_t smem[];
     uint32_t *s_bits = reinterpret_cast<uint32_t *>(smem);
@@ -181,7 +183,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) star_scan_kernel(StarArgs A) 
                 p = filter_pass(A.fb, cur[u]);
             }
             if (!full && r0 + u >= A.n) p = false;
-            if (A.v_fk_b && p && !bit_get(A.v_fk_b, A.o_fk_b, r0 + u)) p = false;
+            if (NULLS && p && !bit_get(A.v_fk_b, A.o_fk_b, r0 + u)) p = false;
             m |= (unsigned)p << u;
         }
         // fk_a's 32-byte sectors of the passing rows will be read by stage 2.
@@ -279,7 +281,7 @@ __device__ __forceinline__ void star_filterk(const KeyFilterDev &f, const long l
 // DIRECT: both dimensions have direct indexes; KB32 as in the scan. Each
 // thread takes two survivors per step, each stage's loads issued together,
 // so a thread keeps two probe chains in flight.
-template <bool DIRECT, bool KB32>
+template <bool DIRECT, bool KB32, bool NULLS>
 __global__ void __launch_bounds__(kJoinThreads, 2) star_join_kernel(StarArgs A, int regions, int slices, int G) {
     extern __shared__ __align__(16) uint8_t smem[];
     constexpr int kWarps = kJoinThreads / 32;
@@ -333,7 +335,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) star_join_kernel(StarArgs A, 
 #pragma unroll
             for (int j = 0; j < kK; j++) pa[j] = has[j];
         }
-        if (A.v_fk_a) {
+        if (NULLS) {
 #pragma unroll
             for (int j = 0; j < kK; j++) pa[j] = pa[j] && bit_get(A.v_fk_a, A.o_fk_a, row[j]);
         }
@@ -345,7 +347,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) star_join_kernel(StarArgs A, 
                 g[j] = A.group_by == 0 ? ga[j] : gb[j];
                 v[j] = 0.0;
                 if (hit[j]) {
-                    if (star_value_null(A, row[j])) atomicAdd(A.nulls + g[j], 1ull);
+                    if (NULLS && star_value_null(A, row[j])) atomicAdd(A.nulls + g[j], 1ull);
                     else v[j] = __dmul_rn((double)__ldcs(A.price + row[j]), __dsub_rn(1.0, __ldcs(A.disc + row[j])));
                 }
             }
@@ -373,7 +375,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) star_join_kernel(StarArgs A, 
                     if (ra != kStarNone) rb0 = star_lookup(A.tb, kb[j]);
                 }
                 const bool h = ra != kStarNone && rb0 != kStarNone;
-                const bool vnull = h && star_value_null(A, row[j]);
+                const bool vnull = NULLS && h && star_value_null(A, row[j]);
                 double vv = 0.0;
                 if (h && !vnull) vv = __dmul_rn((double)__ldcs(A.price + row[j]), __dsub_rn(1.0, __ldcs(A.disc + row[j])));
                 unsigned pend = __ballot_sync(0xFFFFFFFFu, h);
