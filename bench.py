@@ -846,11 +846,22 @@ def run_agg(args, kb, W, rt, rank, world, pg, device):
     n = int(cols[0][1].shape[0])
     aggs = [(f, c) for c in (1, 2, 3) for f in ("sum", "count", "min", "max", "avg")]
 
-    def step(mode):
+    phase_ev = []
+
+    def step(mode, ev=None):
         a = kb.HashAggregate(rt, kb.agg_spec(0, aggs, mode=mode, expected_groups=1_000_000))
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)] if ev is not None else None
+        if e:
+            e[0].record(stream)
         a.push_device(db)
         a.finish()
-        return a.result_device()
+        if e:
+            e[1].record(stream)
+        r = a.result_device()
+        if e:
+            e[2].record(stream)
+            ev.append(e)
+        return r
 
     res, clocks = {}, {}
     for mode, name in ((kb.MODE_SHARED, "shared"), (kb.MODE_GLOBAL, "global")):
@@ -863,7 +874,7 @@ def run_agg(args, kb, W, rt, rank, world, pg, device):
         with Clocks(device) as clk:
             s.record(stream)
             for _ in range(args.steps):
-                r = step(mode)
+                r = step(mode, phase_ev if name == "shared" else None)
             e.record(stream)
             torch.cuda.synchronize()
         clocks[name] = clk.summary()
@@ -878,6 +889,8 @@ def run_agg(args, kb, W, rt, rank, world, pg, device):
                                             "rows": n, "groups": groups,
                                             "l2": "inputs (2.8 GB) larger than L2; no flush"},
             "gpu_launches": launches,
+            "phases_ms": {"push": statistics.median(x[0].elapsed_time(x[1]) for x in phase_ev),
+                          "result": statistics.median(x[1].elapsed_time(x[2]) for x in phase_ev)},
             "plain_global_table": {"ms_per_step": res["global"][0], "value": world * n / (res["global"][0] * 1e-3) / 1e6},
             "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "peak_source": kind,
                          "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None,

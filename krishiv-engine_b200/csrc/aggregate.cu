@@ -466,6 +466,10 @@ __global__ void __launch_bounds__(kAggThreads) agg_shared_kernel(AggPlanDev P, T
 //     and the partition stops there to run again after the host grows the table.
 // Row records: key (8 B) at 0, the validity word (bit c: plan column c valid)
 // at 8, values at off_val[c] (4-byte values from 12, then 8- and 16-byte ones).
+// Shared-memory records are laid out P.rec + 8 bytes apart: an odd number of
+// 8-byte words, so one field of 32 different records falls in 32 different
+// 8-byte bank pairs.
+__host__ __device__ __forceinline__ int smem_stride(const AggPlanDev &P) { return P.rec + 8; }
 constexpr int kHotMax = 512;
 constexpr int kSplitThreads = 512;
 constexpr int kPartThreads = 512;
@@ -553,7 +557,7 @@ __device__ __forceinline__ void hot_rows(const AggPlanDev &P, uint8_t *hrec, int
     const unsigned lead_lane = __ffs(peers) - 1;
     const bool lead = hot && lane == lead_lane;
     const unsigned turns = __reduce_max_sync(kFullMask, hot ? (unsigned)__popc(peers) : 1u);
-    uint8_t *rec = hrec + (size_t)(hot ? hi : 0) * P.rec;
+    uint8_t *rec = hrec + (size_t)(hot ? hi : 0) * smem_stride(P);
     if (lead) atomicAdd(reinterpret_cast<unsigned long long *>(rec + P.off_rows), (unsigned long long)__popc(peers));
     for (int c = 0; c < P.ncols; c++) {
         const AggColDev &C = P.c[c];
@@ -636,10 +640,10 @@ __global__ void __launch_bounds__(kSplitThreads) agg_split_kernel(AggPlanDev P, 
     extern __shared__ __align__(16) uint8_t smem[];
     const int NH = S.H + 2;
     uint8_t *hrec = smem;                                                          // NH records
-    long long *hkeys = reinterpret_cast<long long *>(hrec + (size_t)NH * P.rec);   // hot_slots
+    long long *hkeys = reinterpret_cast<long long *>(hrec + (size_t)NH * smem_stride(P));   // hot_slots
     int16_t *hidx = reinterpret_cast<int16_t *>(hkeys + S.hot_slots);              // hot_slots
     const unsigned lane = threadIdx.x & 31u;
-    for (int e = threadIdx.x; e < NH; e += blockDim.x) init_record(P, hrec + (size_t)e * P.rec);
+    for (int e = threadIdx.x; e < NH; e += blockDim.x) init_record(P, hrec + (size_t)e * smem_stride(P));
     for (int e = threadIdx.x; e < S.hot_slots; e += blockDim.x) {
         hkeys[e] = kEmptyKey;
         hidx[e] = -1;
@@ -689,7 +693,8 @@ __global__ void __launch_bounds__(kSplitThreads) agg_split_kernel(AggPlanDev P, 
     }
     __syncthreads();
     for (int e = threadIdx.x; e < NH; e += blockDim.x) {
-        if (S.hot_gids[e] < kOverflowGid) merge_record(P, T.states + (size_t)S.hot_gids[e] * P.rec, hrec + (size_t)e * P.rec);
+        if (S.hot_gids[e] < kOverflowGid)
+            merge_record(P, T.states + (size_t)S.hot_gids[e] * P.rec, hrec + (size_t)e * smem_stride(P));
         else atomicOr(T.status, ST_CAPACITY);
     }
 }
@@ -727,42 +732,27 @@ __device__ __forceinline__ void fold_row(const AggPlanDev &P, const int16_t *off
 }
 
 // The local record of key k, claimed (and initialised) when new; -1 when the
-// table has no record left or a wait gave up.
-__device__ __forceinline__ int local_record(const AggPlanDev &P, const PartDev &D, long long *skeys, uint16_t *sidx,
-                                            long long *rkeys, uint8_t *lrec, int *fill, long long k, uint64_t h,
-                                            uint32_t *status) {
+// table has no record left. A slot holds a record index (0xFFFF: free); the
+// record's key is written before the slot is claimed, so a reader that finds
+// the slot taken compares the key at once and never waits.
+__device__ __forceinline__ int local_record(const AggPlanDev &P, const PartDev &D, uint16_t *sidx, long long *rkeys,
+                                            uint8_t *lrec, int *fill, long long k, uint64_t h) {
     const int mask = D.slots - 1;
     int pos = (int)(h & (uint64_t)mask);
     for (int t = 0; t < D.slots; t++) {
-        long long cur = *reinterpret_cast<volatile long long *>(skeys + pos);
-        if (cur == kEmptyKey) {
+        uint16_t cur = *reinterpret_cast<volatile uint16_t *>(sidx + pos);
+        if (cur == 0xFFFFu) {
             const int e = atomicAdd(fill, 1);
             if (e >= D.L) return -1;
-            init_record(P, lrec + (size_t)e * P.rec);
+            init_record(P, lrec + (size_t)e * smem_stride(P));
             rkeys[e] = k;
             __threadfence_block();
-            cur = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(skeys + pos), (unsigned long long)kEmptyKey,
-                                       (unsigned long long)k);
-            if (cur == kEmptyKey) {
-                *reinterpret_cast<volatile uint16_t *>(sidx + pos) = (uint16_t)e;
-                return e;
-            }
-            // another thread claimed the slot: record e stays empty (no rows)
+            cur = atomicCAS(reinterpret_cast<unsigned short *>(sidx + pos), (unsigned short)0xFFFFu, (unsigned short)e);
+            if (cur == 0xFFFFu) return e;
+            // another key (or this one) took the slot first: record e stays empty
         }
-        if (cur == k) {
-            // claimed by a lane of another warp (one lane per key and warp
-            // looks keys up): wait, bounded, for its record id
-            for (int it = 0; it < (1 << 20); it++) {
-                const uint16_t e = *reinterpret_cast<volatile uint16_t *>(sidx + pos);
-                if (e != 0xFFFFu) {
-                    __threadfence_block();
-                    return e;
-                }
-                __nanosleep(20);
-            }
-            atomicOr(status, ST_TIMEOUT);
-            return -1;
-        }
+        __threadfence_block();
+        if (*reinterpret_cast<volatile long long *>(rkeys + cur) == k) return cur;
         pos = (pos + 1) & mask;
     }
     return -1;
@@ -774,7 +764,7 @@ __device__ bool flush_local(const AggPlanDev &P, const TableDev &T, const PartDe
                             uint8_t *lrec, uint32_t *lgid, int m, int *fail) {
     for (int e = threadIdx.x; e < m; e += blockDim.x) {
         uint32_t g = kPending;
-        if (*reinterpret_cast<const unsigned long long *>(lrec + (size_t)e * P.rec + P.off_rows)) {
+        if (*reinterpret_cast<const unsigned long long *>(lrec + (size_t)e * smem_stride(P) + P.off_rows)) {
             g = find_or_insert(T, P, rkeys[e]);
             if (g == kOverflowGid) atomicOr(fail, 1);
         }
@@ -784,18 +774,18 @@ __device__ bool flush_local(const AggPlanDev &P, const TableDev &T, const PartDe
     const bool ok = *reinterpret_cast<volatile int *>(fail) == 0;
     if (ok)
         for (int e = threadIdx.x; e < m; e += blockDim.x)
-            if (lgid[e] != kPending) merge_record(P, T.states + (size_t)lgid[e] * P.rec, lrec + (size_t)e * P.rec);
+            if (lgid[e] != kPending)
+                merge_record(P, T.states + (size_t)lgid[e] * P.rec, lrec + (size_t)e * smem_stride(P));
     __syncthreads();
     return ok;
 }
 
 __global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, TableDev T, PartDev D) {
     extern __shared__ __align__(16) uint8_t smem[];
-    uint8_t *lrec = smem;                                                            // L records
-    long long *rkeys = reinterpret_cast<long long *>(lrec + (size_t)D.L * P.rec);    // L keys
-    long long *skeys = rkeys + D.L;                                                  // slots
-    uint16_t *sidx = reinterpret_cast<uint16_t *>(skeys + D.slots);                  // slots
-    uint32_t *lgid = reinterpret_cast<uint32_t *>(sidx + D.slots);                   // L
+    uint8_t *lrec = smem;                                                                   // L records
+    long long *rkeys = reinterpret_cast<long long *>(lrec + (size_t)D.L * smem_stride(P));  // L keys
+    uint32_t *lgid = reinterpret_cast<uint32_t *>(rkeys + D.L);                             // L
+    uint16_t *sidx = reinterpret_cast<uint16_t *>(lgid + D.L);                              // slots
     __shared__ int s_fill, s_fail;
     const int p = D.todo[blockIdx.x];
     const uint32_t cnt = D.part_cnt[(size_t)p * kCntStride];
@@ -803,10 +793,7 @@ __global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, Ta
     const uint8_t *buf = D.part_buf + (size_t)p * D.cap * D.row_bytes;
     uint32_t window = D.start[p];
     auto reset = [&]() {
-        for (int s = threadIdx.x; s < D.slots; s += blockDim.x) {
-            skeys[s] = kEmptyKey;
-            sidx[s] = 0xFFFFu;
-        }
+        for (int s = threadIdx.x; s < D.slots; s += blockDim.x) sidx[s] = 0xFFFFu;
         if (threadIdx.x == 0) {
             s_fill = 0;
             s_fail = 0;
@@ -827,10 +814,10 @@ __global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, Ta
             const unsigned peers = __match_any_sync(kFullMask, live ? k : kEmptyKey);
             const int lead = __ffs(peers) - 1;
             int e = 0;
-            if (live && (int)lane == lead) e = local_record(P, D, skeys, sidx, rkeys, lrec, &s_fill, k, h, T.status);
+            if (live && (int)lane == lead) e = local_record(P, D, sidx, rkeys, lrec, &s_fill, k, h);
             e = __shfl_sync(kFullMask, e, lead);
             if (!__syncthreads_or(e < 0)) {
-                if (live) fold_row(P, D.off_val, lrec + (size_t)e * P.rec, row);
+                if (live) fold_row(P, D.off_val, lrec + (size_t)e * smem_stride(P), row);
                 break;
             }
             // The table is full: merge the window's rows (those before this
@@ -1461,7 +1448,7 @@ void HashAggregate::plan(const DevBatch &b) {
     // agg_part_kernel, with slots for twice as many keys.
     {
         const int L = kPartThreads;
-        const size_t smem = (size_t)L * (P_.rec + 8 + 4) + (size_t)next_pow2((uint64_t)2 * L) * 10;
+        const size_t smem = (size_t)L * (smem_stride(P_) + 8 + 4) + (size_t)next_pow2((uint64_t)2 * L) * 2;
         part_local_ = smem <= (size_t)rt_->max_smem_optin - 1024 ? L : 0;
         part_smem_ = smem;
     }
@@ -1499,6 +1486,9 @@ void HashAggregate::alloc_table(uint64_t slots) {
 }
 
 void HashAggregate::grow(uint64_t need_groups) {
+    // the records to carry over: every group the device has handed out
+    known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());
+    pending_rows_ = 0;
     DBuf okeys = std::move(keys_), ogids = std::move(gids_);
     const uint64_t oslots = slots_;
     uint64_t ns = next_pow2(std::max<uint64_t>(oslots * 2, need_groups * 2));
@@ -1663,7 +1653,8 @@ void HashAggregate::plan_partitioned(const KeyIn &key, int64_t n) {
     // holds records for beside its lookup table.
     const int smem_cap = std::min(rt_->max_smem_optin - 2048, 72 * 1024);
     int hmax = kHotMax;
-    while (hmax > 0 && (size_t)(hmax + 2) * P_.rec + (size_t)2 * next_pow2(hmax) * 10 > (size_t)smem_cap) hmax /= 2;
+    while (hmax > 0 && (size_t)(hmax + 2) * smem_stride(P_) + (size_t)2 * next_pow2(hmax) * 10 > (size_t)smem_cap)
+        hmax /= 2;
     std::vector<long long> hot;
     int hot_rows = 0;
     for (const auto &rk : runs) {
@@ -1741,6 +1732,7 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
         P.c[c].voff = col.valid_off;
         widths[c] = col.type.width();
     }
+    known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());  // the hot keys' groups too
     const int L = part_local_;
     // Partitions: each to hold about L/2 distinct keys.
     int bits = 5;
@@ -1748,7 +1740,7 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
     const int nparts = 1 << bits;
     const int H = part_hot_;
     const int hot_slots = H ? (int)next_pow2((uint64_t)2 * H) : 0;
-    const size_t split_smem = (size_t)(H + 2) * P.rec + (size_t)hot_slots * 10;
+    const size_t split_smem = (size_t)(H + 2) * smem_stride(P) + (size_t)hot_slots * 10;
     KRV_CUDA(cudaFuncSetAttribute(agg_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)split_smem));
     KRV_CUDA(cudaFuncSetAttribute(agg_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)part_smem_));
     int split_blocks = 0, part_blocks = 0;
