@@ -548,54 +548,72 @@ __device__ __forceinline__ void fold_partial(const AggColDev &C, uint8_t *r, uns
     }
 }
 
-// The hot rows of one warp step: the lanes of each hot key (`hi`, -1 when the
-// lane has none) reduce their values to the key's lowest lane, which folds
-// them into the key's shared-memory record: one update per key and warp step.
+// The hot rows of one warp step (`hi`: the lane's hot key, -1 when none),
+// folded into the CTA's shared-memory records. Counts of a key's lanes go in
+// one update (population counts of the warp's ballots); integer sums and
+// MIN/MAX go in per lane (shared atomics, the lanes of one key served by one
+// instruction); float64 sums, which must stay compensated, are reduced to the
+// key's lowest lane first (TwoSum over the other lanes' values) and added as
+// one double-double.
 __device__ __forceinline__ void hot_rows(const AggPlanDev &P, uint8_t *hrec, int64_t r, int hi, unsigned lane) {
     const bool hot = hi >= 0;
     const unsigned peers = __match_any_sync(kFullMask, hot ? hi : 0x40000 + (int)lane);
     const unsigned lead_lane = __ffs(peers) - 1;
     const bool lead = hot && lane == lead_lane;
-    const unsigned turns = __reduce_max_sync(kFullMask, hot ? (unsigned)__popc(peers) : 1u);
     uint8_t *rec = hrec + (size_t)(hot ? hi : 0) * smem_stride(P);
     if (lead) atomicAdd(reinterpret_cast<unsigned long long *>(rec + P.off_rows), (unsigned long long)__popc(peers));
+    unsigned turns = 0;  // the largest key group of the warp, for the float sums
     for (int c = 0; c < P.ncols; c++) {
         const AggColDev &C = P.c[c];
         const bool v = hot && bit_get(C.valid, C.voff, r);
         const unsigned vm = __ballot_sync(kFullMask, v) & peers;
-        const bool any = (C.flags & (F_SUM | F_MIN | F_MAX)) != 0;
+        if (lead && vm) atomicAdd(reinterpret_cast<unsigned long long *>(rec + C.off_count), (unsigned long long)__popc(vm));
+        if (!(C.flags & (F_SUM | F_MIN | F_MAX))) continue;
         uint64_t lo = 0, hw = 0;
-        if (v && any) value_words(C, C.data, r, lo, hw);
-        const bool f64 = C.type == (int)Type::F64;
-        // this lane's value, then the other lanes of its key
-        uint64_t slo = v ? lo : 0, shi = v ? hw : 0;
-        double ds = (v && f64) ? __longlong_as_double((long long)lo) : 0.0, de = 0.0;
-        long long mn = v ? mm_key(C, lo) : LLONG_MAX, mx = v ? mm_key(C, lo) : LLONG_MIN;
-        if (any) {
-            unsigned rest = peers & (peers - 1u);
-            for (unsigned t = 1; t < turns; t++) {
-                const unsigned src = rest ? (unsigned)__ffs(rest) - 1u : lane;
-                rest &= rest - 1u;
-                const uint64_t xlo = __shfl_sync(kFullMask, lo, src);
-                const uint64_t xhi = __shfl_sync(kFullMask, hw, src);
-                if (src != lane && ((vm >> src) & 1u)) {
-                    if (f64) {
-                        double s, e;
-                        two_sum(ds, __longlong_as_double((long long)xlo), s, e);
-                        ds = s;
-                        de = __dadd_rn(de, e);
-                    } else {
-                        const uint64_t o = slo;
-                        slo += xlo;
-                        shi += xhi + (slo < o ? 1ull : 0ull);
+        if (v) value_words(C, C.data, r, lo, hw);
+        const bool i32 = C.type == (int)Type::I32 || C.type == (int)Type::Date32;
+        if (C.type == (int)Type::F64) {
+            if (C.flags & F_SUM) {
+                if (!turns) turns = __reduce_max_sync(kFullMask, hot ? (unsigned)__popc(peers) : 1u);
+                double ds = v ? __longlong_as_double((long long)lo) : 0.0, de = 0.0;
+                unsigned rest = peers & (peers - 1u);
+                for (unsigned t = 1; t < turns; t++) {
+                    const unsigned src = rest ? (unsigned)__ffs(rest) - 1u : lane;
+                    rest &= rest - 1u;
+                    const double x = __shfl_sync(kFullMask, __longlong_as_double((long long)lo), src);
+                    if (src != lane && ((vm >> src) & 1u)) {
+                        double sum, err;
+                        two_sum(ds, x, sum, err);
+                        ds = sum;
+                        de = __dadd_rn(de, err);
                     }
-                    const long long k = mm_key(C, xlo);
-                    mn = k < mn ? k : mn;
-                    mx = k > mx ? k : mx;
                 }
+                if (lead && vm)
+                    atomic_add_dd2(reinterpret_cast<double *>(rec + C.off_sum),
+                                   reinterpret_cast<double *>(rec + C.off_sum + 8), ds, de);
             }
+            if (v && (C.flags & (F_MIN | F_MAX))) {
+                const unsigned long long key = f64_order_key(__longlong_as_double((long long)lo));
+                if (C.flags & F_MIN) atomicMin(reinterpret_cast<unsigned long long *>(rec + C.off_min), key);
+                if (C.flags & F_MAX) atomicMax(reinterpret_cast<unsigned long long *>(rec + C.off_max), key);
+            }
+            continue;
         }
-        if (lead && vm) fold_partial(C, rec, (unsigned long long)__popc(vm), slo, shi, ds, de, mn, mx);
+        if (!v) continue;
+        if (C.flags & F_SUM) {
+            if (i32) atomicAdd(reinterpret_cast<unsigned long long *>(rec + C.off_sum), (unsigned long long)lo);
+            else
+                atomic_add_i128(reinterpret_cast<unsigned long long *>(rec + C.off_sum),
+                                reinterpret_cast<long long *>(rec + C.off_sum + 8), (int64_t)lo, (int64_t)hw);
+        }
+        if (C.flags & F_MIN) {
+            if (i32) atomicMin(reinterpret_cast<int *>(rec + C.off_min), (int)lo);
+            else atomicMin(reinterpret_cast<long long *>(rec + C.off_min), (long long)lo);
+        }
+        if (C.flags & F_MAX) {
+            if (i32) atomicMax(reinterpret_cast<int *>(rec + C.off_max), (int)lo);
+            else atomicMax(reinterpret_cast<long long *>(rec + C.off_max), (long long)lo);
+        }
     }
 }
 
