@@ -620,8 +620,8 @@ __device__ __forceinline__ void hot_rows(const AggPlanDev &P, uint8_t *hrec, int
 // The cold rows of one warp step: each lane's row into its partition (one
 // counter update per partition and warp step); a row that meets a full
 // partition is listed for the global table instead.
-__device__ __forceinline__ void cold_rows(const AggPlanDev &P, const SplitDev &S, int64_t r, long long k, uint64_t h,
-                                          bool cold, unsigned lane) {
+__device__ __forceinline__ void cold_rows(const AggPlanDev &P, const SplitDev &S, const int16_t *off_val, int64_t r,
+                                          long long k, uint64_t h, bool cold, unsigned lane) {
     const int p = cold ? (int)(h >> (64 - S.part_bits)) : -1 - (int)lane;
     const unsigned peers = __match_any_sync(kFullMask, p);
     const unsigned lead_lane = __ffs(peers) - 1;
@@ -642,7 +642,7 @@ __device__ __forceinline__ void cold_rows(const AggPlanDev &P, const SplitDev &S
         if (!bit_get(C.valid, C.voff, r)) continue;
         bits |= 1u << c;
         if (!(C.flags & (F_SUM | F_MIN | F_MAX))) continue;
-        uint8_t *dst = row + S.off_val[c];
+        uint8_t *dst = row + off_val[c];
         if (C.type == (int)Type::I32 || C.type == (int)Type::Date32)
             *reinterpret_cast<int *>(dst) = static_cast<const int *>(C.data)[r];
         else if (C.type == (int)Type::Dec128)
@@ -661,6 +661,8 @@ __global__ void __launch_bounds__(kSplitThreads) agg_split_kernel(AggPlanDev P, 
     long long *hkeys = reinterpret_cast<long long *>(hrec + (size_t)NH * smem_stride(P));   // hot_slots
     int16_t *hidx = reinterpret_cast<int16_t *>(hkeys + S.hot_slots);              // hot_slots
     const unsigned lane = threadIdx.x & 31u;
+    __shared__ int16_t s_off[kMaxValueCols];  // row record offsets (read with a varying index)
+    if (threadIdx.x < kMaxValueCols) s_off[threadIdx.x] = S.off_val[threadIdx.x];
     for (int e = threadIdx.x; e < NH; e += blockDim.x) init_record(P, hrec + (size_t)e * smem_stride(P));
     for (int e = threadIdx.x; e < S.hot_slots; e += blockDim.x) {
         hkeys[e] = kEmptyKey;
@@ -707,7 +709,7 @@ __global__ void __launch_bounds__(kSplitThreads) agg_split_kernel(AggPlanDev P, 
         }
         if (__any_sync(kFullMask, hi >= 0)) hot_rows(P, hrec, r, hi, lane);
         const bool cold = live && hi < 0;
-        if (__any_sync(kFullMask, cold)) cold_rows(P, S, r, k, h, cold, lane);
+        if (__any_sync(kFullMask, cold)) cold_rows(P, S, s_off, r, k, h, cold, lane);
     }
     __syncthreads();
     for (int e = threadIdx.x; e < NH; e += blockDim.x) {
@@ -805,6 +807,8 @@ __global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, Ta
     uint32_t *lgid = reinterpret_cast<uint32_t *>(rkeys + D.L);                             // L
     uint16_t *sidx = reinterpret_cast<uint16_t *>(lgid + D.L);                              // slots
     __shared__ int s_fill, s_fail;
+    __shared__ int16_t s_off[kMaxValueCols];  // row record offsets (read with a varying index)
+    if (threadIdx.x < kMaxValueCols) s_off[threadIdx.x] = D.off_val[threadIdx.x];
     const int p = D.todo[blockIdx.x];
     const uint32_t cnt = D.part_cnt[(size_t)p * kCntStride];
     const uint32_t rows = cnt < D.cap ? cnt : D.cap;
@@ -835,7 +839,7 @@ __global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, Ta
             if (live && (int)lane == lead) e = local_record(P, D, sidx, rkeys, lrec, &s_fill, k, h);
             e = __shfl_sync(kFullMask, e, lead);
             if (!__syncthreads_or(e < 0)) {
-                if (live) fold_row(P, D.off_val, lrec + (size_t)e * smem_stride(P), row);
+                if (live) fold_row(P, s_off, lrec + (size_t)e * smem_stride(P), row);
                 break;
             }
             // The table is full: merge the window's rows (those before this
