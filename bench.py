@@ -674,6 +674,7 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
     capped = kb.Runtime(device, budget, stream.cuda_stream)
     bstep, pstep = 32 << 20, 32 << 20
     phases = {}
+    step_phases = []
 
     def batches(cols, n, step):
         for r0 in range(0, n, step):
@@ -692,8 +693,12 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
         torch.cuda.synchronize()
         t.append(time.perf_counter())
         total, rows, nbatches = 0, 0, 0
+        calls = []  # host wall time of each probe call (to find stalls)
         for db in batches(probe, np_, pstep):
-            for res in j.probe_device_all(db):
+            c0 = time.perf_counter()
+            outs = j.probe_device_all(db)
+            calls.append((time.perf_counter() - c0) * 1e3)
+            for res in outs:
                 c, n = output_checksum(res)
                 total, rows, nbatches = (total + c) & (2**64 - 1), rows + n, nbatches + 1
         torch.cuda.synchronize()
@@ -703,7 +708,11 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
             total, rows, nbatches = (total + c) & (2**64 - 1), rows + n, nbatches + 1
         torch.cuda.synchronize()
         t.append(time.perf_counter())
-        phases.update(build_s=t[1] - t[0], probe_s=t[2] - t[1], finish_s=t[3] - t[2], output_batches=nbatches)
+        calls.sort()
+        phases.update(build_s=t[1] - t[0], probe_s=t[2] - t[1], finish_s=t[3] - t[2], output_batches=nbatches,
+                      probe_calls=len(calls), probe_call_ms_median=statistics.median(calls) if calls else None,
+                      probe_call_ms_slowest=calls[-5:])
+        step_phases.append(dict(phases))
         return j, total, rows
 
     for _ in range(args.warmup):
@@ -744,7 +753,9 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
                       "consumer": "every output batch read once by an order-independent checksum (timed)",
                       "l2": "inputs (44 GB) larger than L2; no flush"},
            "wall_ms_per_step": statistics.median(w for _, w in times),
+           "steps_ms": [round(t, 1) for t, _ in times],
            "phases": dict(last_phases),
+           "step_phases": step_phases[-args.steps:],
            "checksum_agrees": (total, rows) == (want_total, want_rows),
            "gpu_launches": (launches1 - launches0) // max(1, args.steps),
            "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "peak_source": kind,

@@ -22,6 +22,7 @@
 // MIN/MAX of floats use an order-preserving integer map with NaN largest.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <string>
 
 #include "krv_device.cuh"
@@ -484,9 +485,8 @@ struct SplitDev {
     int part_bits;  // >= 1
     int row_bytes;
     int16_t off_val[kMaxValueCols];
-    uint8_t *part_buf;          // partition p: rows [p * cap, (p + 1) * cap)
-    unsigned int *part_cnt;     // partition p's row count at part_cnt[p * kCntStride]
-    uint32_t cap;
+    uint8_t *part_buf;          // partition p: rows [base_p, base_p + cap_p)
+    unsigned int *part_info;    // partition p's line at p * kCntStride: [0] rows written, [1] cap_p, [2..3] base_p
     uint32_t *ovf_rows;         // rows that met a full partition (aggregated afterwards)
     unsigned long long *ovf_count;
     int64_t row0;               // the batch row of this slice's row 0 (ovf_rows hold batch rows)
@@ -626,15 +626,16 @@ __device__ __forceinline__ void cold_rows(const AggPlanDev &P, const SplitDev &S
     const unsigned peers = __match_any_sync(kFullMask, p);
     const unsigned lead_lane = __ffs(peers) - 1;
     unsigned base = 0;
-    if (cold && lane == lead_lane) base = atomicAdd(S.part_cnt + (size_t)p * kCntStride, (unsigned)__popc(peers));
+    unsigned int *line = S.part_info + (size_t)(cold ? p : 0) * kCntStride;
+    if (cold && lane == lead_lane) base = atomicAdd(line, (unsigned)__popc(peers));
     base = __shfl_sync(kFullMask, base, lead_lane);
     if (!cold) return;
     const unsigned at = base + __popc(peers & ((1u << lane) - 1u));
-    if (at >= S.cap) {
+    if (at >= line[1]) {
         S.ovf_rows[atomicAdd(S.ovf_count, 1ull)] = (uint32_t)(S.row0 + r);
         return;
     }
-    uint8_t *row = S.part_buf + ((size_t)p * S.cap + at) * S.row_bytes;
+    uint8_t *row = S.part_buf + (*reinterpret_cast<const unsigned long long *>(line + 2) + at) * S.row_bytes;
     *reinterpret_cast<long long *>(row) = k;
     uint32_t bits = 0;
     for (int c = 0; c < P.ncols; c++) {
@@ -721,8 +722,7 @@ __global__ void __launch_bounds__(kSplitThreads) agg_split_kernel(AggPlanDev P, 
 
 struct PartDev {
     const uint8_t *part_buf;
-    const unsigned int *part_cnt;
-    uint32_t cap;
+    const unsigned int *part_info;  // as SplitDev::part_info
     int row_bytes;
     int16_t off_val[kMaxValueCols];
     const int *todo;   // the partitions to run: CTA b runs partition todo[b]
@@ -752,40 +752,60 @@ __device__ __forceinline__ void fold_row(const AggPlanDev &P, const int16_t *off
 }
 
 // The local record of key k, claimed (and initialised) when new; -1 when the
-// table has no record left. A slot holds a record index (0xFFFF: free); the
-// record's key is written before the slot is claimed, so a reader that finds
-// the slot taken compares the key at once and never waits.
-__device__ __forceinline__ int local_record(const AggPlanDev &P, const PartDev &D, uint16_t *sidx, long long *rkeys,
-                                            uint8_t *lrec, int *fill, long long k, uint64_t h) {
+// table has no record left or a wait gave up. The key claims its slot first;
+// only the claimer takes a record (so no record is ever wasted, and a
+// partition's tile of at most L keys always fits an emptied table) and then
+// publishes its index. A reader of the same key waits, bounded, for it: one
+// lane per key and warp looks keys up, so the claimer is in another warp.
+constexpr uint16_t kNoRecord = 0xFFFFu, kTableFull = 0xFFFDu;
+__device__ __forceinline__ int local_record(const AggPlanDev &P, const PartDev &D, long long *skeys, uint16_t *sidx,
+                                            uint8_t *lrec, int *fill, long long k, uint64_t h, uint32_t *status) {
     const int mask = D.slots - 1;
     int pos = (int)(h & (uint64_t)mask);
     for (int t = 0; t < D.slots; t++) {
-        uint16_t cur = *reinterpret_cast<volatile uint16_t *>(sidx + pos);
-        if (cur == 0xFFFFu) {
-            const int e = atomicAdd(fill, 1);
-            if (e >= D.L) return -1;
-            init_record(P, lrec + (size_t)e * smem_stride(P));
-            rkeys[e] = k;
-            __threadfence_block();
-            cur = atomicCAS(reinterpret_cast<unsigned short *>(sidx + pos), (unsigned short)0xFFFFu, (unsigned short)e);
-            if (cur == 0xFFFFu) return e;
-            // another key (or this one) took the slot first: record e stays empty
+        long long cur = *reinterpret_cast<volatile long long *>(skeys + pos);
+        if (cur == kEmptyKey) {
+            cur = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(skeys + pos), (unsigned long long)kEmptyKey,
+                                       (unsigned long long)k);
+            if (cur == kEmptyKey) {
+                const int e = atomicAdd(fill, 1);
+                if (e >= D.L) {
+                    *reinterpret_cast<volatile uint16_t *>(sidx + pos) = kTableFull;
+                    return -1;
+                }
+                init_record(P, lrec + (size_t)e * smem_stride(P));
+                __threadfence_block();
+                *reinterpret_cast<volatile uint16_t *>(sidx + pos) = (uint16_t)e;
+                return e;
+            }
         }
-        __threadfence_block();
-        if (*reinterpret_cast<volatile long long *>(rkeys + cur) == k) return cur;
+        if (cur == k) {
+            for (int it = 0; it < (1 << 20); it++) {
+                const uint16_t e = *reinterpret_cast<volatile uint16_t *>(sidx + pos);
+                if (e != kNoRecord) {
+                    __threadfence_block();
+                    return e == kTableFull ? -1 : (int)e;
+                }
+                __nanosleep(20);
+            }
+            atomicOr(status, ST_TIMEOUT);
+            return -1;
+        }
         pos = (pos + 1) & mask;
     }
     return -1;
 }
 
-// Merges the non-empty local records into the global table: first every key's
-// group id (inserting new keys), and only when all found one, the records.
-__device__ bool flush_local(const AggPlanDev &P, const TableDev &T, const PartDev &D, const long long *rkeys,
-                            uint8_t *lrec, uint32_t *lgid, int m, int *fail) {
-    for (int e = threadIdx.x; e < m; e += blockDim.x) {
+// Merges the local records into the global table: first every key's group
+// id (inserting new keys), and only when all found one, the records.
+__device__ bool flush_local(const AggPlanDev &P, const TableDev &T, const PartDev &D, const long long *skeys,
+                            const uint16_t *sidx, uint8_t *lrec, uint32_t *lgid, int m, int *fail) {
+    for (int sl = threadIdx.x; sl < D.slots; sl += blockDim.x) {
+        const uint16_t e = sidx[sl];
+        if (e >= m) continue;  // free, or claimed without a record
         uint32_t g = kPending;
         if (*reinterpret_cast<const unsigned long long *>(lrec + (size_t)e * smem_stride(P) + P.off_rows)) {
-            g = find_or_insert(T, P, rkeys[e]);
+            g = find_or_insert(T, P, skeys[sl]);
             if (g == kOverflowGid) atomicOr(fail, 1);
         }
         lgid[e] = g;
@@ -803,19 +823,23 @@ __device__ bool flush_local(const AggPlanDev &P, const TableDev &T, const PartDe
 __global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, TableDev T, PartDev D) {
     extern __shared__ __align__(16) uint8_t smem[];
     uint8_t *lrec = smem;                                                                   // L records
-    long long *rkeys = reinterpret_cast<long long *>(lrec + (size_t)D.L * smem_stride(P));  // L keys
-    uint32_t *lgid = reinterpret_cast<uint32_t *>(rkeys + D.L);                             // L
+    long long *skeys = reinterpret_cast<long long *>(lrec + (size_t)D.L * smem_stride(P));  // slots
+    uint32_t *lgid = reinterpret_cast<uint32_t *>(skeys + D.slots);                         // L
     uint16_t *sidx = reinterpret_cast<uint16_t *>(lgid + D.L);                              // slots
     __shared__ int s_fill, s_fail;
     __shared__ int16_t s_off[kMaxValueCols];  // row record offsets (read with a varying index)
     if (threadIdx.x < kMaxValueCols) s_off[threadIdx.x] = D.off_val[threadIdx.x];
     const int p = D.todo[blockIdx.x];
-    const uint32_t cnt = D.part_cnt[(size_t)p * kCntStride];
-    const uint32_t rows = cnt < D.cap ? cnt : D.cap;
-    const uint8_t *buf = D.part_buf + (size_t)p * D.cap * D.row_bytes;
+    const unsigned int *line = D.part_info + (size_t)p * kCntStride;
+    const uint32_t cnt = line[0], cap = line[1];
+    const uint32_t rows = cnt < cap ? cnt : cap;
+    const uint8_t *buf = D.part_buf + *reinterpret_cast<const unsigned long long *>(line + 2) * D.row_bytes;
     uint32_t window = D.start[p];
     auto reset = [&]() {
-        for (int s = threadIdx.x; s < D.slots; s += blockDim.x) sidx[s] = 0xFFFFu;
+        for (int s = threadIdx.x; s < D.slots; s += blockDim.x) {
+            skeys[s] = kEmptyKey;
+            sidx[s] = kNoRecord;
+        }
         if (threadIdx.x == 0) {
             s_fill = 0;
             s_fail = 0;
@@ -830,22 +854,25 @@ __global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, Ta
         const long long k = live ? *reinterpret_cast<const long long *>(row) : 0;
         const uint64_t h = hash_word((uint64_t)k);
         const unsigned lane = threadIdx.x & 31u;
-        for (int attempt = 0; attempt < 2; attempt++) {
+        bool folded = false;
+        for (int attempt = 0; attempt < 2 && !folded; attempt++) {
             // One lane per distinct key of the warp looks it up; the lanes of
             // that key take its record (no lane waits on its own warp).
             const unsigned peers = __match_any_sync(kFullMask, live ? k : kEmptyKey);
             const int lead = __ffs(peers) - 1;
             int e = 0;
-            if (live && (int)lane == lead) e = local_record(P, D, sidx, rkeys, lrec, &s_fill, k, h);
+            if (live && (int)lane == lead) e = local_record(P, D, skeys, sidx, lrec, &s_fill, k, h, T.status);
             e = __shfl_sync(kFullMask, e, lead);
             if (!__syncthreads_or(e < 0)) {
                 if (live) fold_row(P, s_off, lrec + (size_t)e * smem_stride(P), row);
-                break;
+                folded = true;
+                continue;
             }
+            if (attempt == 1) break;  // an emptied table did not take the tile: only a wait that gave up does that
             // The table is full: merge the window's rows (those before this
             // tile; the tile's new records are still empty) and retry the tile.
             const int m = s_fill < D.L ? s_fill : D.L;
-            if (!flush_local(P, T, D, rkeys, lrec, lgid, m, &s_fail)) {
+            if (!flush_local(P, T, D, skeys, sidx, lrec, lgid, m, &s_fail)) {
                 if (threadIdx.x == 0) {
                     D.start[p] = window;
                     atomicAdd(D.failed, 1);
@@ -855,10 +882,11 @@ __global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, Ta
             window = base;
             reset();
         }
+        if (!folded && threadIdx.x == 0) atomicOr(T.status, ST_TIMEOUT);
     }
     __syncthreads();
     const int m = s_fill < D.L ? s_fill : D.L;
-    if (!flush_local(P, T, D, rkeys, lrec, lgid, m, &s_fail)) {
+    if (!flush_local(P, T, D, skeys, sidx, lrec, lgid, m, &s_fail)) {
         if (threadIdx.x == 0) {
             D.start[p] = window;
             atomicAdd(D.failed, 1);
@@ -866,6 +894,55 @@ __global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, Ta
         return;
     }
     if (threadIdx.x == 0) D.start[p] = rows;
+}
+
+// Cold rows per partition: the split kernel's own test (a valid key that is
+// not the marker and not hot), so that partition p gets exactly hist[p] rows.
+__global__ void __launch_bounds__(kSplitThreads) agg_count_kernel(KeyIn key, int64_t n, SplitDev S,
+                                                                  unsigned int *hist) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int nparts = 1 << S.part_bits;
+    unsigned int *s_hist = reinterpret_cast<unsigned int *>(smem);                 // nparts
+    long long *hkeys = reinterpret_cast<long long *>(s_hist + ((nparts + 1) & ~1));  // hot_slots
+    for (int q = threadIdx.x; q < nparts; q += blockDim.x) s_hist[q] = 0;
+    for (int e = threadIdx.x; e < S.hot_slots; e += blockDim.x) hkeys[e] = kEmptyKey;
+    __syncthreads();
+    const int hmask = S.hot_slots - 1;
+    for (int j = threadIdx.x; j < S.H; j += blockDim.x) {
+        const long long k = S.hot_keys[j];
+        int pos = (int)(hash_word((uint64_t)k) & (uint64_t)hmask);
+        for (int t = 0; t < S.hot_slots; t++) {
+            if ((long long)atomicCAS(reinterpret_cast<unsigned long long *>(hkeys + pos), (unsigned long long)kEmptyKey,
+                                     (unsigned long long)k) == kEmptyKey)
+                break;
+            pos = (pos + 1) & hmask;
+        }
+    }
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+        if (!bit_get(key.valid, key.voff, r)) continue;
+        const long long k = key_at(key, r);
+        if (k == kEmptyKey) continue;
+        const uint64_t h = hash_word((uint64_t)k);
+        bool hot = false;
+        if (S.H) {
+            int pos = (int)(h & (uint64_t)hmask);
+            for (int t = 0; t < S.hot_slots; t++) {
+                const long long c = hkeys[pos];
+                if (c == k) {
+                    hot = true;
+                    break;
+                }
+                if (c == kEmptyKey) break;
+                pos = (pos + 1) & hmask;
+            }
+        }
+        if (!hot) atomicAdd(&s_hist[(int)(h >> (64 - S.part_bits))], 1u);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < nparts; q += blockDim.x)
+        if (s_hist[q]) atomicAdd(hist + q, s_hist[q]);
 }
 
 // Group ids of the hot keys (inserted into the global table), then the NULL
@@ -1470,7 +1547,7 @@ void HashAggregate::plan(const DevBatch &b) {
     // agg_part_kernel, with slots for twice as many keys.
     {
         const int L = kPartThreads;
-        const size_t smem = (size_t)L * (smem_stride(P_) + 8 + 4) + (size_t)next_pow2((uint64_t)2 * L) * 2;
+        const size_t smem = (size_t)L * (smem_stride(P_) + 4) + (size_t)next_pow2((uint64_t)2 * L) * 10;
         part_local_ = smem <= (size_t)rt_->max_smem_optin - 1024 ? L : 0;
         part_smem_ = smem;
     }
@@ -1560,41 +1637,71 @@ __global__ void sample_keys_kernel(KeyIn key, int64_t n, int64_t step, int m, lo
 }
 }  // namespace
 
+// A strided sample of `m` keys of the batch, counted per key with a flat
+// open-addressing table on the host: (count, key) of each distinct valid key
+// (not the marker), and how many sampled rows had a NULL or the marker key.
+struct KeySample {
+    std::vector<std::pair<int, long long>> runs;
+    int special = 0;
+    int m = 0;
+};
+static KeySample take_sample(Runtime *rt, const KeyIn &key, int64_t n, int m) {
+    KeySample S;
+    S.m = m;
+    if (m <= 0) return S;
+    const int64_t step = std::max<int64_t>(1, n / m);
+    DBuf keys(rt, (size_t)m * 8), ok(rt, (size_t)m);
+    sample_keys_kernel<<<grid_for(rt, m, 256, 4), 256, 0, rt->stream>>>(key, n, step, m, keys.as<long long>(),
+                                                                        ok.as<uint8_t>());
+    rt->launches++;
+    check_launch("sample_keys_kernel");
+    std::vector<long long> hk(m);
+    std::vector<uint8_t> hv(m);
+    KRV_CUDA(cudaMemcpyAsync(hk.data(), keys.get(), (size_t)m * 8, cudaMemcpyDeviceToHost, rt->stream));
+    KRV_CUDA(cudaMemcpyAsync(hv.data(), ok.get(), (size_t)m, cudaMemcpyDeviceToHost, rt->stream));
+    KRV_CUDA(cudaStreamSynchronize(rt->stream));
+    const uint64_t slots = next_pow2((uint64_t)2 * m), mask = slots - 1;
+    std::vector<long long> tk(slots, kEmptyKey);
+    std::vector<int> tc(slots, 0);
+    for (int j = 0; j < m; j++) {
+        const long long k = hk[j];
+        if (!hv[j] || k == kEmptyKey) {
+            S.special++;
+            continue;
+        }
+        uint64_t pos = hash_word((uint64_t)k) & mask;
+        while (tk[pos] != kEmptyKey && tk[pos] != k) pos = (pos + 1) & mask;
+        tk[pos] = k;
+        tc[pos]++;
+    }
+    for (uint64_t i = 0; i < slots; i++)
+        if (tc[i]) S.runs.push_back({tc[i], tk[i]});
+    return S;
+}
+// The `most` keys seen at least `at_least` times, most frequent first.
+static std::vector<long long> top_keys(const KeySample &S, int most, int at_least) {
+    std::vector<std::pair<int, long long>> c;
+    for (const auto &r : S.runs)
+        if (r.first >= at_least) c.push_back(r);
+    const auto by_count = [](const auto &x, const auto &y) { return x.first > y.first || (x.first == y.first && x.second < y.second); };
+    if ((int)c.size() > most) {
+        std::nth_element(c.begin(), c.begin() + most, c.end(), by_count);
+        c.resize(most);
+    }
+    std::sort(c.begin(), c.end(), by_count);
+    std::vector<long long> out;
+    for (const auto &r : c) out.push_back(r.second);
+    return out;
+}
+
 void HashAggregate::sample_hot(const KeyIn &key, int64_t n) {
     sampled_ = true;
     constexpr int kSample = 1 << 16;
     const int m = (int)std::min<int64_t>(n, kSample);
     if (m < 1024) return;  // too few rows for hot keys to matter
-    const int64_t step = n / m;
-    DBuf keys(rt_, (size_t)m * 8), ok(rt_, (size_t)m);
-    sample_keys_kernel<<<grid_for(rt_, m, 256, 4), 256, 0, rt_->stream>>>(key, n, step, m, keys.as<long long>(),
-                                                                          ok.as<uint8_t>());
-    rt_->launches++;
-    check_launch("sample_keys_kernel");
-    std::vector<long long> hk(m);
-    std::vector<uint8_t> hv(m);
-    KRV_CUDA(cudaMemcpyAsync(hk.data(), keys.get(), (size_t)m * 8, cudaMemcpyDeviceToHost, rt_->stream));
-    KRV_CUDA(cudaMemcpyAsync(hv.data(), ok.get(), (size_t)m, cudaMemcpyDeviceToHost, rt_->stream));
-    KRV_CUDA(cudaStreamSynchronize(rt_->stream));
-    std::vector<long long> v;
-    v.reserve(m);
-    for (int j = 0; j < m; j++)
-        if (hv[j] && hk[j] != kEmptyKey) v.push_back(hk[j]);
-    std::sort(v.begin(), v.end());
-    std::vector<std::pair<int, long long>> runs;  // (count, key)
-    for (size_t a = 0; a < v.size();) {
-        size_t b = a;
-        while (b < v.size() && v[b] == v[a]) b++;
-        runs.push_back({(int)(b - a), v[a]});
-        a = b;
-    }
-    std::sort(runs.begin(), runs.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    const KeySample S = take_sample(rt_, key, n, m);
     // hot: at least 0.2% of the sample each
-    std::vector<long long> hot;
-    for (const auto &rk : runs) {
-        if ((int)hot.size() == kHotKeys || rk.first * 500 < m) break;
-        hot.push_back(rk.second);
-    }
+    const std::vector<long long> hot = top_keys(S, kHotKeys, std::max(1, (m + 499) / 500));
     hot_count_ = (int)hot.size();
     if (!hot_count_) return;
     hot_ = DBuf(rt_, hot.size() * 8);
@@ -1645,53 +1752,31 @@ void HashAggregate::plan_partitioned(const KeyIn &key, int64_t n) {
     part_row_bytes_ = (off + 15) / 16 * 16;
     // The sample: a strided 64K rows of the first large batch.
     const int m = (int)std::min<int64_t>(n, kPartSample);
-    const int64_t step = std::max<int64_t>(1, n / m);
-    DBuf keys(rt_, (size_t)m * 8), ok(rt_, (size_t)m);
-    sample_keys_kernel<<<grid_for(rt_, m, 256, 4), 256, 0, rt_->stream>>>(key, n, step, m, keys.as<long long>(),
-                                                                          ok.as<uint8_t>());
-    rt_->launches++;
-    check_launch("sample_keys_kernel");
-    std::vector<long long> hk(m);
-    std::vector<uint8_t> hv(m);
-    KRV_CUDA(cudaMemcpyAsync(hk.data(), keys.get(), (size_t)m * 8, cudaMemcpyDeviceToHost, rt_->stream));
-    KRV_CUDA(cudaMemcpyAsync(hv.data(), ok.get(), (size_t)m, cudaMemcpyDeviceToHost, rt_->stream));
-    KRV_CUDA(cudaStreamSynchronize(rt_->stream));
-    std::vector<long long> v;
-    int special = 0;
-    for (int j = 0; j < m; j++) {
-        if (hv[j] && hk[j] != kEmptyKey) v.push_back(hk[j]);
-        else special++;
-    }
-    std::sort(v.begin(), v.end());
-    std::vector<std::pair<int, long long>> runs;  // (count, key)
-    for (size_t a = 0; a < v.size();) {
-        size_t b = a;
-        while (b < v.size() && v[b] == v[a]) b++;
-        runs.push_back({(int)(b - a), v[a]});
-        a = b;
-    }
-    std::sort(runs.begin(), runs.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    const KeySample S = take_sample(rt_, key, n, m);
+    const int special = S.special;
     // Hot: seen at least 3 times, as many as the split kernel's shared memory
     // holds records for beside its lookup table.
     const int smem_cap = std::min(rt_->max_smem_optin - 2048, 72 * 1024);
     int hmax = kHotMax;
     while (hmax > 0 && (size_t)(hmax + 2) * smem_stride(P_) + (size_t)2 * next_pow2(hmax) * 10 > (size_t)smem_cap)
         hmax /= 2;
-    std::vector<long long> hot;
+    const std::vector<long long> hot = top_keys(S, hmax, 3);
+    std::vector<long long> hot_sorted = hot;
+    std::sort(hot_sorted.begin(), hot_sorted.end());
     int hot_rows = 0;
-    for (const auto &rk : runs) {
-        if ((int)hot.size() == hmax || rk.first < 3) break;
-        hot.push_back(rk.second);
-        hot_rows += rk.first;
+    std::vector<std::pair<int, long long>> runs;  // the cold keys' runs
+    for (const auto &r : S.runs) {
+        if (std::binary_search(hot_sorted.begin(), hot_sorted.end(), r.second)) hot_rows += r.first;
+        else runs.push_back(r);
     }
     part_hot_ = (int)hot.size();
     part_cold_frac_ = m ? std::max(0.0, 1.0 - (double)(hot_rows + special) / m) : 1.0;
     // Distinct cold keys (the guaranteed-error estimator: keys seen once in
     // the sample stand for sqrt(n / m) keys each).
     int64_t d = 0, f1 = 0;
-    for (size_t i = hot.size(); i < runs.size(); i++) {
+    for (const auto &r : runs) {
         d++;
-        if (runs[i].first == 1) f1++;
+        if (r.first == 1) f1++;
     }
     const double est = (double)d + (double)f1 * (std::sqrt((double)n / std::max(1, m)) - 1.0);
     part_groups_est_ = std::max<int64_t>({(int64_t)est, spec_.expected_groups, 1});
@@ -1779,23 +1864,6 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
     const KeyIn key0 = key;
     for (int64_t row0 = 0; row0 < n; row0 += kPartSliceRows) {
         const int64_t ns = std::min<int64_t>(kPartSliceRows, n - row0);
-        const uint64_t cap64 =
-            std::min<uint64_t>((uint64_t)ns, ((uint64_t)((double)ns * part_cold_frac_ * 1.25 / nparts) + 256 + 31) / 32 * 32);
-        const uint32_t cap = (uint32_t)cap64;
-        DBuf part_buf(rt_, (size_t)nparts * cap * part_row_bytes_);
-        DBuf part_cnt(rt_, (size_t)nparts * kCntStride * 4);
-        DBuf start(rt_, (size_t)nparts * 4);
-        DBuf ctl(rt_, 16);  // [0] deferred rows (u64), [8] failed partitions (int)
-        DBuf ovf(rt_, (size_t)ns * 4);
-        KRV_CUDA(cudaMemsetAsync(part_cnt.get(), 0, part_cnt.bytes(), rt_->stream));
-        KRV_CUDA(cudaMemsetAsync(start.get(), 0, start.bytes(), rt_->stream));
-        KRV_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, rt_->stream));
-        // Room in the table for the keys this slice may add (an estimate; a
-        // partition that finds none stops and runs again after a grow).
-        const int64_t want = known_groups_ + std::min<int64_t>(ns, part_groups_est_) + H + 2;
-        if (want > (int64_t)limit_) grow((uint64_t)want);
-        TableDev T{keys_.as<long long>(), gids_.as<uint32_t>(), slots_ - 1, states_.as<uint8_t>(), gkeys_.as<long long>(),
-                   ngroups_.as<unsigned long long>(), limit_, status_word(rt_)};
         SplitDev S{};
         S.hot_keys = part_hot_keys_.as<long long>();
         S.hot_gids = part_hot_gids_.as<uint32_t>();
@@ -1804,24 +1872,63 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
         S.part_bits = bits;
         S.row_bytes = part_row_bytes_;
         for (int c = 0; c < kMaxValueCols; c++) S.off_val[c] = part_off_val_[c];
+        KeyIn ks = key0;
+        ks.data = static_cast<const uint8_t *>(key0.data) + row0 * key0.width;
+        ks.voff = key0.voff + row0;
+        // Exact partition sizes: one pass over the keys with the split's own
+        // test, then the partitions laid out back to back.
+        DBuf hist(rt_, (size_t)nparts * 4);
+        KRV_CUDA(cudaMemsetAsync(hist.get(), 0, hist.bytes(), rt_->stream));
+        {
+            const size_t csmem = (size_t)((nparts + 1) & ~1) * 4 + (size_t)hot_slots * 8;
+            KRV_CUDA(cudaFuncSetAttribute(agg_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem));
+            int cblocks = 0;
+            KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cblocks, agg_count_kernel, kSplitThreads, csmem));
+            const int grid0 = (int)std::min<int64_t>((int64_t)std::max(cblocks, 1) * rt_->sm_count,
+                                                     ceil_div(ns, kSplitThreads));
+            agg_count_kernel<<<grid0, kSplitThreads, csmem, rt_->stream>>>(ks, ns, S, hist.as<unsigned int>());
+            rt_->launches++;
+            check_launch("agg_count_kernel");
+        }
+        std::vector<unsigned int> hh(nparts);
+        KRV_CUDA(cudaMemcpyAsync(hh.data(), hist.get(), (size_t)nparts * 4, cudaMemcpyDeviceToHost, rt_->stream));
+        KRV_CUDA(cudaStreamSynchronize(rt_->stream));
+        std::vector<unsigned int> info((size_t)nparts * kCntStride, 0u);
+        unsigned long long cold = 0;
+        for (int p = 0; p < nparts; p++) {
+            unsigned int *line = info.data() + (size_t)p * kCntStride;
+            line[1] = hh[p];
+            memcpy(line + 2, &cold, 8);
+            cold += hh[p];
+        }
+        DBuf part_info(rt_, info.size() * 4);
+        KRV_CUDA(cudaMemcpyAsync(part_info.get(), info.data(), info.size() * 4, cudaMemcpyHostToDevice, rt_->stream));
+        DBuf part_buf(rt_, (size_t)std::max<unsigned long long>(cold, 1) * part_row_bytes_);
+        DBuf start(rt_, (size_t)nparts * 4);
+        DBuf ctl(rt_, 16);  // [0] deferred rows (u64), [8] failed partitions (int)
+        DBuf ovf(rt_, (size_t)ns * 4);
+        KRV_CUDA(cudaMemsetAsync(start.get(), 0, start.bytes(), rt_->stream));
+        KRV_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, rt_->stream));
+        KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // `info` is a stack vector
+        // Room in the table for the keys this slice may add (an estimate; a
+        // partition that finds none stops and runs again after a grow).
+        const int64_t want = known_groups_ + std::min<int64_t>(ns, part_groups_est_) + H + 2;
+        if (want > (int64_t)limit_) grow((uint64_t)want);
+        TableDev T{keys_.as<long long>(), gids_.as<uint32_t>(), slots_ - 1, states_.as<uint8_t>(), gkeys_.as<long long>(),
+                   ngroups_.as<unsigned long long>(), limit_, status_word(rt_)};
         S.part_buf = part_buf.as<uint8_t>();
-        S.part_cnt = part_cnt.as<unsigned int>();
-        S.cap = cap;
+        S.part_info = part_info.as<unsigned int>();
         S.ovf_rows = ovf.as<uint32_t>();
         S.ovf_count = ctl.as<unsigned long long>();
         S.row0 = row0;
         const AggPlanDev PS = slice_plan(P, row0, widths);
-        KeyIn ks = key0;
-        ks.data = static_cast<const uint8_t *>(key0.data) + row0 * key0.width;
-        ks.voff = key0.voff + row0;
         const int grid1 = (int)std::min<int64_t>((int64_t)split_blocks * rt_->sm_count, ceil_div(ns, kSplitThreads));
         agg_split_kernel<<<grid1, kSplitThreads, split_smem, rt_->stream>>>(PS, T, ks, ns, S);
         rt_->launches++;
         check_launch("agg_split_kernel");
         PartDev D{};
         D.part_buf = part_buf.as<uint8_t>();
-        D.part_cnt = part_cnt.as<unsigned int>();
-        D.cap = cap;
+        D.part_info = part_info.as<unsigned int>();
         D.row_bytes = part_row_bytes_;
         for (int c = 0; c < kMaxValueCols; c++) D.off_val[c] = part_off_val_[c];
         D.todo = todo_all.as<int>();
@@ -1851,11 +1958,12 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
             // Partitions that stopped: their windows run again on a bigger table.
             std::vector<uint32_t> hs(nparts), hc((size_t)nparts * kCntStride);
             KRV_CUDA(cudaMemcpyAsync(hs.data(), start.get(), (size_t)nparts * 4, cudaMemcpyDeviceToHost, rt_->stream));
-            KRV_CUDA(cudaMemcpyAsync(hc.data(), part_cnt.get(), part_cnt.bytes(), cudaMemcpyDeviceToHost, rt_->stream));
+            KRV_CUDA(cudaMemcpyAsync(hc.data(), part_info.get(), part_info.bytes(), cudaMemcpyDeviceToHost, rt_->stream));
             KRV_CUDA(cudaStreamSynchronize(rt_->stream));
             std::vector<int> again;
             for (int p = 0; p < nparts; p++)
-                if (hs[p] < std::min<uint32_t>(hc[(size_t)p * kCntStride], cap)) again.push_back(p);
+                if (hs[p] < std::min<uint32_t>(hc[(size_t)p * kCntStride], hc[(size_t)p * kCntStride + 1]))
+                    again.push_back(p);
             grow((uint64_t)known_groups_ + (uint64_t)again.size() * L + 1);
             todo = DBuf(rt_, again.size() * 4);
             KRV_CUDA(cudaMemcpyAsync(todo.get(), again.data(), again.size() * 4, cudaMemcpyHostToDevice, rt_->stream));
