@@ -693,14 +693,13 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
         torch.cuda.synchronize()
         t.append(time.perf_counter())
         total, rows, nbatches = 0, 0, 0
-        calls = []  # host wall time of each probe call (to find stalls)
+        calls = []  # host wall time of each probe batch, its output batches consumed (to find stalls)
         for db in batches(probe, np_, pstep):
             c0 = time.perf_counter()
-            outs = j.probe_device_all(db)
-            calls.append((time.perf_counter() - c0) * 1e3)
-            for res in outs:
+            for res in j.probe_device_all(db):
                 c, n = output_checksum(res)
                 total, rows, nbatches = (total + c) & (2**64 - 1), rows + n, nbatches + 1
+            calls.append((time.perf_counter() - c0) * 1e3)
         torch.cuda.synchronize()
         t.append(time.perf_counter())
         for res in j.finish_device():
@@ -708,11 +707,12 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
             total, rows, nbatches = (total + c) & (2**64 - 1), rows + n, nbatches + 1
         torch.cuda.synchronize()
         t.append(time.perf_counter())
-        calls.sort()
-        phases.update(build_s=t[1] - t[0], probe_s=t[2] - t[1], finish_s=t[3] - t[2], output_batches=nbatches,
-                      probe_calls=len(calls), probe_call_ms_median=statistics.median(calls) if calls else None,
-                      probe_call_ms_slowest=calls[-5:])
-        step_phases.append(dict(phases))
+        if partitioned:
+            slowest = sorted(range(len(calls)), key=lambda i: calls[i])[-5:]
+            phases.update(build_s=t[1] - t[0], probe_s=t[2] - t[1], finish_s=t[3] - t[2], output_batches=nbatches,
+                          probe_calls=len(calls), probe_call_ms_median=statistics.median(calls) if calls else None,
+                          probe_call_ms_slowest={i: round(calls[i], 1) for i in slowest})
+            step_phases.append(dict(phases))
         return j, total, rows
 
     for _ in range(args.warmup):
@@ -858,20 +858,31 @@ def run_agg(args, kb, W, rt, rank, world, pg, device):
     aggs = [(f, c) for c in (1, 2, 3) for f in ("sum", "count", "min", "max", "avg")]
 
     phase_ev = []
+    host = {"create": [], "push": [], "finish": [], "result": [], "release": []}  # host wall ms per call
 
     def step(mode, ev=None):
+        h = [time.perf_counter()]
         a = kb.HashAggregate(rt, kb.agg_spec(0, aggs, mode=mode, expected_groups=1_000_000))
+        h.append(time.perf_counter())
         e = [torch.cuda.Event(enable_timing=True) for _ in range(3)] if ev is not None else None
         if e:
             e[0].record(stream)
         a.push_device(db)
+        h.append(time.perf_counter())
         a.finish()
+        h.append(time.perf_counter())
         if e:
             e[1].record(stream)
         r = a.result_device()
         if e:
             e[2].record(stream)
             ev.append(e)
+        h.append(time.perf_counter())
+        del a
+        h.append(time.perf_counter())
+        if ev is not None:
+            for k, t0, t1 in zip(host, h, h[1:]):
+                host[k].append((t1 - t0) * 1e3)
         return r
 
     res, clocks = {}, {}
@@ -902,6 +913,7 @@ def run_agg(args, kb, W, rt, rank, world, pg, device):
             "gpu_launches": launches,
             "phases_ms": {"push": statistics.median(x[0].elapsed_time(x[1]) for x in phase_ev),
                           "result": statistics.median(x[1].elapsed_time(x[2]) for x in phase_ev)},
+            "host_ms": {k: round(statistics.median(v), 3) for k, v in host.items() if v},
             "plain_global_table": {"ms_per_step": res["global"][0], "value": world * n / (res["global"][0] * 1e-3) / 1e6},
             "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "peak_source": kind,
                          "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None,

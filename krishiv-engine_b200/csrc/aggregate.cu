@@ -485,12 +485,52 @@ struct SplitDev {
     int part_bits;  // >= 1
     int row_bytes;
     int16_t off_val[kMaxValueCols];
-    uint8_t *part_buf;          // partition p: rows [base_p, base_p + cap_p)
-    unsigned int *part_info;    // partition p's line at p * kCntStride: [0] rows written, [1] cap_p, [2..3] base_p
-    uint32_t *ovf_rows;         // rows that met a full partition (aggregated afterwards)
-    unsigned long long *ovf_count;
-    int64_t row0;               // the batch row of this slice's row 0 (ovf_rows hold batch rows)
+    int ctas;                   // CTAs of the count and split kernels: CTA b takes the tiles of
+                                // kSplitThreads rows b, b + ctas, b + 2 ctas, ...
+    unsigned *cta_rows;         // [p * ctas + b]: partition p's cold rows of CTA b (count), then
+                                // the rows of p before CTA b's (after part_offsets_kernel)
+    uint8_t *part_buf;          // partition p: rows [base_p, base_p + rows_p)
+    const unsigned int *part_info;  // partition p's line at p * kCntStride: [0] rows, [1] rows, [2..3] base_p
+    unsigned long long cold;    // rows in part_buf (the bound of every write)
 };
+
+// Shared-memory accumulators. On the SM a 32-bit shared atomic add is one
+// instruction, while 64-bit adds (integer or float) are compare-and-swap
+// loops that retry whenever lanes meet on one word. So shared-memory records
+// count in the low word of their 64-bit counters (one CTA folds fewer than
+// 2^32 rows: batches are shorter) and add integer sums limb by limb, each
+// 32-bit limb's carry taken from the value its own add returned. The limb
+// adds of concurrent updaters commute, so the field is exact once they are
+// all done (after a barrier).
+__device__ __forceinline__ void s_count(uint8_t *field, unsigned v) {
+    atomicAdd(reinterpret_cast<unsigned *>(field), v);
+}
+// Adds the N-limb two's-complement value `a` (least significant limb first)
+// to the N-limb field at f.
+template <int N>
+__device__ __forceinline__ void s_add_limbs(uint8_t *f, const unsigned (&a)[N]) {
+    unsigned *w = reinterpret_cast<unsigned *>(f);
+    unsigned carry = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        const unsigned x = a[i] + carry;
+        carry = x < carry ? 1u : 0u;  // a[i] + carry wrapped (x is 0 then)
+        if (x) {
+            const unsigned old = atomicAdd(w + i, x);
+            carry = old + x < old ? 1u : 0u;
+        }
+    }
+}
+// A signed 64-bit value added to a 64-bit field.
+__device__ __forceinline__ void s_add_i64(uint8_t *f, long long v) {
+    const unsigned a[2] = {(unsigned)v, (unsigned)((unsigned long long)v >> 32)};
+    s_add_limbs<2>(f, a);
+}
+// A 128-bit value (lo, hi) added to a 128-bit field.
+__device__ __forceinline__ void s_add_i128(uint8_t *f, uint64_t lo, uint64_t hi) {
+    const unsigned a[4] = {(unsigned)lo, (unsigned)(lo >> 32), (unsigned)hi, (unsigned)(hi >> 32)};
+    s_add_limbs<4>(f, a);
+}
 
 // A value as the accumulators take it: `lo`/`hi` the 128-bit sum operand of
 // integer and decimal types (f64: the value's bits in lo); `mm` a signed
@@ -512,65 +552,109 @@ __device__ __forceinline__ void value_words(const AggColDev &C, const void *data
         hi = v < 0 ? ~0ull : 0ull;
     }
 }
-__device__ __forceinline__ long long mm_key(const AggColDev &C, uint64_t lo) {
-    if (C.type == (int)Type::F64) return (long long)(f64_order_key(__longlong_as_double((long long)lo)) ^ 0x8000000000000000ull);
-    return (long long)lo;
-}
-
-// Folds (count, 128-bit sum or double-double sum, min and max keys) of one
-// key's rows into its record; shared or global memory, concurrent updaters.
-__device__ __forceinline__ void fold_partial(const AggColDev &C, uint8_t *r, unsigned long long cnt, uint64_t slo,
-                                             uint64_t shi, double ds, double de, long long mn, long long mx) {
-    atomicAdd(reinterpret_cast<unsigned long long *>(r + C.off_count), cnt);
+// Folds one row's value (lo, hi as value_words gives them) into a
+// shared-memory record with concurrent updaters.
+__device__ __forceinline__ void s_fold_value(const AggColDev &C, uint8_t *r, uint64_t lo, uint64_t hi) {
+    s_count(r + C.off_count, 1u);
     const bool i32 = C.type == (int)Type::I32 || C.type == (int)Type::Date32;
-    if (C.flags & F_SUM) {
-        if (C.type == (int)Type::F64) {
-            atomic_add_dd2(reinterpret_cast<double *>(r + C.off_sum), reinterpret_cast<double *>(r + C.off_sum + 8), ds,
-                           de);
-        } else if (i32) {
-            atomicAdd(reinterpret_cast<unsigned long long *>(r + C.off_sum), (unsigned long long)slo);
-        } else {
-            atomic_add_i128(reinterpret_cast<unsigned long long *>(r + C.off_sum),
-                            reinterpret_cast<long long *>(r + C.off_sum + 8), (int64_t)slo, (int64_t)shi);
+    if (C.type == (int)Type::F64) {
+        const double v = __longlong_as_double((long long)lo);
+        if (C.flags & F_SUM)
+            atomic_add_dd(reinterpret_cast<double *>(r + C.off_sum), reinterpret_cast<double *>(r + C.off_sum + 8), v);
+        if (C.flags & (F_MIN | F_MAX)) {
+            const unsigned long long key = f64_order_key(v);
+            if (C.flags & F_MIN) atomicMin(reinterpret_cast<unsigned long long *>(r + C.off_min), key);
+            if (C.flags & F_MAX) atomicMax(reinterpret_cast<unsigned long long *>(r + C.off_max), key);
         }
+        return;
+    }
+    if (C.flags & F_SUM) {
+        if (i32) s_add_i64(r + C.off_sum, (long long)lo);
+        else s_add_i128(r + C.off_sum, lo, hi);
     }
     if (C.flags & F_MIN) {
-        if (i32) atomicMin(reinterpret_cast<int *>(r + C.off_min), (int)mn);
-        else if (C.type == (int)Type::F64)
-            atomicMin(reinterpret_cast<unsigned long long *>(r + C.off_min), (unsigned long long)mn ^ 0x8000000000000000ull);
-        else atomicMin(reinterpret_cast<long long *>(r + C.off_min), mn);
+        if (i32) atomicMin(reinterpret_cast<int *>(r + C.off_min), (int)lo);
+        else atomicMin(reinterpret_cast<long long *>(r + C.off_min), (long long)lo);
     }
     if (C.flags & F_MAX) {
-        if (i32) atomicMax(reinterpret_cast<int *>(r + C.off_max), (int)mx);
-        else if (C.type == (int)Type::F64)
-            atomicMax(reinterpret_cast<unsigned long long *>(r + C.off_max), (unsigned long long)mx ^ 0x8000000000000000ull);
-        else atomicMax(reinterpret_cast<long long *>(r + C.off_max), mx);
+        if (i32) atomicMax(reinterpret_cast<int *>(r + C.off_max), (int)lo);
+        else atomicMax(reinterpret_cast<long long *>(r + C.off_max), (long long)lo);
     }
+}
+
+// One row's inputs, loaded a warp step ahead of their use: the loads of a
+// step do not depend on one another, so a warp waits for memory once per
+// step and the wait overlaps the previous step's work. NV bounds the value
+// columns held in registers (the plan's first NV columns; ncols <= NV).
+template <int NV>
+struct RowIn {
+    long long k;
+    uint64_t lo[NV];  // the low word of value_words of each value column (the high
+                      // word: the sign, or for decimal128 read where it is used)
+    uint32_t valid;   // bit c: value column c valid; bit 31: the key valid
+};
+constexpr uint32_t kKeyValid = 1u << 31;
+// The high word of value_words for row r's value `lo` of column C.
+__device__ __forceinline__ uint64_t value_hi(const AggColDev &C, int64_t r, uint64_t lo) {
+    if (C.type == (int)Type::Dec128) return (uint64_t) static_cast<const long long *>(C.data)[2 * r + 1];
+    return (long long)lo < 0 ? ~0ull : 0ull;
+}
+
+template <int NV>
+__device__ __forceinline__ void load_row(const AggPlanDev &P, const KeyIn &key, int64_t r, bool live, RowIn<NV> &in) {
+    in.k = 0;
+    in.valid = 0;
+#pragma unroll
+    for (int c = 0; c < NV; c++) in.lo[c] = 0;
+    if (!live) return;
+    in.k = key_at(key, r);
+    uint8_t vb[NV + 1];
+    vb[NV] = key.valid ? key.valid[(key.voff + r) >> 3] : 0xFF;
+#pragma unroll
+    for (int c = 0; c < NV; c++) {
+        vb[c] = 0;
+        if (c >= P.ncols) continue;
+        const AggColDev &C = P.c[c];
+        vb[c] = C.valid ? C.valid[(C.voff + r) >> 3] : 0xFF;
+        if (C.flags & (F_SUM | F_MIN | F_MAX)) {
+            if (C.type == (int)Type::I32 || C.type == (int)Type::Date32)
+                in.lo[c] = (uint64_t)(long long) static_cast<const int *>(C.data)[r];
+            else if (C.type == (int)Type::Dec128) in.lo[c] = (uint64_t) static_cast<const long long *>(C.data)[2 * r];
+            else in.lo[c] = (uint64_t) static_cast<const long long *>(C.data)[r];
+        }
+    }
+    uint32_t bits = ((vb[NV] >> ((key.voff + r) & 7)) & 1u) ? kKeyValid : 0u;
+#pragma unroll
+    for (int c = 0; c < NV; c++)
+        if (c < P.ncols) bits |= ((uint32_t)(vb[c] >> ((P.c[c].voff + r) & 7)) & 1u) << c;
+    in.valid = bits;
 }
 
 // The hot rows of one warp step (`hi`: the lane's hot key, -1 when none),
 // folded into the CTA's shared-memory records. Counts of a key's lanes go in
-// one update (population counts of the warp's ballots); integer sums and
-// MIN/MAX go in per lane (shared atomics, the lanes of one key served by one
-// instruction); float64 sums, which must stay compensated, are reduced to the
-// key's lowest lane first (TwoSum over the other lanes' values) and added as
-// one double-double.
-__device__ __forceinline__ void hot_rows(const AggPlanDev &P, uint8_t *hrec, int64_t r, int hi, unsigned lane) {
+// one update (population counts of the warp's ballots); integer sums (32-bit
+// limbs) and MIN/MAX go in per lane; float64 sums, which must stay
+// compensated, are reduced to the key's lowest lane first (TwoSum over the
+// other lanes' values) and added as one double-double.
+template <int NV>
+__device__ __forceinline__ void hot_rows(const AggPlanDev &P, uint8_t *hrec, const RowIn<NV> &in, int64_t r, int hi,
+                                         unsigned lane) {
     const bool hot = hi >= 0;
     const unsigned peers = __match_any_sync(kFullMask, hot ? hi : 0x40000 + (int)lane);
     const unsigned lead_lane = __ffs(peers) - 1;
     const bool lead = hot && lane == lead_lane;
     uint8_t *rec = hrec + (size_t)(hot ? hi : 0) * smem_stride(P);
-    if (lead) atomicAdd(reinterpret_cast<unsigned long long *>(rec + P.off_rows), (unsigned long long)__popc(peers));
+    if (lead) s_count(rec + P.off_rows, (unsigned)__popc(peers));
     unsigned turns = 0;  // the largest key group of the warp, for the float sums
-    for (int c = 0; c < P.ncols; c++) {
+#pragma unroll
+    for (int c = 0; c < NV; c++) {
+        if (c >= P.ncols) break;
         const AggColDev &C = P.c[c];
-        const bool v = hot && bit_get(C.valid, C.voff, r);
+        const bool v = hot && ((in.valid >> c) & 1u);
         const unsigned vm = __ballot_sync(kFullMask, v) & peers;
-        if (lead && vm) atomicAdd(reinterpret_cast<unsigned long long *>(rec + C.off_count), (unsigned long long)__popc(vm));
+        if (lead && vm) s_count(rec + C.off_count, (unsigned)__popc(vm));
         if (!(C.flags & (F_SUM | F_MIN | F_MAX))) continue;
-        uint64_t lo = 0, hw = 0;
-        if (v) value_words(C, C.data, r, lo, hw);
+        const uint64_t lo = in.lo[c];
         const bool i32 = C.type == (int)Type::I32 || C.type == (int)Type::Date32;
         if (C.type == (int)Type::F64) {
             if (C.flags & F_SUM) {
@@ -601,10 +685,8 @@ __device__ __forceinline__ void hot_rows(const AggPlanDev &P, uint8_t *hrec, int
         }
         if (!v) continue;
         if (C.flags & F_SUM) {
-            if (i32) atomicAdd(reinterpret_cast<unsigned long long *>(rec + C.off_sum), (unsigned long long)lo);
-            else
-                atomic_add_i128(reinterpret_cast<unsigned long long *>(rec + C.off_sum),
-                                reinterpret_cast<long long *>(rec + C.off_sum + 8), (int64_t)lo, (int64_t)hw);
+            if (i32) s_add_i64(rec + C.off_sum, (long long)lo);
+            else s_add_i128(rec + C.off_sum, lo, value_hi(C, r, lo));
         }
         if (C.flags & F_MIN) {
             if (i32) atomicMin(reinterpret_cast<int *>(rec + C.off_min), (int)lo);
@@ -617,57 +699,49 @@ __device__ __forceinline__ void hot_rows(const AggPlanDev &P, uint8_t *hrec, int
     }
 }
 
-// The cold rows of one warp step: each lane's row into its partition (one
-// counter update per partition and warp step); a row that meets a full
-// partition is listed for the global table instead.
-__device__ __forceinline__ void cold_rows(const AggPlanDev &P, const SplitDev &S, const int16_t *off_val, int64_t r,
-                                          long long k, uint64_t h, bool cold, unsigned lane) {
+// The cold rows of one warp step, each written as a row record into its
+// partition at the CTA's cursor for it (one shared-memory update per
+// partition and warp step). The count pass gave every CTA its exact share of
+// each partition, so a write past the buffer only follows a miscount: it is
+// skipped and reported.
+template <int NV>
+__device__ __forceinline__ void cold_rows(const AggPlanDev &P, const SplitDev &S, const int16_t *off_val,
+                                          unsigned *cursor, const RowIn<NV> &in, int64_t r, uint64_t h,
+                                          bool cold, unsigned lane, uint32_t *status) {
     const int p = cold ? (int)(h >> (64 - S.part_bits)) : -1 - (int)lane;
     const unsigned peers = __match_any_sync(kFullMask, p);
     const unsigned lead_lane = __ffs(peers) - 1;
     unsigned base = 0;
-    unsigned int *line = S.part_info + (size_t)(cold ? p : 0) * kCntStride;
-    if (cold && lane == lead_lane) base = atomicAdd(line, (unsigned)__popc(peers));
+    if (cold && lane == lead_lane) base = atomicAdd(cursor + p, (unsigned)__popc(peers));
     base = __shfl_sync(kFullMask, base, lead_lane);
     if (!cold) return;
     const unsigned at = base + __popc(peers & ((1u << lane) - 1u));
-    if (at >= line[1]) {
-        S.ovf_rows[atomicAdd(S.ovf_count, 1ull)] = (uint32_t)(S.row0 + r);
+    if (at >= S.cold) {
+        atomicOr(status, ST_MISCOUNT);
         return;
     }
-    uint8_t *row = S.part_buf + (*reinterpret_cast<const unsigned long long *>(line + 2) + at) * S.row_bytes;
-    *reinterpret_cast<long long *>(row) = k;
-    uint32_t bits = 0;
-    for (int c = 0; c < P.ncols; c++) {
+    uint8_t *row = S.part_buf + (size_t)at * S.row_bytes;
+    *reinterpret_cast<long long *>(row) = in.k;
+    *reinterpret_cast<uint32_t *>(row + 8) = in.valid & ~kKeyValid;
+#pragma unroll
+    for (int c = 0; c < NV; c++) {
+        if (c >= P.ncols) break;
         const AggColDev &C = P.c[c];
-        if (!bit_get(C.valid, C.voff, r)) continue;
-        bits |= 1u << c;
-        if (!(C.flags & (F_SUM | F_MIN | F_MAX))) continue;
+        if (!((in.valid >> c) & 1u) || !(C.flags & (F_SUM | F_MIN | F_MAX))) continue;
         uint8_t *dst = row + off_val[c];
-        if (C.type == (int)Type::I32 || C.type == (int)Type::Date32)
-            *reinterpret_cast<int *>(dst) = static_cast<const int *>(C.data)[r];
+        if (C.type == (int)Type::I32 || C.type == (int)Type::Date32) *reinterpret_cast<int *>(dst) = (int)in.lo[c];
         else if (C.type == (int)Type::Dec128)
-            *reinterpret_cast<longlong2 *>(dst) = static_cast<const longlong2 *>(C.data)[r];
-        else
-            *reinterpret_cast<long long *>(dst) = static_cast<const long long *>(C.data)[r];
+            *reinterpret_cast<longlong2 *>(dst) =
+                make_longlong2((long long)in.lo[c], (long long)value_hi(C, r, in.lo[c]));
+        else *reinterpret_cast<long long *>(dst) = (long long)in.lo[c];
     }
-    *reinterpret_cast<uint32_t *>(row + 8) = bits;
 }
 
-__global__ void __launch_bounds__(kSplitThreads) agg_split_kernel(AggPlanDev P, TableDev T, KeyIn key, int64_t n,
-                                                                  SplitDev S) {
-    extern __shared__ __align__(16) uint8_t smem[];
-    const int NH = S.H + 2;
-    uint8_t *hrec = smem;                                                          // NH records
-    long long *hkeys = reinterpret_cast<long long *>(hrec + (size_t)NH * smem_stride(P));   // hot_slots
-    int16_t *hidx = reinterpret_cast<int16_t *>(hkeys + S.hot_slots);              // hot_slots
-    const unsigned lane = threadIdx.x & 31u;
-    __shared__ int16_t s_off[kMaxValueCols];  // row record offsets (read with a varying index)
-    if (threadIdx.x < kMaxValueCols) s_off[threadIdx.x] = S.off_val[threadIdx.x];
-    for (int e = threadIdx.x; e < NH; e += blockDim.x) init_record(P, hrec + (size_t)e * smem_stride(P));
+// The hot-key lookup table of a CTA (keys and their indexes in hot_keys).
+__device__ __forceinline__ void hot_table_init(const SplitDev &S, long long *hkeys, int16_t *hidx) {
     for (int e = threadIdx.x; e < S.hot_slots; e += blockDim.x) {
         hkeys[e] = kEmptyKey;
-        hidx[e] = -1;
+        if (hidx) hidx[e] = -1;
     }
     __syncthreads();
     const int hmask = S.hot_slots - 1;
@@ -677,40 +751,76 @@ __global__ void __launch_bounds__(kSplitThreads) agg_split_kernel(AggPlanDev P, 
         for (int t = 0; t < S.hot_slots; t++) {
             if ((long long)atomicCAS(reinterpret_cast<unsigned long long *>(hkeys + pos), (unsigned long long)kEmptyKey,
                                      (unsigned long long)k) == kEmptyKey) {
-                hidx[pos] = (int16_t)j;
+                if (hidx) hidx[pos] = (int16_t)j;
                 break;
             }
             pos = (pos + 1) & hmask;
         }
     }
     __syncthreads();
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
-        const int64_t r = base + threadIdx.x;
+}
+// The index of hot key k, -1 when it is not hot (0 for a hot key when hidx
+// is null).
+__device__ __forceinline__ int hot_index(const SplitDev &S, const long long *hkeys, const int16_t *hidx, long long k,
+                                         uint64_t h) {
+    if (!S.H) return -1;
+    const int hmask = S.hot_slots - 1;
+    int pos = (int)(h & (uint64_t)hmask);
+    for (int t = 0; t < S.hot_slots; t++) {
+        const long long c = hkeys[pos];
+        if (c == k) return hidx ? hidx[pos] : 0;
+        if (c == kEmptyKey) return -1;
+        pos = (pos + 1) & hmask;
+    }
+    return -1;
+}
+// A row's place in the split: hot index (>= 0, then H for the NULL key and
+// H + 1 for the marker key), -1 for a cold row (partition from h), -2 past
+// the end.
+__device__ __forceinline__ int classify(const SplitDev &S, const long long *hkeys, const int16_t *hidx, bool live,
+                                        bool kv, long long k, uint64_t h) {
+    if (!live) return -2;
+    if (!kv) return S.H;
+    if (k == kEmptyKey) return S.H + 1;
+    return hot_index(S, hkeys, hidx, k, h);
+}
+
+template <int NV>
+__global__ void __launch_bounds__(kSplitThreads, 2) agg_split_kernel(AggPlanDev P, TableDev T, KeyIn key, int64_t n,
+                                                                     SplitDev S) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int NH = S.H + 2;
+    const int nparts = 1 << S.part_bits;
+    uint8_t *hrec = smem;                                                                  // NH records
+    long long *hkeys = reinterpret_cast<long long *>(hrec + (size_t)NH * smem_stride(P));  // hot_slots
+    unsigned *cursor = reinterpret_cast<unsigned *>(hkeys + S.hot_slots);                  // nparts
+    int16_t *hidx = reinterpret_cast<int16_t *>(cursor + nparts);                          // hot_slots
+    const unsigned lane = threadIdx.x & 31u;
+    __shared__ int16_t s_off[kMaxValueCols];  // row record offsets (read with a varying index)
+    if (threadIdx.x < kMaxValueCols) s_off[threadIdx.x] = S.off_val[threadIdx.x];
+    for (int e = threadIdx.x; e < NH; e += blockDim.x) init_record(P, hrec + (size_t)e * smem_stride(P));
+    for (int q = threadIdx.x; q < nparts; q += blockDim.x) {
+        const unsigned int *line = S.part_info + (size_t)q * kCntStride;
+        cursor[q] = (unsigned)*reinterpret_cast<const unsigned long long *>(line + 2) +
+                    S.cta_rows[(size_t)q * S.ctas + blockIdx.x];
+    }
+    hot_table_init(S, hkeys, hidx);
+    // Tiles of blockDim rows, CTA b taking tiles b, b + ctas, ... (the
+    // count kernel's assignment).
+    const int64_t step = (int64_t)gridDim.x * blockDim.x;
+    int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    RowIn<NV> cur;
+    load_row(P, key, r, r < n, cur);
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += step, r += step) {
+        RowIn<NV> nxt;
+        load_row(P, key, r + step, r + step < n, nxt);
         const bool live = r < n;
-        const bool kv = live && bit_get(key.valid, key.voff, r);
-        const long long k = kv ? key_at(key, r) : 0;
-        const uint64_t h = hash_word((uint64_t)k);
-        int hi = -1;
-        if (live) {
-            if (!kv) hi = S.H;
-            else if (k == kEmptyKey) hi = S.H + 1;
-            else if (S.H) {
-                int pos = (int)(h & (uint64_t)hmask);
-                for (int t = 0; t < S.hot_slots; t++) {
-                    const long long c = hkeys[pos];
-                    if (c == k) {
-                        hi = hidx[pos];
-                        break;
-                    }
-                    if (c == kEmptyKey) break;
-                    pos = (pos + 1) & hmask;
-                }
-            }
-        }
-        if (__any_sync(kFullMask, hi >= 0)) hot_rows(P, hrec, r, hi, lane);
-        const bool cold = live && hi < 0;
-        if (__any_sync(kFullMask, cold)) cold_rows(P, S, s_off, r, k, h, cold, lane);
+        const uint64_t h = hash_word((uint64_t)cur.k);
+        const int cls = classify(S, hkeys, hidx, live, (cur.valid & kKeyValid) != 0, cur.k, h);
+        if (__any_sync(kFullMask, cls >= 0)) hot_rows(P, hrec, cur, r, cls, lane);
+        const bool cold = cls == -1;
+        if (__any_sync(kFullMask, cold)) cold_rows(P, S, s_off, cursor, cur, r, h, cold, lane, T.status);
+        cur = nxt;
     }
     __syncthreads();
     for (int e = threadIdx.x; e < NH; e += blockDim.x) {
@@ -720,79 +830,162 @@ __global__ void __launch_bounds__(kSplitThreads) agg_split_kernel(AggPlanDev P, 
     }
 }
 
+// Cold rows per partition and CTA, by the split kernel's own test over the
+// split kernel's tiles: cta_rows[p * ctas + b] rows of partition p in CTA b's
+// tiles. Four rows per thread and step, their loads issued together.
+__global__ void __launch_bounds__(kSplitThreads) agg_count_kernel(KeyIn key, int64_t n, SplitDev S) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int nparts = 1 << S.part_bits;
+    unsigned int *s_hist = reinterpret_cast<unsigned int *>(smem);                    // nparts
+    long long *hkeys = reinterpret_cast<long long *>(s_hist + ((nparts + 1) & ~1));  // hot_slots
+    for (int q = threadIdx.x; q < nparts; q += blockDim.x) s_hist[q] = 0;
+    hot_table_init(S, hkeys, nullptr);
+    const int64_t step = (int64_t)gridDim.x * blockDim.x;
+    constexpr int U = 4;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; base < n; base += U * step) {
+        long long k[U];
+        uint8_t vb[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t r = base + u * step;
+            k[u] = r < n ? key_at(key, r) : 0;
+            vb[u] = r < n ? (key.valid ? key.valid[(key.voff + r) >> 3] : 0xFF) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t r = base + u * step;
+            const bool kv = (vb[u] >> ((key.voff + r) & 7)) & 1u;
+            const uint64_t h = hash_word((uint64_t)k[u]);
+            if (classify(S, hkeys, nullptr, r < n, kv, k[u], h) == -1)
+                atomicAdd(&s_hist[(int)(h >> (64 - S.part_bits))], 1u);
+        }
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < nparts; q += blockDim.x) S.cta_rows[(size_t)q * S.ctas + blockIdx.x] = s_hist[q];
+}
+
+// Per partition (one warp each): the exclusive running count of its rows over
+// the CTAs, in place, and the partition's total.
+__global__ void part_offsets_kernel(unsigned *cta_rows, int ctas, int nparts, unsigned *total) {
+    const int p = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const unsigned lane = threadIdx.x & 31u;
+    if (p >= nparts) return;
+    unsigned *row = cta_rows + (size_t)p * ctas;
+    unsigned carry = 0;
+    for (int b0 = 0; b0 < ctas; b0 += 32) {
+        const int b = b0 + (int)lane;
+        const unsigned x = b < ctas ? row[b] : 0u;
+        unsigned incl = x;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned y = __shfl_up_sync(kFullMask, incl, d);
+            if ((int)lane >= d) incl += y;
+        }
+        if (b < ctas) row[b] = carry + incl - x;
+        carry += __shfl_sync(kFullMask, incl, 31);
+    }
+    if (lane == 0) total[p] = carry;
+}
+
+// The partitions laid out back to back: each partition's line [rows, rows,
+// base] and the rows of all (one CTA of 1024 threads).
+__global__ void __launch_bounds__(1024) part_bases_kernel(const unsigned *total, int nparts, unsigned *info,
+                                                          unsigned long long *cold) {
+    __shared__ unsigned long long s_warp[32];
+    const int per = (nparts + blockDim.x - 1) / blockDim.x;
+    const int q0 = threadIdx.x * per;
+    unsigned long long mine = 0;
+    for (int q = q0; q < q0 + per && q < nparts; q++) mine += total[q];
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    unsigned long long incl = mine;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned long long y = __shfl_up_sync(kFullMask, incl, d);
+        if ((int)lane >= d) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const unsigned long long w = lane < blockDim.x / 32 ? s_warp[lane] : 0ull;
+        unsigned long long wi = w;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kFullMask, wi, d);
+            if ((int)lane >= d) wi += y;
+        }
+        s_warp[lane] = wi - w;  // exclusive over the warps
+        if (lane == 31) *cold = wi;
+    }
+    __syncthreads();
+    unsigned long long base = s_warp[warp] + incl - mine;
+    for (int q = q0; q < q0 + per && q < nparts; q++) {
+        unsigned *line = info + (size_t)q * kCntStride;
+        line[0] = line[1] = total[q];
+        *reinterpret_cast<unsigned long long *>(line + 2) = base;
+        base += total[q];
+    }
+}
+
 struct PartDev {
     const uint8_t *part_buf;
     const unsigned int *part_info;  // as SplitDev::part_info
     int row_bytes;
     int16_t off_val[kMaxValueCols];
-    const int *todo;   // the partitions to run: CTA b runs partition todo[b]
+    const int *todo;   // the partitions to run: CTA b runs partition todo[b] (all, in order, when null)
     uint32_t *start;   // per partition: its first row not yet merged (read and written)
     int *failed;       // partitions that stopped for want of room in the global table
     int L;             // local records per CTA (>= the block size)
     int slots;         // local table slots: a power of two >= 2L
 };
 
-// One row record folded into a (shared-memory) record.
+// One row record folded into a shared-memory record.
 __device__ __forceinline__ void fold_row(const AggPlanDev &P, const int16_t *off_val, uint8_t *rec, const uint8_t *row) {
-    atomicAdd(reinterpret_cast<unsigned long long *>(rec + P.off_rows), 1ull);
+    s_count(rec + P.off_rows, 1u);
     const uint32_t bits = *reinterpret_cast<const uint32_t *>(row + 8);
     for (int c = 0; c < P.ncols; c++) {
         if (!((bits >> c) & 1u)) continue;
         const AggColDev &C = P.c[c];
         if (!(C.flags & (F_SUM | F_MIN | F_MAX))) {
-            atomicAdd(reinterpret_cast<unsigned long long *>(rec + C.off_count), 1ull);
+            s_count(rec + C.off_count, 1u);
             continue;
         }
         uint64_t lo, hi;
         value_words(C, row + off_val[c], 0, lo, hi);
-        const bool f64 = C.type == (int)Type::F64;
-        const long long m = mm_key(C, lo);
-        fold_partial(C, rec, 1ull, lo, hi, f64 ? __longlong_as_double((long long)lo) : 0.0, 0.0, m, m);
+        s_fold_value(C, rec, lo, hi);
     }
 }
 
-// The local record of key k, claimed (and initialised) when new; -1 when the
-// table has no record left or a wait gave up. The key claims its slot first;
-// only the claimer takes a record (so no record is ever wasted, and a
-// partition's tile of at most L keys always fits an emptied table) and then
-// publishes its index. A reader of the same key waits, bounded, for it: one
-// lane per key and warp looks keys up, so the claimer is in another warp.
+// The local slot of key k (its key claimed when new); -1 only when every
+// slot is taken. The lane that claims a slot takes the key's record, or
+// marks the slot kTableFull when the table has no record left, and publishes
+// the record's index in sidx; other lanes read it after the next barrier, so
+// no lane waits for another.
 constexpr uint16_t kNoRecord = 0xFFFFu, kTableFull = 0xFFFDu;
-__device__ __forceinline__ int local_record(const AggPlanDev &P, const PartDev &D, long long *skeys, uint16_t *sidx,
-                                            uint8_t *lrec, int *fill, long long k, uint64_t h, uint32_t *status) {
+__device__ __forceinline__ int local_slot(const AggPlanDev &P, const PartDev &D, long long *skeys, uint16_t *sidx,
+                                          uint8_t *lrec, int *fill, long long k, uint64_t h, bool &full) {
     const int mask = D.slots - 1;
     int pos = (int)(h & (uint64_t)mask);
     for (int t = 0; t < D.slots; t++) {
-        long long cur = *reinterpret_cast<volatile long long *>(skeys + pos);
+        long long cur = skeys[pos];
         if (cur == kEmptyKey) {
             cur = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(skeys + pos), (unsigned long long)kEmptyKey,
                                        (unsigned long long)k);
             if (cur == kEmptyKey) {
                 const int e = atomicAdd(fill, 1);
                 if (e >= D.L) {
-                    *reinterpret_cast<volatile uint16_t *>(sidx + pos) = kTableFull;
-                    return -1;
+                    sidx[pos] = kTableFull;
+                    full = true;
+                } else {
+                    init_record(P, lrec + (size_t)e * smem_stride(P));
+                    sidx[pos] = (uint16_t)e;
                 }
-                init_record(P, lrec + (size_t)e * smem_stride(P));
-                __threadfence_block();
-                *reinterpret_cast<volatile uint16_t *>(sidx + pos) = (uint16_t)e;
-                return e;
+                return pos;
             }
         }
-        if (cur == k) {
-            for (int it = 0; it < (1 << 20); it++) {
-                const uint16_t e = *reinterpret_cast<volatile uint16_t *>(sidx + pos);
-                if (e != kNoRecord) {
-                    __threadfence_block();
-                    return e == kTableFull ? -1 : (int)e;
-                }
-                __nanosleep(20);
-            }
-            atomicOr(status, ST_TIMEOUT);
-            return -1;
-        }
+        if (cur == k) return pos;
         pos = (pos + 1) & mask;
     }
+    full = true;
     return -1;
 }
 
@@ -829,7 +1022,7 @@ __global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, Ta
     __shared__ int s_fill, s_fail;
     __shared__ int16_t s_off[kMaxValueCols];  // row record offsets (read with a varying index)
     if (threadIdx.x < kMaxValueCols) s_off[threadIdx.x] = D.off_val[threadIdx.x];
-    const int p = D.todo[blockIdx.x];
+    const int p = D.todo ? D.todo[blockIdx.x] : (int)blockIdx.x;
     const unsigned int *line = D.part_info + (size_t)p * kCntStride;
     const uint32_t cnt = line[0], cap = line[1];
     const uint32_t rows = cnt < cap ? cnt : cap;
@@ -846,6 +1039,17 @@ __global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, Ta
         }
         __syncthreads();
     };
+    // Merges the window's records; false (the partition stopped, to run again
+    // from `window` on a bigger table) when the global table had no room.
+    auto flush = [&]() -> bool {
+        const int m = s_fill < D.L ? s_fill : D.L;
+        if (flush_local(P, T, D, skeys, sidx, lrec, lgid, m, &s_fail)) return true;
+        if (threadIdx.x == 0) {
+            D.start[p] = window;
+            atomicAdd(D.failed, 1);
+        }
+        return false;
+    };
     reset();
     for (uint32_t base = window; base < rows; base += blockDim.x) {
         const uint32_t i = base + threadIdx.x;
@@ -853,96 +1057,27 @@ __global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, Ta
         const uint8_t *row = buf + (size_t)i * D.row_bytes;
         const long long k = live ? *reinterpret_cast<const long long *>(row) : 0;
         const uint64_t h = hash_word((uint64_t)k);
-        const unsigned lane = threadIdx.x & 31u;
-        bool folded = false;
-        for (int attempt = 0; attempt < 2 && !folded; attempt++) {
-            // One lane per distinct key of the warp looks it up; the lanes of
-            // that key take its record (no lane waits on its own warp).
-            const unsigned peers = __match_any_sync(kFullMask, live ? k : kEmptyKey);
-            const int lead = __ffs(peers) - 1;
-            int e = 0;
-            if (live && (int)lane == lead) e = local_record(P, D, skeys, sidx, lrec, &s_fill, k, h, T.status);
-            e = __shfl_sync(kFullMask, e, lead);
-            if (!__syncthreads_or(e < 0)) {
-                if (live) fold_row(P, s_off, lrec + (size_t)e * smem_stride(P), row);
-                folded = true;
-                continue;
-            }
-            if (attempt == 1) break;  // an emptied table did not take the tile: only a wait that gave up does that
-            // The table is full: merge the window's rows (those before this
-            // tile; the tile's new records are still empty) and retry the tile.
-            const int m = s_fill < D.L ? s_fill : D.L;
-            if (!flush_local(P, T, D, skeys, sidx, lrec, lgid, m, &s_fail)) {
-                if (threadIdx.x == 0) {
-                    D.start[p] = window;
-                    atomicAdd(D.failed, 1);
-                }
-                return;
-            }
+        // Slots first, then (after the barrier) the records they name. A tile
+        // that met a full table merges the window's rows (those before the
+        // tile; its own new records are still empty) and runs again on the
+        // emptied table, which holds the tile's at most L keys.
+        bool full = false;
+        int pos = live ? local_slot(P, D, skeys, sidx, lrec, &s_fill, k, h, full) : 0;
+        if (__syncthreads_or(full)) {
+            if (!flush()) return;
             window = base;
             reset();
-        }
-        if (!folded && threadIdx.x == 0) atomicOr(T.status, ST_TIMEOUT);
-    }
-    __syncthreads();
-    const int m = s_fill < D.L ? s_fill : D.L;
-    if (!flush_local(P, T, D, skeys, sidx, lrec, lgid, m, &s_fail)) {
-        if (threadIdx.x == 0) {
-            D.start[p] = window;
-            atomicAdd(D.failed, 1);
-        }
-        return;
-    }
-    if (threadIdx.x == 0) D.start[p] = rows;
-}
-
-// Cold rows per partition: the split kernel's own test (a valid key that is
-// not the marker and not hot), so that partition p gets exactly hist[p] rows.
-__global__ void __launch_bounds__(kSplitThreads) agg_count_kernel(KeyIn key, int64_t n, SplitDev S,
-                                                                  unsigned int *hist) {
-    extern __shared__ __align__(16) uint8_t smem[];
-    const int nparts = 1 << S.part_bits;
-    unsigned int *s_hist = reinterpret_cast<unsigned int *>(smem);                 // nparts
-    long long *hkeys = reinterpret_cast<long long *>(s_hist + ((nparts + 1) & ~1));  // hot_slots
-    for (int q = threadIdx.x; q < nparts; q += blockDim.x) s_hist[q] = 0;
-    for (int e = threadIdx.x; e < S.hot_slots; e += blockDim.x) hkeys[e] = kEmptyKey;
-    __syncthreads();
-    const int hmask = S.hot_slots - 1;
-    for (int j = threadIdx.x; j < S.H; j += blockDim.x) {
-        const long long k = S.hot_keys[j];
-        int pos = (int)(hash_word((uint64_t)k) & (uint64_t)hmask);
-        for (int t = 0; t < S.hot_slots; t++) {
-            if ((long long)atomicCAS(reinterpret_cast<unsigned long long *>(hkeys + pos), (unsigned long long)kEmptyKey,
-                                     (unsigned long long)k) == kEmptyKey)
-                break;
-            pos = (pos + 1) & hmask;
-        }
-    }
-    __syncthreads();
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
-        if (!bit_get(key.valid, key.voff, r)) continue;
-        const long long k = key_at(key, r);
-        if (k == kEmptyKey) continue;
-        const uint64_t h = hash_word((uint64_t)k);
-        bool hot = false;
-        if (S.H) {
-            int pos = (int)(h & (uint64_t)hmask);
-            for (int t = 0; t < S.hot_slots; t++) {
-                const long long c = hkeys[pos];
-                if (c == k) {
-                    hot = true;
-                    break;
-                }
-                if (c == kEmptyKey) break;
-                pos = (pos + 1) & hmask;
+            full = false;
+            pos = live ? local_slot(P, D, skeys, sidx, lrec, &s_fill, k, h, full) : 0;
+            if (__syncthreads_or(full)) {  // cannot happen: a tile has at most L keys
+                if (threadIdx.x == 0) atomicOr(T.status, ST_TOO_MANY);
+                return;
             }
         }
-        if (!hot) atomicAdd(&s_hist[(int)(h >> (64 - S.part_bits))], 1u);
+        if (live) fold_row(P, s_off, lrec + (size_t)sidx[pos] * smem_stride(P), row);
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < nparts; q += blockDim.x)
-        if (s_hist[q]) atomicAdd(hist + q, s_hist[q]);
+    if (flush() && threadIdx.x == 0) D.start[p] = rows;
 }
 
 // Group ids of the hot keys (inserted into the global table), then the NULL
@@ -1352,7 +1487,6 @@ class HashAggregate {
     bool use_partitioned(int64_t n) const;
     void push_partitioned(const DevBatch &b, const KeyIn &key, int64_t n);
     void plan_partitioned(const KeyIn &key, int64_t n);
-    void drain_deferred(const DevBatch &b, const KeyIn &key, DBuf &ovf, DBuf &ovf_count, unsigned long long deferred);
     bool part_planned_ = false;
     DBuf part_hot_keys_, part_hot_gids_;
     int part_hot_ = 0;
@@ -1795,39 +1929,8 @@ void HashAggregate::plan_partitioned(const KeyIn &key, int64_t n) {
     KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // `hot` is a stack vector
 }
 
-// Rows listed in `ovf` (deferred: their partition was full) through the
-// global-table kernel, growing the table when they need room.
-void HashAggregate::drain_deferred(const DevBatch &b, const KeyIn &key, DBuf &ovf, DBuf &ovf_count,
-                                   unsigned long long deferred) {
-    AggPlanDev P = P_;
-    for (int c = 0; c < P.ncols; c++) {
-        const DevCol &col = b.cols[value_cols_[c]];
-        P.c[c].data = col.data;
-        P.c[c].valid = col.valid;
-        P.c[c].voff = col.valid_off;
-    }
-    DBuf idx;
-    for (int round = 0; round < 16; round++) {
-        if (deferred == 0) return;
-        known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());
-        if (known_groups_ + (int64_t)deferred > (int64_t)limit_) grow((uint64_t)known_groups_ + deferred);
-        idx = DBuf(rt_, (size_t)deferred * 4);
-        KRV_CUDA(cudaMemcpyAsync(idx.get(), ovf.get(), (size_t)deferred * 4, cudaMemcpyDeviceToDevice, rt_->stream));
-        KRV_CUDA(cudaMemsetAsync(ovf_count.get(), 0, 8, rt_->stream));
-        TableDev T{keys_.as<long long>(), gids_.as<uint32_t>(), slots_ - 1, states_.as<uint8_t>(), gkeys_.as<long long>(),
-                   ngroups_.as<unsigned long long>(), limit_, status_word(rt_)};
-        agg_global_kernel<<<grid_for(rt_, (int64_t)deferred, 256, 8), 256, 0, rt_->stream>>>(
-            P, T, key, (int64_t)deferred, idx.as<uint32_t>(), ovf.as<uint32_t>(), ovf_count.as<unsigned long long>());
-        rt_->launches++;
-        check_launch("agg_global_kernel");
-        deferred = read_scalar<unsigned long long>(rt_, ovf_count.get());
-    }
-    fail(KRV_INTERNAL, "aggregate: table growth did not converge");
-}
-
 void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_t n) {
     clear_status(rt_);
-    known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());
     pending_rows_ = 0;
     if (!part_planned_) plan_partitioned(key, n);
     AggPlanDev P = P_;
@@ -1841,26 +1944,23 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
     }
     known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());  // the hot keys' groups too
     const int L = part_local_;
-    // Partitions: each to hold about L/2 distinct keys.
+    // Partitions: each to hold about L/2 distinct keys (at most 2^13 of them:
+    // every split CTA keeps a cursor per partition in shared memory).
     int bits = 5;
-    while (bits < 14 && ((int64_t)1 << bits) * (L / 2) < part_groups_est_) bits++;
+    while (bits < 13 && ((int64_t)1 << bits) * (L / 2) < part_groups_est_) bits++;
     const int nparts = 1 << bits;
     const int H = part_hot_;
     const int hot_slots = H ? (int)next_pow2((uint64_t)2 * H) : 0;
-    const size_t split_smem = (size_t)(H + 2) * smem_stride(P) + (size_t)hot_slots * 10;
-    KRV_CUDA(cudaFuncSetAttribute(agg_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)split_smem));
+    const size_t split_smem = (size_t)(H + 2) * smem_stride(P) + (size_t)hot_slots * 10 + (size_t)nparts * 4;
+    const size_t count_smem = (size_t)((nparts + 1) & ~1) * 4 + (size_t)hot_slots * 8;
+    const auto split_kernel = P.ncols <= 4 ? agg_split_kernel<4> : agg_split_kernel<kMaxValueCols>;
+    KRV_CUDA(cudaFuncSetAttribute(split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)split_smem));
+    KRV_CUDA(cudaFuncSetAttribute(agg_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)count_smem));
     KRV_CUDA(cudaFuncSetAttribute(agg_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)part_smem_));
     int split_blocks = 0, part_blocks = 0;
-    KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&split_blocks, agg_split_kernel, kSplitThreads, split_smem));
+    KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&split_blocks, split_kernel, kSplitThreads, split_smem));
     KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&part_blocks, agg_part_kernel, kPartThreads, part_smem_));
     if (split_blocks < 1 || part_blocks < 1) fail(KRV_INTERNAL, "aggregate: partitioned kernels do not fit an SM");
-    DBuf todo_all(rt_, (size_t)nparts * 4);
-    {
-        std::vector<int> iota(nparts);
-        for (int p = 0; p < nparts; p++) iota[p] = p;
-        KRV_CUDA(cudaMemcpyAsync(todo_all.get(), iota.data(), (size_t)nparts * 4, cudaMemcpyHostToDevice, rt_->stream));
-        KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // `iota` is a stack vector
-    }
     const KeyIn key0 = key;
     for (int64_t row0 = 0; row0 < n; row0 += kPartSliceRows) {
         const int64_t ns = std::min<int64_t>(kPartSliceRows, n - row0);
@@ -1872,44 +1972,35 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
         S.part_bits = bits;
         S.row_bytes = part_row_bytes_;
         for (int c = 0; c < kMaxValueCols; c++) S.off_val[c] = part_off_val_[c];
+        // The count and split kernels take the same tiles: one CTA per
+        // resident split CTA.
+        S.ctas = (int)std::min<int64_t>((int64_t)split_blocks * rt_->sm_count, ceil_div(ns, kSplitThreads));
         KeyIn ks = key0;
         ks.data = static_cast<const uint8_t *>(key0.data) + row0 * key0.width;
         ks.voff = key0.voff + row0;
-        // Exact partition sizes: one pass over the keys with the split's own
-        // test, then the partitions laid out back to back.
-        DBuf hist(rt_, (size_t)nparts * 4);
-        KRV_CUDA(cudaMemsetAsync(hist.get(), 0, hist.bytes(), rt_->stream));
-        {
-            const size_t csmem = (size_t)((nparts + 1) & ~1) * 4 + (size_t)hot_slots * 8;
-            KRV_CUDA(cudaFuncSetAttribute(agg_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem));
-            int cblocks = 0;
-            KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cblocks, agg_count_kernel, kSplitThreads, csmem));
-            const int grid0 = (int)std::min<int64_t>((int64_t)std::max(cblocks, 1) * rt_->sm_count,
-                                                     ceil_div(ns, kSplitThreads));
-            agg_count_kernel<<<grid0, kSplitThreads, csmem, rt_->stream>>>(ks, ns, S, hist.as<unsigned int>());
-            rt_->launches++;
-            check_launch("agg_count_kernel");
-        }
-        std::vector<unsigned int> hh(nparts);
-        KRV_CUDA(cudaMemcpyAsync(hh.data(), hist.get(), (size_t)nparts * 4, cudaMemcpyDeviceToHost, rt_->stream));
-        KRV_CUDA(cudaStreamSynchronize(rt_->stream));
-        std::vector<unsigned int> info((size_t)nparts * kCntStride, 0u);
-        unsigned long long cold = 0;
-        for (int p = 0; p < nparts; p++) {
-            unsigned int *line = info.data() + (size_t)p * kCntStride;
-            line[1] = hh[p];
-            memcpy(line + 2, &cold, 8);
-            cold += hh[p];
-        }
-        DBuf part_info(rt_, info.size() * 4);
-        KRV_CUDA(cudaMemcpyAsync(part_info.get(), info.data(), info.size() * 4, cudaMemcpyHostToDevice, rt_->stream));
+        // Exact partition sizes, per partition and CTA: the split's own test
+        // over its own tiles, then the partitions laid out back to back and
+        // every CTA's share of each placed within it.
+        DBuf cta_rows(rt_, (size_t)nparts * S.ctas * 4), totals(rt_, (size_t)nparts * 4);
+        DBuf part_info(rt_, (size_t)nparts * kCntStride * 4);
+        DBuf ctl(rt_, 16);  // [0] rows in the partitions (u64), [8] failed partitions (int)
+        KRV_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, rt_->stream));
+        S.cta_rows = cta_rows.as<unsigned>();
+        agg_count_kernel<<<S.ctas, kSplitThreads, count_smem, rt_->stream>>>(ks, ns, S);
+        rt_->launches++;
+        check_launch("agg_count_kernel");
+        part_offsets_kernel<<<(int)ceil_div((int64_t)nparts * 32, 256), 256, 0, rt_->stream>>>(
+            cta_rows.as<unsigned>(), S.ctas, nparts, totals.as<unsigned>());
+        rt_->launches++;
+        check_launch("part_offsets_kernel");
+        part_bases_kernel<<<1, 1024, 0, rt_->stream>>>(totals.as<unsigned>(), nparts, part_info.as<unsigned>(),
+                                                      ctl.as<unsigned long long>());
+        rt_->launches++;
+        check_launch("part_bases_kernel");
+        const unsigned long long cold = read_scalar<unsigned long long>(rt_, ctl.get());
         DBuf part_buf(rt_, (size_t)std::max<unsigned long long>(cold, 1) * part_row_bytes_);
         DBuf start(rt_, (size_t)nparts * 4);
-        DBuf ctl(rt_, 16);  // [0] deferred rows (u64), [8] failed partitions (int)
-        DBuf ovf(rt_, (size_t)ns * 4);
         KRV_CUDA(cudaMemsetAsync(start.get(), 0, start.bytes(), rt_->stream));
-        KRV_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, rt_->stream));
-        KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // `info` is a stack vector
         // Room in the table for the keys this slice may add (an estimate; a
         // partition that finds none stops and runs again after a grow).
         const int64_t want = known_groups_ + std::min<int64_t>(ns, part_groups_est_) + H + 2;
@@ -1918,12 +2009,9 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
                    ngroups_.as<unsigned long long>(), limit_, status_word(rt_)};
         S.part_buf = part_buf.as<uint8_t>();
         S.part_info = part_info.as<unsigned int>();
-        S.ovf_rows = ovf.as<uint32_t>();
-        S.ovf_count = ctl.as<unsigned long long>();
-        S.row0 = row0;
+        S.cold = cold;
         const AggPlanDev PS = slice_plan(P, row0, widths);
-        const int grid1 = (int)std::min<int64_t>((int64_t)split_blocks * rt_->sm_count, ceil_div(ns, kSplitThreads));
-        agg_split_kernel<<<grid1, kSplitThreads, split_smem, rt_->stream>>>(PS, T, ks, ns, S);
+        split_kernel<<<S.ctas, kSplitThreads, split_smem, rt_->stream>>>(PS, T, ks, ns, S);
         rt_->launches++;
         check_launch("agg_split_kernel");
         PartDev D{};
@@ -1931,7 +2019,7 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
         D.part_info = part_info.as<unsigned int>();
         D.row_bytes = part_row_bytes_;
         for (int c = 0; c < kMaxValueCols; c++) D.off_val[c] = part_off_val_[c];
-        D.todo = todo_all.as<int>();
+        D.todo = nullptr;
         D.start = start.as<uint32_t>();
         D.failed = reinterpret_cast<int *>(ctl.as<uint8_t>() + 8);
         D.L = L;
@@ -1941,19 +2029,14 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
         check_launch("agg_part_kernel");
         DBuf todo;
         for (int round = 0;; round++) {
-            struct {
-                unsigned long long deferred;
-                int failed, pad;
-            } c{};
-            read_device(rt_, ctl.get(), sizeof(c), &c);
+            const int failed = read_scalar<int>(rt_, ctl.as<uint8_t>() + 8);
             const uint32_t st = take_status(rt_);
             if (st & ST_TIMEOUT) fail(KRV_TIMEOUT, "aggregate: a wait for a group id gave up");
             if (st & ST_CAPACITY) fail(KRV_INTERNAL, "aggregate: a hot key has no group");
+            if (st & ST_TOO_MANY) fail(KRV_INTERNAL, "aggregate: a partition tile did not fit an emptied table");
+            if (st & ST_MISCOUNT) fail(KRV_INTERNAL, "aggregate: the split wrote more rows than were counted");
             known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());
-            if (c.failed == 0) {
-                drain_deferred(b, key0, ovf, ctl, c.deferred);
-                break;
-            }
+            if (failed == 0) break;
             if (round == 16) fail(KRV_INTERNAL, "aggregate: table growth did not converge");
             // Partitions that stopped: their windows run again on a bigger table.
             std::vector<uint32_t> hs(nparts), hc((size_t)nparts * kCntStride);

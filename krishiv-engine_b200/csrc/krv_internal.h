@@ -240,6 +240,7 @@ enum StatusBit : uint32_t {
     ST_OVERFLOW = 2u,
     ST_CAPACITY = 4u,
     ST_TOO_MANY = 8u,
+    ST_MISCOUNT = 16u,  // a pass wrote more rows than its counting pass gave it room for
 };
 uint32_t *status_word(Runtime *rt);
 void clear_status(Runtime *rt);
