@@ -297,6 +297,53 @@ __device__ uint32_t find_or_insert(const TableDev &T, const AggPlanDev &P, long 
     return kOverflowGid;
 }
 
+// The group of key k when the table has it, else kPending (a lookup only).
+__device__ __forceinline__ uint32_t table_find(const TableDev &T, long long k) {
+    uint64_t pos = hash_word((uint64_t)k) & T.mask;
+    for (uint64_t p = 0; p <= T.mask; p++) {
+        const long long cur = __ldcg(T.keys + pos);
+        if (cur == k) return wait_gid(T, pos);
+        if (cur == kEmptyKey) return kPending;
+        pos = (pos + 1) & T.mask;
+    }
+    return kPending;
+}
+// Key k of group g inserted into the hash table by the one thread that
+// handles k (its partition's CTA), which looks it up only after a barrier.
+__device__ __forceinline__ void table_index_owned(const TableDev &T, long long k, uint32_t g) {
+    uint64_t pos = hash_word((uint64_t)k) & T.mask;
+    for (uint64_t p = 0; p <= T.mask; p++) {
+        if (__ldcg(T.keys + pos) == kEmptyKey &&
+            atomicCAS(reinterpret_cast<unsigned long long *>(T.keys + pos), (unsigned long long)kEmptyKey,
+                      (unsigned long long)k) == (unsigned long long)kEmptyKey) {
+            T.gids[pos] = g;
+            return;
+        }
+        pos = (pos + 1) & T.mask;
+    }
+}
+
+// Groups [from, to), whose keys and records exist but which the hash table
+// may not index yet, inserted into it: each key once (a key has one group).
+__global__ void index_groups_kernel(const long long *gkeys, uint64_t from, uint64_t to, long long *keys, uint32_t *gids,
+                                    uint64_t mask) {
+    for (uint64_t g = from + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < to;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const long long k = gkeys[g];
+        uint64_t pos = hash_word((uint64_t)k) & mask;
+        for (uint64_t p = 0; p <= mask; p++) {
+            const long long old = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(keys + pos),
+                                                       (unsigned long long)kEmptyKey, (unsigned long long)k);
+            if (old == kEmptyKey) {
+                gids[pos] = (uint32_t)g;
+                break;
+            }
+            if (old == k) break;  // agg_part_kernel indexed it already
+            pos = (pos + 1) & mask;
+        }
+    }
+}
+
 __device__ __forceinline__ uint32_t group_of(const TableDev &T, const AggPlanDev &P, const KeyIn &key, int64_t r,
                                              long long &k) {
     if (!bit_get(key.valid, key.voff, r)) return kNullGid;
@@ -552,36 +599,6 @@ __device__ __forceinline__ void value_words(const AggColDev &C, const void *data
         hi = v < 0 ? ~0ull : 0ull;
     }
 }
-// Folds one row's value (lo, hi as value_words gives them) into a
-// shared-memory record with concurrent updaters.
-__device__ __forceinline__ void s_fold_value(const AggColDev &C, uint8_t *r, uint64_t lo, uint64_t hi) {
-    s_count(r + C.off_count, 1u);
-    const bool i32 = C.type == (int)Type::I32 || C.type == (int)Type::Date32;
-    if (C.type == (int)Type::F64) {
-        const double v = __longlong_as_double((long long)lo);
-        if (C.flags & F_SUM)
-            atomic_add_dd(reinterpret_cast<double *>(r + C.off_sum), reinterpret_cast<double *>(r + C.off_sum + 8), v);
-        if (C.flags & (F_MIN | F_MAX)) {
-            const unsigned long long key = f64_order_key(v);
-            if (C.flags & F_MIN) atomicMin(reinterpret_cast<unsigned long long *>(r + C.off_min), key);
-            if (C.flags & F_MAX) atomicMax(reinterpret_cast<unsigned long long *>(r + C.off_max), key);
-        }
-        return;
-    }
-    if (C.flags & F_SUM) {
-        if (i32) s_add_i64(r + C.off_sum, (long long)lo);
-        else s_add_i128(r + C.off_sum, lo, hi);
-    }
-    if (C.flags & F_MIN) {
-        if (i32) atomicMin(reinterpret_cast<int *>(r + C.off_min), (int)lo);
-        else atomicMin(reinterpret_cast<long long *>(r + C.off_min), (long long)lo);
-    }
-    if (C.flags & F_MAX) {
-        if (i32) atomicMax(reinterpret_cast<int *>(r + C.off_max), (int)lo);
-        else atomicMax(reinterpret_cast<long long *>(r + C.off_max), (long long)lo);
-    }
-}
-
 // One row's inputs, loaded a warp step ahead of their use: the loads of a
 // step do not depend on one another, so a warp waits for memory once per
 // step and the wait overlaps the previous step's work. NV bounds the value
@@ -934,150 +951,483 @@ struct PartDev {
     const int *todo;   // the partitions to run: CTA b runs partition todo[b] (all, in order, when null)
     uint32_t *start;   // per partition: its first row not yet merged (read and written)
     int *failed;       // partitions that stopped for want of room in the global table
-    int L;             // local records per CTA (>= the block size)
-    int slots;         // local table slots: a power of two >= 2L
+    unsigned long long id_limit;  // new group ids only while the count is at most this
+    unsigned long long first_new; // the first group id this launch hands out
+    int lookup;                   // the global table may hold keys of these partitions
 };
 
-// One row record folded into a shared-memory record.
-__device__ __forceinline__ void fold_row(const AggPlanDev &P, const int16_t *off_val, uint8_t *rec, const uint8_t *row) {
-    s_count(rec + P.off_rows, 1u);
+// agg_part_kernel works through a partition in chunks of at most kChunkRows
+// rows:
+//  1. the chunk's row records are copied into shared memory, and every row's
+//     key gets a local slot (claimed when new) and its rank among the chunk's
+//     rows of that slot (the value a 32-bit shared atomic add returned);
+//  2. the slot counts are scanned and the used slots listed by size;
+//  3. each row is placed at its slot's offset plus its rank (a counting sort);
+//     keys new to the local table get their group ids in one step per chunk:
+//     a lookup each (none while the global table holds no cold key), then one
+//     reservation of ids for those it lacks (all or none: a chunk whose keys
+//     find no room is not merged, and the partition stops there to run again
+//     after the host grows the table); a new group's key goes to gkeys, and
+//     the host indexes the new groups in the hash table (index_groups_kernel)
+//     before anything looks keys up again;
+//  4. each key's rows are reduced in registers by a team sized to them (a
+//     lane below kTeamRows rows, kTeamLanes lanes below kWarpRows, a warp
+//     per kSegRows rows from there on), and the sums merged into the key's
+//     global record with plain loads and stores: a cold key lives in one
+//     partition only, so its record has one writer, and the chunks of a
+//     partition run in turn. Only a key of more than kSegRows rows, whose
+//     segments several warps reduce at once, merges through atomics.
+// The local table and its group ids carry over from chunk to chunk, until
+// its keys pass a quarter of its slots.
+constexpr int kChunkRows = 1024;
+constexpr int kChunkSlots = 2048;
+constexpr int kTeamRows = 8, kTeamLanes = 8, kWarpRows = 32, kSegRows = 128;
+constexpr int kAccCols = 2;  // value columns reduced per pass over a key's rows (three spill at 64 registers)
+constexpr uint32_t kNoGid = 0xFFFFFFFFu, kNewGid = 0x80000000u;
+
+__host__ __device__ __forceinline__ size_t part_smem_bytes(int row_bytes) {
+    return (size_t)kChunkRows * row_bytes + (size_t)kChunkSlots * (8 + 4 + 4 + 2) + (size_t)kChunkRows * 2 * 5;
+}
+
+// The accumulators of up to kAccCols value columns: the record's fields in
+// registers. Sums: int32 columns in s0 (64-bit); int64 and decimal columns as
+// 128 bits (s0 low, s1 high); float64 as a double-double (s0 high, s1 low,
+// as bits). MIN/MAX: float64 as order keys (unsigned), the rest signed.
+struct ColAcc {
+    uint32_t cnt;  // a chunk has fewer than 2^32 rows
+    uint64_t s0, s1;
+    uint64_t mn, mx;
+};
+struct RowAcc {
+    uint32_t rows;
+    ColAcc c[kAccCols];
+};
+
+__device__ __forceinline__ bool acc_f64(const AggColDev &C) { return C.type == (int)Type::F64; }
+__device__ __forceinline__ bool acc_i32(const AggColDev &C) {
+    return C.type == (int)Type::I32 || C.type == (int)Type::Date32;
+}
+
+__device__ __forceinline__ void acc_init(const AggPlanDev &P, int cb, RowAcc &a) {
+    a.rows = 0;
+#pragma unroll
+    for (int u = 0; u < kAccCols; u++) {
+        ColAcc &x = a.c[u];
+        x.cnt = 0;
+        x.s0 = x.s1 = 0;
+        const bool f = cb + u < P.ncols && acc_f64(P.c[cb + u]);
+        x.mn = f ? ~0ull : (uint64_t)LLONG_MAX;
+        x.mx = f ? 0ull : (uint64_t)LLONG_MIN;
+    }
+}
+
+__device__ __forceinline__ void acc_min_max(bool f64, ColAcc &x, uint64_t mn, uint64_t mx) {
+    if (f64) {
+        x.mn = mn < x.mn ? mn : x.mn;
+        x.mx = mx > x.mx ? mx : x.mx;
+    } else {
+        x.mn = (long long)mn < (long long)x.mn ? mn : x.mn;
+        x.mx = (long long)mx > (long long)x.mx ? mx : x.mx;
+    }
+}
+// x += the sums of another partial y (counts apart).
+__device__ __forceinline__ void acc_add(const AggColDev &C, ColAcc &x, const ColAcc &y) {
+    if (C.flags & F_SUM) {
+        if (acc_f64(C)) {
+            double s, e;
+            two_sum(__longlong_as_double((long long)x.s0), __longlong_as_double((long long)y.s0), s, e);
+            const double lo = __dadd_rn(__dadd_rn(__longlong_as_double((long long)x.s1),
+                                                  __longlong_as_double((long long)y.s1)), e);
+            x.s0 = (uint64_t)__double_as_longlong(s);
+            x.s1 = (uint64_t)__double_as_longlong(lo);
+        } else if (acc_i32(C)) {
+            x.s0 += y.s0;
+        } else {
+            const uint64_t lo = x.s0 + y.s0;
+            x.s1 += y.s1 + (lo < x.s0 ? 1ull : 0ull);
+            x.s0 = lo;
+        }
+    }
+    if (C.flags & (F_MIN | F_MAX)) acc_min_max(acc_f64(C), x, y.mn, y.mx);
+}
+
+// One row record's columns [cb, cb + kAccCols) folded into the accumulators.
+__device__ __forceinline__ void acc_row(const AggPlanDev &P, const int16_t *off_val, int cb, RowAcc &a,
+                                        const uint8_t *row) {
+    a.rows++;
     const uint32_t bits = *reinterpret_cast<const uint32_t *>(row + 8);
-    for (int c = 0; c < P.ncols; c++) {
+#pragma unroll
+    for (int u = 0; u < kAccCols; u++) {
+        const int c = cb + u;
+        if (c >= P.ncols) break;
         if (!((bits >> c) & 1u)) continue;
         const AggColDev &C = P.c[c];
-        if (!(C.flags & (F_SUM | F_MIN | F_MAX))) {
-            s_count(rec + C.off_count, 1u);
-            continue;
-        }
+        ColAcc &x = a.c[u];
+        x.cnt++;
+        if (!(C.flags & (F_SUM | F_MIN | F_MAX))) continue;
         uint64_t lo, hi;
         value_words(C, row + off_val[c], 0, lo, hi);
-        s_fold_value(C, rec, lo, hi);
-    }
-}
-
-// The local slot of key k (its key claimed when new); -1 only when every
-// slot is taken. The lane that claims a slot takes the key's record, or
-// marks the slot kTableFull when the table has no record left, and publishes
-// the record's index in sidx; other lanes read it after the next barrier, so
-// no lane waits for another.
-constexpr uint16_t kNoRecord = 0xFFFFu, kTableFull = 0xFFFDu;
-__device__ __forceinline__ int local_slot(const AggPlanDev &P, const PartDev &D, long long *skeys, uint16_t *sidx,
-                                          uint8_t *lrec, int *fill, long long k, uint64_t h, bool &full) {
-    const int mask = D.slots - 1;
-    int pos = (int)(h & (uint64_t)mask);
-    for (int t = 0; t < D.slots; t++) {
-        long long cur = skeys[pos];
-        if (cur == kEmptyKey) {
-            cur = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(skeys + pos), (unsigned long long)kEmptyKey,
-                                       (unsigned long long)k);
-            if (cur == kEmptyKey) {
-                const int e = atomicAdd(fill, 1);
-                if (e >= D.L) {
-                    sidx[pos] = kTableFull;
-                    full = true;
-                } else {
-                    init_record(P, lrec + (size_t)e * smem_stride(P));
-                    sidx[pos] = (uint16_t)e;
-                }
-                return pos;
+        if (acc_f64(C)) {
+            const double v = __longlong_as_double((long long)lo);
+            if (C.flags & F_SUM) {
+                double s, e;
+                two_sum(__longlong_as_double((long long)x.s0), v, s, e);
+                x.s0 = (uint64_t)__double_as_longlong(s);
+                x.s1 = (uint64_t)__double_as_longlong(__dadd_rn(__longlong_as_double((long long)x.s1), e));
+            }
+            if (C.flags & (F_MIN | F_MAX)) {
+                const uint64_t k = f64_order_key(v);
+                acc_min_max(true, x, k, k);
+            }
+            continue;
+        }
+        if (C.flags & F_SUM) {
+            if (acc_i32(C)) {
+                x.s0 += lo;
+            } else {
+                const uint64_t s = x.s0 + lo;
+                x.s1 += hi + (s < x.s0 ? 1ull : 0ull);
+                x.s0 = s;
             }
         }
-        if (cur == k) return pos;
-        pos = (pos + 1) & mask;
+        if (C.flags & (F_MIN | F_MAX)) acc_min_max(false, x, lo, lo);
     }
-    full = true;
-    return -1;
 }
 
-// Merges the local records into the global table: first every key's group
-// id (inserting new keys), and only when all found one, the records.
-__device__ bool flush_local(const AggPlanDev &P, const TableDev &T, const PartDev &D, const long long *skeys,
-                            const uint16_t *sidx, uint8_t *lrec, uint32_t *lgid, int m, int *fail) {
-    for (int sl = threadIdx.x; sl < D.slots; sl += blockDim.x) {
-        const uint16_t e = sidx[sl];
-        if (e >= m) continue;  // free, or claimed without a record
-        uint32_t g = kPending;
-        if (*reinterpret_cast<const unsigned long long *>(lrec + (size_t)e * smem_stride(P) + P.off_rows)) {
-            g = find_or_insert(T, P, skeys[sl]);
-            if (g == kOverflowGid) atomicOr(fail, 1);
+// A team's accumulators summed into its first lane's (teams of `width`
+// lanes, aligned; every lane of the warp takes part).
+__device__ __forceinline__ void acc_team_sum(const AggPlanDev &P, int cb, RowAcc &a, int width) {
+    for (int d = width >> 1; d >= 1; d >>= 1) {
+        a.rows += __shfl_down_sync(kFullMask, a.rows, d, width);
+#pragma unroll
+        for (int u = 0; u < kAccCols; u++) {
+            if (cb + u >= P.ncols) break;
+            ColAcc y;
+            y.cnt = __shfl_down_sync(kFullMask, a.c[u].cnt, d, width);
+            y.s0 = __shfl_down_sync(kFullMask, a.c[u].s0, d, width);
+            y.s1 = __shfl_down_sync(kFullMask, a.c[u].s1, d, width);
+            y.mn = __shfl_down_sync(kFullMask, a.c[u].mn, d, width);
+            y.mx = __shfl_down_sync(kFullMask, a.c[u].mx, d, width);
+            a.c[u].cnt += y.cnt;
+            acc_add(P.c[cb + u], a.c[u], y);
         }
-        lgid[e] = g;
     }
-    __syncthreads();
-    const bool ok = *reinterpret_cast<volatile int *>(fail) == 0;
-    if (ok)
-        for (int e = threadIdx.x; e < m; e += blockDim.x)
-            if (lgid[e] != kPending)
-                merge_record(P, T.states + (size_t)lgid[e] * P.rec, lrec + (size_t)e * smem_stride(P));
-    __syncthreads();
-    return ok;
 }
 
-__global__ void __launch_bounds__(kPartThreads) agg_part_kernel(AggPlanDev P, TableDev T, PartDev D) {
+// The accumulators merged into a global record that nothing else writes
+// meanwhile (Accumulator::merge, accumulator.rs:1159). Every field is read
+// before any is written: the field offsets are runtime values, so loads
+// placed after stores would each wait for the stores before them.
+__device__ __forceinline__ void acc_merge(const AggPlanDev &P, int cb, const RowAcc &a, uint8_t *r) {
+    unsigned long long rows = 0, cnt[kAccCols];
+    ColAcc x[kAccCols];
+    if (cb == 0) rows = *reinterpret_cast<const unsigned long long *>(r + P.off_rows);
+#pragma unroll
+    for (int u = 0; u < kAccCols; u++) {
+        const int c = cb + u;
+        cnt[u] = 0;
+        x[u].cnt = 0;
+        x[u].s0 = x[u].s1 = x[u].mn = x[u].mx = 0;
+        if (c >= P.ncols || !a.c[u].cnt) continue;
+        const AggColDev &C = P.c[c];
+        cnt[u] = *reinterpret_cast<const unsigned long long *>(r + C.off_count);
+        if (C.flags & F_SUM) {
+            x[u].s0 = *reinterpret_cast<const uint64_t *>(r + C.off_sum);
+            if (!acc_i32(C)) x[u].s1 = *reinterpret_cast<const uint64_t *>(r + C.off_sum + 8);
+        }
+        if (acc_i32(C)) {
+            x[u].mn = (uint64_t)(long long)((C.flags & F_MIN) ? *reinterpret_cast<const int *>(r + C.off_min) : INT_MAX);
+            x[u].mx = (uint64_t)(long long)((C.flags & F_MAX) ? *reinterpret_cast<const int *>(r + C.off_max) : INT_MIN);
+        } else {
+            x[u].mn = (C.flags & F_MIN) ? *reinterpret_cast<const uint64_t *>(r + C.off_min) : a.c[u].mn;
+            x[u].mx = (C.flags & F_MAX) ? *reinterpret_cast<const uint64_t *>(r + C.off_max) : a.c[u].mx;
+        }
+    }
+    if (cb == 0) *reinterpret_cast<unsigned long long *>(r + P.off_rows) = rows + a.rows;
+#pragma unroll
+    for (int u = 0; u < kAccCols; u++) {
+        const int c = cb + u;
+        if (c >= P.ncols || !a.c[u].cnt) continue;
+        const AggColDev &C = P.c[c];
+        *reinterpret_cast<unsigned long long *>(r + C.off_count) = cnt[u] + a.c[u].cnt;
+        if (!(C.flags & (F_SUM | F_MIN | F_MAX))) continue;
+        acc_add(C, x[u], a.c[u]);
+        if (C.flags & F_SUM) {
+            *reinterpret_cast<uint64_t *>(r + C.off_sum) = x[u].s0;
+            if (!acc_i32(C)) *reinterpret_cast<uint64_t *>(r + C.off_sum + 8) = x[u].s1;
+        }
+        if (acc_i32(C)) {
+            if (C.flags & F_MIN) *reinterpret_cast<int *>(r + C.off_min) = (int)(long long)x[u].mn;
+            if (C.flags & F_MAX) *reinterpret_cast<int *>(r + C.off_max) = (int)(long long)x[u].mx;
+        } else {
+            if (C.flags & F_MIN) *reinterpret_cast<uint64_t *>(r + C.off_min) = x[u].mn;
+            if (C.flags & F_MAX) *reinterpret_cast<uint64_t *>(r + C.off_max) = x[u].mx;
+        }
+    }
+}
+
+// The accumulators merged into a global record that other warps update at
+// the same time (the segments of one key): global atomics.
+__device__ __forceinline__ void acc_merge_atomic(const AggPlanDev &P, int cb, const RowAcc &a, uint8_t *r) {
+    if (cb == 0) atomicAdd(reinterpret_cast<unsigned long long *>(r + P.off_rows), (unsigned long long)a.rows);
+#pragma unroll
+    for (int u = 0; u < kAccCols; u++) {
+        const int c = cb + u;
+        if (c >= P.ncols || !a.c[u].cnt) continue;
+        const AggColDev &C = P.c[c];
+        const ColAcc &y = a.c[u];
+        atomicAdd(reinterpret_cast<unsigned long long *>(r + C.off_count), (unsigned long long)y.cnt);
+        if (C.flags & F_SUM) {
+            if (acc_f64(C))
+                atomic_add_dd2(reinterpret_cast<double *>(r + C.off_sum), reinterpret_cast<double *>(r + C.off_sum + 8),
+                               __longlong_as_double((long long)y.s0), __longlong_as_double((long long)y.s1));
+            else if (acc_i32(C)) atomicAdd(reinterpret_cast<unsigned long long *>(r + C.off_sum), (unsigned long long)y.s0);
+            else
+                atomic_add_i128(reinterpret_cast<unsigned long long *>(r + C.off_sum),
+                                reinterpret_cast<long long *>(r + C.off_sum + 8), (int64_t)y.s0, (int64_t)y.s1);
+        }
+        if (acc_i32(C)) {
+            if (C.flags & F_MIN) atomicMin(reinterpret_cast<int *>(r + C.off_min), (int)(long long)y.mn);
+            if (C.flags & F_MAX) atomicMax(reinterpret_cast<int *>(r + C.off_max), (int)(long long)y.mx);
+        } else if (acc_f64(C)) {
+            if (C.flags & F_MIN) atomicMin(reinterpret_cast<unsigned long long *>(r + C.off_min), (unsigned long long)y.mn);
+            if (C.flags & F_MAX) atomicMax(reinterpret_cast<unsigned long long *>(r + C.off_max), (unsigned long long)y.mx);
+        } else {
+            if (C.flags & F_MIN) atomicMin(reinterpret_cast<long long *>(r + C.off_min), (long long)y.mn);
+            if (C.flags & F_MAX) atomicMax(reinterpret_cast<long long *>(r + C.off_max), (long long)y.mx);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kPartThreads, 2) agg_part_kernel(AggPlanDev P, TableDev T, PartDev D) {
     extern __shared__ __align__(16) uint8_t smem[];
-    uint8_t *lrec = smem;                                                                   // L records
-    long long *skeys = reinterpret_cast<long long *>(lrec + (size_t)D.L * smem_stride(P));  // slots
-    uint32_t *lgid = reinterpret_cast<uint32_t *>(skeys + D.slots);                         // L
-    uint16_t *sidx = reinterpret_cast<uint16_t *>(lgid + D.L);                              // slots
-    __shared__ int s_fill, s_fail;
+    uint8_t *srows = smem;                                                                       // kChunkRows rows
+    long long *skeys = reinterpret_cast<long long *>(srows + (size_t)kChunkRows * D.row_bytes);  // slots
+    uint32_t *sgid = reinterpret_cast<uint32_t *>(skeys + kChunkSlots);                          // slots
+    uint32_t *scnt = sgid + kChunkSlots;                                                         // slots
+    uint16_t *soff = reinterpret_cast<uint16_t *>(scnt + kChunkSlots);                           // slots
+    uint16_t *slot_of = soff + kChunkSlots;  // per chunk row: its slot
+    uint16_t *rank_of = slot_of + kChunkRows;  // per chunk row: its rank among its slot's rows
+    uint16_t *order = rank_of + kChunkRows;    // chunk rows sorted by slot
+    uint16_t *big = order + kChunkRows;        // warp keys from the front, team keys from the back
+    uint16_t *small = big + kChunkRows;        // one-lane keys
+    __shared__ uint32_t s_warp[kPartThreads / 32];
+    __shared__ int s_seg[kChunkRows / kWarpRows + 1];  // warp keys' first segments (then their count)
+    __shared__ int s_keys, s_nw, s_nt, s_n1, s_fail, s_new;
+    __shared__ unsigned long long s_base;
     __shared__ int16_t s_off[kMaxValueCols];  // row record offsets (read with a varying index)
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    constexpr int kWarps = kPartThreads / 32;
     if (threadIdx.x < kMaxValueCols) s_off[threadIdx.x] = D.off_val[threadIdx.x];
     const int p = D.todo ? D.todo[blockIdx.x] : (int)blockIdx.x;
     const unsigned int *line = D.part_info + (size_t)p * kCntStride;
     const uint32_t cnt = line[0], cap = line[1];
     const uint32_t rows = cnt < cap ? cnt : cap;
     const uint8_t *buf = D.part_buf + *reinterpret_cast<const unsigned long long *>(line + 2) * D.row_bytes;
-    uint32_t window = D.start[p];
-    auto reset = [&]() {
-        for (int s = threadIdx.x; s < D.slots; s += blockDim.x) {
-            skeys[s] = kEmptyKey;
-            sidx[s] = kNoRecord;
+    constexpr int kMask = kChunkSlots - 1;
+    bool fresh = true;  // the local table is empty
+    bool lookup = D.lookup != 0;
+    for (uint32_t c0 = D.start[p]; c0 < rows; c0 += kChunkRows) {
+        const int n = (int)(rows - c0 < (uint32_t)kChunkRows ? rows - c0 : (uint32_t)kChunkRows);
+        // the table: emptied when new, or when its keys passed a quarter of
+        // its slots (a chunk adds at most kChunkRows more); the counts always
+        const bool clear = fresh || s_keys > kChunkSlots / 4;
+        __syncthreads();  // every thread has read s_keys
+        if (clear) {
+            if (!fresh) {
+                // The keys this CTA gave new groups go into the hash table
+                // before the local table forgets them: later chunks look
+                // them up there.
+                for (int s = threadIdx.x; s < kChunkSlots; s += blockDim.x)
+                    if (skeys[s] != kEmptyKey && sgid[s] != kNoGid && sgid[s] >= D.first_new)
+                        table_index_owned(T, skeys[s], sgid[s]);
+                lookup = true;
+                __syncthreads();
+            }
+            for (int s = threadIdx.x; s < kChunkSlots; s += blockDim.x) {
+                skeys[s] = kEmptyKey;
+                sgid[s] = kNoGid;
+            }
+            if (threadIdx.x == 0) s_keys = 0;
+            fresh = false;
         }
+        for (int s = threadIdx.x; s < kChunkSlots; s += blockDim.x) scnt[s] = 0;
         if (threadIdx.x == 0) {
-            s_fill = 0;
+            s_nw = s_nt = s_n1 = 0;
             s_fail = 0;
+            s_new = 0;
+            s_base = ~0ull;
+        }
+        // 1. the chunk's rows into shared memory (16-byte words), then slots and ranks
+        {
+            const uint4 *src = reinterpret_cast<const uint4 *>(buf + (size_t)c0 * D.row_bytes);
+            uint4 *dst = reinterpret_cast<uint4 *>(srows);
+            const int words = n * D.row_bytes / 16;
+            for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
         }
         __syncthreads();
-    };
-    // Merges the window's records; false (the partition stopped, to run again
-    // from `window` on a bigger table) when the global table had no room.
-    auto flush = [&]() -> bool {
-        const int m = s_fill < D.L ? s_fill : D.L;
-        if (flush_local(P, T, D, skeys, sidx, lrec, lgid, m, &s_fail)) return true;
-        if (threadIdx.x == 0) {
-            D.start[p] = window;
-            atomicAdd(D.failed, 1);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const long long k = *reinterpret_cast<const long long *>(srows + (size_t)i * D.row_bytes);
+            int pos = (int)(hash_word((uint64_t)k) & (uint64_t)kMask);
+            for (int t = 0; t < kChunkSlots; t++) {
+                long long cur = skeys[pos];
+                if (cur == kEmptyKey) {
+                    cur = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(skeys + pos),
+                                               (unsigned long long)kEmptyKey, (unsigned long long)k);
+                    if (cur == kEmptyKey) {
+                        atomicAdd(&s_keys, 1);
+                        break;
+                    }
+                }
+                if (cur == k) break;
+                pos = (pos + 1) & kMask;
+            }
+            slot_of[i] = (uint16_t)pos;
+            rank_of[i] = (uint16_t)atomicAdd(&scnt[pos], 1u);
         }
-        return false;
-    };
-    reset();
-    for (uint32_t base = window; base < rows; base += blockDim.x) {
-        const uint32_t i = base + threadIdx.x;
-        const bool live = i < rows;
-        const uint8_t *row = buf + (size_t)i * D.row_bytes;
-        const long long k = live ? *reinterpret_cast<const long long *>(row) : 0;
-        const uint64_t h = hash_word((uint64_t)k);
-        // Slots first, then (after the barrier) the records they name. A tile
-        // that met a full table merges the window's rows (those before the
-        // tile; its own new records are still empty) and runs again on the
-        // emptied table, which holds the tile's at most L keys.
-        bool full = false;
-        int pos = live ? local_slot(P, D, skeys, sidx, lrec, &s_fill, k, h, full) : 0;
-        if (__syncthreads_or(full)) {
-            if (!flush()) return;
-            window = base;
-            reset();
-            full = false;
-            pos = live ? local_slot(P, D, skeys, sidx, lrec, &s_fill, k, h, full) : 0;
-            if (__syncthreads_or(full)) {  // cannot happen: a tile has at most L keys
-                if (threadIdx.x == 0) atomicOr(T.status, ST_TOO_MANY);
-                return;
+        __syncthreads();
+        // 2. exclusive scan of the slot counts, and the used slots listed by size
+        constexpr int kPer = kChunkSlots / kPartThreads;
+        const int s0 = threadIdx.x * kPer;
+        uint32_t mine = 0;
+#pragma unroll
+        for (int j = 0; j < kPer; j++) mine += scnt[s0 + j];
+        uint32_t incl = mine;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFullMask, incl, d);
+            if ((int)lane >= d) incl += y;
+        }
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t w = lane < kWarps ? s_warp[lane] : 0u;
+            uint32_t wi = w;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(kFullMask, wi, d);
+                if ((int)lane >= d) wi += y;
+            }
+            if (lane < kWarps) s_warp[lane] = wi - w;
+        }
+        __syncthreads();
+        uint32_t run = s_warp[warp] + incl - mine;
+#pragma unroll
+        for (int j = 0; j < kPer; j++) {
+            const int s = s0 + j;
+            const uint32_t c = scnt[s];
+            soff[s] = (uint16_t)run;
+            run += c;
+            if (c >= (uint32_t)kWarpRows) big[atomicAdd(&s_nw, 1)] = (uint16_t)s;
+            else if (c >= (uint32_t)kTeamRows) big[kChunkRows - 1 - atomicAdd(&s_nt, 1)] = (uint16_t)s;
+            else if (c) small[atomicAdd(&s_n1, 1)] = (uint16_t)s;
+        }
+        __syncthreads();
+        // 3. the counting sort's scatter, and group ids for keys new to the local table
+        for (int i = threadIdx.x; i < n; i += blockDim.x) order[soff[slot_of[i]] + rank_of[i]] = (uint16_t)i;
+        const int nw = s_nw, nt = s_nt, n1 = s_n1;
+        const int nused = nw + nt + n1;
+        auto used_slot = [&](int u) -> int {
+            if (u < nw) return big[u];
+            u -= nw;
+            if (u < nt) return big[kChunkRows - 1 - u];
+            return small[u - nt];
+        };
+        if (threadIdx.x == 0) {  // the warp keys' segments of kSegRows rows
+            int acc = 0;
+            for (int u = 0; u < nw; u++) {
+                s_seg[u] = acc;
+                acc += ((int)scnt[big[u]] + kSegRows - 1) / kSegRows;
+            }
+            s_seg[nw] = acc;
+        }
+        for (int u = threadIdx.x; u < nused; u += blockDim.x) {  // found, or kNewGid + local index
+            const int s = used_slot(u);
+            if (sgid[s] != kNoGid) continue;
+            const uint32_t g = lookup ? table_find(T, skeys[s]) : kPending;
+            if (g == kOverflowGid) {  // a wait that gave up (reported as ST_TIMEOUT)
+                atomicOr(&s_fail, 1);
+                continue;
+            }
+            sgid[s] = g != kPending ? g : kNewGid | (uint32_t)atomicAdd(&s_new, 1);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && s_new) {  // ids for the new keys, all or none
+            // Checked, then added: CTAs that pass the check together take at
+            // most D.id_room more ids than D.id_limit, which the table holds.
+            if (__ldcg(T.ngroups) + (unsigned long long)s_new > D.id_limit) s_fail = 1;
+            else s_base = atomicAdd(T.ngroups, (unsigned long long)s_new);
+        }
+        if (__syncthreads_or(s_fail)) {
+            if (threadIdx.x == 0) {
+                D.start[p] = c0;
+                atomicAdd(D.failed, 1);
+            }
+            return;
+        }
+        if (s_new) {
+            for (int u = threadIdx.x; u < nused; u += blockDim.x) {
+                const int s = used_slot(u);
+                const uint32_t v = sgid[s];
+                if (v == kNoGid || !(v & kNewGid)) continue;
+                const uint32_t g = (uint32_t)s_base + (v & ~kNewGid);
+                init_record(P, T.states + (size_t)g * P.rec);
+                T.gkeys[g] = skeys[s];
+                sgid[s] = g;
+            }
+            __syncthreads();
+        }
+        // 4. reduce and merge
+        for (int cb = 0; cb < P.ncols || cb == 0; cb += kAccCols) {
+            const int nseg = s_seg[nw];
+            for (int it = warp; it < nseg; it += kWarps) {  // a warp per kSegRows rows of a key
+                int u = 0;
+                while (s_seg[u + 1] <= it) u++;
+                const int s = big[u];
+                const int m = (int)scnt[s];
+                const int j0 = (it - s_seg[u]) * kSegRows, j1 = j0 + kSegRows < m ? j0 + kSegRows : m;
+                RowAcc a;
+                acc_init(P, cb, a);
+                for (int j = j0 + (int)lane; j < j1; j += 32)
+                    acc_row(P, s_off, cb, a, srows + (size_t)order[soff[s] + j] * D.row_bytes);
+                acc_team_sum(P, cb, a, 32);
+                if (lane == 0) {
+                    uint8_t *rec = T.states + (size_t)sgid[s] * P.rec;
+                    if (m > kSegRows) acc_merge_atomic(P, cb, a, rec);
+                    else acc_merge(P, cb, a, rec);
+                }
+            }
+            // team keys from the warp after the warp keys' last one, one-lane
+            // keys from the last warp down: the classes fall on different warps
+            constexpr int kTeams = 32 / kTeamLanes;
+            const int team = (int)(lane / kTeamLanes), tl = (int)(lane % kTeamLanes);
+            const int twarp = (int)((warp + kWarps - (unsigned)(nseg % kWarps)) % kWarps);
+            for (int u0 = twarp * kTeams; u0 < nt; u0 += kWarps * kTeams) {  // a team per key
+                const int u = u0 + team;
+                RowAcc a;
+                acc_init(P, cb, a);
+                int s = -1;
+                if (u < nt) {
+                    s = big[kChunkRows - 1 - u];
+                    const int first = soff[s], m = (int)scnt[s];
+                    for (int j = tl; j < m; j += kTeamLanes)
+                        acc_row(P, s_off, cb, a, srows + (size_t)order[first + j] * D.row_bytes);
+                }
+                acc_team_sum(P, cb, a, kTeamLanes);
+                if (tl == 0 && s >= 0) acc_merge(P, cb, a, T.states + (size_t)sgid[s] * P.rec);
+            }
+            for (int u = (int)(blockDim.x - 1 - threadIdx.x); u < n1; u += blockDim.x) {  // a lane per key
+                const int s = small[u];
+                const int first = soff[s], m = (int)scnt[s];
+                RowAcc a;
+                acc_init(P, cb, a);
+                for (int j = 0; j < m; j++) acc_row(P, s_off, cb, a, srows + (size_t)order[first + j] * D.row_bytes);
+                acc_merge(P, cb, a, T.states + (size_t)sgid[s] * P.rec);
             }
         }
-        if (live) fold_row(P, s_off, lrec + (size_t)sidx[pos] * smem_stride(P), row);
+        __syncthreads();
     }
-    __syncthreads();
-    if (flush() && threadIdx.x == 0) D.start[p] = rows;
+    if (threadIdx.x == 0) D.start[p] = rows;
 }
 
 // Group ids of the hot keys (inserted into the global table), then the NULL
@@ -1487,6 +1837,19 @@ class HashAggregate {
     bool use_partitioned(int64_t n) const;
     void push_partitioned(const DevBatch &b, const KeyIn &key, int64_t n);
     void plan_partitioned(const KeyIn &key, int64_t n);
+    void plan_row_records();
+    // Groups from unindexed_from_ on (when >= 0) have keys and records but no
+    // hash table entry yet (agg_part_kernel appends them); index_pending
+    // inserts them before anything looks keys up or rehashes the table.
+    int64_t unindexed_from_ = -1;
+    void index_pending();
+    // agg_part_kernel's bound on new group ids: the table's limit, less the
+    // ids that the resident CTAs may take past a check they passed together.
+    uint64_t part_id_room(int part_blocks) const { return (uint64_t)part_blocks * rt_->sm_count * kChunkRows; }
+    unsigned long long part_id_limit(int part_blocks) const {
+        const uint64_t room = part_id_room(part_blocks), cap = slots_ / 8 * 7;
+        return cap > room ? std::min<unsigned long long>(limit_, cap - room) : 0ull;
+    }
     bool part_planned_ = false;
     DBuf part_hot_keys_, part_hot_gids_;
     int part_hot_ = 0;
@@ -1494,8 +1857,6 @@ class HashAggregate {
     int64_t part_groups_est_ = 0;
     int part_row_bytes_ = 0;
     int16_t part_off_val_[kMaxValueCols] = {};
-    int part_local_ = 0;      // local records per agg_part_kernel CTA
-    size_t part_smem_ = 0;    // its shared memory
 };
 
 HashAggregate::HashAggregate(Runtime *rt, const krv_agg_spec &spec) : rt_(rt), spec_(spec) {
@@ -1677,14 +2038,7 @@ void HashAggregate::plan(const DevBatch &b) {
     while ((e * 2) * per + 64 <= std::min(rt_->max_smem_optin, 200 * 1024)) e *= 2;
     smem_entries_ = e >= 64 ? e : 0;
     if (smem_entries_ == 0) mode_ = KRV_AGG_MODE_GLOBAL;
-    // The partitioned path's local table: at least one record per thread of
-    // agg_part_kernel, with slots for twice as many keys.
-    {
-        const int L = kPartThreads;
-        const size_t smem = (size_t)L * (smem_stride(P_) + 4) + (size_t)next_pow2((uint64_t)2 * L) * 10;
-        part_local_ = smem <= (size_t)rt_->max_smem_optin - 1024 ? L : 0;
-        part_smem_ = smem;
-    }
+    plan_row_records();
     const uint64_t hint = spec_.expected_groups > 0 ? (uint64_t)spec_.expected_groups : 65536;
     alloc_table(std::max<uint64_t>(1024, next_pow2((uint64_t)(hint * 2))));
     planned_ = true;
@@ -1730,6 +2084,19 @@ void HashAggregate::grow(uint64_t need_groups) {
         okeys.as<long long>(), ogids.as<uint32_t>(), oslots, keys_.as<long long>(), gids_.as<uint32_t>(), slots_ - 1);
     rt_->launches++;
     check_launch("rehash_kernel");
+    index_pending();
+}
+
+void HashAggregate::index_pending() {
+    if (unindexed_from_ < 0) return;
+    const uint64_t from = (uint64_t)unindexed_from_;
+    const uint64_t to = read_scalar<unsigned long long>(rt_, ngroups_.get());
+    unindexed_from_ = -1;
+    if (to <= from) return;
+    index_groups_kernel<<<grid_for(rt_, (int64_t)(to - from), 256, 8), 256, 0, rt_->stream>>>(
+        gkeys_.as<long long>(), from, to, keys_.as<long long>(), gids_.as<uint32_t>(), slots_ - 1);
+    rt_->launches++;
+    check_launch("index_groups_kernel");
 }
 
 void HashAggregate::launch(const DevBatch &b, const KeyIn &key, int64_t n, const uint32_t *rows_idx, uint32_t *ovf,
@@ -1861,12 +2228,13 @@ AggPlanDev slice_plan(const AggPlanDev &P, int64_t row0, const std::vector<int> 
 }  // namespace
 
 bool HashAggregate::use_partitioned(int64_t n) const {
-    return mode_ == KRV_AGG_MODE_SHARED && n >= kPartMinRows && part_local_ > 0;
+    return mode_ == KRV_AGG_MODE_SHARED && n >= kPartMinRows &&
+           part_smem_bytes(part_row_bytes_) + 1024 <= (size_t)rt_->max_smem_optin;
 }
 
-void HashAggregate::plan_partitioned(const KeyIn &key, int64_t n) {
-    part_planned_ = true;
-    // Row records: key, validity word, then the values the accumulators read.
+// Row records of the partitioned path: key, validity word, then the values
+// the accumulators read (4-, then 8-, then 16-byte ones), 16-byte aligned.
+void HashAggregate::plan_row_records() {
     int off = 12;
     for (int c = 0; c < P_.ncols; c++) part_off_val_[c] = 0;
     for (int pass = 0; pass < 3; pass++) {
@@ -1884,6 +2252,10 @@ void HashAggregate::plan_partitioned(const KeyIn &key, int64_t n) {
         }
     }
     part_row_bytes_ = (off + 15) / 16 * 16;
+}
+
+void HashAggregate::plan_partitioned(const KeyIn &key, int64_t n) {
+    part_planned_ = true;
     // The sample: a strided 64K rows of the first large batch.
     const int m = (int)std::min<int64_t>(n, kPartSample);
     const KeySample S = take_sample(rt_, key, n, m);
@@ -1943,11 +2315,11 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
         widths[c] = col.type.width();
     }
     known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());  // the hot keys' groups too
-    const int L = part_local_;
-    // Partitions: each to hold about L/2 distinct keys (at most 2^13 of them:
-    // every split CTA keeps a cursor per partition in shared memory).
+    // Partitions: each to hold about kPartKeys distinct keys (at most 2^13
+    // of them: every split CTA keeps a cursor per partition in shared memory).
+    constexpr int kPartKeys = 256;
     int bits = 5;
-    while (bits < 13 && ((int64_t)1 << bits) * (L / 2) < part_groups_est_) bits++;
+    while (bits < 13 && ((int64_t)1 << bits) * kPartKeys < part_groups_est_) bits++;
     const int nparts = 1 << bits;
     const int H = part_hot_;
     const int hot_slots = H ? (int)next_pow2((uint64_t)2 * H) : 0;
@@ -1956,10 +2328,11 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
     const auto split_kernel = P.ncols <= 4 ? agg_split_kernel<4> : agg_split_kernel<kMaxValueCols>;
     KRV_CUDA(cudaFuncSetAttribute(split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)split_smem));
     KRV_CUDA(cudaFuncSetAttribute(agg_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)count_smem));
-    KRV_CUDA(cudaFuncSetAttribute(agg_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)part_smem_));
+    const size_t part_smem = part_smem_bytes(part_row_bytes_);
+    KRV_CUDA(cudaFuncSetAttribute(agg_part_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)part_smem));
     int split_blocks = 0, part_blocks = 0;
     KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&split_blocks, split_kernel, kSplitThreads, split_smem));
-    KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&part_blocks, agg_part_kernel, kPartThreads, part_smem_));
+    KRV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&part_blocks, agg_part_kernel, kPartThreads, part_smem));
     if (split_blocks < 1 || part_blocks < 1) fail(KRV_INTERNAL, "aggregate: partitioned kernels do not fit an SM");
     const KeyIn key0 = key;
     for (int64_t row0 = 0; row0 < n; row0 += kPartSliceRows) {
@@ -2004,7 +2377,7 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
         // Room in the table for the keys this slice may add (an estimate; a
         // partition that finds none stops and runs again after a grow).
         const int64_t want = known_groups_ + std::min<int64_t>(ns, part_groups_est_) + H + 2;
-        if (want > (int64_t)limit_) grow((uint64_t)want);
+        if (want > (int64_t)part_id_limit(part_blocks)) grow((uint64_t)want + part_id_room(part_blocks));
         TableDev T{keys_.as<long long>(), gids_.as<uint32_t>(), slots_ - 1, states_.as<uint8_t>(), gkeys_.as<long long>(),
                    ngroups_.as<unsigned long long>(), limit_, status_word(rt_)};
         S.part_buf = part_buf.as<uint8_t>();
@@ -2022,9 +2395,13 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
         D.todo = nullptr;
         D.start = start.as<uint32_t>();
         D.failed = reinterpret_cast<int *>(ctl.as<uint8_t>() + 8);
-        D.L = L;
-        D.slots = (int)next_pow2((uint64_t)2 * L);
-        agg_part_kernel<<<nparts, kPartThreads, part_smem_, rt_->stream>>>(P, T, D);
+        D.id_limit = part_id_limit(part_blocks);
+        // Cold keys already in the table (from earlier batches or slices)
+        // are looked up; the first slice's are all new.
+        D.lookup = known_groups_ > (int64_t)kFirstGid + H ? 1 : 0;
+        D.first_new = (unsigned long long)known_groups_;
+        unindexed_from_ = known_groups_;
+        agg_part_kernel<<<nparts, kPartThreads, part_smem, rt_->stream>>>(P, T, D);
         rt_->launches++;
         check_launch("agg_part_kernel");
         DBuf todo;
@@ -2033,7 +2410,6 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
             const uint32_t st = take_status(rt_);
             if (st & ST_TIMEOUT) fail(KRV_TIMEOUT, "aggregate: a wait for a group id gave up");
             if (st & ST_CAPACITY) fail(KRV_INTERNAL, "aggregate: a hot key has no group");
-            if (st & ST_TOO_MANY) fail(KRV_INTERNAL, "aggregate: a partition tile did not fit an emptied table");
             if (st & ST_MISCOUNT) fail(KRV_INTERNAL, "aggregate: the split wrote more rows than were counted");
             known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());
             if (failed == 0) break;
@@ -2047,14 +2423,18 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
             for (int p = 0; p < nparts; p++)
                 if (hs[p] < std::min<uint32_t>(hc[(size_t)p * kCntStride], hc[(size_t)p * kCntStride + 1]))
                     again.push_back(p);
-            grow((uint64_t)known_groups_ + (uint64_t)again.size() * L + 1);
+            grow((uint64_t)known_groups_ + (uint64_t)again.size() * kChunkRows + part_id_room(part_blocks) + 1);
+            unindexed_from_ = known_groups_;  // grow indexed every group so far
             todo = DBuf(rt_, again.size() * 4);
             KRV_CUDA(cudaMemcpyAsync(todo.get(), again.data(), again.size() * 4, cudaMemcpyHostToDevice, rt_->stream));
             KRV_CUDA(cudaMemsetAsync(ctl.as<uint8_t>() + 8, 0, 4, rt_->stream));
             TableDev T2{keys_.as<long long>(), gids_.as<uint32_t>(), slots_ - 1, states_.as<uint8_t>(),
                         gkeys_.as<long long>(), ngroups_.as<unsigned long long>(), limit_, status_word(rt_)};
             D.todo = todo.as<int>();
-            agg_part_kernel<<<(int)again.size(), kPartThreads, part_smem_, rt_->stream>>>(P, T2, D);
+            D.id_limit = part_id_limit(part_blocks);
+            D.lookup = 1;
+            D.first_new = (unsigned long long)known_groups_;
+            agg_part_kernel<<<(int)again.size(), kPartThreads, part_smem, rt_->stream>>>(P, T2, D);
             rt_->launches++;
             check_launch("agg_part_kernel");
             KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // `again` is a stack vector
@@ -2105,6 +2485,7 @@ void HashAggregate::push(const DevBatch &in) {
     }
     const DevCol &kc = b.cols[key_col_];
     KeyIn key{kc.data, kc.valid, kc.valid_off, kc.type.width(), 0};
+    index_pending();
     if (use_partitioned(n)) {
         push_partitioned(b, key, n);
         return;

@@ -435,45 +435,10 @@ class GraceJoin {
         counters_.probe_rows += in.rows;
         std::vector<DevBatch> out;
         int64_t out_rows = 0;
+        // The batches go out as they are, one per call of krv_join_probe: one
+        // batch would cost a copy of them all (and its allocation).
         for (int64_t from = 0; from < in.rows; from += slice_rows()) probe_slice(slice(in, from), out, out_rows);
-        if (out.size() > 1) {
-            DevBatch one = concat(out);
-            out.clear();
-            out.push_back(std::move(one));
-        }
         return out;
-    }
-
-    // The batches `bs` (one shape) as one batch: a device copy per column
-    // and batch, validity bits appended at their row offsets.
-    DevBatch concat(const std::vector<DevBatch> &bs) {
-        DevBatch o;
-        for (const DevBatch &b : bs) o.rows += b.rows;
-        const size_t ncols = bs[0].cols.size();
-        for (size_t c = 0; c < ncols; c++) {
-            const DevCol &m = bs[0].cols[c];
-            bool nullable = false;
-            for (const DevBatch &b : bs) nullable = nullable || b.cols[c].valid;
-            DevCol col = make_col(rt_, m.type, o.rows, nullable || m.nullable, m.name);
-            if (col.hold_valid) KRV_CUDA(cudaMemsetAsync(col.hold_valid->get(), 0, col.hold_valid->bytes(), rt_->stream));
-            const size_t w = (size_t)m.type.width();
-            int64_t at = 0;
-            for (const DevBatch &b : bs) {
-                const DevCol &x = b.cols[c];
-                if (b.rows)
-                    KRV_CUDA(cudaMemcpyAsync(static_cast<uint8_t *>(const_cast<void *>(col.data)) + at * w, x.data,
-                                             (size_t)b.rows * w, cudaMemcpyDeviceToDevice, rt_->stream));
-                if (col.hold_valid && b.rows) {
-                    uint8_t *dst = col.hold_valid->as<uint8_t>();
-                    if (x.valid) append_bits(rt_, x.valid, x.valid_off, b.rows, dst, at);
-                    else set_bits(rt_, dst, at, b.rows);
-                }
-                at += b.rows;
-            }
-            if (!col.hold_valid) col.valid = nullptr;
-            o.cols.push_back(col);
-        }
-        return o;
     }
 
     // One slice: NULL-key rows padded now (left outer); rows of resident
