@@ -451,6 +451,29 @@ krv_status krv_star_reset(krv_star *s);
 krv_status krv_star_counters_get(const krv_star *s, krv_star_counters *out);
 void krv_star_destroy(krv_star *s);
 
+/* The fused plan recognised in an operator chain: fact batch -> join_a ->
+ * join_b -> grouped SUM(price * (1 - discount)), as HashJoinNode twice and a
+ * HashAggregate would run it (join/mod.rs:1188-1211; runtime filters applied
+ * to the fact scan, operators/runtime_filter.rs:1-45). join_a is probed by
+ * the fact batch; join_b by join_a's output (probe columns, then build
+ * columns, as the join specs project them). Both joins are inner, on one
+ * int64 key, unpartitioned, without residual filter, with their build sides
+ * finished: those rows, after whatever predicate the caller applied before
+ * building, are the dimensions. The chain names, in join_b's output, the
+ * int32 build column grouped by and the fact's price (int64) and discount
+ * (float64) columns; the runtime filters apply when both joins publish one.
+ * The dimensions' rows are copied at the call: the joins may go afterwards.
+ * KRV_UNSUPPORTED when the chain is not of this shape (the caller runs the
+ * operators one by one). Then krv_star_probe(_device), _result, _destroy. */
+typedef struct {
+    int32_t n_fact_columns;          /* columns of the fact batch */
+    int32_t group_col;               /* column of join_b's output: a build column of either join */
+    int32_t price_col, discount_col; /* columns of join_b's output: fact columns */
+    int32_t mode;                    /* KRV_STAR_FUSED or KRV_STAR_PLAIN */
+} krv_star_chain;
+krv_status krv_star_from_joins(krv_runtime *rt, const krv_join *join_a, const krv_join *join_b,
+                               const krv_star_chain *chain, krv_star **out);
+
 /* ---- synthetic data on the device (benchmarks) ----------------------------
  * Counter-based SplitMix64 generators: value(seed, column, row) is the same
  * function on every device and in the CPU test oracle. */

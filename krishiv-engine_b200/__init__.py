@@ -173,6 +173,11 @@ class StarSpec(C.Structure):
                                          "mode")]
 
 
+class StarChain(C.Structure):
+    _fields_ = [("n_fact_columns", C.c_int32), ("group_col", C.c_int32), ("price_col", C.c_int32),
+                ("discount_col", C.c_int32), ("mode", C.c_int32)]
+
+
 class StarCounters(C.Structure):
     _fields_ = [("fact_rows", C.c_int64), ("passed_filters", C.c_int64), ("joined_rows", C.c_int64),
                 ("dim_a_keys", C.c_int64), ("dim_b_keys", C.c_int64), ("filter_a_form", C.c_int32),
@@ -257,6 +262,8 @@ _SIGS = {
     "krv_key_filter_destroy": (None, [C.c_void_p]),
     "krv_star_spec_init": (None, [C.POINTER(StarSpec)]),
     "krv_star_create": (C.c_int32, [C.c_void_p, C.POINTER(StarSpec), C.POINTER(C.c_void_p)]),
+    "krv_star_from_joins": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(StarChain),
+                                        C.POINTER(C.c_void_p)]),
     "krv_star_build": (C.c_int32, [C.c_void_p, C.POINTER(ArrowArray), C.POINTER(ArrowSchema),
                                    C.POINTER(ArrowArray), C.POINTER(ArrowSchema)]),
     "krv_star_build_device": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema),
@@ -856,11 +863,26 @@ def star_spec(pred_a: int, pred_b: int, group_by: int = 0, use_filters: bool = T
 class StarPipeline:
     """Star join with runtime filters and a grouped sum (krv_star_*)."""
 
-    def __init__(self, rt: Runtime, spec: StarSpec):
+    def __init__(self, rt: Runtime, spec: StarSpec = None, _handle=None):
         self.rt = rt
+        if _handle is not None:
+            self.h = _handle
+            return
         h = C.c_void_p()
         check(lib().krv_star_create(rt.h, C.byref(spec), C.byref(h)))
         self.h = h
+
+    @classmethod
+    def from_joins(cls, rt: Runtime, join_a: "HashJoin", join_b: "HashJoin", n_fact_columns: int, group_col: int,
+                   price_col: int, discount_col: int, mode: int = STAR_FUSED) -> "StarPipeline":
+        """The fused plan of the operator chain fact -> join_a -> join_b ->
+        SUM(price * (1 - discount)) GROUP BY group_col (columns of join_b's
+        output), from the joins' finished build sides (krv_star_from_joins).
+        Raises KrvError(KRV_UNSUPPORTED) when the chain is not of that shape."""
+        chain = StarChain(n_fact_columns, group_col, price_col, discount_col, mode)
+        h = C.c_void_p()
+        check(lib().krv_star_from_joins(rt.h, join_a.h, join_b.h, C.byref(chain), C.byref(h)))
+        return cls(rt, _handle=h)
 
     def build(self, dim_a, dim_b):
         with HostBatch(dim_a) as a, HostBatch(dim_b) as b:

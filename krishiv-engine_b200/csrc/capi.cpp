@@ -585,6 +585,24 @@ krv_status krv_star_create(krv_runtime *rt, const krv_star_spec *spec, krv_star 
         return KRV_OK;
     });
 }
+krv_status krv_star_from_joins(krv_runtime *rt, const krv_join *join_a, const krv_join *join_b,
+                               const krv_star_chain *chain, krv_star **out) {
+    return guard([&] {
+        need(rt, "runtime");
+        need(join_a, "join_a");
+        need(join_b, "join_b");
+        need(chain, "chain");
+        need(out, "out");
+        *out = nullptr;
+        if (join_a->g || join_b->g) krv::fail(KRV_UNSUPPORTED, "star chain: partitioned joins are not fused");
+        krv::DeviceGuard g(&rt->rt);
+        auto h = std::make_unique<krv_star>();
+        h->owner = rt;
+        h->s = krv::make_star_from_joins(&rt->rt, *join_a->j, *join_b->j, *chain);
+        *out = h.release();
+        return KRV_OK;
+    });
+}
 krv_status krv_star_build(krv_star *s, const ArrowArray *a, const ArrowSchema *sa, const ArrowArray *b,
                           const ArrowSchema *sb) {
     return guard([&] {

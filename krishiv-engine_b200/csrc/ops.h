@@ -138,6 +138,8 @@ class HashJoin {
     std::shared_ptr<KeyFilterImpl> key_filter() const { return filter_; }
     krv_join_counters counters() const { return counters_; }
     const krv_join_spec &spec() const { return spec_; }
+    bool built() const { return built_; }
+    bool has_residual() const { return residual_set_; }
     // Takes the probe key columns and the output projection of `s` (a plan
     // that probes one built table with batches of another shape).
     void set_probe_shape(const krv_join_spec &s) {
@@ -272,6 +274,7 @@ void agg_destroy(HashAggregate *a);
 // ---- star pipeline -------------------------------------------------------------
 class StarPipeline;
 StarPipeline *make_star(Runtime *rt, const krv_star_spec &spec);
+StarPipeline *make_star_from_joins(Runtime *rt, const HashJoin &ja, const HashJoin &jb, const krv_star_chain &c);
 void star_build(StarPipeline *s, const DevBatch &a, const DevBatch &b);
 void star_probe(StarPipeline *s, const DevBatch &fact);
 DevBatch star_result(StarPipeline *s);

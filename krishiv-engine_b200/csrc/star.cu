@@ -22,6 +22,7 @@
 // 1.0 - discount and one product, each rounded (no fused multiply-add).
 #include <algorithm>
 #include <climits>
+#include <functional>
 #include <memory>
 
 #include "krv_device.cuh"
@@ -39,11 +40,12 @@ constexpr long long kAttrEmpty = (long long)0x8080808080808080ULL;
 // (the filter below the join build). Each warp takes 16 x 32 rows of the
 // block's tile, reading pred once per row (one ballot per 32 rows); the
 // block reserves its tile's output with one atomic, so the shared counter
-// sees one update per 16K rows; the survivors are written in row order.
+// sees one update per 4K rows; the survivors are written in row order.
 // `range` (when given) gets the selected keys' min and max, `arange` the
-// selected attributes' (one update per block each).
+// selected attributes' (one update per block each). Without `pred` every row
+// is selected; without `attr` the attribute written is 0.
 constexpr int kSelectSteps = 16;
-constexpr int kSelectThreads = 1024;
+constexpr int kSelectThreads = 256;
 constexpr int kSelectTile = kSelectThreads * kSelectSteps;
 __global__ void __launch_bounds__(kSelectThreads) dim_select_kernel(const long long *key, const int32_t *pred,
                                                                     const int32_t *attr, int64_t n, int32_t value,
@@ -62,7 +64,7 @@ __global__ void __launch_bounds__(kSelectThreads) dim_select_kernel(const long l
 #pragma unroll
         for (int s = 0; s < kSelectSteps; s++) {
             const int64_t i = c0 + s * 32 + lane;
-            ballots[s] = __ballot_sync(0xFFFFFFFFu, i < n && pred[i] == value);
+            ballots[s] = __ballot_sync(0xFFFFFFFFu, i < n && (!pred || pred[i] == value));
             total += __popc(ballots[s]);
         }
         if (lane == 0) s_tot[warp] = total;
@@ -76,23 +78,41 @@ __global__ void __launch_bounds__(kSelectThreads) dim_select_kernel(const long l
             }
             s_base = acc ? atomicAdd(count, (unsigned long long)acc) : 0ull;
         }
+        // The selected rows' keys and attributes, all loads issued before
+        // any store (a load placed after a store to the output would wait
+        // for it: the compiler cannot tell the arrays apart).
+        // Half the steps at a time, to stay within the registers.
+        constexpr int kHalf = kSelectSteps / 2;
         __syncthreads();
         unsigned long long base = s_base + s_tot[warp];
 #pragma unroll
-        for (int s = 0; s < kSelectSteps; s++) {
-            if ((ballots[s] >> lane) & 1u) {
+        for (int h = 0; h < 2; h++) {
+            long long ks[kHalf];
+            int32_t as[kHalf];
+#pragma unroll
+            for (int q = 0; q < kHalf; q++) {
+                const int s = h * kHalf + q;
                 const int64_t i = c0 + s * 32 + lane;
-                const unsigned long long pos = base + __popc(ballots[s] & lanemask_lt());
-                const long long k = key[i];
-                const int32_t a = attr[i];
-                okey[pos] = k;
-                oattr[pos] = a;
-                lo = k < lo ? k : lo;
-                hi = k > hi ? k : hi;
-                alo = a < alo ? a : alo;
-                ahi = a > ahi ? a : ahi;
+                const bool mine = (ballots[s] >> lane) & 1u;
+                ks[q] = mine ? key[i] : 0;
+                as[q] = mine && attr ? attr[i] : 0;
             }
-            base += __popc(ballots[s]);
+#pragma unroll
+            for (int q = 0; q < kHalf; q++) {
+                const int s = h * kHalf + q;
+                if ((ballots[s] >> lane) & 1u) {
+                    const unsigned long long pos = base + __popc(ballots[s] & lanemask_lt());
+                    const long long k = ks[q];
+                    const int32_t a = as[q];
+                    okey[pos] = k;
+                    oattr[pos] = a;
+                    lo = k < lo ? k : lo;
+                    hi = k > hi ? k : hi;
+                    alo = a < alo ? a : alo;
+                    ahi = a > ahi ? a : ahi;
+                }
+                base += __popc(ballots[s]);
+            }
         }
         __syncthreads();  // s_tot is rewritten by the next tile
     }
@@ -221,8 +241,8 @@ __device__ __forceinline__ int32_t attr_gid_of(long long k, long long *tkeys, in
 // fewer than kDirectAttrSpan values, else the attribute table's id. Two rows
 // with one key set the dimension's duplicate flag.
 __global__ void dim_index_fast_kernel(const long long *key, const int32_t *attr, long long *ctl, int d,
-                                      unsigned short *direct, long long *tkeys, int32_t *tgid, uint64_t mask,
-                                      int32_t *gattr) {
+                                      int grouping, unsigned short *direct, long long *tkeys, int32_t *tgid,
+                                      uint64_t mask, int32_t *gattr) {
     const unsigned long long n = (unsigned long long)ctl[d];
     const long long lo = ctl[2 + 2 * d], hi = ctl[3 + 2 * d];
     if (lo > hi || (unsigned long long)(hi - lo) >= kMaxDirectSpan) return;
@@ -234,7 +254,8 @@ __global__ void dim_index_fast_kernel(const long long *key, const int32_t *attr,
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
          i += (unsigned long long)gridDim.x * blockDim.x) {
         const long long a = attr[i];
-        const int32_t g = own ? (int32_t)(a - alo) : attr_gid_of(a, tkeys, tgid, mask, gattr, ngroups, status);
+        // the other dimension's entries only mark its keys present
+        const int32_t g = !grouping ? 0 : own ? (int32_t)(a - alo) : attr_gid_of(a, tkeys, tgid, mask, gattr, ngroups, status);
         const unsigned long long off = (unsigned long long)(key[i] - lo);
         const unsigned short old = atomicCAS(direct + off, (unsigned short)0xFFFFu, (unsigned short)g);
         if (old != (unsigned short)0xFFFFu) atomicOr(dup, 1u);
@@ -347,6 +368,7 @@ class StarPipeline {
     StarPipeline(Runtime *rt, const krv_star_spec &s) : rt_(rt), spec_(s) {
         if (s.group_by != 0 && s.group_by != 1) fail(KRV_INVALID_ARGUMENT, "group_by is 0 (dim a) or 1 (dim b)");
         if (s.mode != KRV_STAR_FUSED && s.mode != KRV_STAR_PLAIN) fail(KRV_INVALID_ARGUMENT, "unknown star mode");
+        for (int d = 0; d < 2; d++) set_dim_cols(d, s.dim_key, s.dim_pred, s.dim_attr);
     }
 
     struct Dim {
@@ -355,16 +377,31 @@ class StarPipeline {
         int64_t rows = 0;
     };
 
-    void check_dim(const DevBatch &d) const {
-        const int c_key = spec_.dim_key, c_pred = spec_.dim_pred, c_attr = spec_.dim_attr;
-        const int nc = (int)d.cols.size();
-        if (c_key < 0 || c_key >= nc || c_pred < 0 || c_pred >= nc || c_attr < 0 || c_attr >= nc)
+    // Dimension d's columns: key, predicate (-1: every row qualifies, the
+    // rows being those of a join's finished build side) and attribute (-1 on
+    // the dimension not grouped by).
+    void set_dim_cols(int d, int key, int pred, int attr) {
+        dkey_[d] = key;
+        dpred_[d] = pred;
+        dattr_[d] = attr;
+    }
+    void check_dim(const DevBatch &b, int d) const {
+        const int c_key = dkey_[d], c_pred = dpred_[d], c_attr = dattr_[d];
+        const int nc = (int)b.cols.size();
+        if (c_key < 0 || c_key >= nc || c_pred < -1 || c_pred >= nc || c_attr < -1 || c_attr >= nc ||
+            (c_attr < 0 && d == spec_.group_by))
             fail(KRV_INVALID_ARGUMENT, "dimension column out of range");
-        if (d.cols[c_key].type.id != Type::I64 || d.cols[c_pred].type.id != Type::I32 ||
-            d.cols[c_attr].type.id != Type::I32)
+        if (b.cols[c_key].type.id != Type::I64 || (c_pred >= 0 && b.cols[c_pred].type.id != Type::I32) ||
+            (c_attr >= 0 && b.cols[c_attr].type.id != Type::I32))
             fail(KRV_UNSUPPORTED, "star dimension columns are (int64 key, int32 pred, int32 attr)");
-        if (d.cols[c_key].valid || d.cols[c_pred].valid || d.cols[c_attr].valid)
+        if (b.cols[c_key].valid || (c_pred >= 0 && b.cols[c_pred].valid) || (c_attr >= 0 && b.cols[c_attr].valid))
             fail(KRV_UNSUPPORTED, "star dimension columns without NULLs");
+    }
+    const int32_t *dim_pred(const DevBatch &b, int d) const {
+        return dpred_[d] >= 0 ? static_cast<const int32_t *>(b.cols[dpred_[d]].data) : nullptr;
+    }
+    const int32_t *dim_attr(const DevBatch &b, int d) const {
+        return dattr_[d] >= 0 ? static_cast<const int32_t *>(b.cols[dattr_[d]].data) : nullptr;
     }
 
     // The fused plan's build when both dimensions have unique keys over spans
@@ -375,7 +412,7 @@ class StarPipeline {
     // range. False (nothing kept) when a dimension does not qualify: the
     // join-table build runs.
     int select_grid(int64_t n) const {
-        return (int)std::max<int64_t>(1, std::min<int64_t>(2 * rt_->sm_count, ceil_div(n, kSelectTile)));
+        return (int)std::max<int64_t>(1, std::min<int64_t>(8 * rt_->sm_count, ceil_div(n, kSelectTile)));
     }
     bool build_fast(const DevBatch *dims[2], const int32_t values[2]) {
         struct Sel {
@@ -394,11 +431,10 @@ class StarPipeline {
             sel[d].attr = DBuf(rt_, (size_t)std::max<int64_t>(n, 1) * 4);
             if (n > 0) {
                 dim_select_kernel<<<select_grid(n), kSelectThreads, 0, rt_->stream>>>(
-                    static_cast<const long long *>(b.cols[spec_.dim_key].data),
-                    static_cast<const int32_t *>(b.cols[spec_.dim_pred].data),
-                    static_cast<const int32_t *>(b.cols[spec_.dim_attr].data), n, values[d], sel[d].key.as<long long>(),
+                    static_cast<const long long *>(b.cols[dkey_[d]].data), dim_pred(b, d), dim_attr(b, d), n,
+                    values[d], sel[d].key.as<long long>(),
                     sel[d].attr.as<int32_t>(), ctl.as<unsigned long long>() + d, ctl.as<long long>() + 2 + 2 * d,
-                    ctl.as<long long>() + 6);
+                    d == spec_.group_by ? ctl.as<long long>() + 6 : nullptr);
                 rt_->launches++;
                 check_launch("dim_select_kernel");
             }
@@ -415,7 +451,8 @@ class StarPipeline {
             if (n <= 0) continue;
             dim_index_fast_kernel<<<grid_for(rt_, std::max<int64_t>(1, n / 16), 256, 8), 256, 0, rt_->stream>>>(
                 sel[d].key.as<long long>(), sel[d].attr.as<int32_t>(), ctl.as<long long>(), d,
-                direct_full_[d].as<unsigned short>(), gkeys_.as<long long>(), gtab_.as<int32_t>(), gmask_,
+                d == spec_.group_by ? 1 : 0, direct_full_[d].as<unsigned short>(), gkeys_.as<long long>(),
+                gtab_.as<int32_t>(), gmask_,
                 gattr_.as<int32_t>());
             rt_->launches++;
             check_launch("dim_index_fast_kernel");
@@ -468,9 +505,8 @@ class StarPipeline {
         return true;
     }
 
-    void build_dim(const DevBatch &d, int32_t value, Dim &out) {
-        check_dim(d);
-        const int c_key = spec_.dim_key, c_pred = spec_.dim_pred, c_attr = spec_.dim_attr;
+    void build_dim(const DevBatch &d, int di, int32_t value, Dim &out) {
+        check_dim(d, di);
         const int64_t n = d.rows;
         out.key = DBuf(rt_, (size_t)std::max<int64_t>(n, 1) * 8);
         out.attr = DBuf(rt_, (size_t)std::max<int64_t>(n, 1) * 4);
@@ -478,16 +514,17 @@ class StarPipeline {
         KRV_CUDA(cudaMemsetAsync(cnt.get(), 0, 8, rt_->stream));
         if (n > 0) {
             dim_select_kernel<<<select_grid(n), kSelectThreads, 0, rt_->stream>>>(
-                static_cast<const long long *>(d.cols[c_key].data), static_cast<const int32_t *>(d.cols[c_pred].data),
-                static_cast<const int32_t *>(d.cols[c_attr].data), n, value, out.key.as<long long>(),
-                out.attr.as<int32_t>(), cnt.as<unsigned long long>(), nullptr, nullptr);
+                static_cast<const long long *>(d.cols[dkey_[di]].data), dim_pred(d, di), dim_attr(d, di), n, value,
+                out.key.as<long long>(), out.attr.as<int32_t>(), cnt.as<unsigned long long>(), nullptr, nullptr);
             rt_->launches++;
             check_launch("dim_select_kernel");
         }
         out.rows = (int64_t)read_scalar<unsigned long long>(rt_, cnt.get());
-        // Dense group ids of the attribute (shared by both dimensions).
+        // Dense group ids of the grouping dimension's attribute (the other's
+        // are never read: zeros).
         out.gid = DBuf(rt_, (size_t)std::max<int64_t>(out.rows, 1) * 4);
-        if (out.rows > 0) {
+        if (di != spec_.group_by) KRV_CUDA(cudaMemsetAsync(out.gid.get(), 0, out.gid.bytes(), rt_->stream));
+        if (out.rows > 0 && di == spec_.group_by) {
             attr_gid_kernel<<<grid_for(rt_, out.rows, 256, 8), 256, 0, rt_->stream>>>(
                 out.attr.as<int32_t>(), out.rows, gkeys_.as<long long>(), gtab_.as<int32_t>(), gmask_, out.gid.as<int32_t>(),
                 gattr_.as<int32_t>(), ngroups_.as<unsigned int>(), status_word(rt_));
@@ -541,8 +578,8 @@ class StarPipeline {
             direct_[d] = StarDirect{nullptr, 0, 0, 0};
             direct_buf_[d].reset();
         }
-        check_dim(a);
-        check_dim(b);
+        check_dim(a, 0);
+        check_dim(b, 1);
         const DevBatch *dims[2] = {&a, &b};
         const int32_t values[2] = {spec_.pred_a, spec_.pred_b};
         const bool fast = spec_.mode == KRV_STAR_FUSED && build_fast(dims, values);
@@ -554,8 +591,8 @@ class StarPipeline {
             clear_status(rt_);
             // Only the grouping dimension's attribute names groups; the other's
             // ids are never read.
-            build_dim(a, spec_.pred_a, dims_[0]);
-            build_dim(b, spec_.pred_b, dims_[1]);
+            build_dim(a, 0, spec_.pred_a, dims_[0]);
+            build_dim(b, 1, spec_.pred_b, dims_[1]);
             if (take_status(rt_) & ST_TIMEOUT) fail(KRV_TIMEOUT, "star build: a wait for a group id gave up");
             ngroups_host_ = (int)read_scalar<unsigned int>(rt_, ngroups_.get());
             if (ngroups_host_ > (int)gmask_ / 2) fail(KRV_UNSUPPORTED, "more than 32768 distinct attribute values");
@@ -1060,6 +1097,7 @@ class StarPipeline {
     DBuf gkeys_, gtab_, gattr_, ngroups_;
     uint32_t gmask_ = 0;
     int ngroups_host_ = 0;
+    int dkey_[2] = {0, 0}, dpred_[2] = {1, 1}, dattr_[2] = {2, 2};  // each dimension's columns
     DBuf sum_hi_, sum_lo_, cnt_, nulls_, stats_;
     DBuf bits_[2];               // filter answer bitmaps of dimensions a and b
     DBuf direct_buf_[2];         // direct key -> group id indexes
@@ -1096,6 +1134,71 @@ class StarPipeline {
 };
 
 StarPipeline *make_star(Runtime *rt, const krv_star_spec &spec) { return new StarPipeline(rt, spec); }
+
+// ---- the star plan from an operator chain ---------------------------------------
+namespace {
+// Where a column of a join's output comes from: the fact batch, or a build
+// column of join a (side 1) or b (side 2).
+struct ColFrom {
+    int side, col;
+};
+// The columns of one join's output: its probe projection, then its build
+// projection (join/mod.rs output order; a negative count takes them all).
+ColFrom out_col(const krv_join_spec &s, int j, int n_probe_in, int n_build, int build_side,
+                const std::function<ColFrom(int)> &probe_from) {
+    const int np = s.n_probe_out < 0 ? n_probe_in : s.n_probe_out;
+    const int nb = s.n_build_out < 0 ? n_build : s.n_build_out;
+    if (j < 0 || j >= np + nb) fail(KRV_INVALID_ARGUMENT, "star chain: column out of range");
+    if (j < np) return probe_from(s.n_probe_out < 0 ? j : s.probe_out[j]);
+    const int b = s.n_build_out < 0 ? j - np : s.build_out[j - np];
+    return ColFrom{build_side, b};
+}
+// A finished join's build rows as a star dimension: its columns, validity
+// dropped where the column holds no NULL.
+DevBatch dim_view(const HashJoin &J) {
+    DevBatch d = J.arena();
+    for (DevCol &c : d.cols)
+        if (!c.nullable) c.valid = nullptr;
+    return d;
+}
+}  // namespace
+
+StarPipeline *make_star_from_joins(Runtime *rt, const HashJoin &ja, const HashJoin &jb, const krv_star_chain &c) {
+    const HashJoin *J[2] = {&ja, &jb};
+    for (const HashJoin *j : J) {
+        const krv_join_spec &s = j->spec();
+        if (s.join_type != KRV_JOIN_INNER || s.n_keys != 1 || s.null_safe[0] || j->has_residual())
+            fail(KRV_UNSUPPORTED, "star chain: joins are inner, on one `=` key, without residual filter");
+        if (!j->built()) fail(KRV_INVALID_ARGUMENT, "star chain: a join's build side is not finished");
+        if (j->arena().cols.empty()) fail(KRV_UNSUPPORTED, "star chain: a join without build columns");
+    }
+    const krv_join_spec &sa = ja.spec(), &sb = jb.spec();
+    const int nba = (int)ja.arena().cols.size(), nbb = (int)jb.arena().cols.size();
+    const int npa = sa.n_probe_out < 0 ? c.n_fact_columns : sa.n_probe_out;
+    const int nout_a = npa + (sa.n_build_out < 0 ? nba : sa.n_build_out);
+    auto from_fact = [](int j) { return ColFrom{0, j}; };
+    auto from_a = [&](int j) { return out_col(sa, j, c.n_fact_columns, nba, 1, from_fact); };
+    auto from_b = [&](int j) { return out_col(sb, j, nout_a, nbb, 2, from_a); };
+    const ColFrom fk_b = from_a(sb.probe_keys[0]);
+    const ColFrom grp = from_b(c.group_col), price = from_b(c.price_col), disc = from_b(c.discount_col);
+    if (fk_b.side != 0 || price.side != 0 || disc.side != 0)
+        fail(KRV_UNSUPPORTED, "star chain: join_b's key, price and discount are fact columns");
+    if (grp.side == 0) fail(KRV_UNSUPPORTED, "star chain: the grouped column is a dimension's");
+    krv_star_spec spec;
+    krv_star_spec_init(&spec);
+    spec.fact_fk_a = sa.probe_keys[0];
+    spec.fact_fk_b = fk_b.col;
+    spec.fact_price = price.col;
+    spec.fact_discount = disc.col;
+    spec.group_by = grp.side - 1;
+    spec.use_filters = sa.runtime_filter && sb.runtime_filter ? 1 : 0;
+    spec.mode = c.mode;
+    std::unique_ptr<StarPipeline> sp(new StarPipeline(rt, spec));
+    for (int d = 0; d < 2; d++)
+        sp->set_dim_cols(d, J[d]->spec().build_keys[0], -1, d == spec.group_by ? grp.col : -1);
+    sp->build(dim_view(ja), dim_view(jb));
+    return sp.release();
+}
 void star_build(StarPipeline *s, const DevBatch &a, const DevBatch &b) { s->build(a, b); }
 void star_probe(StarPipeline *s, const DevBatch &fact) { s->probe(fact); }
 DevBatch star_result(StarPipeline *s) { return s->result(); }
