@@ -528,7 +528,9 @@ struct SplitDev {
     const long long *hot_keys;  // H distinct keys, none equal to kEmptyKey
     const uint32_t *hot_gids;   // H + 2 global group ids (then the NULL and marker groups)
     int H;
-    int hot_slots;  // power of two >= 2H (0 when H == 0)
+    int hot_slots;  // the hot table: hot_slots / kHotWays buckets (a power of two; 0 when H == 0)
+    const long long *hot_tab;   // its keys (kEmptyKey: free), bucket by bucket
+    const int16_t *hot_tab_idx; // their indexes in hot_keys
     int part_bits;  // >= 1
     int row_bytes;
     int16_t off_val[kMaxValueCols];
@@ -754,25 +756,21 @@ __device__ __forceinline__ void cold_rows(const AggPlanDev &P, const SplitDev &S
     }
 }
 
-// The hot-key lookup table of a CTA (keys and their indexes in hot_keys).
+// The hot-key table: kHotWays keys per bucket, every key in one of its two
+// buckets (hot_buckets), placed on the host (a key that fits neither is left
+// cold). A lookup reads both buckets whole: no probe loop, so the lanes of a
+// warp do not diverge on it.
+constexpr int kHotWays = 4;
+__host__ __device__ __forceinline__ void hot_buckets(uint64_t h, int nbuckets, int &b1, int &b2) {
+    b1 = (int)(h & (uint64_t)(nbuckets - 1));
+    b2 = (int)((h >> 32) & (uint64_t)(nbuckets - 1));
+    if (b2 == b1) b2 = b1 ^ 1;
+}
+// The CTA's copy of the table in shared memory (the indexes when hidx).
 __device__ __forceinline__ void hot_table_init(const SplitDev &S, long long *hkeys, int16_t *hidx) {
     for (int e = threadIdx.x; e < S.hot_slots; e += blockDim.x) {
-        hkeys[e] = kEmptyKey;
-        if (hidx) hidx[e] = -1;
-    }
-    __syncthreads();
-    const int hmask = S.hot_slots - 1;
-    for (int j = threadIdx.x; j < S.H; j += blockDim.x) {
-        const long long k = S.hot_keys[j];
-        int pos = (int)(hash_word((uint64_t)k) & (uint64_t)hmask);
-        for (int t = 0; t < S.hot_slots; t++) {
-            if ((long long)atomicCAS(reinterpret_cast<unsigned long long *>(hkeys + pos), (unsigned long long)kEmptyKey,
-                                     (unsigned long long)k) == kEmptyKey) {
-                if (hidx) hidx[pos] = (int16_t)j;
-                break;
-            }
-            pos = (pos + 1) & hmask;
-        }
+        hkeys[e] = S.hot_tab[e];
+        if (hidx) hidx[e] = S.hot_tab_idx[e];
     }
     __syncthreads();
 }
@@ -781,15 +779,21 @@ __device__ __forceinline__ void hot_table_init(const SplitDev &S, long long *hke
 __device__ __forceinline__ int hot_index(const SplitDev &S, const long long *hkeys, const int16_t *hidx, long long k,
                                          uint64_t h) {
     if (!S.H) return -1;
-    const int hmask = S.hot_slots - 1;
-    int pos = (int)(h & (uint64_t)hmask);
-    for (int t = 0; t < S.hot_slots; t++) {
-        const long long c = hkeys[pos];
-        if (c == k) return hidx ? hidx[pos] : 0;
-        if (c == kEmptyKey) return -1;
-        pos = (pos + 1) & hmask;
-    }
-    return -1;
+    int b1, b2;
+    hot_buckets(h, S.hot_slots / kHotWays, b1, b2);
+    const longlong2 *t = reinterpret_cast<const longlong2 *>(hkeys);
+    const longlong2 x0 = t[2 * b1], x1 = t[2 * b1 + 1], y0 = t[2 * b2], y1 = t[2 * b2 + 1];
+    int slot = -1;
+    slot = x0.x == k ? 4 * b1 : slot;
+    slot = x0.y == k ? 4 * b1 + 1 : slot;
+    slot = x1.x == k ? 4 * b1 + 2 : slot;
+    slot = x1.y == k ? 4 * b1 + 3 : slot;
+    slot = y0.x == k ? 4 * b2 : slot;
+    slot = y0.y == k ? 4 * b2 + 1 : slot;
+    slot = y1.x == k ? 4 * b2 + 2 : slot;
+    slot = y1.y == k ? 4 * b2 + 3 : slot;
+    if (slot < 0) return -1;
+    return hidx ? hidx[slot] : 0;
 }
 // A row's place in the split: hot index (>= 0, then H for the NULL key and
 // H + 1 for the marker key), -1 for a cold row (partition from h), -2 past
@@ -809,7 +813,7 @@ __global__ void __launch_bounds__(kSplitThreads, 2) agg_split_kernel(AggPlanDev 
     const int NH = S.H + 2;
     const int nparts = 1 << S.part_bits;
     uint8_t *hrec = smem;                                                                  // NH records
-    long long *hkeys = reinterpret_cast<long long *>(hrec + (size_t)NH * smem_stride(P));  // hot_slots
+    long long *hkeys = reinterpret_cast<long long *>(hrec + ((size_t)NH * smem_stride(P) + 15) / 16 * 16);  // hot_slots
     unsigned *cursor = reinterpret_cast<unsigned *>(hkeys + S.hot_slots);                  // nparts
     int16_t *hidx = reinterpret_cast<int16_t *>(cursor + nparts);                          // hot_slots
     const unsigned lane = threadIdx.x & 31u;
@@ -1851,7 +1855,8 @@ class HashAggregate {
         return cap > room ? std::min<unsigned long long>(limit_, cap - room) : 0ull;
     }
     bool part_planned_ = false;
-    DBuf part_hot_keys_, part_hot_gids_;
+    DBuf part_hot_keys_, part_hot_gids_, part_hot_tab_, part_hot_tab_idx_;
+    int part_hot_slots_ = 0;
     int part_hot_ = 0;
     double part_cold_frac_ = 1.0;
     int64_t part_groups_est_ = 0;
@@ -2128,55 +2133,95 @@ void HashAggregate::launch(const DevBatch &b, const KeyIn &key, int64_t n, const
 }
 
 namespace {
-__global__ void sample_keys_kernel(KeyIn key, int64_t n, int64_t step, int m, long long *out, uint8_t *ok) {
+// The sampled rows' keys counted in an open-addressing table (each key once,
+// its count in tcnt); stats[0]: the sampled rows with a NULL or the marker key.
+__global__ void sample_count_kernel(KeyIn key, int64_t n, int64_t step, int m, long long *tkeys, unsigned *tcnt,
+                                    uint64_t mask, unsigned *stats) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
         const int64_t r = (int64_t)j * step;
-        const bool v = r < n && bit_get(key.valid, key.voff, r);
-        out[j] = v ? key_at(key, r) : 0;
-        ok[j] = v;
+        if (r >= n) continue;
+        const long long k = bit_get(key.valid, key.voff, r) ? key_at(key, r) : kEmptyKey;
+        if (k == kEmptyKey) {
+            atomicAdd(stats, 1u);
+            continue;
+        }
+        uint64_t pos = hash_word((uint64_t)k) & mask;
+        for (uint64_t t = 0; t <= mask; t++) {
+            const long long cur = (long long)atomicCAS(reinterpret_cast<unsigned long long *>(tkeys + pos),
+                                                       (unsigned long long)kEmptyKey, (unsigned long long)k);
+            if (cur == kEmptyKey || cur == k) {
+                atomicAdd(tcnt + pos, 1u);
+                break;
+            }
+            pos = (pos + 1) & mask;
+        }
+    }
+}
+// The counted keys: stats[1] distinct, stats[2] seen once, and those seen
+// at least `at_least` times listed (stats[3] of them, at most `cap` kept).
+__global__ void sample_runs_kernel(const long long *tkeys, const unsigned *tcnt, uint64_t slots, unsigned at_least,
+                                   long long *okeys, unsigned *ocnt, unsigned cap, unsigned *stats) {
+    for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < slots; s += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned c = tcnt[s];
+        if (!c) continue;
+        atomicAdd(stats + 1, 1u);
+        if (c == 1) atomicAdd(stats + 2, 1u);
+        if (c >= at_least) {
+            const unsigned i = atomicAdd(stats + 3, 1u);
+            if (i < cap) {
+                okeys[i] = tkeys[s];
+                ocnt[i] = c;
+            }
+        }
     }
 }
 }  // namespace
 
-// A strided sample of `m` keys of the batch, counted per key with a flat
-// open-addressing table on the host: (count, key) of each distinct valid key
-// (not the marker), and how many sampled rows had a NULL or the marker key.
+// A strided sample of `m` keys of the batch, counted on the device: the keys
+// seen at least `at_least` times (count, key), the distinct keys, those seen
+// once, and the sampled rows with a NULL or the marker key. One host read.
 struct KeySample {
-    std::vector<std::pair<int, long long>> runs;
+    std::vector<std::pair<int, long long>> runs;  // the keys seen at least at_least times
     int special = 0;
+    int distinct = 0;  // distinct valid keys (not the marker)
+    int singles = 0;   // of them, seen once
     int m = 0;
 };
-static KeySample take_sample(Runtime *rt, const KeyIn &key, int64_t n, int m) {
+static KeySample take_sample(Runtime *rt, const KeyIn &key, int64_t n, int m, int at_least) {
     KeySample S;
     S.m = m;
     if (m <= 0) return S;
+    constexpr unsigned kCap = 8192;
     const int64_t step = std::max<int64_t>(1, n / m);
-    DBuf keys(rt, (size_t)m * 8), ok(rt, (size_t)m);
-    sample_keys_kernel<<<grid_for(rt, m, 256, 4), 256, 0, rt->stream>>>(key, n, step, m, keys.as<long long>(),
-                                                                        ok.as<uint8_t>());
+    const uint64_t slots = next_pow2((uint64_t)2 * m);
+    DBuf tkeys(rt, slots * 8), tcnt(rt, slots * 4);
+    DBuf out(rt, 16 + (size_t)kCap * 12);  // stats[4], then kCap keys, then kCap counts
+    KRV_CUDA(cudaMemsetAsync(tkeys.get(), 0x80, slots * 8, rt->stream));
+    KRV_CUDA(cudaMemsetAsync(tcnt.get(), 0, slots * 4, rt->stream));
+    KRV_CUDA(cudaMemsetAsync(out.get(), 0, 16, rt->stream));
+    unsigned *stats = out.as<unsigned>();
+    long long *okeys = reinterpret_cast<long long *>(out.as<uint8_t>() + 16);
+    unsigned *ocnt = reinterpret_cast<unsigned *>(okeys + kCap);
+    sample_count_kernel<<<grid_for(rt, m, 256, 4), 256, 0, rt->stream>>>(key, n, step, m, tkeys.as<long long>(),
+                                                                         tcnt.as<unsigned>(), slots - 1, stats);
     rt->launches++;
-    check_launch("sample_keys_kernel");
-    std::vector<long long> hk(m);
-    std::vector<uint8_t> hv(m);
-    KRV_CUDA(cudaMemcpyAsync(hk.data(), keys.get(), (size_t)m * 8, cudaMemcpyDeviceToHost, rt->stream));
-    KRV_CUDA(cudaMemcpyAsync(hv.data(), ok.get(), (size_t)m, cudaMemcpyDeviceToHost, rt->stream));
+    check_launch("sample_count_kernel");
+    sample_runs_kernel<<<grid_for(rt, (int64_t)slots, 256, 4), 256, 0, rt->stream>>>(
+        tkeys.as<long long>(), tcnt.as<unsigned>(), slots, (unsigned)std::max(1, at_least), okeys, ocnt, kCap, stats);
+    rt->launches++;
+    check_launch("sample_runs_kernel");
+    std::vector<uint8_t> h(out.bytes());
+    KRV_CUDA(cudaMemcpyAsync(h.data(), out.get(), out.bytes(), cudaMemcpyDeviceToHost, rt->stream));
     KRV_CUDA(cudaStreamSynchronize(rt->stream));
-    const uint64_t slots = next_pow2((uint64_t)2 * m), mask = slots - 1;
-    std::vector<long long> tk(slots, kEmptyKey);
-    std::vector<int> tc(slots, 0);
-    for (int j = 0; j < m; j++) {
-        const long long k = hk[j];
-        if (!hv[j] || k == kEmptyKey) {
-            S.special++;
-            continue;
-        }
-        uint64_t pos = hash_word((uint64_t)k) & mask;
-        while (tk[pos] != kEmptyKey && tk[pos] != k) pos = (pos + 1) & mask;
-        tk[pos] = k;
-        tc[pos]++;
-    }
-    for (uint64_t i = 0; i < slots; i++)
-        if (tc[i]) S.runs.push_back({tc[i], tk[i]});
+    unsigned st[4];
+    memcpy(st, h.data(), 16);
+    S.special = (int)st[0];
+    S.distinct = (int)st[1];
+    S.singles = (int)st[2];
+    const unsigned got = std::min(st[3], kCap);
+    const long long *hk = reinterpret_cast<const long long *>(h.data() + 16);
+    const unsigned *hc = reinterpret_cast<const unsigned *>(hk + kCap);
+    for (unsigned i = 0; i < got; i++) S.runs.push_back({(int)hc[i], hk[i]});
     return S;
 }
 // The `most` keys seen at least `at_least` times, most frequent first.
@@ -2200,9 +2245,10 @@ void HashAggregate::sample_hot(const KeyIn &key, int64_t n) {
     constexpr int kSample = 1 << 16;
     const int m = (int)std::min<int64_t>(n, kSample);
     if (m < 1024) return;  // too few rows for hot keys to matter
-    const KeySample S = take_sample(rt_, key, n, m);
     // hot: at least 0.2% of the sample each
-    const std::vector<long long> hot = top_keys(S, kHotKeys, std::max(1, (m + 499) / 500));
+    const int at_least = std::max(1, (m + 499) / 500);
+    const KeySample S = take_sample(rt_, key, n, m, at_least);
+    const std::vector<long long> hot = top_keys(S, kHotKeys, at_least);
     hot_count_ = (int)hot.size();
     if (!hot_count_) return;
     hot_ = DBuf(rt_, hot.size() * 8);
@@ -2258,7 +2304,7 @@ void HashAggregate::plan_partitioned(const KeyIn &key, int64_t n) {
     part_planned_ = true;
     // The sample: a strided 64K rows of the first large batch.
     const int m = (int)std::min<int64_t>(n, kPartSample);
-    const KeySample S = take_sample(rt_, key, n, m);
+    const KeySample S = take_sample(rt_, key, n, m, 3);
     const int special = S.special;
     // Hot: seen at least 3 times, as many as the split kernel's shared memory
     // holds records for beside its lookup table.
@@ -2266,24 +2312,43 @@ void HashAggregate::plan_partitioned(const KeyIn &key, int64_t n) {
     int hmax = kHotMax;
     while (hmax > 0 && (size_t)(hmax + 2) * smem_stride(P_) + (size_t)2 * next_pow2(hmax) * 10 > (size_t)smem_cap)
         hmax /= 2;
-    const std::vector<long long> hot = top_keys(S, hmax, 3);
+    const std::vector<long long> ranked = top_keys(S, hmax, 3);
+    // The hot-key table: each key, most frequent first, into the emptier of
+    // its two buckets; a key that finds both full stays cold.
+    const int nb = ranked.empty() ? 0 : (int)std::max<uint64_t>(2, next_pow2((ranked.size() + 1) / 2));
+    std::vector<long long> tab((size_t)nb * kHotWays, kEmptyKey);
+    std::vector<int16_t> tidx((size_t)nb * kHotWays, -1);
+    std::vector<int> fill(nb, 0);
+    std::vector<long long> hot;
+    for (long long k : ranked) {
+        int b1, b2;
+        hot_buckets(hash_word((uint64_t)k), nb, b1, b2);
+        const int b = fill[b1] <= fill[b2] ? b1 : b2;
+        if (fill[b] >= kHotWays) continue;
+        tab[(size_t)b * kHotWays + fill[b]] = k;
+        tidx[(size_t)b * kHotWays + fill[b]] = (int16_t)hot.size();
+        fill[b]++;
+        hot.push_back(k);
+    }
+    part_hot_slots_ = nb * kHotWays;
+    part_hot_tab_ = DBuf(rt_, (size_t)std::max(1, part_hot_slots_) * 8);
+    part_hot_tab_idx_ = DBuf(rt_, (size_t)std::max(1, part_hot_slots_) * 2);
+    if (nb) {
+        KRV_CUDA(cudaMemcpyAsync(part_hot_tab_.get(), tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, rt_->stream));
+        KRV_CUDA(cudaMemcpyAsync(part_hot_tab_idx_.get(), tidx.data(), tidx.size() * 2, cudaMemcpyHostToDevice,
+                                 rt_->stream));
+    }
     std::vector<long long> hot_sorted = hot;
     std::sort(hot_sorted.begin(), hot_sorted.end());
     int hot_rows = 0;
-    std::vector<std::pair<int, long long>> runs;  // the cold keys' runs
-    for (const auto &r : S.runs) {
+    for (const auto &r : S.runs)
         if (std::binary_search(hot_sorted.begin(), hot_sorted.end(), r.second)) hot_rows += r.first;
-        else runs.push_back(r);
-    }
     part_hot_ = (int)hot.size();
     part_cold_frac_ = m ? std::max(0.0, 1.0 - (double)(hot_rows + special) / m) : 1.0;
     // Distinct cold keys (the guaranteed-error estimator: keys seen once in
-    // the sample stand for sqrt(n / m) keys each).
-    int64_t d = 0, f1 = 0;
-    for (const auto &r : runs) {
-        d++;
-        if (r.first == 1) f1++;
-    }
+    // the sample stand for sqrt(n / m) keys each; hot keys are seen 3 times
+    // or more).
+    const int64_t d = std::max<int64_t>(0, (int64_t)S.distinct - part_hot_), f1 = S.singles;
     const double est = (double)d + (double)f1 * (std::sqrt((double)n / std::max(1, m)) - 1.0);
     part_groups_est_ = std::max<int64_t>({(int64_t)est, spec_.expected_groups, 1});
     // Hot keys' group ids: the table first gets room for them.
@@ -2298,7 +2363,7 @@ void HashAggregate::plan_partitioned(const KeyIn &key, int64_t n) {
                                                                                   part_hot_, part_hot_gids_.as<uint32_t>());
     rt_->launches++;
     check_launch("hot_gid_kernel");
-    KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // `hot` is a stack vector
+    KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // `hot`, `tab` and `tidx` are stack vectors
 }
 
 void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_t n) {
@@ -2322,8 +2387,8 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
     while (bits < 13 && ((int64_t)1 << bits) * kPartKeys < part_groups_est_) bits++;
     const int nparts = 1 << bits;
     const int H = part_hot_;
-    const int hot_slots = H ? (int)next_pow2((uint64_t)2 * H) : 0;
-    const size_t split_smem = (size_t)(H + 2) * smem_stride(P) + (size_t)hot_slots * 10 + (size_t)nparts * 4;
+    const int hot_slots = H ? part_hot_slots_ : 0;
+    const size_t split_smem = ((size_t)(H + 2) * smem_stride(P) + 15) / 16 * 16 + (size_t)hot_slots * 10 + (size_t)nparts * 4;
     const size_t count_smem = (size_t)((nparts + 1) & ~1) * 4 + (size_t)hot_slots * 8;
     const auto split_kernel = P.ncols <= 4 ? agg_split_kernel<4> : agg_split_kernel<kMaxValueCols>;
     KRV_CUDA(cudaFuncSetAttribute(split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)split_smem));
@@ -2342,6 +2407,8 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
         S.hot_gids = part_hot_gids_.as<uint32_t>();
         S.H = H;
         S.hot_slots = hot_slots;
+        S.hot_tab = part_hot_tab_.as<long long>();
+        S.hot_tab_idx = part_hot_tab_idx_.as<int16_t>();
         S.part_bits = bits;
         S.row_bytes = part_row_bytes_;
         for (int c = 0; c < kMaxValueCols; c++) S.off_val[c] = part_off_val_[c];
