@@ -16,10 +16,16 @@
 // small table of (key, group id, record) for the keys it sees first (under
 // Zipf keys, the heavy ones) and merges it into the global records at the end.
 //
+// Large batches take the partitioned path instead (count, split and
+// partition kernels below): hot keys folded into per-CTA shared-memory
+// records, every other row sorted into hash partitions and each partition's
+// keys reduced in registers and merged once per chunk.
+//
 // Accumulation is exact and order-independent: counts and integer sums are
-// integer atomics, decimal and int64 sums are 128-bit (two 64-bit atomics
-// with carry), float64 sums are double-double (TwoSum-compensated atomics),
-// MIN/MAX of floats use an order-preserving integer map with NaN largest.
+// integer adds (64-bit atomics in global memory, 32-bit limbs with carries in
+// shared memory), decimal and int64 sums are 128-bit, float64 sums are
+// double-double (TwoSum-compensated), MIN/MAX of floats use an
+// order-preserving integer map with NaN largest.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -852,8 +858,10 @@ __global__ void __launch_bounds__(kSplitThreads, 2) agg_split_kernel(AggPlanDev 
 }
 
 // Cold rows per partition and CTA, by the split kernel's own test over the
-// split kernel's tiles: cta_rows[p * ctas + b] rows of partition p in CTA b's
-// tiles. Four rows per thread and step, their loads issued together.
+// split kernel's tiles: cta_rows[p * ctas + b] (zeroed first) gets the rows of
+// partition p in split CTA b's tiles. Two CTAs share each split CTA's tiles
+// (twice the warps to hide the loads); four rows per thread and step, their
+// loads issued together.
 __global__ void __launch_bounds__(kSplitThreads) agg_count_kernel(KeyIn key, int64_t n, SplitDev S) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int nparts = 1 << S.part_bits;
@@ -861,9 +869,12 @@ __global__ void __launch_bounds__(kSplitThreads) agg_count_kernel(KeyIn key, int
     long long *hkeys = reinterpret_cast<long long *>(s_hist + ((nparts + 1) & ~1));  // hot_slots
     for (int q = threadIdx.x; q < nparts; q += blockDim.x) s_hist[q] = 0;
     hot_table_init(S, hkeys, nullptr);
-    const int64_t step = (int64_t)gridDim.x * blockDim.x;
+    // gridDim.x = K * ctas: CTA (b, q) takes every K-th of split CTA b's
+    // tiles from its q-th on.
+    const int G = S.ctas, K = (int)gridDim.x / G, b = (int)blockIdx.x % G, q0 = (int)blockIdx.x / G;
+    const int64_t step = (int64_t)K * G * blockDim.x;  // rows between this CTA's tiles
     constexpr int U = 4;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; base < n; base += U * step) {
+    for (int64_t base = ((int64_t)b + (int64_t)G * q0) * blockDim.x + threadIdx.x; base < n; base += U * step) {
         long long k[U];
         uint8_t vb[U];
 #pragma unroll
@@ -882,7 +893,8 @@ __global__ void __launch_bounds__(kSplitThreads) agg_count_kernel(KeyIn key, int
         }
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < nparts; q += blockDim.x) S.cta_rows[(size_t)q * S.ctas + blockIdx.x] = s_hist[q];
+    for (int q = threadIdx.x; q < nparts; q += blockDim.x)
+        if (s_hist[q]) atomicAdd(&S.cta_rows[(size_t)q * G + b], s_hist[q]);
 }
 
 // Per partition (one warp each): the exclusive running count of its rows over
@@ -985,7 +997,7 @@ struct PartDev {
 // its keys pass a quarter of its slots.
 constexpr int kChunkRows = 1024;
 constexpr int kChunkSlots = 2048;
-constexpr int kTeamRows = 8, kTeamLanes = 8, kWarpRows = 32, kSegRows = 128;
+constexpr int kTeamRows = 8, kTeamLanes = 8, kWarpRows = 64, kSegRows = 128;
 constexpr int kAccCols = 2;  // value columns reduced per pass over a key's rows (three spill at 64 registers)
 constexpr uint32_t kNoGid = 0xFFFFFFFFu, kNewGid = 0x80000000u;
 
@@ -2390,7 +2402,11 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
     const int hot_slots = H ? part_hot_slots_ : 0;
     const size_t split_smem = ((size_t)(H + 2) * smem_stride(P) + 15) / 16 * 16 + (size_t)hot_slots * 10 + (size_t)nparts * 4;
     const size_t count_smem = (size_t)((nparts + 1) & ~1) * 4 + (size_t)hot_slots * 8;
-    const auto split_kernel = P.ncols <= 4 ? agg_split_kernel<4> : agg_split_kernel<kMaxValueCols>;
+    // Value columns held in registers: as few as the plan has (fewer
+    // registers for the row loaded ahead).
+    const auto split_kernel = P.ncols <= 3   ? agg_split_kernel<3>
+                              : P.ncols <= 4 ? agg_split_kernel<4>
+                                             : agg_split_kernel<kMaxValueCols>;
     KRV_CUDA(cudaFuncSetAttribute(split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)split_smem));
     KRV_CUDA(cudaFuncSetAttribute(agg_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)count_smem));
     const size_t part_smem = part_smem_bytes(part_row_bytes_);
@@ -2426,7 +2442,8 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
         DBuf ctl(rt_, 16);  // [0] rows in the partitions (u64), [8] failed partitions (int)
         KRV_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, rt_->stream));
         S.cta_rows = cta_rows.as<unsigned>();
-        agg_count_kernel<<<S.ctas, kSplitThreads, count_smem, rt_->stream>>>(ks, ns, S);
+        KRV_CUDA(cudaMemsetAsync(cta_rows.get(), 0, cta_rows.bytes(), rt_->stream));
+        agg_count_kernel<<<2 * S.ctas, kSplitThreads, count_smem, rt_->stream>>>(ks, ns, S);
         rt_->launches++;
         check_launch("agg_count_kernel");
         part_offsets_kernel<<<(int)ceil_div((int64_t)nparts * 32, 256), 256, 0, rt_->stream>>>(
