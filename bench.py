@@ -685,7 +685,8 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
     def run_join(partitioned, r):
         spec = kb.join_spec("left_outer", probe_out=[0, 1], build_out=[1, 2], build_rows_hint=nb,
                             max_output_rows=64 << 20, max_load=args.max_load, radix_bits=args.radix_bits)
-        j = kb.HashJoin(r, spec, partitioned=partitioned, device_budget=budget if partitioned else 0)
+        j = kb.HashJoin(r, spec, partitioned=partitioned, device_budget=budget if partitioned else 0,
+                        probe_filter_bits=args.grace_filter_bits if partitioned else None)
         t = [time.perf_counter()]
         for db in batches(build, nb, bstep):
             j.build_push_device(db)
@@ -735,6 +736,7 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
     ms = max_over_ranks(pg, statistics.median(t for t, _ in times), device)
     counters = j.counters()
     spilled = j.spilled_partitions()
+    filtered = j.filtered_probe_rows()
     last_phases = dict(phases)
     launches1 = capped.launches
     del j
@@ -750,6 +752,7 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
            "config": {"workload": "left outer join 500M build x 2B probe, 100 heavy probe keys, 1% NULL keys",
                       "build_rows": nb, "probe_rows": np_, "output_rows": rows, "device_budget_bytes": budget,
                       "partitions": counters["partitions"], "spilled_partitions": spilled,
+                      "probe_filter_bits_per_key": args.grace_filter_bits, "probe_rows_ruled_out_by_filter": filtered,
                       "consumer": "every output batch read once by an order-independent checksum (timed)",
                       "l2": "inputs (44 GB) larger than L2; no flush"},
            "wall_ms_per_step": statistics.median(w for _, w in times),
@@ -948,6 +951,8 @@ def main():
     ap.add_argument("--grace-budget", type=int, default=24 << 30, help="grace: device budget of the join")
     ap.add_argument("--max-load", type=float, default=0.0, help="join, grace: hash table load factor (0: default)")
     ap.add_argument("--radix-bits", type=int, default=0, help="grace: level-0 partition bits (0: chosen)")
+    ap.add_argument("--grace-filter-bits", type=int, default=10,
+                    help="grace: bits per build key of the partition pass's Bloom filter (0: none)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     threads = os.cpu_count() or 1

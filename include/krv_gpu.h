@@ -250,13 +250,25 @@ krv_status krv_hash_rows_device(krv_runtime *rt, const struct ArrowDeviceArray *
  * when set, decides the partitions and which of them spill up front. */
 typedef struct {
     int64_t device_budget_bytes;  /* device bytes for the join (0: the runtime's budget, else half the free memory) */
-    int64_t reserved[3];
+    /* Bits per build key of the blocked Bloom filter that the build side's
+     * partition pass fills (one 32-byte block per key, keyed by the row hash
+     * h) and the probe side's partition pass tests: a probe row it rules out
+     * matches nothing, so it is padded at once (left outer) or dropped
+     * (inner) and is never partitioned or spilled. Sized from
+     * spec->build_rows_hint, else 1/32 of the budget up to 64 MiB; at most
+     * 1/16 of the budget. 0: no filter. krv_grace_options_init sets 10. */
+    int32_t probe_filter_bits;
+    int32_t pad0;
+    int64_t reserved[2];
 } krv_grace_options;
 void krv_grace_options_init(krv_grace_options *o);
 krv_status krv_join_create_partitioned(krv_runtime *rt, const krv_join_spec *spec, const krv_grace_options *opt,
                                        krv_join **out);
 /* Partitions of a partitioned join that spilled to host memory. */
 int64_t krv_join_spilled_partitions(const krv_join *j);
+/* Probe rows of a partitioned join that its Bloom filter ruled out in the
+ * partition pass (0 for an unpartitioned join or without the filter). */
+int64_t krv_join_filtered_probe_rows(const krv_join *j);
 
 /* ---- grouped hash aggregate ---------------------------------------------- */
 /* AggregateFunction (aggregate/mod.rs:134), the core five. MIN/MAX take
@@ -396,6 +408,54 @@ krv_status krv_key_filter_info_get(const krv_key_filter *f, krv_key_filter_info 
 /* The Bloom bits in the Parquet SBBF layout (RuntimeBloom::to_bytes). */
 krv_status krv_key_filter_bloom_bytes(const krv_key_filter *f, void *host_out, int64_t nbytes);
 void krv_key_filter_destroy(krv_key_filter *f);
+
+/* ---- Parquet column chunks decoded on the device -----------------------------
+ * The engine's Parquet reader (crates/krishiv-io/src/parquet/decode.rs) decodes
+ * row groups on the host and evaluates pushed predicates once per dictionary
+ * entry of a dictionary-encoded chunk (parquet/dict_probe.rs:1-27, `passes`,
+ * `any_entry_in`). krv_parquet_decode_chunk takes one column chunk's bytes as
+ * the file stores them (host memory, from the chunk's dictionary page, or
+ * first data page, through its last page: ColumnMetaData.dictionary_page_offset
+ * or data_page_offset, total_compressed_size), walks the page headers on the
+ * host, and decompresses and decodes every page on the device into one Arrow
+ * column of `num_values` rows. With a key filter, the batch gets a second,
+ * boolean column "pass": TRUE where the row may match (KeyFilter::evaluate,
+ * filter.rs:776-798), evaluated on the encoded pages: once per dictionary
+ * entry for dictionary-encoded pages, per value for PLAIN ones; a NULL row
+ * passes only if the filter lets NULLs pass. info->dictionary_passing = 0
+ * says that no row of the chunk can pass but a NULL (the row group can be
+ * skipped, as any_entry_in decides). Flat columns (max definition level 0 or
+ * 1, no repetition); physical INT32 (as "i", "tdD", "l", "d:p,s,64" or
+ * "d:p,s"), INT64 (as "l", "d:p,s,64" or "d:p,s") and DOUBLE (as "g");
+ * PLAIN, PLAIN_DICTIONARY and RLE_DICTIONARY values; UNCOMPRESSED and SNAPPY
+ * chunks; data pages v1 and v2. Others: KRV_UNSUPPORTED. Bytes that do not
+ * decode: KRV_INVALID_ARGUMENT. The filter applies to integer columns. */
+#define KRV_PQ_INT32 1         /* parquet.thrift Type */
+#define KRV_PQ_INT64 2
+#define KRV_PQ_DOUBLE 5
+#define KRV_PQ_UNCOMPRESSED 0  /* parquet.thrift CompressionCodec */
+#define KRV_PQ_SNAPPY 1
+typedef struct {
+    int32_t physical_type;  /* KRV_PQ_INT32, KRV_PQ_INT64 or KRV_PQ_DOUBLE */
+    int32_t codec;          /* KRV_PQ_UNCOMPRESSED or KRV_PQ_SNAPPY */
+    int32_t max_def_level;  /* 0: required, 1: optional */
+    int32_t pad0;
+    int64_t num_values;     /* ColumnMetaData.num_values: the chunk's rows */
+    const char *format;     /* Arrow format of the decoded column */
+    const char *name;       /* its name (may be NULL) */
+} krv_parquet_column;
+typedef struct {
+    int64_t rows;
+    int64_t pages;               /* data pages */
+    int64_t dictionary_entries;  /* 0 without a dictionary page */
+    int64_t dictionary_passing;  /* entries the filter passes (-1: no filter, no dictionary, or
+                                    some data page not dictionary encoded) */
+    int64_t passing_rows;        /* rows the filter passes (-1: no filter) */
+} krv_parquet_info;
+krv_status krv_parquet_decode_chunk(krv_runtime *rt, const void *chunk, int64_t chunk_bytes,
+                                    const krv_parquet_column *column, const krv_key_filter *filter,
+                                    struct ArrowDeviceArray *out, struct ArrowSchema *out_schema,
+                                    krv_parquet_info *info);
 
 /* ---- star join pipeline (runtime filter + two joins + grouped sum) --------
  * The fused plan shape

@@ -167,6 +167,20 @@ class KeyFilterInfo(C.Structure):
                 ("bloom_bytes", C.c_int64)]
 
 
+class ParquetColumn(C.Structure):
+    _fields_ = [("physical_type", C.c_int32), ("codec", C.c_int32), ("max_def_level", C.c_int32), ("pad0", C.c_int32),
+                ("num_values", C.c_int64), ("format", C.c_char_p), ("name", C.c_char_p)]
+
+
+class ParquetInfo(C.Structure):
+    _fields_ = [("rows", C.c_int64), ("pages", C.c_int64), ("dictionary_entries", C.c_int64),
+                ("dictionary_passing", C.c_int64), ("passing_rows", C.c_int64)]
+
+
+PQ_INT32, PQ_INT64, PQ_DOUBLE = 1, 2, 5
+PQ_UNCOMPRESSED, PQ_SNAPPY = 0, 1
+
+
 class StarSpec(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("dim_key", "dim_pred", "dim_attr", "pred_a", "pred_b", "fact_fk_a",
                                          "fact_fk_b", "fact_price", "fact_discount", "group_by", "use_filters",
@@ -186,7 +200,8 @@ class StarCounters(C.Structure):
 
 
 class GraceOptions(C.Structure):
-    _fields_ = [("device_budget_bytes", C.c_int64), ("reserved", C.c_int64 * 3)]
+    _fields_ = [("device_budget_bytes", C.c_int64), ("probe_filter_bits", C.c_int32), ("pad0", C.c_int32),
+                ("reserved", C.c_int64 * 2)]
 
 
 class ServerOptions(C.Structure):
@@ -279,6 +294,10 @@ _SIGS = {
     "krv_join_create_partitioned": (C.c_int32, [C.c_void_p, C.POINTER(JoinSpec), C.POINTER(GraceOptions),
                                                 C.POINTER(C.c_void_p)]),
     "krv_join_spilled_partitions": (C.c_int64, [C.c_void_p]),
+    "krv_join_filtered_probe_rows": (C.c_int64, [C.c_void_p]),
+    "krv_parquet_decode_chunk": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(ParquetColumn), C.c_void_p,
+                                             C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema),
+                                             C.POINTER(ParquetInfo)]),
     "krv_server_options_init": (None, [C.POINTER(ServerOptions)]),
     "krv_server_create": (C.c_int32, [C.c_void_p, C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
     "krv_server_add_table": (C.c_int32, [C.c_void_p, C.POINTER(ArrowDeviceArray), C.POINTER(ArrowSchema), C.c_int32,
@@ -574,16 +593,21 @@ class HashJoin:
     `partitioned=True` makes the partitioned (grace) join of
     crates/krishiv-exec/src/join/grace.rs (krv_join_create_partitioned): inner
     or left outer on one int64 key, within `device_budget` bytes (0: the
-    runtime's budget), spilling partitions to page-locked host memory."""
+    runtime's budget), spilling partitions to page-locked host memory;
+    `probe_filter_bits` (partitioned only) sets the bits per build key of the
+    Bloom filter its partition passes build and test (None: the default, 10;
+    0: no filter)."""
 
     def __init__(self, rt: Runtime, spec: JoinSpec, partitioned: bool = False, device_budget: int = 0,
-                 filter=None):
+                 filter=None, probe_filter_bits=None):
         self.rt = rt
         h = C.c_void_p()
         if partitioned:
             o = GraceOptions()
             lib().krv_grace_options_init(C.byref(o))
             o.device_budget_bytes = device_budget
+            if probe_filter_bits is not None:
+                o.probe_filter_bits = int(probe_filter_bits)
             check(lib().krv_join_create_partitioned(rt.h, C.byref(spec), C.byref(o), C.byref(h)))
         else:
             check(lib().krv_join_create(rt.h, C.byref(spec), C.byref(h)))
@@ -644,6 +668,10 @@ class HashJoin:
 
     def spilled_partitions(self) -> int:
         return lib().krv_join_spilled_partitions(self.h)
+
+    def filtered_probe_rows(self) -> int:
+        """Probe rows the partitioned join's Bloom filter ruled out."""
+        return lib().krv_join_filtered_probe_rows(self.h)
 
     def finish(self) -> list:
         out = []
@@ -851,6 +879,24 @@ class KeyFilter:
             self.close()
         except Exception:
             pass
+
+
+def parquet_decode_chunk(rt: Runtime, chunk, physical_type: int, codec: int, max_def_level: int, num_values: int,
+                         fmt: str, name: str = "", key_filter: Optional[KeyFilter] = None):
+    """One Parquet column chunk (its bytes as the file stores them: bytes, or
+    a uint8 numpy array) decoded on the device (krv_parquet_decode_chunk):
+    a DeviceResult of the column and, with `key_filter`, the filter's
+    boolean "pass" column, and the decode's counts."""
+    import numpy as np
+    buf = np.frombuffer(chunk, dtype=np.uint8) if isinstance(chunk, (bytes, bytearray, memoryview)) else chunk
+    buf = np.ascontiguousarray(buf, dtype=np.uint8)
+    col = ParquetColumn(physical_type=physical_type, codec=codec, max_def_level=max_def_level, num_values=num_values,
+                        format=fmt.encode(), name=name.encode())
+    dev, sch, info = ArrowDeviceArray(), ArrowSchema(), ParquetInfo()
+    check(lib().krv_parquet_decode_chunk(rt.h, buf.ctypes.data_as(C.c_void_p), buf.size, C.byref(col),
+                                         key_filter.h if key_filter is not None else None, C.byref(dev),
+                                         C.byref(sch), C.byref(info)))
+    return DeviceResult(dev, sch), {n: getattr(info, n) for n, _ in ParquetInfo._fields_}
 
 
 def star_spec(pred_a: int, pred_b: int, group_by: int = 0, use_filters: bool = True, mode: int = STAR_FUSED):

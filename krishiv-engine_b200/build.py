@@ -23,7 +23,7 @@ INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libkrv_gpu.so")
 
-SOURCES = ["runtime.cu", "util.cu", "join.cu", "bloom.cu", "aggregate.cu", "star.cu", "gen.cu", "scratch_agg.cu", "serve.cu", "grace.cu", "keydict.cu", "varcol.cu", "capi.cpp"]
+SOURCES = ["runtime.cu", "util.cu", "join.cu", "bloom.cu", "aggregate.cu", "star.cu", "gen.cu", "scratch_agg.cu", "serve.cu", "grace.cu", "keydict.cu", "varcol.cu", "parquet.cu", "capi.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden", "--expt-relaxed-constexpr",

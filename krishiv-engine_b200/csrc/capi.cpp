@@ -210,7 +210,9 @@ krv_status krv_join_create(krv_runtime *rt, const krv_join_spec *spec, krv_join 
 }
 
 void krv_grace_options_init(krv_grace_options *o) {
-    if (o) *o = krv_grace_options{};
+    if (!o) return;
+    *o = krv_grace_options{};
+    o->probe_filter_bits = 10;
 }
 krv_status krv_join_create_partitioned(krv_runtime *rt, const krv_join_spec *spec, const krv_grace_options *opt,
                                        krv_join **out) {
@@ -232,6 +234,9 @@ krv_status krv_join_create_partitioned(krv_runtime *rt, const krv_join_spec *spe
 }
 int64_t krv_join_spilled_partitions(const krv_join *j) {
     return j && j->g ? krv::grace_spilled_partitions(j->g) : 0;
+}
+int64_t krv_join_filtered_probe_rows(const krv_join *j) {
+    return j && j->g ? krv::grace_filtered_probe_rows(j->g) : 0;
 }
 
 krv_status krv_join_build_push(krv_join *j, const ArrowArray *batch, const ArrowSchema *schema) {
@@ -533,6 +538,22 @@ krv_status krv_key_filter_evaluate(krv_key_filter *f, const ArrowArray *batch, c
 krv_status krv_key_filter_evaluate_device(krv_key_filter *f, const ArrowDeviceArray *batch, const ArrowSchema *schema,
                                           int32_t column, ArrowDeviceArray *out, ArrowSchema *out_schema) {
     return filter_eval_impl<true>(f, batch, schema, column, out, out_schema);
+}
+krv_status krv_parquet_decode_chunk(krv_runtime *rt, const void *chunk, int64_t chunk_bytes,
+                                    const krv_parquet_column *column, const krv_key_filter *filter,
+                                    ArrowDeviceArray *out, ArrowSchema *out_schema, krv_parquet_info *info) {
+    return guard([&] {
+        need(rt, "runtime");
+        need(column, "column");
+        need(out, "out");
+        need(out_schema, "out_schema");
+        krv::DeviceGuard g(&rt->rt);
+        krv::ParquetChunk r = krv::decode_parquet_chunk(&rt->rt, static_cast<const uint8_t *>(chunk), chunk_bytes,
+                                                        *column, filter ? filter->f.get() : nullptr);
+        krv::export_device(&rt->rt, r.batch, out, out_schema);
+        if (info) *info = r.info;
+        return KRV_OK;
+    });
 }
 krv_status krv_key_filter_info_get(const krv_key_filter *f, krv_key_filter_info *out) {
     return guard([&] {

@@ -53,43 +53,60 @@ struct PartArgs {
     int64_t n;
     int level, bits;
     uint64_t seed;
-    int nparts;      // partitions; bucket `nparts` holds NULL keys
+    int nparts;      // partitions; bucket `nparts` holds NULL keys, `nparts + 1` filtered rows
     int keep_nulls;  // write the NULL bucket (probe side) or drop it (build side)
+    int keep_filtered;  // write the filtered bucket (left outer) or drop it (inner)
+    int filter_mode;    // kFilterNone, kFilterInsert (build side) or kFilterTest (probe side)
+    uint32_t *bloom;    // blocked Bloom filter over h: 8 words (one 32-byte block) per key
+    uint64_t bloom_blocks;
     PartCol c[kMaxCols];
     int ncols;
 };
+constexpr int kFilterNone = 0, kFilterInsert = 1, kFilterTest = 2;
 
-__device__ __forceinline__ int part_of(const PartArgs &A, int64_t r) {
+// The partition of row r and its key hash h. With kFilterTest, a row whose
+// key the build side's Bloom filter rules out goes to bucket nparts + 1.
+__device__ __forceinline__ int part_of(const PartArgs &A, int64_t r, uint64_t &h) {
+    h = 0;
     if (A.kvalid && !bit_get(A.kvalid, A.kvoff, r)) return A.nparts;
-    const uint64_t h = hash_word((uint64_t)A.key[r]);
+    h = hash_word((uint64_t)A.key[r]);
+    if (A.filter_mode == kFilterTest &&
+        !sbbf_check_words(A.bloom + 8 * sbbf_block(h, A.bloom_blocks), (uint32_t)h))
+        return A.nparts + 1;
     if (A.level == 0) return (int)(h >> (64 - A.bits));
     return (int)((finalize(h, A.seed) >> (48 - 3 * A.level)) & 7u);
 }
 
 __global__ void __launch_bounds__(256) part_hist_kernel(PartArgs A, unsigned long long *hist) {
-    __shared__ unsigned int s_hist[kMaxParts + 1];
-    for (int p = threadIdx.x; p <= A.nparts; p += blockDim.x) s_hist[p] = 0;
+    __shared__ unsigned int s_hist[kMaxParts + 2];
+    for (int p = threadIdx.x; p <= A.nparts + 1; p += blockDim.x) s_hist[p] = 0;
     __syncthreads();
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += (int64_t)gridDim.x * blockDim.x)
-        atomicAdd(&s_hist[part_of(A, r)], 1u);
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t h;
+        atomicAdd(&s_hist[part_of(A, r, h)], 1u);
+    }
     __syncthreads();
-    for (int p = threadIdx.x; p <= A.nparts; p += blockDim.x)
+    for (int p = threadIdx.x; p <= A.nparts + 1; p += blockDim.x)
         if (s_hist[p]) atomicAdd(hist + p, (unsigned long long)s_hist[p]);
 }
 
 // Tiles of kPartTile rows: rank every row within its partition in shared
 // memory, claim each partition's run of the output with one atomic per tile,
 // then write the tile column by column in partition order (coalesced runs).
+//
+// With kFilterInsert every non-NULL key also goes into the Bloom filter (one
+// 32-byte block per key: 8 lanes of a warp set one word each), so that the
+// filter is complete when the build side's partition passes end.
 __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(PartArgs A, unsigned long long *cursor) {
-    __shared__ unsigned int s_cnt[kMaxParts + 1], s_off[kMaxParts + 2];
-    __shared__ unsigned long long s_base[kMaxParts + 1];
+    __shared__ unsigned int s_cnt[kMaxParts + 2], s_off[kMaxParts + 3];
+    __shared__ unsigned long long s_base[kMaxParts + 2];
     __shared__ uint8_t s_part[kPartTile];
     __shared__ __align__(16) unsigned long long s_val[kPartTile];
     constexpr int U = kPartTile / kPartThreads;
     const int64_t ntiles = (A.n + kPartTile - 1) / kPartTile;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t row0 = t * kPartTile;
-        for (int p = threadIdx.x; p <= A.nparts; p += kPartThreads) s_cnt[p] = 0;
+        for (int p = threadIdx.x; p <= A.nparts + 1; p += kPartThreads) s_cnt[p] = 0;
         __syncthreads();
         int part[U];
         unsigned rank[U];
@@ -97,26 +114,41 @@ __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(PartArgs A, 
         for (int u = 0; u < U; u++) {
             const int i = u * kPartThreads + threadIdx.x;
             const int64_t r = row0 + i;
-            part[u] = r < A.n ? part_of(A, r) : -1;
+            uint64_t h = 0;
+            part[u] = r < A.n ? part_of(A, r, h) : -1;
+            if (A.filter_mode == kFilterInsert) {
+                // four keys per round, each key's 8 words set by 8 lanes
+                unsigned todo = __ballot_sync(0xFFFFFFFFu, part[u] >= 0 && part[u] < A.nparts);
+                const int w = (int)(lane_id() & 7u), q = (int)(lane_id() >> 3);
+                while (todo) {
+                    unsigned m = todo;
+                    for (int j = 0; j < q; j++) m &= m - 1;  // drop the q lowest keys of the round
+                    const int src = m ? __ffs(m) - 1 : 0;
+                    const uint64_t hs = __shfl_sync(0xFFFFFFFFu, h, src);
+                    if (m) atomicOr(A.bloom + 8 * sbbf_block(hs, A.bloom_blocks) + w, sbbf_bit((uint32_t)hs, w));
+                    for (int j = 0; j < 4 && todo; j++) todo &= todo - 1;
+                }
+            }
             if (part[u] == A.nparts && !A.keep_nulls) part[u] = -1;
+            if (part[u] == A.nparts + 1 && !A.keep_filtered) part[u] = -1;
             rank[u] = part[u] >= 0 ? atomicAdd(&s_cnt[part[u]], 1u) : 0u;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
             unsigned acc = 0;
-            for (int p = 0; p <= A.nparts; p++) {
+            for (int p = 0; p <= A.nparts + 1; p++) {
                 s_off[p] = acc;
                 acc += s_cnt[p];
             }
-            s_off[A.nparts + 1] = acc;
+            s_off[A.nparts + 2] = acc;
         }
-        for (int p = threadIdx.x; p <= A.nparts; p += kPartThreads)
+        for (int p = threadIdx.x; p <= A.nparts + 1; p += kPartThreads)
             s_base[p] = s_cnt[p] ? atomicAdd(cursor + p, (unsigned long long)s_cnt[p]) : 0ull;
         __syncthreads();
 #pragma unroll
         for (int u = 0; u < U; u++)
             if (part[u] >= 0) s_part[s_off[part[u]] + rank[u]] = (uint8_t)part[u];
-        const unsigned total = s_off[A.nparts + 1];
+        const unsigned total = s_off[A.nparts + 2];
         for (int c = 0; c < A.ncols; c++) {
             const PartCol C = A.c[c];
 #pragma unroll
@@ -389,7 +421,7 @@ class GraceJoin {
     }
 
     void build_slice(const DevBatch &b) {
-        std::vector<Segment> segs = partition(b, spec_.build_keys[0], 0, parts_bits_, false);
+        std::vector<Segment> segs = partition(b, spec_.build_keys[0], 0, parts_bits_, false, bloom_ ? kFilterInsert : kFilterNone);
         for (int p = 0; p < nparts_; p++) {
             Segment &s = segs[p];
             if (s.rows == 0) continue;
@@ -446,11 +478,19 @@ class GraceJoin {
     // of the budget, else deferred to host memory like those of spilled
     // partitions (and joined at finish by the same resident tables).
     void probe_slice(const DevBatch &in, std::vector<DevBatch> &out, int64_t &out_rows) {
-        std::vector<Segment> segs = partition(in, spec_.probe_keys[0], 0, parts_bits_, true);
+        std::vector<Segment> segs = partition(in, spec_.probe_keys[0], 0, parts_bits_, true, bloom_ ? kFilterTest : kFilterNone);
         Segment &nulls = segs[nparts_];
         if (nulls.rows > 0 && spec_.join_type == KRV_JOIN_LEFT_OUTER) {
             out_rows += nulls.rows;
             keep(out, null_join_->probe(with_null_keys(nulls)));
+        }
+        // Rows whose key the build side's Bloom filter rules out match no
+        // build row: padded now (left outer), never partitioned or spilled.
+        Segment &ruled_out = segs[nparts_ + 1];
+        counters_filtered_ += last_filtered_;
+        if (ruled_out.rows > 0 && spec_.join_type == KRV_JOIN_LEFT_OUTER) {
+            out_rows += ruled_out.rows;
+            keep(out, null_join_->probe(ruled_out.batch));
         }
         const int64_t out_cap = budget_ / 8 / out_row_bytes();
         const double ratio = out_ratio();
@@ -689,6 +729,7 @@ class GraceJoin {
         c.partitions = nparts_ + splits_;
         return c;
     }
+    int64_t filtered_probe_rows() const { return counters_filtered_; }
     int64_t spilled_partitions() const {
         int64_t n = 0;
         for (const auto &P : parts_) n += P.spilled;
@@ -732,6 +773,15 @@ class GraceJoin {
                                             : radix_for(spec_.build_rows_hint, row_bytes_, budget_);
         nparts_ = 1 << parts_bits_;
         parts_.resize(nparts_);
+        if (opt_.probe_filter_bits > 0) {
+            // the Bloom filter the build side's partition passes fill
+            const int64_t want = spec_.build_rows_hint > 0 ? spec_.build_rows_hint * opt_.probe_filter_bits / 8
+                                                           : std::min<int64_t>(budget_ / 32, 64 << 20);
+            bloom_bytes_ = std::max<int64_t>(32, std::min<int64_t>(want, budget_ / 16)) / 32 * 32;
+            bloom_blocks_ = (uint64_t)bloom_bytes_ / 32;
+            bloom_.reset(new DBuf(rt_, (size_t)bloom_bytes_));
+            KRV_CUDA(cudaMemsetAsync(bloom_->get(), 0, (size_t)bloom_bytes_, rt_->stream));
+        }
         // With a size hint the spilled partitions are known up front; without
         // one, partitions spill as the resident footprint passes its share.
         int resident = nparts_;
@@ -770,7 +820,7 @@ class GraceJoin {
     }
     // The share of the budget that resident tables may take; the rest holds
     // a slice's partitioned copy and a call's output.
-    int64_t resident_cap() const { return budget_ / 10 * 6; }
+    int64_t resident_cap() const { return (budget_ - bloom_bytes_) / 10 * 6; }
     int64_t resident_bytes() const {
         int64_t b = 0;
         for (const auto &P : parts_)
@@ -799,7 +849,8 @@ class GraceJoin {
     // Partitions batch `b` by its key column at `level`: one segment (a
     // device batch of the partition's rows) per partition, plus the NULL-key
     // bucket at index nparts (kept when keep_nulls).
-    std::vector<Segment> partition(const DevBatch &b, int key, int level, int bits, bool keep_nulls) {
+    std::vector<Segment> partition(const DevBatch &b, int key, int level, int bits, bool keep_nulls,
+                                   int filter_mode = kFilterNone) {
         const int nparts = level == 0 ? (1 << bits) : 8;
         PartArgs A{};
         A.key = static_cast<const long long *>(b.cols[key].data);
@@ -811,23 +862,32 @@ class GraceJoin {
         A.seed = spec_.seed;
         A.nparts = nparts;
         A.keep_nulls = keep_nulls ? 1 : 0;
+        A.filter_mode = filter_mode;
+        A.keep_filtered = spec_.join_type == KRV_JOIN_LEFT_OUTER ? 1 : 0;
+        A.bloom = bloom_ ? bloom_->as<uint32_t>() : nullptr;
+        A.bloom_blocks = bloom_blocks_;
         A.ncols = (int)b.cols.size();
-        DBuf ctr(rt_, (size_t)(nparts + 1) * 8 * 2);
-        unsigned long long *hist = ctr.as<unsigned long long>(), *cursor = hist + nparts + 1;
-        KRV_CUDA(cudaMemsetAsync(hist, 0, (size_t)(nparts + 1) * 8, rt_->stream));
+        const int nb = nparts + 2;  // partitions, the NULL bucket, the filtered bucket
+        DBuf ctr(rt_, (size_t)nb * 8 * 2);
+        unsigned long long *hist = ctr.as<unsigned long long>(), *cursor = hist + nb;
+        KRV_CUDA(cudaMemsetAsync(hist, 0, (size_t)nb * 8, rt_->stream));
         part_hist_kernel<<<grid_for(rt_, b.rows, 256, 8), 256, 0, rt_->stream>>>(A, hist);
         rt_->launches++;
         check_launch("part_hist_kernel");
-        std::vector<unsigned long long> h(nparts + 1);
-        KRV_CUDA(cudaMemcpyAsync(h.data(), hist, (nparts + 1) * 8, cudaMemcpyDeviceToHost, rt_->stream));
+        std::vector<unsigned long long> h(nb);
+        KRV_CUDA(cudaMemcpyAsync(h.data(), hist, nb * 8, cudaMemcpyDeviceToHost, rt_->stream));
         KRV_CUDA(cudaStreamSynchronize(rt_->stream));
-        std::vector<unsigned long long> start(nparts + 1);
+        last_filtered_ = (int64_t)h[nparts + 1];  // counted whether the bucket is kept or dropped
+        std::vector<unsigned long long> start(nb);
+        std::vector<bool> kept_bucket(nb, true);
+        kept_bucket[nparts] = keep_nulls;
+        kept_bucket[nparts + 1] = A.keep_filtered != 0;
         unsigned long long acc = 0;
-        for (int p = 0; p <= nparts; p++) {
+        for (int p = 0; p < nb; p++) {
             start[p] = acc;
-            if (p < nparts || keep_nulls) acc += h[p];
+            if (kept_bucket[p]) acc += h[p];
         }
-        KRV_CUDA(cudaMemcpyAsync(cursor, start.data(), (nparts + 1) * 8, cudaMemcpyHostToDevice, rt_->stream));
+        KRV_CUDA(cudaMemcpyAsync(cursor, start.data(), nb * 8, cudaMemcpyHostToDevice, rt_->stream));
         const int64_t kept = (int64_t)acc;
         std::vector<std::shared_ptr<DBuf>> outs;
         for (int c = 0; c < A.ncols; c++) {
@@ -841,10 +901,10 @@ class GraceJoin {
             rt_->launches++;
             check_launch("part_scatter_kernel");
         }
-        std::vector<Segment> segs(nparts + 1);
-        for (int p = 0; p <= nparts; p++) {
+        std::vector<Segment> segs(nb);
+        for (int p = 0; p < nb; p++) {
             Segment &s = segs[p];
-            s.rows = (p < nparts || keep_nulls) ? (int64_t)h[p] : 0;
+            s.rows = kept_bucket[p] ? (int64_t)h[p] : 0;
             s.batch.rows = s.rows;
             for (int c = 0; c < A.ncols; c++) {
                 DevCol col;
@@ -1229,6 +1289,11 @@ class GraceJoin {
     krv_join_spec spec_;
     krv_grace_options opt_;
     int64_t budget_ = 0;
+    std::unique_ptr<DBuf> bloom_;  // the probe-side filter over the build keys (none: no filter)
+    int64_t bloom_bytes_ = 0;
+    uint64_t bloom_blocks_ = 0;
+    int64_t counters_filtered_ = 0;
+    int64_t last_filtered_ = 0;  // rows the last partition pass's filter ruled out
     bool schema_ = false, built_ = false, finishing_ = false;
     std::vector<DevCol> build_types_, probe_types_;
     int64_t row_bytes_ = 0;
@@ -1276,5 +1341,6 @@ DevBatch grace_empty_output(GraceJoin *g) { return g->empty_output(); }
 const krv_join_spec &grace_spec(const GraceJoin *g) { return g->spec(); }
 krv_join_counters grace_counters(const GraceJoin *g) { return g->counters(); }
 int64_t grace_spilled_partitions(const GraceJoin *g) { return g->spilled_partitions(); }
+int64_t grace_filtered_probe_rows(const GraceJoin *g) { return g->filtered_probe_rows(); }
 
 }  // namespace krv

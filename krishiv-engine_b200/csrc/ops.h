@@ -261,6 +261,15 @@ DevBatch grace_empty_output(GraceJoin *g);
 const krv_join_spec &grace_spec(const GraceJoin *g);
 krv_join_counters grace_counters(const GraceJoin *g);
 int64_t grace_spilled_partitions(const GraceJoin *g);
+int64_t grace_filtered_probe_rows(const GraceJoin *g);
+
+// ---- Parquet column chunks decoded on the device (parquet.cu) ---------------------
+struct ParquetChunk {
+    DevBatch batch;  // the decoded column, then (with a filter) the filter's boolean column
+    krv_parquet_info info;
+};
+ParquetChunk decode_parquet_chunk(Runtime *rt, const uint8_t *chunk, int64_t bytes, const krv_parquet_column &col,
+                                  const KeyFilterImpl *filter);
 
 // ---- grouped hash aggregate (crates/krishiv-exec/src/aggregate/sink.rs:181) ----
 class HashAggregate;

@@ -13,7 +13,15 @@ that the operators take as host batches (or that a caller copies to the
 device). Which row groups are read never changes a result: a skipped row
 group holds no row that the filter passes.
 
-Decoding Parquet pages on the device is not done here."""
+`DeviceParquetScan` reads the same row groups, but hands each column chunk's
+bytes, as the file stores them, to the device decoder
+(`krv_parquet_decode_chunk`): pages are decompressed and decoded in HBM, and
+the key filter is evaluated on the encoded pages (once per dictionary entry
+of a dictionary-encoded chunk, as the reference's dictionary stage does,
+crates/krishiv-io/src/parquet/dict_probe.rs); a row group whose key chunk
+passes no row is skipped once that chunk is decoded, before its other
+columns are read (the reference's `any_entry_in` skips a dictionary-encoded
+one of them before its data pages)."""
 from __future__ import annotations
 
 from typing import Dict, Iterator, List, Optional, Sequence
@@ -87,3 +95,88 @@ class ParquetScan:
         for rg in self.row_groups:
             t = self.file.read_row_group(rg, columns=self.columns)
             yield from t.to_batches(max_chunksize=self.batch_rows)
+
+
+# pyarrow names of the Parquet physical types and codecs the device decoder takes
+_PHYSICAL = {"INT32": 1, "INT64": 2, "DOUBLE": 5}
+_CODEC = {"UNCOMPRESSED": 0, "SNAPPY": 1}
+
+
+def arrow_format(t) -> str:
+    """The Arrow C format string of a pyarrow type the device decoder writes."""
+    import pyarrow as pa
+    if pa.types.is_int32(t):
+        return "i"
+    if pa.types.is_int64(t):
+        return "l"
+    if pa.types.is_float64(t):
+        return "g"
+    if pa.types.is_date32(t):
+        return "tdD"
+    if pa.types.is_decimal(t):
+        width = getattr(t, "bit_width", 128)
+        return f"d:{t.precision},{t.scale}" + (",64" if width == 64 else "")
+    raise ValueError(f"the device decoder does not write {t}")
+
+
+def column_chunk(f, metadata, rg: int, ci: int):
+    """The bytes of column chunk `ci` of row group `rg` (from its dictionary
+    page, if any, through its last page) and the decoder's description of it."""
+    cc = metadata.row_group(rg).column(ci)
+    start = cc.dictionary_page_offset if cc.has_dictionary_page and cc.dictionary_page_offset else cc.data_page_offset
+    f.seek(start)
+    data = f.read(cc.total_compressed_size)
+    if cc.physical_type not in _PHYSICAL or cc.compression not in _CODEC:
+        raise ValueError(f"column chunk of {cc.physical_type} / {cc.compression}: not taken by the device decoder")
+    desc = {"physical_type": _PHYSICAL[cc.physical_type], "codec": _CODEC[cc.compression],
+            "max_def_level": metadata.schema.column(ci).max_definition_level, "num_values": cc.num_values}
+    return data, desc
+
+
+class DeviceParquetScan:
+    """The row groups of a Parquet file that may pass a key filter, decoded on
+    the device: each yields (row group, {column: DeviceResult}, pass) where
+    `pass` is the key filter's DeviceResult "pass" column over the key column
+    (None without a filter). Row groups skipped on their statistics, or
+    after their key chunk passed no row, are counted in `stats`."""
+
+    def __init__(self, rt, path, columns: Sequence[str], key_column: Optional[str] = None, key_filter=None):
+        import pyarrow.parquet as pq
+        self.rt = rt
+        self.path = path
+        self.pf = pq.ParquetFile(path)
+        md = self.pf.metadata
+        self.columns = list(columns)
+        self.key_column = key_column
+        self.key_filter = key_filter
+        info = key_filter.info() if key_filter is not None else None
+        self.row_groups = prune_row_groups(md, key_column, info) if key_column else list(range(md.num_row_groups))
+        names = [md.schema.column(i).path for i in range(md.num_columns)]
+        self.index = {c: names.index(c) for c in set(self.columns) | ({key_column} if key_column else set())}
+        self.types = {c: self.pf.schema_arrow.field(c).type for c in self.index}
+        self.stats = {"row_groups": md.num_row_groups, "row_groups_after_statistics": len(self.row_groups),
+                      "row_groups_skipped_after_key_decode": 0, "rows": md.num_rows}
+
+    def _decode(self, f, rg, c, key_filter=None):
+        from importlib import import_module
+        kb = import_module(__name__.rsplit(".", 1)[0])
+        data, d = column_chunk(f, self.pf.metadata, rg, self.index[c])
+        return kb.parquet_decode_chunk(self.rt, data, d["physical_type"], d["codec"], d["max_def_level"],
+                                       d["num_values"], arrow_format(self.types[c]), c, key_filter)
+
+    def __iter__(self):
+        with open(self.path, "rb") as f:
+            for rg in self.row_groups:
+                cols, passing = {}, None
+                if self.key_column and self.key_filter is not None:
+                    res, info = self._decode(f, rg, self.key_column, self.key_filter)
+                    if info["passing_rows"] == 0:
+                        # no row passes (with a dictionary: no entry did): the other columns are not read
+                        self.stats["row_groups_skipped_after_key_decode"] += 1
+                        continue
+                    cols[self.key_column] = res
+                    passing = res
+                for c in self.columns:
+                    if c not in cols:
+                        cols[c] = self._decode(f, rg, c)[0]
+                yield rg, cols, passing

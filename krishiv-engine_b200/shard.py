@@ -12,7 +12,19 @@ KRV_AGG_OUTPUT_PARTIAL), `exchange` sends every state row to the rank that
 owns its key (`key_owner`) with one all-to-all per column (NCCL over NVLink
 for device tensors, gloo for host tensors), and each rank merges the states
 of the keys it owns (KRV_AGG_INPUT_STATE): every group ends on exactly one
-rank."""
+rank.
+
+A hash join whose both sides are sharded exchanges both sides by key
+(`join_owner`, `exchange_join_sides`): the top bits of the join's own row
+hash h (the bits the reference's level-0 partition takes,
+crates/krishiv-exec/src/join/keys.rs:118-128; `krv_hash_rows_device` gives
+them on the device) choose the owning rank, one all-to-all per column moves
+each side's rows there, and every rank then builds and probes its own rows:
+equal keys meet on one rank, so every output row (padded outer rows
+included) is made exactly once. Rows whose key is NULL match nothing and
+stay where they are. The ranks' runtime key filters combine by a bitwise OR
+of their Bloom words (`union_bloom`, RuntimeBloom::union_with,
+crates/krishiv-io/src/runtime_filter/bloom.rs:153)."""
 from __future__ import annotations
 
 import math
@@ -109,3 +121,47 @@ def exchange(dist, columns, owner):
         dist.all_to_all_single(dst, src, recv_l, send_l)
         out.append(dst)
     return out
+
+
+def join_owner(h, key_valid, world: int, rank: int):
+    """The rank that joins each row: the top 32 bits of its key hash `h`
+    (int64 tensor holding the uint64 h) scaled to `world`; a row whose key is
+    NULL (`key_valid` False; None: no NULLs) stays on `rank`."""
+    import torch
+    owner = (_shr(h.to(torch.int64), 32) * world) >> 32
+    if key_valid is not None:
+        owner = torch.where(key_valid.to(torch.bool), owner, torch.full_like(owner, rank))
+    return owner
+
+
+def exchange_join_sides(dist, build_columns, build_h, build_valid, probe_columns, probe_h, probe_valid):
+    """Both sides of a sharded hash join moved to the ranks that own their
+    keys (one `exchange` per side): returns (build columns, build key
+    validity, probe columns, probe key validity) of this rank. Validity
+    tensors (bool, or None for no NULLs) travel with their rows."""
+    import torch
+    world, rank = dist.get_world_size(), dist.get_rank()
+    out = []
+    for cols, h, valid in ((build_columns, build_h, build_valid), (probe_columns, probe_h, probe_valid)):
+        owner = join_owner(h, valid, world, rank)
+        extra = [valid.to(torch.uint8)] if valid is not None else []
+        moved = exchange(dist, list(cols) + extra, owner)
+        if valid is not None:
+            out += [moved[:-1], moved[-1].to(torch.bool)]
+        else:
+            out += [moved, None]
+    return tuple(out)
+
+
+def union_bloom(dist, words):
+    """The bitwise OR of every rank's Bloom words (equal-length integer
+    tensors): the filter of all ranks' keys. An all-gather and a local OR,
+    so that it runs on NCCL (which has no bitwise reduction) as on gloo."""
+    import torch
+    world = dist.get_world_size()
+    got = [torch.empty_like(words) for _ in range(world)]
+    dist.all_gather(got, words)
+    acc = got[0].clone()
+    for g in got[1:]:
+        acc |= g
+    return acc

@@ -64,7 +64,8 @@ def test_version(kb):
 STRUCTS = {"krv_join_spec": "JoinSpec", "krv_join_counters": "JoinCounters", "krv_grace_options": "GraceOptions",
            "krv_agg_expr": "AggExpr", "krv_agg_spec": "AggSpec", "krv_key_filter_options": "KeyFilterOptions",
            "krv_key_filter_info": "KeyFilterInfo", "krv_star_spec": "StarSpec", "krv_star_counters": "StarCounters",
-           "krv_gen_spec": "GenSpec", "krv_server_options": "ServerOptions", "krv_server_stats": "ServerStats"}
+           "krv_gen_spec": "GenSpec", "krv_server_options": "ServerOptions", "krv_server_stats": "ServerStats",
+           "krv_parquet_column": "ParquetColumn", "krv_parquet_info": "ParquetInfo"}
 
 
 def test_header_is_c_and_structs_match_the_binding(kb, tmp_path):

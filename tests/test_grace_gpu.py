@@ -54,12 +54,13 @@ def rows_of(res):
     return [tuple(int(cols[c][i]) if valid[c][i] else None for c in range(len(cols))) for i in range(res.rows)]
 
 
-def run(kb, rt, build, probe, jt, partitioned, budget=0, radix=3, batches=3, max_out=50_000):
+def run(kb, rt, build, probe, jt, partitioned, budget=0, radix=3, batches=3, max_out=50_000, filter_bits=None):
     bk, bval, b1, b2 = build
     pk, pval, pp = probe
     spec = kb.join_spec(jt, probe_keys=(0,), build_keys=(0,), probe_out=[0, 1], build_out=[1, 2], radix_bits=radix,
                         max_output_rows=max_out)
-    j = kb.HashJoin(rt, spec, partitioned=partitioned, device_budget=budget)
+    j = kb.HashJoin(rt, spec, partitioned=partitioned, device_budget=budget,
+                    probe_filter_bits=filter_bits if partitioned else None)
     keep = []
     for s in np.array_split(np.arange(bk.size), batches):
         db = dev(kb, [("k", bk[s], bval[s]), ("p1", b1[s], None), ("p2", b2[s], None)])
@@ -89,18 +90,29 @@ def oracle_rows(oracle, build, probe, jt):
     return collections.Counter(out)
 
 
+@pytest.mark.parametrize("filter_bits", [None, 0])
 @pytest.mark.parametrize("jt", ["left_outer", "inner"])
 @pytest.mark.parametrize("budget", [0, 2 << 20, 256 << 10])
-def test_partitioned_join_matches_the_oracle(kb, rt, oracle, jt, budget):
+def test_partitioned_join_matches_the_oracle(kb, rt, oracle, jt, budget, filter_bits):
     """budget 0: every partition resident; 2 MiB: some spill (and rows of
     resident partitions are deferred once a call's output reaches its cap);
-    256 KiB: all spill and split again at finish."""
+    256 KiB: all spill and split again at finish. With the Bloom filter of
+    the partition pass (the default) and without it (0 bits)."""
     build, probe = make()
-    got, j = run(kb, rt, build, probe, jt, True, budget=budget)
+    got, j = run(kb, rt, build, probe, jt, True, budget=budget, filter_bits=filter_bits)
     want = oracle_rows(oracle, build, probe, jt)
     assert got == want
     c = j.counters()
     assert c["output_rows"] == sum(want.values())
+    # about 60% of the probe rows have a key no build row holds
+    filtered = j.filtered_probe_rows()
+    if filter_bits == 0:
+        assert filtered == 0
+    elif budget == 0:
+        bk, bval = build[0], build[1]
+        pk, pval = probe[0], probe[1]
+        absent = int((pval & ~np.isin(pk, bk[bval])).sum())
+        assert 0.5 * absent < filtered <= absent  # no false negatives: only absent keys are ruled out
     if budget == 256 << 10:
         assert j.spilled_partitions() == 8 and c["partitions"] > 8  # spilled, then split
     if budget == 0:

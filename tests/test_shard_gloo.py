@@ -190,3 +190,102 @@ def test_key_owner_is_balanced_and_stable():
         counts = torch.bincount(o, minlength=world).tolist()
         assert max(counts) - min(counts) < 0.05 * len(k) / world * world
         assert torch.equal(o, shard.key_owner(k.clone(), world))
+
+
+def _join_rows(rank, n_build=20_000, n_probe=60_000):
+    """One rank's own build rows (k, b) and probe rows (k, p): keys with
+    duplicates and 2% NULLs, payloads that name the row uniquely."""
+    import numpy as np
+    rng = np.random.default_rng(300 + rank)
+    bk = rng.integers(0, 30_000, n_build).astype(np.int64)
+    bv = rng.random(n_build) > 0.02
+    pk = rng.integers(0, 60_000, n_probe).astype(np.int64)
+    pv = rng.random(n_probe) > 0.02
+    b = np.arange(n_build, dtype=np.int64) + rank * 10**9
+    p = np.arange(n_probe, dtype=np.int64) + rank * 10**9
+    return bk, bv, b, pk, pv, p
+
+
+def _join_output(oracle, jt, bk, bv, b, pk, pv, p):
+    """The join's output rows (probe key or None, p, b or None) as a multiset
+    (the oracle joins; the device's HashJoin gives the same rows)."""
+    import collections
+    pi, bi = oracle.hash_join(jt, [(bk, bv.astype("uint8"), False)],
+                              [(pk, pv.astype("uint8"), False)])
+    out = collections.Counter()
+    for i, j in zip(pi.tolist(), bi.tolist()):
+        out[(int(pk[i]) if pv[i] else None, int(p[i]), int(b[j]) if j >= 0 else None)] += 1
+    return out
+
+
+def _join_rank(rank, world, port, jt, queue):
+    """One rank of a sharded hash join: its own rows of both sides, hashed by
+    the join's row hash h (the oracle's restatement; krv_hash_rows_device on
+    the device), exchanged by key owner, joined locally; and the union of the
+    ranks' Bloom filters."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import oracle as O
+    shard = importlib.import_module("krishiv-engine_b200.shard")
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        bk, bv, b, pk, pv, p = _join_rows(rank)
+        hb = O.row_hash([(bk, bv.astype(np.uint8), False)]).view(np.int64)
+        hp = O.row_hash([(pk, pv.astype(np.uint8), False)]).view(np.int64)
+        rb, rbv, rp, rpv = shard.exchange_join_sides(
+            dist, [torch.tensor(bk), torch.tensor(b)], torch.tensor(hb), torch.tensor(bv),
+            [torch.tensor(pk), torch.tensor(p)], torch.tensor(hp), torch.tensor(pv))
+        lbk, lb = rb[0].numpy(), rb[1].numpy()
+        lpk, lp = rp[0].numpy(), rp[1].numpy()
+        lbv, lpv = rbv.numpy(), rpv.numpy()
+        # every non-NULL key landed on its owner
+        own_b = shard.join_owner(torch.tensor(O.row_hash([(lbk, lbv.astype(np.uint8), False)]).view(np.int64)),
+                                 torch.tensor(lbv), world, rank)
+        own_p = shard.join_owner(torch.tensor(O.row_hash([(lpk, lpv.astype(np.uint8), False)]).view(np.int64)),
+                                 torch.tensor(lpv), world, rank)
+        mine = bool((own_b == rank).all()) and bool((own_p == rank).all())
+        out = _join_output(O, jt, lbk, lbv, lb, lpk, lpv, lp)
+        nbytes = O.bloom_bytes_for(40_000, 0.01)
+        words = torch.tensor(O.bloom_build(O.xxh64_int(bk[bv]), nbytes).view(np.int32))
+        union = shard.union_bloom(dist, words).numpy().view(np.uint32)
+        dist.barrier()
+        queue.put((rank, out, mine, union, len(lbk), len(lpk)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+@pytest.mark.parametrize("jt", [0, 1])  # inner, left outer
+def test_sharded_join_exchange_on_two_gloo_ranks(oracle, jt):
+    """Both sides exchanged by the owner of their key hash, then joined on
+    each rank: the union of the ranks' outputs is the one-rank join of all
+    rows (NULL keys never match; left outer pads every unmatched probe row
+    once), every key sits on its owner, and the OR of the ranks' Bloom words
+    is the filter of all build keys."""
+    import numpy as np
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.SimpleQueue()
+    port = _free_port()
+    procs = [ctx.Process(target=_join_rank, args=(r, 2, port, jt, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    # read the results before joining: a result larger than the pipe's buffer
+    # holds its rank in put() until it is read
+    got = [q.get() for _ in range(2)]
+    for p in procs:
+        p.join(timeout=240)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    rows = [_join_rows(r) for r in range(2)]
+    cat = [np.concatenate([rows[0][i], rows[1][i]]) for i in range(6)]
+    want = _join_output(oracle, jt, *cat)
+    total = got[0][1] + got[1][1]
+    assert total == want
+    assert all(g[2] for g in got)
+    assert sum(g[4] for g in got) == len(cat[0]) and sum(g[5] for g in got) == len(cat[3])
+    nbytes = oracle.bloom_bytes_for(40_000, 0.01)
+    all_words = oracle.bloom_build(oracle.xxh64_int(cat[0][cat[1]]), nbytes)
+    assert np.array_equal(got[0][3], all_words) and np.array_equal(got[1][3], all_words)
