@@ -271,8 +271,10 @@ int64_t krv_join_spilled_partitions(const krv_join *j);
 int64_t krv_join_filtered_probe_rows(const krv_join *j);
 
 /* ---- grouped hash aggregate ---------------------------------------------- */
-/* AggregateFunction (aggregate/mod.rs:134), the core five. MIN/MAX take
- * decimals of precision up to 18 (decimal64 or decimal128 carrier). */
+/* AggregateFunction (aggregate/mod.rs:134), the core five. MIN/MAX of a
+ * decimal128 column of precision 19 to 38 keep all 128 bits (the reference's
+ * MinMax over Values::Int(i128), aggregate/accumulator.rs:238-248); such an
+ * aggregate runs its global-table kernels only. */
 #define KRV_AGG_COUNT_STAR 0
 #define KRV_AGG_COUNT 1
 #define KRV_AGG_SUM 2

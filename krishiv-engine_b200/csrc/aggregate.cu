@@ -44,7 +44,10 @@ constexpr uint32_t kOverflowGid = 0xFFFFFFFEu;
 constexpr uint32_t kNullGid = 0, kMarkerGid = 1, kFirstGid = 2;
 constexpr int kMaxValueCols = 16;
 
-enum : int32_t { F_SUM = 1, F_MIN = 2, F_MAX = 4 };
+// F_WIDE: MIN/MAX of a decimal128 column of precision 19 to 38, kept in 16
+// bytes (lo, hi) and updated by 128-bit compare-and-swap; such a plan runs
+// the global-table kernels only.
+enum : int32_t { F_SUM = 1, F_MIN = 2, F_MAX = 4, F_WIDE = 8 };
 
 struct AggColDev {
     const void *data;
@@ -84,10 +87,61 @@ __device__ __forceinline__ long long key_at(const KeyIn &k, int64_t i) {
                         : static_cast<const long long *>(k.data)[i];
 }
 
+// 128-bit compare-and-swap (atom.cas.b128) on the 16-byte aligned pair
+// p[0] (low word), p[1] (high word): lo/hi in, the old value out.
+__device__ __forceinline__ void cas128(unsigned long long *p, unsigned long long &lo, unsigned long long &hi,
+                                       unsigned long long nlo, unsigned long long nhi) {
+    asm volatile(
+        "{\n\t.reg .b128 cmp, swp, old;\n\t"
+        "mov.b128 cmp, {%0, %1};\n\t"
+        "mov.b128 swp, {%3, %4};\n\t"
+        "atom.cas.b128 old, [%2], cmp, swp;\n\t"
+        "mov.b128 {%0, %1}, old;\n\t}"
+        : "+l"(lo), "+l"(hi)
+        : "l"(p), "l"(nlo), "l"(nhi)
+        : "memory");
+}
+__device__ __forceinline__ bool i128_less(long long ahi, unsigned long long alo, long long bhi, unsigned long long blo) {
+    return ahi < bhi || (ahi == bhi && alo < blo);
+}
+// MIN (or MAX) of the signed 128-bit value (vlo, vhi) into p: read the pair
+// atomically (a compare-and-swap that changes nothing), then swap while the
+// value is still better. Every failed swap saw a better value stored, so the
+// loop ends; the bound is a guard only.
+__device__ __forceinline__ void atomic_minmax_i128(unsigned long long *p, unsigned long long vlo, long long vhi,
+                                                   bool is_max) {
+    unsigned long long clo = 0, chi = 0;
+    cas128(p, clo, chi, 0ull, 0ull);
+    for (int it = 0; it < (1 << 20); it++) {
+        const bool better = is_max ? i128_less((long long)chi, clo, vhi, vlo) : i128_less(vhi, vlo, (long long)chi, clo);
+        if (!better) return;
+        unsigned long long olo = clo, ohi = chi;
+        cas128(p, olo, ohi, vlo, (unsigned long long)vhi);
+        if (olo == clo && ohi == chi) return;
+        clo = olo;
+        chi = ohi;
+    }
+}
+__device__ __forceinline__ void plain_minmax_i128(unsigned long long *p, unsigned long long vlo, long long vhi,
+                                                  bool is_max) {
+    const bool better = is_max ? i128_less((long long)p[1], p[0], vhi, vlo) : i128_less(vhi, vlo, (long long)p[1], p[0]);
+    if (better) {
+        p[0] = vlo;
+        p[1] = (unsigned long long)vhi;
+    }
+}
+
 __device__ __forceinline__ void init_record(const AggPlanDev &P, uint8_t *r) {
     for (int b = 0; b < P.rec; b += 8) *reinterpret_cast<unsigned long long *>(r + b) = 0ull;
     for (int c = 0; c < P.ncols; c++) {
         const AggColDev &C = P.c[c];
+        if (C.flags & F_WIDE) {
+            unsigned long long *mn = reinterpret_cast<unsigned long long *>(r + C.off_min);
+            unsigned long long *mx = reinterpret_cast<unsigned long long *>(r + C.off_max);
+            if (C.flags & F_MIN) mn[0] = ~0ull, mn[1] = (unsigned long long)LLONG_MAX;
+            if (C.flags & F_MAX) mx[0] = 0ull, mx[1] = (unsigned long long)LLONG_MIN;
+            continue;
+        }
         if (C.flags & F_MIN) {
             if (C.type == (int)Type::I32 || C.type == (int)Type::Date32) *reinterpret_cast<int *>(r + C.off_min) = INT_MAX;
             else if (C.type == (int)Type::F64) *reinterpret_cast<unsigned long long *>(r + C.off_min) = ~0ull;
@@ -128,9 +182,16 @@ __device__ __forceinline__ void update_record(const AggPlanDev &P, uint8_t *r, i
             if (C.flags & F_SUM)
                 atomic_add_i128(reinterpret_cast<unsigned long long *>(r + C.off_sum),
                                 reinterpret_cast<long long *>(r + C.off_sum + 8), p[0], p[1]);
-            // MIN/MAX only for precision <= 18: the value is its low word
-            if (C.flags & F_MIN) atomicMin(reinterpret_cast<long long *>(r + C.off_min), p[0]);
-            if (C.flags & F_MAX) atomicMax(reinterpret_cast<long long *>(r + C.off_max), p[0]);
+            if (C.flags & F_WIDE) {
+                if (C.flags & F_MIN)
+                    atomic_minmax_i128(reinterpret_cast<unsigned long long *>(r + C.off_min), p[0], p[1], false);
+                if (C.flags & F_MAX)
+                    atomic_minmax_i128(reinterpret_cast<unsigned long long *>(r + C.off_max), p[0], p[1], true);
+            } else {
+                // precision <= 18: the value is its low word
+                if (C.flags & F_MIN) atomicMin(reinterpret_cast<long long *>(r + C.off_min), p[0]);
+                if (C.flags & F_MAX) atomicMax(reinterpret_cast<long long *>(r + C.off_max), p[0]);
+            }
         } else {  // I64, Dec64
             const long long v = static_cast<const long long *>(C.data)[i];
             if (C.flags & F_SUM)
@@ -190,13 +251,18 @@ __device__ __forceinline__ void update_record_plain(const AggPlanDev &P, uint8_t
                 *lo = old + (unsigned long long)p[0];
                 *hi += p[1] + (long long)(*lo < old);
             }
-            if (C.flags & F_MIN) {
-                long long *m = reinterpret_cast<long long *>(r + C.off_min);
-                *m = p[0] < *m ? p[0] : *m;
-            }
-            if (C.flags & F_MAX) {
-                long long *m = reinterpret_cast<long long *>(r + C.off_max);
-                *m = p[0] > *m ? p[0] : *m;
+            if (C.flags & F_WIDE) {
+                if (C.flags & F_MIN) plain_minmax_i128(reinterpret_cast<unsigned long long *>(r + C.off_min), p[0], p[1], false);
+                if (C.flags & F_MAX) plain_minmax_i128(reinterpret_cast<unsigned long long *>(r + C.off_max), p[0], p[1], true);
+            } else {
+                if (C.flags & F_MIN) {
+                    long long *m = reinterpret_cast<long long *>(r + C.off_min);
+                    *m = p[0] < *m ? p[0] : *m;
+                }
+                if (C.flags & F_MAX) {
+                    long long *m = reinterpret_cast<long long *>(r + C.off_max);
+                    *m = p[0] > *m ? p[0] : *m;
+                }
             }
         } else {  // I64, Dec64
             const long long v = static_cast<const long long *>(C.data)[i];
@@ -253,6 +319,17 @@ __device__ __forceinline__ void merge_record(const AggPlanDev &P, uint8_t *dst, 
                                 reinterpret_cast<long long *>(dst + C.off_sum + 8),
                                 *reinterpret_cast<const long long *>(src + C.off_sum),
                                 *reinterpret_cast<const long long *>(src + C.off_sum + 8));
+            if (C.flags & F_WIDE) {
+                if (C.flags & F_MIN) {
+                    const long long *m = reinterpret_cast<const long long *>(src + C.off_min);
+                    atomic_minmax_i128(reinterpret_cast<unsigned long long *>(dst + C.off_min), (unsigned long long)m[0], m[1], false);
+                }
+                if (C.flags & F_MAX) {
+                    const long long *m = reinterpret_cast<const long long *>(src + C.off_max);
+                    atomic_minmax_i128(reinterpret_cast<unsigned long long *>(dst + C.off_max), (unsigned long long)m[0], m[1], true);
+                }
+                continue;
+            }
             if (C.flags & F_MIN)
                 atomicMin(reinterpret_cast<long long *>(dst + C.off_min), *reinterpret_cast<const long long *>(src + C.off_min));
             if (C.flags & F_MAX)
@@ -1687,7 +1764,11 @@ __global__ void __launch_bounds__(256) finalize_kernel(AggPlanDev P, OutPlanDev 
                         const bool i32 = C.type == (int)Type::I32 || C.type == (int)Type::Date32;
                         if (X.func == KRV_AGG_MIN || X.func == KRV_AGG_MAX) {
                             const int off = X.func == KRV_AGG_MIN ? C.off_min : C.off_max;
-                            if (i32) static_cast<int *>(X.dst)[r] = *reinterpret_cast<const int *>(rec + off);
+                            if (C.flags & F_WIDE) {
+                                const long long *m = reinterpret_cast<const long long *>(rec + off);
+                                static_cast<long long *>(X.dst)[2 * r] = m[0];
+                                static_cast<long long *>(X.dst)[2 * r + 1] = m[1];
+                            } else if (i32) static_cast<int *>(X.dst)[r] = *reinterpret_cast<const int *>(rec + off);
                             else if (C.type == (int)Type::F64)
                                 static_cast<double *>(X.dst)[r] =
                                     f64_from_order_key(*reinterpret_cast<const unsigned long long *>(rec + off));
@@ -1954,12 +2035,11 @@ void HashAggregate::plan(const DevBatch &b) {
         if (!state) {
             if (x.function == KRV_AGG_COUNT_STAR) continue;
             const DType t = check_col(x.column);
-            if (t.id == Type::Dec128 && t.precision > 18 && (x.function == KRV_AGG_MIN || x.function == KRV_AGG_MAX))
-                fail(KRV_UNSUPPORTED, "MIN/MAX of decimals of precision 19 to 38 on the GPU aggregate");
             int32_t f = 0;
             if (x.function == KRV_AGG_SUM || x.function == KRV_AGG_AVG) f = F_SUM;
             if (x.function == KRV_AGG_MIN) f = F_MIN;
             if (x.function == KRV_AGG_MAX) f = F_MAX;
+            if (t.id == Type::Dec128 && t.precision > 18 && (f & (F_MIN | F_MAX))) f |= F_WIDE;
             expr_col_[e] = plan_col(x.column, f);
             continue;
         }
@@ -1990,9 +2070,8 @@ void HashAggregate::plan(const DevBatch &b) {
             break;
         case KRV_AGG_MIN:
         case KRV_AGG_MAX:
-            if (t.id == Type::Dec128 && t.precision > 18)
-                fail(KRV_UNSUPPORTED, "MIN/MAX of decimals of precision 19 to 38 on the GPU aggregate");
-            expr_col_[e] = plan_col(x.column, x.function == KRV_AGG_MIN ? F_MIN : F_MAX);
+            expr_col_[e] = plan_col(x.column, (x.function == KRV_AGG_MIN ? F_MIN : F_MAX) |
+                                                  (t.id == Type::Dec128 && t.precision > 18 ? F_WIDE : 0));
             break;
         }
     }
@@ -2010,6 +2089,16 @@ void HashAggregate::plan(const DevBatch &b) {
             C.off_sum = off;
             off += 16;
         }
+        if (C.flags & F_WIDE) {  // 128-bit MIN/MAX: 16-byte aligned pairs
+            if (C.flags & F_MIN) {
+                C.off_min = off;
+                off += 16;
+            }
+            if (C.flags & F_MAX) {
+                C.off_max = off;
+                off += 16;
+            }
+        }
     }
     P_.off_rows = off;
     off += 8;
@@ -2022,7 +2111,7 @@ void HashAggregate::plan(const DevBatch &b) {
             C.off_sum = off;
             off += 8;
         }
-        if (!i32) {
+        if (!i32 && !(C.flags & F_WIDE)) {
             if (C.flags & F_MIN) {
                 C.off_min = off;
                 off += 8;
@@ -2055,6 +2144,8 @@ void HashAggregate::plan(const DevBatch &b) {
     while ((e * 2) * per + 64 <= std::min(rt_->max_smem_optin, 200 * 1024)) e *= 2;
     smem_entries_ = e >= 64 ? e : 0;
     if (smem_entries_ == 0) mode_ = KRV_AGG_MODE_GLOBAL;
+    for (int c = 0; c < P_.ncols; c++)
+        if (P_.c[c].flags & F_WIDE) mode_ = KRV_AGG_MODE_GLOBAL;  // 128-bit MIN/MAX: the global-table kernels
     plan_row_records();
     const uint64_t hint = spec_.expected_groups > 0 ? (uint64_t)spec_.expected_groups : 65536;
     alloc_table(std::max<uint64_t>(1024, next_pow2((uint64_t)(hint * 2))));

@@ -59,6 +59,7 @@ struct PartArgs {
     int filter_mode;    // kFilterNone, kFilterInsert (build side) or kFilterTest (probe side)
     uint32_t *bloom;    // blocked Bloom filter over h: 8 words (one 32-byte block) per key
     uint64_t bloom_blocks;
+    uint8_t *bucket;    // with kFilterTest: each row's bucket, written by the histogram pass for the scatter
     PartCol c[kMaxCols];
     int ncols;
 };
@@ -83,7 +84,9 @@ __global__ void __launch_bounds__(256) part_hist_kernel(PartArgs A, unsigned lon
     __syncthreads();
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += (int64_t)gridDim.x * blockDim.x) {
         uint64_t h;
-        atomicAdd(&s_hist[part_of(A, r, h)], 1u);
+        const int p = part_of(A, r, h);
+        atomicAdd(&s_hist[p], 1u);
+        if (A.bucket) A.bucket[r] = (uint8_t)p;  // the scatter reads it: no second hash or filter lookup
     }
     __syncthreads();
     for (int p = threadIdx.x; p <= A.nparts + 1; p += blockDim.x)
@@ -115,7 +118,7 @@ __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(PartArgs A, 
             const int i = u * kPartThreads + threadIdx.x;
             const int64_t r = row0 + i;
             uint64_t h = 0;
-            part[u] = r < A.n ? part_of(A, r, h) : -1;
+            part[u] = r >= A.n ? -1 : A.bucket ? (int)A.bucket[r] : part_of(A, r, h);
             if (A.filter_mode == kFilterInsert) {
                 // four keys per round, each key's 8 words set by 8 lanes
                 unsigned todo = __ballot_sync(0xFFFFFFFFu, part[u] >= 0 && part[u] < A.nparts);
@@ -869,6 +872,11 @@ class GraceJoin {
         A.ncols = (int)b.cols.size();
         const int nb = nparts + 2;  // partitions, the NULL bucket, the filtered bucket
         DBuf ctr(rt_, (size_t)nb * 8 * 2);
+        DBuf bucket;
+        if (filter_mode == kFilterTest && b.rows > 0) {
+            bucket = DBuf(rt_, (size_t)b.rows);
+            A.bucket = bucket.as<uint8_t>();
+        }
         unsigned long long *hist = ctr.as<unsigned long long>(), *cursor = hist + nb;
         KRV_CUDA(cudaMemsetAsync(hist, 0, (size_t)nb * 8, rt_->stream));
         part_hist_kernel<<<grid_for(rt_, b.rows, 256, 8), 256, 0, rt_->stream>>>(A, hist);

@@ -737,7 +737,7 @@ typedef struct {
     double fseq;     /* sequential += (accumulator/fold.rs:401-426) */
     double fs, fc;   /* Neumaier compensated sum */
     int64_t count;
-    int64_t imin, imax;
+    i128 imin, imax;  /* MinMax holds Values::Int(i128) (aggregate/accumulator.rs:238-248) */
     double fmin, fmax;
     uint8_t seen, overflow;
 } acc_t;
@@ -842,10 +842,10 @@ int64_t orc_hash_aggregate(const void *key, const uint8_t *key_valid, int32_t ke
             } else {
                 i128 v = value_i128(c, i);
                 if (!a->seen) {
-                    a->imin = a->imax = (int64_t)v;
+                    a->imin = a->imax = v;
                 } else {
-                    if ((int64_t)v < a->imin) a->imin = (int64_t)v;
-                    if ((int64_t)v > a->imax) a->imax = (int64_t)v;
+                    if (v < a->imin) a->imin = v;
+                    if (v > a->imax) a->imax = v;
                 }
                 if (!is_dec && x->func == ORC_SUM) {
                     /* SumInt: ANSI raises on overflow, else wraps */
@@ -905,8 +905,14 @@ int64_t orc_hash_aggregate(const void *key, const uint8_t *key_valid, int32_t ke
             case ORC_MIN:
             case ORC_MAX:
                 if (!a->seen) break;
-                if (is_float) o->f64[gi] = x->func == ORC_MIN ? a->fmin : a->fmax;
-                else o->i64[gi] = x->func == ORC_MIN ? a->imin : a->imax;
+                if (is_float) {
+                    o->f64[gi] = x->func == ORC_MIN ? a->fmin : a->fmax;
+                } else {
+                    const i128 m = x->func == ORC_MIN ? a->imin : a->imax;
+                    o->i64[gi] = (int64_t)m;
+                    o->lo[gi] = (uint64_t)m;
+                    o->hi[gi] = (int64_t)(m >> 64);
+                }
                 o->valid[gi] = 1;
                 break;
             case ORC_AVG:

@@ -5,6 +5,8 @@ MIN/MAX and COUNT are exact."""
 import os
 from decimal import Decimal
 
+import decimal
+
 import numpy as np
 import pyarrow as pa
 import pytest
@@ -197,8 +199,7 @@ def test_device_path(kb, rt, oracle):
 def test_decimal128_columns(kb, rt, oracle, mode):
     """decimal128(15,2) values (the carrier Spark-written Arrow files use for
     decimal(15,2)), negative and NULL: SUM, COUNT, MIN, MAX and AVG exact
-    against the oracle; MIN/MAX keep the input type. MIN/MAX of a
-    decimal(20,2) column are not taken (UNSUPPORTED)."""
+    against the oracle; MIN/MAX keep the input type."""
     rng = np.random.default_rng(41)
     n = 200_000
     key = rng.integers(0, 3000, n, dtype=np.int64)
@@ -232,8 +233,73 @@ def test_decimal128_columns(kb, rt, oracle, mode):
                 assert int(vals[e].scaleb(scale)) == int(r["lo"][gi]) + (int(r["hi"][gi]) << 64), (f, k)
             else:
                 assert int(vals[e].scaleb(2)) == int(r["i64"][gi]), (f, k)
-    wide = batch(k=pa.array([1, 2]), d=pa.array([Decimal(1), Decimal(2)], pa.decimal128(20, 2)))
-    a = kb.HashAggregate(rt, kb.agg_spec(0, [("min", 1)]))
-    with pytest.raises(kb.KrvError) as e:
-        a.push(wide)
-    assert e.value.status == kb.UNSUPPORTED
+
+
+def dec38(rng, n):
+    """decimal(38,4) words (lo, hi per value) across the 128-bit range: large
+    values of both signs, values inside and at the edges of int64, ties."""
+    hi = rng.integers(-2**40, 2**40, n, dtype=np.int64)
+    lo = rng.integers(-2**63, 2**63 - 1, n, dtype=np.int64)
+    small = rng.random(n) < 0.4  # int64 values: hi is lo's sign
+    lo[small] = rng.choice(np.array([-2**63, -1, 0, 1, 2**63 - 1], np.int64), int(small.sum()))
+    hi[small] = np.where(lo[small] < 0, -1, 0)
+    return np.stack([lo, hi], 1).reshape(-1)
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_decimal38_min_max(kb, rt, oracle, mode):
+    """MIN/MAX of decimal(38,4) values beyond int64 (both signs, NULLs, three
+    batches) equal the oracle's 128-bit MinMax (Values::Int(i128),
+    aggregate/accumulator.rs:238-248); SUM and COUNT beside them exact. The
+    same aggregates run in two phases (partial states, then their merge)
+    give the same answer."""
+    rng = np.random.default_rng(77)
+    n = 150_000
+    key = rng.integers(0, 700, n, dtype=np.int64)
+    words = dec38(rng, n)
+    valid = rng.random(n) > 0.03
+    t = pa.decimal128(38, 4)
+    dec = pa.Array.from_buffers(t, n, [pa.py_buffer(np.packbits(valid, bitorder="little").tobytes()),
+                                       pa.py_buffer(words.tobytes())])
+    b = batch(k=pa.array(key), d=dec)
+    aggs = [("min", 1), ("max", 1), ("sum", 1), ("count", 1)]
+    out = run(kb, rt, b, 0, aggs, mode, batches=3)
+    assert [out.schema.field(i).type for i in range(1, 5)] == [t, t, pa.decimal128(38, 4), pa.int64()]
+    cols = [{"values": words, "valid": valid.astype(np.uint8), "type": oracle.T_DEC128, "precision": 38, "scale": 4}]
+    F = {"sum": oracle.SUM, "count": oracle.COUNT, "min": oracle.MIN, "max": oracle.MAX}
+    keys, _, res = oracle.hash_aggregate(key, None, cols, [(F[f], 0) for f, _ in aggs])
+    order = {int(k): i for i, k in enumerate(keys)}
+
+    def check(got):
+        assert sorted(got) == sorted(order)
+        beyond = 0
+        for k, vals in got.items():
+            gi = order[k]
+            for e, (f, _) in enumerate(aggs):
+                r = res[e]
+                if not r["valid"][gi]:
+                    assert vals[e] is None
+                    continue
+                if f == "count":
+                    assert vals[e] == r["i64"][gi]
+                    continue
+                want = int(r["lo"][gi]) + (int(r["hi"][gi]) << 64)
+                # exact: 38 digits need more than the default 28-digit context
+                assert int(vals[e].scaleb(4, decimal.Context(prec=80))) == want, (f, k)
+                beyond += f in ("min", "max") and not -2**63 <= want < 2**63
+        assert beyond > 100  # the extremes are beyond int64
+
+    check({k: r for k, *r in zip(*[c.to_pylist() for c in out.columns])})
+    # two phases: each batch's partial states, then one merge of them all
+    parts = []
+    for s_ in np.array_split(np.arange(n), 3):
+        pa_ = kb.HashAggregate(rt, kb.agg_spec(0, aggs, mode=mode, partial=True))
+        pa_.push(b.slice(int(s_[0]), len(s_)))
+        pa_.finish()
+        parts += pa_.result()
+    states = pa.Table.from_batches(parts).combine_chunks().to_batches()[0]
+    m = kb.HashAggregate(rt, kb.agg_spec(0, kb.merging(aggs, 1, [t] * 4), mode=mode))
+    m.push(states)
+    m.finish()
+    merged = pa.Table.from_batches(m.result())
+    check({k: r for k, *r in zip(*[c.to_pylist() for c in merged.columns])})
