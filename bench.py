@@ -1,7 +1,7 @@
 """Benchmark of the B200 join + runtime-filter + aggregate path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload star|join|agg] [--scale S]
+                    [--workload star|join|agg|serve|grace|parquet] [--scale S]
 
 Default workload (`star`): the star join with runtime Bloom filters --
 fact 300M rows {fk_a in [0, 20M), fk_b in [0, 1M), price, discount}, dim_a
@@ -773,6 +773,116 @@ def run_grace(args, kb, W, rt, rank, world, pg, device):
     return out
 
 
+def run_parquet(args, kb, W, rt, rank, world, pg, device):
+    """Parquet column chunks decoded on the device: a file of 64M rows x
+    (k int64 in [0, 100K) with 2% NULLs, dictionary encoded; x float64, PLAIN),
+    Snappy, row groups of 8M rows, written once to a temporary file. One
+    step = every row group's two chunks decoded (their bytes read into
+    page-locked host memory beforehand, crossing to the device inside the
+    step) with a 5%-of-keys runtime filter evaluated on k's encoded pages.
+    The CPU baseline is pyarrow's reader (Arrow C++, all host threads)
+    decoding the same columns from the same bytes in memory."""
+    import tempfile
+
+    import numpy as np
+    import pyarrow as pa
+    import pyarrow.parquet as pq
+    import torch
+    S = importlib.import_module("krishiv-engine_b200.scan")
+    n = int(64_000_000 * args.scale)
+    rng = np.random.default_rng(5)
+    k = rng.integers(0, 100_000, n).astype(np.int64)
+    kv = rng.random(n) >= 0.02
+    x = rng.random(n)
+    table = pa.table({"k": pa.array(k, mask=~kv), "x": x})
+    path = os.path.join(tempfile.mkdtemp(), "bench.parquet")
+    pq.write_table(table, path, compression=args.parquet_codec, row_group_size=8 << 20, use_dictionary=["k"])
+    del table
+    md = pq.ParquetFile(path).metadata
+    chunks = []
+    with open(path, "rb") as f:
+        for rg in range(md.num_row_groups):
+            for ci, fmt in ((0, "l"), (1, "g")):
+                data, d = S.column_chunk(f, md, rg, ci)
+                host = torch.empty(len(data), dtype=torch.uint8, pin_memory=True)
+                host.numpy()[:] = np.frombuffer(data, dtype=np.uint8)
+                chunks.append((host.numpy(), d, fmt, ci == 0))
+    encoded = sum(c[0].size for c in chunks)
+    build = rng.choice(100_000, 5_000, replace=False).astype(np.int64)
+    kf = kb.KeyFilter.build(rt, pa.record_batch([pa.array(build)], names=["k"]), 0)
+    stream = torch.cuda.current_stream()
+
+    per_chunk = []  # host wall ms of each call (each call waits for its kernels)
+
+    def step():
+        passing, keep = 0, []
+        per_chunk.clear()
+        for buf, d, fmt, key in chunks:
+            t0 = time.perf_counter()
+            res, info = kb.parquet_decode_chunk(rt, buf, d["physical_type"], d["codec"], d["max_def_level"],
+                                                d["num_values"], fmt, "", kf if key else None)
+            per_chunk.append((fmt, info["pages"], round((time.perf_counter() - t0) * 1e3, 2)))
+            keep.append(res)
+            if key:
+                passing += info["passing_rows"]
+        return passing, keep
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = rt.launches
+    times = []
+    with Clocks(device) as clk:
+        for _ in range(args.steps):
+            s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_.record(stream)
+            passing, keep = step()
+            e_.record(stream)
+            torch.cuda.synchronize()
+            times.append(s_.elapsed_time(e_))
+            del keep
+    ms = max_over_ranks(pg, statistics.median(times), device)
+    # the same filter evaluated on the decoded keys (KeyFilter::evaluate over pyarrow's decode of k)
+    import pyarrow.compute as pc
+    ev = kf.evaluate(pa.record_batch([pa.array(k, mask=~kv)], names=["k"]), 0)
+    want = int(pc.sum(ev).as_py() or 0)
+    decoded = n * 8 * 2 + n // 8
+    peak, kind = hbm_peak()
+    out = {"metric": "Parquet column chunks decoded on the device (rows per second, two columns, filter on the key)",
+           "value": world * n / (ms * 1e-3) / 1e6, "unit": "Mrows/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "int64 / float64", "data": "synthetic (seeded numpy, written by pyarrow)",
+           "config": {"workload": f"{n} rows x (k int64 dictionary 2% NULLs, x float64 PLAIN), "
+                                  f"{args.parquet_codec}, row groups of 8M rows", "encoded_bytes": encoded,
+                      "decoded_bytes": decoded,
+                      "filter": "5,000 of 100,000 keys, evaluated once per dictionary entry",
+                      "transfer": "chunk bytes in page-locked host memory, copied to the device inside the step"},
+           "encoded_GBps": encoded / (ms * 1e-3) / 1e9, "decoded_GBps": decoded / (ms * 1e-3) / 1e9,
+           "steps_ms": [round(t, 2) for t in times],
+           "filter_agrees": passing == want, "passing_rows": passing,
+           "calls_ms": [list(c) for c in per_chunk],
+           "gpu_launches": (rt.launches - launches0) // max(1, args.steps),
+           "roofline": {"bound": "hbm", "achieved": (encoded * 2 + decoded) / (ms * 1e-3) / 1e9, "peak": peak,
+                        "peak_source": kind, "unit": "GB/s", "frac": (encoded * 2 + decoded) / (ms * 1e-3) / 1e9 / peak,
+                        "traffic": None, "note": "encoded bytes staged (read + write) + decoded column bytes written; "
+                                                 "the host-to-device copy of the encoded bytes is inside the step"},
+           "clocks": clk.summary()}
+    if rank == 0 and not args.no_cpu:
+        import pyarrow as pa_
+        raw = open(path, "rb").read()
+        t = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            pq.read_table(pa_.BufferReader(raw), columns=["k", "x"], use_threads=True)
+            t.append(time.perf_counter() - t0)
+        cpu_ms = statistics.median(t) * 1e3
+        out["cpu_baseline"] = {"value": n / (cpu_ms * 1e-3) / 1e6, "unit": "Mrows/s", "cores": os.cpu_count(),
+                               "kind": "pyarrow", "sample": "pyarrow 24 (Arrow C++) read_table of the same two columns "
+                                                          "from the file's bytes in memory, all host threads, median of 3"}
+    os.remove(path)
+    return out
+
+
 def profile_traffic(name, rows):
     """DRAM bytes (read + write) of one launch of `name` over `rows` fact
     rows, from the committed ncu summary profiles/<name>_traffic.txt (line
@@ -933,7 +1043,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["star", "join", "agg", "serve", "grace"], default="star")
+    ap.add_argument("--workload", choices=["star", "join", "agg", "serve", "grace", "parquet"], default="star")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--fact-scale", type=float, default=None,
                     help="size the fact table alone (profiling small cases with full dimensions)")
@@ -951,6 +1061,8 @@ def main():
     ap.add_argument("--grace-budget", type=int, default=24 << 30, help="grace: device budget of the join")
     ap.add_argument("--max-load", type=float, default=0.0, help="join, grace: hash table load factor (0: default)")
     ap.add_argument("--radix-bits", type=int, default=0, help="grace: level-0 partition bits (0: chosen)")
+    ap.add_argument("--parquet-codec", default="SNAPPY", choices=["SNAPPY", "NONE"],
+                    help="parquet: the file's compression codec")
     ap.add_argument("--grace-filter-bits", type=int, default=10,
                     help="grace: bits per build key of the partition pass's Bloom filter (0: none)")
     args = ap.parse_args()
@@ -1003,7 +1115,8 @@ def main():
     kb = importlib.import_module("krishiv-engine_b200")
     W = importlib.import_module("krishiv-engine_b200.workloads")
     rt = kb.Runtime.on_torch_stream(local)
-    runner = {"star": run_star, "join": run_join, "agg": run_agg, "serve": run_serve, "grace": run_grace}[args.workload]
+    runner = {"star": run_star, "join": run_join, "agg": run_agg, "serve": run_serve, "grace": run_grace,
+              "parquet": run_parquet}[args.workload]
     out = runner(args, kb, W, rt, rank, world, pg, device)
     if rank == 0:
         print(json.dumps(out))
