@@ -11,8 +11,9 @@
 //  - the host walks the page headers (Thrift compact protocol: parquet.thrift
 //    PageHeader, DataPageHeader, DataPageHeaderV2, DictionaryPageHeader) and
 //    lays every page out at a 16-byte aligned place of a staging buffer;
-//  - stage_kernel (one CTA per page) copies each page there, decompressing
-//    Snappy (the raw format Parquet uses) with one warp per page;
+//  - stage_kernel (one CTA per page) copies each page's raw bytes there and
+//    snappy_kernel decompresses Snappy (the raw format Parquet uses), one
+//    warp per page, the stream and the last 32 KiB of output in shared memory;
 //  - dict_filter_kernel tests every dictionary entry against the key filter
 //    (one byte per entry);
 //  - page_decode_kernel (one CTA per data page, tiles of 1024 rows) decodes
@@ -220,84 +221,195 @@ struct DecodeArgs {
 };
 
 // ---- stage: copy or Snappy-decompress each page ------------------------------------------
-// Snappy (raw format): a varint of the uncompressed length, then elements:
-// literals (tag & 3 == 0) and back-references with 1-, 2- or 4-byte offsets.
-// Every lane of the warp parses the same tags (uniform control flow, the tag
-// bytes broadcast), and the lanes share each element's bytes; a
-// back-reference that overlaps its own output is copied in steps of its
-// offset, each step reading only bytes that earlier steps wrote.
-__device__ bool snappy_warp(const uint8_t *src, int64_t slen, uint8_t *dst, int64_t dlen) {
-    const unsigned lane = lane_id();
-    if (slen == 0) return dlen == 0;  // an empty values section may be stored without a stream
-    int64_t ip = 0, op = 0;
-    uint64_t n = 0;
-    for (int s = 0;; s += 7) {
-        if (ip >= slen || s > 28) return false;
-        const uint8_t b = src[ip++];
-        n |= (uint64_t)(b & 0x7F) << s;
-        if (!(b & 0x80)) break;
-    }
-    if ((int64_t)n != dlen) return false;
-    while (ip < slen) {
-        const uint8_t tag = src[ip++];
-        const int kind = tag & 3;
-        int64_t len, off = 0;
-        if (kind == 0) {
-            len = tag >> 2;
-            if (len >= 60) {
-                const int nb = (int)len - 59;
-                if (ip + nb > slen) return false;
-                len = 0;
-                for (int i = 0; i < nb; i++) len |= (int64_t)src[ip + i] << (8 * i);
-                ip += nb;
-            }
-            len += 1;
-            if (ip + len > slen || op + len > dlen) return false;
-            for (int64_t i = lane; i < len; i += 32) dst[op + i] = src[ip + i];
-            ip += len;
-            op += len;
-        } else {
-            if (kind == 1) {
-                if (ip + 1 > slen) return false;
-                len = 4 + ((tag >> 2) & 7);
-                off = ((int64_t)(tag >> 5) << 8) | src[ip];
-                ip += 1;
-            } else if (kind == 2) {
-                if (ip + 2 > slen) return false;
-                len = 1 + (tag >> 2);
-                off = (int64_t)src[ip] | ((int64_t)src[ip + 1] << 8);
-                ip += 2;
-            } else {
-                if (ip + 4 > slen) return false;
-                len = 1 + (tag >> 2);
-                off = (int64_t)src[ip] | ((int64_t)src[ip + 1] << 8) | ((int64_t)src[ip + 2] << 16) |
-                      ((int64_t)src[ip + 3] << 24);
-                ip += 4;
-            }
-            if (off <= 0 || off > op || op + len > dlen) return false;
-            for (int64_t done = 0; done < len; done += off) {
-                const int64_t step = min(off, len - done);
-                for (int64_t i = lane; i < step; i += 32) dst[op + done + i] = dst[op + done + i - off];
-                __syncwarp();
-            }
-            op += len;
+// Copies n bytes (any alignment) with `threads` threads, thread t taking
+// bytes t, t + threads, ...: every thread issues kCopyDepth loads before its
+// stores, so that many bytes are in flight per thread instead of one
+// load-to-store round trip per byte. src and dst do not overlap.
+constexpr int kCopyDepth = 16;
+__device__ __forceinline__ void copy_bytes(uint8_t *dst, const uint8_t *src, int64_t n, int t, int threads) {
+    for (int64_t i0 = 0; i0 < n; i0 += (int64_t)threads * kCopyDepth) {
+        uint8_t v[kCopyDepth];
+#pragma unroll
+        for (int u = 0; u < kCopyDepth; u++) {
+            const int64_t i = i0 + (int64_t)u * threads + t;
+            v[u] = i < n ? src[i] : 0;
         }
-        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < kCopyDepth; u++) {
+            const int64_t i = i0 + (int64_t)u * threads + t;
+            if (i < n) dst[i] = v[u];
+        }
     }
-    return op == dlen;
 }
 
+// Snappy (raw format): a varint of the uncompressed length, then elements:
+// literals (tag & 3 == 0) and back-references with 1-, 2- or 4-byte offsets.
+// One warp decodes a page; its lanes all parse the same tags (uniform
+// control flow) and share each element's bytes. The latency of a page is
+// its chain of elements (a dictionary page of small integers is hundreds of
+// thousands of short elements), so each element's work stays in shared
+// memory: the compressed stream passes through an 8 KiB window, loaded in
+// bulk as parsing reaches its end, and the last 32 KiB of output are kept
+// in a ring, from which a back-reference reads its bytes (one from further
+// back reads global memory). A back-reference that overlaps its own output
+// is copied in steps of its offset.
+constexpr int kSnappyWin = 8192;
+constexpr int kSnappyRing = 32768;
+constexpr int kSnappySmem = kSnappyWin + kSnappyRing;
+
+struct SnappyWarp {
+    const uint8_t *src;
+    int64_t slen;
+    uint8_t *dst;
+    int64_t dlen;
+    uint8_t *win, *ring;
+    int64_t w0 = 0, wn = 0;  // the window holds src[w0, w0 + wn)
+    unsigned lane;
+
+    __device__ void refill(int64_t at) {
+        __syncwarp();
+        w0 = at;
+        wn = min((int64_t)kSnappyWin, slen - at);
+        copy_bytes(win, src + at, wn, (int)lane, 32);
+        __syncwarp();
+    }
+    __device__ __forceinline__ uint8_t at(int64_t i) const { return win[i - w0]; }
+    // Output bytes [op, op + n) from stream bytes [ip, ip + n).
+    __device__ void literal(int64_t ip, int64_t op, int64_t n) {
+        if (ip + n <= w0 + wn) {
+            for (int64_t i = lane; i < n; i += 32) {
+                const uint8_t b = win[ip - w0 + i];
+                dst[op + i] = b;
+                ring[(op + i) & (kSnappyRing - 1)] = b;
+            }
+            return;
+        }
+        for (int64_t i0 = 0; i0 < n; i0 += 32 * kCopyDepth) {  // beyond the window: global, many loads in flight
+            uint8_t v[kCopyDepth];
+#pragma unroll
+            for (int u = 0; u < kCopyDepth; u++) {
+                const int64_t i = i0 + u * 32 + lane;
+                v[u] = i < n ? src[ip + i] : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < kCopyDepth; u++) {
+                const int64_t i = i0 + u * 32 + lane;
+                if (i < n) {
+                    dst[op + i] = v[u];
+                    ring[(op + i) & (kSnappyRing - 1)] = v[u];
+                }
+            }
+        }
+    }
+    // Output bytes [op, op + n) from output bytes [op - off, op - off + n), off >= n.
+    __device__ void backref(int64_t op, int64_t off, int64_t n) {
+        const bool near = off <= kSnappyRing - 64;  // read and written ring slots never meet
+        for (int64_t i = lane; i < n; i += 32) {
+            const uint8_t b = near ? ring[(op - off + i) & (kSnappyRing - 1)] : dst[op - off + i];
+            dst[op + i] = b;
+            ring[(op + i) & (kSnappyRing - 1)] = b;
+        }
+    }
+
+    __device__ bool run() {
+        if (slen == 0) return dlen == 0;  // an empty values section may be stored without a stream
+        refill(0);
+        int64_t ip = 0, op = 0;
+        uint64_t n = 0;
+        for (int s = 0;; s += 7) {
+            if (ip >= wn || s > 28) return false;
+            const uint8_t b = at(ip++);
+            n |= (uint64_t)(b & 0x7F) << s;
+            if (!(b & 0x80)) break;
+        }
+        if ((int64_t)n != dlen) return false;
+        while (ip < slen) {
+            if (ip + 5 > w0 + wn && w0 + wn < slen) refill(ip);  // a tag and up to 4 more bytes
+            const uint8_t tag = at(ip++);
+            const int kind = tag & 3;
+            int64_t len, off = 0;
+            if (kind == 0) {
+                len = tag >> 2;
+                if (len >= 60) {
+                    const int nb = (int)len - 59;
+                    if (ip + nb > slen) return false;
+                    len = 0;
+                    for (int i = 0; i < nb; i++) len |= (int64_t)at(ip + i) << (8 * i);
+                    ip += nb;
+                }
+                len += 1;
+                if (ip + len > slen || op + len > dlen) return false;
+                literal(ip, op, len);
+                ip += len;
+                op += len;
+            } else {
+                if (kind == 1) {
+                    if (ip + 1 > slen) return false;
+                    len = 4 + ((tag >> 2) & 7);
+                    off = ((int64_t)(tag >> 5) << 8) | at(ip);
+                    ip += 1;
+                } else if (kind == 2) {
+                    if (ip + 2 > slen) return false;
+                    len = 1 + (tag >> 2);
+                    off = (int64_t)at(ip) | ((int64_t)at(ip + 1) << 8);
+                    ip += 2;
+                } else {
+                    if (ip + 4 > slen) return false;
+                    len = 1 + (tag >> 2);
+                    off = (int64_t)at(ip) | ((int64_t)at(ip + 1) << 8) | ((int64_t)at(ip + 2) << 16) |
+                          ((int64_t)at(ip + 3) << 24);
+                    ip += 4;
+                }
+                if (off <= 0 || off > op || op + len > dlen) return false;
+                if (off >= len) {
+                    backref(op, off, len);
+                } else {
+                    for (int64_t done = 0; done < len; done += off) {
+                        backref(op + done, off, min(off, len - done));
+                        __syncwarp();
+                    }
+                }
+                op += len;
+            }
+            __syncwarp();
+        }
+        return op == dlen;
+    }
+};
+
+// Copies each page's leading raw bytes (all of an uncompressed page, a v2
+// page's levels) to its staged place, one CTA per page.
 __global__ void __launch_bounds__(kStageThreads) stage_kernel(const StageDev *pages, const uint8_t *chunk,
-                                                              uint8_t *staged, uint32_t *status) {
+                                                              uint8_t *staged) {
     const StageDev P = pages[blockIdx.x];
     const uint8_t *src = chunk + P.src;
     uint8_t *dst = staged + P.dst;
     const int64_t raw = P.snappy ? P.raw : P.usize;  // uncompressed: the whole page is copied
-    for (int64_t i = threadIdx.x; i < raw; i += blockDim.x) dst[i] = src[i];
-    if (!P.snappy || threadIdx.x >= 32) return;
-    if (!snappy_warp(src + P.raw, (int64_t)P.csize - P.raw, dst + P.raw, (int64_t)P.usize - P.raw) &&
-        threadIdx.x == 0)
-        atomicOr(status, ST_CORRUPT);
+    if (((uintptr_t)src & 15) == 0) {  // dst is 16-byte aligned: whole 16-byte words where src is too
+        const int64_t words = raw / 16;
+        for (int64_t i = threadIdx.x; i < words; i += blockDim.x)
+            reinterpret_cast<uint4 *>(dst)[i] = reinterpret_cast<const uint4 *>(src)[i];
+        for (int64_t i = words * 16 + threadIdx.x; i < raw; i += blockDim.x) dst[i] = src[i];
+    } else {
+        copy_bytes(dst, src, raw, threadIdx.x, blockDim.x);
+    }
+}
+
+// Decompresses the Snappy part of each page: one warp per page (CTA).
+__global__ void __launch_bounds__(32) snappy_kernel(const StageDev *pages, const uint8_t *chunk, uint8_t *staged,
+                                                    uint32_t *status) {
+    extern __shared__ __align__(16) uint8_t snappy_smem[];
+    const StageDev P = pages[blockIdx.x];
+    if (!P.snappy) return;
+    SnappyWarp w;
+    w.src = chunk + P.src + P.raw;
+    w.slen = (int64_t)P.csize - P.raw;
+    w.dst = staged + P.dst + P.raw;
+    w.dlen = (int64_t)P.usize - P.raw;
+    w.win = snappy_smem;
+    w.ring = snappy_smem + kSnappyWin;
+    w.lane = threadIdx.x;
+    if (!w.run() && threadIdx.x == 0) atomicOr(status, ST_CORRUPT);
 }
 
 // ---- the filter over the dictionary entries ------------------------------------------------
@@ -731,9 +843,22 @@ ParquetChunk decode_parquet_chunk(Runtime *rt, const uint8_t *chunk, int64_t byt
         KRV_CUDA(cudaMemsetAsync(counts.get(), 0, 16, rt->stream));
         clear_status(rt);
         stage_kernel<<<(unsigned)stages.size(), kStageThreads, 0, rt->stream>>>(
-            dstages.as<StageDev>(), dchunk.as<uint8_t>(), staged.as<uint8_t>(), status_word(rt));
+            dstages.as<StageDev>(), dchunk.as<uint8_t>(), staged.as<uint8_t>());
         rt->launches++;
         check_launch("stage_kernel");
+        if (col.codec == KRV_PQ_SNAPPY) {
+            static bool smem_set[64] = {};  // the kernel's attribute, set once per device
+            int dev = 0;
+            KRV_CUDA(cudaGetDevice(&dev));
+            if (dev < 0 || dev >= 64 || !smem_set[dev]) {
+                KRV_CUDA(cudaFuncSetAttribute(snappy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSnappySmem));
+                if (dev >= 0 && dev < 64) smem_set[dev] = true;
+            }
+            snappy_kernel<<<(unsigned)stages.size(), 32, kSnappySmem, rt->stream>>>(
+                dstages.as<StageDev>(), dchunk.as<uint8_t>(), staged.as<uint8_t>(), status_word(rt));
+            rt->launches++;
+            check_launch("snappy_kernel");
+        }
         DecodeArgs A{};
         A.pages = dpages.as<PageDev>();
         A.staged = staged.as<uint8_t>();
