@@ -256,3 +256,53 @@ def test_corrupt_and_unsupported_chunks_fail_cleanly(kb, rt, tmp_path):
         kb.parquet_decode_chunk(rt, data, d["physical_type"], 6, d["max_def_level"], n, "l")  # ZSTD
     with pytest.raises(kb.KrvError):
         kb.parquet_decode_chunk(rt, data, 6, d["codec"], d["max_def_level"], n, "l")  # BYTE_ARRAY
+
+
+def _varint(v):
+    out = bytearray()
+    while True:
+        b = v & 0x7F
+        v >>= 7
+        out.append(b | (0x80 if v else 0))
+        if not v:
+            return bytes(out)
+
+
+def _i32_field(delta, v):
+    return bytes([(delta << 4) | 5]) + _varint(((v << 1) ^ (v >> 31)) & 0xFFFFFFFF)
+
+
+def _data_page(payload, usize, n):
+    """A Thrift compact PageHeader of a v1 data page (PLAIN values, RLE levels)."""
+    dph = _i32_field(1, n) + _i32_field(1, 0) + _i32_field(1, 3) + _i32_field(1, 3) + b"\x00"
+    return (_i32_field(1, 0) + _i32_field(1, usize) + _i32_field(1, len(payload)) + bytes([(2 << 4) | 12]) + dph
+            + b"\x00" + payload)
+
+
+def test_snappy_back_references_across_fragments(kb, rt):
+    """A Snappy page written by hand (not by Google's compressor): a 72 KB
+    literal, then the same bytes again as 64-byte back-references 72,000
+    bytes behind, so that references reach across the 64 KiB points where
+    the decoder would split the stream: the fragments merge, the far
+    references read back, and the values are exact; a second page of short
+    overlapping references (offset 8) follows."""
+    rng = np.random.default_rng(8)
+    half = rng.integers(-2**62, 2**62, 9000).astype(np.int64)
+    raw1 = half.tobytes() * 2
+    body = bytearray(_varint(len(raw1)))
+    body += bytes([62 << 2]) + (len(half.tobytes()) - 1).to_bytes(3, "little") + half.tobytes()
+    for _ in range(len(half.tobytes()) // 64):
+        body += bytes([(63 << 2) | 3]) + (len(half.tobytes())).to_bytes(4, "little")
+    v8 = np.full(30_000, 7, np.int64)  # 240 KB of one value: a literal of 8 bytes, then offset-8 copies
+    raw2 = v8.tobytes()
+    body2 = bytearray(_varint(len(raw2))) + bytes([7 << 2]) + raw2[:8]
+    left = len(raw2) - 8
+    while left:
+        n = min(64, left)
+        body2 += bytes([((n - 1) << 2) | 2]) + (8).to_bytes(2, "little")
+        left -= n
+    chunk = _data_page(bytes(body), len(raw1), 2 * half.size) + _data_page(bytes(body2), len(raw2), v8.size)
+    res, info = kb.parquet_decode_chunk(rt, chunk, kb.PQ_INT64, kb.PQ_SNAPPY, 0, 2 * half.size + v8.size, "l")
+    assert info["pages"] == 2 and res.rows == 2 * half.size + v8.size
+    got = res.columns[0].cpu().numpy()
+    assert np.array_equal(got, np.concatenate([half, half, v8]))
