@@ -13,7 +13,9 @@
 //    lays every page out at a 16-byte aligned place of a staging buffer;
 //  - stage_kernel (one CTA per page) copies each page's raw bytes there and
 //    snappy_kernel decompresses Snappy (the raw format Parquet uses), one
-//    warp per page, the stream and the last 32 KiB of output in shared memory;
+//    warp per fragment of a page (runs of about 64 KiB of output that the
+//    host finds by walking the tags), the stream and the last 32 KiB of
+//    output in shared memory;
 //  - dict_filter_kernel tests every dictionary entry against the key filter
 //    (one byte per entry);
 //  - page_decode_kernel (one CTA per data page, tiles of 1024 rows) decodes
@@ -189,6 +191,12 @@ struct StageDev {
     int32_t raw;        // leading bytes copied as they are (v2 levels)
     int32_t snappy;     // the rest is Snappy-compressed
 };
+// A run of a Snappy stream's elements that decodes alone: its first element
+// in the chunk, its first output byte in the staging buffer, their lengths.
+struct FragDev {
+    int64_t src, dst;
+    int32_t slen, dlen;
+};
 struct PageDev {
     int64_t staged;     // offset of the staged (uncompressed) page
     int64_t row0;       // the page's first row in the chunk
@@ -311,18 +319,12 @@ struct SnappyWarp {
         }
     }
 
+    // The elements of one fragment: stream bytes [0, slen) to output bytes
+    // [0, dlen); a back-reference reaching before the fragment is corrupt.
     __device__ bool run() {
-        if (slen == 0) return dlen == 0;  // an empty values section may be stored without a stream
+        if (slen == 0) return dlen == 0;
         refill(0);
         int64_t ip = 0, op = 0;
-        uint64_t n = 0;
-        for (int s = 0;; s += 7) {
-            if (ip >= wn || s > 28) return false;
-            const uint8_t b = at(ip++);
-            n |= (uint64_t)(b & 0x7F) << s;
-            if (!(b & 0x80)) break;
-        }
-        if ((int64_t)n != dlen) return false;
         while (ip < slen) {
             if (ip + 5 > w0 + wn && w0 + wn < slen) refill(ip);  // a tag and up to 4 more bytes
             const uint8_t tag = at(ip++);
@@ -395,17 +397,16 @@ __global__ void __launch_bounds__(kStageThreads) stage_kernel(const StageDev *pa
     }
 }
 
-// Decompresses the Snappy part of each page: one warp per page (CTA).
-__global__ void __launch_bounds__(32) snappy_kernel(const StageDev *pages, const uint8_t *chunk, uint8_t *staged,
+// Decompresses the Snappy fragments: one warp (CTA) per fragment.
+__global__ void __launch_bounds__(32) snappy_kernel(const FragDev *frags, const uint8_t *chunk, uint8_t *staged,
                                                     uint32_t *status) {
     extern __shared__ __align__(16) uint8_t snappy_smem[];
-    const StageDev P = pages[blockIdx.x];
-    if (!P.snappy) return;
+    const FragDev F = frags[blockIdx.x];
     SnappyWarp w;
-    w.src = chunk + P.src + P.raw;
-    w.slen = (int64_t)P.csize - P.raw;
-    w.dst = staged + P.dst + P.raw;
-    w.dlen = (int64_t)P.usize - P.raw;
+    w.src = chunk + F.src;
+    w.slen = F.slen;
+    w.dst = staged + F.dst;
+    w.dlen = F.dlen;
     w.win = snappy_smem;
     w.ring = snappy_smem + kSnappyWin;
     w.lane = threadIdx.x;
@@ -710,6 +711,82 @@ __global__ void __launch_bounds__(kDecodeThreads) page_decode_kernel(DecodeArgs 
 }  // namespace
 
 // ---- the operator ----------------------------------------------------------------------------
+namespace {
+// The fragments of one page's Snappy stream. A page's elements are a chain
+// (each starts where the last ended), so one warp decoding a large page is
+// slow; but a Snappy compressor codes its input in independent blocks of
+// 64 KiB (Google's snappy::Compress), so the stream splits into runs of
+// elements whose back-references stay inside the run. The host walks the
+// tags (skipping literal bytes), starts a fragment at the first element
+// boundary after each 64 KiB of output, and merges a fragment back into the
+// one before whenever a back-reference reaches behind its start, so every
+// fragment decodes alone whatever compressor wrote the stream. The host
+// copies no data: the warps decompress every byte. A stream that does not
+// parse stays one fragment, whose warp reports it.
+constexpr int64_t kFragBytes = 65536;
+void plan_fragments(const uint8_t *chunk, const StageDev &s, std::vector<FragDev> &out) {
+    const uint8_t *p = chunk + s.src + s.raw;
+    const int64_t slen = (int64_t)s.csize - s.raw, dlen = (int64_t)s.usize - s.raw;
+    if (slen == 0) {
+        if (dlen != 0) fail(KRV_INVALID_ARGUMENT, "corrupt Parquet page: an empty Snappy stream");
+        return;
+    }
+    int64_t ip = 0;
+    uint64_t n = 0;
+    for (int sh = 0;; sh += 7) {
+        if (ip >= slen || sh > 28) fail(KRV_INVALID_ARGUMENT, "corrupt Parquet page: the Snappy length");
+        const uint8_t b = p[ip++];
+        n |= (uint64_t)(b & 0x7F) << sh;
+        if (!(b & 0x80)) break;
+    }
+    if ((int64_t)n != dlen) fail(KRV_INVALID_ARGUMENT, "corrupt Parquet page: the Snappy length");
+    std::vector<std::pair<int64_t, int64_t>> starts{{ip, 0}};  // (stream, output) offsets of each fragment
+    if (dlen > 2 * kFragBytes) {
+        int64_t op = 0;
+        while (ip < slen) {
+            const uint8_t tag = p[ip++];
+            int64_t len, off = 0;
+            const int kind = tag & 3;
+            if (kind == 0) {
+                len = tag >> 2;
+                if (len >= 60) {
+                    const int nb = (int)len - 59;
+                    if (ip + nb > slen) break;
+                    len = 0;
+                    for (int i = 0; i < nb; i++) len |= (int64_t)p[ip + i] << (8 * i);
+                    ip += nb;
+                }
+                len += 1;
+                if (ip + len > slen) break;
+                ip += len;
+            } else {
+                const int nb = kind == 1 ? 1 : kind == 2 ? 2 : 4;
+                if (ip + nb > slen) break;
+                if (kind == 1) {
+                    len = 4 + ((tag >> 2) & 7);
+                    off = ((int64_t)(tag >> 5) << 8) | p[ip];
+                } else {
+                    len = 1 + (tag >> 2);
+                    for (int i = 0; i < nb; i++) off |= (int64_t)p[ip + i] << (8 * i);
+                }
+                ip += nb;
+                if (off <= 0 || off > op) break;
+                while (starts.size() > 1 && op - off < starts.back().second) starts.pop_back();
+            }
+            op += len;
+            if (op > dlen) break;
+            if (op - starts.back().second >= kFragBytes && ip < slen) starts.push_back({ip, op});
+        }
+    }
+    for (size_t k = 0; k < starts.size(); k++) {
+        const int64_t ip0 = starts[k].first, op0 = starts[k].second;
+        const int64_t ip1 = k + 1 < starts.size() ? starts[k + 1].first : slen;
+        const int64_t op1 = k + 1 < starts.size() ? starts[k + 1].second : dlen;
+        out.push_back(FragDev{s.src + s.raw + ip0, s.dst + s.raw + op0, (int32_t)(ip1 - ip0), (int32_t)(op1 - op0)});
+    }
+}
+}  // namespace
+
 ParquetChunk decode_parquet_chunk(Runtime *rt, const uint8_t *chunk, int64_t bytes, const krv_parquet_column &col,
                                   const KeyFilterImpl *filter) {
     if (!chunk && bytes > 0) fail(KRV_INVALID_ARGUMENT, "chunk is NULL");
@@ -836,6 +913,13 @@ ParquetChunk decode_parquet_chunk(Runtime *rt, const uint8_t *chunk, int64_t byt
         DBuf dstages(rt, stages.size() * sizeof(StageDev));
         DBuf dpages(rt, std::max<size_t>(pages.size(), 1) * sizeof(PageDev));
         DBuf counts(rt, 16);
+        std::vector<FragDev> frags;
+        for (const StageDev &st : stages)
+            if (st.snappy) plan_fragments(chunk, st, frags);
+        DBuf dfrags(rt, std::max<size_t>(frags.size(), 1) * sizeof(FragDev));
+        if (!frags.empty())
+            KRV_CUDA(cudaMemcpyAsync(dfrags.get(), frags.data(), frags.size() * sizeof(FragDev), cudaMemcpyHostToDevice,
+                                     rt->stream));
         KRV_CUDA(cudaMemcpyAsync(dstages.get(), stages.data(), stages.size() * sizeof(StageDev), cudaMemcpyHostToDevice,
                                  rt->stream));
         KRV_CUDA(cudaMemcpyAsync(dpages.get(), pages.data(), pages.size() * sizeof(PageDev), cudaMemcpyHostToDevice,
@@ -854,10 +938,12 @@ ParquetChunk decode_parquet_chunk(Runtime *rt, const uint8_t *chunk, int64_t byt
                 KRV_CUDA(cudaFuncSetAttribute(snappy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSnappySmem));
                 if (dev >= 0 && dev < 64) smem_set[dev] = true;
             }
-            snappy_kernel<<<(unsigned)stages.size(), 32, kSnappySmem, rt->stream>>>(
-                dstages.as<StageDev>(), dchunk.as<uint8_t>(), staged.as<uint8_t>(), status_word(rt));
-            rt->launches++;
-            check_launch("snappy_kernel");
+            if (!frags.empty()) {
+                snappy_kernel<<<(unsigned)frags.size(), 32, kSnappySmem, rt->stream>>>(
+                    dfrags.as<FragDev>(), dchunk.as<uint8_t>(), staged.as<uint8_t>(), status_word(rt));
+                rt->launches++;
+                check_launch("snappy_kernel");
+            }
         }
         DecodeArgs A{};
         A.pages = dpages.as<PageDev>();
