@@ -880,6 +880,7 @@ def run_parquet(args, kb, W, rt, rank, world, pg, device):
                                "kind": "pyarrow", "sample": "pyarrow 24 (Arrow C++) read_table of the same two columns "
                                                           "from the file's bytes in memory, all host threads, median of 3"}
     os.remove(path)
+    os.rmdir(os.path.dirname(path))
     return out
 
 
