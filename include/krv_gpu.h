@@ -103,8 +103,8 @@ int64_t krv_runtime_launches(const krv_runtime *rt);
  * registry_join.rs:11-160) and the runtime filter options. Key columns are
  * int32/int64/date32/decimal/float64, or (unpartitioned joins) UTF-8 ("u")
  * and binary ("z") columns, whose key tuples are then coded as one int64;
- * string columns may not be projected into the output, and such a join
- * publishes no runtime filter. */
+ * string columns (keys included) may be projected into the output, and such
+ * a join publishes no runtime filter. */
 typedef struct {
     int32_t join_type;                     /* KRV_JOIN_* */
     int32_t n_keys;                        /* 1..KRV_MAX_KEYS */

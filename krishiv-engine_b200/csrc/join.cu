@@ -836,21 +836,17 @@ void HashJoin::decide(const DevBatch &b) {
         meta.push_back(m);
     }
     coded_->dict = make_key_dict(rt_, meta);
-    // the build side's columns without its string columns, then the code
-    std::vector<int> map;
-    int inner = 0;
-    for (const DevCol &c : b.cols) map.push_back(c.type.var() ? -1 : inner++);
+    // the build side's columns (string key columns stay, as payload), then the code
     const krv_join_spec &o = coded_->outer;
     spec_.n_keys = 1;
-    spec_.build_keys[0] = inner;
+    spec_.build_keys[0] = (int32_t)b.cols.size();
     spec_.null_safe[0] = 0;
     spec_.runtime_filter = 0;  // a filter over codes answers nothing outside
     const int nb = o.n_build_out < 0 ? (int)b.cols.size() : o.n_build_out;
     for (int i = 0; i < nb; i++) {
         const int c = o.n_build_out < 0 ? i : o.build_out[i];
         if (c < 0 || c >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "projection column out of range");
-        if (map[c] < 0) fail(KRV_UNSUPPORTED, "string and binary columns in a join's output");
-        spec_.build_out[i] = map[c];
+        spec_.build_out[i] = c;
     }
     spec_.n_build_out = nb;
 }
@@ -866,8 +862,9 @@ __global__ void code_valid_kernel(KeysDev k, int64_t n, uint32_t *bits) {
     }
 }
 
-// The batch the table sees: b without its string columns, then the key
-// code (NULL where an `=` key is NULL: such a row never matches).
+// The batch the table sees: b's columns (string and binary ones included,
+// as payload the output can carry), then the key code (NULL where an `=`
+// key is NULL: such a row never matches).
 DevBatch HashJoin::coded_batch(const DevBatch &b, bool build) {
     const krv_join_spec &o = coded_->outer;
     const int32_t *keys = build ? o.build_keys : o.probe_keys;
@@ -879,12 +876,7 @@ DevBatch HashJoin::coded_batch(const DevBatch &b, bool build) {
     auto codes = std::make_shared<DBuf>(key_dict_encode(coded_->dict, b, cols, build));
     DevBatch in;
     in.rows = b.rows;
-    std::vector<int> map;
-    int inner = 0;
-    for (const DevCol &c : b.cols) {
-        map.push_back(c.type.var() ? -1 : inner++);
-        if (!c.type.var()) in.cols.push_back(c);
-    }
+    in.cols = b.cols;
     // validity of the code: every `=` key component valid
     KeysDev kd{};
     kd.n = o.n_keys;
@@ -912,13 +904,12 @@ DevBatch HashJoin::coded_batch(const DevBatch &b, bool build) {
     in.cols.push_back(cc);
     if (!build && !coded_->probe_mapped) {
         coded_->probe_mapped = true;
-        spec_.probe_keys[0] = inner;
+        spec_.probe_keys[0] = (int32_t)b.cols.size();
         const int np = o.n_probe_out < 0 ? (int)b.cols.size() : o.n_probe_out;
         for (int i = 0; i < np; i++) {
             const int c = o.n_probe_out < 0 ? i : o.probe_out[i];
             if (c < 0 || c >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "projection column out of range");
-            if (map[c] < 0) fail(KRV_UNSUPPORTED, "string and binary columns in a join's output");
-            spec_.probe_out[i] = map[c];
+            spec_.probe_out[i] = c;
         }
         spec_.n_probe_out = np;
     }

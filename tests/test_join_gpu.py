@@ -235,7 +235,7 @@ def rows_batch_str(rows, idname):
 
 def gpu_pairs_str(kb, rt, jt, probe, build, nkeys, null_safe, build_batches=1):
     """gpu_pairs with a string first key: the id columns are projected, the
-    string key is not (string columns never reach a join's output)."""
+    string key is not (`test_string_keys_in_the_output` projects it)."""
     spec = kb.join_spec(jt, probe_keys=tuple(range(nkeys)), build_keys=tuple(range(nkeys)),
                         null_safe=[null_safe] * nkeys, probe_out=[2], build_out=[2])
     j = kb.HashJoin(rt, spec)
@@ -285,3 +285,30 @@ def test_string_key_types_must_agree(kb, rt):
     with pytest.raises(kb.KrvError) as e:
         j.probe(batch(k=pa.array([1, 2]), pid=pa.array([0, 1])))
     assert e.value.status in (kb.INVALID_ARGUMENT, kb.UNSUPPORTED)
+
+
+@pytest.mark.parametrize("jt", ["inner", "left_outer", "right_outer", "full_outer", "left_semi", "existence"])
+def test_string_keys_in_the_output(kb, rt, oracle, jt):
+    """A join on a string key (plus an int32 key) that projects the string
+    keys of both sides: the pairs are the oracle's, and every output row's
+    strings are those of the rows it came from (NULL on a padded side)."""
+    rng = np.random.default_rng(21)
+    probe = [(int(x) if x >= 0 else None, int(y)) for x, y in zip(rng.integers(-20, 400, 3000), rng.integers(0, 2, 3000))]
+    build = [(int(x) if x >= 0 else None, int(y)) for x, y in zip(rng.integers(-20, 400, 1500), rng.integers(0, 2, 1500))]
+    spec = kb.join_spec(jt, probe_keys=(0, 1), build_keys=(0, 1), probe_out=[2, 0], build_out=[2, 0])
+    j = kb.HashJoin(rt, spec)
+    j.build_push(rows_batch_str(build, "bid"))
+    j.build_finish()
+    t = concat(j.probe(rows_batch_str(probe, "pid")) + j.finish())
+    pk, pid = t.column(1).to_pylist(), t.column("pid").to_pylist()
+    for i, p in enumerate(pid):
+        assert pk[i] == (str_of(probe[p][0]) if p is not None else None)
+    want = oracle_pairs(oracle, jt, probe, build, 2, False)
+    if jt == "existence":
+        assert collections.Counter(zip(pid, [int(x) for x in t.column("exists").to_pylist()])) == want
+        return
+    if jt != "left_semi":
+        bk, bid = t.column(3).to_pylist(), t.column("bid").to_pylist()
+        for i, b in enumerate(bid):
+            assert bk[i] == (str_of(build[b][0]) if b is not None else None)
+    assert pairs_from_output(t) == want
