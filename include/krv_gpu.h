@@ -428,17 +428,19 @@ void krv_key_filter_destroy(krv_key_filter *f);
  * says that no row of the chunk can pass but a NULL (the row group can be
  * skipped, as any_entry_in decides). Flat columns (max definition level 0 or
  * 1, no repetition); physical INT32 (as "i", "tdD", "l", "d:p,s,64" or
- * "d:p,s"), INT64 (as "l", "d:p,s,64" or "d:p,s") and DOUBLE (as "g");
+ * "d:p,s"), INT64 (as "l", "d:p,s,64" or "d:p,s"), DOUBLE (as "g") and
+ * BYTE_ARRAY (as "u" or "z": int32 offsets and bytes);
  * PLAIN, PLAIN_DICTIONARY and RLE_DICTIONARY values; UNCOMPRESSED and SNAPPY
  * chunks; data pages v1 and v2. Others: KRV_UNSUPPORTED. Bytes that do not
  * decode: KRV_INVALID_ARGUMENT. The filter applies to integer columns. */
 #define KRV_PQ_INT32 1         /* parquet.thrift Type */
 #define KRV_PQ_INT64 2
 #define KRV_PQ_DOUBLE 5
+#define KRV_PQ_BYTE_ARRAY 6
 #define KRV_PQ_UNCOMPRESSED 0  /* parquet.thrift CompressionCodec */
 #define KRV_PQ_SNAPPY 1
 typedef struct {
-    int32_t physical_type;  /* KRV_PQ_INT32, KRV_PQ_INT64 or KRV_PQ_DOUBLE */
+    int32_t physical_type;  /* KRV_PQ_INT32, KRV_PQ_INT64, KRV_PQ_DOUBLE or KRV_PQ_BYTE_ARRAY */
     int32_t codec;          /* KRV_PQ_UNCOMPRESSED or KRV_PQ_SNAPPY */
     int32_t max_def_level;  /* 0: required, 1: optional */
     int32_t pad0;

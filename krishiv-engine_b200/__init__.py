@@ -177,7 +177,7 @@ class ParquetInfo(C.Structure):
                 ("dictionary_passing", C.c_int64), ("passing_rows", C.c_int64)]
 
 
-PQ_INT32, PQ_INT64, PQ_DOUBLE = 1, 2, 5
+PQ_INT32, PQ_INT64, PQ_DOUBLE, PQ_BYTE_ARRAY = 1, 2, 5, 6
 PQ_UNCOMPRESSED, PQ_SNAPPY = 0, 1
 
 
@@ -463,6 +463,7 @@ class DeviceResult:
         self.schema = schema
         self.rows = dev.array.length
         self.names, self.formats, self.columns, self.valid = [], [], [], []
+        self.heaps = []  # UTF-8 / binary columns: their bytes (columns[i] holds the int32 offsets)
         for i in range(dev.array.n_children):
             cs = schema.children[i].contents
             fmt = cs.format.decode()
@@ -471,7 +472,14 @@ class DeviceResult:
             ch = dev.array.children[i].contents
             data = ch.buffers[1]
             vptr = ch.buffers[0]
-            if fmt.startswith("d:"):
+            heap = None
+            if fmt in ("u", "z"):
+                ts, n = "<i4", self.rows + 1
+                offs = torch.as_tensor(_CudaArray(data, n, ts), device="cuda") if data else None
+                nbytes = int(offs[-1].item()) if offs is not None else 0
+                if nbytes and ch.buffers[2]:
+                    heap = torch.as_tensor(_CudaArray(ch.buffers[2], nbytes, "|u1"), device="cuda")
+            elif fmt.startswith("d:"):
                 width = 8 if fmt.endswith(",64") else 16
                 ts, n = "<i8", self.rows * (width // 8)
             elif fmt == "b":
@@ -479,6 +487,7 @@ class DeviceResult:
             else:
                 ts, n = self._TYPESTR[fmt], self.rows
             self.columns.append(torch.as_tensor(_CudaArray(data, n, ts), device="cuda") if n and data else None)
+            self.heaps.append(heap)
             self.valid.append(torch.as_tensor(_CudaArray(vptr, (self.rows + 7) // 8, "|u1"), device="cuda")
                               if vptr and self.rows else None)
 

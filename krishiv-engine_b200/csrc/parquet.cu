@@ -207,7 +207,11 @@ struct PageDev {
     int32_t def_len;    // v2: bytes of the definition levels
     int32_t pad;
 };
-enum OutKind : int32_t { OUT_SAME = 0, OUT_I32_TO_I64 = 1, OUT_TO_DEC128 = 2 };
+// OUT_REF (BYTE_ARRAY): each row's value is written as a reference, its
+// dictionary entry or dict_n + (its page's first row) + (its rank among the
+// page's non-NULL values), into the (start, length) table the walk filled;
+// -1 for NULL. The string column is then gathered by those references.
+enum OutKind : int32_t { OUT_SAME = 0, OUT_I32_TO_I64 = 1, OUT_TO_DEC128 = 2, OUT_REF = 3 };
 struct DecodeArgs {
     const PageDev *pages;
     const uint8_t *staged;
@@ -226,6 +230,20 @@ struct DecodeArgs {
     uint32_t *pass;     // the filter's bit per row
     unsigned long long *counts;  // [0] rows passing the filter
     uint32_t *status;
+    long long *ref;      // OUT_REF: each row's value reference
+    const int32_t *walked;  // OUT_REF: the values the walk found in each PLAIN page
+};
+// A BYTE_ARRAY page whose values are walked: PLAIN values, each a 4-byte
+// little-endian length and its bytes, one after another.
+struct WalkDev {
+    int64_t staged;     // the staged page
+    int64_t base;       // its first value's slot in the (start, length) table
+    int32_t usize;
+    int32_t kind;       // 0 dictionary page, 1 data page v1, 2 data page v2
+    int32_t def_len;    // v2: bytes of the definition levels
+    int32_t limit;      // the values it may hold
+    int32_t page;       // the data page's index (walked[page]); -1 for the dictionary
+    int32_t pad;
 };
 
 // ---- stage: copy or Snappy-decompress each page ------------------------------------------
@@ -543,6 +561,44 @@ __device__ __forceinline__ void bitmap_or(uint32_t *words, int64_t row, unsigned
     }
 }
 
+// The PLAIN BYTE_ARRAY values of a dictionary page or a data page, one warp
+// (lane 0) per page: each value's start in the staging buffer and its length
+// into the table, every length checked against the page.
+__global__ void __launch_bounds__(32) ba_walk_kernel(const WalkDev *items, const uint8_t *staged, int max_def,
+                                                     long long *starts, int32_t *lens, int32_t *walked,
+                                                     uint32_t *status) {
+    if (threadIdx.x != 0) return;
+    const WalkDev W = items[blockIdx.x];
+    const uint8_t *page = staged + W.staged;
+    auto le32 = [&](int64_t at) {
+        return (uint32_t)page[at] | ((uint32_t)page[at + 1] << 8) | ((uint32_t)page[at + 2] << 16) |
+               ((uint32_t)page[at + 3] << 24);
+    };
+    int64_t pos = 0;
+    const int64_t end = W.usize;
+    if (W.kind == 1 && max_def > 0) {  // v1: the levels' 4-byte length, then the levels
+        if (end < 4 || (int64_t)le32(0) > end - 4) {
+            atomicOr(status, ST_CORRUPT);
+            return;
+        }
+        pos = 4 + (int64_t)le32(0);
+    } else if (W.kind == 2) {
+        pos = W.def_len;
+    }
+    int32_t n = 0;
+    while (pos < end && n < W.limit) {
+        if (end - pos < 4) break;
+        const int64_t len = le32(pos);
+        if (len > end - pos - 4) break;
+        starts[W.base + n] = (long long)(W.staged + pos + 4);
+        lens[W.base + n] = (int32_t)len;
+        pos += 4 + len;
+        n++;
+    }
+    if (W.page >= 0) walked[W.page] = n;
+    if (pos != end || (W.page < 0 && n != W.limit)) atomicOr(status, ST_CORRUPT);
+}
+
 __global__ void __launch_bounds__(kDecodeThreads) page_decode_kernel(DecodeArgs A) {
     constexpr int U = kTile / kDecodeThreads;
     __shared__ Hybrid s_def, s_idx;
@@ -635,6 +691,28 @@ __global__ void __launch_bounds__(kDecodeThreads) page_decode_kernel(DecodeArgs 
             const int i = tid * U + u;
             if (i >= n) break;
             const int64_t row = P.row0 + t0 + i;
+            if (A.out_kind == OUT_REF) {
+                long long rf = -1;
+                if (v[u]) {
+                    const int64_t k = rank++;  // within the tile; nn_base + k within the page
+                    if (P.dict) {
+                        const uint32_t idx = run_value(s_runs, s_ni, (int)k, s_idx.bw, page);
+                        if ((int64_t)idx >= A.dict_n) {
+                            atomicOr(A.status, ST_CORRUPT);
+                            continue;
+                        }
+                        rf = (long long)idx;
+                    } else {
+                        if (nn_base + k >= A.walked[blockIdx.x]) {
+                            atomicOr(A.status, ST_CORRUPT);
+                            continue;
+                        }
+                        rf = (long long)(A.dict_n + P.row0 + nn_base + k);
+                    }
+                }
+                A.ref[row] = rf;
+                continue;
+            }
             int64_t ival = 0;
             uint64_t raw = 0;
             bool pass = A.f.nulls_pass != 0;
@@ -796,10 +874,12 @@ ParquetChunk decode_parquet_chunk(Runtime *rt, const uint8_t *chunk, int64_t byt
         fail(KRV_UNSUPPORTED, "the GPU Parquet decoder takes flat columns (max definition level 0 or 1)");
     if (col.codec != KRV_PQ_UNCOMPRESSED && col.codec != KRV_PQ_SNAPPY)
         fail(KRV_UNSUPPORTED, "Parquet codec " + std::to_string(col.codec) + " on the GPU decoder (UNCOMPRESSED, SNAPPY)");
-    int pwidth = 0;
+    int pwidth = 0;  // 0: BYTE_ARRAY (a 4-byte length before each value)
     if (col.physical_type == KRV_PQ_INT32) pwidth = 4;
     else if (col.physical_type == KRV_PQ_INT64 || col.physical_type == KRV_PQ_DOUBLE) pwidth = 8;
-    else fail(KRV_UNSUPPORTED, "Parquet physical type " + std::to_string(col.physical_type) + " on the GPU decoder");
+    else if (col.physical_type != KRV_PQ_BYTE_ARRAY)
+        fail(KRV_UNSUPPORTED, "Parquet physical type " + std::to_string(col.physical_type) + " on the GPU decoder");
+    const bool var = col.physical_type == KRV_PQ_BYTE_ARRAY;
     if (!col.format) fail(KRV_INVALID_ARGUMENT, "format is NULL");
     const DType out_t = parse_format(col.format);
     int out_kind = -1;
@@ -810,11 +890,13 @@ ParquetChunk decode_parquet_chunk(Runtime *rt, const uint8_t *chunk, int64_t byt
     } else if (col.physical_type == KRV_PQ_INT64) {
         if (out_t.id == Type::I64 || out_t.id == Type::Dec64) out_kind = OUT_SAME;
         else if (out_t.id == Type::Dec128) out_kind = OUT_TO_DEC128;
-    } else if (out_t.id == Type::F64) {
-        out_kind = OUT_SAME;
+    } else if (col.physical_type == KRV_PQ_DOUBLE) {
+        if (out_t.id == Type::F64) out_kind = OUT_SAME;
+    } else if (out_t.id == Type::Utf8 || out_t.id == Type::Binary) {
+        out_kind = OUT_REF;
     }
     if (out_kind < 0) fail(KRV_UNSUPPORTED, std::string("Parquet column decoded as ") + col.format);
-    const bool is_int = col.physical_type != KRV_PQ_DOUBLE;
+    const bool is_int = col.physical_type == KRV_PQ_INT32 || col.physical_type == KRV_PQ_INT64;
     if (filter && !is_int) fail(KRV_UNSUPPORTED, "key filters test integer columns");
 
     // The page headers, on the host.
@@ -855,7 +937,7 @@ ParquetChunk decode_parquet_chunk(Runtime *rt, const uint8_t *chunk, int64_t byt
             if (dict_stage >= 0 || !pages.empty()) fail(KRV_INVALID_ARGUMENT, "a dictionary page after the first page");
             if (h.encoding != kEncPlain && h.encoding != kEncPlainDict)
                 fail(KRV_UNSUPPORTED, "Parquet dictionary encoding " + std::to_string(h.encoding));
-            if ((int64_t)h.nvalues * pwidth > h.usize) fail(KRV_INVALID_ARGUMENT, "corrupt Parquet dictionary page");
+            if ((int64_t)h.nvalues * (var ? 4 : pwidth) > h.usize) fail(KRV_INVALID_ARGUMENT, "corrupt Parquet dictionary page");
             dict_stage = (int)stages.size();
             dict_n = h.nvalues;
         } else {
@@ -892,7 +974,8 @@ ParquetChunk decode_parquet_chunk(Runtime *rt, const uint8_t *chunk, int64_t byt
     r.info.dictionary_entries = dict_n;
     r.info.dictionary_passing = -1;
     r.info.passing_rows = -1;
-    DevCol out = make_col(rt, out_t, rows, col.max_def_level > 0, col.name ? col.name : "");
+    const std::string name = col.name ? col.name : "";
+    DevCol out = var ? DevCol{} : make_col(rt, out_t, rows, col.max_def_level > 0, name);
     r.batch.rows = rows;
     DevCol pass;
     if (filter) {
@@ -976,6 +1059,38 @@ ParquetChunk decode_parquet_chunk(Runtime *rt, const uint8_t *chunk, int64_t byt
         } else {
             A.f.nulls_pass = 1;
         }
+        // BYTE_ARRAY: the (start, length) table of the dictionary's entries,
+        // then of every PLAIN page's values at the page's first row; each
+        // row's reference into it.
+        DBuf vstarts, vlens, walked, refs, dwalk;
+        if (var) {
+            const int64_t slots = dict_n + rows;
+            vstarts = DBuf(rt, (size_t)std::max<int64_t>(slots, 1) * 8);
+            vlens = DBuf(rt, (size_t)std::max<int64_t>(slots, 1) * 4);
+            walked = DBuf(rt, std::max<size_t>(pages.size(), 1) * 4);
+            refs = DBuf(rt, (size_t)rows * 8);
+            KRV_CUDA(cudaMemsetAsync(walked.get(), 0, walked.bytes(), rt->stream));
+            std::vector<WalkDev> items;
+            if (dict_stage >= 0 && dict_n > 0)
+                items.push_back(WalkDev{stages[dict_stage].dst, 0, stages[dict_stage].usize, 0, 0, (int32_t)dict_n, -1, 0});
+            for (size_t i = 0; i < pages.size(); i++)
+                if (!pages[i].dict)
+                    items.push_back(WalkDev{pages[i].staged, dict_n + pages[i].row0, pages[i].usize, pages[i].v2 ? 2 : 1,
+                                            pages[i].def_len, pages[i].nvalues, (int32_t)i, 0});
+            if (!items.empty()) {
+                dwalk = DBuf(rt, items.size() * sizeof(WalkDev));
+                KRV_CUDA(cudaMemcpyAsync(dwalk.get(), items.data(), items.size() * sizeof(WalkDev),
+                                         cudaMemcpyHostToDevice, rt->stream));
+                ba_walk_kernel<<<(unsigned)items.size(), 32, 0, rt->stream>>>(
+                    dwalk.as<WalkDev>(), staged.as<uint8_t>(), col.max_def_level, vstarts.as<long long>(),
+                    vlens.as<int32_t>(), walked.as<int32_t>(), status_word(rt));
+                rt->launches++;
+                check_launch("ba_walk_kernel");
+            }
+            A.ref = refs.as<long long>();
+            A.walked = walked.as<int32_t>();
+            A.valid = nullptr;  // the gather writes the validity
+        }
         if (!pages.empty()) {
             page_decode_kernel<<<(unsigned)pages.size(), kDecodeThreads, 0, rt->stream>>>(A);
             rt->launches++;
@@ -986,13 +1101,18 @@ ParquetChunk decode_parquet_chunk(Runtime *rt, const uint8_t *chunk, int64_t byt
         const uint32_t st = take_status(rt);
         if (st & ST_CORRUPT) fail(KRV_INVALID_ARGUMENT, "corrupt Parquet page: its bytes do not decode");
         if (st) fail(KRV_CUDA_ERROR, "Parquet decode status " + std::to_string(st));
+        if (var) {
+            const VarSrc src{nullptr, vstarts.as<long long>(), vlens.as<int32_t>(), staged.as<uint8_t>(), nullptr, 0};
+            out = var_gather(rt, src, refs.as<long long>(), rows, out_t, col.max_def_level > 0, name);
+        }
         if (filter) {
             r.info.passing_rows = (int64_t)c[0];
             // the dictionary decides for the chunk only when every data page uses it
             if (dict_stage >= 0 && all_dict) r.info.dictionary_passing = (int64_t)c[1];
         }
-    } else if (filter) {
-        r.info.passing_rows = 0;
+    } else {
+        if (filter) r.info.passing_rows = 0;
+        if (var) out = var_gather(rt, VarSrc{}, nullptr, 0, out_t, col.max_def_level > 0, name);
     }
     r.batch.cols.push_back(out);
     if (filter) r.batch.cols.push_back(pass);

@@ -98,7 +98,7 @@ class ParquetScan:
 
 
 # pyarrow names of the Parquet physical types and codecs the device decoder takes
-_PHYSICAL = {"INT32": 1, "INT64": 2, "DOUBLE": 5}
+_PHYSICAL = {"INT32": 1, "INT64": 2, "DOUBLE": 5, "BYTE_ARRAY": 6}
 _CODEC = {"UNCOMPRESSED": 0, "SNAPPY": 1}
 
 
@@ -111,6 +111,10 @@ def arrow_format(t) -> str:
         return "l"
     if pa.types.is_float64(t):
         return "g"
+    if pa.types.is_string(t):
+        return "u"
+    if pa.types.is_binary(t):
+        return "z"
     if pa.types.is_date32(t):
         return "tdD"
     if pa.types.is_decimal(t):

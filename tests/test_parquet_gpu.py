@@ -255,7 +255,9 @@ def test_corrupt_and_unsupported_chunks_fail_cleanly(kb, rt, tmp_path):
     with pytest.raises(kb.KrvError):
         kb.parquet_decode_chunk(rt, data, d["physical_type"], 6, d["max_def_level"], n, "l")  # ZSTD
     with pytest.raises(kb.KrvError):
-        kb.parquet_decode_chunk(rt, data, 6, d["codec"], d["max_def_level"], n, "l")  # BYTE_ARRAY
+        kb.parquet_decode_chunk(rt, data, 7, d["codec"], d["max_def_level"], n, "l")  # FIXED_LEN_BYTE_ARRAY
+    with pytest.raises(kb.KrvError):
+        kb.parquet_decode_chunk(rt, data, d["physical_type"], d["codec"], d["max_def_level"], n, "u")  # INT64 as UTF-8
 
 
 def _varint(v):
@@ -306,3 +308,60 @@ def test_snappy_back_references_across_fragments(kb, rt):
     assert info["pages"] == 2 and res.rows == 2 * half.size + v8.size
     got = res.columns[0].cpu().numpy()
     assert np.array_equal(got, np.concatenate([half, half, v8]))
+
+
+def strings_of(res):
+    """A decoded UTF-8 / binary column as Python values (None for NULL)."""
+    if res.rows == 0:
+        return []
+    offs = res.columns[0].cpu().numpy()
+    heap = res.heaps[0].cpu().numpy().tobytes() if res.heaps[0] is not None else b""
+    valid = bits(res, 0)
+    return [heap[offs[i]:offs[i + 1]] if valid[i] else None for i in range(res.rows)]
+
+
+@pytest.mark.parametrize("compression", ["NONE", "SNAPPY"])
+@pytest.mark.parametrize("use_dictionary", [True, False])
+@pytest.mark.parametrize("page_version", ["1.0", "2.0"])
+def test_string_and_binary_columns(kb, rt, tmp_path, compression, use_dictionary, page_version):
+    """BYTE_ARRAY chunks (UTF-8 and binary, NULLs, empty values, values of
+    a few KB, many pages and row groups, a dictionary of repeated strings)
+    decode to pyarrow's values byte for byte."""
+    from importlib import import_module
+    S = import_module("krishiv-engine_b200.scan")
+    rng = np.random.default_rng(31)
+    n = 60_000
+    words = ["", "a", "krishiv", "ä-ö-ü", "x" * 3000] + ["w%05d" % i for i in range(2000)]
+    s = [None if rng.random() < 0.03 else words[int(rng.integers(0, len(words)))] for _ in range(n)]
+    b = [None if rng.random() < 0.03 else bytes(rng.integers(0, 256, int(rng.integers(0, 40)), dtype=np.uint8))
+         for _ in range(n)]
+    t = pa.table({"s": pa.array(s, pa.string()), "b": pa.array(b, pa.binary())})
+    path = write(tmp_path, t, compression=compression, use_dictionary=use_dictionary, data_page_version=page_version,
+                 row_group_size=25_000, data_page_size=16 << 10)
+    pf = pq.ParquetFile(path)
+    md = pf.metadata
+    for ci, name in enumerate(("s", "b")):
+        got = []
+        with open(path, "rb") as f:
+            for rg in range(md.num_row_groups):
+                data, d = S.column_chunk(f, md, rg, ci)
+                res, info = kb.parquet_decode_chunk(rt, data, d["physical_type"], d["codec"], d["max_def_level"],
+                                                    d["num_values"], S.arrow_format(pf.schema_arrow.field(name).type),
+                                                    name)
+                assert res.formats[0] == ("u" if name == "s" else "z")
+                got += strings_of(res)
+        want = [x.encode() if isinstance(x, str) else x for x in pq.read_table(path, columns=[name]).column(0).to_pylist()]
+        assert got == want
+
+
+def test_string_filter_is_unsupported(kb, rt, tmp_path):
+    from importlib import import_module
+    S = import_module("krishiv-engine_b200.scan")
+    path = write(tmp_path, pa.table({"s": pa.array(["a", "b"])}))
+    md = pq.ParquetFile(path).metadata
+    with open(path, "rb") as f:
+        data, d = S.column_chunk(f, md, 0, 0)
+    kf = kb.KeyFilter.build(rt, pa.record_batch([pa.array(np.arange(5, dtype=np.int64))], names=["k"]), 0)
+    with pytest.raises(kb.KrvError) as e:
+        kb.parquet_decode_chunk(rt, data, d["physical_type"], d["codec"], d["max_def_level"], 2, "u", "s", kf)
+    assert e.value.status == kb.UNSUPPORTED
