@@ -2003,6 +2003,9 @@ void HashAggregate::plan(const DevBatch &b) {
     const int hidden_base = (int)b.cols.size() + (dict_ ? 1 : 0);
     auto type_of = [&](int col) -> DType {
         if (col >= hidden_base) return DType{Type::I64, 0, 0};
+        // a UTF-8 / binary column counted by COUNT: its int32 offsets stand in
+        // for values (never read: only the validity counts)
+        if (b.cols[col].type.var()) return DType{Type::I32, 0, 0};
         return b.cols[col].type;
     };
     P_.ncols = 0;
@@ -2026,6 +2029,12 @@ void HashAggregate::plan(const DevBatch &b) {
         if (t.id == Type::Bool || t.id == Type::U8 || t.var()) fail(KRV_UNSUPPORTED, "aggregate over " + t.format());
         return t;
     };
+    // COUNT(column) also takes UTF-8 and binary columns (AggregateFunction::Count
+    // counts the non-NULL values of any type, aggregate/mod.rs:134)
+    auto check_counted = [&](int col) {
+        if (col < 0 || col >= (int)b.cols.size()) fail(KRV_INVALID_ARGUMENT, "aggregate column out of range");
+        if (!b.cols[col].type.var()) check_col(col);
+    };
     expr_col_.assign(spec_.n_aggregates, -1);
     expr_aux_.assign(spec_.n_aggregates, -1);
     for (int e = 0; e < spec_.n_aggregates; e++) {
@@ -2034,6 +2043,11 @@ void HashAggregate::plan(const DevBatch &b) {
         if (x.input != KRV_AGG_INPUT_RAW && !state) fail(KRV_INVALID_ARGUMENT, "unknown aggregate input");
         if (!state) {
             if (x.function == KRV_AGG_COUNT_STAR) continue;
+            if (x.function == KRV_AGG_COUNT && b.cols[std::max(0, std::min(x.column, (int)b.cols.size() - 1))].type.var()) {
+                check_counted(x.column);
+                expr_col_[e] = plan_col(x.column, 0);
+                continue;
+            }
             const DType t = check_col(x.column);
             int32_t f = 0;
             if (x.function == KRV_AGG_SUM || x.function == KRV_AGG_AVG) f = F_SUM;
@@ -2480,7 +2494,7 @@ void HashAggregate::push_partitioned(const DevBatch &b, const KeyIn &key, int64_
         P.c[c].data = col.data;
         P.c[c].valid = col.valid;
         P.c[c].voff = col.valid_off;
-        widths[c] = col.type.width();
+        widths[c] = col.type.var() ? 4 : col.type.width();  // a counted string column: its offsets
     }
     known_groups_ = (int64_t)read_scalar<unsigned long long>(rt_, ngroups_.get());  // the hot keys' groups too
     // Partitions: each to hold about kPartKeys distinct keys (at most 2^13
