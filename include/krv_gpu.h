@@ -273,8 +273,10 @@ int64_t krv_join_filtered_probe_rows(const krv_join *j);
 /* ---- grouped hash aggregate ---------------------------------------------- */
 /* AggregateFunction (aggregate/mod.rs:134), the core five. MIN/MAX of a
  * decimal128 column of precision 19 to 38 keep all 128 bits (the reference's
- * MinMax over Values::Int(i128), aggregate/accumulator.rs:238-248); such an
- * aggregate runs its global-table kernels only. */
+ * MinMax over Values::Int(i128), aggregate/accumulator.rs:238-248); MIN/MAX
+ * of UTF-8 and binary columns compare bytes (MinMax over Values::Bytes);
+ * COUNT takes any column. An aggregate with 128-bit or string MIN/MAX runs
+ * its global-table kernels only. */
 #define KRV_AGG_COUNT_STAR 0
 #define KRV_AGG_COUNT 1
 #define KRV_AGG_SUM 2

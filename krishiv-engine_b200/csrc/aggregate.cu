@@ -30,6 +30,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <tuple>
 
 #include "krv_device.cuh"
 #include "ops.h"
@@ -47,7 +48,11 @@ constexpr int kMaxValueCols = 16;
 // F_WIDE: MIN/MAX of a decimal128 column of precision 19 to 38, kept in 16
 // bytes (lo, hi) and updated by 128-bit compare-and-swap; such a plan runs
 // the global-table kernels only.
-enum : int32_t { F_SUM = 1, F_MIN = 2, F_MAX = 4, F_WIDE = 8 };
+// F_STR: MIN/MAX of a UTF-8 or binary column, whose values arrive as codes
+// of a value dictionary; a record keeps the best code (-1: none yet),
+// replaced by compare-and-swap after a byte-wise compare of the strings.
+// Such a plan, too, runs the global-table kernels only.
+enum : int32_t { F_SUM = 1, F_MIN = 2, F_MAX = 4, F_WIDE = 8, F_STR = 16 };
 
 struct AggColDev {
     const void *data;
@@ -56,6 +61,10 @@ struct AggColDev {
     int32_t type;  // Type
     int32_t flags;
     int32_t off_count, off_sum, off_min, off_max;
+    // F_STR: the value dictionary's strings (start, length per code; bytes)
+    const long long *s_off;
+    const int32_t *s_len;
+    const uint8_t *s_heap;
 };
 struct AggPlanDev {
     AggColDev c[kMaxValueCols];
@@ -131,10 +140,47 @@ __device__ __forceinline__ void plain_minmax_i128(unsigned long long *p, unsigne
     }
 }
 
+// Byte-wise order of two dictionary strings (Spark orders strings and binary
+// by their unsigned bytes, a prefix first).
+__device__ __forceinline__ int str_cmp(const AggColDev &C, long long a, long long b) {
+    const uint8_t *pa = C.s_heap + C.s_off[a], *pb = C.s_heap + C.s_off[b];
+    const int la = C.s_len[a], lb = C.s_len[b];
+    const int m = la < lb ? la : lb;
+    for (int i = 0; i < m; i++)
+        if (pa[i] != pb[i]) return pa[i] < pb[i] ? -1 : 1;
+    return la < lb ? -1 : la > lb ? 1 : 0;
+}
+// MIN (or MAX) of string code `v` into the record's code slot: swap while
+// the stored code's string is worse. Each failed swap saw a better stored
+// value, so the loop ends; the bound is a guard only.
+__device__ __forceinline__ void atomic_minmax_str(const AggColDev &C, uint8_t *slot, long long v, bool is_max) {
+    unsigned long long *p = reinterpret_cast<unsigned long long *>(slot);
+    long long cur = *reinterpret_cast<volatile long long *>(p);
+    for (int it = 0; it < (1 << 20); it++) {
+        if (cur == v) return;
+        if (cur >= 0) {
+            const int c = str_cmp(C, v, cur);
+            if (is_max ? c <= 0 : c >= 0) return;
+        }
+        const long long old = (long long)atomicCAS(p, (unsigned long long)cur, (unsigned long long)v);
+        if (old == cur) return;
+        cur = old;
+    }
+}
+__device__ __forceinline__ void plain_minmax_str(const AggColDev &C, uint8_t *slot, long long v, bool is_max) {
+    long long *p = reinterpret_cast<long long *>(slot);
+    if (*p < 0 || (is_max ? str_cmp(C, v, *p) > 0 : str_cmp(C, v, *p) < 0)) *p = v;
+}
+
 __device__ __forceinline__ void init_record(const AggPlanDev &P, uint8_t *r) {
     for (int b = 0; b < P.rec; b += 8) *reinterpret_cast<unsigned long long *>(r + b) = 0ull;
     for (int c = 0; c < P.ncols; c++) {
         const AggColDev &C = P.c[c];
+        if (C.flags & F_STR) {
+            if (C.flags & F_MIN) *reinterpret_cast<long long *>(r + C.off_min) = -1;
+            if (C.flags & F_MAX) *reinterpret_cast<long long *>(r + C.off_max) = -1;
+            continue;
+        }
         if (C.flags & F_WIDE) {
             unsigned long long *mn = reinterpret_cast<unsigned long long *>(r + C.off_min);
             unsigned long long *mx = reinterpret_cast<unsigned long long *>(r + C.off_max);
@@ -163,6 +209,12 @@ __device__ __forceinline__ void update_record(const AggPlanDev &P, uint8_t *r, i
         const AggColDev &C = P.c[c];
         if (!bit_get(C.valid, C.voff, i)) continue;
         atomicAdd(reinterpret_cast<unsigned long long *>(r + C.off_count), 1ull);
+        if (C.flags & F_STR) {
+            const long long code = static_cast<const long long *>(C.data)[i];
+            if (C.flags & F_MIN) atomic_minmax_str(C, r + C.off_min, code, false);
+            if (C.flags & F_MAX) atomic_minmax_str(C, r + C.off_max, code, true);
+            continue;
+        }
         if (C.type == (int)Type::I32 || C.type == (int)Type::Date32) {
             const int v = static_cast<const int *>(C.data)[i];
             if (C.flags & F_SUM) atomicAdd(reinterpret_cast<unsigned long long *>(r + C.off_sum), (unsigned long long)(long long)v);
@@ -211,6 +263,12 @@ __device__ __forceinline__ void update_record_plain(const AggPlanDev &P, uint8_t
         const AggColDev &C = P.c[c];
         if (!bit_get(C.valid, C.voff, i)) continue;
         *reinterpret_cast<unsigned long long *>(r + C.off_count) += 1ull;
+        if (C.flags & F_STR) {
+            const long long code = static_cast<const long long *>(C.data)[i];
+            if (C.flags & F_MIN) plain_minmax_str(C, r + C.off_min, code, false);
+            if (C.flags & F_MAX) plain_minmax_str(C, r + C.off_max, code, true);
+            continue;
+        }
         if (C.type == (int)Type::I32 || C.type == (int)Type::Date32) {
             const int v = static_cast<const int *>(C.data)[i];
             if (C.flags & F_SUM) *reinterpret_cast<long long *>(r + C.off_sum) += (long long)v;
@@ -296,6 +354,11 @@ __device__ __forceinline__ void merge_record(const AggPlanDev &P, uint8_t *dst, 
         const unsigned long long cnt = *reinterpret_cast<const unsigned long long *>(src + C.off_count);
         if (!cnt) continue;
         atomicAdd(reinterpret_cast<unsigned long long *>(dst + C.off_count), cnt);
+        if (C.flags & F_STR) {
+            if (C.flags & F_MIN) atomic_minmax_str(C, dst + C.off_min, *reinterpret_cast<const long long *>(src + C.off_min), false);
+            if (C.flags & F_MAX) atomic_minmax_str(C, dst + C.off_max, *reinterpret_cast<const long long *>(src + C.off_max), true);
+            continue;
+        }
         if (C.type == (int)Type::I32 || C.type == (int)Type::Date32) {
             if (C.flags & F_SUM)
                 atomicAdd(reinterpret_cast<unsigned long long *>(dst + C.off_sum),
@@ -1895,6 +1958,7 @@ class HashAggregate {
     // dictionary gives each key a dense int64 code, appended to every batch
     // as column key_col_ and aggregated as the key.
     KeyDict *dict_ = nullptr;
+    std::vector<KeyDict *> vdicts_;  // per plan column: the value dictionary of a string MIN/MAX column
     std::vector<int> dict_cols_;
     int key_col_ = -1;
     // Plan columns of each aggregate (col, aux: see OutExprDev) and the
@@ -1906,6 +1970,8 @@ class HashAggregate {
   public:
     ~HashAggregate() {
         if (dict_) key_dict_destroy(dict_);
+        for (KeyDict *d : vdicts_)
+            if (d) key_dict_destroy(d);
     }
 
   private:
@@ -2001,15 +2067,20 @@ void HashAggregate::plan(const DevBatch &b) {
     // Merges of decimal SUM states add a hidden int64 column per state pair:
     // 1 where the state overflowed (its sum NULL, its nonempty flag set).
     const int hidden_base = (int)b.cols.size() + (dict_ ? 1 : 0);
+    std::vector<int32_t> flags;
     auto type_of = [&](int col) -> DType {
         if (col >= hidden_base) return DType{Type::I64, 0, 0};
-        // a UTF-8 / binary column counted by COUNT: its int32 offsets stand in
-        // for values (never read: only the validity counts)
-        if (b.cols[col].type.var()) return DType{Type::I32, 0, 0};
+        // a UTF-8 / binary column: for MIN/MAX its value dictionary's int64
+        // codes; counted by COUNT alone, its int32 offsets stand in for values
+        // (never read: only the validity counts)
+        if (b.cols[col].type.var()) {
+            for (size_t i = 0; i < value_cols_.size(); i++)
+                if (value_cols_[i] == col && (flags[i] & F_STR)) return DType{Type::I64, 0, 0};
+            return DType{Type::I32, 0, 0};
+        }
         return b.cols[col].type;
     };
     P_.ncols = 0;
-    std::vector<int32_t> flags;
     auto plan_col = [&](int col, int32_t flag) -> int {
         int at = -1;
         for (size_t i = 0; i < value_cols_.size(); i++)
@@ -2043,9 +2114,14 @@ void HashAggregate::plan(const DevBatch &b) {
         if (x.input != KRV_AGG_INPUT_RAW && !state) fail(KRV_INVALID_ARGUMENT, "unknown aggregate input");
         if (!state) {
             if (x.function == KRV_AGG_COUNT_STAR) continue;
-            if (x.function == KRV_AGG_COUNT && b.cols[std::max(0, std::min(x.column, (int)b.cols.size() - 1))].type.var()) {
+            const bool var_arg = x.column >= 0 && x.column < (int)b.cols.size() && b.cols[x.column].type.var();
+            if (x.function == KRV_AGG_COUNT && var_arg) {
                 check_counted(x.column);
                 expr_col_[e] = plan_col(x.column, 0);
+                continue;
+            }
+            if ((x.function == KRV_AGG_MIN || x.function == KRV_AGG_MAX) && var_arg) {
+                expr_col_[e] = plan_col(x.column, (x.function == KRV_AGG_MIN ? F_MIN : F_MAX) | F_STR);
                 continue;
             }
             const DType t = check_col(x.column);
@@ -2058,6 +2134,11 @@ void HashAggregate::plan(const DevBatch &b) {
             continue;
         }
         // Partial states (AggregateExpr::merging, aggregate/mod.rs:561-569).
+        if ((x.function == KRV_AGG_MIN || x.function == KRV_AGG_MAX) && x.column >= 0 &&
+            x.column < (int)b.cols.size() && b.cols[x.column].type.var()) {
+            expr_col_[e] = plan_col(x.column, (x.function == KRV_AGG_MIN ? F_MIN : F_MAX) | F_STR);
+            continue;
+        }
         const DType t = check_col(x.column);
         const bool dec = t.id == Type::Dec64 || t.id == Type::Dec128;
         switch (x.function) {
@@ -2159,7 +2240,17 @@ void HashAggregate::plan(const DevBatch &b) {
     smem_entries_ = e >= 64 ? e : 0;
     if (smem_entries_ == 0) mode_ = KRV_AGG_MODE_GLOBAL;
     for (int c = 0; c < P_.ncols; c++)
-        if (P_.c[c].flags & F_WIDE) mode_ = KRV_AGG_MODE_GLOBAL;  // 128-bit MIN/MAX: the global-table kernels
+        if (P_.c[c].flags & (F_WIDE | F_STR)) mode_ = KRV_AGG_MODE_GLOBAL;  // 128-bit or string MIN/MAX: global kernels
+    // a value dictionary per string MIN/MAX column
+    vdicts_.assign(P_.ncols, nullptr);
+    for (int c = 0; c < P_.ncols; c++)
+        if (P_.c[c].flags & F_STR) {
+            DevCol m;
+            m.type = b.cols[value_cols_[c]].type;
+            m.name = b.cols[value_cols_[c]].name;
+            m.nullable = true;
+            vdicts_[c] = make_key_dict(rt_, {m});
+        }
     plan_row_records();
     const uint64_t hint = spec_.expected_groups > 0 ? (uint64_t)spec_.expected_groups : 65536;
     alloc_table(std::max<uint64_t>(1024, next_pow2((uint64_t)(hint * 2))));
@@ -2656,6 +2747,15 @@ void HashAggregate::push(const DevBatch &in) {
         cc.data = codes.get();
         b.cols.push_back(cc);
     }
+    // string MIN/MAX columns: their values as codes of the column's value dictionary
+    std::vector<DBuf> vcodes;
+    for (int c = 0; c < P_.ncols; c++) {
+        if (!(P_.c[c].flags & F_STR)) continue;
+        const int col = value_cols_[c];
+        vcodes.push_back(key_dict_encode(vdicts_[c], in, {col}, true));
+        b.cols[col].data = vcodes.back().get();
+        key_dict_strings(vdicts_[c], &P_.c[c].s_off, &P_.c[c].s_len, &P_.c[c].s_heap);
+    }
     std::vector<DBuf> hidden;
     for (const auto &ps : poison_src_) {
         const DevCol &sc = in.cols[ps.first], &nc = in.cols[ps.second];
@@ -2711,6 +2811,15 @@ void HashAggregate::push(const DevBatch &in) {
     }
     fail(KRV_INTERNAL, "aggregate: table growth did not converge");
 }
+
+namespace {
+// A code where the group has no value (validity bit clear): 0, which names
+// some stored string, so that the gather reads inside the dictionary.
+__global__ void str_code_clean_kernel(long long *codes, const uint8_t *valid, int64_t n) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+        if (!valid || !((valid[j >> 3] >> (j & 7)) & 1) || codes[j] < 0) codes[j] = 0;
+}
+}  // namespace
 
 DevBatch HashAggregate::result() {
     DeviceGuard g(rt_);
@@ -2807,9 +2916,16 @@ DevBatch HashAggregate::result() {
     }
     if ((int)outs.size() > kMaxExprs) fail(KRV_UNSUPPORTED, "more than 32 output columns of aggregates");
     O.n = (int)outs.size();
+    // string MIN/MAX outputs: (position in out.cols, output spec, plan column),
+    // finalized as codes and then gathered from the value dictionary
+    std::vector<std::tuple<int, OutSpec, int>> str_outs;
     for (int e = 0; e < O.n; e++) {
-        const OutSpec &o = outs[e];
+        OutSpec o = outs[e];
         OutExprDev &X = O.e[e];
+        if ((o.func == KRV_AGG_MIN || o.func == KRV_AGG_MAX) && o.col >= 0 && (P_.c[o.col].flags & F_STR)) {
+            str_outs.emplace_back((int)out.cols.size(), o, o.col);
+            o.type = DType{Type::I64, 0, 0};
+        }
         X.func = o.func;
         X.col = o.col;
         X.aux = o.aux;
@@ -2847,6 +2963,29 @@ DevBatch HashAggregate::result() {
     const uint32_t st = take_status(rt_);
     if (st & ST_OVERFLOW)
         fail(KRV_ARITHMETIC_OVERFLOW, "ARITHMETIC_OVERFLOW: an aggregate overflowed its result type (ANSI mode)");
+    for (const auto &so : str_outs) {
+        const int pos = std::get<0>(so);
+        const OutSpec &o = std::get<1>(so);
+        DevCol codes = out.cols[pos];
+        DevCol col;
+        if (nout > 0) {
+            // groups with no value: a code that exists (their validity stays clear)
+            str_code_clean_kernel<<<grid_for(rt_, nout, 256, 8), 256, 0, rt_->stream>>>(
+                static_cast<long long *>(const_cast<void *>(codes.data)), codes.valid, nout);
+            rt_->launches++;
+            check_launch("str_code_clean_kernel");
+            col = key_dict_decode(vdicts_[std::get<2>(so)], static_cast<const long long *>(codes.data), nout)[0];
+            col.hold_valid = codes.hold_valid;
+            col.valid = codes.valid;
+            col.valid_off = 0;
+        } else {
+            col = var_gather(rt_, VarSrc{}, nullptr, 0, o.type, true, o.name);
+        }
+        col.name = o.name;
+        col.nullable = true;
+        out.cols[pos] = col;
+    }
+    if (!str_outs.empty()) KRV_CUDA(cudaStreamSynchronize(rt_->stream));  // the codes are read by the gathers
     if (dict_) {
         // the group-by columns in place of the codes
         std::vector<DevCol> keys = key_dict_decode(dict_, static_cast<const long long *>(out.cols[0].data), out.rows);

@@ -300,6 +300,12 @@ class KeyDict {
     }
 
     int64_t size() const { return count_; }
+    // Device views of column 0's stored strings (valid until the next encode).
+    void strings(const long long **off, const int32_t **len, const uint8_t **heap) const {
+        *off = store_[0].str_off.as<long long>();
+        *len = store_[0].str_len.as<int32_t>();
+        *heap = heap_.as<uint8_t>();
+    }
 
     // The int64 code of each row's key (columns `cols` of b); unseen keys get
     // new codes (insert) or -1 (lookup only).
@@ -533,5 +539,8 @@ DBuf key_dict_encode(KeyDict *d, const DevBatch &b, const std::vector<int> &cols
 }
 std::vector<DevCol> key_dict_decode(KeyDict *d, const long long *codes, int64_t n) { return d->decode(codes, n); }
 int64_t key_dict_size(const KeyDict *d) { return d->size(); }
+void key_dict_strings(const KeyDict *d, const long long **off, const int32_t **len, const uint8_t **heap) {
+    d->strings(off, len, heap);
+}
 
 }  // namespace krv

@@ -72,6 +72,7 @@ void key_dict_destroy(KeyDict *d);
 DBuf key_dict_encode(KeyDict *d, const DevBatch &b, const std::vector<int> &cols, bool insert = true);
 std::vector<DevCol> key_dict_decode(KeyDict *d, const long long *codes, int64_t n);
 int64_t key_dict_size(const KeyDict *d);
+void key_dict_strings(const KeyDict *d, const long long **off, const int32_t **len, const uint8_t **heap);
 
 // ---- residual join filter, device form (join/probe.rs:425-436) -------------------
 // A conjunction of comparisons; a pair counts only where every one is TRUE
