@@ -88,3 +88,39 @@ def test_scan_reads_every_passing_row(tmp_path):
         assert got == want
         assert scan.stats["row_groups"] == 30 and scan.stats["row_groups_read"] <= 30
         assert scan.stats["rows_read"] == 700 * scan.stats["row_groups_read"]
+
+
+def test_column_chunk_bytes_and_description(tmp_path):
+    """The bytes the device decoder is handed for a column chunk: from its
+    dictionary page (a dictionary-encoded chunk) or its first data page,
+    `total_compressed_size` bytes, starting with a Thrift compact PageHeader
+    whose first field is the page type (DICTIONARY_PAGE 2, DATA_PAGE 0,
+    DATA_PAGE_V2 3); the description carries the physical type, codec,
+    maximum definition level and value count; the Arrow formats."""
+    S = importlib.import_module("krishiv-engine_b200.scan")
+    n = 10_000
+    t = pa.table({"k": pa.array(np.arange(n) % 7, type=pa.int64()),
+                  "x": pa.array(np.linspace(0, 1, n)),
+                  "s": pa.array([None if i % 5 == 0 else "v%d" % (i % 3) for i in range(n)]),
+                  "r": pa.array(np.arange(n, dtype=np.int32))})
+    schema = pa.schema([pa.field("k", pa.int64()), pa.field("x", pa.float64()), pa.field("s", pa.string()),
+                        pa.field("r", pa.int32(), nullable=False)])
+    t = t.cast(schema)
+    for version, data_type in (("1.0", 0), ("2.0", 3)):
+        path = str(tmp_path / f"c{version}.parquet")
+        pq.write_table(t, path, use_dictionary=["k", "s"], compression="SNAPPY", data_page_version=version)
+        md = pq.ParquetFile(path).metadata
+        with open(path, "rb") as f:
+            for ci, (phys, dict_, max_def) in enumerate(((2, True, 1), (5, False, 1), (6, True, 1), (1, False, 0))):
+                data, d = S.column_chunk(f, md, 0, ci)
+                cc = md.row_group(0).column(ci)
+                assert len(data) == cc.total_compressed_size
+                assert d == {"physical_type": phys, "codec": 1, "max_def_level": max_def, "num_values": n}
+                # field 1 (delta 1, i32) of the PageHeader: the page type, zigzag-coded
+                assert data[0] == 0x15 and data[1] == 2 * (2 if dict_ else data_type)
+    fmt = {pa.int32(): "i", pa.int64(): "l", pa.float64(): "g", pa.date32(): "tdD", pa.string(): "u",
+           pa.binary(): "z", pa.decimal128(15, 2): "d:15,2"}
+    for typ, want in fmt.items():
+        assert S.arrow_format(typ) == want
+    with pytest.raises(ValueError):
+        S.arrow_format(pa.list_(pa.int64()))
