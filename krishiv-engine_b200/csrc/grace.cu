@@ -491,11 +491,15 @@ class GraceJoin {
         // build row: padded now (left outer), never partitioned or spilled.
         Segment &ruled_out = segs[nparts_ + 1];
         counters_filtered_ += last_filtered_;
-        if (ruled_out.rows > 0 && spec_.join_type == KRV_JOIN_LEFT_OUTER) {
-            out_rows += ruled_out.rows;
-            keep(out, null_join_->probe(ruled_out.batch));
-        }
         const int64_t out_cap = budget_ / 8 / out_row_bytes();
+        if (ruled_out.rows > 0 && spec_.join_type == KRV_JOIN_LEFT_OUTER) {
+            if (out_rows + ruled_out.rows > out_cap) {
+                pad_later_.push_back(spill(ruled_out));  // past this call's output share: padded at finish
+            } else {
+                out_rows += ruled_out.rows;
+                keep(out, null_join_->probe(ruled_out.batch));
+            }
+        }
         const double ratio = out_ratio();
         std::vector<int> now;  // resident partitions joined by this slice's launch
         double expect = 0;
@@ -658,6 +662,15 @@ class GraceJoin {
             for (int p = 0; p < nparts_; p++)
                 if (parts_[p].spilled) tasks_.push_back(Task{0, std::move(parts_[p].build_host), std::move(parts_[p].probe_host)});
         }
+        // Ruled-out rows that did not fit their call's output: padded now.
+        while (pad_chunk_ < pad_later_.size()) {
+            DevBatch o = null_join_->probe(load_group(pad_later_, pad_chunk_));
+            counters_.output_rows += o.rows;
+            if (o.rows > 0) {
+                out = o;
+                return true;
+            }
+        }
         // Deferred rows of resident partitions, by their resident tables.
         for (; deferred_part_ < nparts_; deferred_part_++, deferred_chunk_ = 0) {
             Part &P = parts_[deferred_part_];
@@ -719,7 +732,8 @@ class GraceJoin {
     }
 
     bool done() const {
-        return finishing_ && deferred_part_ >= nparts_ && !cur_join_ && tasks_.empty() && !fb_.active;
+        return finishing_ && pad_chunk_ >= pad_later_.size() && deferred_part_ >= nparts_ && !cur_join_ &&
+               tasks_.empty() && !fb_.active;
     }
     // A zero-row batch of the output's shape.
     DevBatch empty_output() {
@@ -1302,6 +1316,8 @@ class GraceJoin {
     uint64_t bloom_blocks_ = 0;
     int64_t counters_filtered_ = 0;
     int64_t last_filtered_ = 0;  // rows the last partition pass's filter ruled out
+    std::vector<HostChunk> pad_later_;  // ruled-out probe rows past a call's output share (left outer)
+    size_t pad_chunk_ = 0;
     bool schema_ = false, built_ = false, finishing_ = false;
     std::vector<DevCol> build_types_, probe_types_;
     int64_t row_bytes_ = 0;
