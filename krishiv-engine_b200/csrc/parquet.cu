@@ -23,9 +23,13 @@
 //    hybrid: one thread lists the runs a tile needs, every thread decodes
 //    its rows from them), ranks the tile's non-NULL rows with a block scan,
 //    and writes the Arrow column, its validity and the filter's bit per row
-//    (a dictionary entry's answer, or the member test of a PLAIN value).
+//    (a dictionary entry's answer, or the member test of a PLAIN value);
+//  - BYTE_ARRAY columns: ba_walk_kernel walks the PLAIN values of the
+//    dictionary page and of PLAIN data pages into a (start, length) table,
+//    page_decode_kernel writes each row's reference into it, and the string
+//    gather of the join's payloads makes the UTF-8 / binary column.
 // Flat columns only (max repetition level 0, max definition level 0 or 1);
-// physical types INT32, INT64 and DOUBLE; PLAIN, PLAIN_DICTIONARY and
+// physical types INT32, INT64, DOUBLE and BYTE_ARRAY; PLAIN, PLAIN_DICTIONARY and
 // RLE_DICTIONARY values; UNCOMPRESSED and SNAPPY chunks; data pages v1 and
 // v2. Anything else returns KRV_UNSUPPORTED; bytes that do not decode return
 // KRV_INVALID_ARGUMENT. Kernels read only inside their page's bytes.
