@@ -289,3 +289,24 @@ def test_sharded_join_exchange_on_two_gloo_ranks(oracle, jt):
     nbytes = oracle.bloom_bytes_for(40_000, 0.01)
     all_words = oracle.bloom_build(oracle.xxh64_int(cat[0][cat[1]]), nbytes)
     assert np.array_equal(got[0][3], all_words) and np.array_equal(got[1][3], all_words)
+
+
+def test_join_owner_is_balanced_and_keeps_null_keys_local(oracle):
+    """The owner of a row is the top bits of its key hash h scaled to the
+    world size: every rank gets a near-equal share of distinct keys, equal
+    keys one owner, and a NULL key stays on the rank that holds it."""
+    import numpy as np
+    import torch
+    shard = importlib.import_module("krishiv-engine_b200.shard")
+    rng = np.random.default_rng(3)
+    keys = rng.integers(0, 1 << 40, 200_000).astype(np.int64)
+    valid = rng.random(keys.size) > 0.01
+    h = torch.tensor(oracle.row_hash([(keys, valid.astype(np.uint8), False)]).view(np.int64))
+    for world in (2, 3, 8):
+        o = shard.join_owner(h, torch.tensor(valid), world, rank=1)
+        assert int(o.min()) >= 0 and int(o.max()) < world
+        assert bool((o[~torch.tensor(valid)] == 1).all())
+        counts = torch.bincount(o[torch.tensor(valid)], minlength=world).double()
+        assert float(counts.max() / counts.min()) < 1.05
+        dup = shard.join_owner(h[:1000].clone(), torch.tensor(valid[:1000]), world, rank=1)
+        assert torch.equal(dup, o[:1000])
