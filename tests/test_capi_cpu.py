@@ -158,3 +158,14 @@ def test_merging_specs(kb):
         ("sum", "state", 1), ("min", "state", 2), ("avg", "state", 3, 4), ("count", "state", 5), ("max", "state", 6)]
     s = kb.agg_spec([0, 1], kb.merging(q1, 2, types))
     assert s.aggregates[4].arg_bits == 128 and s.aggregates[0].column2 == 3
+
+
+def test_option_defaults(kb):
+    """The partitioned join's options: the device budget from the runtime
+    and a Bloom filter of 10 bits per build key in the partition pass."""
+    import ctypes as C
+    o = kb.GraceOptions()
+    o.probe_filter_bits = -1
+    kb.lib().krv_grace_options_init(C.byref(o))
+    assert o.device_budget_bytes == 0 and o.probe_filter_bits == 10
+    assert (kb.PQ_INT32, kb.PQ_INT64, kb.PQ_DOUBLE, kb.PQ_BYTE_ARRAY) == (1, 2, 5, 6)  # parquet.thrift Type
